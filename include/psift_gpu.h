@@ -1,0 +1,128 @@
+/*
+ * psift_gpu.h -- C ABI of libpsift_gpu.so, the sm_100a (B200) implementation of
+ * pure-sift's feature hot path.
+ *
+ * The reference exposes this path as a Rust API (src/lib.rs:26-52) with no FFI
+ * of its own.  Each entry point below names the reference function it replaces;
+ * a Rust binding crate maps the reference's structs onto
+ * these plain-pointer signatures so `Sift::detect_and_compute`, `Matcher::match_`,
+ * `Homography::estimate` and the catalog search keep their signatures.
+ *
+ * Conventions
+ *  - Every call returns psift_status; nothing aborts.  A failing call leaves a
+ *    message retrievable with psift_last_error(ctx).
+ *  - Pointers are HOST memory unless the function name ends in `_dev`, in which
+ *    case every array argument is device memory on the context's GPU.
+ *  - Outputs are caller-owned.  When an output would exceed the capacity the
+ *    caller gave, the call returns PSIFT_ERR_CAPACITY and stores the required
+ *    size in the `count` field / out-parameter.
+ *  - A context owns one CUDA stream and its workspaces; it is not thread-safe.
+ *    Use one context per host thread.
+ *  - There is no CPU fallback: without a usable CUDA device psift_ctx_create
+ *    returns PSIFT_ERR_NO_DEVICE.
+ */
+#ifndef PSIFT_GPU_H
+#define PSIFT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSIFT_DESCRIPTOR_LEN 128u          /* SIFT_DESCRIPTOR_LEN, src/pipeline.rs:1000 */
+#define PSIFT_MAX_FEATURES_PER_IMAGE 4096u /* MAX_FEATURES_PER_IMAGE, src/pipeline.rs:1054 */
+
+typedef enum psift_status {
+  PSIFT_OK = 0,
+  PSIFT_ERR_INVALID_ARGUMENT = 1, /* null pointer, zero size, bad enum */
+  PSIFT_ERR_INVALID_CONFIG = 2,   /* SiftConfig::validate / Matcher::new / RansacOptions::validate failed */
+  PSIFT_ERR_CAPACITY = 3,         /* output larger than the caller's capacity (required size reported) */
+  PSIFT_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+  PSIFT_ERR_OUT_OF_MEMORY = 5,    /* device or pinned allocation failed */
+  PSIFT_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up */
+  PSIFT_ERR_NO_DEVICE = 7,        /* no usable sm_100 device */
+  PSIFT_ERR_INTERNAL = 8
+} psift_status;
+
+typedef struct psift_ctx psift_ctx;
+
+/* SiftConfig (src/pipeline.rs:22-104) plus the feature cap that
+ * extract_sift_features_with_kind applies (src/pipeline.rs:1643-1656). */
+typedef struct psift_sift_config {
+  uint32_t octaves;            /* 1..=8, default 3 */
+  uint32_t scales;             /* 3..=10, default 3 */
+  float contrast_threshold;    /* (0, 1], default 0.015 */
+  int32_t upsample_first_octave; /* default 1 */
+  int32_t descriptor_kind;     /* 0 = Sift (default), 1 = RootSift */
+  uint32_t max_features;       /* default 4096 (the reference's cap); 0 = uncapped */
+} psift_sift_config;
+
+/* Keypoint (src/pipeline.rs:252-267). */
+typedef struct psift_keypoint {
+  float x, y, scale, response;
+  uint32_t octave, layer;
+} psift_keypoint;
+
+/* Structure-of-arrays SiftFeature list (src/pipeline.rs:1059-1072). */
+typedef struct psift_features {
+  uint32_t capacity;   /* in: number of features the arrays can hold */
+  uint32_t count;      /* out: features produced (or required, on PSIFT_ERR_CAPACITY) */
+  float* x;
+  float* y;
+  float* scale;
+  float* response;
+  float* orientation;
+  float* descriptors;  /* capacity * 128, row-major */
+} psift_features;
+
+/* ---------------------------------------------------------------- context */
+psift_status psift_ctx_create(int device, psift_ctx** out);
+psift_status psift_ctx_destroy(psift_ctx* ctx);
+const char* psift_last_error(const psift_ctx* ctx);
+/* Number of this library's kernel launches issued on the context so far. */
+uint64_t psift_ctx_launch_count(const psift_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t) for event timing / interop. */
+void* psift_ctx_stream(const psift_ctx* ctx);
+psift_status psift_ctx_synchronize(psift_ctx* ctx);
+
+/* ---------------------------------------------------------------- config */
+/* SiftConfig::default() (src/pipeline.rs:36-46) with max_features = 4096. */
+void psift_sift_config_default(psift_sift_config* cfg);
+/* SiftConfig::validate (src/pipeline.rs:80-103); message copied into msg. */
+psift_status psift_sift_config_validate(const psift_sift_config* cfg, char* msg, size_t msg_capacity);
+
+/* ---------------------------------------------------------------- SIFT */
+/* Sift::detect_and_compute (src/pipeline.rs:136-145) on a row-major f32 image
+ * (luma in [0, 1], `Array2<f32>`); row_stride in elements (>= width). */
+psift_status psift_detect_and_compute(psift_ctx* ctx, const float* image, uint32_t height,
+                                      uint32_t width, size_t row_stride,
+                                      const psift_sift_config* cfg, psift_features* out);
+/* Same, from u8 luma; fuses luma_to_array2 (src/pipeline.rs:957-966). */
+psift_status psift_detect_and_compute_u8(psift_ctx* ctx, const uint8_t* luma, uint32_t height,
+                                         uint32_t width, size_t row_stride,
+                                         const psift_sift_config* cfg, psift_features* out);
+/* Sift::detect_keypoints (src/pipeline.rs:125-133). */
+psift_status psift_detect_keypoints(psift_ctx* ctx, const float* image, uint32_t height,
+                                    uint32_t width, size_t row_stride,
+                                    const psift_sift_config* cfg, psift_keypoint* out,
+                                    uint32_t capacity, uint32_t* count);
+
+/* Device-resident batch: `n` u8 images already in device memory, results left
+ * in device memory (feature SoA pointers in outs[i] are device pointers) and the
+ * per-image feature counts written to the device array d_counts.  No host
+ * synchronisation; work is queued on the context's stream. */
+typedef struct psift_image_u8 {
+  const uint8_t* data;   /* device pointer */
+  uint32_t height, width;
+  size_t row_stride;     /* elements */
+} psift_image_u8;
+psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_image_u8* images,
+                                                uint32_t n, const psift_sift_config* cfg,
+                                                psift_features* outs, uint32_t* d_counts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSIFT_GPU_H */

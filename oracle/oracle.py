@@ -1,0 +1,336 @@
+"""ctypes binding of the CPU restatement (``oracle/psift_oracle.cpp``).
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA build.  Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference leg import
+this module.  The product library never calls it.
+
+Parity pinning: the reference (Rust) cannot be built here and ships no numeric
+golden vectors; the restatement is pinned by the reference's own known-answer and
+property tests, ported in ``tests/test_oracle_pins.py``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libpsift_oracle.so")
+_lock = threading.Lock()
+_lib = None
+
+
+class Keypoint(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("scale", C.c_float), ("response", C.c_float),
+                ("octave", C.c_uint32), ("layer", C.c_uint32)]
+
+
+class Match(C.Structure):
+    _fields_ = [("query_index", C.c_uint32), ("target_index", C.c_uint32),
+                ("qx", C.c_float), ("qy", C.c_float), ("tx", C.c_float), ("ty", C.c_float),
+                ("distance", C.c_float), ("ratio", C.c_float), ("dx", C.c_float), ("dy", C.c_float)]
+
+
+class Tracking(C.Structure):
+    _fields_ = [("raw_match_count", C.c_uint32), ("match_count", C.c_uint32),
+                ("inlier_ratio", C.c_float), ("mean_dx", C.c_float), ("mean_dy", C.c_float),
+                ("median_dx", C.c_float), ("median_dy", C.c_float),
+                ("mean_scale_ratio", C.c_float), ("mean_rotation_deg", C.c_float)]
+
+
+KEYPOINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("scale", "<f4"), ("response", "<f4"),
+                           ("octave", "<u4"), ("layer", "<u4")])
+MATCH_DTYPE = np.dtype([("query_index", "<u4"), ("target_index", "<u4"), ("qx", "<f4"), ("qy", "<f4"),
+                        ("tx", "<f4"), ("ty", "<f4"), ("distance", "<f4"), ("ratio", "<f4"),
+                        ("dx", "<f4"), ("dy", "<f4")])
+
+_fp = C.POINTER(C.c_float)
+_u8p = C.POINTER(C.c_uint8)
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_i64p = C.POINTER(C.c_int64)
+_ip = C.POINTER(C.c_int)
+
+
+def build() -> str:
+    """Compile the restatement with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            src = os.path.join(_HERE, "psift_oracle.cpp")
+            if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+                build()
+            L = C.CDLL(_LIB_PATH)
+            L.oracle_gaussian_kernel_1d.argtypes = [C.c_float, _fp, C.c_int]
+            L.oracle_gaussian_kernel_1d.restype = C.c_int
+            L.oracle_gaussian_blur.argtypes = [_fp, C.c_int, C.c_int, C.c_float, _fp]
+            L.oracle_upsample_2x.argtypes = [_fp, C.c_int, C.c_int, _fp]
+            L.oracle_luma_to_f32.argtypes = [_u8p, C.c_size_t, _fp]
+            L.oracle_pyramid_build.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+            L.oracle_pyramid_build.restype = C.c_void_p
+            L.oracle_pyramid_num_octaves.argtypes = [C.c_void_p]
+            L.oracle_pyramid_num_octaves.restype = C.c_int
+            L.oracle_pyramid_octave_info.argtypes = [C.c_void_p, C.c_int, _ip, _ip, _fp]
+            L.oracle_pyramid_copy_plane.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _fp]
+            L.oracle_pyramid_extract_extrema.argtypes = [C.c_void_p, C.c_float, C.c_void_p, C.c_int]
+            L.oracle_pyramid_extract_extrema.restype = C.c_int
+            L.oracle_pyramid_free.argtypes = [C.c_void_p]
+            L.oracle_detect_and_compute.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                                    C.c_int, C.c_int, C.c_int, _fp, _fp, C.c_int]
+            L.oracle_detect_and_compute.restype = C.c_int
+            L.oracle_detect_keypoints.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                                  C.c_int, C.c_void_p, C.c_int]
+            L.oracle_detect_keypoints.restype = C.c_int
+            L.oracle_compute_descriptors.argtypes = [_fp, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                                     _fp, _fp, C.c_int]
+            L.oracle_compute_descriptors.restype = C.c_int
+            L.oracle_rootsift.argtypes = [_fp, _fp]
+            L.oracle_quantize_u8.argtypes = [_fp, C.c_int, _u8p]
+            L.oracle_dequantize_u8.argtypes = [_u8p, C.c_int, _fp]
+            L.oracle_quantize_u128.argtypes = [_fp, C.c_int, _u64p]
+            L.oracle_match_descriptors.argtypes = [_fp, C.c_int, _fp, C.c_int, _fp, _fp, C.c_float, C.c_int,
+                                                   C.c_void_p, C.c_int]
+            L.oracle_match_descriptors.restype = C.c_int
+            L.oracle_similarity_ransac.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_uint64, _u8p, _fp, _ip]
+            L.oracle_similarity_ransac.restype = C.c_int
+            L.oracle_homography_ransac.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_uint64, C.c_uint64,
+                                                   _u8p, _fp, _ip]
+            L.oracle_homography_ransac.restype = C.c_int
+            L.oracle_summarize_tracking.argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp,
+                                                    C.POINTER(Tracking)]
+            L.oracle_hamming_votes.argtypes = [_u64p, C.c_int, _u64p, _i64p, C.c_int, C.c_int, _u32p]
+            L.oracle_hamming_topk.argtypes = [_u64p, C.c_int, _u64p, C.c_int64, C.c_int, _u32p, _u32p]
+            L.oracle_l2_rerank.argtypes = [_fp, C.c_int, _fp, _u32p, C.c_int, _u32p, _fp]
+            L.oracle_splitmix64_next.argtypes = [_u64p]
+            L.oracle_splitmix64_next.restype = C.c_uint64
+            _lib = L
+    return _lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+DEFAULT_SIMILARITY_RANSAC_SEED = 0xD1B54A32D192ED03
+DEFAULT_HOMOGRAPHY_RANSAC_SEED = 0x517CC1B727220A95
+
+
+def gaussian_kernel_1d(sigma: float) -> np.ndarray:
+    out = np.zeros(4096, np.float32)
+    n = lib().oracle_gaussian_kernel_1d(sigma, _p(out, _fp), out.size)
+    return out[:n].copy()
+
+
+def gaussian_blur(img, sigma: float) -> np.ndarray:
+    img = _f32(img)
+    out = np.empty_like(img)
+    lib().oracle_gaussian_blur(_p(img, _fp), img.shape[0], img.shape[1], sigma, _p(out, _fp))
+    return out
+
+
+def upsample_2x(img) -> np.ndarray:
+    img = _f32(img)
+    out = np.empty((img.shape[0] * 2, img.shape[1] * 2), np.float32)
+    lib().oracle_upsample_2x(_p(img, _fp), img.shape[0], img.shape[1], _p(out, _fp))
+    return out
+
+
+def luma_to_f32(u8) -> np.ndarray:
+    u8 = np.ascontiguousarray(u8, dtype=np.uint8)
+    out = np.empty(u8.shape, np.float32)
+    lib().oracle_luma_to_f32(_p(u8, _u8p), u8.size, _p(out, _fp))
+    return out
+
+
+class Pyramid:
+    """Gaussian/DoG pyramid exactly as the reference materialises it."""
+
+    def __init__(self, img, octaves=3, scales=3, upsample=True):
+        img = _f32(img)
+        self.scales = scales
+        self._h = lib().oracle_pyramid_build(_p(img, _fp), img.shape[0], img.shape[1], octaves, scales,
+                                             int(bool(upsample)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().oracle_pyramid_free(self._h)
+            self._h = None
+
+    @property
+    def num_octaves(self) -> int:
+        return lib().oracle_pyramid_num_octaves(self._h)
+
+    def octave_info(self, o):
+        h, w, sf = C.c_int(), C.c_int(), C.c_float()
+        lib().oracle_pyramid_octave_info(self._h, o, C.byref(h), C.byref(w), C.byref(sf))
+        return h.value, w.value, sf.value
+
+    def plane(self, o, kind, idx) -> np.ndarray:
+        h, w, _ = self.octave_info(o)
+        out = np.empty((h, w), np.float32)
+        lib().oracle_pyramid_copy_plane(self._h, o, 0 if kind == "g" else 1, idx, _p(out, _fp))
+        return out
+
+    def extract_extrema(self, threshold: float) -> np.ndarray:
+        cap = 1 << 16
+        while True:
+            out = np.zeros(cap, KEYPOINT_DTYPE)
+            n = lib().oracle_pyramid_extract_extrema(self._h, threshold, out.ctypes.data, cap)
+            if n <= cap:
+                return out[:n]
+            cap = n
+
+
+def detect_keypoints(img, octaves=3, scales=3, threshold=0.015, upsample=True) -> np.ndarray:
+    img = _f32(img)
+    cap = 1 << 16
+    while True:
+        out = np.zeros(cap, KEYPOINT_DTYPE)
+        n = lib().oracle_detect_keypoints(_p(img, _fp), img.shape[0], img.shape[1], octaves, scales,
+                                          threshold, int(bool(upsample)), out.ctypes.data, cap)
+        if n <= cap:
+            return out[:n]
+        cap = n
+
+
+def detect_and_compute(img, octaves=3, scales=3, threshold=0.015, upsample=True, kind=0,
+                       max_features=4096):
+    """Returns (meta[n,5] = x, y, scale, response, orientation; desc[n,128])."""
+    img = _f32(img)
+    cap = max(max_features, 1) if max_features > 0 else 1 << 15
+    while True:
+        meta = np.zeros((cap, 5), np.float32)
+        desc = np.zeros((cap, 128), np.float32)
+        n = lib().oracle_detect_and_compute(_p(img, _fp), img.shape[0], img.shape[1], octaves, scales,
+                                            threshold, int(bool(upsample)), int(kind), int(max_features),
+                                            _p(meta, _fp), _p(desc, _fp), cap)
+        if n <= cap:
+            return meta[:n].copy(), desc[:n].copy()
+        cap = n
+
+
+def compute_descriptors(img, keypoints, kind=0):
+    img = _f32(img)
+    kps = np.ascontiguousarray(keypoints, dtype=KEYPOINT_DTYPE)
+    cap = max(4 * len(kps), 1)
+    meta = np.zeros((cap, 5), np.float32)
+    desc = np.zeros((cap, 128), np.float32)
+    n = lib().oracle_compute_descriptors(_p(img, _fp), img.shape[0], img.shape[1], kps.ctypes.data, len(kps),
+                                         int(kind), _p(meta, _fp), _p(desc, _fp), cap)
+    return meta[:n].copy(), desc[:n].copy()
+
+
+def rootsift(desc) -> np.ndarray:
+    d = _f32(desc).reshape(-1, 128)
+    out = np.empty_like(d)
+    for i in range(d.shape[0]):
+        lib().oracle_rootsift(_p(d[i], _fp), _p(out[i], _fp))
+    return out
+
+
+def quantize_u8(desc) -> np.ndarray:
+    d = _f32(desc).ravel()
+    out = np.empty(d.size, np.uint8)
+    lib().oracle_quantize_u8(_p(d, _fp), d.size, _p(out, _u8p))
+    return out.reshape(np.shape(desc))
+
+
+def dequantize_u8(q) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.uint8).reshape(-1, 128)
+    out = np.empty(q.shape, np.float32)
+    for i in range(q.shape[0]):
+        lib().oracle_dequantize_u8(_p(q[i], _u8p), 128, _p(out[i], _fp))
+    return out
+
+
+def quantize_u128(desc) -> np.ndarray:
+    d = _f32(desc).reshape(-1, 128)
+    out = np.empty((d.shape[0], 2), np.uint64)
+    lib().oracle_quantize_u128(_p(d, _fp), d.shape[0], _p(out, _u64p))
+    return out
+
+
+def match(q_desc, t_desc, q_xy, t_xy, ratio=0.75, mutual=False) -> np.ndarray:
+    qd, td = _f32(q_desc).reshape(-1, 128), _f32(t_desc).reshape(-1, 128)
+    qxy, txy = _f32(q_xy).reshape(-1, 2), _f32(t_xy).reshape(-1, 2)
+    cap = max(qd.shape[0], 1)
+    out = np.zeros(cap, MATCH_DTYPE)
+    n = lib().oracle_match_descriptors(_p(qd, _fp), qd.shape[0], _p(td, _fp), td.shape[0], _p(qxy, _fp),
+                                       _p(txy, _fp), ratio, int(bool(mutual)), out.ctypes.data, cap)
+    return out[:n].copy()
+
+
+def similarity_ransac(matches, thr=3.0, seed=DEFAULT_SIMILARITY_RANSAC_SEED):
+    m = np.ascontiguousarray(matches, dtype=MATCH_DTYPE)
+    mask = np.zeros(max(len(m), 1), np.uint8)
+    model = np.zeros(6, np.float32)
+    has = C.c_int()
+    lib().oracle_similarity_ransac(m.ctypes.data, len(m), thr, seed, _p(mask, _u8p), _p(model, _fp),
+                                   C.byref(has))
+    return mask[:len(m)].astype(bool), (model if has.value else None)
+
+
+def homography_ransac(matches, thr=3.0, seed=None):
+    m = np.ascontiguousarray(matches, dtype=MATCH_DTYPE)
+    if seed is None:
+        s1, s2 = DEFAULT_SIMILARITY_RANSAC_SEED, DEFAULT_HOMOGRAPHY_RANSAC_SEED
+    else:
+        s1, s2 = seed, seed ^ 0x9E3779B97F4A7C15
+    mask = np.zeros(max(len(m), 1), np.uint8)
+    h9 = np.zeros(9, np.float32)
+    has = C.c_int()
+    lib().oracle_homography_ransac(m.ctypes.data, len(m), thr, s1, s2, _p(mask, _u8p), _p(h9, _fp),
+                                   C.byref(has))
+    return mask[:len(m)].astype(bool), (h9.reshape(3, 3) if has.value else None)
+
+
+def summarize_tracking(matches, q_scale, q_ori, t_scale, t_ori) -> Tracking:
+    m = np.ascontiguousarray(matches, dtype=MATCH_DTYPE)
+    qs, qo, ts, to = (_f32(a) for a in (q_scale, q_ori, t_scale, t_ori))
+    out = Tracking()
+    lib().oracle_summarize_tracking(m.ctypes.data, len(m), _p(qs, _fp), _p(qo, _fp), _p(ts, _fp),
+                                    _p(to, _fp), C.byref(out))
+    return out
+
+
+def hamming_votes(q_codes, cat_codes, offsets, mih: bool) -> np.ndarray:
+    q = np.ascontiguousarray(q_codes, dtype=np.uint64).reshape(-1, 2)
+    c = np.ascontiguousarray(cat_codes, dtype=np.uint64).reshape(-1, 2)
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    votes = np.zeros(len(off) - 1, np.uint32)
+    lib().oracle_hamming_votes(_p(q, _u64p), q.shape[0], _p(c, _u64p), _p(off, _i64p), len(off) - 1,
+                               int(bool(mih)), _p(votes, _u32p))
+    return votes
+
+
+def hamming_topk(q_codes, cat_codes, k: int):
+    q = np.ascontiguousarray(q_codes, dtype=np.uint64).reshape(-1, 2)
+    c = np.ascontiguousarray(cat_codes, dtype=np.uint64).reshape(-1, 2)
+    idx = np.empty((q.shape[0], k), np.uint32)
+    dist = np.empty((q.shape[0], k), np.uint32)
+    lib().oracle_hamming_topk(_p(q, _u64p), q.shape[0], _p(c, _u64p), c.shape[0], k, _p(idx, _u32p),
+                              _p(dist, _u32p))
+    return idx, dist
+
+
+def l2_rerank(q_desc, cat_desc, cand):
+    qd, cd = _f32(q_desc).reshape(-1, 128), _f32(cat_desc).reshape(-1, 128)
+    cand = np.ascontiguousarray(cand, dtype=np.uint32)
+    k = cand.shape[1]
+    out_idx = np.empty_like(cand)
+    out_d2 = np.empty(cand.shape, np.float32)
+    lib().oracle_l2_rerank(_p(qd, _fp), qd.shape[0], _p(cd, _fp), _p(cand, _u32p), k, _p(out_idx, _u32p),
+                           _p(out_d2, _fp))
+    return out_idx, out_d2

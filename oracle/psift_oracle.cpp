@@ -1,0 +1,1613 @@
+// psift_oracle.cpp -- CPU restatement of pure-sift 0.2.0's feature hot path.
+//
+// TEST INFRASTRUCTURE ONLY (the checker, never the product).  Pinning and the
+// arithmetic rules are described in psift_oracle.h.  Every function names the
+// reference lines it restates (paths are relative to the pure-sift project).
+//
+// Parallelism: OpenMP over exactly the loops the reference hands to rayon
+// (blur rows, DoG slices, gradient levels, keypoints, queries, catalog entries).
+// Every parallel loop writes disjoint, pre-sized outputs, so results are
+// identical for any thread count (reference property: tests/invariance_sweeps.rs:219-244).
+#include "psift_oracle.h"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+namespace {
+
+constexpr float BASE_SIGMA = 1.6f;            // src/pipeline.rs:10
+constexpr float ASSUMED_INPUT_SIGMA = 0.5f;   // src/pipeline.rs:13
+constexpr float PI_F = 3.14159265358979323846f;
+constexpr float SQRT_2_F = 1.41421356237309504880f;
+constexpr size_t DESC_LEN = 128;              // src/pipeline.rs:1000
+constexpr float SECONDARY_ORI_PEAK_RATIO = 0.80f;  // src/pipeline.rs:1155
+constexpr float RAD_TO_DEG_F = 57.2957795130823208767981548141051703f;
+constexpr int PAR_MIN_PIXELS = 16384;         // src/pipeline.rs:381,:410,:901
+
+struct Plane {
+  int h = 0, w = 0;
+  std::vector<float> d;
+  Plane() = default;
+  Plane(int hh, int ww) : h(hh), w(ww), d((size_t)hh * ww, 0.0f) {}
+  float* row(int y) { return d.data() + (size_t)y * w; }
+  const float* row(int y) const { return d.data() + (size_t)y * w; }
+};
+
+struct Octave {
+  std::vector<Plane> g, dog;
+  float scale_factor = 1.0f;
+};
+
+// Rust `f32::rem_euclid`: r = a % b; if r < 0 { r + |b| } else { r }.
+inline float rem_euclid_f(float a, float b) {
+  float r = std::fmod(a, b);
+  return r < 0.0f ? r + std::fabs(b) : r;
+}
+
+// Rust `f32::clamp(lo, hi)`.
+inline float clampf(float x, float lo, float hi) {
+  if (x < lo) x = lo;
+  if (x > hi) x = hi;
+  return x;
+}
+
+// Rust `f32 as isize` / `as usize`: saturating, NaN -> 0.
+inline long long f2i_sat(float v) {
+  if (std::isnan(v)) return 0;
+  if (v >= 9.2233720368547758e18f) return std::numeric_limits<long long>::max();
+  if (v <= -9.2233720368547758e18f) return std::numeric_limits<long long>::min();
+  return (long long)v;
+}
+inline unsigned long long f2u_sat(float v) {
+  if (std::isnan(v) || v <= 0.0f) return 0;
+  if (v >= 1.8446744073709552e19f) return std::numeric_limits<unsigned long long>::max();
+  return (unsigned long long)v;
+}
+inline unsigned long long d2u_sat(double v) {
+  if (std::isnan(v) || v <= 0.0) return 0;
+  if (v >= 1.8446744073709552e19) return std::numeric_limits<unsigned long long>::max();
+  return (unsigned long long)v;
+}
+
+// `f32::powi(i32)` lowers to the compiler runtime's binary exponentiation
+// (square-and-multiply, low bit first); restated here.
+inline float powi_f(float a, int b) {
+  const bool recip = b < 0;
+  float r = 1.0f;
+  for (;;) {
+    if (b & 1) r *= a;
+    b /= 2;
+    if (b == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0f / r : r;
+}
+inline double powi_d(double a, int b) {
+  const bool recip = b < 0;
+  double r = 1.0;
+  for (;;) {
+    if (b & 1) r *= a;
+    b /= 2;
+    if (b == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0 / r : r;
+}
+
+// src/pipeline.rs:275-296
+std::vector<float> gaussian_kernel_1d(float sigma) {
+  const float cs = std::fmax(sigma, 1e-3f);
+  long long radius = f2i_sat(std::ceil(3.0f * cs));
+  if (radius < 1) radius = 1;
+  const float two_sigma_sq = 2.0f * cs * cs;
+  const float norm_factor = 1.0f / (std::sqrt(2.0f * PI_F) * cs);
+  std::vector<float> k;
+  k.reserve((size_t)(2 * radius + 1));
+  for (long long x = -radius; x <= radius; ++x) {
+    const float xf = (float)x;
+    k.push_back(norm_factor * std::exp(-((xf * xf) / two_sigma_sq)));
+  }
+  float sum = 0.0f;
+  for (float v : k) sum += v;
+  if (sum > 0.0f) {
+    const float inv = 1.0f / sum;
+    for (float& v : k) v *= inv;
+  }
+  return k;
+}
+
+// src/pipeline.rs:314-425 (horizontal pass :329-377, vertical AXPY pass :395-406).
+Plane gaussian_blur(const Plane& img, float sigma) {
+  const int h = img.h, w = img.w;
+  if (h == 0 || w == 0) return Plane(h, w);
+  const std::vector<float> kernel = gaussian_kernel_1d(sigma);
+  const int klen = (int)kernel.size();
+  const int radius = klen / 2;
+  const bool par = (long long)h * w >= PAR_MIN_PIXELS;
+
+  Plane temp(h, w);
+#pragma omp parallel for schedule(static) if (par)
+  for (int y = 0; y < h; ++y) {
+    const float* in_row = img.row(y);
+    float* out_row = temp.row(y);
+    for (int x = 0; x < w; ++x) {
+      float acc = 0.0f;
+      for (int k = 0; k < klen; ++k) {
+        int sx = x + k - radius;            // (x + k).saturating_sub(r).min(w-1)
+        if (sx < 0) sx = 0;
+        if (sx > w - 1) sx = w - 1;
+        acc += in_row[sx] * kernel[k];
+      }
+      out_row[x] = acc;
+    }
+  }
+
+  Plane dst(h, w);
+#pragma omp parallel for schedule(static) if (par)
+  for (int y = 0; y < h; ++y) {
+    float* out_row = dst.row(y);
+    for (int k = 0; k < klen; ++k) {
+      int sy = y + k - radius;
+      if (sy < 0) sy = 0;
+      if (sy > h - 1) sy = h - 1;
+      const float* in_row = temp.row(sy);
+      const float wgt = kernel[k];
+      for (int x = 0; x < w; ++x) out_row[x] += in_row[x] * wgt;
+    }
+  }
+  return dst;
+}
+
+// src/pipeline.rs:429-449
+Plane downsample_2x(const Plane& img) {
+  const int nh = img.h / 2, nw = img.w / 2;
+  if (nh == 0 || nw == 0) return Plane(0, 0);
+  Plane out(nh, nw);
+  for (int y = 0; y < nh; ++y)
+    for (int x = 0; x < nw; ++x) out.row(y)[x] = img.row(2 * y)[2 * x];
+  return out;
+}
+
+// src/pipeline.rs:455-483
+Plane upsample_2x_bilinear(const Plane& img) {
+  const int h = img.h, w = img.w;
+  const int nh = h * 2, nw = w * 2;
+  if (nh == 0 || nw == 0) return Plane(0, 0);
+  Plane out(nh, nw);
+  for (int uy = 0; uy < nh; ++uy) {
+    const int y0 = uy / 2;
+    const int y1 = std::min(y0 + (uy & 1), h - 1);
+    const float* r0 = img.row(y0);
+    const float* r1 = img.row(y1);
+    float* o = out.row(uy);
+    for (int ux = 0; ux < nw; ++ux) {
+      const int x0 = ux / 2;
+      const int x1 = std::min(x0 + (ux & 1), w - 1);
+      o[ux] = 0.25f * (r0[x0] + r0[x1] + r1[x0] + r1[x1]);
+    }
+  }
+  return out;
+}
+
+// src/pipeline.rs:550-638
+std::vector<Octave> build_pyramid(const Plane& img, int octaves, int scales, bool upsample) {
+  std::vector<Octave> pyr;
+  if (img.h == 0 || img.w == 0 || octaves == 0 || scales == 0) return pyr;
+  const int dog_slices = scales + 2;
+  const float k = std::pow(2.0f, 1.0f / (float)scales);
+
+  Plane base;
+  float base_mult;
+  if (upsample) {
+    Plane up = upsample_2x_bilinear(img);
+    const float sigma_in = 2.0f * ASSUMED_INPUT_SIGMA;
+    const float init_sigma = std::sqrt(std::fmax(BASE_SIGMA * BASE_SIGMA - sigma_in * sigma_in, 1e-4f));
+    base = gaussian_blur(up, init_sigma);
+    base_mult = 0.5f;
+  } else {
+    const float sigma_in = ASSUMED_INPUT_SIGMA;
+    const float init_sigma = std::sqrt(std::fmax(BASE_SIGMA * BASE_SIGMA - sigma_in * sigma_in, 1e-4f));
+    base = gaussian_blur(img, init_sigma);
+    base_mult = 1.0f;
+  }
+
+  for (int o = 0; o < octaves; ++o) {
+    const int h = base.h, w = base.w;
+    if (h < 3 || w < 3) break;
+    Octave oct;
+    oct.g.push_back(base);
+    float prev_sigma = BASE_SIGMA;
+    for (int s = 1; s <= dog_slices; ++s) {
+      const float target = BASE_SIGMA * powi_f(k, s);
+      const float delta = std::sqrt(std::fmax(target * target - prev_sigma * prev_sigma, 1e-4f));
+      Plane next = gaussian_blur(oct.g.back(), delta);
+      Plane dog(h, w);
+      const Plane& prev = oct.g.back();
+      for (size_t i = 0; i < dog.d.size(); ++i) dog.d[i] = next.d[i] - prev.d[i];
+      oct.dog.push_back(std::move(dog));
+      oct.g.push_back(std::move(next));
+      prev_sigma = target;
+    }
+    if (o + 1 < octaves) base = downsample_2x(oct.g[scales]);
+    else base = oct.g.back();
+    oct.scale_factor = base_mult * (float)(1ull << o);
+    pyr.push_back(std::move(oct));
+  }
+  return pyr;
+}
+
+// src/pipeline.rs:664-687
+bool passes_hessian_edge_test(const Plane& c, int x, int y, float center) {
+  const float* rp = c.row(y - 1);
+  const float* rc = c.row(y);
+  const float* rn = c.row(y + 1);
+  const float dxx = rc[x + 1] - 2.0f * center + rc[x - 1];
+  const float dyy = rn[x] - 2.0f * center + rp[x];
+  const float dxy = 0.25f * ((rn[x + 1] - rn[x - 1]) - (rp[x + 1] - rp[x - 1]));
+  const float trace = dxx + dyy;
+  const float det = dxx * dyy - dxy * dxy;
+  const float threshold_ratio = (11.0f * 11.0f) / 10.0f;
+  return det > 1e-9f && (trace * trace) < threshold_ratio * det;
+}
+
+// src/pipeline.rs:697-770
+void refine_extremum_3d(const Plane& p, const Plane& c, const Plane& n, int x, int y, float& ox_out,
+                        float& oy_out, float& os_out, float& interp_out) {
+  const float* c_prev = c.row(y - 1);
+  const float* c_curr = c.row(y);
+  const float* c_next = c.row(y + 1);
+  const float* p_prev = p.row(y - 1);
+  const float* p_curr = p.row(y);
+  const float* p_next = p.row(y + 1);
+  const float* n_prev = n.row(y - 1);
+  const float* n_curr = n.row(y);
+  const float* n_next = n.row(y + 1);
+  const float center = c_curr[x];
+
+  const float gx = 0.5f * (c_curr[x + 1] - c_curr[x - 1]);
+  const float gy = 0.5f * (c_next[x] - c_prev[x]);
+  const float gs = 0.5f * (n_curr[x] - p_curr[x]);
+
+  const float dxx = c_curr[x + 1] - 2.0f * center + c_curr[x - 1];
+  const float dyy = c_next[x] - 2.0f * center + c_prev[x];
+  const float dss = n_curr[x] - 2.0f * center + p_curr[x];
+
+  const float dxy = 0.25f * ((c_next[x + 1] - c_next[x - 1]) - (c_prev[x + 1] - c_prev[x - 1]));
+  const float dxs = 0.25f * ((n_curr[x + 1] - n_curr[x - 1]) - (p_curr[x + 1] - p_curr[x - 1]));
+  const float dys = 0.25f * ((n_next[x] - n_prev[x]) - (p_next[x] - p_prev[x]));
+
+  const float c00 = dyy * dss - dys * dys;
+  const float c01 = dys * dxs - dxy * dss;
+  const float c02 = dxy * dys - dyy * dxs;
+  const float c11 = dxx * dss - dxs * dxs;
+  const float c12 = dxy * dxs - dxx * dys;
+  const float c22 = dxx * dyy - dxy * dxy;
+
+  const float det3 = dxx * c00 + dxy * c01 + dxs * c02;
+  if (std::fabs(det3) > 1e-9f) {
+    const float inv_det = -1.0f / det3;
+    const float ox = (c00 * gx + c01 * gy + c02 * gs) * inv_det;
+    const float oy = (c01 * gx + c11 * gy + c12 * gs) * inv_det;
+    const float os = (c02 * gx + c12 * gy + c22 * gs) * inv_det;
+    if (std::fabs(ox) <= 0.5f && std::fabs(oy) <= 0.5f && std::fabs(os) <= 0.5f) {
+      ox_out = ox;
+      oy_out = oy;
+      os_out = os;
+      interp_out = center + 0.5f * (gx * ox + gy * oy + gs * os);
+      return;
+    }
+  }
+  if (std::fabs(c22) > 1e-9f) {
+    const float inv_det2 = -1.0f / c22;
+    const float ox = clampf((dyy * gx - dxy * gy) * inv_det2, -0.5f, 0.5f);
+    const float oy = clampf((-dxy * gx + dxx * gy) * inv_det2, -0.5f, 0.5f);
+    const float os = std::fabs(dss) > 1e-6f ? clampf(-gs / dss, -0.5f, 0.5f) : 0.0f;
+    ox_out = ox;
+    oy_out = oy;
+    os_out = os;
+    interp_out = center + 0.5f * (gx * ox + gy * oy + gs * os);
+    return;
+  }
+  ox_out = oy_out = os_out = 0.0f;
+  interp_out = center;
+}
+
+inline bool gt_patch(const Plane& pl, int x, int y, float v) {
+  const float* r0 = pl.row(y - 1);
+  const float* r1 = pl.row(y);
+  const float* r2 = pl.row(y + 1);
+  return v > r0[x - 1] && v > r0[x] && v > r0[x + 1] && v > r1[x - 1] && v > r1[x] &&
+         v > r1[x + 1] && v > r2[x - 1] && v > r2[x] && v > r2[x + 1];
+}
+inline bool lt_patch(const Plane& pl, int x, int y, float v) {
+  const float* r0 = pl.row(y - 1);
+  const float* r1 = pl.row(y);
+  const float* r2 = pl.row(y + 1);
+  return v < r0[x - 1] && v < r0[x] && v < r0[x + 1] && v < r1[x - 1] && v < r1[x] &&
+         v < r1[x + 1] && v < r2[x - 1] && v < r2[x] && v < r2[x + 1];
+}
+
+// src/pipeline.rs:810-916
+void extract_extrema_in_octave(int octave_idx, const std::vector<Plane>& dogs, float mult,
+                               float threshold, std::vector<oracle_keypoint>& out) {
+  if (dogs.size() < 3) return;
+  const int h = dogs[0].h, w = dogs[0].w;
+  if (h < 3 || w < 3) return;
+  const int searchable = std::max((int)dogs.size() - 2, 1);
+  const float k = std::pow(2.0f, 1.0f / (float)searchable);
+  const int nslices = (int)dogs.size() - 2;
+  std::vector<std::vector<oracle_keypoint>> per_slice(nslices);
+  const bool par = (long long)h * w >= PAR_MIN_PIXELS;
+
+#pragma omp parallel for schedule(dynamic, 1) if (par)
+  for (int si = 0; si < nslices; ++si) {
+    const int s = si + 1;
+    const Plane& prev = dogs[s - 1];
+    const Plane& curr = dogs[s];
+    const Plane& next = dogs[s + 1];
+    const float eff_scale = BASE_SIGMA * mult * powi_f(k, s);
+    auto& kps = per_slice[si];
+    for (int y = 1; y < h - 1; ++y) {
+      const float* ra = curr.row(y - 1);
+      const float* rc = curr.row(y);
+      const float* rb = curr.row(y + 1);
+      for (int x = 1; x < w - 1; ++x) {
+        const float v = rc[x];
+        if (std::fabs(v) <= threshold) continue;
+        bool ext;
+        if (v > 0.0f) {
+          ext = v > rc[x - 1] && v > rc[x + 1] && v > ra[x - 1] && v > ra[x] && v > ra[x + 1] &&
+                v > rb[x - 1] && v > rb[x] && v > rb[x + 1] && gt_patch(prev, x, y, v) &&
+                gt_patch(next, x, y, v);
+        } else {
+          ext = v < rc[x - 1] && v < rc[x + 1] && v < ra[x - 1] && v < ra[x] && v < ra[x + 1] &&
+                v < rb[x - 1] && v < rb[x] && v < rb[x + 1] && lt_patch(prev, x, y, v) &&
+                lt_patch(next, x, y, v);
+        }
+        if (ext && passes_hessian_edge_test(curr, x, y, v)) {
+          float dx, dy, ds, interp;
+          refine_extremum_3d(prev, curr, next, x, y, dx, dy, ds, interp);
+          if (std::fabs(interp) > threshold) {
+            const float refined_scale = eff_scale * std::pow(k, ds);
+            const float lf = clampf(std::round((float)s + ds), 1.0f, (float)searchable);
+            oracle_keypoint kp;
+            kp.x = ((float)x + dx) * mult;
+            kp.y = ((float)y + dy) * mult;
+            kp.scale = std::fmax(refined_scale, 0.25f * BASE_SIGMA);
+            kp.response = interp;
+            kp.octave = (uint32_t)octave_idx;
+            kp.layer = (uint32_t)f2u_sat(lf);
+            kps.push_back(kp);
+          }
+        }
+      }
+    }
+  }
+  for (auto& v : per_slice) out.insert(out.end(), v.begin(), v.end());
+}
+
+// src/pipeline.rs:535-547
+std::vector<oracle_keypoint> pyramid_extract(const std::vector<Octave>& pyr, float thr) {
+  std::vector<oracle_keypoint> kps;
+  for (size_t o = 0; o < pyr.size(); ++o)
+    extract_extrema_in_octave((int)o, pyr[o].dog, pyr[o].scale_factor, thr, kps);
+  return kps;
+}
+
+// src/pipeline.rs:1158-1203
+struct GradPlanes {
+  int octave, layer, w, h;
+  std::vector<float> mag, ang;
+};
+GradPlanes gradient_planes(int octave, int layer, const Plane& g) {
+  GradPlanes gp;
+  gp.octave = octave;
+  gp.layer = layer;
+  gp.w = g.w;
+  gp.h = g.h;
+  gp.mag.assign((size_t)g.h * g.w, 0.0f);
+  gp.ang.assign((size_t)g.h * g.w, 0.0f);
+  const float two_pi = 2.0f * PI_F;
+  if (g.h >= 3 && g.w >= 3) {
+    for (int y = 1; y < g.h - 1; ++y) {
+      const float* ra = g.row(y - 1);
+      const float* rc = g.row(y);
+      const float* rb = g.row(y + 1);
+      for (int x = 1; x < g.w - 1; ++x) {
+        const float dx = rc[x + 1] - rc[x - 1];
+        const float dy = rb[x] - ra[x];
+        gp.mag[(size_t)y * g.w + x] = std::sqrt(dx * dx + dy * dy);
+        gp.ang[(size_t)y * g.w + x] = rem_euclid_f(std::atan2(dy, dx), two_pi);
+      }
+    }
+  }
+  return gp;
+}
+
+// src/pipeline.rs:1206-1227
+void resolve_octave_and_layer(const oracle_keypoint& kp, const std::vector<Octave>& pyr, int& oct,
+                              int& layer) {
+  if (pyr.empty()) {
+    oct = layer = 0;
+    return;
+  }
+  const int nocts = (int)pyr.size();
+  if (kp.layer > 0) {
+    oct = std::min((int)kp.octave, nocts - 1);
+  } else {
+    const float ratio = std::fmax(kp.scale / BASE_SIGMA, 1.0f);
+    oct = (int)std::min<unsigned long long>(f2u_sat(std::floor(std::log2(ratio))), (unsigned long long)(nocts - 1));
+  }
+  const int g_len = (int)pyr[oct].g.size();
+  const int searchable = std::max(g_len - 3, 1);
+  if (kp.layer > 0) {
+    layer = std::min((int)kp.layer, g_len - 1);
+  } else {
+    const float oct_mult = (float)(1ull << oct);
+    const float local_sigma = std::fmax(kp.scale / (BASE_SIGMA * oct_mult), 1.0f);
+    const unsigned long long l = f2u_sat(std::round(std::log2(local_sigma) * (float)searchable));
+    const int hi = std::max(g_len - 2, 1);
+    layer = (int)std::min<unsigned long long>(std::max<unsigned long long>(l, 1ull), (unsigned long long)hi);
+  }
+}
+
+// src/pipeline.rs:1233-1347
+std::vector<float> keypoint_orientations(const GradPlanes& gp, const oracle_keypoint& kp) {
+  const int NB = 36;
+  const float two_pi = 2.0f * PI_F;
+  const float sigma_ori = std::fmax(1.5f * kp.scale, 1.0f);
+  const float two_sigma_sq = 2.0f * sigma_ori * sigma_ori;
+  long long radius = f2i_sat(std::ceil(3.0f * sigma_ori));
+  if (radius < 2) radius = 2;
+  const long long cx = f2i_sat(std::round(kp.x));
+  const long long cy = f2i_sat(std::round(kp.y));
+  float hist[NB] = {0};
+  const float bin_scale = (float)NB / two_pi;
+  const long long H = gp.h, W = gp.w;
+  const long long y_min = std::max(cy - radius, 1ll);
+  const long long y_max = std::max(std::min(cy + radius, H - 2), 1ll);
+  const long long x_min = std::max(cx - radius, 1ll);
+  const long long x_max = std::max(std::min(cx + radius, W - 2), 1ll);
+  const float r_sq_max = (float)(radius * radius);
+  for (long long y = y_min; y <= y_max; ++y) {
+    const float dy = (float)(y - cy);
+    for (long long x = x_min; x <= x_max; ++x) {
+      const float dx = (float)(x - cx);
+      const float r_sq = dx * dx + dy * dy;
+      if (r_sq > r_sq_max) continue;
+      const float m = gp.mag[(size_t)(y * W + x)];
+      if (m <= 1e-7f) continue;
+      const float weight = std::exp(-r_sq / two_sigma_sq);
+      const float ang = gp.ang[(size_t)(y * W + x)];
+      const int bin = (int)(f2u_sat(std::floor(ang * bin_scale)) % NB);
+      hist[bin] += m * weight;
+    }
+  }
+  float sm[NB];
+  for (int b = 0; b < NB; ++b) {
+    const float prev = hist[(b + NB - 1) % NB];
+    const float curr = hist[b];
+    const float next = hist[(b + 1) % NB];
+    sm[b] = (prev + curr + next) * (1.0f / 3.0f);
+  }
+  int best_bin = 0;
+  float best_val = sm[0];
+  for (int b = 1; b < NB; ++b)
+    if (sm[b] > best_val) {
+      best_val = sm[b];
+      best_bin = b;
+    }
+  if (best_val <= 1e-7f) return {0.0f};
+  const float split = SECONDARY_ORI_PEAK_RATIO * best_val;
+  std::vector<std::pair<int, float>> peaks;
+  for (int b = 0; b < NB; ++b) {
+    const float v = sm[b];
+    if (v < split) continue;
+    const float l = sm[(b + NB - 1) % NB];
+    const float r = sm[(b + 1) % NB];
+    if (v > l && v >= r) peaks.push_back({b, v});
+  }
+  if (peaks.empty()) {
+    peaks.push_back({best_bin, best_val});
+  } else {
+    std::stable_sort(peaks.begin(), peaks.end(), [](const auto& a, const auto& b) {
+      if (b.second > a.second) return false;  // b.1.partial_cmp(a.1): a before b iff b.1 < a.1
+      if (b.second < a.second) return true;
+      return a.first < b.first;
+    });
+    if (peaks.size() > 4) peaks.resize(4);
+  }
+  std::vector<float> oris;
+  for (const auto& pk : peaks) {
+    const int bin = pk.first;
+    const float val = pk.second;
+    const float l = sm[(bin + NB - 1) % NB];
+    const float r = sm[(bin + 1) % NB];
+    const float denom = l - 2.0f * val + r;
+    float off = std::fabs(denom) > 1e-6f ? 0.5f * (l - r) / denom : 0.0f;
+    off = clampf(off, -0.5f, 0.5f);
+    oris.push_back(rem_euclid_f((((float)bin + 0.5f) + off) * (two_pi / (float)NB), two_pi));
+  }
+  return oris;
+}
+
+// src/pipeline.rs:1352-1480
+void descriptor_128(const GradPlanes& gp, const oracle_keypoint& kp, float orientation, float* desc) {
+  const int GW = 4;
+  const float two_pi = 2.0f * PI_F;
+  std::fill(desc, desc + DESC_LEN, 0.0f);
+  if (gp.w < 3 || gp.h < 3) return;
+  const float cos_t = std::cos(orientation);
+  const float sin_t = std::sin(orientation);
+  const float hist_width = std::fmax(3.0f * kp.scale, 1.5f);
+  const float inv_hw = 1.0f / hist_width;
+  const float exp_scale = -1.0f / (2.0f * 2.0f * 2.0f);
+  long long max_radius = f2i_sat(std::ceil(hist_width * SQRT_2_F * ((float)GW + 1.0f) * 0.5f));
+  if (max_radius < 4) max_radius = 4;
+  const long long cx = f2i_sat(std::round(kp.x));
+  const long long cy = f2i_sat(std::round(kp.y));
+  const long long H = gp.h, W = gp.w;
+  const long long y_min = std::max(cy - max_radius, 1ll);
+  const long long y_max = std::max(std::min(cy + max_radius, H - 2), 1ll);
+  const long long x_min = std::max(cx - max_radius, 1ll);
+  const long long x_max = std::max(std::min(cx + max_radius, W - 2), 1ll);
+  const float bin_per_rad = 8.0f / two_pi;
+  for (long long y = y_min; y <= y_max; ++y) {
+    const float dy = (float)y - kp.y;
+    for (long long x = x_min; x <= x_max; ++x) {
+      const float dx = (float)x - kp.x;
+      const float r_rot = (dx * cos_t + dy * sin_t) * inv_hw;
+      const float c_rot = (-dx * sin_t + dy * cos_t) * inv_hw;
+      const float r_bin = r_rot + (float)GW * 0.5f - 0.5f;
+      const float c_bin = c_rot + (float)GW * 0.5f - 0.5f;
+      if (r_bin <= -1.0f || r_bin >= (float)GW || c_bin <= -1.0f || c_bin >= (float)GW) continue;
+      const float m = gp.mag[(size_t)(y * W + x)];
+      if (m <= 1e-7f) continue;
+      const float w_gauss = std::exp((r_rot * r_rot + c_rot * c_rot) * exp_scale);
+      const float wm = m * w_gauss;
+      const float rel = rem_euclid_f(gp.ang[(size_t)(y * W + x)] - orientation, two_pi);
+      const float o_bin = rel * bin_per_rad;
+      const long long r0 = f2i_sat(std::floor(r_bin));
+      const long long c0 = f2i_sat(std::floor(c_bin));
+      const long long o0 = f2i_sat(std::floor(o_bin));
+      const float dr = r_bin - (float)r0;
+      const float dc = c_bin - (float)c0;
+      const float dof = o_bin - (float)o0;
+      for (int ir = 0; ir <= 1; ++ir) {
+        const long long rb = r0 + ir;
+        if (rb < 0 || rb >= GW) continue;
+        const float wr = ir == 0 ? 1.0f - dr : dr;
+        for (int ic = 0; ic <= 1; ++ic) {
+          const long long cb = c0 + ic;
+          if (cb < 0 || cb >= GW) continue;
+          const float wc = ic == 0 ? 1.0f - dc : dc;
+          for (int io = 0; io <= 1; ++io) {
+            long long ob = (o0 + io) % 8;
+            if (ob < 0) ob += 8;
+            const float wo = io == 0 ? 1.0f - dof : dof;
+            const size_t idx = (size_t)((rb * GW + cb) * 8 + ob);
+            desc[idx] += wm * wr * wc * wo;
+          }
+        }
+      }
+    }
+  }
+  float n1 = 0.0f;
+  for (size_t i = 0; i < DESC_LEN; ++i) n1 += desc[i] * desc[i];
+  n1 = std::sqrt(n1);
+  if (n1 > 1e-7f) {
+    const float inv1 = 1.0f / n1;
+    for (size_t i = 0; i < DESC_LEN; ++i) desc[i] = std::fmin(desc[i] * inv1, 0.2f);
+    float n2 = 0.0f;
+    for (size_t i = 0; i < DESC_LEN; ++i) n2 += desc[i] * desc[i];
+    n2 = std::sqrt(n2);
+    if (n2 > 1e-7f) {
+      const float inv2 = 1.0f / n2;
+      for (size_t i = 0; i < DESC_LEN; ++i) desc[i] *= inv2;
+    }
+  }
+}
+
+// src/pipeline.rs:1012-1019
+void rootsift(const float* d, float* out) {
+  float l1 = 0.0f;
+  for (size_t i = 0; i < DESC_LEN; ++i) l1 += std::fmax(d[i], 0.0f);
+  if (l1 <= 1e-7f) {
+    std::memmove(out, d, DESC_LEN * sizeof(float));
+    return;
+  }
+  const float inv = 1.0f / l1;
+  for (size_t i = 0; i < DESC_LEN; ++i) out[i] = std::sqrt(std::fmax(d[i], 0.0f) * inv);
+}
+
+struct Feature {
+  float x, y, scale, response, orientation;
+  float desc[DESC_LEN];
+};
+
+// src/pipeline.rs:1482-1577
+std::vector<Feature> describe_from_pyramid(const std::vector<Octave>& pyr,
+                                           const std::vector<oracle_keypoint>& kps, int kind) {
+  std::vector<Feature> feats;
+  if (pyr.empty() || kps.empty()) return feats;
+  std::vector<std::pair<int, int>> levels;
+  for (const auto& kp : kps) {
+    int o, l;
+    resolve_octave_and_layer(kp, pyr, o, l);
+    if (std::find(levels.begin(), levels.end(), std::make_pair(o, l)) == levels.end())
+      levels.push_back({o, l});
+  }
+  std::vector<GradPlanes> cache(levels.size());
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < (int)levels.size(); ++i)
+    cache[i] = gradient_planes(levels[i].first, levels[i].second, pyr[levels[i].first].g[levels[i].second]);
+
+  std::vector<std::vector<Feature>> per_kp(kps.size());
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long long i = 0; i < (long long)kps.size(); ++i) {
+    const oracle_keypoint& kp = kps[i];
+    int o, l;
+    resolve_octave_and_layer(kp, pyr, o, l);
+    const GradPlanes* gp = nullptr;
+    for (const auto& c : cache)
+      if (c.octave == o && c.layer == l) {
+        gp = &c;
+        break;
+      }
+    const float oct_mult = pyr[o].scale_factor;
+    const float inv = 1.0f / oct_mult;
+    oracle_keypoint okp;
+    okp.x = kp.x * inv;
+    okp.y = kp.y * inv;
+    okp.scale = std::fmax(kp.scale * inv, 0.5f * BASE_SIGMA);
+    okp.response = kp.response;
+    okp.octave = (uint32_t)o;
+    okp.layer = (uint32_t)l;
+    const std::vector<float> oris = keypoint_orientations(*gp, okp);
+    for (float ori : oris) {
+      Feature f;
+      f.x = kp.x;
+      f.y = kp.y;
+      f.scale = kp.scale;
+      f.response = kp.response;
+      f.orientation = ori;
+      float raw[DESC_LEN];
+      descriptor_128(*gp, okp, ori, raw);
+      if (kind == 1) rootsift(raw, f.desc);
+      else std::memcpy(f.desc, raw, sizeof(raw));
+      per_kp[i].push_back(f);
+    }
+  }
+  for (auto& v : per_kp) feats.insert(feats.end(), v.begin(), v.end());
+  return feats;
+}
+
+Plane make_plane(const float* img, int h, int w) {
+  Plane p(h, w);
+  std::memcpy(p.d.data(), img, sizeof(float) * (size_t)h * w);
+  return p;
+}
+
+int write_features(const std::vector<Feature>& f, float* meta, float* desc, int cap) {
+  const int n = (int)f.size();
+  for (int i = 0; i < n && i < cap; ++i) {
+    if (meta) {
+      meta[5 * i + 0] = f[i].x;
+      meta[5 * i + 1] = f[i].y;
+      meta[5 * i + 2] = f[i].scale;
+      meta[5 * i + 3] = f[i].response;
+      meta[5 * i + 4] = f[i].orientation;
+    }
+    if (desc) std::memcpy(desc + (size_t)i * DESC_LEN, f[i].desc, sizeof(float) * DESC_LEN);
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------- matching
+// src/pipeline.rs:1700-1717
+inline float dist_sq_early_exit(const float* a, const float* b, float cutoff) {
+  float sum = 0.0f;
+  for (int c = 0; c < 4; ++c) {
+    for (int i = 0; i < 32; ++i) {
+      const float d = a[c * 32 + i] - b[c * 32 + i];
+      sum += d * d;
+    }
+    if (sum >= cutoff) return sum;
+  }
+  return sum;
+}
+
+// ---------------------------------------------------------------- RANSAC
+uint64_t splitmix64(uint64_t& s) {  // src/pipeline.rs:1862-1868
+  s += 0x9E3779B97F4A7C15ull;
+  uint64_t z = s;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// src/pipeline.rs:1873-1897
+void eval_similarity(const oracle_match* m, int n, float a, float b, float tx, float ty,
+                     float thresh_sq, size_t& count, float& err_sum) {
+  count = 0;
+  err_sum = 0.0f;
+  for (int i = 0; i < n; ++i) {
+    const float px = a * m[i].qx - b * m[i].qy + tx;
+    const float py = b * m[i].qx + a * m[i].qy + ty;
+    const float dx = px - m[i].tx;
+    const float dy = py - m[i].ty;
+    const float e = dx * dx + dy * dy;
+    if (e <= thresh_sq) {
+      ++count;
+      err_sum += e;
+    }
+  }
+}
+
+struct Sim {
+  float a, b, tx, ty, scale, rot;
+};
+
+// src/pipeline.rs:1900-1975
+bool procrustes(const std::vector<oracle_match>& in, Sim& out) {
+  if (in.empty()) return false;
+  if (in.size() == 1) {
+    out = {1.0f, 0.0f, in[0].dx, in[0].dy, 1.0f, 0.0f};
+    return true;
+  }
+  const float inv_n = 1.0f / (float)in.size();
+  float mqx = 0, mqy = 0, mtx = 0, mty = 0;
+  for (const auto& m : in) {
+    mqx += m.qx;
+    mqy += m.qy;
+    mtx += m.tx;
+    mty += m.ty;
+  }
+  mqx *= inv_n;
+  mqy *= inv_n;
+  mtx *= inv_n;
+  mty *= inv_n;
+  float sqq = 0, na = 0, nb = 0;
+  for (const auto& m : in) {
+    const float qx = m.qx - mqx, qy = m.qy - mqy, tx = m.tx - mtx, ty = m.ty - mty;
+    sqq += qx * qx + qy * qy;
+    na += qx * tx + qy * ty;
+    nb += qx * ty - qy * tx;
+  }
+  float a = 1.0f, b = 0.0f;
+  if (sqq > 1e-5f) {
+    const float af = na / sqq, bf = nb / sqq;
+    const float s2 = af * af + bf * bf;
+    if (s2 >= 0.04f && s2 <= 25.0f) {
+      a = af;
+      b = bf;
+    }
+  }
+  out.a = a;
+  out.b = b;
+  out.tx = mtx - (a * mqx - b * mqy);
+  out.ty = mty - (b * mqx + a * mqy);
+  out.scale = std::sqrt(a * a + b * b);
+  out.rot = std::atan2(b, a) * RAD_TO_DEG_F;
+  return true;
+}
+
+// src/pipeline.rs:1979-2002
+size_t adaptive_iters(size_t inl, size_t total, int ss, double conf, size_t min_it, size_t cap) {
+  if (total == 0 || inl == 0) return cap;
+  double w = (double)inl / (double)total;
+  if (w < 1e-3) w = 1e-3;
+  if (w > 1.0 - 1e-6) w = 1.0 - 1e-6;
+  double p = powi_d(w, ss);
+  if (p < 1e-12) p = 1e-12;
+  if (p > 1.0 - 1e-9) p = 1.0 - 1e-9;
+  const double num = std::log(1.0 - conf);
+  const double den = std::log(1.0 - p);
+  if (std::fabs(den) < 1e-12) return min_it;
+  const double est = std::ceil(num / den);
+  if (!std::isfinite(est)) return cap;
+  size_t e = (size_t)d2u_sat(est);
+  if (e < min_it) e = min_it;
+  if (e > cap) e = cap;
+  return e;
+}
+
+// src/pipeline.rs:2006-2026
+std::vector<double> ratio_cdf(const oracle_match* m, int n) {
+  std::vector<double> cdf;
+  cdf.reserve(n);
+  double acc = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double r = 1.0;
+    if (std::isfinite(m[i].ratio)) {
+      r = (double)m[i].ratio;
+      if (r < 0.05) r = 0.05;
+      if (r > 1.0) r = 1.0;
+    }
+    acc += 1.0 / r;
+    cdf.push_back(acc);
+  }
+  if (acc > 0.0) {
+    const double inv = 1.0 / acc;
+    for (double& v : cdf) v *= inv;
+  }
+  if (!cdf.empty()) cdf.back() = 1.0;
+  return cdf;
+}
+
+// src/pipeline.rs:2029-2036
+size_t sample_weighted(const std::vector<double>& cdf, uint64_t& st) {
+  const double u = (double)(splitmix64(st) >> 11) * (1.0 / (double)(1ull << 53));
+  size_t lo = (size_t)(std::lower_bound(cdf.begin(), cdf.end(), u) - cdf.begin());
+  const size_t hi = cdf.empty() ? 0 : cdf.size() - 1;
+  return std::min(lo, hi);
+}
+
+// src/pipeline.rs:2055-2191
+int similarity_ransac(const oracle_match* m, int n, float thr, uint64_t seed, std::vector<uint8_t>& mask,
+                      Sim& model, bool& has_model) {
+  mask.assign(n, 0);
+  has_model = false;
+  if (n == 0) return 0;
+  if (n == 1) {
+    std::vector<oracle_match> v(m, m + 1);
+    has_model = procrustes(v, model);
+    mask[0] = 1;
+    return 1;
+  }
+  const float thresh = std::fmax(thr, 0.5f);
+  const float tsq = thresh * thresh;
+  std::vector<int> sorted(n);
+  for (int i = 0; i < n; ++i) sorted[i] = i;
+  std::stable_sort(sorted.begin(), sorted.end(), [&](int i, int j) { return m[i].ratio < m[j].ratio; });
+
+  float ba = 1.0f, bb = 0.0f, btx = m[sorted[0]].dx, bty = m[sorted[0]].dy;
+  size_t best_count;
+  float best_err;
+  eval_similarity(m, n, ba, bb, btx, bty, tsq, best_count, best_err);
+  for (int i = 0; i < n && i < 32; ++i) {
+    const int idx = sorted[i];
+    size_t c;
+    float e;
+    eval_similarity(m, n, 1.0f, 0.0f, m[idx].dx, m[idx].dy, tsq, c, e);
+    if (c > best_count || (c == best_count && e < best_err)) {
+      best_count = c;
+      best_err = e;
+      ba = 1.0f;
+      bb = 0.0f;
+      btx = m[idx].dx;
+      bty = m[idx].dy;
+    }
+  }
+  const std::vector<double> cdf = ratio_cdf(m, n);
+  uint64_t rng = seed;
+  const size_t hard_cap = 1000, min_iters = 64;
+  size_t max_iters = adaptive_iters(best_count, n, 2, 0.999, min_iters, hard_cap);
+  size_t iter = 0;
+  while (iter < max_iters) {
+    ++iter;
+    const size_t i1 = sample_weighted(cdf, rng);
+    size_t i2 = sample_weighted(cdf, rng);
+    if (i2 == i1) i2 = (i1 + 1) % n;
+    const oracle_match& m1 = m[i1];
+    const oracle_match& m2 = m[i2];
+    const float dxq = m2.qx - m1.qx, dyq = m2.qy - m1.qy;
+    const float dq = dxq * dxq + dyq * dyq;
+    if (dq < 16.0f) continue;
+    const float dxt = m2.tx - m1.tx, dyt = m2.ty - m1.ty;
+    const float a = (dxq * dxt + dyq * dyt) / dq;
+    const float b = (dxq * dyt - dyq * dxt) / dq;
+    const float s2 = a * a + b * b;
+    if (!(s2 >= 0.04f && s2 <= 25.0f)) continue;
+    const float tx = m1.tx - (a * m1.qx - b * m1.qy);
+    const float ty = m1.ty - (b * m1.qx + a * m1.qy);
+    size_t c;
+    float e;
+    eval_similarity(m, n, a, b, tx, ty, tsq, c, e);
+    if (c > best_count || (c == best_count && e < best_err)) {
+      best_count = c;
+      best_err = e;
+      ba = a;
+      bb = b;
+      btx = tx;
+      bty = ty;
+      max_iters = adaptive_iters(best_count, n, 2, 0.999, min_iters, hard_cap);
+    }
+  }
+  std::vector<oracle_match> inl;
+  std::vector<uint8_t> inl_mask(n, 0);
+  for (int i = 0; i < n; ++i) {
+    const float dx = (ba * m[i].qx - bb * m[i].qy + btx) - m[i].tx;
+    const float dy = (bb * m[i].qx + ba * m[i].qy + bty) - m[i].ty;
+    if (dx * dx + dy * dy <= tsq) {
+      inl.push_back(m[i]);
+      inl_mask[i] = 1;
+    }
+  }
+  Sim refined;
+  const bool has_refined = procrustes(inl, refined);
+  if (has_refined) {
+    std::vector<oracle_match> rin;
+    std::vector<uint8_t> rmask(n, 0);
+    for (int i = 0; i < n; ++i) {
+      const float dx = (refined.a * m[i].qx - refined.b * m[i].qy + refined.tx) - m[i].tx;
+      const float dy = (refined.b * m[i].qx + refined.a * m[i].qy + refined.ty) - m[i].ty;
+      if (dx * dx + dy * dy <= tsq) {
+        rin.push_back(m[i]);
+        rmask[i] = 1;
+      }
+    }
+    if (rin.size() >= inl.size()) {
+      inl = std::move(rin);
+      inl_mask = std::move(rmask);
+    }
+  }
+  Sim fin;
+  if (procrustes(inl, fin)) {
+    model = fin;
+    has_model = true;
+  } else if (has_refined) {
+    model = refined;
+    has_model = true;
+  }
+  mask = inl_mask;
+  return (int)inl.size();
+}
+
+using H3 = double[3][3];
+
+// src/pipeline.rs:2276-2353
+bool smallest_eigvec9(double a[9][9], double h[9]) {
+  double v[9][9] = {{0}};
+  for (int i = 0; i < 9; ++i) v[i][i] = 1.0;
+  for (int sweep = 0; sweep < 20; ++sweep) {
+    double max_off = 0.0;
+    for (int p = 0; p < 9; ++p)
+      for (int q = p + 1; q < 9; ++q)
+        if (std::fabs(a[p][q]) > max_off) max_off = std::fabs(a[p][q]);
+    if (max_off < 1e-13) break;
+    for (int p = 0; p < 8; ++p)
+      for (int q = p + 1; q < 9; ++q) {
+        const double apq = a[p][q];
+        if (std::fabs(apq) < 1e-15) continue;
+        const double app = a[p][p], aqq = a[q][q];
+        const double tau = (aqq - app) / (2.0 * apq);
+        const double t = tau >= 0.0 ? 1.0 / (tau + std::sqrt(1.0 + tau * tau))
+                                    : -1.0 / (-tau + std::sqrt(1.0 + tau * tau));
+        const double c = 1.0 / std::sqrt(1.0 + t * t);
+        const double s = t * c;
+        a[p][p] = app - t * apq;
+        a[q][q] = aqq + t * apq;
+        a[p][q] = 0.0;
+        a[q][p] = 0.0;
+        for (int r = 0; r < 9; ++r) {
+          if (r != p && r != q) {
+            const double arp = a[r][p], arq = a[r][q];
+            a[r][p] = c * arp - s * arq;
+            a[p][r] = a[r][p];
+            a[r][q] = s * arp + c * arq;
+            a[q][r] = a[r][q];
+          }
+          const double vrp = v[r][p], vrq = v[r][q];
+          v[r][p] = c * vrp - s * vrq;
+          v[r][q] = s * vrp + c * vrq;
+        }
+      }
+  }
+  int mi = 0;
+  double me = a[0][0];
+  for (int i = 1; i < 9; ++i)
+    if (a[i][i] < me) {
+      me = a[i][i];
+      mi = i;
+    }
+  for (int r = 0; r < 9; ++r) {
+    h[r] = v[r][mi];
+    if (!std::isfinite(h[r])) return false;
+  }
+  return true;
+}
+
+// src/pipeline.rs:2357-2404
+bool degenerate_triangle(const double p[4][2]) {
+  static const int T[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+  for (const auto& t : T) {
+    const double xi = p[t[0]][0], yi = p[t[0]][1], xj = p[t[1]][0], yj = p[t[1]][1];
+    const double xk = p[t[2]][0], yk = p[t[2]][1];
+    if (!std::isfinite(xi) || !std::isfinite(yi) || !std::isfinite(xj) || !std::isfinite(yj) ||
+        !std::isfinite(xk) || !std::isfinite(yk))
+      return true;
+    const double dx1 = xj - xi, dy1 = yj - yi, dx2 = xk - xi, dy2 = yk - yi, dx3 = xk - xj, dy3 = yk - yj;
+    const double cross = std::fabs(dx1 * dy2 - dy1 * dx2);
+    const double me = std::fmax(std::fmax(dx1 * dx1 + dy1 * dy1, dx2 * dx2 + dy2 * dy2), dx3 * dx3 + dy3 * dy3);
+    if (cross < 4.0 || cross < 1e-3 * me) return true;
+  }
+  return false;
+}
+bool degenerate_quad(const oracle_match* q[4]) {
+  double qp[4][2], tp[4][2];
+  for (int i = 0; i < 4; ++i) {
+    qp[i][0] = q[i]->qx;
+    qp[i][1] = q[i]->qy;
+    tp[i][0] = q[i]->tx;
+    tp[i][1] = q[i]->ty;
+  }
+  return degenerate_triangle(qp) || degenerate_triangle(tp);
+}
+
+// src/pipeline.rs:2408-2528
+bool fit_dlt(const oracle_match* const* s, int n, double H[3][3]) {
+  if (n < 4) return false;
+  const double inv_n = 1.0 / (double)n;
+  double cxq = 0, cyq = 0, cxt = 0, cyt = 0;
+  for (int i = 0; i < n; ++i) {
+    const double qx = s[i]->qx, qy = s[i]->qy, tx = s[i]->tx, ty = s[i]->ty;
+    if (!std::isfinite(qx) || !std::isfinite(qy) || !std::isfinite(tx) || !std::isfinite(ty)) return false;
+    cxq += qx;
+    cyq += qy;
+    cxt += tx;
+    cyt += ty;
+  }
+  cxq *= inv_n;
+  cyq *= inv_n;
+  cxt *= inv_n;
+  cyt *= inv_n;
+  double mdq = 0, mdt = 0;
+  for (int i = 0; i < n; ++i) {
+    const double dxq = (double)s[i]->qx - cxq, dyq = (double)s[i]->qy - cyq;
+    const double dxt = (double)s[i]->tx - cxt, dyt = (double)s[i]->ty - cyt;
+    mdq += std::sqrt(dxq * dxq + dyq * dyq);
+    mdt += std::sqrt(dxt * dxt + dyt * dyt);
+  }
+  mdq *= inv_n;
+  mdt *= inv_n;
+  if (!std::isfinite(mdq) || !std::isfinite(mdt) || mdq < 1e-6 || mdt < 1e-6) return false;
+  const double sq = 1.41421356237309504880 / mdq;
+  const double st = 1.41421356237309504880 / mdt;
+  double ata[9][9] = {{0}};
+  for (int i = 0; i < n; ++i) {
+    const double x = ((double)s[i]->qx - cxq) * sq;
+    const double y = ((double)s[i]->qy - cyq) * sq;
+    const double xp = ((double)s[i]->tx - cxt) * st;
+    const double yp = ((double)s[i]->ty - cyt) * st;
+    const double r1[9] = {-x, -y, -1.0, 0.0, 0.0, 0.0, x * xp, y * xp, xp};
+    const double r2[9] = {0.0, 0.0, 0.0, -x, -y, -1.0, x * yp, y * yp, yp};
+    for (int a = 0; a < 9; ++a)
+      for (int b = a; b < 9; ++b) ata[a][b] += r1[a] * r1[b] + r2[a] * r2[b];
+  }
+  for (int a = 0; a < 9; ++a)
+    for (int b = 0; b < a; ++b) ata[a][b] = ata[b][a];
+  double hv[9];
+  if (!smallest_eigvec9(ata, hv)) return false;
+  const double hn[3][3] = {{hv[0], hv[1], hv[2]}, {hv[3], hv[4], hv[5]}, {hv[6], hv[7], hv[8]}};
+  const double tq[3][3] = {{sq, 0.0, -sq * cxq}, {0.0, sq, -sq * cyq}, {0.0, 0.0, 1.0}};
+  const double ist = 1.0 / st;
+  const double tti[3][3] = {{ist, 0.0, cxt}, {0.0, ist, cyt}, {0.0, 0.0, 1.0}};
+  double tmp[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) tmp[r][c] = hn[r][0] * tq[0][c] + hn[r][1] * tq[1][c] + hn[r][2] * tq[2][c];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) H[r][c] = tti[r][0] * tmp[0][c] + tti[r][1] * tmp[1][c] + tti[r][2] * tmp[2][c];
+  if (std::fabs(H[2][2]) > 1e-12) {
+    const double inv = 1.0 / H[2][2];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) H[r][c] *= inv;
+  }
+  return true;
+}
+
+// src/pipeline.rs:2550-2576
+void eval_h(const oracle_match* m, int n, const double H[3][3], double tsq, size_t& count, double& err) {
+  count = 0;
+  err = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double qx = m[i].qx, qy = m[i].qy;
+    const double w = H[2][0] * qx + H[2][1] * qy + H[2][2];
+    if (std::fabs(w) < 1e-9) continue;
+    const double iw = 1.0 / w;
+    const double px = (H[0][0] * qx + H[0][1] * qy + H[0][2]) * iw;
+    const double py = (H[1][0] * qx + H[1][1] * qy + H[1][2]) * iw;
+    const double dx = px - (double)m[i].tx, dy = py - (double)m[i].ty;
+    const double e = dx * dx + dy * dy;
+    if (e <= tsq) {
+      ++count;
+      err += e;
+    }
+  }
+}
+
+// src/pipeline.rs:2578-2601
+std::vector<int> collect_h(const oracle_match* m, int n, const double H[3][3], double tsq) {
+  std::vector<int> out;
+  for (int i = 0; i < n; ++i) {
+    const double qx = m[i].qx, qy = m[i].qy;
+    const double w = H[2][0] * qx + H[2][1] * qy + H[2][2];
+    if (std::fabs(w) < 1e-9) continue;
+    const double iw = 1.0 / w;
+    const double px = (H[0][0] * qx + H[0][1] * qy + H[0][2]) * iw;
+    const double py = (H[1][0] * qx + H[1][1] * qy + H[1][2]) * iw;
+    const double dx = px - (double)m[i].tx, dy = py - (double)m[i].ty;
+    if (dx * dx + dy * dy <= tsq) out.push_back(i);
+  }
+  return out;
+}
+
+// src/pipeline.rs:2605-2631
+void local_optimize(const oracle_match* m, int n, double H[3][3], size_t& count, double& err, double tsq) {
+  for (int it = 0; it < 2; ++it) {
+    const std::vector<int> in = collect_h(m, n, H, tsq);
+    if (in.size() < 4) break;
+    std::vector<const oracle_match*> ptr(in.size());
+    for (size_t i = 0; i < in.size(); ++i) ptr[i] = &m[in[i]];
+    double R[3][3];
+    if (!fit_dlt(ptr.data(), (int)ptr.size(), R)) break;
+    size_t rc;
+    double re;
+    eval_h(m, n, R, tsq, rc, re);
+    if (rc > count || (rc == count && re < err)) {
+      std::memcpy(H, R, sizeof(R));
+      count = rc;
+      err = re;
+    } else {
+      break;
+    }
+  }
+}
+
+// src/pipeline.rs:2663-2755
+int homography_ransac(const oracle_match* m, int n, float thr, uint64_t sim_seed, uint64_t hom_seed,
+                      std::vector<uint8_t>& mask, double H_out[3][3], bool& has_h) {
+  mask.assign(n, 0);
+  has_h = false;
+  if (n == 0) return 0;
+  const double thresh = (double)std::fmax(thr, 0.5f);
+  const double tsq = thresh * thresh;
+  std::vector<uint8_t> sim_mask;
+  Sim sim;
+  bool has_sim;
+  const int sim_count = similarity_ransac(m, n, thr, sim_seed, sim_mask, sim, has_sim);
+  double best[3][3] = {{0}};
+  bool has_best = false;
+  size_t best_count = 0;
+  double best_err = std::numeric_limits<double>::infinity();
+  if (has_sim) {
+    const double hs[3][3] = {{(double)sim.a, -(double)sim.b, (double)sim.tx},
+                             {(double)sim.b, (double)sim.a, (double)sim.ty},
+                             {0.0, 0.0, 1.0}};
+    std::memcpy(best, hs, sizeof(hs));
+    has_best = true;
+    eval_h(m, n, best, tsq, best_count, best_err);
+  }
+  if (n < 4) {
+    mask = sim_mask;
+    if (has_best) {
+      std::memcpy(H_out, best, sizeof(best));
+      has_h = true;
+    }
+    return sim_count;
+  }
+  const std::vector<double> cdf = ratio_cdf(m, n);
+  uint64_t rng = hom_seed;
+  const size_t hard_cap = 2000, min_iters = 64;
+  size_t max_iters = adaptive_iters(best_count, n, 4, 0.999, min_iters, hard_cap);
+  size_t iter = 0;
+  while (iter < max_iters) {
+    ++iter;
+    size_t idx[4] = {0, 0, 0, 0};
+    int chosen = 0, attempts = 0;
+    while (chosen < 4 && attempts < 16) {
+      ++attempts;
+      const size_t c = sample_weighted(cdf, rng);
+      bool dup = false;
+      for (int j = 0; j < chosen; ++j)
+        if (idx[j] == c) dup = true;
+      if (!dup) idx[chosen++] = c;
+    }
+    if (chosen < 4) continue;
+    const oracle_match* quad[4] = {&m[idx[0]], &m[idx[1]], &m[idx[2]], &m[idx[3]]};
+    if (degenerate_quad(quad)) continue;
+    double Hc[3][3];
+    if (fit_dlt(quad, 4, Hc)) {
+      size_t c;
+      double e;
+      eval_h(m, n, Hc, tsq, c, e);
+      if (c > best_count || (c == best_count && e < best_err)) {
+        local_optimize(m, n, Hc, c, e, tsq);
+        best_count = c;
+        best_err = e;
+        std::memcpy(best, Hc, sizeof(Hc));
+        has_best = true;
+        max_iters = adaptive_iters(best_count, n, 4, 0.999, min_iters, hard_cap);
+      }
+    }
+  }
+  if (!has_best) {
+    mask = sim_mask;
+    return sim_count;
+  }
+  local_optimize(m, n, best, best_count, best_err, tsq);
+  const std::vector<int> in = collect_h(m, n, best, tsq);
+  for (int i : in) mask[i] = 1;
+  std::memcpy(H_out, best, sizeof(best));
+  has_h = true;
+  return (int)in.size();
+}
+
+float median_f32(std::vector<float> v) {  // src/pipeline.rs:2195-2206
+  if (v.empty()) return 0.0f;
+  std::stable_sort(v.begin(), v.end(), [](float a, float b) { return a < b; });
+  const size_t mid = v.size() / 2;
+  return v.size() % 2 == 1 ? v[mid] : 0.5f * (v[mid - 1] + v[mid]);
+}
+
+inline int popc128(uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1) {
+  return __builtin_popcountll(a0 ^ b0) + __builtin_popcountll(a1 ^ b1);
+}
+inline bool has_zero_byte128(uint64_t x0, uint64_t x1) {
+  for (int i = 0; i < 8; ++i) {
+    if (((x0 >> (8 * i)) & 0xFF) == 0) return true;
+    if (((x1 >> (8 * i)) & 0xFF) == 0) return true;
+  }
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t oracle_splitmix64_next(uint64_t* state) { return splitmix64(*state); }
+
+int oracle_gaussian_kernel_1d(float sigma, float* out, int cap) {
+  const std::vector<float> k = gaussian_kernel_1d(sigma);
+  for (int i = 0; i < (int)k.size() && i < cap; ++i) out[i] = k[i];
+  return (int)k.size();
+}
+
+void oracle_gaussian_blur(const float* img, int h, int w, float sigma, float* out) {
+  const Plane r = gaussian_blur(make_plane(img, h, w), sigma);
+  std::memcpy(out, r.d.data(), sizeof(float) * (size_t)h * w);
+}
+
+void oracle_upsample_2x(const float* img, int h, int w, float* out) {
+  const Plane r = upsample_2x_bilinear(make_plane(img, h, w));
+  std::memcpy(out, r.d.data(), sizeof(float) * r.d.size());
+}
+
+// src/pipeline.rs:957-966
+void oracle_luma_to_f32(const uint8_t* px, size_t n, float* out) {
+  const float inv_255 = 1.0f / 255.0f;
+  for (size_t i = 0; i < n; ++i) out[i] = (float)px[i] * inv_255;
+}
+
+void* oracle_pyramid_build(const float* img, int h, int w, int octaves, int scales, int upsample) {
+  return new std::vector<Octave>(build_pyramid(make_plane(img, h, w), octaves, scales, upsample != 0));
+}
+int oracle_pyramid_num_octaves(const void* pyr) { return (int)((const std::vector<Octave>*)pyr)->size(); }
+void oracle_pyramid_octave_info(const void* pyr, int o, int* h, int* w, float* sf) {
+  const auto& oc = (*(const std::vector<Octave>*)pyr)[o];
+  *h = oc.g[0].h;
+  *w = oc.g[0].w;
+  *sf = oc.scale_factor;
+}
+void oracle_pyramid_copy_plane(const void* pyr, int o, int kind, int idx, float* out) {
+  const auto& oc = (*(const std::vector<Octave>*)pyr)[o];
+  const Plane& p = kind == 0 ? oc.g[idx] : oc.dog[idx];
+  std::memcpy(out, p.d.data(), sizeof(float) * p.d.size());
+}
+int oracle_pyramid_extract_extrema(const void* pyr, float thr, oracle_keypoint* out, int cap) {
+  const auto kps = pyramid_extract(*(const std::vector<Octave>*)pyr, thr);
+  for (int i = 0; i < (int)kps.size() && i < cap; ++i) out[i] = kps[i];
+  return (int)kps.size();
+}
+void oracle_pyramid_free(void* pyr) { delete (std::vector<Octave>*)pyr; }
+
+int oracle_detect_keypoints(const float* img, int h, int w, int octaves, int scales, float thr,
+                            int upsample, oracle_keypoint* out, int cap) {
+  const auto pyr = build_pyramid(make_plane(img, h, w), octaves, scales, upsample != 0);
+  const auto kps = pyramid_extract(pyr, thr);
+  for (int i = 0; i < (int)kps.size() && i < cap; ++i) out[i] = kps[i];
+  return (int)kps.size();
+}
+
+// src/pipeline.rs:1633-1658.  max_features = 0 disables the cap (the reference
+// always caps at MAX_FEATURES_PER_IMAGE = 4096, src/pipeline.rs:1054).
+int oracle_detect_and_compute(const float* img, int h, int w, int octaves, int scales, float thr,
+                              int upsample, int kind, int max_features, float* meta, float* desc,
+                              int cap) {
+  const auto pyr = build_pyramid(make_plane(img, h, w), octaves, scales, upsample != 0);
+  auto kps = pyramid_extract(pyr, thr);
+  if (max_features > 0 && (int)kps.size() > max_features) {
+    std::stable_sort(kps.begin(), kps.end(), [](const oracle_keypoint& a, const oracle_keypoint& b) {
+      return std::fabs(b.response) < std::fabs(a.response);
+    });
+    kps.resize(max_features);
+  }
+  auto feats = describe_from_pyramid(pyr, kps, kind);
+  if (max_features > 0 && (int)feats.size() > max_features) feats.resize(max_features);
+  return write_features(feats, meta, desc, cap);
+}
+
+// src/pipeline.rs:1581-1629
+int oracle_compute_descriptors(const float* img, int h, int w, const oracle_keypoint* kps_in, int n,
+                               int kind, float* meta, float* desc, int cap) {
+  if (h < 3 || w < 3 || n == 0) return 0;
+  std::vector<oracle_keypoint> kps(kps_in, kps_in + n);
+  unsigned max_layer = 0;
+  for (const auto& kp : kps) max_layer = std::max(max_layer, kp.layer);
+  const int scales = (int)std::max(max_layer, 3u);
+  const float k = std::pow(2.0f, 1.0f / (float)scales);
+  bool upsample = false;
+  for (const auto& kp : kps)
+    if (kp.layer > 0) {
+      const float expected = BASE_SIGMA * (float)(1ull << kp.octave) * powi_f(k, (int)kp.layer);
+      upsample = (kp.scale / expected) < 0.707f;
+      break;
+    }
+  unsigned long long max_oct = 0;
+  for (const auto& kp : kps) {
+    unsigned long long o = kp.layer > 0 ? kp.octave
+                                        : f2u_sat(std::floor(std::log2(std::fmax(kp.scale / BASE_SIGMA, 1.0f))));
+    max_oct = std::max(max_oct, o);
+  }
+  const auto pyr = build_pyramid(make_plane(img, h, w), (int)(max_oct + 1), scales, upsample);
+  return write_features(describe_from_pyramid(pyr, kps, kind), meta, desc, cap);
+}
+
+void oracle_rootsift(const float* d, float* out) { rootsift(d, out); }
+
+// src/pipeline.rs:1024-1030
+void oracle_quantize_u8(const float* d, int n, uint8_t* out) {
+  for (int i = 0; i < n; ++i) {
+    const float v = clampf(std::round(d[i] * 512.0f), 0.0f, 255.0f);
+    out[i] = (uint8_t)f2u_sat(v);
+  }
+}
+
+// src/pipeline.rs:1034-1044
+void oracle_dequantize_u8(const uint8_t* q, int n, float* out) {
+  for (int i = 0; i < n; ++i) out[i] = (float)q[i] * (1.0f / 512.0f);
+  float s = 0.0f;
+  for (int i = 0; i < n; ++i) s += out[i] * out[i];
+  const float norm = std::sqrt(s);
+  if (norm > 1e-7f) {
+    const float inv = 1.0f / norm;
+    for (int i = 0; i < n; ++i) out[i] *= inv;
+  }
+}
+
+// src/catalog.rs:37-45 (u128 little endian: bits 0..63 in word 0)
+void oracle_quantize_u128(const float* d, int n, uint64_t* out) {
+  for (int f = 0; f < n; ++f) {
+    uint64_t lo = 0, hi = 0;
+    for (int i = 0; i < 128; ++i)
+      if (d[(size_t)f * 128 + i] > 0.065f) {
+        if (i < 64) lo |= 1ull << i;
+        else hi |= 1ull << (i - 64);
+      }
+    out[2 * f] = lo;
+    out[2 * f + 1] = hi;
+  }
+}
+
+// src/pipeline.rs:1744-1841
+int oracle_match_descriptors(const float* qd, int nq, const float* td, int nt, const float* qxy, const float* txy,
+                 float ratio, int mutual, oracle_match* out, int cap) {
+  if (nq == 0 || nt < 2) return 0;
+  std::vector<int> ok(nq, 0);
+  std::vector<oracle_match> fwd_all(nq);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int q = 0; q < nq; ++q) {
+    float best = std::numeric_limits<float>::infinity();
+    float second = best;
+    int bi = 0;
+    const float* a = qd + (size_t)q * 128;
+    for (int t = 0; t < nt; ++t) {
+      const float d = dist_sq_early_exit(a, td + (size_t)t * 128, second);
+      if (d < best) {
+        second = best;
+        best = d;
+        bi = t;
+      } else if (d < second) {
+        second = d;
+      }
+    }
+    if (second > 1e-12f && std::isfinite(best)) {
+      const float d1 = std::sqrt(best), d2 = std::sqrt(second);
+      const float r = d1 / d2;
+      if (r < ratio) {
+        oracle_match m;
+        m.query_index = (uint32_t)q;
+        m.target_index = (uint32_t)bi;
+        m.qx = qxy[2 * q];
+        m.qy = qxy[2 * q + 1];
+        m.tx = txy[2 * bi];
+        m.ty = txy[2 * bi + 1];
+        m.distance = d1;
+        m.ratio = r;
+        m.dx = m.tx - m.qx;
+        m.dy = m.ty - m.qy;
+        fwd_all[q] = m;
+        ok[q] = 1;
+      }
+    }
+  }
+  std::vector<oracle_match> fwd;
+  for (int q = 0; q < nq; ++q)
+    if (ok[q]) fwd.push_back(fwd_all[q]);
+  if (mutual && !fwd.empty()) {
+    std::vector<int> keep(fwd.size(), 0);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long long i = 0; i < (long long)fwd.size(); ++i) {
+      const float* t = td + (size_t)fwd[i].target_index * 128;
+      float best = std::numeric_limits<float>::infinity();
+      long long bq = -1;
+      for (int q = 0; q < nq; ++q) {
+        const float d = dist_sq_early_exit(t, qd + (size_t)q * 128, best);
+        if (d < best) {
+          best = d;
+          bq = q;
+        }
+      }
+      keep[i] = bq == (long long)fwd[i].query_index;
+    }
+    std::vector<oracle_match> kept;
+    for (size_t i = 0; i < fwd.size(); ++i)
+      if (keep[i]) kept.push_back(fwd[i]);
+    fwd.swap(kept);
+  }
+  for (int i = 0; i < (int)fwd.size() && i < cap; ++i) out[i] = fwd[i];
+  return (int)fwd.size();
+}
+
+int oracle_similarity_ransac(const oracle_match* m, int n, float thr, uint64_t seed, uint8_t* inlier_mask,
+                             float* model, int* has_model) {
+  std::vector<uint8_t> mask;
+  Sim s{};
+  bool hm = false;
+  const int c = similarity_ransac(m, n, thr, seed, mask, s, hm);
+  if (inlier_mask && n > 0) std::memcpy(inlier_mask, mask.data(), n);
+  if (model) {
+    model[0] = s.a;
+    model[1] = s.b;
+    model[2] = s.tx;
+    model[3] = s.ty;
+    model[4] = s.scale;
+    model[5] = s.rot;
+  }
+  if (has_model) *has_model = hm ? 1 : 0;
+  return c;
+}
+
+int oracle_homography_ransac(const oracle_match* m, int n, float thr, uint64_t sim_seed, uint64_t hom_seed,
+                             uint8_t* inlier_mask, float* h9, int* has_h) {
+  std::vector<uint8_t> mask;
+  double H[3][3] = {{0}};
+  bool hh = false;
+  const int c = homography_ransac(m, n, thr, sim_seed, hom_seed, mask, H, hh);
+  if (inlier_mask && n > 0) std::memcpy(inlier_mask, mask.data(), n);
+  if (h9)
+    for (int r = 0; r < 3; ++r)
+      for (int cc = 0; cc < 3; ++cc) h9[3 * r + cc] = (float)H[r][cc];
+  if (has_h) *has_h = hh ? 1 : 0;
+  return c;
+}
+
+// src/pipeline.rs:2210-2272
+void oracle_summarize_tracking(const oracle_match* m, int n, const float* q_scale, const float* q_ori,
+                               const float* t_scale, const float* t_ori, oracle_tracking* out) {
+  if (n == 0) {
+    *out = {0, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f};
+    return;
+  }
+  std::vector<uint8_t> mask;
+  Sim s;
+  bool hm;
+  similarity_ransac(m, n, 3.0f, 0xD1B54A32D192ED03ull, mask, s, hm);
+  std::vector<const oracle_match*> act;
+  for (int i = 0; i < n; ++i)
+    if (mask[i]) act.push_back(&m[i]);
+  if (act.empty())
+    for (int i = 0; i < n; ++i) act.push_back(&m[i]);
+  const float inv_n = 1.0f / (float)act.size();
+  float sdx = 0, sdy = 0, ssr = 0, ssin = 0, scos = 0;
+  std::vector<float> dxs, dys;
+  for (const oracle_match* a : act) {
+    sdx += a->dx;
+    sdy += a->dy;
+    dxs.push_back(a->dx);
+    dys.push_back(a->dy);
+    const float qs = q_scale[a->query_index], ts = t_scale[a->target_index];
+    if (qs > 1e-6f) ssr += ts / qs;
+    const float dth = t_ori[a->target_index] - q_ori[a->query_index];
+    ssin += std::sin(dth);
+    scos += std::cos(dth);
+  }
+  const float mrot = std::atan2(ssin, scos);
+  out->raw_match_count = (uint32_t)n;
+  out->match_count = (uint32_t)act.size();
+  out->inlier_ratio = (float)act.size() / (float)n;
+  out->mean_dx = sdx * inv_n;
+  out->mean_dy = sdy * inv_n;
+  out->median_dx = median_f32(dxs);
+  out->median_dy = median_f32(dys);
+  out->mean_scale_ratio = ssr * inv_n;
+  out->mean_rotation_deg = mrot * RAD_TO_DEG_F;
+}
+
+// src/catalog.rs:596-633 (MIH: entries > 32) and :707-728 (exhaustive)
+void oracle_hamming_votes(const uint64_t* q, int nq, const uint64_t* cat, const int64_t* offsets, int ne,
+                          int mih, uint32_t* votes) {
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int e = 0; e < ne; ++e) {
+    uint32_t v = 0;
+    for (int qi = 0; qi < nq; ++qi) {
+      const uint64_t q0 = q[2 * qi], q1 = q[2 * qi + 1];
+      bool hit = false;
+      for (int64_t s = offsets[e]; s < offsets[e + 1] && !hit; ++s) {
+        const uint64_t x0 = q0 ^ cat[2 * s], x1 = q1 ^ cat[2 * s + 1];
+        const int d = __builtin_popcountll(x0) + __builtin_popcountll(x1);
+        if (d <= 24 && (!mih || has_zero_byte128(x0, x1))) hit = true;
+      }
+      v += hit ? 1 : 0;
+    }
+    votes[e] = v;
+  }
+}
+
+void oracle_hamming_topk(const uint64_t* q, int nq, const uint64_t* cat, int64_t ncat, int k, uint32_t* idx,
+                         uint32_t* dist) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int qi = 0; qi < nq; ++qi) {
+    // bounded max-heap keyed by (dist, index)
+    std::vector<std::pair<uint32_t, uint32_t>> heap;
+    heap.reserve(k + 1);
+    for (int64_t c = 0; c < ncat; ++c) {
+      const uint32_t d = (uint32_t)popc128(q[2 * qi], q[2 * qi + 1], cat[2 * c], cat[2 * c + 1]);
+      const std::pair<uint32_t, uint32_t> key{d, (uint32_t)c};
+      if ((int)heap.size() < k) {
+        heap.push_back(key);
+        std::push_heap(heap.begin(), heap.end());
+      } else if (key < heap.front()) {
+        std::pop_heap(heap.begin(), heap.end());
+        heap.back() = key;
+        std::push_heap(heap.begin(), heap.end());
+      }
+    }
+    std::sort(heap.begin(), heap.end());
+    for (int j = 0; j < k; ++j) {
+      idx[(size_t)qi * k + j] = j < (int)heap.size() ? heap[j].second : 0xFFFFFFFFu;
+      dist[(size_t)qi * k + j] = j < (int)heap.size() ? heap[j].first : 0xFFFFFFFFu;
+    }
+  }
+}
+
+void oracle_l2_rerank(const float* qd, int nq, const float* cat_desc, const uint32_t* cand, int k,
+                      uint32_t* out_idx, float* out_d2) {
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int qi = 0; qi < nq; ++qi) {
+    std::vector<std::pair<float, uint32_t>> v;
+    for (int j = 0; j < k; ++j) {
+      const uint32_t c = cand[(size_t)qi * k + j];
+      if (c == 0xFFFFFFFFu) continue;
+      float s = 0.0f;
+      for (int i = 0; i < 128; ++i) {
+        const float d = qd[(size_t)qi * 128 + i] - cat_desc[(size_t)c * 128 + i];
+        s += d * d;
+      }
+      v.push_back({s, c});
+    }
+    std::sort(v.begin(), v.end());
+    for (int j = 0; j < k; ++j) {
+      out_idx[(size_t)qi * k + j] = j < (int)v.size() ? v[j].second : 0xFFFFFFFFu;
+      out_d2[(size_t)qi * k + j] = j < (int)v.size() ? v[j].first : INFINITY;
+    }
+  }
+}
+
+}  // extern "C"

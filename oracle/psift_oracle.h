@@ -1,0 +1,109 @@
+/*
+ * psift_oracle.h -- CPU restatement of the pure-sift 0.2.0 feature hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA build:
+ * only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+ * leg may load it.  The product library (libpsift_gpu.so) never links or calls it.
+ *
+ * Pinning: the reference is Rust and cannot be compiled in this environment
+ * (no cargo/rustc, crates.io dependencies not vendored), and the reference
+ * ships no numeric golden vectors.  The restatement is pinned against every
+ * known-answer and property test the reference holds for this path
+ * (tests/pipeline_tests.rs, tests/homography_properties.rs), ported to
+ * tests/test_oracle_pins.py.  Bit-level numeric parity with a Rust build of the
+ * reference is therefore "pinned by the reference's known-answer tests, not by
+ * reference-produced vectors".
+ *
+ * Each function cites the reference file:line it restates.  Arithmetic follows
+ * the Rust source operation by operation: f32 everywhere the reference uses f32,
+ * no FMA contraction (built with -ffp-contract=off), glibc libm for
+ * exp/atan2/sin/cos/pow/log2 (what Rust's f32 methods call on Linux), sequential
+ * summation in the reference's order.
+ */
+#ifndef PSIFT_ORACLE_H
+#define PSIFT_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  float x, y, scale, response;
+  uint32_t octave, layer;
+} oracle_keypoint;
+
+typedef struct {
+  uint32_t query_index, target_index;
+  float qx, qy, tx, ty;
+  float distance, ratio;
+  float dx, dy;
+} oracle_match;
+
+typedef struct {
+  uint32_t raw_match_count, match_count;
+  float inlier_ratio;
+  float mean_dx, mean_dy, median_dx, median_dy;
+  float mean_scale_ratio, mean_rotation_deg;
+} oracle_tracking;
+
+int oracle_gaussian_kernel_1d(float sigma, float* out, int cap);
+void oracle_gaussian_blur(const float* img, int h, int w, float sigma, float* out);
+void oracle_upsample_2x(const float* img, int h, int w, float* out);
+void oracle_luma_to_f32(const uint8_t* px, size_t n, float* out);
+
+void* oracle_pyramid_build(const float* img, int h, int w, int octaves, int scales, int upsample);
+int oracle_pyramid_num_octaves(const void* pyr);
+void oracle_pyramid_octave_info(const void* pyr, int octave, int* h, int* w, float* scale_factor);
+/* kind 0 = Gaussian level idx (0..scales+2), kind 1 = DoG slice idx (0..scales+1) */
+void oracle_pyramid_copy_plane(const void* pyr, int octave, int kind, int idx, float* out);
+int oracle_pyramid_extract_extrema(const void* pyr, float threshold, oracle_keypoint* out, int cap);
+void oracle_pyramid_free(void* pyr);
+
+/* Returns the total feature count (may exceed cap; only cap are written).
+ * meta: 5 floats per feature (x, y, scale, response, orientation). */
+int oracle_detect_and_compute(const float* img, int h, int w, int octaves, int scales,
+                              float threshold, int upsample, int kind, int max_features,
+                              float* meta, float* desc, int cap);
+int oracle_detect_keypoints(const float* img, int h, int w, int octaves, int scales,
+                            float threshold, int upsample, oracle_keypoint* out, int cap);
+int oracle_compute_descriptors(const float* img, int h, int w, const oracle_keypoint* kps, int n,
+                               int kind, float* meta, float* desc, int cap);
+
+void oracle_rootsift(const float* desc, float* out);
+void oracle_quantize_u8(const float* desc, int n, uint8_t* out);
+void oracle_dequantize_u8(const uint8_t* q, int n, float* out);
+void oracle_quantize_u128(const float* desc, int n, uint64_t* out);
+
+int oracle_match_descriptors(const float* qd, int nq, const float* td, int nt, const float* qxy,
+                 const float* txy, float ratio, int mutual, oracle_match* out, int cap);
+
+/* model: a, b, tx, ty, scale, rotation_deg.  Returns inlier count; mask[i] = 1 for inliers. */
+int oracle_similarity_ransac(const oracle_match* m, int n, float thr, uint64_t seed,
+                             uint8_t* inlier_mask, float* model, int* has_model);
+int oracle_homography_ransac(const oracle_match* m, int n, float thr, uint64_t sim_seed,
+                             uint64_t hom_seed, uint8_t* inlier_mask, float* h9, int* has_h);
+/* scales/orientations indexed by the matches' query/target indices. */
+void oracle_summarize_tracking(const oracle_match* m, int n, const float* q_scale,
+                               const float* q_ori, const float* t_scale, const float* t_ori,
+                               oracle_tracking* out);
+
+/* Catalog coarse votes.  codes are 2 x u64 (lo, hi) per signature; entry e owns
+ * codes [offsets[e], offsets[e+1]).  mih != 0 selects the multi-index-hashing
+ * semantics, else the exhaustive scan. */
+void oracle_hamming_votes(const uint64_t* q, int nq, const uint64_t* cat, const int64_t* offsets,
+                          int n_entries, int mih, uint32_t* votes);
+/* Per-query top-k nearest codes by (Hamming distance, global index). */
+void oracle_hamming_topk(const uint64_t* q, int nq, const uint64_t* cat, int64_t ncat, int k,
+                         uint32_t* idx, uint32_t* dist);
+/* Exact FP32 L2^2 re-rank of k candidates per query, sorted by (d2, index). */
+void oracle_l2_rerank(const float* qd, int nq, const float* cat_desc, const uint32_t* cand, int k,
+                      uint32_t* out_idx, float* out_d2);
+
+uint64_t oracle_splitmix64_next(uint64_t* state);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,393 @@
+// K5/K6: canonical orientations (36-bin histogram, circular smoothing, >=80%
+// secondary peaks) and 128-D SIFT / RootSIFT descriptors.
+//
+// Reference: OctaveGradientPlanes::from_gaussian (src/pipeline.rs:1158-1203),
+// resolve_octave_and_layer (:1206-1227), compute_keypoint_orientations
+// (:1233-1347), compute_128d_descriptor (:1352-1480), to_rootsift_descriptor
+// (:1012-1019), compute_sift_descriptors_from_pyramid_with_kind (:1482-1577),
+// and the feature truncation of extract_sift_features_with_kind (:1653-1656).
+//
+// Gradients are computed on the fly from the keypoint's Gaussian level (the
+// reference materialises magnitude/angle planes for every used level; the values
+// per pixel are the same expression).  One warp handles one keypoint (orientation)
+// or one keypoint's orientations in turn (descriptor).  Histogram accumulation is
+// deterministic: each lane owns a private column of a bin-major shared-memory
+// histogram ([bin][lane], conflict-free), and columns are summed in lane order.
+// Per-bin sums therefore differ from the reference's raster-order sums only by
+// f32 rounding; all selection logic (peak tests, sort, truncation) and the final
+// normalisation repeat the reference's sequence exactly.
+#include "detect_plan.cuh"
+#include "psift_internal.cuh"
+
+namespace psift {
+
+constexpr int kOriBins = 36;
+constexpr int kOriWarps = 8;
+constexpr int kDescWarps = 4;
+
+// rem_euclid(v, 2pi) for |v| <= 2pi (fmod is exact: identity below 2pi).
+__device__ __forceinline__ float rem_2pi(float v, float two_pi) {
+  float r = fabsf(v) < two_pi ? v : fmodf(v, two_pi);
+  return r < 0.0f ? r + two_pi : r;
+}
+
+struct OctKp {
+  float x, y, scale;
+  int o, l;
+};
+
+// resolve_octave_and_layer (src/pipeline.rs:1206-1227) + the octave-local keypoint (:1516-1526).
+__device__ __forceinline__ OctKp to_octave(const ImagePlan& P, const psift_keypoint& kp) {
+  OctKp r;
+  const int n_oct = P.n_oct;
+  if (kp.layer > 0) {
+    r.o = min((int)kp.octave, n_oct - 1);
+  } else {
+    const float ratio = fmaxf(kp.scale / kBaseSigma, 1.0f);
+    const float f = floorf(log2f(ratio));
+    r.o = f <= 0.0f ? 0 : min((int)f, n_oct - 1);
+  }
+  r.l = 0;  // resolved by resolve_layer
+  const float sf = P.oct[r.o].scale_factor;
+  const float inv = 1.0f / sf;
+  r.x = kp.x * inv;
+  r.y = kp.y * inv;
+  r.scale = fmaxf(kp.scale * inv, 0.5f * kBaseSigma);
+  return r;
+}
+
+__device__ __forceinline__ int resolve_layer(const psift_keypoint& kp, int o, int scales) {
+  const int g_len = scales + 3;
+  if (kp.layer > 0) return min((int)kp.layer, g_len - 1);
+  const int searchable = max(g_len - 3, 1);
+  const float oct_mult = (float)(1u << o);
+  const float local_sigma = fmaxf(kp.scale / (kBaseSigma * oct_mult), 1.0f);
+  const float v = roundf(log2f(local_sigma) * (float)searchable);
+  const int l = v <= 0.0f ? 0 : (int)v;
+  const int hi = max(g_len - 2, 1);
+  return l < 1 ? 1 : (l > hi ? hi : l);
+}
+
+// Gradient magnitude and angle at interior pixel (x, y) of plane g.
+__device__ __forceinline__ void grad_at(const float* __restrict__ g, long long pitch, int x, int y, float& mag,
+                                        float& ang, float two_pi) {
+  const float* rc = g + (long long)y * pitch;
+  const float dx = rc[x + 1] - rc[x - 1];
+  const float dy = rc[pitch + x] - rc[x - pitch];
+  mag = sqrtf(dx * dx + dy * dy);
+  float a = atan2f(dy, dx);
+  ang = a < 0.0f ? a + two_pi : a;  // rem_euclid(2pi) of a value in [-pi, pi]
+}
+
+// Grid (ceil(sel_cap / 8), images), 256 threads: one warp per selected keypoint.
+__global__ void __launch_bounds__(kOriWarps * 32) orientation_kernel(const ImagePlan* __restrict__ plans,
+                                                                     DescribeParams prm) {
+  const ImagePlan& P = plans[blockIdx.y];
+  __shared__ float s_hist[kOriWarps][kOriBins][32];
+  __shared__ float s_bins[kOriWarps][kOriBins];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t i = blockIdx.x * kOriWarps + warp;
+  if (i >= *P.sel_count) return;
+  const psift_keypoint kp = P.sel[i];
+  OctKp ok = to_octave(P, kp);
+  ok.l = resolve_layer(kp, ok.o, prm.scales);
+  const OctaveDev& O = P.oct[ok.o];
+  const float* g = O.g + (long long)ok.l * O.plane_stride;
+  const float two_pi = 2.0f * kPiF;
+
+  float (*hist)[32] = s_hist[warp];
+  for (int b = 0; b < kOriBins; ++b) hist[b][lane] = 0.0f;
+
+  const float sigma_ori = fmaxf(1.5f * ok.scale, 1.0f);
+  const float two_sigma_sq = 2.0f * sigma_ori * sigma_ori;
+  int radius = (int)ceilf(3.0f * sigma_ori);
+  radius = radius < 2 ? 2 : radius;
+  const int cx = (int)roundf(ok.x), cy = (int)roundf(ok.y);
+  const float bin_scale = (float)kOriBins / two_pi;
+  const int y_min = max(cy - radius, 1);
+  const int y_max = max(min(cy + radius, O.h - 2), 1);
+  const int x_min = max(cx - radius, 1);
+  const int x_max = max(min(cx + radius, O.w - 2), 1);
+  const float r_sq_max = (float)(radius * radius);
+  const int wx = x_max - x_min + 1;
+  const int n = (y_max >= y_min && x_max >= x_min) ? (y_max - y_min + 1) * wx : 0;
+  const bool planes_ok = O.h >= 3 && O.w >= 3;
+  for (int t = lane; planes_ok && t < n; t += 32) {
+    const int yy = y_min + t / wx, xx = x_min + t % wx;
+    const float dy = (float)(yy - cy), dx = (float)(xx - cx);
+    const float r_sq = dx * dx + dy * dy;
+    if (r_sq > r_sq_max) continue;
+    float m, ang;
+    grad_at(g, O.pitch, xx, yy, m, ang, two_pi);
+    if (m <= 1e-7f) continue;
+    const float weight = expf(-r_sq / two_sigma_sq);
+    const int bin = ((int)floorf(ang * bin_scale)) % kOriBins;
+    hist[bin][lane] += m * weight;
+  }
+  __syncwarp();
+  for (int b = lane; b < kOriBins; b += 32) {
+    float s = 0.0f;
+    for (int j = 0; j < 32; ++j) s += hist[b][j];
+    s_bins[warp][b] = s;
+  }
+  __syncwarp();
+  if (lane != 0) return;
+  const float* hb = s_bins[warp];
+  float sm[kOriBins];
+  for (int b = 0; b < kOriBins; ++b) {
+    const float prev = hb[(b + kOriBins - 1) % kOriBins];
+    const float cur = hb[b];
+    const float next = hb[(b + 1) % kOriBins];
+    sm[b] = (prev + cur + next) * (1.0f / 3.0f);
+  }
+  int best_bin = 0;
+  float best_val = sm[0];
+  for (int b = 1; b < kOriBins; ++b)
+    if (sm[b] > best_val) {
+      best_val = sm[b];
+      best_bin = b;
+    }
+  float* out = P.oris + (size_t)i * 4;
+  if (best_val <= 1e-7f) {
+    out[0] = 0.0f;
+    P.ori_count[i] = 1;
+    return;
+  }
+  const float split = 0.80f * best_val;
+  // Peaks sorted by (value desc, bin asc), at most 4: insertion into a 4-slot list.
+  int pk_bin[4];
+  float pk_val[4];
+  int np = 0;
+  for (int b = 0; b < kOriBins; ++b) {
+    const float v = sm[b];
+    if (v < split) continue;
+    const float l = sm[(b + kOriBins - 1) % kOriBins];
+    const float r = sm[(b + 1) % kOriBins];
+    if (v > l && v >= r) {
+      // bins arrive ascending: a new peak goes after every peak with value >= v
+      int pos = np;
+      while (pos > 0 && pk_val[pos - 1] < v) --pos;
+      if (pos < 4) {
+        const int last = np < 4 ? np : 3;
+        for (int q = last; q > pos; --q) {
+          pk_bin[q] = pk_bin[q - 1];
+          pk_val[q] = pk_val[q - 1];
+        }
+        pk_bin[pos] = b;
+        pk_val[pos] = v;
+        if (np < 4) ++np;
+      }
+    }
+  }
+  if (np == 0) {
+    pk_bin[0] = best_bin;
+    pk_val[0] = best_val;
+    np = 1;
+  }
+  for (int q = 0; q < np; ++q) {
+    const int bin = pk_bin[q];
+    const float val = pk_val[q];
+    const float l = sm[(bin + kOriBins - 1) % kOriBins];
+    const float r = sm[(bin + 1) % kOriBins];
+    const float denom = l - 2.0f * val + r;
+    float off = fabsf(denom) > 1e-6f ? 0.5f * (l - r) / denom : 0.0f;
+    off = off < -0.5f ? -0.5f : (off > 0.5f ? 0.5f : off);
+    const float th = (((float)bin + 0.5f) + off) * (two_pi / (float)kOriBins);
+    out[q] = rem_2pi(th, two_pi);
+  }
+  P.ori_count[i] = (uint32_t)np;
+}
+
+// Exclusive offsets of orientations per keypoint; feature count = min(total, cap).
+__global__ void __launch_bounds__(1024) feature_scan_kernel(const ImagePlan* __restrict__ plans, uint32_t max_features) {
+  const ImagePlan& P = plans[blockIdx.x];
+  __shared__ uint32_t s_warp[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint32_t n = *P.sel_count;
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < n; base += 1024) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = i < n ? P.ori_count[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t w = s_warp[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += t;
+      }
+      s_warp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t pre = wid > 0 ? s_warp[wid - 1] : 0u;
+    if (i < n) P.feat_offsets[i] = carry + pre + x - v;
+    carry += s_warp[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    uint32_t f = carry;
+    if (max_features > 0 && f > max_features) f = max_features;
+    if (f > P.feat_cap) f = P.feat_cap;
+    *P.feat_count = f;
+    *P.feat_total = carry;
+    if (P.out_count) *P.out_count = f;
+  }
+}
+
+// Grid (ceil(sel_cap / 4), images), 128 threads: one warp per keypoint, one
+// descriptor per orientation.
+__global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const ImagePlan* __restrict__ plans,
+                                                                     DescribeParams prm) {
+  const ImagePlan& P = plans[blockIdx.y];
+  extern __shared__ float s_dyn[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t i = blockIdx.x * kDescWarps + warp;
+  if (i >= *P.sel_count) return;
+  const uint32_t fcount = *P.feat_count;
+  const uint32_t f0 = P.feat_offsets[i];
+  if (f0 >= fcount) return;
+  float (*hist)[32] = reinterpret_cast<float (*)[32]>(s_dyn + warp * (kDescLen * 32 + kDescLen));
+  float* desc = s_dyn + warp * (kDescLen * 32 + kDescLen) + kDescLen * 32;
+
+  const psift_keypoint kp = P.sel[i];
+  OctKp ok = to_octave(P, kp);
+  ok.l = resolve_layer(kp, ok.o, prm.scales);
+  const OctaveDev& O = P.oct[ok.o];
+  const float* g = O.g + (long long)ok.l * O.plane_stride;
+  const float two_pi = 2.0f * kPiF;
+  const uint32_t nori = P.ori_count[i];
+
+  const float hist_width = fmaxf(3.0f * ok.scale, 1.5f);
+  const float inv_hw = 1.0f / hist_width;
+  const float exp_scale = -1.0f / (2.0f * 2.0f * 2.0f);
+  const float sqrt2 = 1.41421356237309504880f;
+  int max_radius = (int)ceilf(hist_width * sqrt2 * (4.0f + 1.0f) * 0.5f);
+  max_radius = max_radius < 4 ? 4 : max_radius;
+  const int cx = (int)roundf(ok.x), cy = (int)roundf(ok.y);
+  const int y_min = max(cy - max_radius, 1);
+  const int y_max = max(min(cy + max_radius, O.h - 2), 1);
+  const int x_min = max(cx - max_radius, 1);
+  const int x_max = max(min(cx + max_radius, O.w - 2), 1);
+  const int wx = x_max - x_min + 1;
+  const int n = (y_max >= y_min && x_max >= x_min) ? (y_max - y_min + 1) * wx : 0;
+  const float bin_per_rad = 8.0f / two_pi;
+  const bool planes_ok = O.h >= 3 && O.w >= 3;
+
+  for (uint32_t q = 0; q < nori; ++q) {
+    const uint32_t f = f0 + q;
+    if (f >= fcount) break;
+    const float theta = P.oris[(size_t)i * 4 + q];
+    for (int b = 0; b < kDescLen; ++b) hist[b][lane] = 0.0f;
+    const float cos_t = cosf(theta), sin_t = sinf(theta);
+    for (int t = lane; planes_ok && t < n; t += 32) {
+      const int yy = y_min + t / wx, xx = x_min + t % wx;
+      const float dy = (float)yy - ok.y;
+      const float dx = (float)xx - ok.x;
+      const float r_rot = (dx * cos_t + dy * sin_t) * inv_hw;
+      const float c_rot = (-dx * sin_t + dy * cos_t) * inv_hw;
+      const float r_bin = r_rot + 4.0f * 0.5f - 0.5f;
+      const float c_bin = c_rot + 4.0f * 0.5f - 0.5f;
+      if (r_bin <= -1.0f || r_bin >= 4.0f || c_bin <= -1.0f || c_bin >= 4.0f) continue;
+      float m, ang;
+      grad_at(g, O.pitch, xx, yy, m, ang, two_pi);
+      if (m <= 1e-7f) continue;
+      const float w_gauss = expf((r_rot * r_rot + c_rot * c_rot) * exp_scale);
+      const float wm = m * w_gauss;
+      const float rel = rem_2pi(ang - theta, two_pi);
+      const float o_bin = rel * bin_per_rad;
+      const int r0 = (int)floorf(r_bin), c0 = (int)floorf(c_bin), o0 = (int)floorf(o_bin);
+      const float dr = r_bin - (float)r0, dc = c_bin - (float)c0, dof = o_bin - (float)o0;
+#pragma unroll
+      for (int ir = 0; ir <= 1; ++ir) {
+        const int rb = r0 + ir;
+        if (rb < 0 || rb >= 4) continue;
+        const float wr = ir == 0 ? 1.0f - dr : dr;
+#pragma unroll
+        for (int ic = 0; ic <= 1; ++ic) {
+          const int cb = c0 + ic;
+          if (cb < 0 || cb >= 4) continue;
+          const float wc = ic == 0 ? 1.0f - dc : dc;
+#pragma unroll
+          for (int io = 0; io <= 1; ++io) {
+            const int ob = (o0 + io) & 7;
+            const float wo = io == 0 ? 1.0f - dof : dof;
+            hist[(rb * 4 + cb) * 8 + ob][lane] += wm * wr * wc * wo;
+          }
+        }
+      }
+    }
+    __syncwarp();
+    for (int b = lane; b < kDescLen; b += 32) {
+      float s = 0.0f;
+      for (int j = 0; j < 32; ++j) s += hist[b][j];
+      desc[b] = s;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      // L2 -> clamp 0.2 -> L2 (src/pipeline.rs:1462-1477), sequential sums.
+      float n1 = 0.0f;
+      for (int b = 0; b < kDescLen; ++b) n1 += desc[b] * desc[b];
+      n1 = sqrtf(n1);
+      if (n1 > 1e-7f) {
+        const float inv1 = 1.0f / n1;
+        for (int b = 0; b < kDescLen; ++b) desc[b] = fminf(desc[b] * inv1, 0.2f);
+        float n2 = 0.0f;
+        for (int b = 0; b < kDescLen; ++b) n2 += desc[b] * desc[b];
+        n2 = sqrtf(n2);
+        if (n2 > 1e-7f) {
+          const float inv2 = 1.0f / n2;
+          for (int b = 0; b < kDescLen; ++b) desc[b] *= inv2;
+        }
+      }
+      if (prm.descriptor_kind == 1) {
+        // to_rootsift_descriptor (src/pipeline.rs:1012-1019)
+        float l1 = 0.0f;
+        for (int b = 0; b < kDescLen; ++b) l1 += fmaxf(desc[b], 0.0f);
+        if (l1 > 1e-7f) {
+          const float inv = 1.0f / l1;
+          for (int b = 0; b < kDescLen; ++b) desc[b] = sqrtf(fmaxf(desc[b], 0.0f) * inv);
+        }
+      }
+      P.fx[f] = kp.x;
+      P.fy[f] = kp.y;
+      P.fscale[f] = kp.scale;
+      P.fresp[f] = kp.response;
+      P.fori[f] = theta;
+    }
+    __syncwarp();
+    float4* dst = reinterpret_cast<float4*>(P.fdesc + (size_t)f * kDescLen);
+    dst[lane] = reinterpret_cast<const float4*>(desc)[lane];
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_orientation(const ImagePlan* plans, int n, uint32_t sel_cap, const DescribeParams& prm,
+                               cudaStream_t st) {
+  dim3 grid((sel_cap + kOriWarps - 1) / kOriWarps, n);
+  orientation_kernel<<<grid, kOriWarps * 32, 0, st>>>(plans, prm);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_feature_scan(const ImagePlan* plans, int n, uint32_t max_features, cudaStream_t st) {
+  feature_scan_kernel<<<n, 1024, 0, st>>>(plans, max_features);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_descriptor(const ImagePlan* plans, int n, uint32_t sel_cap, const DescribeParams& prm,
+                              cudaStream_t st) {
+  const size_t smem = sizeof(float) * kDescWarps * (kDescLen * 32 + kDescLen);
+  cudaError_t e = ensure_smem_attr((const void*)descriptor_kernel, smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((sel_cap + kDescWarps - 1) / kDescWarps, n);
+  descriptor_kernel<<<grid, kDescWarps * 32, smem, st>>>(plans, prm);
+  return cudaGetLastError();
+}
+
+}  // namespace psift

@@ -1,0 +1,520 @@
+// Orchestration of the detect-and-describe path and its C-ABI entry points.
+//
+// Reference call stack (src/pipeline.rs): Sift::detect_and_compute (:136-145)
+// -> extract_sift_features_with_kind (:1633-1658) -> Pyramid::build_with_params
+// (:519-530) -> build_scale_space_pyramid_with_options (:550-638), then
+// Pyramid::extract_extrema (:535-547), the 4096 cap, and
+// compute_sift_descriptors_from_pyramid_with_kind (:1482-1577).
+//
+// One call processes a batch of images; every kernel covers the whole batch
+// (blockIdx.z / blockIdx.y = image), so uneven image sizes share one launch per
+// stage.  Host code only computes the octave geometry and the f32 blur weights
+// (the reference's own formula, evaluated with the same libm) and carves the
+// workspace; all data-dependent work stays on the device.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "detect_plan.cuh"
+#include "psift_internal.cuh"
+
+namespace psift {
+
+// Declared in pyramid.cu / extrema.cu / describe.cu.
+cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
+                        int level, int down_level, int max_h, int max_w, cudaStream_t st);
+cudaError_t launch_extrema_mark(const ImagePlan* plans, int n, int octave, int max_h, const ExtremaParams& prm,
+                                cudaStream_t st);
+cudaError_t launch_row_scan(const ImagePlan* plans, int n, uint32_t kp_cap, uint32_t* err, cudaStream_t st);
+cudaError_t launch_extrema_emit(const ImagePlan* plans, int n, int octave, int max_h, const ExtremaParams& prm,
+                                uint32_t kp_cap, cudaStream_t st);
+cudaError_t launch_select_topk(const ImagePlan* plans, int n, uint32_t kp_cap, uint32_t max_features, uint32_t* err,
+                               cudaStream_t st);
+cudaError_t launch_orientation(const ImagePlan* plans, int n, uint32_t sel_cap, const DescribeParams& prm,
+                               cudaStream_t st);
+cudaError_t launch_feature_scan(const ImagePlan* plans, int n, uint32_t max_features, cudaStream_t st);
+cudaError_t launch_descriptor(const ImagePlan* plans, int n, uint32_t sel_cap, const DescribeParams& prm,
+                              cudaStream_t st);
+
+namespace {
+
+constexpr uint32_t kDefaultKeypointCapacity = 1u << 18;
+
+// f32::powi lowers to square-and-multiply (low bit first); same sequence here.
+float powi_f(float a, int b) {
+  const bool recip = b < 0;
+  float r = 1.0f;
+  for (;;) {
+    if (b & 1) r *= a;
+    b /= 2;
+    if (b == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0f / r : r;
+}
+
+// gaussian_kernel_1d (src/pipeline.rs:275-296), evaluated on the host in f32.
+std::vector<float> gaussian_taps(float sigma) {
+  const float cs = std::fmax(sigma, 1e-3f);
+  long long radius = (long long)std::ceil(3.0f * cs);
+  if (radius < 1) radius = 1;
+  const float two_sigma_sq = 2.0f * cs * cs;
+  const float norm = 1.0f / (std::sqrt(2.0f * kPiF) * cs);
+  std::vector<float> k;
+  for (long long x = -radius; x <= radius; ++x) {
+    const float xf = (float)x;
+    k.push_back(norm * std::exp(-((xf * xf) / two_sigma_sq)));
+  }
+  float sum = 0.0f;
+  for (float v : k) sum += v;
+  if (sum > 0.0f) {
+    const float inv = 1.0f / sum;
+    for (float& v : k) v *= inv;
+  }
+  return k;
+}
+
+struct HostOctave {
+  int h, w;
+  long long pitch;
+};
+
+// Octave geometry of build_scale_space_pyramid_with_options: stop when the base
+// is smaller than 3x3; downsample_2x floors and returns 0x0 when a side hits 0.
+int plan_octaves(int h, int w, int octaves, bool upsample, HostOctave* out) {
+  int ch = upsample ? 2 * h : h, cw = upsample ? 2 * w : w;
+  int n = 0;
+  if (h == 0 || w == 0) return 0;
+  for (int o = 0; o < octaves && o < kMaxOctaves; ++o) {
+    if (ch < 3 || cw < 3) break;
+    out[n++] = {ch, cw, (long long)align_up((size_t)cw, 32)};
+    int nh = ch / 2, nw = cw / 2;
+    if (nh == 0 || nw == 0) nh = nw = 0;
+    ch = nh;
+    cw = nw;
+  }
+  return n;
+}
+
+struct SigmaSchedule {
+  std::vector<float> init_taps;
+  int init_radius;
+  std::vector<std::vector<float>> level_taps;  // index s = 1..S+2
+  std::vector<int> level_radius;
+  float k;
+};
+
+SigmaSchedule make_schedule(int scales, bool upsample) {
+  SigmaSchedule sc;
+  sc.k = std::pow(2.0f, 1.0f / (float)scales);
+  const float sigma_in = upsample ? 2.0f * kAssumedInputSigma : kAssumedInputSigma;
+  const float init_sigma = std::sqrt(std::fmax(kBaseSigma * kBaseSigma - sigma_in * sigma_in, 1e-4f));
+  sc.init_taps = gaussian_taps(init_sigma);
+  sc.init_radius = (int)sc.init_taps.size() / 2;
+  sc.level_taps.resize(scales + 3);
+  sc.level_radius.assign(scales + 3, 0);
+  float prev = kBaseSigma;
+  for (int s = 1; s <= scales + 2; ++s) {
+    const float target = kBaseSigma * powi_f(sc.k, s);
+    const float delta = std::sqrt(std::fmax(target * target - prev * prev, 1e-4f));
+    sc.level_taps[s] = gaussian_taps(delta);
+    sc.level_radius[s] = (int)sc.level_taps[s].size() / 2;
+    prev = target;
+  }
+  return sc;
+}
+
+struct DetectJob {
+  int n = 0;
+  std::vector<ImagePlan> plans;      // host copy
+  std::vector<HostOctave> oct;       // n * kMaxOctaves
+  std::vector<int> n_oct;
+  ImagePlan* d_plans = nullptr;
+  uint32_t kp_cap = 0, sel_cap = 0;
+};
+
+struct ImageDesc {
+  const void* src;      // device pointer
+  long long stride;
+  int h, w;
+  int kind;             // SRC_F32 / SRC_U8
+  // device outputs (nullptr: allocate in the workspace)
+  float *fx, *fy, *fscale, *fresp, *fori, *fdesc;
+  uint32_t feat_cap;
+  uint32_t* out_count;
+};
+
+size_t plane_bytes(const HostOctave& o) { return sizeof(float) * (size_t)o.pitch * o.h; }
+
+// Sizes and carves the workspace for n images; fills job.plans (host) with device pointers.
+psift_status build_job(psift_ctx* ctx, const std::vector<ImageDesc>& imgs, const psift_sift_config& cfg,
+                       DetectJob& job, size_t extra_bytes, void** extra_ptr) {
+  const int n = (int)imgs.size();
+  const int S = (int)cfg.scales;
+  job.n = n;
+  job.kp_cap = kDefaultKeypointCapacity;
+  job.sel_cap = cfg.max_features ? cfg.max_features : job.kp_cap;
+  job.oct.assign((size_t)n * kMaxOctaves, HostOctave{0, 0, 0});
+  job.n_oct.assign(n, 0);
+  size_t total = align_up(sizeof(ImagePlan) * n, 256) + align_up(extra_bytes, 256);
+  for (int i = 0; i < n; ++i) {
+    job.n_oct[i] = plan_octaves(imgs[i].h, imgs[i].w, (int)cfg.octaves, cfg.upsample_first_octave != 0,
+                                &job.oct[(size_t)i * kMaxOctaves]);
+    int rows = 0;
+    for (int o = 0; o < job.n_oct[i]; ++o) {
+      const HostOctave& O = job.oct[(size_t)i * kMaxOctaves + o];
+      total += align_up(plane_bytes(O) * (2 * S + 5), 256);
+      total += align_up(sizeof(uint32_t) * (size_t)S * O.h * ((O.w + 31) / 32), 256);
+      rows += S * O.h;
+    }
+    total += 2 * align_up(sizeof(uint32_t) * (size_t)rows + 4, 256);
+    total += align_up(sizeof(psift_keypoint) * job.kp_cap, 256) + align_up(sizeof(psift_keypoint) * job.sel_cap, 256);
+    total += align_up(sizeof(float) * 4 * job.sel_cap, 256) + 2 * align_up(sizeof(uint32_t) * job.sel_cap, 256);
+    total += 256;  // counters
+    if (!imgs[i].fx) total += align_up(sizeof(float) * imgs[i].feat_cap * (5 + kDescLen), 256) + 5 * 256;
+  }
+  psift_status st = arena_reserve(ctx, total);
+  if (st != PSIFT_OK) return st;
+  job.d_plans = (ImagePlan*)arena_alloc(ctx, sizeof(ImagePlan) * n);
+  if (extra_ptr) *extra_ptr = extra_bytes ? arena_alloc(ctx, extra_bytes) : nullptr;
+  job.plans.assign(n, ImagePlan{});
+  for (int i = 0; i < n; ++i) {
+    ImagePlan& P = job.plans[i];
+    std::memset(&P, 0, sizeof(P));
+    P.src = imgs[i].src;
+    P.src_stride = imgs[i].stride;
+    P.src_h = imgs[i].h;
+    P.src_w = imgs[i].w;
+    P.src_kind = imgs[i].kind;
+    P.upsample = cfg.upsample_first_octave != 0;
+    P.n_oct = job.n_oct[i];
+    int row_base = 0;
+    const float base_mult = cfg.upsample_first_octave ? 0.5f : 1.0f;
+    for (int o = 0; o < P.n_oct; ++o) {
+      const HostOctave& H = job.oct[(size_t)i * kMaxOctaves + o];
+      OctaveDev& O = P.oct[o];
+      O.h = H.h;
+      O.w = H.w;
+      O.pitch = H.pitch;
+      O.plane_stride = H.pitch * H.h;
+      float* planes = (float*)arena_alloc(ctx, plane_bytes(H) * (2 * S + 5));
+      O.g = planes;
+      O.d = planes + O.plane_stride * (S + 3);
+      O.words = (H.w + 31) / 32;
+      O.masks = (uint32_t*)arena_alloc(ctx, sizeof(uint32_t) * (size_t)S * H.h * O.words);
+      O.row_base = row_base;
+      O.scale_factor = base_mult * (float)(1ull << o);
+      row_base += S * H.h;
+    }
+    P.total_rows = row_base;
+    P.row_counts = (uint32_t*)arena_alloc(ctx, sizeof(uint32_t) * (size_t)row_base + 4);
+    P.row_offsets = (uint32_t*)arena_alloc(ctx, sizeof(uint32_t) * (size_t)row_base + 4);
+    P.kps = (psift_keypoint*)arena_alloc(ctx, sizeof(psift_keypoint) * job.kp_cap);
+    P.sel = (psift_keypoint*)arena_alloc(ctx, sizeof(psift_keypoint) * job.sel_cap);
+    P.oris = (float*)arena_alloc(ctx, sizeof(float) * 4 * job.sel_cap);
+    P.ori_count = (uint32_t*)arena_alloc(ctx, sizeof(uint32_t) * job.sel_cap);
+    P.feat_offsets = (uint32_t*)arena_alloc(ctx, sizeof(uint32_t) * job.sel_cap);
+    uint32_t* counters = (uint32_t*)arena_alloc(ctx, 256);
+    P.kp_count = counters + 0;
+    P.sel_count = counters + 1;
+    P.feat_count = counters + 2;
+    P.feat_total = counters + 3;
+    P.out_count = imgs[i].out_count;
+    P.feat_cap = imgs[i].feat_cap;
+    if (imgs[i].fx) {
+      P.fx = imgs[i].fx;
+      P.fy = imgs[i].fy;
+      P.fscale = imgs[i].fscale;
+      P.fresp = imgs[i].fresp;
+      P.fori = imgs[i].fori;
+      P.fdesc = imgs[i].fdesc;
+    } else {
+      const size_t fc = imgs[i].feat_cap;
+      P.fx = (float*)arena_alloc(ctx, sizeof(float) * fc);
+      P.fy = (float*)arena_alloc(ctx, sizeof(float) * fc);
+      P.fscale = (float*)arena_alloc(ctx, sizeof(float) * fc);
+      P.fresp = (float*)arena_alloc(ctx, sizeof(float) * fc);
+      P.fori = (float*)arena_alloc(ctx, sizeof(float) * fc);
+      P.fdesc = (float*)arena_alloc(ctx, sizeof(float) * fc * kDescLen);
+    }
+    if (!P.row_offsets || !P.kps || !P.fdesc || !counters) return set_error(ctx, PSIFT_ERR_INTERNAL, "workspace carve overflow");
+  }
+  return PSIFT_OK;
+}
+
+// Queue every stage of the path for the batch (no host synchronisation).
+// stop_after_keypoints: end after extrema_emit (Sift::detect_keypoints).
+psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_config& cfg, bool stop_after_keypoints) {
+  cudaStream_t st = ctx->stream;
+  const int n = job.n;
+  const int S = (int)cfg.scales;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice, st));
+  const SigmaSchedule sc = make_schedule(S, cfg.upsample_first_octave != 0);
+  int max_oct = 0;
+  for (int i = 0; i < n; ++i) max_oct = std::max(max_oct, job.n_oct[i]);
+  if (max_oct == 0) {
+    // Every image is empty/too small: zero all counters.
+    for (int i = 0; i < n; ++i) {
+      PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(job.plans[i].kp_count, 0, 16, st));
+      if (job.plans[i].out_count) PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(job.plans[i].out_count, 0, 4, st));
+    }
+    return PSIFT_OK;
+  }
+  auto max_dims = [&](int o, int& mh, int& mw) {
+    mh = mw = 0;
+    for (int i = 0; i < n; ++i)
+      if (o < job.n_oct[i]) {
+        mh = std::max(mh, job.oct[(size_t)i * kMaxOctaves + o].h);
+        mw = std::max(mw, job.oct[(size_t)i * kMaxOctaves + o].w);
+      }
+  };
+  // Octave-0 base: luma -> f32 (+ 2x bilinear upsample) + initial blur.
+  {
+    int mh, mw;
+    max_dims(0, mh, mw);
+    const bool up = cfg.upsample_first_octave != 0;
+    const int kind = job.plans[0].src_kind;
+    const int mode = kind == SRC_U8 ? (up ? 4 : 2) : (up ? 3 : 1);
+    cudaError_t e = launch_blur(mode, sc.init_taps.data(), sc.init_radius, job.d_plans, n, 0, 0, -1, mh, mw, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "blur(init)");
+  }
+  ExtremaParams xp;
+  std::memset(&xp, 0, sizeof xp);
+  xp.threshold = cfg.contrast_threshold;
+  xp.scales = S;
+  xp.k = sc.k;
+  const float base_mult = cfg.upsample_first_octave ? 0.5f : 1.0f;
+  for (int o = 0; o < kMaxOctaves; ++o) {
+    const float mult = base_mult * (float)(1ull << o);
+    for (int s = 0; s <= S && s < 11; ++s) xp.eff_scale[o][s] = kBaseSigma * mult * powi_f(sc.k, s);
+  }
+  for (int o = 0; o < max_oct; ++o) {
+    int mh, mw;
+    max_dims(o, mh, mw);
+    for (int s = 1; s <= S + 2; ++s) {
+      cudaError_t e = launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, n, o, s, S, mh, mw, st);
+      ctx->launches++;
+      if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
+    }
+    cudaError_t e = launch_extrema_mark(job.d_plans, n, o, mh, xp, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "extrema_mark");
+  }
+  cudaError_t e = launch_row_scan(job.d_plans, n, job.kp_cap, ctx->d_error, st);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "row_scan");
+  for (int o = 0; o < max_oct; ++o) {
+    int mh, mw;
+    max_dims(o, mh, mw);
+    e = launch_extrema_emit(job.d_plans, n, o, mh, xp, job.kp_cap, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "extrema_emit");
+  }
+  if (stop_after_keypoints) return PSIFT_OK;
+  e = launch_select_topk(job.d_plans, n, job.kp_cap, cfg.max_features, ctx->d_error, st);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "select_topk");
+  DescribeParams dp{S, cfg.max_features, cfg.descriptor_kind};
+  e = launch_orientation(job.d_plans, n, job.sel_cap, dp, st);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "orientation");
+  e = launch_feature_scan(job.d_plans, n, cfg.max_features, st);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "feature_scan");
+  e = launch_descriptor(job.d_plans, n, job.sel_cap, dp, st);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "descriptor");
+  return PSIFT_OK;
+}
+
+psift_status check_common(psift_ctx* ctx, const psift_sift_config* cfg) {
+  if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  char msg[256];
+  psift_status st = psift_sift_config_validate(cfg, msg, sizeof msg);
+  if (st != PSIFT_OK) return set_error(ctx, st, msg);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_error(ctx, e, "cudaSetDevice");
+  return PSIFT_OK;
+}
+
+psift_status read_error_word(psift_ctx* ctx, uint32_t* host_word) {
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(host_word, ctx->d_error, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  return PSIFT_OK;
+}
+
+psift_status error_from_word(psift_ctx* ctx, uint32_t w) {
+  if (w & kErrKeypointCapacity)
+    return set_error(ctx, PSIFT_ERR_CAPACITY, "more DoG extrema than the keypoint workspace holds (262144)");
+  if (w & kErrSortCapacity) return set_error(ctx, PSIFT_ERR_INTERNAL, "top-K selection inconsistency");
+  if (w & kErrTimeout) return set_error(ctx, PSIFT_ERR_TIMEOUT, "device wait timed out");
+  return PSIFT_OK;
+}
+
+// Host-pointer detect_and_compute for one image (f32 or u8 source).
+psift_status detect_host(psift_ctx* ctx, const void* image, int kind, uint32_t h, uint32_t w, size_t stride,
+                         const psift_sift_config* cfg, psift_features* out) {
+  psift_status st = check_common(ctx, cfg);
+  if (st != PSIFT_OK) return st;
+  if (!out || (h && w && !image) || stride < w) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad image/output argument");
+  const size_t esz = kind == SRC_U8 ? 1 : 4;
+  const size_t img_bytes = esz * (size_t)h * w;
+  const uint32_t feat_cap = cfg->max_features ? cfg->max_features : std::min<uint32_t>(out->capacity ? out->capacity : 1, 4u * kDefaultKeypointCapacity);
+  ImageDesc d{};
+  d.stride = w;
+  d.h = (int)h;
+  d.w = (int)w;
+  d.kind = kind;
+  d.feat_cap = feat_cap;
+  std::vector<ImageDesc> imgs{d};
+  DetectJob job;
+  void* d_img = nullptr;
+  st = build_job(ctx, imgs, *cfg, job, img_bytes, &d_img);
+  if (st != PSIFT_OK) return st;
+  job.plans[0].src = d_img;
+  // stage the image (tight rows) through pinned memory
+  const size_t meta_bytes = 64;
+  st = pinned_reserve(ctx, std::max(img_bytes, (size_t)feat_cap * sizeof(float) * (5 + kDescLen)) + meta_bytes);
+  if (st != PSIFT_OK) return st;
+  char* pin = ctx->pinned.base;
+  for (uint32_t y = 0; y < h; ++y)
+    std::memcpy(pin + (size_t)y * w * esz, (const char*)image + (size_t)y * stride * esz, (size_t)w * esz);
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream));
+  if (img_bytes) PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_img, pin, img_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  st = launch_detect(ctx, job, *cfg, false);
+  if (st != PSIFT_OK) return st;
+  uint32_t* hmeta = (uint32_t*)(pin + ctx->pinned.capacity - meta_bytes);
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hmeta, job.plans[0].kp_count, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  st = read_error_word(ctx, hmeta + 4);
+  if (st != PSIFT_OK) return st;
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  st = error_from_word(ctx, hmeta[4]);
+  if (st != PSIFT_OK) return st;
+  const uint32_t count = hmeta[2];
+  const uint32_t total = cfg->max_features ? count : hmeta[3];
+  if (total > out->capacity) {
+    out->count = total;
+    return set_error(ctx, PSIFT_ERR_CAPACITY, "feature output capacity too small");
+  }
+  if (count && (!out->x || !out->y || !out->scale || !out->response || !out->orientation || !out->descriptors))
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null feature output array");
+  const ImagePlan& P = job.plans[0];
+  float* hp = (float*)pin;
+  const size_t c = count;
+  if (c) {
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 0 * c, P.fx, 4 * c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 1 * c, P.fy, 4 * c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 2 * c, P.fscale, 4 * c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 3 * c, P.fresp, 4 * c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 4 * c, P.fori, 4 * c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 5 * c, P.fdesc, 4 * c * kDescLen, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out->x, hp + 0 * c, 4 * c);
+    std::memcpy(out->y, hp + 1 * c, 4 * c);
+    std::memcpy(out->scale, hp + 2 * c, 4 * c);
+    std::memcpy(out->response, hp + 3 * c, 4 * c);
+    std::memcpy(out->orientation, hp + 4 * c, 4 * c);
+    std::memcpy(out->descriptors, hp + 5 * c, 4 * c * kDescLen);
+  }
+  out->count = count;
+  return PSIFT_OK;
+}
+
+}  // namespace
+}  // namespace psift
+
+using namespace psift;
+
+extern "C" {
+
+psift_status psift_detect_and_compute(psift_ctx* ctx, const float* image, uint32_t height, uint32_t width,
+                                      size_t row_stride, const psift_sift_config* cfg, psift_features* out) {
+  return detect_host(ctx, image, SRC_F32, height, width, row_stride, cfg, out);
+}
+
+psift_status psift_detect_and_compute_u8(psift_ctx* ctx, const uint8_t* luma, uint32_t height, uint32_t width,
+                                         size_t row_stride, const psift_sift_config* cfg, psift_features* out) {
+  return detect_host(ctx, luma, SRC_U8, height, width, row_stride, cfg, out);
+}
+
+psift_status psift_detect_keypoints(psift_ctx* ctx, const float* image, uint32_t h, uint32_t w, size_t stride,
+                                    const psift_sift_config* cfg, psift_keypoint* out, uint32_t capacity,
+                                    uint32_t* count) {
+  psift_status st = check_common(ctx, cfg);
+  if (st != PSIFT_OK) return st;
+  if (!count || (h && w && !image) || stride < w) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad argument");
+  const size_t img_bytes = sizeof(float) * (size_t)h * w;
+  ImageDesc d{};
+  d.stride = w;
+  d.h = (int)h;
+  d.w = (int)w;
+  d.kind = SRC_F32;
+  d.feat_cap = 1;
+  std::vector<ImageDesc> imgs{d};
+  DetectJob job;
+  void* d_img = nullptr;
+  st = build_job(ctx, imgs, *cfg, job, img_bytes, &d_img);
+  if (st != PSIFT_OK) return st;
+  job.plans[0].src = d_img;
+  st = pinned_reserve(ctx, std::max(img_bytes, sizeof(psift_keypoint) * (size_t)job.kp_cap) + 64);
+  if (st != PSIFT_OK) return st;
+  char* pin = ctx->pinned.base;
+  for (uint32_t y = 0; y < h; ++y) std::memcpy(pin + (size_t)y * w * 4, image + (size_t)y * stride, (size_t)w * 4);
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream));
+  if (img_bytes) PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_img, pin, img_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  st = launch_detect(ctx, job, *cfg, true);
+  if (st != PSIFT_OK) return st;
+  uint32_t* hmeta = (uint32_t*)(pin + ctx->pinned.capacity - 64);
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hmeta, job.plans[0].kp_count, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  st = read_error_word(ctx, hmeta + 4);
+  if (st != PSIFT_OK) return st;
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  st = error_from_word(ctx, hmeta[4]);
+  if (st != PSIFT_OK) return st;
+  const uint32_t n = job.n_oct[0] ? hmeta[0] : 0;
+  *count = n;
+  if (n > capacity) return set_error(ctx, PSIFT_ERR_CAPACITY, "keypoint output capacity too small");
+  if (n) {
+    if (!out) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null keypoint output");
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(pin, job.plans[0].kps, sizeof(psift_keypoint) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out, pin, sizeof(psift_keypoint) * n);
+  }
+  return PSIFT_OK;
+}
+
+psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
+                                                const psift_sift_config* cfg, psift_features* outs,
+                                                uint32_t* d_counts) {
+  psift_status st = check_common(ctx, cfg);
+  if (st != PSIFT_OK) return st;
+  if (!images || !outs || n == 0) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad batch argument");
+  std::vector<ImageDesc> imgs(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const psift_image_u8& im = images[i];
+    const psift_features& o = outs[i];
+    if ((im.height && im.width && !im.data) || im.row_stride < im.width || !o.x || !o.y || !o.scale || !o.response ||
+        !o.orientation || !o.descriptors || o.capacity == 0)
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad batch image/output descriptor");
+    ImageDesc& d = imgs[i];
+    d.src = im.data;
+    d.stride = (long long)im.row_stride;
+    d.h = (int)im.height;
+    d.w = (int)im.width;
+    d.kind = SRC_U8;
+    d.fx = o.x;
+    d.fy = o.y;
+    d.fscale = o.scale;
+    d.fresp = o.response;
+    d.fori = o.orientation;
+    d.fdesc = o.descriptors;
+    d.feat_cap = o.capacity;
+    d.out_count = d_counts ? d_counts + i : nullptr;
+  }
+  DetectJob job;
+  st = build_job(ctx, imgs, *cfg, job, 0, nullptr);
+  if (st != PSIFT_OK) return st;
+  return launch_detect(ctx, job, *cfg, false);
+}
+
+}  // extern "C"

@@ -1,0 +1,80 @@
+// Internal declarations shared by the libpsift_gpu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "psift_gpu.h"
+
+namespace psift {
+
+constexpr float kBaseSigma = 1.6f;          // BASE_SIGMA, src/pipeline.rs:10
+constexpr float kAssumedInputSigma = 0.5f;  // ASSUMED_INPUT_SIGMA, src/pipeline.rs:13
+constexpr float kPiF = 3.14159265358979323846f;
+constexpr int kDescLen = 128;
+constexpr int kMaxOctaves = 8;
+constexpr int kMaxTaps = 32;                // radius <= 15 (largest used: 10)
+
+// Grows-only device arena: one cudaMalloc, bump sub-allocation per call.
+struct DeviceArena {
+  char* base = nullptr;
+  size_t capacity = 0;
+  size_t offset = 0;
+};
+
+// Pinned host staging used for host<->device transfers of the host-pointer API.
+struct PinnedBuffer {
+  char* base = nullptr;
+  size_t capacity = 0;
+};
+
+}  // namespace psift
+
+struct psift_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  uint64_t launches = 0;
+  psift::DeviceArena arena;
+  psift::PinnedBuffer pinned;
+  int num_sms = 148;
+  // Device error word for bounded waits and capacity overflows (see kErr* below).
+  uint32_t* d_error = nullptr;
+};
+
+namespace psift {
+
+// Device error-word bits.
+constexpr uint32_t kErrKeypointCapacity = 1u;
+constexpr uint32_t kErrSortCapacity = 2u;
+constexpr uint32_t kErrTimeout = 4u;
+
+psift_status set_error(psift_ctx* ctx, psift_status st, const std::string& msg);
+psift_status cuda_error(psift_ctx* ctx, cudaError_t e, const char* what);
+// Ensure the arena can hold `bytes`; resets the bump pointer.  Synchronises the
+// stream before reallocating.
+psift_status arena_reserve(psift_ctx* ctx, size_t bytes);
+// Bump-allocate (256-byte aligned).  Caller must have reserved enough.
+void* arena_alloc(psift_ctx* ctx, size_t bytes);
+psift_status pinned_reserve(psift_ctx* ctx, size_t bytes);
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+// Raise a kernel's dynamic shared-memory limit once per (kernel, device).
+cudaError_t ensure_smem_attr(const void* func, size_t bytes);
+
+#define PSIFT_CUDA_TRY(ctx, expr)                                   \
+  do {                                                              \
+    cudaError_t _e = (expr);                                        \
+    if (_e != cudaSuccess) return ::psift::cuda_error(ctx, _e, #expr); \
+  } while (0)
+
+#define PSIFT_LAUNCH_CHECK(ctx)                                            \
+  do {                                                                     \
+    (ctx)->launches++;                                                     \
+    cudaError_t _e = cudaGetLastError();                                   \
+    if (_e != cudaSuccess) return ::psift::cuda_error(ctx, _e, "kernel launch"); \
+  } while (0)
+
+}  // namespace psift

@@ -1,0 +1,286 @@
+"""Python mirror of pure-sift's hot-path API over the sm_100a C ABI (libpsift_gpu.so).
+
+Names, argument meaning and error behaviour follow the reference's Rust API
+(src/lib.rs:26-52, src/pipeline.rs:22-247, src/catalog.rs:37-45, :576-702):
+
+* ``SiftConfig`` builder + ``validate()``; ``Sift.new(config)`` raises
+  ``ValueError`` with the reference's message where Rust returns ``Err(String)``.
+* ``Sift.detect_and_compute(img)`` / ``detect_keypoints(img)`` take a float32
+  ``(H, W)`` luma array in [0, 1] (the reference's ``Array2<f32>``); ``*_u8``
+  variants take u8 luma (``luma_to_array2`` is fused on the device).
+* Compute calls are infallible in the reference; here a device failure raises
+  ``PsiftError`` (there is no CPU fallback).
+
+Every compute call runs on the GPU through the C ABI; importing this module on
+a machine without the built library raises ``ImportError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from dataclasses import dataclass, field, replace
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpsift_gpu.so")
+
+BASE_SIGMA = 1.6
+DEFAULT_CONTRAST_THRESHOLD = 0.015
+DEFAULT_MATCH_RATIO = 0.75
+DEFAULT_RANSAC_REPROJ_THRESHOLD = 3.0
+MAX_FEATURES_PER_IMAGE = 4096
+SIFT_DESCRIPTOR_LEN = 128
+DEFAULT_SIMILARITY_RANSAC_SEED = 0xD1B54A32D192ED03
+DEFAULT_HOMOGRAPHY_RANSAC_SEED = 0x517CC1B727220A95
+
+PSIFT_OK = 0
+PSIFT_ERR_INVALID_ARGUMENT = 1
+PSIFT_ERR_INVALID_CONFIG = 2
+PSIFT_ERR_CAPACITY = 3
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "INVALID_CONFIG", 3: "CAPACITY", 4: "CUDA",
+                5: "OUT_OF_MEMORY", 6: "TIMEOUT", 7: "NO_DEVICE", 8: "INTERNAL"}
+
+
+class PsiftError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"psift {STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class CSiftConfig(C.Structure):
+    _fields_ = [("octaves", C.c_uint32), ("scales", C.c_uint32), ("contrast_threshold", C.c_float),
+                ("upsample_first_octave", C.c_int32), ("descriptor_kind", C.c_int32),
+                ("max_features", C.c_uint32)]
+
+
+class CKeypoint(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("scale", C.c_float), ("response", C.c_float),
+                ("octave", C.c_uint32), ("layer", C.c_uint32)]
+
+
+class CFeatures(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("count", C.c_uint32), ("x", C.c_void_p), ("y", C.c_void_p),
+                ("scale", C.c_void_p), ("response", C.c_void_p), ("orientation", C.c_void_p),
+                ("descriptors", C.c_void_p)]
+
+
+class CImageU8(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("height", C.c_uint32), ("width", C.c_uint32), ("row_stride", C.c_size_t)]
+
+
+KEYPOINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("scale", "<f4"), ("response", "<f4"),
+                           ("octave", "<u4"), ("layer", "<u4")])
+
+# Every entry point declared in include/psift_gpu.h, with its ctypes signature.
+_SIGS = {
+    "psift_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "psift_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "psift_last_error": (C.c_char_p, [C.c_void_p]),
+    "psift_ctx_launch_count": (C.c_uint64, [C.c_void_p]),
+    "psift_ctx_stream": (C.c_void_p, [C.c_void_p]),
+    "psift_ctx_synchronize": (C.c_int, [C.c_void_p]),
+    "psift_sift_config_default": (None, [C.POINTER(CSiftConfig)]),
+    "psift_sift_config_validate": (C.c_int, [C.POINTER(CSiftConfig), C.c_char_p, C.c_size_t]),
+    "psift_detect_and_compute": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
+                                           C.POINTER(CSiftConfig), C.POINTER(CFeatures)]),
+    "psift_detect_and_compute_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
+                                              C.POINTER(CSiftConfig), C.POINTER(CFeatures)]),
+    "psift_detect_keypoints": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
+                                         C.POINTER(CSiftConfig), C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "psift_detect_and_compute_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CImageU8), C.c_uint32,
+                                                     C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p]),
+}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def load_library() -> C.CDLL:
+    """Load libpsift_gpu.so (built in-tree by ``make -C pure-sift_b200``)."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(f"{LIB_PATH} is not built; run `make -C {_HERE}` (nvcc, sm_100a)")
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in _SIGS.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+class Context:
+    """One CUDA stream + workspace on one GPU (``psift_ctx``); not thread-safe."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        st = self.lib.psift_ctx_create(device, C.byref(h))
+        if st != PSIFT_OK:
+            raise PsiftError(st, "psift_ctx_create failed (no usable sm_100 device?)")
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.psift_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, st: int):
+        if st != PSIFT_OK:
+            raise PsiftError(st, self.lib.psift_last_error(self.handle).decode())
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.psift_ctx_launch_count(self.handle))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.psift_ctx_stream(self.handle) or 0)
+
+    def synchronize(self):
+        self.check(self.lib.psift_ctx_synchronize(self.handle))
+
+
+_tls = threading.local()
+
+
+def default_context() -> Context:
+    ctx = getattr(_tls, "ctx", None)
+    if ctx is None:
+        ctx = Context(int(os.environ.get("PSIFT_DEVICE", "0")))
+        _tls.ctx = ctx
+    return ctx
+
+
+@dataclass(frozen=True)
+class SiftConfig:
+    """``SiftConfig`` (src/pipeline.rs:22-104) with the builder methods."""
+    octaves: int = 3
+    scales: int = 3
+    contrast_threshold: float = DEFAULT_CONTRAST_THRESHOLD
+    upsample_first_octave_: bool = True
+    descriptor_kind_: int = 0  # 0 = Sift, 1 = RootSift
+    max_features_: int = MAX_FEATURES_PER_IMAGE
+
+    @staticmethod
+    def default() -> "SiftConfig":
+        return SiftConfig()
+
+    def with_octaves(self, n): return replace(self, octaves=n)
+    def with_scales(self, n): return replace(self, scales=n)
+    def with_contrast_threshold(self, t): return replace(self, contrast_threshold=t)
+    def upsample_first_octave(self, up): return replace(self, upsample_first_octave_=bool(up))
+    def descriptor_kind(self, kind): return replace(self, descriptor_kind_=int(kind))
+    def max_features(self, n): return replace(self, max_features_=int(n))
+
+    def to_c(self) -> CSiftConfig:
+        return CSiftConfig(self.octaves, self.scales, self.contrast_threshold, int(self.upsample_first_octave_),
+                           self.descriptor_kind_, self.max_features_)
+
+    def validate(self):
+        """Returns None when valid, else raises ValueError with the reference's message."""
+        lib = load_library()
+        buf = C.create_string_buffer(256)
+        c = self.to_c()
+        st = lib.psift_sift_config_validate(C.byref(c), buf, 256)
+        if st != PSIFT_OK:
+            raise ValueError(buf.value.decode())
+
+
+@dataclass
+class Features:
+    """Structure-of-arrays ``Vec<SiftFeature>``."""
+    x: np.ndarray
+    y: np.ndarray
+    scale: np.ndarray
+    response: np.ndarray
+    orientation: np.ndarray
+    descriptors: np.ndarray  # (n, 128)
+
+    def __len__(self):
+        return int(self.x.shape[0])
+
+    @property
+    def xy(self) -> np.ndarray:
+        return np.stack([self.x, self.y], axis=1)
+
+    @staticmethod
+    def empty(n: int) -> "Features":
+        return Features(*(np.zeros(n, np.float32) for _ in range(5)), np.zeros((n, 128), np.float32))
+
+    def head(self, n: int) -> "Features":
+        return Features(self.x[:n].copy(), self.y[:n].copy(), self.scale[:n].copy(), self.response[:n].copy(),
+                        self.orientation[:n].copy(), self.descriptors[:n].copy())
+
+
+def _c_features(f: Features) -> CFeatures:
+    return CFeatures(len(f), 0, f.x.ctypes.data, f.y.ctypes.data, f.scale.ctypes.data, f.response.ctypes.data,
+                     f.orientation.ctypes.data, f.descriptors.ctypes.data)
+
+
+@dataclass(frozen=True)
+class Sift:
+    """``Sift`` (src/pipeline.rs:106-146)."""
+    config: SiftConfig = field(default_factory=SiftConfig)
+
+    @staticmethod
+    def new(config: SiftConfig) -> "Sift":
+        config.validate()
+        return Sift(config)
+
+    def _run(self, img: np.ndarray, u8: bool, ctx: Context | None) -> Features:
+        ctx = ctx or default_context()
+        dt = np.uint8 if u8 else np.float32
+        img = np.ascontiguousarray(img, dtype=dt)
+        if img.ndim != 2:
+            raise ValueError("image must be 2-D (H, W)")
+        h, w = img.shape
+        cfg = self.config.to_c()
+        cap = self.config.max_features_ or 16384
+        fn = ctx.lib.psift_detect_and_compute_u8 if u8 else ctx.lib.psift_detect_and_compute
+        while True:
+            out = Features.empty(cap)
+            cf = _c_features(out)
+            st = fn(ctx.handle, img.ctypes.data, h, w, w, C.byref(cfg), C.byref(cf))
+            if st == PSIFT_ERR_CAPACITY and cf.count > cap:
+                cap = int(cf.count)
+                continue
+            ctx.check(st)
+            return out.head(int(cf.count))
+
+    def detect_and_compute(self, img: np.ndarray, ctx: Context | None = None) -> Features:
+        return self._run(img, False, ctx)
+
+    def detect_and_compute_u8(self, img: np.ndarray, ctx: Context | None = None) -> Features:
+        return self._run(img, True, ctx)
+
+    def detect_keypoints(self, img: np.ndarray, ctx: Context | None = None) -> np.ndarray:
+        ctx = ctx or default_context()
+        img = np.ascontiguousarray(img, dtype=np.float32)
+        h, w = img.shape
+        cfg = self.config.to_c()
+        cap = 1 << 16
+        while True:
+            out = np.zeros(cap, KEYPOINT_DTYPE)
+            n = C.c_uint32()
+            st = ctx.lib.psift_detect_keypoints(ctx.handle, img.ctypes.data, h, w, w, C.byref(cfg), out.ctypes.data,
+                                                cap, C.byref(n))
+            if st == PSIFT_ERR_CAPACITY and n.value > cap:
+                cap = n.value
+                continue
+            ctx.check(st)
+            return out[:n.value].copy()
