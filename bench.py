@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Headline benchmark: 1080p SIFT detect+describe images/s on B200.
+
+Workload (one "step"): one pass of Sift::detect_and_compute over a batch of
+synthetic 1920x1080 u8 luma images (2000 Gaussian blobs, sigma ~ U(1.5, 20),
+N(0,3) noise) with SiftConfig::default().octaves(4).contrast_threshold(0.015),
+first-octave upsampling, Lowe's 4096-feature cap.  Inputs are resident in HBM
+for `value`; `e2e` runs the same images through the public host-pointer API
+(psift_detect_and_compute_u8) with the host->device copy of every image and the
+device->host copy of every feature list inside the timed region.
+
+Multi-GPU: images are independent, so each rank processes its own batch (weak
+scaling, no data-path collective); the step time is the max over ranks.
+
+`--impl reference` times the CPU restatement of the reference path (the
+reference itself is Rust and cannot be built here) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pure-sift_b200"))
+
+import numpy as np  # noqa: E402
+
+import synth  # noqa: E402
+
+WIDTH, HEIGHT = 1920, 1080
+OCTAVES, SCALES, THRESH, MAX_FEATURES = 4, 3, 0.015, 4096
+METRIC = "1080p SIFT detect+describe images/s"
+WORKLOAD = ("1920x1080 u8 blob images (2000 blobs, sigma U(1.5,20), N(0,3) noise); "
+            "SiftConfig octaves=4 scales=3 threshold=0.015 upsample=on, cap 4096")
+L2_NOTE = "no flush: per-step working set (~0.5 GB of scale-space planes per image) >> 126 MB L2"
+# DRAM bytes per blur_level_kernel launch from one ncu capture (octave 0, 1080p
+# image, radius-10 level); profiles/blur_level_1080p.md gives the command.
+NCU_TRAFFIC_BLUR_LEVEL = None
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_images(n: int, seed0: int):
+    imgs = []
+    for i in range(n):
+        imgs.append(synth.blob_image(WIDTH, HEIGHT, 2000, 1.5, 20.0, seed=seed0 + i))
+    return imgs
+
+
+def pyramid_bytes_per_image(h: int, w: int) -> tuple[float, int]:
+    """Algorithmic HBM bytes of the pyramid stage for one image, and its launch count.
+
+    Octave-0 base: read u8 image (W*H), write G0 (4 B/px).  Each blur level:
+    read G[s-1], write G[s], write D[s-1] (12 B/px); the level that seeds the
+    next octave also writes its base (4 B per next-octave px).
+    """
+    hh, ww = 2 * h, 2 * w
+    total = float(h * w) + 4.0 * hh * ww
+    launches = 1
+    for o in range(OCTAVES):
+        if hh < 3 or ww < 3:
+            break
+        p = hh * ww
+        total += (SCALES + 2) * 12.0 * p
+        launches += SCALES + 2
+        nh, nw = hh // 2, ww // 2
+        if o + 1 < OCTAVES and nh >= 3 and nw >= 3:
+            total += 4.0 * nh * nw
+        hh, ww = nh, nw
+    return total, launches
+
+
+def cpu_reference(steps: int, warmup: int, budget_s: float):
+    """Time the CPU restatement (OpenMP over all host cores) on 1080p images."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    img = O.luma_to_f32(make_images(1, 0)[0])
+    for _ in range(warmup):
+        O.detect_and_compute(img, OCTAVES, SCALES, THRESH, True, 0, MAX_FEATURES)
+    t0 = time.perf_counter()
+    n = 0
+    while n < steps and (time.perf_counter() - t0) < budget_s:
+        O.detect_and_compute(img, OCTAVES, SCALES, THRESH, True, 0, MAX_FEATURES)
+        n += 1
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt, os.cpu_count()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    steps = max(args.steps, 1)
+    ips, n, dt, cores = cpu_reference(steps, min(args.warmup, 1), budget_s=120.0)
+    line = {
+        "metric": METRIC, "value": ips, "unit": "images/s", "n_gpus": args.gpus, "steps": n,
+        "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * dt / max(n, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "batch_per_step": 1},
+        "cpu_baseline": {"value": ips, "unit": "images/s", "cores": cores, "kind": "port",
+                         "sample": f"{n} x 1080p detect+describe, CPU restatement of pure-sift 0.2.0 "
+                                   "(OpenMP over the loops rayon parallelises)"},
+        "e2e": {"value": ips, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import psift
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    B = args.batch
+    host_imgs = make_images(B, seed0=1000 * rank + 1)
+    d_imgs = [torch.from_numpy(im).cuda() for im in host_imgs]
+    cap = MAX_FEATURES
+    outs = [{k: torch.empty(cap, dtype=torch.float32, device="cuda") for k in ("x", "y", "s", "r", "o")}
+            for _ in range(B)]
+    for o in outs:
+        o["d"] = torch.empty((cap, 128), dtype=torch.float32, device="cuda")
+    d_counts = torch.zeros(B, dtype=torch.int32, device="cuda")
+    ctx = psift.Context(local)
+    cfg = psift.SiftConfig().with_octaves(OCTAVES).with_scales(SCALES).with_contrast_threshold(THRESH)
+    ccfg = cfg.to_c()
+    cimgs = (psift.CImageU8 * B)(*[psift.CImageU8(t.data_ptr(), HEIGHT, WIDTH, WIDTH) for t in d_imgs])
+    couts = (psift.CFeatures * B)(*[psift.CFeatures(cap, 0, o["x"].data_ptr(), o["y"].data_ptr(),
+                                                    o["s"].data_ptr(), o["r"].data_ptr(), o["o"].data_ptr(),
+                                                    o["d"].data_ptr()) for o in outs])
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def step():
+        ctx.check(ctx.lib.psift_detect_and_compute_batch_dev(ctx.handle, cimgs, B, C.byref(ccfg), couts,
+                                                             C.c_void_p(d_counts.data_ptr())))
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ctx.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launch_count - launches0
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_per_step = ms / args.steps
+    value = world * B * args.steps / (ms / 1e3)
+    counts = d_counts.cpu().numpy()
+    if args.only_device:
+        # profiling case: the timed device path only
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "images/s", "ms_per_step": ms_per_step,
+                              "batch_per_gpu": B, "gpu_launches": int(launches)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        ctx.close()
+        return 0
+
+    # Per-stage device times (separate pass; events around each stage).
+    ctx.enable_stage_timing(True)
+    ctx.stage_times(reset=True)
+    reps = 3
+    for _ in range(reps):
+        step()
+    st = ctx.stage_times(reset=True)
+    ctx.enable_stage_timing(False)
+    pyr_ms, pyr_intervals = st["pyramid"]
+    bytes_img, blur_launches = pyramid_bytes_per_image(HEIGHT, WIDTH)
+    # one pyramid interval = the init blur, or one octave's levels (all images of the batch)
+    blur_launch_total = reps * blur_launches
+    avg_launch_s = (pyr_ms / 1e3) / blur_launch_total
+    bytes_per_launch = B * bytes_img / blur_launches
+    achieved = bytes_per_launch / avg_launch_s / 1e9
+    peak, peak_kind = peaks()
+
+    # End to end through the public host-pointer API.
+    sift = psift.Sift.new(cfg)
+    pinned = [torch.from_numpy(im).pin_memory() for im in host_imgs]
+    for im in pinned[:2]:
+        sift.detect_and_compute_u8(im.numpy(), ctx=ctx)
+    if dist:
+        dist.barrier()
+    e2e_steps = max(1, min(args.steps, 10))
+    d2h = 0
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        d2h = 0
+        for im in pinned:
+            f = sift.detect_and_compute_u8(im.numpy(), ctx=ctx)
+            d2h += len(f) * (5 + 128) * 4 + 16
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * B * e2e_steps / e2e_s
+
+    result = None
+    if rank == 0:
+        result = {
+            "metric": METRIC, "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "batch_per_gpu": B, "global_batch": world * B, "l2": L2_NOTE,
+                       "features_per_image": [int(c) for c in counts[:4]]},
+            "gpu_launches": int(launches),
+            "e2e": {"value": e2e_value, "unit": "images/s", "h2d_bytes_per_step": B * WIDTH * HEIGHT,
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"kernel": "blur_level_kernel (pyramid: blur + DoG + decimation)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "traffic": NCU_TRAFFIC_BLUR_LEVEL,
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "avg_launch_ms": avg_launch_s * 1e3},
+            "stage_ms_per_step": {k: v[0] / reps for k, v in st.items() if v[1]},
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            ips, n, dt, cores = cpu_reference(steps=30, warmup=1, budget_s=20.0)
+            result["cpu_baseline"] = {
+                "value": ips, "unit": "images/s", "cores": cores, "kind": "port",
+                "sample": f"{n} x 1080p detect+describe of the same image, CPU restatement of pure-sift 0.2.0 "
+                          f"(OpenMP, {cores} threads), {dt:.1f} s"}
+        print(json.dumps(result), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-device", action="store_true", help="time the device path only (profiling case)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -86,6 +86,13 @@ uint64_t psift_ctx_launch_count(const psift_ctx* ctx);
 /* The context's CUDA stream (cudaStream_t) for event timing / interop. */
 void* psift_ctx_stream(const psift_ctx* ctx);
 psift_status psift_ctx_synchronize(psift_ctx* ctx);
+/* Optional per-stage device timing (CUDA events on the context stream).
+ * Stages: 0 pyramid (octave base + blur/DoG levels), 1 extrema (mark, scan,
+ * emit), 2 top-K cap, 3 orientation, 4 descriptors, 5 matching, 6 Hamming,
+ * 7 RANSAC, 8 MLP.  psift_ctx_stage_times synchronises the stream and returns
+ * the accumulated milliseconds and the number of timed intervals per stage. */
+psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
+psift_status psift_ctx_stage_times(psift_ctx* ctx, double* ms, uint64_t* counts, uint32_t n, int reset);
 
 /* ---------------------------------------------------------------- config */
 /* SiftConfig::default() (src/pipeline.rs:36-46) with max_features = 4096. */

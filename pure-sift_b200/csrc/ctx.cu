@@ -56,6 +56,47 @@ cudaError_t ensure_smem_attr(const void* func, size_t bytes) {
   return e;
 }
 
+static cudaEvent_t take_event(psift_ctx* ctx) {
+  if (!ctx->timer.pool.empty()) {
+    cudaEvent_t e = ctx->timer.pool.back();
+    ctx->timer.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+StageScope::StageScope(psift_ctx* c, int s) : ctx(c), stage(s) {
+  if (ctx && ctx->timer.enabled) {
+    start = take_event(ctx);
+    cudaEventRecord(start, ctx->stream);
+  }
+}
+
+StageScope::~StageScope() {
+  if (start) {
+    cudaEvent_t end = take_event(ctx);
+    cudaEventRecord(end, ctx->stream);
+    ctx->timer.pending.push_back({stage, {start, end}});
+  }
+}
+
+static void drain_timer(psift_ctx* ctx) {
+  if (ctx->timer.pending.empty()) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& p : ctx->timer.pending) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
+      ctx->timer.ms[p.first] += ms;
+      ctx->timer.count[p.first] += 1;
+    }
+    ctx->timer.pool.push_back(p.second.first);
+    ctx->timer.pool.push_back(p.second.second);
+  }
+  ctx->timer.pending.clear();
+}
+
 psift_status pinned_reserve(psift_ctx* ctx, size_t bytes) {
   if (bytes <= ctx->pinned.capacity) return PSIFT_OK;
   bytes = align_up(bytes, 1 << 20);
@@ -110,6 +151,11 @@ psift_status psift_ctx_destroy(psift_ctx* ctx) {
   if (ctx->arena.base) cudaFree(ctx->arena.base);
   if (ctx->pinned.base) cudaFreeHost(ctx->pinned.base);
   if (ctx->d_error) cudaFree(ctx->d_error);
+  for (auto& p : ctx->timer.pending) {
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  for (cudaEvent_t e : ctx->timer.pool) cudaEventDestroy(e);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PSIFT_OK;
@@ -126,6 +172,29 @@ void* psift_ctx_stream(const psift_ctx* ctx) { return ctx ? (void*)ctx->stream :
 psift_status psift_ctx_synchronize(psift_ctx* ctx) {
   if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
   PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PSIFT_OK;
+}
+
+psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable) {
+  if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  ctx->timer.enabled = enable != 0;
+  return PSIFT_OK;
+}
+
+psift_status psift_ctx_stage_times(psift_ctx* ctx, double* ms, uint64_t* counts, uint32_t n, int reset) {
+  if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  psift::drain_timer(ctx);
+  for (uint32_t i = 0; i < n && i < psift::STAGE_COUNT; ++i) {
+    if (ms) ms[i] = ctx->timer.ms[i];
+    if (counts) counts[i] = ctx->timer.count[i];
+  }
+  if (reset) {
+    for (int i = 0; i < psift::STAGE_COUNT; ++i) {
+      ctx->timer.ms[i] = 0.0;
+      ctx->timer.count[i] = 0;
+    }
+  }
   return PSIFT_OK;
 }
 

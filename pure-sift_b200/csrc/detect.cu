@@ -270,6 +270,7 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
   };
   // Octave-0 base: luma -> f32 (+ 2x bilinear upsample) + initial blur.
   {
+    StageScope sc_pyr(ctx, STAGE_PYRAMID);
     int mh, mw;
     max_dims(0, mh, mw);
     const bool up = cfg.upsample_first_octave != 0;
@@ -292,16 +293,23 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
   for (int o = 0; o < max_oct; ++o) {
     int mh, mw;
     max_dims(o, mh, mw);
-    for (int s = 1; s <= S + 2; ++s) {
-      cudaError_t e = launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, n, o, s, S, mh, mw, st);
-      ctx->launches++;
-      if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
+    {
+      StageScope sc_pyr(ctx, STAGE_PYRAMID);
+      for (int s = 1; s <= S + 2; ++s) {
+        cudaError_t e = launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, n, o, s, S, mh, mw, st);
+        ctx->launches++;
+        if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
+      }
     }
+    StageScope sc_x(ctx, STAGE_EXTREMA);
     cudaError_t e = launch_extrema_mark(job.d_plans, n, o, mh, xp, st);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "extrema_mark");
   }
-  cudaError_t e = launch_row_scan(job.d_plans, n, job.kp_cap, ctx->d_error, st);
+  cudaError_t e;
+  {
+  StageScope sc_x2(ctx, STAGE_EXTREMA);
+  e = launch_row_scan(job.d_plans, n, job.kp_cap, ctx->d_error, st);
   ctx->launches++;
   if (e != cudaSuccess) return cuda_error(ctx, e, "row_scan");
   for (int o = 0; o < max_oct; ++o) {
@@ -311,20 +319,30 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "extrema_emit");
   }
+  }
   if (stop_after_keypoints) return PSIFT_OK;
-  e = launch_select_topk(job.d_plans, n, job.kp_cap, cfg.max_features, ctx->d_error, st);
-  ctx->launches++;
-  if (e != cudaSuccess) return cuda_error(ctx, e, "select_topk");
+  {
+    StageScope sc_s(ctx, STAGE_SELECT);
+    e = launch_select_topk(job.d_plans, n, job.kp_cap, cfg.max_features, ctx->d_error, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "select_topk");
+  }
   DescribeParams dp{S, cfg.max_features, cfg.descriptor_kind};
-  e = launch_orientation(job.d_plans, n, job.sel_cap, dp, st);
-  ctx->launches++;
-  if (e != cudaSuccess) return cuda_error(ctx, e, "orientation");
-  e = launch_feature_scan(job.d_plans, n, cfg.max_features, st);
-  ctx->launches++;
-  if (e != cudaSuccess) return cuda_error(ctx, e, "feature_scan");
-  e = launch_descriptor(job.d_plans, n, job.sel_cap, dp, st);
-  ctx->launches++;
-  if (e != cudaSuccess) return cuda_error(ctx, e, "descriptor");
+  {
+    StageScope sc_o(ctx, STAGE_ORIENTATION);
+    e = launch_orientation(job.d_plans, n, job.sel_cap, dp, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "orientation");
+  }
+  {
+    StageScope sc_d(ctx, STAGE_DESCRIPTOR);
+    e = launch_feature_scan(job.d_plans, n, cfg.max_features, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "feature_scan");
+    e = launch_descriptor(job.d_plans, n, job.sel_cap, dp, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "descriptor");
+  }
   return PSIFT_OK;
 }
 

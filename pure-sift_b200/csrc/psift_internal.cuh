@@ -33,6 +33,29 @@ struct PinnedBuffer {
 
 }  // namespace psift
 
+namespace psift {
+// Stages timed by the optional per-stage CUDA-event timer.
+enum Stage : int {
+  STAGE_PYRAMID = 0,     // octave base + blur/DoG levels
+  STAGE_EXTREMA = 1,     // mark + scan + emit
+  STAGE_SELECT = 2,      // top-K cap
+  STAGE_ORIENTATION = 3,
+  STAGE_DESCRIPTOR = 4,  // feature scan + descriptors
+  STAGE_MATCH = 5,
+  STAGE_HAMMING = 6,
+  STAGE_RANSAC = 7,
+  STAGE_MLP = 8,
+  STAGE_COUNT = 16
+};
+struct StageTimer {
+  bool enabled = false;
+  std::vector<cudaEvent_t> pool;                    // free events
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  double ms[STAGE_COUNT] = {0};
+  uint64_t count[STAGE_COUNT] = {0};
+};
+}  // namespace psift
+
 struct psift_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -43,6 +66,7 @@ struct psift_ctx {
   int num_sms = 148;
   // Device error word for bounded waits and capacity overflows (see kErr* below).
   uint32_t* d_error = nullptr;
+  psift::StageTimer timer;
 };
 
 namespace psift {
@@ -63,6 +87,16 @@ psift_status pinned_reserve(psift_ctx* ctx, size_t bytes);
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Raise a kernel's dynamic shared-memory limit once per (kernel, device).
 cudaError_t ensure_smem_attr(const void* func, size_t bytes);
+
+// Stage timing: `StageScope sc(ctx, STAGE_X);` records events around the launches
+// issued while it is alive (no-op unless timing is enabled).
+struct StageScope {
+  psift_ctx* ctx;
+  int stage;
+  cudaEvent_t start = nullptr;
+  StageScope(psift_ctx* c, int s);
+  ~StageScope();
+};
 
 #define PSIFT_CUDA_TRY(ctx, expr)                                   \
   do {                                                              \

@@ -81,6 +81,8 @@ _SIGS = {
     "psift_ctx_launch_count": (C.c_uint64, [C.c_void_p]),
     "psift_ctx_stream": (C.c_void_p, [C.c_void_p]),
     "psift_ctx_synchronize": (C.c_int, [C.c_void_p]),
+    "psift_ctx_enable_stage_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "psift_ctx_stage_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int]),
     "psift_sift_config_default": (None, [C.POINTER(CSiftConfig)]),
     "psift_sift_config_validate": (C.c_int, [C.POINTER(CSiftConfig), C.c_char_p, C.c_size_t]),
     "psift_detect_and_compute": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
@@ -153,6 +155,18 @@ class Context:
 
     def synchronize(self):
         self.check(self.lib.psift_ctx_synchronize(self.handle))
+
+    STAGES = ("pyramid", "extrema", "select", "orientation", "descriptor", "match", "hamming", "ransac", "mlp")
+
+    def enable_stage_timing(self, on: bool = True):
+        self.check(self.lib.psift_ctx_enable_stage_timing(self.handle, int(on)))
+
+    def stage_times(self, reset: bool = True) -> dict:
+        """{stage: (total_ms, intervals)} accumulated since the last reset."""
+        ms = np.zeros(16, np.float64)
+        cnt = np.zeros(16, np.uint64)
+        self.check(self.lib.psift_ctx_stage_times(self.handle, ms.ctypes.data, cnt.ctypes.data, 16, int(reset)))
+        return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(self.STAGES)}
 
 
 _tls = threading.local()
