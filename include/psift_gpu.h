@@ -129,6 +129,28 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
                                                 uint32_t n, const psift_sift_config* cfg,
                                                 psift_features* outs, uint32_t* d_counts);
 
+/* Allocation-free variant of psift_detect_and_compute_batch_dev for one u8 image.
+ * No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory -- plugin hosts that hand out only a stream, real-time loops in
+ * which cudaMalloc's implicit device synchronisation is not acceptable.  All
+ * scratch lives in a 32 MiB file-scope device array inside this library (held by
+ * every GPU that loads it until exit); the call makes no cudaMalloc/cudaFree or
+ * other allocating call.  Enough for a 320x240 image at the reference defaults
+ * (octaves <= 4, scales 3, first-octave upsampling); a request needing more
+ * scratch returns PSIFT_ERR_CAPACITY without touching the GPU.
+ *  - luma, out->x..descriptors (capacity out->capacity) and d_count are device
+ *    pointers; cuda_stream is a cudaStream_t (NULL = legacy default stream).
+ *  - The first call on a device looks up the scratch array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - The call queues the work on cuda_stream and waits for it to finish.
+ *  - Every call shares the one scratch array: calls that overlap on the GPU
+ *    (other streams, other host threads) race and corrupt each other. */
+psift_status psift_detect_and_compute_u8_noalloc_dev(const uint8_t* luma, uint32_t height,
+                                                     uint32_t width, size_t row_stride,
+                                                     const psift_sift_config* cfg,
+                                                     psift_features* out, uint32_t* d_count,
+                                                     void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

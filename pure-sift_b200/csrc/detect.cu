@@ -13,6 +13,7 @@
 // workspace; all data-dependent work stays on the device.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "detect_plan.cuh"
@@ -536,3 +537,174 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free detect+describe.
+//
+// For callers that must not allocate device memory: code running inside a
+// memory-pool-less plugin host, a real-time loop where cudaMalloc's implicit
+// device synchronisation is not allowed, or an embedding that hands this library
+// only a stream.  Their scratch lives in one file-scope device array that every
+// GPU loading this library holds until the process exits.  Inputs and outputs
+// stay caller-owned device memory.
+//
+// Size limit: kNoAllocScratchBytes (32 MiB).  That holds the scale space of a
+// 320x240 image with the reference's defaults (octaves <= 4, scales 3, first-octave
+// upsampling) plus 65536 keypoint slots; requests needing more are rejected.
+// ---------------------------------------------------------------------------
+namespace psift {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 32u << 20;
+constexpr uint32_t kNoAllocKeypointCapacity = 1u << 16;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device (host code may not use the
+// symbol itself: on the host it names a stand-in, not device memory).
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {nullptr};
+
+psift_status noalloc_scratch_address(psift_ctx* ctx, void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return PSIFT_OK;
+}
+
+// Bump carve inside the fixed scratch; returns nullptr when it would overflow.
+struct FixedCarver {
+  char* base;
+  size_t cap, off = 0, need = 0;
+  void* take(size_t bytes) {
+    const size_t o = align_up(off, 256);
+    off = o + bytes;
+    need = off;
+    return off <= cap ? base + o : nullptr;
+  }
+};
+
+// Lays out one image's buffers (same layout as build_job) inside the scratch.
+bool carve_noalloc_job(FixedCarver& cv, const ImageDesc& img, const psift_sift_config& cfg, DetectJob& job) {
+  const int S = (int)cfg.scales;
+  job.n = 1;
+  job.kp_cap = kNoAllocKeypointCapacity;
+  job.sel_cap = cfg.max_features ? cfg.max_features : job.kp_cap;
+  job.oct.assign(kMaxOctaves, HostOctave{0, 0, 0});
+  job.n_oct.assign(1, plan_octaves(img.h, img.w, (int)cfg.octaves, cfg.upsample_first_octave != 0, job.oct.data()));
+  job.plans.assign(1, ImagePlan{});
+  ImagePlan& P = job.plans[0];
+  std::memset(&P, 0, sizeof(P));
+  job.d_plans = (ImagePlan*)cv.take(sizeof(ImagePlan));
+  P.src = img.src;
+  P.src_stride = img.stride;
+  P.src_h = img.h;
+  P.src_w = img.w;
+  P.src_kind = img.kind;
+  P.upsample = cfg.upsample_first_octave != 0;
+  P.n_oct = job.n_oct[0];
+  int row_base = 0;
+  const float base_mult = cfg.upsample_first_octave ? 0.5f : 1.0f;
+  for (int o = 0; o < P.n_oct; ++o) {
+    const HostOctave& H = job.oct[o];
+    OctaveDev& O = P.oct[o];
+    O.h = H.h;
+    O.w = H.w;
+    O.pitch = H.pitch;
+    O.plane_stride = H.pitch * H.h;
+    float* planes = (float*)cv.take(plane_bytes(H) * (2 * S + 5));
+    O.g = planes;
+    O.d = planes ? planes + O.plane_stride * (S + 3) : nullptr;
+    O.words = (H.w + 31) / 32;
+    O.masks = (uint32_t*)cv.take(sizeof(uint32_t) * (size_t)S * H.h * O.words);
+    O.row_base = row_base;
+    O.scale_factor = base_mult * (float)(1ull << o);
+    row_base += S * H.h;
+  }
+  P.total_rows = row_base;
+  P.row_counts = (uint32_t*)cv.take(sizeof(uint32_t) * (size_t)row_base + 4);
+  P.row_offsets = (uint32_t*)cv.take(sizeof(uint32_t) * (size_t)row_base + 4);
+  P.kps = (psift_keypoint*)cv.take(sizeof(psift_keypoint) * job.kp_cap);
+  P.sel = (psift_keypoint*)cv.take(sizeof(psift_keypoint) * job.sel_cap);
+  P.oris = (float*)cv.take(sizeof(float) * 4 * job.sel_cap);
+  P.ori_count = (uint32_t*)cv.take(sizeof(uint32_t) * job.sel_cap);
+  P.feat_offsets = (uint32_t*)cv.take(sizeof(uint32_t) * job.sel_cap);
+  uint32_t* counters = (uint32_t*)cv.take(256);
+  if (counters) {
+    P.kp_count = counters + 0;
+    P.sel_count = counters + 1;
+    P.feat_count = counters + 2;
+    P.feat_total = counters + 3;
+  }
+  P.out_count = img.out_count;
+  P.feat_cap = img.feat_cap;
+  P.fx = img.fx;
+  P.fy = img.fy;
+  P.fscale = img.fscale;
+  P.fresp = img.fresp;
+  P.fori = img.fori;
+  P.fdesc = img.fdesc;
+  return cv.need <= cv.cap;
+}
+
+}  // namespace
+}  // namespace psift
+
+extern "C" psift_status psift_detect_and_compute_u8_noalloc_dev(const uint8_t* luma, uint32_t height, uint32_t width,
+                                                                size_t row_stride, const psift_sift_config* cfg,
+                                                                psift_features* out, uint32_t* d_count,
+                                                                void* cuda_stream) {
+  // A stack context carries the caller's stream and the error message; it owns
+  // no device memory and is never passed to an allocating helper.
+  psift_ctx local;
+  local.stream = (cudaStream_t)cuda_stream;
+  char msg[256];
+  psift_status st = psift_sift_config_validate(cfg, msg, sizeof msg);
+  if (st != PSIFT_OK) return st;
+  if (!out || !d_count || (height && width && !luma) || row_stride < width || !out->x || !out->y || !out->scale ||
+      !out->response || !out->orientation || !out->descriptors || out->capacity == 0)
+    return PSIFT_ERR_INVALID_ARGUMENT;
+  void* scratch = nullptr;
+  st = noalloc_scratch_address(&local, &scratch);
+  if (st != PSIFT_OK) return st;
+  // First 256 bytes: the device error word; the job is carved after it.
+  uint32_t* d_err = (uint32_t*)scratch;
+  FixedCarver cv{(char*)scratch + 256, kNoAllocScratchBytes - 256};
+  ImageDesc img{};
+  img.src = luma;
+  img.stride = (long long)row_stride;
+  img.h = (int)height;
+  img.w = (int)width;
+  img.kind = SRC_U8;
+  img.fx = out->x;
+  img.fy = out->y;
+  img.fscale = out->scale;
+  img.fresp = out->response;
+  img.fori = out->orientation;
+  img.fdesc = out->descriptors;
+  img.feat_cap = out->capacity;
+  img.out_count = d_count;
+  DetectJob job;
+  if (!carve_noalloc_job(cv, img, *cfg, job)) return PSIFT_ERR_CAPACITY;
+  local.d_error = d_err;
+  cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(uint32_t), local.stream);
+  if (e != cudaSuccess) return PSIFT_ERR_CUDA;
+  st = launch_detect(&local, job, *cfg, false);
+  if (st != PSIFT_OK) return st;
+  uint32_t h_err = 0;
+  e = cudaMemcpyAsync(&h_err, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, local.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(local.stream);
+  if (e != cudaSuccess) return PSIFT_ERR_CUDA;
+  if (h_err & kErrKeypointCapacity) return PSIFT_ERR_CAPACITY;
+  if (h_err) return PSIFT_ERR_INTERNAL;
+  return PSIFT_OK;
+}

@@ -93,6 +93,9 @@ _SIGS = {
                                          C.POINTER(CSiftConfig), C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "psift_detect_and_compute_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CImageU8), C.c_uint32,
                                                      C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p]),
+    "psift_detect_and_compute_u8_noalloc_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
+                                                          C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p,
+                                                          C.c_void_p]),
 }
 
 _lib = None
