@@ -77,6 +77,16 @@ typedef struct psift_features {
   float* descriptors;  /* capacity * 128, row-major */
 } psift_features;
 
+/* FeatureMatch (src/pipeline.rs:1076-1091); 40 bytes. */
+typedef struct psift_match {
+  uint32_t query_index, target_index;
+  float query_x, query_y;
+  float target_x, target_y;
+  float distance;   /* sqrt of the best squared distance */
+  float ratio;      /* d1 / d2 */
+  float displacement_x, displacement_y;
+} psift_match;
+
 /* ---------------------------------------------------------------- context */
 psift_status psift_ctx_create(int device, psift_ctx** out);
 psift_status psift_ctx_destroy(psift_ctx* ctx);
@@ -128,6 +138,45 @@ typedef struct psift_image_u8 {
 psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_image_u8* images,
                                                 uint32_t n, const psift_sift_config* cfg,
                                                 psift_features* outs, uint32_t* d_counts);
+
+/* ---------------------------------------------------------------- matching */
+#define PSIFT_PRECISION_FP32 0        /* exact f32 distances, the reference's summation order */
+#define PSIFT_PRECISION_BF16_RERANK 1 /* bf16 tcgen05 distances + certified exact f32 re-rank:
+                                         the same match list as PSIFT_PRECISION_FP32 */
+/* MatchOptions (src/pipeline.rs:1721-1736) plus the arithmetic path. */
+typedef struct psift_match_options {
+  float ratio;        /* (0, 1], default 0.75 (DEFAULT_MATCH_RATIO) */
+  int32_t mutual;     /* mutual nearest-neighbour cross-check, default 0 */
+  int32_t precision;  /* PSIFT_PRECISION_*, default BF16_RERANK */
+} psift_match_options;
+void psift_match_options_default(psift_match_options* opt);
+/* Matcher::new (src/pipeline.rs:156-164). */
+psift_status psift_match_options_validate(const psift_match_options* opt, char* msg, size_t msg_capacity);
+/* Matcher::match_ (src/pipeline.rs:167-169 -> :1744-1841).  Descriptors are
+ * n x 128 f32 row-major, coordinates n x 2 (x, y).  Matches come out in query
+ * order; at most nq of them. */
+psift_status psift_match_descriptors(psift_ctx* ctx, const float* query_descriptors, uint32_t nq,
+                                     const float* target_descriptors, uint32_t nt, const float* query_xy,
+                         const float* target_xy, const psift_match_options* opt,
+                         psift_match* out, uint32_t capacity, uint32_t* count);
+/* Device-resident batch of independent matching problems (one launch per stage
+ * for all of them); every pointer is device memory; capacity must be >= nq.
+ * The match count of each problem is written to its d_count.  Asynchronous. */
+typedef struct psift_match_job {
+  const float* query_descriptors;
+  const float* target_descriptors;
+  const float* query_xy;
+  const float* target_xy;
+  uint32_t nq, nt;
+  psift_match* out;
+  uint32_t capacity;
+  uint32_t* d_count;
+} psift_match_job;
+psift_status psift_match_batch_dev(psift_ctx* ctx, const psift_match_job* jobs, uint32_t n,
+                                   const psift_match_options* opt);
+/* Rows (queries, or targets in the mutual pass) whose bf16 candidate list could
+ * not be certified and were matched by an exact scan, since context creation. */
+psift_status psift_ctx_rerank_fallbacks(psift_ctx* ctx, uint64_t* rows);
 
 /* Allocation-free variant of psift_detect_and_compute_batch_dev for one u8 image.
  * No counterpart in the reference: it exists for callers that cannot allocate

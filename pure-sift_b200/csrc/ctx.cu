@@ -97,6 +97,24 @@ static void drain_timer(psift_ctx* ctx) {
   ctx->timer.pending.clear();
 }
 
+psift_status io_reserve(psift_ctx* ctx, size_t bytes) {
+  bytes = align_up(bytes + 4096, 1 << 20);
+  if (bytes > ctx->io.capacity) {
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->io.base) cudaFree(ctx->io.base);
+    ctx->io.base = nullptr;
+    ctx->io.capacity = 0;
+    cudaError_t e = cudaMalloc(&ctx->io.base, bytes);
+    if (e != cudaSuccess) {
+      ctx->io.base = nullptr;
+      return cuda_error(ctx, e, "cudaMalloc(io)");
+    }
+    ctx->io.capacity = bytes;
+  }
+  ctx->io.offset = 0;
+  return PSIFT_OK;
+}
+
 psift_status pinned_reserve(psift_ctx* ctx, size_t bytes) {
   if (bytes <= ctx->pinned.capacity) return PSIFT_OK;
   bytes = align_up(bytes, 1 << 20);
@@ -134,8 +152,7 @@ psift_status psift_ctx_create(int device, psift_ctx** out) {
     delete ctx;
     return PSIFT_ERR_CUDA;
   }
-  if (cudaMalloc(&ctx->d_error, sizeof(uint32_t)) != cudaSuccess ||
-      cudaMemset(ctx->d_error, 0, sizeof(uint32_t)) != cudaSuccess) {
+  if (cudaMalloc(&ctx->d_error, 64) != cudaSuccess || cudaMemset(ctx->d_error, 0, 64) != cudaSuccess) {
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PSIFT_ERR_OUT_OF_MEMORY;
@@ -149,6 +166,7 @@ psift_status psift_ctx_destroy(psift_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   if (ctx->arena.base) cudaFree(ctx->arena.base);
+  if (ctx->io.base) cudaFree(ctx->io.base);
   if (ctx->pinned.base) cudaFreeHost(ctx->pinned.base);
   if (ctx->d_error) cudaFree(ctx->d_error);
   for (auto& p : ctx->timer.pending) {

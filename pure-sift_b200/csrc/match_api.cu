@@ -1,0 +1,414 @@
+// Orchestration and C-ABI entry points of the matcher (Matcher::new / match_).
+//
+// Reference: Matcher::new (src/pipeline.rs:156-164), Matcher::match_ (:167-169),
+// match_descriptors_with_options (:1744-1841).
+#include <cuda.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "match_common.cuh"
+#include "psift_internal.cuh"
+
+namespace psift {
+
+cudaError_t launch_match_fp32(const MatchPair* d_pairs, int n_pairs, int max_q_tiles, int t_splits, float* part,
+                              int* part_idx, float* cpart, int* cpart_idx, const long long* part_off,
+                              const long long* cpart_off, bool mutual, cudaStream_t st);
+cudaError_t launch_match_merge(const MatchPair* d_pairs, int n_pairs, int max_n, int t_splits, const float* part,
+                               const int* part_idx, const float* cpart, const int* cpart_idx,
+                               const long long* part_off, const long long* cpart_off, bool mutual, cudaStream_t st);
+cudaError_t launch_match_emit(const MatchPair* d_pairs, int n_pairs, float ratio, bool mutual, cudaStream_t st);
+bool make_operand_map(CUtensorMap* tm, const void* base, long long rows, int box_rows);
+cudaError_t launch_to_bf16(const float* x, int n, void* out, float* norms, float* norm_max, cudaStream_t st);
+cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcItem* items, int n_items,
+                            const TcPair* pairs, uint32_t* err, cudaStream_t st);
+cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
+
+namespace {
+
+constexpr int kTile = 128;
+constexpr int kTcBM = 128, kTcBN = 256;
+
+// Matcher::new (src/pipeline.rs:156-164): same message.
+psift_status validate_match_options(psift_ctx* ctx, const psift_match_options* o) {
+  if (!o) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null match options");
+  if (!(o->ratio == o->ratio) || o->ratio > 3.4e38f || o->ratio <= 0.0f || o->ratio > 1.0f) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "Invalid `ratio`=%g: must be finite and in (0.0, 1.0]", (double)o->ratio);
+    return set_error(ctx, PSIFT_ERR_INVALID_CONFIG, buf);
+  }
+  if (o->precision != PSIFT_PRECISION_FP32 && o->precision != PSIFT_PRECISION_BF16_RERANK)
+    return set_error(ctx, PSIFT_ERR_INVALID_CONFIG, "Invalid `precision`: must be FP32 (0) or BF16_RERANK (1)");
+  return PSIFT_OK;
+}
+
+long long pad_rows(int n) { return ((long long)n + 255) / 256 * 256; }
+
+// Device-side batch: every pointer in jobs is device memory.  Queues all work.
+psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, const psift_match_options& opt) {
+  cudaStream_t st = ctx->stream;
+  const bool mutual = opt.mutual != 0;
+  const bool tc = opt.precision == PSIFT_PRECISION_BF16_RERANK;
+  // Active problems: the reference returns nothing for an empty query set or < 2 targets.
+  std::vector<int> active;
+  for (int i = 0; i < n; ++i) {
+    const psift_match_job& J = jobs[i];
+    if (J.nq > 0 && J.nt >= 2) active.push_back(i);
+  }
+  // zero the counts of inactive problems
+  for (int i = 0; i < n; ++i)
+    if (std::find(active.begin(), active.end(), i) == active.end())
+      PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(jobs[i].d_count, 0, sizeof(uint32_t), st));
+  const int na = (int)active.size();
+  if (na == 0) return PSIFT_OK;
+
+  // ---- sizes
+  size_t bytes = sizeof(MatchPair) * na + 4096;
+  int max_q_tiles = 0, max_n = 0;
+  std::vector<int> t_splits_v(na), q_tiles(na);
+  long long part_total = 0, cpart_total = 0;
+  long long q_rows = 0, t_rows = 0;
+  long long cand_f = 0, cand_r = 0;
+  std::vector<int> tc_split_f(na), tc_split_r(na);
+  int n_items_f = 0, n_items_r = 0;
+  const int target_ctas = 2 * ctx->num_sms;
+  for (int k = 0; k < na; ++k) {
+    const psift_match_job& J = jobs[active[k]];
+    const int qt = (int)((J.nq + kTile - 1) / kTile);
+    q_tiles[k] = qt;
+    max_q_tiles = std::max(max_q_tiles, qt);
+    max_n = std::max(max_n, (int)std::max(J.nq, J.nt));
+    bytes += 3 * sizeof(float) * (size_t)J.nq + 2 * sizeof(float) * (size_t)J.nt + 1024;
+    if (!tc) {
+      const int tt = (int)((J.nt + kTile - 1) / kTile);
+      int sp = (target_ctas + na * qt - 1) / (na * qt);
+      sp = std::max(1, std::min(sp, tt));
+      t_splits_v[k] = sp;
+      part_total += (long long)sp * J.nq;
+      if (mutual) cpart_total += (long long)qt * J.nt;
+    } else {
+      q_rows += pad_rows((int)J.nq);
+      t_rows += pad_rows((int)J.nt);
+      const int at = (int)((J.nq + kTcBM - 1) / kTcBM), bt = (int)((J.nt + kTcBN - 1) / kTcBN);
+      int sp = std::max(1, std::min(bt, (target_ctas + na * at - 1) / (na * at)));
+      tc_split_f[k] = sp;
+      n_items_f += at * sp;
+      cand_f += (long long)sp * J.nq * 8;
+      if (mutual) {
+        const int at2 = (int)((J.nt + kTcBM - 1) / kTcBM), bt2 = (int)((J.nq + kTcBN - 1) / kTcBN);
+        int sp2 = std::max(1, std::min(bt2, (target_ctas + na * at2 - 1) / (na * at2)));
+        tc_split_r[k] = sp2;
+        n_items_r += at2 * sp2;
+        cand_r += (long long)sp2 * J.nt * 8;
+      }
+    }
+  }
+  int t_splits = 1;
+  for (int k = 0; k < na; ++k) t_splits = std::max(t_splits, t_splits_v[k]);
+  if (!tc) {
+    // one uniform split count (grid x); per-pair offsets cover it
+    part_total = 0;
+    cpart_total = 0;
+    for (int k = 0; k < na; ++k) {
+      const psift_match_job& J = jobs[active[k]];
+      part_total += (long long)t_splits * J.nq;
+      if (mutual) cpart_total += (long long)q_tiles[k] * J.nt;
+    }
+    bytes += (size_t)part_total * 12 + (size_t)cpart_total * 8 + 2 * sizeof(long long) * na + 1024;
+  } else {
+    bytes += (size_t)(q_rows + t_rows) * 256 + (size_t)(q_rows + t_rows) * 4 + 4096;
+    bytes += (size_t)(cand_f + cand_r) * 8 + sizeof(TcItem) * (n_items_f + n_items_r) +
+             sizeof(TcPair) * 2 * na + sizeof(RerankJob) * 2 * na + 8192 + (size_t)t_rows * 4;
+  }
+  psift_status s = arena_reserve(ctx, bytes);
+  if (s != PSIFT_OK) return s;
+
+  // ---- pairs
+  std::vector<MatchPair> pairs(na);
+  MatchPair* d_pairs = (MatchPair*)arena_alloc(ctx, sizeof(MatchPair) * na);
+  for (int k = 0; k < na; ++k) {
+    const psift_match_job& J = jobs[active[k]];
+    MatchPair& P = pairs[k];
+    std::memset(&P, 0, sizeof P);
+    P.q = J.query_descriptors;
+    P.t = J.target_descriptors;
+    P.qxy = J.query_xy;
+    P.txy = J.target_xy;
+    P.nq = (int)J.nq;
+    P.nt = (int)J.nt;
+    P.best = (float*)arena_alloc(ctx, sizeof(float) * J.nq);
+    P.second = (float*)arena_alloc(ctx, sizeof(float) * J.nq);
+    P.best_idx = (int*)arena_alloc(ctx, sizeof(int) * J.nq);
+    P.col_best = (float*)arena_alloc(ctx, sizeof(float) * J.nt);
+    P.col_idx = (int*)arena_alloc(ctx, sizeof(int) * J.nt);
+    P.out = J.out;
+    P.out_count = J.d_count;
+  }
+
+  if (!tc) {
+    std::vector<long long> poff(na), cpoff(na);
+    long long a = 0, b = 0;
+    for (int k = 0; k < na; ++k) {
+      poff[k] = a;
+      cpoff[k] = b;
+      a += (long long)t_splits * pairs[k].nq;
+      b += (long long)q_tiles[k] * pairs[k].nt;
+    }
+    float* part = (float*)arena_alloc(ctx, sizeof(float) * 2 * std::max<long long>(part_total, 1));
+    int* part_idx = (int*)arena_alloc(ctx, sizeof(int) * std::max<long long>(part_total, 1));
+    float* cpart = (float*)arena_alloc(ctx, sizeof(float) * std::max<long long>(cpart_total, 1));
+    int* cpart_idx = (int*)arena_alloc(ctx, sizeof(int) * std::max<long long>(cpart_total, 1));
+    long long* d_poff = (long long*)arena_alloc(ctx, sizeof(long long) * na);
+    long long* d_cpoff = (long long*)arena_alloc(ctx, sizeof(long long) * na);
+    if (!part || !d_cpoff) return set_error(ctx, PSIFT_ERR_INTERNAL, "match workspace carve overflow");
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(MatchPair) * na, cudaMemcpyHostToDevice, st));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_poff, poff.data(), sizeof(long long) * na, cudaMemcpyHostToDevice, st));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_cpoff, cpoff.data(), sizeof(long long) * na, cudaMemcpyHostToDevice, st));
+    StageScope sc(ctx, STAGE_MATCH);
+    cudaError_t e = launch_match_fp32(d_pairs, na, max_q_tiles, t_splits, part, part_idx, cpart, cpart_idx, d_poff,
+                                      d_cpoff, mutual, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "match_fp32");
+    e = launch_match_merge(d_pairs, na, max_n, t_splits, part, part_idx, cpart, cpart_idx, d_poff, d_cpoff, mutual, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "match_merge");
+    e = launch_match_emit(d_pairs, na, opt.ratio, mutual, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "match_emit");
+    return PSIFT_OK;
+  }
+
+  // ---- BF16 tensor-core path
+  uint16_t* qb = (uint16_t*)arena_alloc(ctx, (size_t)q_rows * 256);
+  uint16_t* tb = (uint16_t*)arena_alloc(ctx, (size_t)t_rows * 256);
+  float* qn = (float*)arena_alloc(ctx, sizeof(float) * q_rows);
+  float* tn = (float*)arena_alloc(ctx, sizeof(float) * t_rows);
+  float* maxes = (float*)arena_alloc(ctx, sizeof(float) * 2 * na);  // [k]: t max, [na + k]: q max
+  float* cand_v = (float*)arena_alloc(ctx, sizeof(float) * std::max<long long>(cand_f + cand_r, 1));
+  int* cand_i = (int*)arena_alloc(ctx, sizeof(int) * std::max<long long>(cand_f + cand_r, 1));
+  TcItem* d_items = (TcItem*)arena_alloc(ctx, sizeof(TcItem) * (n_items_f + n_items_r));
+  TcPair* d_tcp = (TcPair*)arena_alloc(ctx, sizeof(TcPair) * 2 * na);
+  RerankJob* d_rj = (RerankJob*)arena_alloc(ctx, sizeof(RerankJob) * 2 * na);
+  int* flags = mutual ? (int*)arena_alloc(ctx, sizeof(int) * t_rows) : nullptr;  // matched-target marks
+  if (!qb || !tb || !cand_i || !d_rj || (mutual && !flags))
+    return set_error(ctx, PSIFT_ERR_INTERNAL, "match workspace carve overflow");
+  if (mutual) PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * t_rows, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(qb, 0, (size_t)q_rows * 256, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(tb, 0, (size_t)t_rows * 256, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(maxes, 0, sizeof(float) * 2 * na, st));
+  std::vector<long long> q0(na), t0(na);
+  {
+    long long a = 0, b = 0;
+    for (int k = 0; k < na; ++k) {
+      q0[k] = a;
+      t0[k] = b;
+      a += pad_rows(pairs[k].nq);
+      b += pad_rows(pairs[k].nt);
+    }
+  }
+  CUtensorMap tmQA, tmTB, tmTA, tmQB;
+  if (!make_operand_map(&tmQA, qb, q_rows, kTcBM) || !make_operand_map(&tmTB, tb, t_rows, kTcBN) ||
+      (mutual && (!make_operand_map(&tmTA, tb, t_rows, kTcBM) || !make_operand_map(&tmQB, qb, q_rows, kTcBN))))
+    return set_error(ctx, PSIFT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  std::vector<TcItem> items;
+  std::vector<TcPair> tcp(2 * na);
+  std::vector<RerankJob> rj(2 * na);
+  long long cf = 0;
+  for (int k = 0; k < na; ++k) {
+    MatchPair& P = pairs[k];
+    P.q_row0 = (int)q0[k];
+    P.t_row0 = (int)t0[k];
+    P.qn = qn + q0[k];
+    P.tn = tn + t0[k];
+    P.tn_max = maxes + k;
+    P.qn_max = maxes + na + k;
+    // forward: A = queries, B = targets
+    {
+      TcPair& T = tcp[k];
+      T.na = P.nq;
+      T.nb = P.nt;
+      T.an = P.qn;
+      T.bn = P.tn;
+      T.cand_val = cand_v + cf;
+      T.cand_idx = cand_i + cf;
+      T.splits = tc_split_f[k];
+      cf += (long long)T.splits * P.nq * 8;
+      const int at = (P.nq + kTcBM - 1) / kTcBM, bt = (P.nt + kTcBN - 1) / kTcBN;
+      for (int a = 0; a < at; ++a)
+        for (int s = 0; s < T.splits; ++s) {
+          const int b0 = (int)((long long)bt * s / T.splits), b1 = (int)((long long)bt * (s + 1) / T.splits);
+          items.push_back({k, (int)q0[k] + a * kTcBM, a * kTcBM, (int)t0[k] + b0 * kTcBN, b0 * kTcBN, b1 - b0, s});
+        }
+      RerankJob& R = rj[k];
+      R = RerankJob{P.q, P.t, P.nq, P.nt, P.qn, P.tn_max, T.cand_val, T.cand_idx, T.splits,
+                    P.best, P.second, P.best_idx, ctx->d_error + 1, opt.ratio,
+                    mutual ? flags + t0[k] : nullptr};
+    }
+  }
+  const int n_f = (int)items.size();
+  if (mutual) {
+    for (int k = 0; k < na; ++k) {
+      MatchPair& P = pairs[k];
+      TcPair& T = tcp[na + k];
+      T.na = P.nt;
+      T.nb = P.nq;
+      T.an = P.tn;
+      T.bn = P.qn;
+      T.cand_val = cand_v + cf;
+      T.cand_idx = cand_i + cf;
+      T.splits = tc_split_r[k];
+      cf += (long long)T.splits * P.nt * 8;
+      const int at = (P.nt + kTcBM - 1) / kTcBM, bt = (P.nq + kTcBN - 1) / kTcBN;
+      for (int a = 0; a < at; ++a)
+        for (int s = 0; s < T.splits; ++s) {
+          const int b0 = (int)((long long)bt * s / T.splits), b1 = (int)((long long)bt * (s + 1) / T.splits);
+          items.push_back({na + k, (int)t0[k] + a * kTcBM, a * kTcBM, (int)q0[k] + b0 * kTcBN, b0 * kTcBN, b1 - b0, s});
+        }
+      rj[na + k] = RerankJob{P.t, P.q, P.nt, P.nq, P.tn, P.qn_max, T.cand_val, T.cand_idx, T.splits,
+                             P.col_best, nullptr, P.col_idx, ctx->d_error + 1, opt.ratio, flags + t0[k]};
+    }
+  }
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(MatchPair) * na, cudaMemcpyHostToDevice, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(TcItem) * items.size(), cudaMemcpyHostToDevice, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_tcp, tcp.data(), sizeof(TcPair) * tcp.size(), cudaMemcpyHostToDevice, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_rj, rj.data(), sizeof(RerankJob) * rj.size(), cudaMemcpyHostToDevice, st));
+  StageScope sc(ctx, STAGE_MATCH);
+  for (int k = 0; k < na; ++k) {
+    cudaError_t e = launch_to_bf16(pairs[k].q, pairs[k].nq, qb + (size_t)q0[k] * 128, qn + q0[k], maxes + na + k, st);
+    if (e == cudaSuccess) e = launch_to_bf16(pairs[k].t, pairs[k].nt, tb + (size_t)t0[k] * 128, tn + t0[k], maxes + k, st);
+    ctx->launches += 2;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "to_bf16");
+  }
+  int max_a = 0, max_b = 0;
+  for (int k = 0; k < na; ++k) {
+    max_a = std::max(max_a, pairs[k].nq);
+    max_b = std::max(max_b, pairs[k].nt);
+  }
+  cudaError_t e = launch_match_tc(tmQA, tmTB, d_items, n_f, d_tcp, ctx->d_error, st);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc");
+  e = launch_rerank(d_rj, na, max_a, st);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "rerank");
+  if (mutual) {
+    e = launch_match_tc(tmTA, tmQB, d_items + n_f, (int)items.size() - n_f, d_tcp, ctx->d_error, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc(reverse)");
+    e = launch_rerank(d_rj + na, na, max_b, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "rerank(reverse)");
+  }
+  e = launch_match_emit(d_pairs, na, opt.ratio, mutual, st);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "match_emit");
+  return PSIFT_OK;
+}
+
+}  // namespace
+}  // namespace psift
+
+using namespace psift;
+
+extern "C" {
+
+void psift_match_options_default(psift_match_options* o) {
+  if (!o) return;
+  o->ratio = 0.75f;  // DEFAULT_MATCH_RATIO, src/pipeline.rs:1047
+  o->mutual = 0;
+  o->precision = PSIFT_PRECISION_BF16_RERANK;
+}
+
+psift_status psift_match_options_validate(const psift_match_options* o, char* msg, size_t cap) {
+  psift_ctx tmp;
+  psift_status st = validate_match_options(&tmp, o);
+  if (msg && cap) {
+    strncpy(msg, tmp.last_error.c_str(), cap - 1);
+    msg[cap - 1] = 0;
+  }
+  return st;
+}
+
+psift_status psift_match_batch_dev(psift_ctx* ctx, const psift_match_job* jobs, uint32_t n,
+                                   const psift_match_options* opt) {
+  if (!ctx || !jobs) return PSIFT_ERR_INVALID_ARGUMENT;
+  psift_status st = validate_match_options(ctx, opt);
+  if (st != PSIFT_OK) return st;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_error(ctx, e, "cudaSetDevice");
+  for (uint32_t i = 0; i < n; ++i) {
+    const psift_match_job& J = jobs[i];
+    if (!J.d_count || (J.nq && (!J.query_descriptors || !J.query_xy || !J.out)) ||
+        (J.nt && (!J.target_descriptors || !J.target_xy)))
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null pointer in match job");
+    if (J.nq > 0 && J.nt >= 2 && J.capacity < J.nq)
+      return set_error(ctx, PSIFT_ERR_CAPACITY, "match output capacity must be >= number of queries");
+  }
+  if (n == 0) return PSIFT_OK;
+  return match_batch(ctx, jobs, (int)n, *opt);
+}
+
+psift_status psift_match_descriptors(psift_ctx* ctx, const float* q_desc, uint32_t nq, const float* t_desc, uint32_t nt,
+                         const float* q_xy, const float* t_xy, const psift_match_options* opt, psift_match* out,
+                         uint32_t capacity, uint32_t* count) {
+  if (!ctx || !count) return PSIFT_ERR_INVALID_ARGUMENT;
+  psift_status st = validate_match_options(ctx, opt);
+  if (st != PSIFT_OK) return st;
+  if ((nq && (!q_desc || !q_xy)) || (nt && (!t_desc || !t_xy)))
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null descriptor/coordinate array");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_error(ctx, e, "cudaSetDevice");
+  *count = 0;
+  if (nq == 0 || nt < 2) return PSIFT_OK;
+  // Stage inputs in a separate device buffer (the batch path owns the arena).
+  const size_t in_bytes = sizeof(float) * ((size_t)nq * 130 + (size_t)nt * 130) + sizeof(psift_match) * nq + 1024;
+  st = io_reserve(ctx, in_bytes);
+  if (st != PSIFT_OK) return st;
+  char* base = ctx->io.base;
+  float* d_q = (float*)base;
+  float* d_t = d_q + (size_t)nq * 128;
+  float* d_qxy = d_t + (size_t)nt * 128;
+  float* d_txy = d_qxy + (size_t)nq * 2;
+  psift_match* d_out = (psift_match*)align_up((size_t)(d_txy + (size_t)nt * 2), 16);
+  uint32_t* d_count = (uint32_t*)(d_out + nq);
+  st = pinned_reserve(ctx, std::max(sizeof(psift_match) * nq, (size_t)64) + 64);
+  if (st != PSIFT_OK) return st;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_q, q_desc, sizeof(float) * nq * 128, cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_t, t_desc, sizeof(float) * nt * 128, cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_qxy, q_xy, sizeof(float) * nq * 2, cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_txy, t_xy, sizeof(float) * nt * 2, cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, sizeof(uint32_t), ctx->stream));
+  psift_match_job job{d_q, d_t, d_qxy, d_txy, nq, nt, d_out, nq, d_count};
+  st = match_batch(ctx, &job, 1, *opt);
+  if (st != PSIFT_OK) return st;
+  uint32_t* hm = (uint32_t*)(ctx->pinned.base + ctx->pinned.capacity - 64);
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hm, d_count, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hm + 1, ctx->d_error, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (hm[1] & kErrTimeout) return set_error(ctx, PSIFT_ERR_TIMEOUT, "tensor-core matcher wait timed out");
+  const uint32_t c = hm[0];
+  *count = c;
+  if (c > capacity) return set_error(ctx, PSIFT_ERR_CAPACITY, "match output capacity too small");
+  if (c) {
+    if (!out) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null match output");
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pinned.base, d_out, sizeof(psift_match) * c, cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out, ctx->pinned.base, sizeof(psift_match) * c);
+  }
+  return PSIFT_OK;
+}
+
+psift_status psift_ctx_rerank_fallbacks(psift_ctx* ctx, uint64_t* rows) {
+  if (!ctx || !rows) return PSIFT_ERR_INVALID_ARGUMENT;
+  uint32_t h = 0;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(&h, ctx->d_error + 1, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  *rows = h;
+  return PSIFT_OK;
+}
+
+}  // extern "C"

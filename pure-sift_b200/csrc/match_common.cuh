@@ -1,0 +1,99 @@
+// Shared definitions of the descriptor matcher (Matcher::match_).
+#pragma once
+
+#include <stdint.h>
+
+#include "psift_gpu.h"
+
+namespace psift {
+
+// One matching problem (query set vs target set), device pointers.
+struct MatchPair {
+  const float* q;      // nq x 128 descriptors
+  const float* t;      // nt x 128
+  const float* qxy;    // nq x 2 keypoint coordinates
+  const float* txy;    // nt x 2
+  int nq, nt;
+  // per-query exact top-2 (filled by the FP32 kernels or the re-rank)
+  float* best;         // nq
+  float* second;       // nq
+  int* best_idx;       // nq
+  // reverse nearest query per target (mutual check)
+  float* col_best;     // nt
+  int* col_idx;        // nt
+  // outputs
+  psift_match* out;    // capacity >= nq
+  uint32_t* out_count;
+  // BF16 path: row offsets of this pair in the concatenated bf16 operands
+  int q_row0, t_row0;  // rows in the concatenated (padded) bf16 buffers
+  const float* qn;     // nq exact f32 squared norms
+  const float* tn;     // nt
+  float* tn_max;       // scalar: max target squared norm
+  float* qn_max;       // scalar: max query squared norm
+};
+
+// Tensor-core matcher work item: one 128-row A tile x a range of 256-row B tiles.
+struct TcItem {
+  int pair;
+  int a_row;    // first row of the A tile in the concatenated A operand
+  int a_local;  // its index within the pair
+  int b_row;    // first row of the first B tile in the concatenated B operand
+  int b_local;  // its index within the pair
+  int n_tiles;  // B tiles (256 rows each) in this item
+  int split;
+};
+
+// Tensor-core matcher problem (A rows matched against B rows).
+struct TcPair {
+  int na, nb;
+  const float* an;   // f32 squared norms of A rows
+  const float* bn;   // f32 squared norms of B rows
+  float* cand_val;   // [splits][na][8]
+  int* cand_idx;
+  int splits;
+};
+
+// Certified re-rank job (one per problem and direction).
+struct RerankJob {
+  const float* a;       // A descriptors (f32)
+  const float* b;       // B descriptors (f32)
+  int na, nb;
+  const float* an;
+  const float* bn_max;  // scalar
+  const float* cand_val;
+  const int* cand_idx;
+  int splits;
+  float* best;          // outputs; `second` is null for the reverse (best-only) pass
+  float* second;
+  int* best_idx;
+  uint32_t* fallbacks;  // rows that needed the exact scan
+  float ratio;          // Lowe ratio (forward pass: rows certified to fail it are skipped)
+  int* flags;           // forward: set flags[best] = 1 for accepted matches (mutual);
+                        // reverse: only rows with flags[row] != 0 are ranked (null = all)
+};
+
+// Merge of two (best, idx, second) triples over disjoint target sets where ties
+// on the best value keep the lower index and `second` is the second smallest
+// value of the union multiset.  Commutative and associative, so any reduction
+// order gives the sequential loop's result (src/pipeline.rs:1768-1786).
+__device__ __forceinline__ void top2_merge(float& b, int& bi, float& s, float b2, int bi2, float s2) {
+  if (b2 < b || (b2 == b && bi2 < bi)) {
+    s = fminf(b, s2);
+    b = b2;
+    bi = bi2;
+  } else {
+    s = fminf(s, b2);
+  }
+}
+
+__device__ __forceinline__ void top2_push(float& b, int& bi, float& s, float d, int idx) {
+  if (d < b || (d == b && idx < bi)) {
+    s = b;
+    b = d;
+    bi = idx;
+  } else if (d < s) {
+    s = d;
+  }
+}
+
+}  // namespace psift

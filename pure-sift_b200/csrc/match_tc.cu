@@ -1,0 +1,500 @@
+// K8: BF16 tcgen05 distance GEMM with a fused top-8 epilogue, and the certified
+// exact FP32 re-rank that makes its match list identical to the FP32 path.
+//
+// Reference: match_descriptors_with_options (src/pipeline.rs:1744-1841).
+//
+// Scheme.  a_ij = |q_i|^2 + |t_j|^2 - 2 <bf16(q_i), bf16(t_j)> (f32 accumulate in
+// TMEM) approximates the reference's f32 squared distance d_ij with
+//   |a_ij - d_ij| <= eps_i = 0.008 |q_i| max_j|t_j| + 5e-5 (|q_i|^2 + max_j|t_j|^2) + 1e-6
+// (bf16 rounding of both operands <= 2^-8 relative per product, tensor-core f32
+// accumulation, the f32 norms and the reference's own sequential f32 rounding, all
+// bounded with margin).  Every target that can be the exact best or second has
+// a_ij <= a_(2) + 2 eps_i.  The epilogue keeps each row's 8 smallest a_ij (ties by
+// index); if the 8th is > a_(2) + 2 eps_i the 8 candidates provably contain the
+// exact best and second, and their exact reference distances are recomputed in
+// f32 (sequential order).  Otherwise the row falls back to an exact scan of all
+// targets.  Either way best/second/index equal the FP32 path bit for bit.
+//
+// Kernel structure (one CTA = one 128-row A tile x a range of 256-row B tiles,
+// 192 threads): warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
+// operand tile, double-buffered B), warp 1 owns TMEM (512 columns = two 128x256
+// f32 accumulators) and issues tcgen05.mma (M=128, N=256, K=16) from one thread,
+// warps 2-5 read the accumulators with tcgen05.ld and maintain the top-8 lists.
+// All waits are bounded: on timeout the CTA records kErrTimeout, stops issuing,
+// drains what it issued and frees its TMEM.
+#include <cuda.h>
+
+#include "match_common.cuh"
+#include "psift_internal.cuh"
+
+namespace psift {
+
+constexpr int kTcThreads = 192;
+constexpr int kBM = 128;
+constexpr int kBN = 256;
+constexpr uint32_t kSpinLimit = 1u << 25;
+constexpr int kTopK = 8;
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait; false on timeout or when the CTA is aborting.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255u) == 255u && *abort_flag) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap* tm, uint64_t* bar, void* dst, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte-swizzled operand tile: rows of 128 B, 8-row atoms 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);  // start address
+  d |= (uint64_t)1 << 16;                    // leading byte offset (unused when swizzled)
+  d |= (uint64_t)(1024u >> 4) << 32;         // stride byte offset: 8 rows x 128 B
+  d |= (uint64_t)1 << 46;                    // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                    // SWIZZLE_128B
+  return d;
+}
+
+// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=256.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
+                            ((uint32_t)(kBM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Smem map (offsets from a 1024-aligned base).
+constexpr uint32_t kSmA = 0;                      // 2 halves x 128 rows x 128 B = 32 KB
+constexpr uint32_t kSmB = 32768;                  // 2 stages x 2 halves x 256 rows x 128 B = 128 KB
+constexpr uint32_t kSmBar = kSmB + 2 * 65536;     // barriers
+constexpr uint32_t kSmTotal = kSmBar + 256 + 1024;  // + alignment slack
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    match_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    const TcItem* __restrict__ items, const TcPair* __restrict__ pairs, uint32_t* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kSmBar);  // [2]
+  uint64_t* empty = full + 2;                                    // [2]
+  uint64_t* afull = full + 4;                                    // [1]
+  uint64_t* accf = full + 5;                                     // [2]
+  uint64_t* acce = full + 7;                                     // [2]
+  volatile uint32_t* taddr_slot = reinterpret_cast<volatile uint32_t*>(full + 9);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(full + 10);
+
+  const TcItem it = items[blockIdx.x];
+  const TcPair& PR = pairs[it.pair];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&empty[0], 1);
+    mbar_init(&empty[1], 1);
+    mbar_init(afull, 1);
+    mbar_init(&accf[0], 1);
+    mbar_init(&accf[1], 1);
+    mbar_init(&acce[0], 4);
+    mbar_init(&acce[1], 4);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32((const void*)taddr_slot)),
+                 "r"(512u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *taddr_slot;
+  const int nt = it.n_tiles;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // A tile: two 64-column boxes of 128 rows
+      mbar_expect_tx(afull, 2u * kBM * 128u);
+      tma_load_2d(&tmA, afull, smem + kSmA, 0, it.a_row);
+      tma_load_2d(&tmA, afull, smem + kSmA + kBM * 128, 64, it.a_row);
+      for (int j = 0; j < nt; ++j) {
+        const int s = j & 1;
+        const uint32_t use = (uint32_t)(j >> 1);
+        if (!mbar_wait(&empty[s], (use & 1u) ^ 1u, abort_flag)) {
+          atomicOr(err, kErrTimeout);
+          *abort_flag = 1;
+          break;
+        }
+        uint8_t* bst = smem + kSmB + s * 65536;
+        mbar_expect_tx(&full[s], 2u * kBN * 128u);
+        tma_load_2d(&tmB, &full[s], bst, 0, it.b_row + j * kBN);
+        tma_load_2d(&tmB, &full[s], bst + kBN * 128, 64, it.b_row + j * kBN);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int issued = 0;
+      bool ok = mbar_wait(afull, 0, abort_flag);
+      for (int j = 0; ok && j < nt; ++j) {
+        const int s = j & 1;
+        const uint32_t use = (uint32_t)(j >> 1);
+        if (!mbar_wait(&full[s], use & 1u, abort_flag) || !mbar_wait(&acce[s], (use & 1u) ^ 1u, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a_base = smem_u32(smem + kSmA);
+        const uint32_t b_base = smem_u32(smem + kSmB + s * 65536);
+        const uint32_t d = tmem + (uint32_t)(s * kBN);
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+          const uint32_t half = (uint32_t)(kk >> 2), koff = (uint32_t)(kk & 3) * 32u;
+          umma_bf16(d, sw128_desc(a_base + half * (kBM * 128) + koff), sw128_desc(b_base + half * (kBN * 128) + koff),
+                    kk > 0 ? 1u : 0u);
+        }
+        umma_commit(&empty[s]);
+        umma_commit(&accf[s]);
+        ++issued;
+      }
+      if (!ok) {
+        atomicOr(err, kErrTimeout);
+        *abort_flag = 1;
+        // drain: wait (bounded, ignoring the abort flag) for the last issued MMA group
+        if (issued > 0) {
+          const int j = issued - 1;
+          const int s = j & 1;
+          const uint32_t use = (uint32_t)(j >> 1);
+          for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(&accf[s], use & 1u); ++i) {
+          }
+        }
+      }
+    }
+  } else {
+    // epilogue: warps 2..5 -> TMEM lane quarter (warp % 4)
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    const int a_local = it.a_local + row;
+    const bool row_ok = a_local < PR.na;
+    const float an = row_ok ? PR.an[a_local] : 0.0f;
+    float v[kTopK];
+    int vi[kTopK];
+#pragma unroll
+    for (int k = 0; k < kTopK; ++k) {
+      v[k] = __int_as_float(0x7f800000);
+      vi[k] = 0x7fffffff;
+    }
+    for (int j = 0; j < nt; ++j) {
+      const int s = j & 1;
+      const uint32_t use = (uint32_t)(j >> 1);
+      if (!mbar_wait(&accf[s], use & 1u, abort_flag)) {
+        atomicOr(err, kErrTimeout);
+        *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(s * kBN);
+      const int col0 = it.b_local + j * kBN;
+#pragma unroll 1
+      for (int c = 0; c < kBN / 32; ++c) {
+        uint32_t r[32];
+        __syncwarp();
+        tmem_ld32(taddr + (uint32_t)(c * 32), r);
+        const int cb = col0 + c * 32;
+        const float bnl = (cb + lane < PR.nb) ? PR.bn[cb + lane] : __int_as_float(0x7f800000);
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {
+          const float bn = __shfl_sync(0xffffffffu, bnl, q);
+          const float a = __fmaf_rn(-2.0f, __uint_as_float(r[q]), an + bn);
+          if (a < v[kTopK - 1]) {
+            float x = a;
+            int xi = cb + q;
+#pragma unroll
+            for (int k = 0; k < kTopK; ++k) {
+              if (x < v[k]) {
+                const float tv = v[k];
+                const int ti = vi[k];
+                v[k] = x;
+                vi[k] = xi;
+                x = tv;
+                xi = ti;
+              }
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[s]);
+    }
+    if (row_ok) {
+      const long long o = ((long long)it.split * PR.na + a_local) * kTopK;
+#pragma unroll
+      for (int k = 0; k < kTopK; ++k) {
+        PR.cand_val[o + k] = v[k];
+        PR.cand_idx[o + k] = vi[k];
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+  }
+}
+
+// ------------------------------------------------------------ bf16 operands
+// One warp per row: bf16 copy (zero rows for padding are pre-cleared), exact f32
+// squared norm (sequential), running max of the norms.
+__global__ void to_bf16_kernel(const float* __restrict__ x, int n, uint16_t* __restrict__ out,
+                               float* __restrict__ norms, float* norm_max) {
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const float4 v = reinterpret_cast<const float4*>(x + (size_t)row * 128)[lane];
+  const float e[4] = {v.x, v.y, v.z, v.w};
+  unsigned short b[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    // round to nearest even
+    const uint32_t u = __float_as_uint(e[i]);
+    const uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
+    b[i] = (unsigned short)(r >> 16);
+  }
+  uint2 packed;
+  packed.x = (uint32_t)b[0] | ((uint32_t)b[1] << 16);
+  packed.y = (uint32_t)b[2] | ((uint32_t)b[3] << 16);
+  reinterpret_cast<uint2*>(out + (size_t)row * 128)[lane] = packed;
+  // exact sequential norm: lane 0 gathers the 128 values in order
+  float s = 0.0f;
+  for (int i = 0; i < 128; ++i) {
+    const float xi = __shfl_sync(0xffffffffu, e[i & 3], i >> 2);
+    s += xi * xi;
+  }
+  if (lane == 0) {
+    norms[row] = s;
+    atomicMax(reinterpret_cast<unsigned int*>(norm_max), __float_as_uint(s));
+  }
+}
+
+// Exact reference distance between two descriptors (sequential order).
+__device__ __forceinline__ float exact_d2(const float* __restrict__ a, const float* __restrict__ b) {
+  float s = 0.0f;
+#pragma unroll 4
+  for (int i = 0; i < 128; i += 4) {
+    const float4 x = *reinterpret_cast<const float4*>(a + i);
+    const float4 y = *reinterpret_cast<const float4*>(b + i);
+    float d = x.x - y.x;
+    s += d * d;
+    d = x.y - y.y;
+    s += d * d;
+    d = x.z - y.z;
+    s += d * d;
+    d = x.w - y.w;
+    s += d * d;
+  }
+  return s;
+}
+
+// One warp per A row.
+__global__ void rerank_kernel(const RerankJob* __restrict__ jobs) {
+  const RerankJob& J = jobs[blockIdx.y];
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= J.na) return;
+  const bool forward = J.second != nullptr;
+  // global top-8 over the splits' candidate lists (lane-parallel bitonic would be
+  // overkill: lane 0 merges at most 8*splits entries)
+  float v[kTopK];
+  int vi[kTopK];
+#pragma unroll
+  for (int k = 0; k < kTopK; ++k) {
+    v[k] = __int_as_float(0x7f800000);
+    vi[k] = 0x7fffffff;
+  }
+  for (int s = 0; s < J.splits; ++s) {
+    const long long o = ((long long)s * J.na + row) * kTopK;
+    for (int k = 0; k < kTopK; ++k) {
+      float x = J.cand_val[o + k];
+      int xi = J.cand_idx[o + k];
+      if (xi == 0x7fffffff) break;
+#pragma unroll
+      for (int m = 0; m < kTopK; ++m) {
+        if (x < v[m] || (x == v[m] && xi < vi[m])) {
+          const float tv = v[m];
+          const int ti = vi[m];
+          v[m] = x;
+          vi[m] = xi;
+          x = tv;
+          xi = ti;
+        }
+      }
+    }
+  }
+  const float an = J.an[row];
+  const float bmax = *J.bn_max;
+  const float eps = 0.008f * sqrtf(an) * sqrtf(bmax) + 5e-5f * (an + bmax) + 1e-6f;
+  const float inf = __int_as_float(0x7f800000);
+  if (!forward && J.flags && J.flags[row] == 0) {
+    if (lane == 0) {
+      J.best[row] = inf;
+      J.best_idx[row] = 0x7fffffff;
+    }
+    return;
+  }
+  if (forward && J.nb > 1 && v[1] < inf) {
+    // Certified rejection: exact d1 >= a_(1) - eps and exact d2 <= a_(2) + eps, so
+    // if (a_(1) - eps) >= R^2 (a_(2) + eps)(1 + 1e-5) the reference's
+    // sqrt(d1)/sqrt(d2) (three f32 roundings) is >= R and the query has no match.
+    const double lo1 = (double)v[0] - (double)eps;
+    const double hi2 = (double)v[1] + (double)eps;
+    const double r = (double)J.ratio;
+    if (lo1 > 0.0 && lo1 >= r * r * hi2 * (1.0 + 1e-5)) {
+      if (lane == 0) {
+        J.best[row] = inf;
+        J.second[row] = inf;
+        J.best_idx[row] = 0x7fffffff;
+      }
+      return;
+    }
+  }
+  const bool all_in = J.nb <= kTopK;
+  const bool certified = all_in || (forward ? v[kTopK - 1] > v[1] + 2.0f * eps : v[kTopK - 1] > v[0] + 2.0f * eps);
+  const float* arow = J.a + (size_t)row * 128;
+  float b = inf, sec = b;
+  int bi = 0x7fffffff;
+  if (certified) {
+    if (lane < kTopK && vi[lane] < J.nb) {
+      const float d = exact_d2(arow, J.b + (size_t)vi[lane] * 128);
+      top2_push(b, bi, sec, d, vi[lane]);
+    }
+  } else {
+    if (lane == 0) atomicAdd(J.fallbacks, 1u);
+    for (int t = lane; t < J.nb; t += 32) top2_push(b, bi, sec, exact_d2(arow, J.b + (size_t)t * 128), t);
+  }
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    const float b2 = __shfl_xor_sync(0xffffffffu, b, off);
+    const int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
+    const float s2 = __shfl_xor_sync(0xffffffffu, sec, off);
+    top2_merge(b, bi, sec, b2, i2, s2);
+  }
+  if (forward && J.flags && lane == 0 && sec > 1e-12f && b < inf && bi < J.nb) {
+    // the reference's ratio test (src/pipeline.rs:1789-1794): mark the target for the reverse pass
+    if (sqrtf(b) / sqrtf(sec) < J.ratio) J.flags[bi] = 1;
+  }
+  if (lane == 0) {
+    J.best[row] = b;
+    J.best_idx[row] = bi;
+    if (forward) J.second[row] = sec;
+  }
+}
+
+// ------------------------------------------------------------------- host
+namespace {
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+}  // namespace
+
+// 2D bf16 tensor map over `rows` x 128, box = 64 columns x box_rows, 128B swizzle.
+bool make_operand_map(CUtensorMap* tm, const void* base, long long rows, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {128, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {256};
+  cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t launch_to_bf16(const float* x, int n, void* out, float* norms, float* norm_max, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  to_bf16_kernel<<<(n + 7) / 8, 256, 0, st>>>(x, n, (uint16_t*)out, norms, norm_max);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcItem* items, int n_items,
+                            const TcPair* pairs, uint32_t* err, cudaStream_t st) {
+  cudaError_t e = ensure_smem_attr((const void*)match_tc_kernel, kSmTotal);
+  if (e != cudaSuccess) return e;
+  match_tc_kernel<<<n_items, kTcThreads, kSmTotal, st>>>(tmA, tmB, items, pairs, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st) {
+  dim3 grid((max_rows + 7) / 8, n_jobs);
+  rerank_kernel<<<grid, 256, 0, st>>>(jobs);
+  return cudaGetLastError();
+}
+
+}  // namespace psift

@@ -61,10 +61,11 @@ struct psift_ctx {
   cudaStream_t stream = nullptr;
   std::string last_error;
   uint64_t launches = 0;
-  psift::DeviceArena arena;
+  psift::DeviceArena arena;   // per-call workspace
+  psift::DeviceArena io;      // device copies of host-pointer inputs/outputs
   psift::PinnedBuffer pinned;
   int num_sms = 148;
-  // Device error word for bounded waits and capacity overflows (see kErr* below).
+  // Device status words: [0] error bits (kErr* below), [1] re-rank fallback rows.
   uint32_t* d_error = nullptr;
   psift::StageTimer timer;
 };
@@ -84,6 +85,8 @@ psift_status arena_reserve(psift_ctx* ctx, size_t bytes);
 // Bump-allocate (256-byte aligned).  Caller must have reserved enough.
 void* arena_alloc(psift_ctx* ctx, size_t bytes);
 psift_status pinned_reserve(psift_ctx* ctx, size_t bytes);
+// Grow-only device buffer for the host-pointer entry points' inputs/outputs.
+psift_status io_reserve(psift_ctx* ctx, size_t bytes);
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Raise a kernel's dynamic shared-memory limit once per (kernel, device).
 cudaError_t ensure_smem_attr(const void* func, size_t bytes);

@@ -70,6 +70,22 @@ class CImageU8(C.Structure):
     _fields_ = [("data", C.c_void_p), ("height", C.c_uint32), ("width", C.c_uint32), ("row_stride", C.c_size_t)]
 
 
+class CMatchOptions(C.Structure):
+    _fields_ = [("ratio", C.c_float), ("mutual", C.c_int32), ("precision", C.c_int32)]
+
+
+class CMatchJob(C.Structure):
+    _fields_ = [("query_descriptors", C.c_void_p), ("target_descriptors", C.c_void_p), ("query_xy", C.c_void_p),
+                ("target_xy", C.c_void_p), ("nq", C.c_uint32), ("nt", C.c_uint32), ("out", C.c_void_p),
+                ("capacity", C.c_uint32), ("d_count", C.c_void_p)]
+
+
+MATCH_DTYPE = np.dtype([("query_index", "<u4"), ("target_index", "<u4"), ("query_x", "<f4"), ("query_y", "<f4"),
+                        ("target_x", "<f4"), ("target_y", "<f4"), ("distance", "<f4"), ("ratio", "<f4"),
+                        ("displacement_x", "<f4"), ("displacement_y", "<f4")])
+PRECISION_FP32 = 0
+PRECISION_BF16_RERANK = 1
+
 KEYPOINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("scale", "<f4"), ("response", "<f4"),
                            ("octave", "<u4"), ("layer", "<u4")])
 
@@ -93,6 +109,13 @@ _SIGS = {
                                          C.POINTER(CSiftConfig), C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "psift_detect_and_compute_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CImageU8), C.c_uint32,
                                                      C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p]),
+    "psift_match_options_default": (None, [C.POINTER(CMatchOptions)]),
+    "psift_match_options_validate": (C.c_int, [C.POINTER(CMatchOptions), C.c_char_p, C.c_size_t]),
+    "psift_match_descriptors": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                          C.c_void_p, C.POINTER(CMatchOptions), C.c_void_p, C.c_uint32,
+                                          C.POINTER(C.c_uint32)]),
+    "psift_match_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CMatchJob), C.c_uint32, C.POINTER(CMatchOptions)]),
+    "psift_ctx_rerank_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "psift_detect_and_compute_u8_noalloc_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
                                                           C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p,
                                                           C.c_void_p]),
@@ -301,3 +324,59 @@ class Sift:
                 continue
             ctx.check(st)
             return out[:n.value].copy()
+
+
+@dataclass(frozen=True)
+class MatchOptions:
+    """``MatchOptions`` (src/pipeline.rs:1721-1736) plus the arithmetic path.
+
+    ``precision=PRECISION_BF16_RERANK`` (default) computes distances on the
+    tensor cores in bf16 and re-ranks every query's candidates in exact f32; the
+    match list is identical to ``PRECISION_FP32``.
+    """
+    ratio: float = DEFAULT_MATCH_RATIO
+    mutual: bool = False
+    precision: int = PRECISION_BF16_RERANK
+
+    def to_c(self) -> CMatchOptions:
+        return CMatchOptions(self.ratio, int(self.mutual), int(self.precision))
+
+
+@dataclass(frozen=True)
+class Matcher:
+    """``Matcher`` (src/pipeline.rs:148-170)."""
+    options: MatchOptions = field(default_factory=MatchOptions)
+
+    @staticmethod
+    def new(options: MatchOptions) -> "Matcher":
+        lib = load_library()
+        buf = C.create_string_buffer(256)
+        c = options.to_c()
+        if lib.psift_match_options_validate(C.byref(c), buf, 256) != PSIFT_OK:
+            raise ValueError(buf.value.decode())
+        return Matcher(options)
+
+    def match_(self, query: Features, target: Features, ctx: Context | None = None) -> np.ndarray:
+        return match_arrays(query.descriptors, target.descriptors, query.xy, target.xy, self.options, ctx)
+
+
+def match_arrays(q_desc, t_desc, q_xy, t_xy, options: MatchOptions = MatchOptions(), ctx: Context | None = None):
+    """Matches raw arrays (n x 128 descriptors, n x 2 coordinates); returns MATCH_DTYPE records."""
+    ctx = ctx or default_context()
+    qd = np.ascontiguousarray(q_desc, dtype=np.float32).reshape(-1, 128)
+    td = np.ascontiguousarray(t_desc, dtype=np.float32).reshape(-1, 128)
+    qxy = np.ascontiguousarray(q_xy, dtype=np.float32).reshape(-1, 2)
+    txy = np.ascontiguousarray(t_xy, dtype=np.float32).reshape(-1, 2)
+    nq, nt = qd.shape[0], td.shape[0]
+    out = np.zeros(max(nq, 1), MATCH_DTYPE)
+    n = C.c_uint32()
+    c = options.to_c()
+    ctx.check(ctx.lib.psift_match_descriptors(ctx.handle, qd.ctypes.data, nq, td.ctypes.data, nt, qxy.ctypes.data,
+                                              txy.ctypes.data, C.byref(c), out.ctypes.data, out.shape[0],
+                                              C.byref(n)))
+    return out[:n.value].copy()
+
+
+def match_descriptors(query: Features, target: Features, ratio_threshold: float, ctx: Context | None = None):
+    """``match_descriptors`` (src/pipeline.rs:1845-1858)."""
+    return Matcher.new(MatchOptions(ratio=ratio_threshold)).match_(query, target, ctx)

@@ -63,3 +63,16 @@ def test_valid_configs_accepted():
     for o in (1, 8):
         for s in (3, 10):
             psift.SiftConfig(octaves=o, scales=s, contrast_threshold=1.0).validate()
+
+
+@pytest.mark.parametrize("ratio", [0.0, -1.0, 1.5, float("nan"), float("inf")])
+def test_invalid_match_ratio_rejected(ratio):
+    # Matcher::new, src/pipeline.rs:156-164
+    with pytest.raises(ValueError) as ei:
+        psift.Matcher.new(psift.MatchOptions(ratio=ratio))
+    assert "must be finite and in (0.0, 1.0]" in str(ei.value)
+
+
+def test_valid_match_options():
+    psift.Matcher.new(psift.MatchOptions(ratio=1.0))
+    psift.Matcher.new(psift.MatchOptions(ratio=0.01, mutual=True, precision=psift.PRECISION_FP32))
