@@ -23,15 +23,24 @@ cudaError_t launch_match_merge(const MatchPair* d_pairs, int n_pairs, int max_n,
                                const long long* part_off, const long long* cpart_off, bool mutual, cudaStream_t st);
 cudaError_t launch_match_emit(const MatchPair* d_pairs, int n_pairs, float ratio, bool mutual, cudaStream_t st);
 bool make_operand_map(CUtensorMap* tm, const void* base, long long rows, int box_rows);
-cudaError_t launch_to_bf16(const float* x, int n, void* out, float* norms, float* norm_max, cudaStream_t st);
+struct Bf16Job {
+  const float* x;
+  int n;
+  uint16_t* out;
+  float* norms;
+  float* norm_max;
+};
+cudaError_t launch_to_bf16(const void* jobs, int n_jobs, int max_rows, cudaStream_t st);
 cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcItem* items, int n_items,
-                            const TcPair* pairs, uint32_t* err, cudaStream_t st);
+                            const TcPair* pairs, uint32_t* err, int mode, cudaStream_t st);
+cudaError_t launch_window(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 
 namespace {
 
 constexpr int kTile = 128;
 constexpr int kTcBM = 128, kTcBN = 256;
+constexpr int kCollRows = 32;  // window indices kept per (split, row); equals kColl in match_tc.cu
 
 // Matcher::new (src/pipeline.rs:156-164): same message.
 psift_status validate_match_options(psift_ctx* ctx, const psift_match_options* o) {
@@ -97,13 +106,13 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
       int sp = std::max(1, std::min(bt, (target_ctas + na * at - 1) / (na * at)));
       tc_split_f[k] = sp;
       n_items_f += at * sp;
-      cand_f += (long long)sp * J.nq * 8;
+      cand_f += (long long)sp * J.nq;
       if (mutual) {
         const int at2 = (int)((J.nt + kTcBM - 1) / kTcBM), bt2 = (int)((J.nq + kTcBN - 1) / kTcBN);
         int sp2 = std::max(1, std::min(bt2, (target_ctas + na * at2 - 1) / (na * at2)));
         tc_split_r[k] = sp2;
         n_items_r += at2 * sp2;
-        cand_r += (long long)sp2 * J.nt * 8;
+        cand_r += (long long)sp2 * J.nt;
       }
     }
   }
@@ -121,8 +130,10 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     bytes += (size_t)part_total * 12 + (size_t)cpart_total * 8 + 2 * sizeof(long long) * na + 1024;
   } else {
     bytes += (size_t)(q_rows + t_rows) * 256 + (size_t)(q_rows + t_rows) * 4 + 4096;
-    bytes += (size_t)(cand_f + cand_r) * 8 + sizeof(TcItem) * (n_items_f + n_items_r) +
-             sizeof(TcPair) * 2 * na + sizeof(RerankJob) * 2 * na + 8192 + (size_t)t_rows * 4;
+    bytes += (size_t)(cand_f + cand_r) * (8 + 4 * kCollRows + 4) + (size_t)(q_rows + t_rows) * 4 +
+             sizeof(TcItem) * (n_items_f + n_items_r) +
+             sizeof(TcPair) * 2 * na + sizeof(RerankJob) * 2 * na + 8192 + (size_t)t_rows * 4 +
+             sizeof(Bf16Job) * 2 * na + 512;
   }
   psift_status s = arena_reserve(ctx, bytes);
   if (s != PSIFT_OK) return s;
@@ -188,13 +199,18 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   float* qn = (float*)arena_alloc(ctx, sizeof(float) * q_rows);
   float* tn = (float*)arena_alloc(ctx, sizeof(float) * t_rows);
   float* maxes = (float*)arena_alloc(ctx, sizeof(float) * 2 * na);  // [k]: t max, [na + k]: q max
-  float* cand_v = (float*)arena_alloc(ctx, sizeof(float) * std::max<long long>(cand_f + cand_r, 1));
-  int* cand_i = (int*)arena_alloc(ctx, sizeof(int) * std::max<long long>(cand_f + cand_r, 1));
+  const long long cand = std::max<long long>(cand_f + cand_r, 1);
+  float* top2 = (float*)arena_alloc(ctx, sizeof(float) * 2 * cand);
+  int* coll_idx = (int*)arena_alloc(ctx, sizeof(int) * kCollRows * cand);
+  int* coll_cnt = (int*)arena_alloc(ctx, sizeof(int) * cand);
+  float* thr = (float*)arena_alloc(ctx, sizeof(float) * (q_rows + t_rows));
   TcItem* d_items = (TcItem*)arena_alloc(ctx, sizeof(TcItem) * (n_items_f + n_items_r));
   TcPair* d_tcp = (TcPair*)arena_alloc(ctx, sizeof(TcPair) * 2 * na);
   RerankJob* d_rj = (RerankJob*)arena_alloc(ctx, sizeof(RerankJob) * 2 * na);
   int* flags = mutual ? (int*)arena_alloc(ctx, sizeof(int) * t_rows) : nullptr;  // matched-target marks
-  if (!qb || !tb || !cand_i || !d_rj || (mutual && !flags))
+  Bf16Job* d_bj = (Bf16Job*)arena_alloc(ctx, sizeof(Bf16Job) * 2 * na);
+  std::vector<Bf16Job> bj(2 * na);
+  if (!qb || !tb || !thr || !coll_cnt || !d_rj || !d_bj || (mutual && !flags))
     return set_error(ctx, PSIFT_ERR_INTERNAL, "match workspace carve overflow");
   if (mutual) PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * t_rows, st));
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(qb, 0, (size_t)q_rows * 256, st));
@@ -218,6 +234,28 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   std::vector<TcPair> tcp(2 * na);
   std::vector<RerankJob> rj(2 * na);
   long long cf = 0;
+  // one direction: A rows matched against B rows
+  auto add_problem = [&](int slot, int pair_k, int nA, int nB, const float* an, const float* bn, int splits,
+                         long long a_row0, long long b_row0, float* thr_rows) {
+    TcPair& T = tcp[slot];
+    T.na = nA;
+    T.nb = nB;
+    T.an = an;
+    T.bn = bn;
+    T.top2 = top2 + 2 * cf;
+    T.thr = thr_rows;
+    T.coll_idx = coll_idx + (long long)kCollRows * cf;
+    T.coll_cnt = coll_cnt + cf;
+    T.splits = splits;
+    cf += (long long)splits * nA;
+    const int at = (nA + kTcBM - 1) / kTcBM, bt = (nB + kTcBN - 1) / kTcBN;
+    for (int a = 0; a < at; ++a)
+      for (int sp = 0; sp < splits; ++sp) {
+        const int b0 = (int)((long long)bt * sp / splits), b1 = (int)((long long)bt * (sp + 1) / splits);
+        items.push_back({slot, (int)a_row0 + a * kTcBM, a * kTcBM, (int)b_row0 + b0 * kTcBN, b0 * kTcBN, b1 - b0, sp});
+      }
+    (void)pair_k;
+  };
   for (int k = 0; k < na; ++k) {
     MatchPair& P = pairs[k];
     P.q_row0 = (int)q0[k];
@@ -226,50 +264,21 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     P.tn = tn + t0[k];
     P.tn_max = maxes + k;
     P.qn_max = maxes + na + k;
-    // forward: A = queries, B = targets
-    {
-      TcPair& T = tcp[k];
-      T.na = P.nq;
-      T.nb = P.nt;
-      T.an = P.qn;
-      T.bn = P.tn;
-      T.cand_val = cand_v + cf;
-      T.cand_idx = cand_i + cf;
-      T.splits = tc_split_f[k];
-      cf += (long long)T.splits * P.nq * 8;
-      const int at = (P.nq + kTcBM - 1) / kTcBM, bt = (P.nt + kTcBN - 1) / kTcBN;
-      for (int a = 0; a < at; ++a)
-        for (int s = 0; s < T.splits; ++s) {
-          const int b0 = (int)((long long)bt * s / T.splits), b1 = (int)((long long)bt * (s + 1) / T.splits);
-          items.push_back({k, (int)q0[k] + a * kTcBM, a * kTcBM, (int)t0[k] + b0 * kTcBN, b0 * kTcBN, b1 - b0, s});
-        }
-      RerankJob& R = rj[k];
-      R = RerankJob{P.q, P.t, P.nq, P.nt, P.qn, P.tn_max, T.cand_val, T.cand_idx, T.splits,
-                    P.best, P.second, P.best_idx, ctx->d_error + 1, opt.ratio,
-                    mutual ? flags + t0[k] : nullptr};
-    }
+    add_problem(k, k, P.nq, P.nt, P.qn, P.tn, tc_split_f[k], q0[k], t0[k], thr + q0[k]);
+    const TcPair& T = tcp[k];
+    rj[k] = RerankJob{P.q, P.t, P.nq, P.nt, P.qn, P.tn_max, T.top2, thr + q0[k], T.coll_idx, T.coll_cnt,
+                      T.splits, P.best, P.second, P.best_idx, ctx->d_error + 1, opt.ratio,
+                      mutual ? flags + t0[k] : nullptr};
   }
   const int n_f = (int)items.size();
   if (mutual) {
     for (int k = 0; k < na; ++k) {
       MatchPair& P = pairs[k];
-      TcPair& T = tcp[na + k];
-      T.na = P.nt;
-      T.nb = P.nq;
-      T.an = P.tn;
-      T.bn = P.qn;
-      T.cand_val = cand_v + cf;
-      T.cand_idx = cand_i + cf;
-      T.splits = tc_split_r[k];
-      cf += (long long)T.splits * P.nt * 8;
-      const int at = (P.nt + kTcBM - 1) / kTcBM, bt = (P.nq + kTcBN - 1) / kTcBN;
-      for (int a = 0; a < at; ++a)
-        for (int s = 0; s < T.splits; ++s) {
-          const int b0 = (int)((long long)bt * s / T.splits), b1 = (int)((long long)bt * (s + 1) / T.splits);
-          items.push_back({na + k, (int)t0[k] + a * kTcBM, a * kTcBM, (int)q0[k] + b0 * kTcBN, b0 * kTcBN, b1 - b0, s});
-        }
-      rj[na + k] = RerankJob{P.t, P.q, P.nt, P.nq, P.tn, P.qn_max, T.cand_val, T.cand_idx, T.splits,
-                             P.col_best, nullptr, P.col_idx, ctx->d_error + 1, opt.ratio, flags + t0[k]};
+      add_problem(na + k, k, P.nt, P.nq, P.tn, P.qn, tc_split_r[k], t0[k], q0[k], thr + q_rows + t0[k]);
+      const TcPair& T = tcp[na + k];
+      rj[na + k] = RerankJob{P.t, P.q, P.nt, P.nq, P.tn, P.qn_max, T.top2, thr + q_rows + t0[k], T.coll_idx,
+                             T.coll_cnt, T.splits, P.col_best, nullptr, P.col_idx, ctx->d_error + 1, opt.ratio,
+                             flags + t0[k]};
     }
   }
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(MatchPair) * na, cudaMemcpyHostToDevice, st));
@@ -277,32 +286,35 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_tcp, tcp.data(), sizeof(TcPair) * tcp.size(), cudaMemcpyHostToDevice, st));
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_rj, rj.data(), sizeof(RerankJob) * rj.size(), cudaMemcpyHostToDevice, st));
   StageScope sc(ctx, STAGE_MATCH);
-  for (int k = 0; k < na; ++k) {
-    cudaError_t e = launch_to_bf16(pairs[k].q, pairs[k].nq, qb + (size_t)q0[k] * 128, qn + q0[k], maxes + na + k, st);
-    if (e == cudaSuccess) e = launch_to_bf16(pairs[k].t, pairs[k].nt, tb + (size_t)t0[k] * 128, tn + t0[k], maxes + k, st);
-    ctx->launches += 2;
+  int max_a = 0, max_b = 0;
+  {
+    for (int k = 0; k < na; ++k) {
+      bj[2 * k] = Bf16Job{pairs[k].q, pairs[k].nq, qb + (size_t)q0[k] * 128, qn + q0[k], maxes + na + k};
+      bj[2 * k + 1] = Bf16Job{pairs[k].t, pairs[k].nt, tb + (size_t)t0[k] * 128, tn + t0[k], maxes + k};
+      max_a = std::max(max_a, pairs[k].nq);
+      max_b = std::max(max_b, pairs[k].nt);
+    }
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_bj, bj.data(), sizeof(Bf16Job) * bj.size(), cudaMemcpyHostToDevice, st));
+    cudaError_t e = launch_to_bf16(d_bj, 2 * na, std::max(max_a, max_b), st);
+    ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "to_bf16");
   }
-  int max_a = 0, max_b = 0;
-  for (int k = 0; k < na; ++k) {
-    max_a = std::max(max_a, pairs[k].nq);
-    max_b = std::max(max_b, pairs[k].nt);
+  // forward: queries vs targets; reverse (mutual): matched targets vs queries
+  for (int dir = 0; dir < (mutual ? 2 : 1); ++dir) {
+    const CUtensorMap& A = dir == 0 ? tmQA : tmTA;
+    const CUtensorMap& B = dir == 0 ? tmTB : tmQB;
+    const TcItem* it0 = d_items + (dir == 0 ? 0 : n_f);
+    const int n_it = dir == 0 ? n_f : (int)items.size() - n_f;
+    const RerankJob* jobs_dir = d_rj + dir * na;
+    const int rows = dir == 0 ? max_a : max_b;
+    cudaError_t e = launch_match_tc(A, B, it0, n_it, d_tcp, ctx->d_error, 0, st);
+    if (e == cudaSuccess) e = launch_window(jobs_dir, na, rows, st);
+    if (e == cudaSuccess) e = launch_match_tc(A, B, it0, n_it, d_tcp, ctx->d_error, 1, st);
+    if (e == cudaSuccess) e = launch_rerank(jobs_dir, na, rows, st);
+    ctx->launches += 4;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc / window / rerank");
   }
-  cudaError_t e = launch_match_tc(tmQA, tmTB, d_items, n_f, d_tcp, ctx->d_error, st);
-  ctx->launches++;
-  if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc");
-  e = launch_rerank(d_rj, na, max_a, st);
-  ctx->launches++;
-  if (e != cudaSuccess) return cuda_error(ctx, e, "rerank");
-  if (mutual) {
-    e = launch_match_tc(tmTA, tmQB, d_items + n_f, (int)items.size() - n_f, d_tcp, ctx->d_error, st);
-    ctx->launches++;
-    if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc(reverse)");
-    e = launch_rerank(d_rj + na, na, max_b, st);
-    ctx->launches++;
-    if (e != cudaSuccess) return cuda_error(ctx, e, "rerank(reverse)");
-  }
-  e = launch_match_emit(d_pairs, na, opt.ratio, mutual, st);
+  cudaError_t e = launch_match_emit(d_pairs, na, opt.ratio, mutual, st);
   ctx->launches++;
   if (e != cudaSuccess) return cuda_error(ctx, e, "match_emit");
   return PSIFT_OK;

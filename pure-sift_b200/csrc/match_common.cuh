@@ -48,8 +48,10 @@ struct TcPair {
   int na, nb;
   const float* an;   // f32 squared norms of A rows
   const float* bn;   // f32 squared norms of B rows
-  float* cand_val;   // [splits][na][8]
-  int* cand_idx;
+  float* top2;       // pass 1 output: [splits][na][2] two smallest approximate distances
+  const float* thr;  // pass 2 input: [na] candidate window (-inf: nothing to collect)
+  int* coll_idx;     // pass 2 output: [splits][na][kColl] window indices
+  int* coll_cnt;     // [splits][na] window sizes (may exceed kColl = overflow)
   int splits;
 };
 
@@ -60,8 +62,10 @@ struct RerankJob {
   int na, nb;
   const float* an;
   const float* bn_max;  // scalar
-  const float* cand_val;
-  const int* cand_idx;
+  const float* top2;    // [splits][na][2]
+  float* thr;           // [na]
+  const int* coll_idx;  // [splits][na][kColl]
+  const int* coll_cnt;  // [splits][na]
   int splits;
   float* best;          // outputs; `second` is null for the reverse (best-only) pass
   float* second;

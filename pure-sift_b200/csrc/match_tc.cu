@@ -9,11 +9,13 @@
 // (bf16 rounding of both operands <= 2^-8 relative per product, tensor-core f32
 // accumulation, the f32 norms and the reference's own sequential f32 rounding, all
 // bounded with margin).  Every target that can be the exact best or second has
-// a_ij <= a_(2) + 2 eps_i.  The epilogue keeps each row's 8 smallest a_ij (ties by
-// index); if the 8th is > a_(2) + 2 eps_i the 8 candidates provably contain the
-// exact best and second, and their exact reference distances are recomputed in
-// f32 (sequential order).  Otherwise the row falls back to an exact scan of all
-// targets.  Either way best/second/index equal the FP32 path bit for bit.
+// a_ij <= a_(2) + 2 eps_i.  Pass 1 of the GEMM keeps each row's two smallest a_ij;
+// window_kernel either certifies that the row fails the ratio test (then no exact
+// work is needed) or sets the row's window thr = a_(2) + 2 eps_i; pass 2 (same
+// GEMM, deterministic) collects every index with a_ij <= thr, and the exact
+// reference distances of those candidates give best/second/index equal to the
+// FP32 path bit for bit.  A row whose window holds more than kColl indices in
+// one split is matched by an exact scan of all targets.
 //
 // Kernel structure (one CTA = one 128-row A tile x a range of 256-row B tiles,
 // 192 threads): warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
@@ -33,7 +35,7 @@ constexpr int kTcThreads = 192;
 constexpr int kBM = 128;
 constexpr int kBN = 256;
 constexpr uint32_t kSpinLimit = 1u << 25;
-constexpr int kTopK = 8;
+constexpr int kColl = 32;  // window indices kept per (split, row)
 
 // ---------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -125,7 +127,7 @@ constexpr uint32_t kSmTotal = kSmBar + 256 + 1024;  // + alignment slack
 
 __global__ void __launch_bounds__(kTcThreads, 1)
     match_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                    const TcItem* __restrict__ items, const TcPair* __restrict__ pairs, uint32_t* err) {
+                    const TcItem* __restrict__ items, const TcPair* __restrict__ pairs, uint32_t* err, int mode) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kSmBar);  // [2]
@@ -232,13 +234,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int a_local = it.a_local + row;
     const bool row_ok = a_local < PR.na;
     const float an = row_ok ? PR.an[a_local] : 0.0f;
-    float v[kTopK];
-    int vi[kTopK];
-#pragma unroll
-    for (int k = 0; k < kTopK; ++k) {
-      v[k] = __int_as_float(0x7f800000);
-      vi[k] = 0x7fffffff;
-    }
+    const float inf = __int_as_float(0x7f800000);
+    // mode 0: the two smallest values; mode 1: indices with a <= thr (the row's window)
+    float v0 = inf, v1 = inf;
+    const float thr = (mode == 1 && row_ok) ? PR.thr[a_local] : -inf;
+    int cnt = 0;
+    int* coll = PR.coll_idx + ((long long)it.split * PR.na + (row_ok ? a_local : 0)) * kColl;
     for (int j = 0; j < nt; ++j) {
       const int s = j & 1;
       const uint32_t use = (uint32_t)(j >> 1);
@@ -256,24 +257,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncwarp();
         tmem_ld32(taddr + (uint32_t)(c * 32), r);
         const int cb = col0 + c * 32;
-        const float bnl = (cb + lane < PR.nb) ? PR.bn[cb + lane] : __int_as_float(0x7f800000);
+        const float bnl = (cb + lane < PR.nb) ? PR.bn[cb + lane] : inf;
+        if (mode == 0) {
 #pragma unroll
-        for (int q = 0; q < 32; ++q) {
-          const float bn = __shfl_sync(0xffffffffu, bnl, q);
-          const float a = __fmaf_rn(-2.0f, __uint_as_float(r[q]), an + bn);
-          if (a < v[kTopK - 1]) {
-            float x = a;
-            int xi = cb + q;
+          for (int q = 0; q < 32; ++q) {
+            const float a = __fmaf_rn(-2.0f, __uint_as_float(r[q]), an + __shfl_sync(0xffffffffu, bnl, q));
+            const float hi = fmaxf(v0, a);
+            v0 = fminf(v0, a);
+            v1 = fminf(v1, hi);
+          }
+        } else {
 #pragma unroll
-            for (int k = 0; k < kTopK; ++k) {
-              if (x < v[k]) {
-                const float tv = v[k];
-                const int ti = vi[k];
-                v[k] = x;
-                vi[k] = xi;
-                x = tv;
-                xi = ti;
-              }
+          for (int q = 0; q < 32; ++q) {
+            const float a = __fmaf_rn(-2.0f, __uint_as_float(r[q]), an + __shfl_sync(0xffffffffu, bnl, q));
+            if (a <= thr) {
+              if (cnt < kColl) coll[cnt] = cb + q;
+              ++cnt;
             }
           }
         }
@@ -283,11 +282,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if (lane == 0) mbar_arrive(&acce[s]);
     }
     if (row_ok) {
-      const long long o = ((long long)it.split * PR.na + a_local) * kTopK;
-#pragma unroll
-      for (int k = 0; k < kTopK; ++k) {
-        PR.cand_val[o + k] = v[k];
-        PR.cand_idx[o + k] = vi[k];
+      const long long o = (long long)it.split * PR.na + a_local;
+      if (mode == 0) {
+        PR.top2[2 * o] = v0;
+        PR.top2[2 * o + 1] = v1;
+      } else {
+        PR.coll_cnt[o] = cnt;
       }
     }
   }
@@ -302,11 +302,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ------------------------------------------------------------ bf16 operands
 // One warp per row: bf16 copy (zero rows for padding are pre-cleared), exact f32
 // squared norm (sequential), running max of the norms.
-__global__ void to_bf16_kernel(const float* __restrict__ x, int n, uint16_t* __restrict__ out,
-                               float* __restrict__ norms, float* norm_max) {
+struct Bf16Job {
+  const float* x;
+  int n;
+  uint16_t* out;
+  float* norms;
+  float* norm_max;
+};
+
+__global__ void to_bf16_kernel(const Bf16Job* __restrict__ jobs) {
+  const Bf16Job& J = jobs[blockIdx.y];
+  const float* __restrict__ x = J.x;
+  uint16_t* __restrict__ out = J.out;
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (row >= n) return;
+  if (row >= J.n) return;
   const float4 v = reinterpret_cast<const float4*>(x + (size_t)row * 128)[lane];
   const float e[4] = {v.x, v.y, v.z, v.w};
   unsigned short b[4];
@@ -328,8 +338,8 @@ __global__ void to_bf16_kernel(const float* __restrict__ x, int n, uint16_t* __r
     s += xi * xi;
   }
   if (lane == 0) {
-    norms[row] = s;
-    atomicMax(reinterpret_cast<unsigned int*>(norm_max), __float_as_uint(s));
+    J.norms[row] = s;
+    atomicMax(reinterpret_cast<unsigned int*>(J.norm_max), __float_as_uint(s));
   }
 }
 
@@ -352,92 +362,80 @@ __device__ __forceinline__ float exact_d2(const float* __restrict__ a, const flo
   return s;
 }
 
-// One warp per A row.
+// Per A row (thread): merge the splits' two smallest values, certify rejection
+// or set the candidate window thr = a_(2) + 2 eps (forward) / a_(1) + 2 eps (reverse).
+__global__ void window_kernel(const RerankJob* __restrict__ jobs) {
+  const RerankJob& J = jobs[blockIdx.y];
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= J.na) return;
+  const bool forward = J.second != nullptr;
+  const float inf = __int_as_float(0x7f800000);
+  float v0 = inf, v1 = inf;
+  for (int s = 0; s < J.splits; ++s) {
+    const long long o = (long long)s * J.na + row;
+    const float a = J.top2[2 * o], b = J.top2[2 * o + 1];
+    // union multiset of {v0, v1} and {a, b}: two smallest
+    const float lo = fminf(v0, a), hi = fmaxf(v0, a);
+    v1 = fminf(fminf(v1, b), hi);
+    v0 = lo;
+  }
+  const float an = J.an[row];
+  const float bmax = *J.bn_max;
+  const float eps = 0.008f * sqrtf(an) * sqrtf(bmax) + 5e-5f * (an + bmax) + 1e-6f;
+  float thr = (forward ? v1 : v0) + 2.0f * eps;
+  if (!forward && J.flags && J.flags[row] == 0) thr = -inf;
+  if (forward && v1 < inf) {
+    // Certified rejection: exact d1 >= a_(1) - eps and exact d2 <= a_(2) + eps, so
+    // if (a_(1) - eps) >= R^2 (a_(2) + eps)(1 + 1e-5) the reference's
+    // sqrt(d1)/sqrt(d2) (three f32 roundings) is >= R and the query has no match.
+    const double lo1 = (double)v0 - (double)eps;
+    const double hi2 = (double)v1 + (double)eps;
+    const double r = (double)J.ratio;
+    if (lo1 > 0.0 && lo1 >= r * r * hi2 * (1.0 + 1e-5)) thr = -inf;
+  }
+  J.thr[row] = thr;
+}
+
+// One warp per A row: exact reference distances over the window candidates
+// (every index with a <= thr, collected by the second GEMM pass), or over all
+// B rows when a split's window overflowed kColl.
 __global__ void rerank_kernel(const RerankJob* __restrict__ jobs) {
   const RerankJob& J = jobs[blockIdx.y];
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= J.na) return;
   const bool forward = J.second != nullptr;
-  // global top-8 over the splits' candidate lists (lane-parallel bitonic would be
-  // overkill: lane 0 merges at most 8*splits entries)
-  float v[kTopK];
-  int vi[kTopK];
-#pragma unroll
-  for (int k = 0; k < kTopK; ++k) {
-    v[k] = __int_as_float(0x7f800000);
-    vi[k] = 0x7fffffff;
-  }
-  for (int s = 0; s < J.splits; ++s) {
-    const long long o = ((long long)s * J.na + row) * kTopK;
-    for (int k = 0; k < kTopK; ++k) {
-      float x = J.cand_val[o + k];
-      int xi = J.cand_idx[o + k];
-      if (xi == 0x7fffffff) break;
-#pragma unroll
-      for (int m = 0; m < kTopK; ++m) {
-        if (x < v[m] || (x == v[m] && xi < vi[m])) {
-          const float tv = v[m];
-          const int ti = vi[m];
-          v[m] = x;
-          vi[m] = xi;
-          x = tv;
-          xi = ti;
+  const float inf = __int_as_float(0x7f800000);
+  float b = inf, sec = inf;
+  int bi = 0x7fffffff;
+  if (J.thr[row] != -inf) {
+    bool overflow = false;
+    for (int s = 0; s < J.splits; ++s) overflow |= J.coll_cnt[(long long)s * J.na + row] > kColl;
+    const float* arow = J.a + (size_t)row * 128;
+    if (!overflow) {
+      for (int s = 0; s < J.splits; ++s) {
+        const long long o = (long long)s * J.na + row;
+        const int c = J.coll_cnt[o];
+        for (int k = lane; k < c; k += 32) {
+          const int t = J.coll_idx[o * kColl + k];
+          top2_push(b, bi, sec, exact_d2(arow, J.b + (size_t)t * 128), t);
         }
       }
+    } else {
+      if (lane == 0) atomicAdd(J.fallbacks, 1u);
+      for (int t = lane; t < J.nb; t += 32) top2_push(b, bi, sec, exact_d2(arow, J.b + (size_t)t * 128), t);
     }
-  }
-  const float an = J.an[row];
-  const float bmax = *J.bn_max;
-  const float eps = 0.008f * sqrtf(an) * sqrtf(bmax) + 5e-5f * (an + bmax) + 1e-6f;
-  const float inf = __int_as_float(0x7f800000);
-  if (!forward && J.flags && J.flags[row] == 0) {
-    if (lane == 0) {
-      J.best[row] = inf;
-      J.best_idx[row] = 0x7fffffff;
-    }
-    return;
-  }
-  if (forward && J.nb > 1 && v[1] < inf) {
-    // Certified rejection: exact d1 >= a_(1) - eps and exact d2 <= a_(2) + eps, so
-    // if (a_(1) - eps) >= R^2 (a_(2) + eps)(1 + 1e-5) the reference's
-    // sqrt(d1)/sqrt(d2) (three f32 roundings) is >= R and the query has no match.
-    const double lo1 = (double)v[0] - (double)eps;
-    const double hi2 = (double)v[1] + (double)eps;
-    const double r = (double)J.ratio;
-    if (lo1 > 0.0 && lo1 >= r * r * hi2 * (1.0 + 1e-5)) {
-      if (lane == 0) {
-        J.best[row] = inf;
-        J.second[row] = inf;
-        J.best_idx[row] = 0x7fffffff;
-      }
-      return;
-    }
-  }
-  const bool all_in = J.nb <= kTopK;
-  const bool certified = all_in || (forward ? v[kTopK - 1] > v[1] + 2.0f * eps : v[kTopK - 1] > v[0] + 2.0f * eps);
-  const float* arow = J.a + (size_t)row * 128;
-  float b = inf, sec = b;
-  int bi = 0x7fffffff;
-  if (certified) {
-    if (lane < kTopK && vi[lane] < J.nb) {
-      const float d = exact_d2(arow, J.b + (size_t)vi[lane] * 128);
-      top2_push(b, bi, sec, d, vi[lane]);
-    }
-  } else {
-    if (lane == 0) atomicAdd(J.fallbacks, 1u);
-    for (int t = lane; t < J.nb; t += 32) top2_push(b, bi, sec, exact_d2(arow, J.b + (size_t)t * 128), t);
-  }
 #pragma unroll
-  for (int off = 16; off >= 1; off >>= 1) {
-    const float b2 = __shfl_xor_sync(0xffffffffu, b, off);
-    const int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
-    const float s2 = __shfl_xor_sync(0xffffffffu, sec, off);
-    top2_merge(b, bi, sec, b2, i2, s2);
-  }
-  if (forward && J.flags && lane == 0 && sec > 1e-12f && b < inf && bi < J.nb) {
-    // the reference's ratio test (src/pipeline.rs:1789-1794): mark the target for the reverse pass
-    if (sqrtf(b) / sqrtf(sec) < J.ratio) J.flags[bi] = 1;
+    for (int off = 16; off >= 1; off >>= 1) {
+      const float b2 = __shfl_xor_sync(0xffffffffu, b, off);
+      const int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
+      const float s2 = __shfl_xor_sync(0xffffffffu, sec, off);
+      top2_merge(b, bi, sec, b2, i2, s2);
+    }
+    if (forward && J.flags && lane == 0 && sec > 1e-12f && b < inf && bi < J.nb) {
+      // the reference's ratio test (src/pipeline.rs:1789-1794): mark the target for the reverse pass
+      if (sqrtf(b) / sqrtf(sec) < J.ratio) J.flags[bi] = 1;
+    }
   }
   if (lane == 0) {
     J.best[row] = b;
@@ -477,17 +475,24 @@ bool make_operand_map(CUtensorMap* tm, const void* base, long long rows, int box
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-cudaError_t launch_to_bf16(const float* x, int n, void* out, float* norms, float* norm_max, cudaStream_t st) {
-  if (n <= 0) return cudaSuccess;
-  to_bf16_kernel<<<(n + 7) / 8, 256, 0, st>>>(x, n, (uint16_t*)out, norms, norm_max);
+cudaError_t launch_to_bf16(const void* jobs, int n_jobs, int max_rows, cudaStream_t st) {
+  if (n_jobs <= 0 || max_rows <= 0) return cudaSuccess;
+  dim3 grid((max_rows + 7) / 8, n_jobs);
+  to_bf16_kernel<<<grid, 256, 0, st>>>((const Bf16Job*)jobs);
   return cudaGetLastError();
 }
 
 cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcItem* items, int n_items,
-                            const TcPair* pairs, uint32_t* err, cudaStream_t st) {
+                            const TcPair* pairs, uint32_t* err, int mode, cudaStream_t st) {
   cudaError_t e = ensure_smem_attr((const void*)match_tc_kernel, kSmTotal);
   if (e != cudaSuccess) return e;
-  match_tc_kernel<<<n_items, kTcThreads, kSmTotal, st>>>(tmA, tmB, items, pairs, err);
+  match_tc_kernel<<<n_items, kTcThreads, kSmTotal, st>>>(tmA, tmB, items, pairs, err, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_window(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st) {
+  dim3 grid((max_rows + 255) / 256, n_jobs);
+  window_kernel<<<grid, 256, 0, st>>>(jobs);
   return cudaGetLastError();
 }
 
