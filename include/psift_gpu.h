@@ -178,6 +178,41 @@ psift_status psift_match_batch_dev(psift_ctx* ctx, const psift_match_job* jobs, 
  * not be certified and were matched by an exact scan, since context creation. */
 psift_status psift_ctx_rerank_fallbacks(psift_ctx* ctx, uint64_t* rows);
 
+/* ---------------------------------------------------------------- catalog */
+/* quantize_descriptor_u128 (src/catalog.rs:37-45): bit i set iff desc[i] > 0.065.
+ * codes: 2 x u64 per descriptor, little endian (word 0 = bits 0..63). */
+psift_status psift_quantize_u128(psift_ctx* ctx, const float* desc, uint32_t n, uint64_t* codes);
+/* quantize_descriptor_u8 (src/pipeline.rs:1024-1030): round(v * 512) clamped to [0, 255]. */
+psift_status psift_quantize_u8(psift_ctx* ctx, const float* desc, uint32_t n, uint8_t* out);
+/* dequantize_descriptor_u8 (src/pipeline.rs:1034-1044): v / 512, then L2 renormalised. */
+psift_status psift_dequantize_u8(psift_ctx* ctx, const uint8_t* q, uint32_t n, float* out);
+/* Coarse Hamming votes of FeatureCatalog::search_features (src/catalog.rs:588-633,
+ * :707-728).  Entry e owns catalog codes [entry_offsets[e], entry_offsets[e+1]).
+ * votes[e] = number of queries with a signature of the entry within 24 bits; with
+ * mih != 0 the signature must also share one exact byte band with the query
+ * (the multi-index-hashing path the reference takes for catalogs of > 32 entries). */
+psift_status psift_hamming_votes(psift_ctx* ctx, const uint64_t* query_codes, uint32_t nq,
+                                 const uint64_t* catalog_codes, const int64_t* entry_offsets,
+                                 uint32_t n_entries, int32_t mih, uint32_t* votes);
+/* Per query, the k (<= 64) catalog codes nearest in Hamming distance, ordered by
+ * (distance, catalog index); missing entries are 0xFFFFFFFF.  No counterpart in
+ * the reference (its shortlist is per entry); used to shortlist catalogs of
+ * millions of descriptors before an exact re-rank. */
+psift_status psift_hamming_topk(psift_ctx* ctx, const uint64_t* query_codes, uint32_t nq,
+                                const uint64_t* catalog_codes, uint64_t ncat, uint32_t k,
+                                uint32_t* idx, uint32_t* dist);
+psift_status psift_hamming_topk_dev(psift_ctx* ctx, const uint64_t* query_codes, uint32_t nq,
+                                    const uint64_t* catalog_codes, uint64_t ncat, uint32_t k,
+                                    uint32_t* idx, uint32_t* dist);
+/* Exact f32 squared L2 distances (the reference's summation order) between each
+ * query and its k candidates, re-sorted by (d2, index). */
+psift_status psift_l2_rerank(psift_ctx* ctx, const float* query_desc, uint32_t nq,
+                             const float* catalog_desc, uint64_t ncat, const uint32_t* candidates,
+                             uint32_t k, uint32_t* out_idx, float* out_d2);
+psift_status psift_l2_rerank_dev(psift_ctx* ctx, const float* query_desc, uint32_t nq,
+                                 const float* catalog_desc, const uint32_t* candidates, uint32_t k,
+                                 uint32_t* out_idx, float* out_d2);
+
 /* Allocation-free variant of psift_detect_and_compute_batch_dev for one u8 image.
  * No counterpart in the reference: it exists for callers that cannot allocate
  * device memory -- plugin hosts that hand out only a stream, real-time loops in

@@ -2,7 +2,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
-#include <set>
+#include <map>
 
 #include "psift_internal.cuh"
 
@@ -44,15 +44,19 @@ void* arena_alloc(psift_ctx* ctx, size_t bytes) {
 }
 
 cudaError_t ensure_smem_attr(const void* func, size_t bytes) {
+  // The attribute is an upper bound: only ever raise it (a lower value set for a
+  // small launch would make a later, larger launch fail).
   static std::mutex mu;
-  static std::set<std::pair<const void*, int>> done;
+  static std::map<std::pair<const void*, int>, size_t> limit;
+  if (bytes <= 48 * 1024) return cudaSuccess;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(mu);
-  if (done.count({func, dev})) return cudaSuccess;
+  auto it = limit.find({func, dev});
+  if (it != limit.end() && it->second >= bytes) return cudaSuccess;
   e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess) done.insert({func, dev});
+  if (e == cudaSuccess) limit[{func, dev}] = bytes;
   return e;
 }
 

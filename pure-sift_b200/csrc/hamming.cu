@@ -1,0 +1,362 @@
+// K9: 128-bit binary signatures and the catalog's Hamming stages.
+//
+// Reference: quantize_descriptor_u128 (src/catalog.rs:37-45),
+// FeatureCatalog::search_features coarse voting (src/catalog.rs:588-641) with the
+// multi-index-hashing tables (:291-321) and count_coarse_hamming_votes
+// (:707-728); quantize_descriptor_u8 / dequantize_descriptor_u8
+// (src/pipeline.rs:1024-1044).
+//
+// Signatures are two little-endian u64 words (bit i of the u128 = bit i%64 of
+// word i/64).  All comparisons are integer: results are bit-exact.
+//
+// Votes.  The exhaustive path counts the queries whose nearest signature in the
+// entry is within 24 bits.  The MIH path (more than 32 entries) only reaches a
+// signature through one of its 16 byte bands, i.e. when some byte of q ^ s is
+// zero; a (query, entry) pair votes iff some signature of the entry has
+// popcount(q ^ s) <= 24 AND a zero byte in q ^ s.  Both are evaluated directly,
+// without the inverted tables.
+//
+// Top-k shortlist (no reference counterpart; the catalog search at scale): the k
+// codes nearest to each query by (Hamming distance, catalog index).  One warp
+// serves 16 queries over one chunk of codes: lane i scores code base+i against the
+// 16 queries (4 XOR + 4 POPC each); a ballot finds codes beating a query's current
+// k-th entry, and the warp replaces that entry cooperatively (rare after the list
+// fills).  Chunk lists are merged per query by a second kernel.
+#include <algorithm>
+
+#include "psift_internal.cuh"
+
+namespace psift {
+
+constexpr int kQG = 16;       // queries per warp
+constexpr int kTopKMax = 64;  // shortlist length upper bound
+constexpr int kHamWarps = 4;
+
+__device__ __forceinline__ int ham128(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint4 c) {
+  return __popc(a0 ^ c.x) + __popc(a1 ^ c.y) + __popc(a2 ^ c.z) + __popc(a3 ^ c.w);
+}
+
+__device__ __forceinline__ bool has_zero_byte(uint32_t x) { return ((x - 0x01010101u) & ~x & 0x80808080u) != 0; }
+
+// quantize_descriptor_u128 + quantize_descriptor_u8: one warp per descriptor.
+__global__ void quantize_kernel(const float* __restrict__ desc, int n, uint64_t* __restrict__ codes,
+                                uint8_t* __restrict__ u8) {
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const float4 v = reinterpret_cast<const float4*>(desc + (size_t)row * 128)[lane];
+  const float e[4] = {v.x, v.y, v.z, v.w};
+  if (codes) {
+    // element 4*lane + j -> bit (4*lane + j)
+    uint32_t nib = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) nib |= (e[j] > 0.065f ? 1u : 0u) << j;
+    uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int l = 0; l < 32; ++l) {
+      const uint32_t x = __shfl_sync(0xffffffffu, nib, l);
+      w[l >> 3] |= x << (4 * (l & 7));
+    }
+    if (lane == 0) {
+      codes[2 * (size_t)row] = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+      codes[2 * (size_t)row + 1] = (uint64_t)w[2] | ((uint64_t)w[3] << 32);
+    }
+  }
+  if (u8) {
+    uint32_t packed = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float q = roundf(e[j] * 512.0f);
+      q = q < 0.0f ? 0.0f : (q > 255.0f ? 255.0f : q);
+      packed |= (uint32_t)q << (8 * j);
+    }
+    reinterpret_cast<uint32_t*>(u8 + (size_t)row * 128)[lane] = packed;
+  }
+}
+
+// dequantize_descriptor_u8: v/512 then L2 renormalisation (sequential sum).
+__global__ void dequantize_kernel(const uint8_t* __restrict__ q, int n, float* __restrict__ out) {
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const uint32_t p = reinterpret_cast<const uint32_t*>(q + (size_t)row * 128)[lane];
+  float e[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) e[j] = (float)((p >> (8 * j)) & 0xFF) * (1.0f / 512.0f);
+  float s = 0.0f;
+  for (int i = 0; i < 128; ++i) {
+    const float x = __shfl_sync(0xffffffffu, e[i & 3], i >> 2);
+    s += x * x;
+  }
+  const float norm = sqrtf(s);
+  if (norm > 1e-7f) {
+    const float inv = 1.0f / norm;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) e[j] *= inv;
+  }
+  reinterpret_cast<float4*>(out + (size_t)row * 128)[lane] = make_float4(e[0], e[1], e[2], e[3]);
+}
+
+// Votes: one block per entry, each thread owns queries tid, tid+blockDim, ...
+// The entry's signatures are read in the same order by every lane (broadcast
+// loads from L1); a query stops at its first qualifying signature.
+__global__ void __launch_bounds__(256) votes_kernel(const uint4* __restrict__ q, int nq, const uint4* __restrict__ cat,
+                                                     const long long* __restrict__ offsets, int mih,
+                                                     uint32_t* __restrict__ votes) {
+  const int e = blockIdx.x;
+  const long long s0 = offsets[e], s1 = offsets[e + 1];
+  uint32_t hits = 0;
+  for (int qi = threadIdx.x; qi < nq; qi += blockDim.x) {
+    const uint4 qq = q[qi];
+    for (long long s = s0; s < s1; ++s) {
+      const uint4 c = cat[s];
+      const uint32_t x0 = qq.x ^ c.x, x1 = qq.y ^ c.y, x2 = qq.z ^ c.z, x3 = qq.w ^ c.w;
+      const int d = __popc(x0) + __popc(x1) + __popc(x2) + __popc(x3);
+      if (d <= 24 && (!mih || has_zero_byte(x0) || has_zero_byte(x1) || has_zero_byte(x2) || has_zero_byte(x3))) {
+        ++hits;
+        break;
+      }
+    }
+  }
+  __shared__ uint32_t s_sum[8];
+  for (int o = 16; o >= 1; o >>= 1) hits += __shfl_xor_sync(0xffffffffu, hits, o);
+  if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = hits;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_sum[w];
+    votes[e] = t;
+  }
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+    v = t > v ? t : v;
+  }
+  return v;
+}
+
+// Per (16-query group, code chunk): the k smallest (distance, index) keys.
+// Grid (n_chunks, ceil(n_groups / kHamWarps)), kHamWarps warps per block.
+__global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4* __restrict__ q, int nq,
+                                                                     const uint4* __restrict__ cat, long long ncat,
+                                                                     int k, int n_chunks,
+                                                                     unsigned long long* __restrict__ part) {
+  __shared__ unsigned long long s_list[kHamWarps][kQG][kTopKMax];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int group = blockIdx.y * kHamWarps + warp;
+  const int q0 = group * kQG;
+  if (q0 >= nq) return;
+  const int chunk = blockIdx.x;
+  const long long c_begin = ncat * chunk / n_chunks, c_end = ncat * (chunk + 1) / n_chunks;
+  unsigned long long(*list)[kTopKMax] = s_list[warp];
+  uint32_t qw[kQG][4];
+#pragma unroll
+  for (int j = 0; j < kQG; ++j) {
+    const uint4 v = (q0 + j < nq) ? q[q0 + j] : make_uint4(0, 0, 0, 0);
+    qw[j][0] = v.x;
+    qw[j][1] = v.y;
+    qw[j][2] = v.z;
+    qw[j][3] = v.w;
+  }
+  unsigned long long maxkey[kQG];
+  int maxpos[kQG];
+#pragma unroll
+  for (int j = 0; j < kQG; ++j) {
+    for (int t = lane; t < kTopKMax; t += 32) list[j][t] = t < k ? ~0ull : 0ull;
+    maxkey[j] = ~0ull;
+    maxpos[j] = 0;
+  }
+  __syncwarp();
+  for (long long base = c_begin; base < c_end; base += 32) {
+    const long long idx = base + lane;
+    const bool valid = idx < c_end;
+    const uint4 c = valid ? cat[idx] : make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int j = 0; j < kQG; ++j) {
+      const uint32_t d = valid ? (uint32_t)ham128(qw[j][0], qw[j][1], qw[j][2], qw[j][3], c) : 0x7fffffffu;
+      const unsigned long long key = ((unsigned long long)d << 32) | (unsigned long long)(uint32_t)idx;
+      unsigned m = __ballot_sync(0xffffffffu, valid && key < maxkey[j]);
+      while (m) {
+        const int L = __ffs(m) - 1;
+        m &= m - 1;
+        const unsigned long long kl = __shfl_sync(0xffffffffu, key, L);
+        if (kl < maxkey[j]) {
+          if (lane == 0) list[j][maxpos[j]] = kl;
+          __syncwarp();
+          // new maximum of the k entries (slots >= k hold 0 and never win)
+          unsigned long long a = list[j][lane], b = list[j][lane + 32];
+          unsigned long long mine = a > b ? a : b;
+          const int mine_pos = a > b ? lane : lane + 32;
+          const unsigned long long mx = warp_max_u64(mine);
+          const unsigned who = __ballot_sync(0xffffffffu, mine == mx);
+          const int src = __ffs(who) - 1;
+          maxpos[j] = __shfl_sync(0xffffffffu, mine_pos, src);
+          maxkey[j] = mx;
+          __syncwarp();
+        }
+      }
+    }
+  }
+  // write this chunk's lists: part[(query * n_chunks + chunk) * k + t]
+#pragma unroll
+  for (int j = 0; j < kQG; ++j) {
+    if (q0 + j >= nq) break;
+    unsigned long long* dst = part + ((long long)(q0 + j) * n_chunks + chunk) * k;
+    for (int t = lane; t < k; t += 32) dst[t] = list[j][t];
+  }
+}
+
+// Per query (one warp): bitonic sort of the chunks' n_chunks*k keys in shared
+// memory, keep the k smallest.
+__global__ void topk_merge_kernel(const unsigned long long* __restrict__ part, int nq, int k, int n_chunks, int n2,
+                                  uint32_t* __restrict__ out_idx, uint32_t* __restrict__ out_dist) {
+  extern __shared__ unsigned long long s_keys[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
+  unsigned long long* keys = s_keys + (size_t)warp * n2;
+  if (qi >= nq) return;
+  const int total = n_chunks * k;
+  const unsigned long long* src = part + (long long)qi * total;
+  for (int t = lane; t < n2; t += 32) keys[t] = t < total ? src[t] : ~0ull;
+  __syncwarp();
+  for (int kk = 2; kk <= n2; kk <<= 1) {
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < n2; i += 32) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = keys[i], b = keys[ixj];
+          const bool up = (i & kk) == 0;
+          if ((a > b) == up) {
+            keys[i] = b;
+            keys[ixj] = a;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  for (int t = lane; t < k; t += 32) {
+    const unsigned long long key = keys[t];
+    const bool ok = key != ~0ull;
+    out_idx[(long long)qi * k + t] = ok ? (uint32_t)(key & 0xFFFFFFFFu) : 0xFFFFFFFFu;
+    out_dist[(long long)qi * k + t] = ok ? (uint32_t)(key >> 32) : 0xFFFFFFFFu;
+  }
+}
+
+// Exact FP32 L2^2 re-rank of each query's k candidates (reference summation
+// order), sorted by (d2, index).  One warp per query.
+__global__ void l2_rerank_kernel(const float* __restrict__ qd, int nq, const float* __restrict__ cd,
+                                 const uint32_t* __restrict__ cand, int k, uint32_t* __restrict__ out_idx,
+                                 float* __restrict__ out_d2) {
+  __shared__ unsigned long long s_keys[8][kTopKMax];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qi = blockIdx.x * 8 + warp;
+  if (qi >= nq) return;
+  unsigned long long* keys = s_keys[warp];
+  const float* a = qd + (size_t)qi * 128;
+  for (int t = lane; t < kTopKMax; t += 32) {
+    unsigned long long key = ~0ull;
+    if (t < k) {
+      const uint32_t c = cand[(long long)qi * k + t];
+      if (c != 0xFFFFFFFFu) {
+        const float* b = cd + (size_t)c * 128;
+        float s = 0.0f;
+        for (int i = 0; i < 128; i += 4) {
+          const float4 x = *reinterpret_cast<const float4*>(a + i);
+          const float4 y = *reinterpret_cast<const float4*>(b + i);
+          float d = x.x - y.x;
+          s += d * d;
+          d = x.y - y.y;
+          s += d * d;
+          d = x.z - y.z;
+          s += d * d;
+          d = x.w - y.w;
+          s += d * d;
+        }
+        // non-negative floats order like their bit patterns
+        key = ((unsigned long long)__float_as_uint(s) << 32) | c;
+      }
+    }
+    keys[t] = key;
+  }
+  __syncwarp();
+  for (int kk = 2; kk <= kTopKMax; kk <<= 1) {
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < kTopKMax; i += 32) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long x = keys[i], y = keys[ixj];
+          const bool up = (i & kk) == 0;
+          if ((x > y) == up) {
+            keys[i] = y;
+            keys[ixj] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  for (int t = lane; t < k; t += 32) {
+    const unsigned long long key = keys[t];
+    const bool ok = key != ~0ull;
+    out_idx[(long long)qi * k + t] = ok ? (uint32_t)(key & 0xFFFFFFFFu) : 0xFFFFFFFFu;
+    out_d2[(long long)qi * k + t] = ok ? __uint_as_float((uint32_t)(key >> 32)) : __int_as_float(0x7f800000);
+  }
+}
+
+cudaError_t launch_quantize(const float* desc, int n, uint64_t* codes, uint8_t* u8, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  quantize_kernel<<<(n + 7) / 8, 256, 0, st>>>(desc, n, codes, u8);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dequantize(const uint8_t* q, int n, float* out, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  dequantize_kernel<<<(n + 7) / 8, 256, 0, st>>>(q, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_votes(const uint64_t* q, int nq, const uint64_t* cat, const long long* offsets, int n_entries,
+                         int mih, uint32_t* votes, cudaStream_t st) {
+  if (n_entries <= 0) return cudaSuccess;
+  votes_kernel<<<n_entries, 256, 0, st>>>((const uint4*)q, nq, (const uint4*)cat, offsets, mih, votes);
+  return cudaGetLastError();
+}
+
+int topk_chunks(long long ncat, int nq, int num_sms) {
+  const int groups = (nq + kQG - 1) / kQG;
+  long long want = (long long)num_sms * 16 * 2 / std::max(groups, 1);  // ~2 waves of 16 warps per SM
+  want = std::max<long long>(1, std::min<long long>(want, 64));
+  want = std::min<long long>(want, std::max<long long>(1, ncat / 1024));
+  return (int)want;
+}
+
+cudaError_t launch_topk(const uint64_t* q, int nq, const uint64_t* cat, long long ncat, int k, int n_chunks,
+                        unsigned long long* part, uint32_t* out_idx, uint32_t* out_dist, cudaStream_t st) {
+  if (nq <= 0) return cudaSuccess;
+  const int groups = (nq + kQG - 1) / kQG;
+  dim3 g1(n_chunks, (groups + kHamWarps - 1) / kHamWarps);
+  topk_chunk_kernel<<<g1, kHamWarps * 32, 0, st>>>((const uint4*)q, nq, (const uint4*)cat, ncat, k, n_chunks, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  int n2 = 1;
+  while (n2 < n_chunks * k) n2 <<= 1;
+  const int warps = std::max(1, std::min(8, (int)(96 * 1024 / (n2 * 8))));
+  const size_t smem = (size_t)warps * n2 * 8;
+  e = ensure_smem_attr((const void*)topk_merge_kernel, smem);
+  if (e != cudaSuccess) return e;
+  topk_merge_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, st>>>(part, nq, k, n_chunks, n2, out_idx, out_dist);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_l2_rerank(const float* qd, int nq, const float* cd, const uint32_t* cand, int k,
+                             uint32_t* out_idx, float* out_d2, cudaStream_t st) {
+  if (nq <= 0) return cudaSuccess;
+  l2_rerank_kernel<<<(nq + 7) / 8, 256, 0, st>>>(qd, nq, cd, cand, k, out_idx, out_d2);
+  return cudaGetLastError();
+}
+
+}  // namespace psift

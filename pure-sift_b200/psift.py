@@ -116,6 +116,19 @@ _SIGS = {
                                           C.POINTER(C.c_uint32)]),
     "psift_match_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CMatchJob), C.c_uint32, C.POINTER(CMatchOptions)]),
     "psift_ctx_rerank_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "psift_quantize_u128": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "psift_quantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "psift_dequantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "psift_hamming_votes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                      C.c_int32, C.c_void_p]),
+    "psift_hamming_topk": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32,
+                                     C.c_void_p, C.c_void_p]),
+    "psift_hamming_topk_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_uint32,
+                                         C.c_void_p, C.c_void_p]),
+    "psift_l2_rerank": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p,
+                                  C.c_uint32, C.c_void_p, C.c_void_p]),
+    "psift_l2_rerank_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                      C.c_void_p, C.c_void_p]),
     "psift_detect_and_compute_u8_noalloc_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
                                                           C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p,
                                                           C.c_void_p]),
@@ -380,3 +393,69 @@ def match_arrays(q_desc, t_desc, q_xy, t_xy, options: MatchOptions = MatchOption
 def match_descriptors(query: Features, target: Features, ratio_threshold: float, ctx: Context | None = None):
     """``match_descriptors`` (src/pipeline.rs:1845-1858)."""
     return Matcher.new(MatchOptions(ratio=ratio_threshold)).match_(query, target, ctx)
+
+
+# ---------------------------------------------------------------- catalog codes
+def quantize_descriptor_u128(desc, ctx: Context | None = None) -> np.ndarray:
+    """``quantize_descriptor_u128`` (src/catalog.rs:37-45) for n descriptors -> (n, 2) u64 (lo, hi)."""
+    ctx = ctx or default_context()
+    d = np.ascontiguousarray(desc, dtype=np.float32).reshape(-1, 128)
+    out = np.zeros((d.shape[0], 2), np.uint64)
+    ctx.check(ctx.lib.psift_quantize_u128(ctx.handle, d.ctypes.data, d.shape[0], out.ctypes.data))
+    return out
+
+
+def quantize_descriptor_u8(desc, ctx: Context | None = None) -> np.ndarray:
+    """``quantize_descriptor_u8`` (src/pipeline.rs:1024-1030)."""
+    ctx = ctx or default_context()
+    d = np.ascontiguousarray(desc, dtype=np.float32).reshape(-1, 128)
+    out = np.zeros(d.shape, np.uint8)
+    ctx.check(ctx.lib.psift_quantize_u8(ctx.handle, d.ctypes.data, d.shape[0], out.ctypes.data))
+    return out
+
+
+def dequantize_descriptor_u8(q, ctx: Context | None = None) -> np.ndarray:
+    """``dequantize_descriptor_u8`` (src/pipeline.rs:1034-1044)."""
+    ctx = ctx or default_context()
+    qq = np.ascontiguousarray(q, dtype=np.uint8).reshape(-1, 128)
+    out = np.zeros(qq.shape, np.float32)
+    ctx.check(ctx.lib.psift_dequantize_u8(ctx.handle, qq.ctypes.data, qq.shape[0], out.ctypes.data))
+    return out
+
+
+def hamming_votes(query_codes, catalog_codes, entry_offsets, mih: bool, ctx: Context | None = None) -> np.ndarray:
+    """Coarse votes per catalog entry (src/catalog.rs:596-633 MIH, :707-728 exhaustive)."""
+    ctx = ctx or default_context()
+    q = np.ascontiguousarray(query_codes, dtype=np.uint64).reshape(-1, 2)
+    c = np.ascontiguousarray(catalog_codes, dtype=np.uint64).reshape(-1, 2)
+    off = np.ascontiguousarray(entry_offsets, dtype=np.int64)
+    votes = np.zeros(len(off) - 1, np.uint32)
+    ctx.check(ctx.lib.psift_hamming_votes(ctx.handle, q.ctypes.data, q.shape[0], c.ctypes.data, off.ctypes.data,
+                                          len(off) - 1, int(bool(mih)), votes.ctypes.data))
+    return votes
+
+
+def hamming_topk(query_codes, catalog_codes, k: int, ctx: Context | None = None):
+    """Per query, the k nearest codes by (Hamming distance, index) -> (idx, dist) (nq, k) u32."""
+    ctx = ctx or default_context()
+    q = np.ascontiguousarray(query_codes, dtype=np.uint64).reshape(-1, 2)
+    c = np.ascontiguousarray(catalog_codes, dtype=np.uint64).reshape(-1, 2)
+    idx = np.zeros((q.shape[0], k), np.uint32)
+    dist = np.zeros((q.shape[0], k), np.uint32)
+    ctx.check(ctx.lib.psift_hamming_topk(ctx.handle, q.ctypes.data, q.shape[0], c.ctypes.data, c.shape[0], k,
+                                         idx.ctypes.data, dist.ctypes.data))
+    return idx, dist
+
+
+def l2_rerank(query_desc, catalog_desc, candidates, ctx: Context | None = None):
+    """Exact f32 L2^2 of each query to its candidates, sorted by (d2, index) -> (idx, d2)."""
+    ctx = ctx or default_context()
+    qd = np.ascontiguousarray(query_desc, dtype=np.float32).reshape(-1, 128)
+    cd = np.ascontiguousarray(catalog_desc, dtype=np.float32).reshape(-1, 128)
+    cand = np.ascontiguousarray(candidates, dtype=np.uint32)
+    k = cand.shape[1]
+    idx = np.zeros_like(cand)
+    d2 = np.zeros(cand.shape, np.float32)
+    ctx.check(ctx.lib.psift_l2_rerank(ctx.handle, qd.ctypes.data, qd.shape[0], cd.ctypes.data, cd.shape[0],
+                                      cand.ctypes.data, k, idx.ctypes.data, d2.ctypes.data))
+    return idx, d2
