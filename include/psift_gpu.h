@@ -178,6 +178,45 @@ psift_status psift_match_batch_dev(psift_ctx* ctx, const psift_match_job* jobs, 
  * not be certified and were matched by an exact scan, since context creation. */
 psift_status psift_ctx_rerank_fallbacks(psift_ctx* ctx, uint64_t* rows);
 
+/* ---------------------------------------------------------------- RANSAC */
+/* RansacOptions (src/pipeline.rs:177-218). */
+typedef struct psift_ransac_options {
+  float reproj_threshold;  /* default 3.0 (DEFAULT_RANSAC_REPROJ_THRESHOLD) */
+  int32_t has_seed;        /* 0: the built-in default seeds */
+  uint64_t seed;
+} psift_ransac_options;
+void psift_ransac_options_default(psift_ransac_options* opt);
+/* RansacOptions::validate (src/pipeline.rs:209-217). */
+psift_status psift_ransac_options_validate(const psift_ransac_options* opt, char* msg, size_t msg_capacity);
+/* Homography::estimate (src/pipeline.rs:225-235 -> :2663-2755): inlier_mask[i] = 1
+ * for the returned inliers (in input order), h9 row-major, has_h = 0 for None.
+ * Same result as the reference for the same seed. */
+psift_status psift_homography_estimate(psift_ctx* ctx, const psift_match* matches, uint32_t n,
+                                       const psift_ransac_options* opt, uint8_t* inlier_mask,
+                                       float* h9, int32_t* has_h, uint32_t* inlier_count);
+/* Homography::estimate_similarity (src/pipeline.rs:238-246 -> :2055-2191):
+ * model6 = a, b, tx, ty, scale, rotation_deg. */
+psift_status psift_similarity_estimate(psift_ctx* ctx, const psift_match* matches, uint32_t n,
+                                       const psift_ransac_options* opt, uint8_t* inlier_mask,
+                                       float* model6, int32_t* has_model, uint32_t* inlier_count);
+/* Device-resident batch of independent estimations, one CTA each.  model holds 9
+ * (homography) or 6 (similarity) floats.  sampling_weights (optional) replaces the
+ * reference's 1/clamp(ratio, 0.05, 1) CDF weights (learned guided sampling);
+ * iterations (optional, 2 ints) receives the similarity and homography iteration
+ * counts.  Asynchronous. */
+typedef struct psift_ransac_job {
+  const psift_match* matches;
+  uint32_t n;
+  uint8_t* inlier_mask;
+  float* model;
+  int32_t* has_model;
+  uint32_t* inlier_count;
+  const float* sampling_weights;
+  uint32_t* iterations;
+} psift_ransac_job;
+psift_status psift_ransac_batch_dev(psift_ctx* ctx, const psift_ransac_job* jobs, uint32_t n,
+                                    const psift_ransac_options* opt, int32_t homography);
+
 /* ---------------------------------------------------------------- catalog */
 /* quantize_descriptor_u128 (src/catalog.rs:37-45): bit i set iff desc[i] > 0.065.
  * codes: 2 x u64 per descriptor, little endian (word 0 = bits 0..63). */

@@ -1,0 +1,184 @@
+// C-ABI entry points of the RANSAC estimators (Homography::estimate,
+// Homography::estimate_similarity, RansacOptions::validate).
+//
+// Reference: src/pipeline.rs:177-247 (options, seeds), :2038-2049, :2635-2661.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "psift_internal.cuh"
+
+namespace psift {
+
+struct RansacJob {
+  const psift_match* m;
+  int n;
+  float thr;
+  uint64_t sim_seed, hom_seed;
+  int homography;
+  const float* weights;
+  double* cdf;
+  double* err;
+  int* list;
+  int* draws;
+  int draw_cap;
+  uint8_t* mask;
+  float* model;
+  int* has_model;
+  int* count;
+  int* iters;
+};
+cudaError_t launch_ransac(const RansacJob* jobs, int n_jobs, cudaStream_t st);
+size_t ransac_job_bytes();
+
+namespace {
+constexpr uint64_t kSimSeed = 0xD1B54A32D192ED03ull;   // DEFAULT_SIMILARITY_RANSAC_SEED, src/pipeline.rs:172
+constexpr uint64_t kHomSeed = 0x517CC1B727220A95ull;   // DEFAULT_HOMOGRAPHY_RANSAC_SEED, src/pipeline.rs:174
+constexpr int kDrawCap = 2000 * 16;
+
+void seeds_for(const psift_ransac_options& o, bool homography, uint64_t& s1, uint64_t& s2) {
+  if (!o.has_seed) {
+    s1 = kSimSeed;
+    s2 = kHomSeed;
+  } else {
+    s1 = o.seed;
+    s2 = homography ? (o.seed ^ 0x9E3779B97F4A7C15ull) : 0;
+  }
+}
+
+psift_status run_batch(psift_ctx* ctx, const psift_ransac_job* jobs, int n, const psift_ransac_options& opt,
+                       bool homography) {
+  if (ransac_job_bytes() != sizeof(RansacJob)) return set_error(ctx, PSIFT_ERR_INTERNAL, "RansacJob layout mismatch");
+  size_t bytes = sizeof(RansacJob) * n + 4096;
+  for (int i = 0; i < n; ++i) {
+    const size_t m = jobs[i].n;
+    bytes += 8 * m + 8 * m + 4 * m + 4 * (size_t)kDrawCap + 4 * 256 + 4096;
+  }
+  psift_status st = arena_reserve(ctx, bytes);
+  if (st != PSIFT_OK) return st;
+  RansacJob* d_jobs = (RansacJob*)arena_alloc(ctx, sizeof(RansacJob) * n);
+  std::vector<RansacJob> hj(n);
+  uint64_t s1, s2;
+  seeds_for(opt, homography, s1, s2);
+  for (int i = 0; i < n; ++i) {
+    const psift_ransac_job& J = jobs[i];
+    RansacJob& R = hj[i];
+    std::memset(&R, 0, sizeof R);
+    const size_t m = J.n;
+    R.m = J.matches;
+    R.n = (int)J.n;
+    R.thr = opt.reproj_threshold;
+    R.sim_seed = s1;
+    R.hom_seed = s2;
+    R.homography = homography ? 1 : 0;
+    R.weights = J.sampling_weights;
+    R.cdf = (double*)arena_alloc(ctx, 8 * m + 8);
+    R.err = (double*)arena_alloc(ctx, 8 * m + 8);
+    R.list = (int*)arena_alloc(ctx, 4 * m + 4);
+    R.draws = (int*)arena_alloc(ctx, 4 * (size_t)kDrawCap);
+    R.draw_cap = kDrawCap;
+    R.mask = J.inlier_mask;
+    R.model = J.model;
+    R.has_model = J.has_model;
+    R.count = (int*)J.inlier_count;
+    R.iters = (int*)J.iterations;
+    if (!R.draws) return set_error(ctx, PSIFT_ERR_INTERNAL, "ransac workspace carve overflow");
+  }
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_jobs, hj.data(), sizeof(RansacJob) * n, cudaMemcpyHostToDevice, ctx->stream));
+  StageScope sc(ctx, STAGE_RANSAC);
+  cudaError_t e = launch_ransac(d_jobs, n, ctx->stream);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "ransac");
+  return PSIFT_OK;
+}
+
+psift_status estimate_host(psift_ctx* ctx, const psift_match* m, uint32_t n, const psift_ransac_options* opt,
+                           bool homography, uint8_t* mask, float* model, int32_t* has_model, uint32_t* count) {
+  if (!ctx || !opt || !count || !has_model || !model) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (n && (!m || !mask)) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null matches/mask");
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaSetDevice");
+  const size_t mb = sizeof(psift_match) * (size_t)n;
+  psift_status st = io_reserve(ctx, mb + n + 256 + 1024);
+  if (st != PSIFT_OK) return st;
+  char* base = ctx->io.base;
+  psift_match* d_m = (psift_match*)base;
+  uint8_t* d_mask = (uint8_t*)(base + align_up(mb, 256));
+  int* d_out = (int*)(base + align_up(mb, 256) + align_up(n + 1, 256));  // [0] count [1] has [2..3] iters [8..16] model
+  if (n) PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_m, m, mb, cudaMemcpyHostToDevice, ctx->stream));
+  psift_ransac_job job{d_m, n, d_mask, (float*)(d_out + 8), d_out + 1, (uint32_t*)d_out, nullptr, (uint32_t*)(d_out + 2)};
+  st = run_batch(ctx, &job, 1, *opt, homography);
+  if (st != PSIFT_OK) return st;
+  st = pinned_reserve(ctx, n + 256);
+  if (st != PSIFT_OK) return st;
+  char* pin = ctx->pinned.base;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(pin, d_out, 17 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (n) PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(pin + 128, d_mask, n, cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  const int* o = (const int*)pin;
+  *count = (uint32_t)o[0];
+  *has_model = o[1];
+  std::memcpy(model, o + 8, sizeof(float) * (homography ? 9 : 6));
+  if (n) std::memcpy(mask, pin + 128, n);
+  return PSIFT_OK;
+}
+
+}  // namespace
+}  // namespace psift
+
+using namespace psift;
+
+extern "C" {
+
+void psift_ransac_options_default(psift_ransac_options* o) {
+  if (!o) return;
+  o->reproj_threshold = 3.0f;  // DEFAULT_RANSAC_REPROJ_THRESHOLD, src/pipeline.rs:1050
+  o->has_seed = 0;
+  o->seed = 0;
+}
+
+// RansacOptions::validate (src/pipeline.rs:209-217).
+psift_status psift_ransac_options_validate(const psift_ransac_options* o, char* msg, size_t cap) {
+  char buf[160] = {0};
+  psift_status st = PSIFT_OK;
+  if (!o) {
+    snprintf(buf, sizeof buf, "null options");
+    st = PSIFT_ERR_INVALID_ARGUMENT;
+  } else if (!(o->reproj_threshold == o->reproj_threshold) || o->reproj_threshold > 3.4e38f ||
+             o->reproj_threshold < -3.4e38f || o->reproj_threshold < 0.5f || o->reproj_threshold > 100.0f) {
+    snprintf(buf, sizeof buf, "Invalid `reproj_threshold`=%g: must be between 0.5 and 100.0",
+             (double)o->reproj_threshold);
+    st = PSIFT_ERR_INVALID_CONFIG;
+  }
+  if (msg && cap) {
+    strncpy(msg, buf, cap - 1);
+    msg[cap - 1] = 0;
+  }
+  return st;
+}
+
+psift_status psift_homography_estimate(psift_ctx* ctx, const psift_match* matches, uint32_t n,
+                                       const psift_ransac_options* opt, uint8_t* inlier_mask, float* h9,
+                                       int32_t* has_h, uint32_t* inlier_count) {
+  return estimate_host(ctx, matches, n, opt, true, inlier_mask, h9, has_h, inlier_count);
+}
+
+psift_status psift_similarity_estimate(psift_ctx* ctx, const psift_match* matches, uint32_t n,
+                                       const psift_ransac_options* opt, uint8_t* inlier_mask, float* model6,
+                                       int32_t* has_model, uint32_t* inlier_count) {
+  return estimate_host(ctx, matches, n, opt, false, inlier_mask, model6, has_model, inlier_count);
+}
+
+psift_status psift_ransac_batch_dev(psift_ctx* ctx, const psift_ransac_job* jobs, uint32_t n,
+                                    const psift_ransac_options* opt, int32_t homography) {
+  if (!ctx || !opt || (n && !jobs)) return PSIFT_ERR_INVALID_ARGUMENT;
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaSetDevice");
+  for (uint32_t i = 0; i < n; ++i)
+    if (!jobs[i].model || !jobs[i].has_model || !jobs[i].inlier_count || (jobs[i].n && (!jobs[i].matches || !jobs[i].inlier_mask)))
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null pointer in ransac job");
+  if (n == 0) return PSIFT_OK;
+  return run_batch(ctx, jobs, (int)n, *opt, homography != 0);
+}
+
+}  // extern "C"

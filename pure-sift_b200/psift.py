@@ -86,6 +86,16 @@ MATCH_DTYPE = np.dtype([("query_index", "<u4"), ("target_index", "<u4"), ("query
 PRECISION_FP32 = 0
 PRECISION_BF16_RERANK = 1
 
+class CRansacOptions(C.Structure):
+    _fields_ = [("reproj_threshold", C.c_float), ("has_seed", C.c_int32), ("seed", C.c_uint64)]
+
+
+class CRansacJob(C.Structure):
+    _fields_ = [("matches", C.c_void_p), ("n", C.c_uint32), ("inlier_mask", C.c_void_p), ("model", C.c_void_p),
+                ("has_model", C.c_void_p), ("inlier_count", C.c_void_p), ("sampling_weights", C.c_void_p),
+                ("iterations", C.c_void_p)]
+
+
 KEYPOINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("scale", "<f4"), ("response", "<f4"),
                            ("octave", "<u4"), ("layer", "<u4")])
 
@@ -116,6 +126,14 @@ _SIGS = {
                                           C.POINTER(C.c_uint32)]),
     "psift_match_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CMatchJob), C.c_uint32, C.POINTER(CMatchOptions)]),
     "psift_ctx_rerank_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "psift_ransac_options_default": (None, [C.POINTER(CRansacOptions)]),
+    "psift_ransac_options_validate": (C.c_int, [C.POINTER(CRansacOptions), C.c_char_p, C.c_size_t]),
+    "psift_homography_estimate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CRansacOptions),
+                                            C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint32)]),
+    "psift_similarity_estimate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CRansacOptions),
+                                            C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint32)]),
+    "psift_ransac_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CRansacJob), C.c_uint32, C.POINTER(CRansacOptions),
+                                         C.c_int32]),
     "psift_quantize_u128": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "psift_quantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "psift_dequantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
@@ -459,3 +477,75 @@ def l2_rerank(query_desc, catalog_desc, candidates, ctx: Context | None = None):
     ctx.check(ctx.lib.psift_l2_rerank(ctx.handle, qd.ctypes.data, qd.shape[0], cd.ctypes.data, cd.shape[0],
                                       cand.ctypes.data, k, idx.ctypes.data, d2.ctypes.data))
     return idx, d2
+
+
+# ---------------------------------------------------------------- RANSAC
+@dataclass(frozen=True)
+class RansacOptions:
+    """``RansacOptions`` (src/pipeline.rs:177-218)."""
+    reproj_threshold: float = DEFAULT_RANSAC_REPROJ_THRESHOLD
+    seed: int | None = None
+
+    def to_c(self) -> CRansacOptions:
+        return CRansacOptions(self.reproj_threshold, 0 if self.seed is None else 1,
+                              0 if self.seed is None else (self.seed & 0xFFFFFFFFFFFFFFFF))
+
+    def validate(self):
+        lib = load_library()
+        buf = C.create_string_buffer(256)
+        c = self.to_c()
+        if lib.psift_ransac_options_validate(C.byref(c), buf, 256) != PSIFT_OK:
+            raise ValueError(buf.value.decode())
+
+
+def _as_matches(matches) -> np.ndarray:
+    m = np.asarray(matches)
+    if m.dtype != MATCH_DTYPE:
+        m = m.astype(MATCH_DTYPE) if m.dtype.names is None else np.array(
+            [tuple(r) for r in m], dtype=MATCH_DTYPE)
+    return np.ascontiguousarray(m)
+
+
+class Homography:
+    """``Homography`` (src/pipeline.rs:220-247): returns (inlier matches, model or None)."""
+
+    @staticmethod
+    def estimate(matches, options: RansacOptions = RansacOptions(), ctx: Context | None = None):
+        ctx = ctx or default_context()
+        m = _as_matches(matches)
+        n = len(m)
+        mask = np.zeros(max(n, 1), np.uint8)
+        h9 = np.zeros(9, np.float32)
+        has = C.c_int32()
+        cnt = C.c_uint32()
+        c = options.to_c()
+        ctx.check(ctx.lib.psift_homography_estimate(ctx.handle, m.ctypes.data, n, C.byref(c), mask.ctypes.data,
+                                                    h9.ctypes.data, C.byref(has), C.byref(cnt)))
+        sel = mask[:n].astype(bool)
+        return m[sel], (h9.reshape(3, 3) if has.value else None)
+
+    @staticmethod
+    def estimate_similarity(matches, options: RansacOptions = RansacOptions(), ctx: Context | None = None):
+        """Returns (inlier matches, (a, b, tx, ty, scale, rotation_deg) or None)."""
+        ctx = ctx or default_context()
+        m = _as_matches(matches)
+        n = len(m)
+        mask = np.zeros(max(n, 1), np.uint8)
+        m6 = np.zeros(9, np.float32)
+        has = C.c_int32()
+        cnt = C.c_uint32()
+        c = options.to_c()
+        ctx.check(ctx.lib.psift_similarity_estimate(ctx.handle, m.ctypes.data, n, C.byref(c), mask.ctypes.data,
+                                                    m6.ctypes.data, C.byref(has), C.byref(cnt)))
+        sel = mask[:n].astype(bool)
+        return m[sel], (m6[:6].copy() if has.value else None)
+
+
+def estimate_homography_ransac(matches, reproj_threshold: float, ctx: Context | None = None):
+    """``estimate_homography_ransac`` (src/pipeline.rs:2635-2646)."""
+    return Homography.estimate(matches, RansacOptions(reproj_threshold), ctx)
+
+
+def filter_matches_ransac(matches, reproj_threshold: float, ctx: Context | None = None):
+    """``filter_matches_ransac`` (src/pipeline.rs:2038-2044)."""
+    return Homography.estimate_similarity(matches, RansacOptions(reproj_threshold), ctx)
