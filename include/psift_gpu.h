@@ -217,6 +217,36 @@ typedef struct psift_ransac_job {
 psift_status psift_ransac_batch_dev(psift_ctx* ctx, const psift_ransac_job* jobs, uint32_t n,
                                     const psift_ransac_options* opt, int32_t homography);
 
+/* ---------------------------------------------------------------- learned sampler */
+/* A small MLP (8 -> 64 -> 64 -> 1, ReLU, ReLU, sigmoid; bf16 operands, f32
+ * accumulation, f32 master weights) scoring each putative match's inlier
+ * probability.  No counterpart in the reference.  Its output, passed as
+ * psift_ransac_job.sampling_weights, drives guided RANSAC sampling.
+ * Parameter layout: W1[64][8], b1[64], W2[64][64], b2[64], W3[64], b3.
+ * Features (8 per match): ratio, log scale ratio, orientation difference,
+ * best distance, query x / width, query y / height, target x / width,
+ * target y / height. */
+#define PSIFT_MLP_NUM_PARAMS 4801u
+#define PSIFT_MLP_NUM_FEATURES 8u
+void psift_mlp_init(uint64_t seed, float* params);
+psift_status psift_mlp_infer(psift_ctx* ctx, const float* params, const float* features, uint32_t n,
+                             float* prob);
+psift_status psift_mlp_infer_dev(psift_ctx* ctx, const float* params, const float* features, uint32_t n,
+                                 float* prob);
+/* Gradients of the mean binary cross-entropy over n samples (labels 0/1). */
+psift_status psift_mlp_gradients(psift_ctx* ctx, const float* params, const float* features,
+                                 const float* labels, uint32_t n, float* grad, float* loss);
+psift_status psift_mlp_gradients_dev(psift_ctx* ctx, const float* params, const float* features,
+                                     const float* labels, uint32_t n, float* grad, float* loss);
+/* Adam (beta 0.9/0.999, eps 1e-8) over seeded-shuffled minibatches; params in/out;
+ * losses (optional, `steps` floats) receives each step's minibatch loss. */
+psift_status psift_mlp_train(psift_ctx* ctx, float* params, const float* features, const float* labels,
+                             uint32_t n, uint32_t steps, uint32_t batch, float lr, uint64_t seed,
+                             float* losses);
+psift_status psift_mlp_train_dev(psift_ctx* ctx, float* params, const float* features,
+                                 const float* labels, uint32_t n, uint32_t steps, uint32_t batch,
+                                 float lr, uint64_t seed, float* losses);
+
 /* ---------------------------------------------------------------- catalog */
 /* quantize_descriptor_u128 (src/catalog.rs:37-45): bit i set iff desc[i] > 0.065.
  * codes: 2 x u64 per descriptor, little endian (word 0 = bits 0..63). */

@@ -1,0 +1,221 @@
+// K11: the learned correspondence scorer that drives guided RANSAC sampling.
+// No counterpart in the reference (its sampler weights matches by 1/ratio,
+// src/pipeline.rs:2006-2036).
+//
+// Network 8 -> 64 -> 64 -> 1, ReLU, ReLU, sigmoid.  Parameters are f32 masters;
+// the forward pass rounds weights and activations to bf16 (round to nearest even)
+// and accumulates in f32.  The backward pass is f32 on the same bf16-rounded
+// operands (straight-through rounding).  Training is deterministic:
+//   mlp_fwd_bwd_kernel   one thread per sample: forward, dL/dz for every layer;
+//   mlp_grad_kernel      one thread per parameter: the batch sum in sample order;
+//   mlp_adam_kernel      Adam update of the f32 masters.
+// Loss: mean binary cross-entropy over the minibatch.
+#include <algorithm>
+
+#include "psift_internal.cuh"
+
+namespace psift {
+
+constexpr int kF = 8, kH = 64;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kH * kF, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH,
+              kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kH, kNP = kOffB3 + 1;  // 4801
+
+__device__ __forceinline__ float bf16r(float x) {
+  const uint32_t u = __float_as_uint(x);
+  if ((u & 0x7f800000u) == 0x7f800000u) return x;  // inf / nan unchanged
+  const uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
+  return __uint_as_float(r & 0xFFFF0000u);
+}
+
+struct MlpSmem {
+  float w1[kH][kF];
+  float b1[kH];
+  float w2[kH][kH];
+  float b2[kH];
+  float w3[kH];
+  float b3;
+};
+
+__device__ void load_params(const float* __restrict__ p, MlpSmem& s) {
+  for (int i = threadIdx.x; i < kH * kF; i += blockDim.x) (&s.w1[0][0])[i] = bf16r(p[kOffW1 + i]);
+  for (int i = threadIdx.x; i < kH * kH; i += blockDim.x) (&s.w2[0][0])[i] = bf16r(p[kOffW2 + i]);
+  for (int i = threadIdx.x; i < kH; i += blockDim.x) {
+    s.b1[i] = p[kOffB1 + i];
+    s.b2[i] = p[kOffB2 + i];
+    s.w3[i] = bf16r(p[kOffW3 + i]);
+  }
+  if (threadIdx.x == 0) s.b3 = p[kOffB3];
+  __syncthreads();
+}
+
+// Forward of one sample; returns z3 and fills xb, h1b (and z1 signs) on request.
+__device__ __forceinline__ float forward1(const MlpSmem& s, const float* __restrict__ x, float (&xb)[kF],
+                                          float (&h1b)[kH], float* h2b_out, uint64_t* z1pos, uint64_t* z2pos) {
+#pragma unroll
+  for (int k = 0; k < kF; ++k) xb[k] = bf16r(x[k]);
+  uint64_t p1 = 0;
+#pragma unroll
+  for (int j = 0; j < kH; ++j) {
+    float z = s.b1[j];
+#pragma unroll
+    for (int k = 0; k < kF; ++k) z = __fmaf_rn(s.w1[j][k], xb[k], z);
+    p1 |= (z > 0.0f ? 1ull : 0ull) << j;
+    h1b[j] = bf16r(z > 0.0f ? z : 0.0f);
+  }
+  float z3 = s.b3;
+  uint64_t p2 = 0;
+#pragma unroll 4
+  for (int j = 0; j < kH; ++j) {
+    float z = s.b2[j];
+#pragma unroll
+    for (int k = 0; k < kH; ++k) z = __fmaf_rn(s.w2[j][k], h1b[k], z);
+    p2 |= (z > 0.0f ? 1ull : 0ull) << j;
+    const float h2 = bf16r(z > 0.0f ? z : 0.0f);
+    if (h2b_out) h2b_out[j] = h2;
+    z3 = __fmaf_rn(s.w3[j], h2, z3);
+  }
+  if (z1pos) *z1pos = p1;
+  if (z2pos) *z2pos = p2;
+  return z3;
+}
+
+__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + expf(-z)); }
+
+__global__ void __launch_bounds__(256) mlp_infer_kernel(const float* __restrict__ params, const float* __restrict__ X,
+                                                        int n, float* __restrict__ prob) {
+  __shared__ MlpSmem s;
+  load_params(params, s);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float xb[kF], h1b[kH];
+    const float z3 = forward1(s, X + (size_t)i * kF, xb, h1b, nullptr, nullptr, nullptr);
+    prob[i] = sigmoidf_(z3);
+  }
+}
+
+// One thread per minibatch sample b (sample index idx[b]).  Stores the operands
+// and deltas the per-parameter gradient sums need.
+__global__ void __launch_bounds__(128) mlp_fwd_bwd_kernel(const float* __restrict__ params,
+                                                          const float* __restrict__ X, const float* __restrict__ Y,
+                                                          const int* __restrict__ idx, int B, float* __restrict__ xb_o,
+                                                          float* __restrict__ h1b_o, float* __restrict__ h2b_o,
+                                                          float* __restrict__ dz1_o, float* __restrict__ dz2_o,
+                                                          float* __restrict__ dz3_o, float* __restrict__ loss_o) {
+  __shared__ MlpSmem s;
+  load_params(params, s);
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const int i = idx ? idx[b] : b;
+  float xb[kF], h1b[kH], h2b[kH];
+  uint64_t p1, p2;
+  const float z3 = forward1(s, X + (size_t)i * kF, xb, h1b, h2b, &p1, &p2);
+  const float p = sigmoidf_(z3);
+  const float y = Y[i];
+  // BCE with logits: softplus(z) - y z, numerically stable form
+  const float l = fmaxf(z3, 0.0f) - z3 * y + log1pf(expf(-fabsf(z3)));
+  const float invB = 1.0f / (float)B;
+  const float dz3 = (p - y) * invB;
+  float dz2[kH];
+#pragma unroll
+  for (int j = 0; j < kH; ++j) dz2[j] = ((p2 >> j) & 1ull) ? dz3 * s.w3[j] : 0.0f;
+#pragma unroll 4
+  for (int k = 0; k < kH; ++k) {
+    float dh = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kH; ++j) dh = __fmaf_rn(s.w2[j][k], dz2[j], dh);
+    dz1_o[(size_t)b * kH + k] = ((p1 >> k) & 1ull) ? dh : 0.0f;
+  }
+#pragma unroll
+  for (int j = 0; j < kH; ++j) {
+    h1b_o[(size_t)b * kH + j] = h1b[j];
+    h2b_o[(size_t)b * kH + j] = h2b[j];
+    dz2_o[(size_t)b * kH + j] = dz2[j];
+  }
+#pragma unroll
+  for (int k = 0; k < kF; ++k) xb_o[(size_t)b * kF + k] = xb[k];
+  dz3_o[b] = dz3;
+  loss_o[b] = l;
+}
+
+// One thread per parameter: sum over the batch in sample order.
+__global__ void mlp_grad_kernel(int B, const float* __restrict__ xb, const float* __restrict__ h1b,
+                                const float* __restrict__ h2b, const float* __restrict__ dz1,
+                                const float* __restrict__ dz2, const float* __restrict__ dz3,
+                                float* __restrict__ grad) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kNP) return;
+  float g = 0.0f;
+  if (p < kOffB1) {
+    const int j = (p - kOffW1) / kF, k = (p - kOffW1) % kF;
+    for (int b = 0; b < B; ++b) g = __fmaf_rn(dz1[(size_t)b * kH + j], xb[(size_t)b * kF + k], g);
+  } else if (p < kOffW2) {
+    const int j = p - kOffB1;
+    for (int b = 0; b < B; ++b) g += dz1[(size_t)b * kH + j];
+  } else if (p < kOffB2) {
+    const int j = (p - kOffW2) / kH, k = (p - kOffW2) % kH;
+    for (int b = 0; b < B; ++b) g = __fmaf_rn(dz2[(size_t)b * kH + j], h1b[(size_t)b * kH + k], g);
+  } else if (p < kOffW3) {
+    const int j = p - kOffB2;
+    for (int b = 0; b < B; ++b) g += dz2[(size_t)b * kH + j];
+  } else if (p < kOffB3) {
+    const int j = p - kOffW3;
+    for (int b = 0; b < B; ++b) g = __fmaf_rn(dz3[b], h2b[(size_t)b * kH + j], g);
+  } else {
+    for (int b = 0; b < B; ++b) g += dz3[b];
+  }
+  grad[p] = g;
+}
+
+__global__ void mlp_adam_kernel(float* __restrict__ params, const float* __restrict__ grad, float* __restrict__ m,
+                                float* __restrict__ v, float lr, float beta1, float beta2, float eps, float bc1,
+                                float bc2) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kNP) return;
+  const float g = grad[p];
+  const float mm = beta1 * m[p] + (1.0f - beta1) * g;
+  const float vv = beta2 * v[p] + (1.0f - beta2) * g * g;
+  m[p] = mm;
+  v[p] = vv;
+  params[p] -= lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
+}
+
+// Sequential sum of the per-sample losses (deterministic) into loss[step].
+__global__ void mlp_loss_kernel(const float* __restrict__ l, int B, float* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    float s = 0.0f;
+    for (int b = 0; b < B; ++b) s += l[b];
+    *out = s / (float)B;
+  }
+}
+
+cudaError_t launch_mlp_infer(const float* params, const float* X, int n, float* prob, int num_sms, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = std::min((n + 255) / 256, num_sms * 8);
+  mlp_infer_kernel<<<blocks, 256, 0, st>>>(params, X, n, prob);
+  return cudaGetLastError();
+}
+
+// Workspace for a minibatch of B: (8 + 64*4 + 2) * B floats.
+size_t mlp_batch_floats(int B) { return (size_t)B * (kF + 4 * kH + 2); }
+
+cudaError_t launch_mlp_step(float* params, const float* X, const float* Y, const int* idx, int B, float* work,
+                            float* grad, float* m, float* v, float lr, int t, float* loss_out, bool update,
+                            cudaStream_t st) {
+  float* xb = work;
+  float* h1b = xb + (size_t)B * kF;
+  float* h2b = h1b + (size_t)B * kH;
+  float* dz1 = h2b + (size_t)B * kH;
+  float* dz2 = dz1 + (size_t)B * kH;
+  float* dz3 = dz2 + (size_t)B * kH;
+  float* lb = dz3 + B;
+  mlp_fwd_bwd_kernel<<<(B + 127) / 128, 128, 0, st>>>(params, X, Y, idx, B, xb, h1b, h2b, dz1, dz2, dz3, lb);
+  mlp_grad_kernel<<<(kNP + 127) / 128, 128, 0, st>>>(B, xb, h1b, h2b, dz1, dz2, dz3, grad);
+  if (loss_out) mlp_loss_kernel<<<1, 32, 0, st>>>(lb, B, loss_out);
+  if (update) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.0f - powf(b1, (float)t), bc2 = 1.0f - powf(b2, (float)t);
+    mlp_adam_kernel<<<(kNP + 255) / 256, 256, 0, st>>>(params, grad, m, v, lr, b1, b2, 1e-8f, bc1, bc2);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace psift

@@ -178,6 +178,38 @@ __device__ __forceinline__ int block_sum_int(int v, RShared& S) {
   return t;
 }
 
+__device__ __forceinline__ double block_sum_double(double v, RShared& S) {
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) S.red_d[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < kRThreads / 32; ++w) t += S.red_d[w];
+  __syncthreads();
+  return t;
+}
+
+// Guided sampling stops on the sampled inlier mass: the probability that one
+// draw hits an inlier of the current model is w = sum over its inliers of the
+// sampling weight / total weight (the reference's count / n when the weights are
+// uniform).  Same formula as adaptive_ransac_iters otherwise.
+__device__ int adaptive_iters_w(double w, int ss, int min_it, int cap) {
+  if (!(w > 0.0)) return cap;
+  w = w < 1e-3 ? 1e-3 : (w > 1.0 - 1e-6 ? 1.0 - 1e-6 : w);
+  double p = w * w;
+  if (ss == 4) p = p * p;
+  p = p < 1e-12 ? 1e-12 : (p > 1.0 - 1e-9 ? 1.0 - 1e-9 : p);
+  const double num = log(1.0 - 0.999);
+  const double den = log(1.0 - p);
+  if (fabs(den) < 1e-12) return min_it;
+  const double est = ceil(num / den);
+  if (!isfinite(est)) return cap;
+  double c = est;
+  if (c < (double)min_it) c = (double)min_it;
+  if (c > (double)cap) c = (double)cap;
+  return (int)c;
+}
+
 // ------------------------------------------------------------- similarity
 __device__ __forceinline__ bool sim_inlier(const psift_match& m, float a, float b, float tx, float ty, float tsq,
                                            float& e) {
@@ -197,6 +229,21 @@ __device__ int sim_count(const RansacJob& J, RShared& S, float a, float b, float
     c += sim_inlier(J.m[i], a, b, tx, ty, S.tsq_f, e) ? 1 : 0;
   }
   return block_sum_int(c, S);
+}
+
+__device__ double weight_total(const RansacJob& J, RShared& S) {
+  double t = 0.0;
+  for (int i = threadIdx.x; i < S.n; i += kRThreads) t += (double)J.weights[i];
+  return block_sum_double(t, S);
+}
+
+__device__ double sim_mass(const RansacJob& J, RShared& S, float a, float b, float tx, float ty) {
+  double t = 0.0;
+  for (int i = threadIdx.x; i < S.n; i += kRThreads) {
+    float e;
+    if (sim_inlier(J.m[i], a, b, tx, ty, S.tsq_f, e)) t += (double)J.weights[i];
+  }
+  return block_sum_double(t, S);
 }
 
 // Sequential f32 error sum over inliers in input order (whole CTA; result broadcast).
@@ -409,9 +456,14 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
   }
   // Phase B: adaptive 2-point hypotheses
   build_cdf(J, S);
-  if (threadIdx.x == 0) {
-    S.max_iters = adaptive_iters(S.best_count, n, 2, 64, 1000);
-    S.stop = 0;
+  const bool guided = J.weights != nullptr;
+  const double wtot = guided ? weight_total(J, S) : 1.0;
+  {
+    const double mass = guided ? sim_mass(J, S, S.ba, S.bb, S.btx, S.bty) : 0.0;
+    if (threadIdx.x == 0) {
+      S.max_iters = guided ? adaptive_iters_w(mass / wtot, 2, 64, 1000) : adaptive_iters(S.best_count, n, 2, 64, 1000);
+      S.stop = 0;
+    }
   }
   __syncthreads();
   int iters_done = 0;
@@ -467,14 +519,19 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
       const int c = S.hcnt[h];
       if (c < S.best_count) continue;
       const float e = sim_err(J, S, S.ha[h], S.hb[h], S.htx[h], S.hty[h]);
-      if (threadIdx.x == 0 && (c > S.best_count || e < S.best_err_f)) {
-        S.best_count = c;
-        S.best_err_f = e;
-        S.ba = S.ha[h];
-        S.bb = S.hb[h];
-        S.btx = S.htx[h];
-        S.bty = S.hty[h];
-        S.max_iters = adaptive_iters(c, n, 2, 64, 1000);
+      const bool improved = c > S.best_count || e < S.best_err_f;
+      __syncthreads();
+      if (improved) {
+        const double mass = guided ? sim_mass(J, S, S.ha[h], S.hb[h], S.htx[h], S.hty[h]) : 0.0;
+        if (threadIdx.x == 0) {
+          S.best_count = c;
+          S.best_err_f = e;
+          S.ba = S.ha[h];
+          S.bb = S.hb[h];
+          S.btx = S.htx[h];
+          S.bty = S.hty[h];
+          S.max_iters = guided ? adaptive_iters_w(mass / wtot, 2, 64, 1000) : adaptive_iters(c, n, 2, 64, 1000);
+        }
       }
       __syncthreads();
     }
@@ -533,6 +590,15 @@ __device__ int h_count(const RansacJob& J, RShared& S, const double* H) {
     c += h_inlier(J.m[i], H, S.tsq_d, e) ? 1 : 0;
   }
   return block_sum_int(c, S);
+}
+
+__device__ double h_mass(const RansacJob& J, RShared& S, const double* H) {
+  double t = 0.0;
+  for (int i = threadIdx.x; i < S.n; i += kRThreads) {
+    double e;
+    if (h_inlier(J.m[i], H, S.tsq_d, e)) t += (double)J.weights[i];
+  }
+  return block_sum_double(t, S);
 }
 
 __device__ double h_err(const RansacJob& J, RShared& S, const double* H) {
@@ -871,11 +937,16 @@ __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __re
   // keep the similarity inliers for the no-model exit: they are in J.list only until
   // the first collection below, so record the flag now
   build_cdf(J, S);
-  if (threadIdx.x == 0) {
-    S.max_iters = adaptive_iters(best_count, n, 4, 64, 2000);
-    S.stop = 0;
-    S.draw_ptr = 0;
-    S.draws_ready = 0;
+  const bool guided = J.weights != nullptr;
+  const double wtot = guided ? weight_total(J, S) : 1.0;
+  {
+    const double mass = (guided && S.has_bh) ? h_mass(J, S, BH) : 0.0;
+    if (threadIdx.x == 0) {
+      S.max_iters = guided ? adaptive_iters_w(mass / wtot, 4, 64, 2000) : adaptive_iters(best_count, n, 4, 64, 2000);
+      S.stop = 0;
+      S.draw_ptr = 0;
+      S.draws_ready = 0;
+    }
   }
   __syncthreads();
   const uint64_t seed = J.hom_seed;
@@ -967,9 +1038,10 @@ __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __re
         best_count = c;
         best_err = e;
         for (int i = 0; i < 9; ++i) BH[i] = Hc[i];
+        const double mass = guided ? h_mass(J, S, BH) : 0.0;
         if (threadIdx.x == 0) {
           S.has_bh = 1;
-          S.max_iters = adaptive_iters(best_count, n, 4, 64, 2000);
+          S.max_iters = guided ? adaptive_iters_w(mass / wtot, 4, 64, 2000) : adaptive_iters(best_count, n, 4, 64, 2000);
         }
       }
       __syncthreads();

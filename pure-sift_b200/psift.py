@@ -134,6 +134,17 @@ _SIGS = {
                                             C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint32)]),
     "psift_ransac_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CRansacJob), C.c_uint32, C.POINTER(CRansacOptions),
                                          C.c_int32]),
+    "psift_mlp_init": (None, [C.c_uint64, C.c_void_p]),
+    "psift_mlp_infer": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "psift_mlp_infer_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "psift_mlp_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                      C.c_void_p]),
+    "psift_mlp_gradients_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                          C.c_void_p]),
+    "psift_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                  C.c_uint32, C.c_float, C.c_uint64, C.c_void_p]),
+    "psift_mlp_train_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                      C.c_uint32, C.c_float, C.c_uint64, C.c_void_p]),
     "psift_quantize_u128": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "psift_quantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "psift_dequantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
@@ -549,3 +560,79 @@ def estimate_homography_ransac(matches, reproj_threshold: float, ctx: Context | 
 def filter_matches_ransac(matches, reproj_threshold: float, ctx: Context | None = None):
     """``filter_matches_ransac`` (src/pipeline.rs:2038-2044)."""
     return Homography.estimate_similarity(matches, RansacOptions(reproj_threshold), ctx)
+
+
+# ---------------------------------------------------------------- learned sampler
+MLP_NUM_PARAMS = 4801
+MLP_NUM_FEATURES = 8
+
+
+class InlierMLP:
+    """The learned correspondence scorer (8-64-64-1, bf16 operands, f32 accumulation)."""
+
+    def __init__(self, params: np.ndarray | None = None, seed: int = 0):
+        if params is None:
+            params = np.zeros(MLP_NUM_PARAMS, np.float32)
+            load_library().psift_mlp_init(seed, params.ctypes.data)
+        self.params = np.ascontiguousarray(params, dtype=np.float32).copy()
+
+    def predict(self, features, ctx: Context | None = None) -> np.ndarray:
+        ctx = ctx or default_context()
+        x = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, MLP_NUM_FEATURES)
+        out = np.zeros(x.shape[0], np.float32)
+        ctx.check(ctx.lib.psift_mlp_infer(ctx.handle, self.params.ctypes.data, x.ctypes.data, x.shape[0],
+                                          out.ctypes.data))
+        return out
+
+    def gradients(self, features, labels, ctx: Context | None = None):
+        ctx = ctx or default_context()
+        x = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, MLP_NUM_FEATURES)
+        y = np.ascontiguousarray(labels, dtype=np.float32)
+        g = np.zeros(MLP_NUM_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        ctx.check(ctx.lib.psift_mlp_gradients(ctx.handle, self.params.ctypes.data, x.ctypes.data, y.ctypes.data,
+                                              x.shape[0], g.ctypes.data, loss.ctypes.data))
+        return float(loss[0]), g
+
+    def train(self, features, labels, steps=300, batch=4096, lr=3e-3, seed=1, ctx: Context | None = None):
+        ctx = ctx or default_context()
+        x = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, MLP_NUM_FEATURES)
+        y = np.ascontiguousarray(labels, dtype=np.float32)
+        losses = np.zeros(steps, np.float32)
+        ctx.check(ctx.lib.psift_mlp_train(ctx.handle, self.params.ctypes.data, x.ctypes.data, y.ctypes.data,
+                                          x.shape[0], steps, batch, lr, seed, losses.ctypes.data))
+        return losses
+
+
+def ransac_batch(match_sets, options: RansacOptions = RansacOptions(), homography: bool = True,
+                 weights=None, ctx: Context | None = None):
+    """Runs many estimations in one launch (device-resident); returns
+    [(inlier mask, model or None, (similarity iters, homography iters))]."""
+    import torch
+    ctx = ctx or default_context()
+    dev = []
+    jobs = (CRansacJob * len(match_sets))()
+    for i, m in enumerate(match_sets):
+        m = _as_matches(m)
+        n = len(m)
+        d_m = torch.from_numpy(m.view(np.uint8).copy()).cuda() if n else torch.zeros(40, dtype=torch.uint8,
+                                                                                       device="cuda")
+        mask = torch.zeros(max(n, 1), dtype=torch.uint8, device="cuda")
+        out = torch.zeros(16, dtype=torch.int32, device="cuda")
+        w = None
+        if weights is not None:
+            w = torch.from_numpy(np.ascontiguousarray(weights[i], dtype=np.float32)).cuda()
+        dev.append((d_m, mask, out, w, n))
+        # out (int32): [0] inlier count, [1] has model, [2] similarity iterations,
+        # [3] homography iterations, [4..13) model floats
+        jobs[i] = CRansacJob(d_m.data_ptr(), n, mask.data_ptr(), out.data_ptr() + 16, out.data_ptr() + 4,
+                             out.data_ptr(), w.data_ptr() if w is not None else None, out.data_ptr() + 8)
+    c = options.to_c()
+    ctx.check(ctx.lib.psift_ransac_batch_dev(ctx.handle, jobs, len(match_sets), C.byref(c), int(homography)))
+    ctx.synchronize()
+    res = []
+    for d_m, mask, out, w, n in dev:
+        o = out.cpu().numpy()
+        model = o[4:4 + (9 if homography else 6)].view(np.float32).copy()
+        res.append((mask[:n].cpu().numpy().astype(bool), model if o[1] else None, (int(o[2]), int(o[3]))))
+    return res

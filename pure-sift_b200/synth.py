@@ -196,3 +196,61 @@ def correspondences(n: int, outlier_ratio: float, H: np.ndarray, width: int, hei
     ru = rng.uniform(n)
     ratio = np.where(inl, 0.2 + 0.6 * ru, 0.5 + 0.5 * ru)
     return q.astype(np.float32), t.astype(np.float32), ratio.astype(np.float32), inl
+
+
+def putative_matches(n: int, outlier_ratio: float, H: np.ndarray, width: int, height: int, seed: int):
+    """Putative matches with per-match attributes for the learned sampler.
+
+    Inliers: target = H p + N(0, 0.5 px); log scale ratio = log of H's local scale
+    + N(0, 0.08); orientation difference = H's local rotation + N(0, 0.08) rad;
+    best descriptor distance U(0.10, 0.40); Lowe ratio U(0.2, 0.8).
+    Outliers: uniform target; log scale ratio N(0, 0.7); orientation difference
+    U(-pi, pi); best distance U(0.25, 0.60); ratio U(0.5, 1.0).
+    Returns (records with fields query_index, target_index, query_x, query_y,
+    target_x, target_y, distance, ratio, displacement_x, displacement_y;
+    features (n, 8) float32; is_inlier (n,) bool).
+    """
+    rng = SplitMix64(seed)
+    q = rng.uniform(2 * n).reshape(n, 2) * np.array([width, height])
+    inl = rng.uniform(n) >= outlier_ratio
+    ph = np.c_[q, np.ones(n)] @ H.T
+    t_in = ph[:, :2] / ph[:, 2:3] + 0.5 * rng.normal(2 * n).reshape(n, 2)
+    t_out = rng.uniform(2 * n).reshape(n, 2) * np.array([width, height])
+    t = np.where(inl[:, None], t_in, t_out)
+    # local similarity of H at q (finite differences)
+    eps = 1.0
+    px = np.c_[q[:, 0] + eps, q[:, 1], np.ones(n)] @ H.T
+    px = px[:, :2] / px[:, 2:3]
+    jac = (px - ph[:, :2] / ph[:, 2:3]) / eps
+    loc_scale = np.log(np.maximum(np.hypot(jac[:, 0], jac[:, 1]), 1e-6))
+    loc_rot = np.arctan2(jac[:, 1], jac[:, 0])
+    g = rng.normal(2 * n).reshape(n, 2)
+    u = rng.uniform(4 * n).reshape(n, 4)
+    lsr = np.where(inl, loc_scale + 0.08 * g[:, 0], 0.7 * g[:, 1])
+    dori = np.where(inl, loc_rot + 0.08 * g[:, 1], -np.pi + 2 * np.pi * u[:, 0])
+    dori = (dori + np.pi) % (2 * np.pi) - np.pi
+    dist = np.where(inl, 0.10 + 0.30 * u[:, 1], 0.25 + 0.35 * u[:, 2])
+    ratio = np.where(inl, 0.2 + 0.6 * u[:, 3], 0.5 + 0.5 * u[:, 3])
+    rec = np.zeros(n, dtype=[("query_index", "<u4"), ("target_index", "<u4"), ("query_x", "<f4"),
+                             ("query_y", "<f4"), ("target_x", "<f4"), ("target_y", "<f4"), ("distance", "<f4"),
+                             ("ratio", "<f4"), ("displacement_x", "<f4"), ("displacement_y", "<f4")])
+    rec["query_index"] = np.arange(n)
+    rec["target_index"] = np.arange(n)
+    rec["query_x"], rec["query_y"] = q[:, 0], q[:, 1]
+    rec["target_x"], rec["target_y"] = t[:, 0], t[:, 1]
+    rec["distance"] = dist
+    rec["ratio"] = ratio
+    rec["displacement_x"] = rec["target_x"] - rec["query_x"]
+    rec["displacement_y"] = rec["target_y"] - rec["query_y"]
+    feats = np.stack([ratio, lsr, dori, dist, q[:, 0] / width, q[:, 1] / height, t[:, 0] / width,
+                      t[:, 1] / height], axis=1).astype(np.float32)
+    return rec, feats, inl
+
+
+def c5_pair(k: int, seed0: int = 500):
+    """Pair k of the learned-sampler workload: 1920x1080 geometry, random
+    perspective homography (as for the 1080p pair), 2k-8k matches, outlier ratio U(0.1, 0.7)."""
+    u = SplitMix64(seed0 + 7919 * k).uniform(6)
+    H = perspective_h(1920, 1080, -30 + 60 * u[0], 0.7 + 0.7 * u[1], -2e-4 + 4e-4 * u[2], -2e-4 + 4e-4 * u[3])
+    n = int(2000 + 6000 * u[4])
+    return putative_matches(n, 0.1 + 0.6 * u[5], H, 1920, 1080, seed0 + 104729 * k)
