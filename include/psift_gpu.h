@@ -126,6 +126,14 @@ psift_status psift_detect_keypoints(psift_ctx* ctx, const float* image, uint32_t
                                     const psift_sift_config* cfg, psift_keypoint* out,
                                     uint32_t capacity, uint32_t* count);
 
+/* compute_sift_descriptors_with_kind (src/pipeline.rs:1585-1629): orientations
+ * and descriptors for caller-given keypoints (the CLI extract path).  The pyramid
+ * is rebuilt with scales / octaves / upsampling inferred from the keypoints as
+ * the reference does; no feature cap.  kind: 0 = Sift, 1 = RootSift. */
+psift_status psift_compute_descriptors(psift_ctx* ctx, const float* image, uint32_t height,
+                                       uint32_t width, size_t row_stride, const psift_keypoint* kps,
+                                       uint32_t n, int32_t kind, psift_features* out);
+
 /* Device-resident batch: `n` u8 images already in device memory, results left
  * in device memory (feature SoA pointers in outs[i] are device pointers) and the
  * per-image feature counts written to the device array d_counts.  No host
@@ -199,6 +207,21 @@ psift_status psift_homography_estimate(psift_ctx* ctx, const psift_match* matche
 psift_status psift_similarity_estimate(psift_ctx* ctx, const psift_match* matches, uint32_t n,
                                        const psift_ransac_options* opt, uint8_t* inlier_mask,
                                        float* model6, int32_t* has_model, uint32_t* inlier_count);
+/* TrackingSummary (src/pipeline.rs:1137-1152) of summarize_tracking
+ * (src/pipeline.rs:2210-2272): similarity RANSAC (default threshold and seed) on
+ * the device, the summary statistics on the host.  Scales / orientations are
+ * indexed by the matches' query / target indices. */
+typedef struct psift_tracking_summary {
+  uint32_t raw_match_count, match_count;
+  float inlier_ratio;
+  float mean_dx, mean_dy, median_dx, median_dy;
+  float mean_scale_ratio, mean_rotation_deg;
+} psift_tracking_summary;
+psift_status psift_summarize_tracking(psift_ctx* ctx, const psift_match* matches, uint32_t n,
+                                      const float* query_scale, const float* query_orientation,
+                                      uint32_t nq, const float* target_scale,
+                                      const float* target_orientation, uint32_t nt,
+                                      psift_tracking_summary* out);
 /* Device-resident batch of independent estimations, one CTA each.  model holds 9
  * (homography) or 6 (similarity) floats.  sampling_weights (optional) replaces the
  * reference's 1/clamp(ratio, 0.05, 1) CDF weights (learned guided sampling);

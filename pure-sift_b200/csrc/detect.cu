@@ -11,6 +11,7 @@
 // stage.  Host code only computes the octave geometry and the f32 blur weights
 // (the reference's own formula, evaluated with the same libm) and carves the
 // workspace; all data-dependent work stays on the device.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -347,6 +348,39 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
   return PSIFT_OK;
 }
 
+// Octave base + blur/DoG levels only (used by the descriptor-only path).
+psift_status launch_pyramid_only(psift_ctx* ctx, DetectJob& job, const psift_sift_config& cfg) {
+  cudaStream_t st = ctx->stream;
+  const int n = job.n;
+  const int S = (int)cfg.scales;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice, st));
+  const SigmaSchedule sc = make_schedule(S, cfg.upsample_first_octave != 0);
+  int max_oct = 0;
+  for (int i = 0; i < n; ++i) max_oct = std::max(max_oct, job.n_oct[i]);
+  StageScope sc_pyr(ctx, STAGE_PYRAMID);
+  for (int o = 0; o < max_oct; ++o) {
+    int mh = 0, mw = 0;
+    for (int i = 0; i < n; ++i)
+      if (o < job.n_oct[i]) {
+        mh = std::max(mh, job.oct[(size_t)i * kMaxOctaves + o].h);
+        mw = std::max(mw, job.oct[(size_t)i * kMaxOctaves + o].w);
+      }
+    if (o == 0) {
+      const bool up = cfg.upsample_first_octave != 0;
+      const int mode = job.plans[0].src_kind == SRC_U8 ? (up ? 4 : 2) : (up ? 3 : 1);
+      cudaError_t e = launch_blur(mode, sc.init_taps.data(), sc.init_radius, job.d_plans, n, 0, 0, -1, mh, mw, st);
+      ctx->launches++;
+      if (e != cudaSuccess) return cuda_error(ctx, e, "blur(init)");
+    }
+    for (int s = 1; s <= S + 2; ++s) {
+      cudaError_t e = launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, n, o, s, S, mh, mw, st);
+      ctx->launches++;
+      if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
+    }
+  }
+  return PSIFT_OK;
+}
+
 psift_status check_common(psift_ctx* ctx, const psift_sift_config* cfg) {
   if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
   char msg[256];
@@ -534,6 +568,120 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
   st = build_job(ctx, imgs, *cfg, job, 0, nullptr);
   if (st != PSIFT_OK) return st;
   return launch_detect(ctx, job, *cfg, false);
+}
+
+
+// compute_sift_descriptors_with_kind (src/pipeline.rs:1585-1620): orientations and
+// descriptors for caller-given keypoints.  Like the reference, the pyramid is
+// rebuilt with scales = max(max layer, 3), the first-octave upsampling inferred
+// from the first layered keypoint's scale, octaves = max octave + 1, and no
+// feature cap.
+psift_status psift_compute_descriptors(psift_ctx* ctx, const float* image, uint32_t h, uint32_t w, size_t stride,
+                                       const psift_keypoint* kps, uint32_t n, int32_t kind, psift_features* out) {
+  if (!ctx || !out) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (kind != 0 && kind != 1) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "descriptor kind must be 0 or 1");
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaSetDevice");
+  out->count = 0;
+  if (h < 3 || w < 3 || n == 0) return PSIFT_OK;
+  if (!image || !kps || stride < w) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad image/keypoint argument");
+  uint32_t max_layer = 0;
+  for (uint32_t i = 0; i < n; ++i) max_layer = std::max(max_layer, kps[i].layer);
+  const uint32_t scales = std::max(max_layer, 3u);
+  if (scales > 10) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "keypoint layer beyond 10 scales");
+  const float k = std::pow(2.0f, 1.0f / (float)scales);
+  bool upsample = false;
+  for (uint32_t i = 0; i < n; ++i)
+    if (kps[i].layer > 0) {
+      const float expected = kBaseSigma * (float)(1ull << std::min(kps[i].octave, 62u)) * powi_f(k, (int)kps[i].layer);
+      upsample = (kps[i].scale / expected) < 0.707f;
+      break;
+    }
+  uint64_t max_oct = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    uint64_t o;
+    if (kps[i].layer > 0) {
+      o = kps[i].octave;
+    } else {
+      const float f = std::floor(std::log2(std::fmax(kps[i].scale / kBaseSigma, 1.0f)));
+      o = f <= 0.0f ? 0 : (uint64_t)f;
+    }
+    max_oct = std::max(max_oct, o);
+  }
+  psift_sift_config cfg;
+  psift_sift_config_default(&cfg);
+  cfg.octaves = (uint32_t)std::min<uint64_t>(max_oct + 1, (uint64_t)kMaxOctaves);
+  cfg.scales = scales;
+  cfg.upsample_first_octave = upsample ? 1 : 0;
+  cfg.descriptor_kind = kind;
+  cfg.max_features = 0;
+  const uint32_t feat_cap = std::min<uint64_t>(4ull * n, 0xFFFFFFFFull);
+  ImageDesc d{};
+  d.stride = w;
+  d.h = (int)h;
+  d.w = (int)w;
+  d.kind = SRC_F32;
+  d.feat_cap = feat_cap;
+  std::vector<ImageDesc> imgs{d};
+  DetectJob job;
+  const size_t img_bytes = sizeof(float) * (size_t)h * w;
+  void* extra = nullptr;
+  psift_status st = build_job(ctx, imgs, cfg, job, img_bytes + sizeof(psift_keypoint) * (size_t)n + 512, &extra);
+  if (st != PSIFT_OK) return st;
+  if (n > job.sel_cap) return set_error(ctx, PSIFT_ERR_CAPACITY, "more keypoints than the workspace holds (262144)");
+  job.plans[0].src = extra;
+  st = pinned_reserve(ctx, std::max(img_bytes + sizeof(psift_keypoint) * (size_t)n,
+                                    (size_t)feat_cap * sizeof(float) * (5 + kDescLen)) + 64);
+  if (st != PSIFT_OK) return st;
+  char* pin = ctx->pinned.base;
+  for (uint32_t y = 0; y < h; ++y) std::memcpy(pin + (size_t)y * w * 4, image + (size_t)y * stride, (size_t)w * 4);
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(extra, pin, img_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  // the keypoints replace the detector's output (sel list) unchanged
+  std::memcpy(pin + img_bytes, kps, sizeof(psift_keypoint) * n);
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.plans[0].sel, pin + img_bytes, sizeof(psift_keypoint) * n,
+                                      cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.plans[0].sel_count, &n, 4, cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));  // staging reuse below
+  // pyramid only (the extrema stages are skipped), then orientation + descriptors
+  st = launch_pyramid_only(ctx, job, cfg);
+  if (st != PSIFT_OK) return st;
+  DescribeParams dp{(int)scales, 0u, kind};
+  cudaError_t e = launch_orientation(job.d_plans, 1, n, dp, ctx->stream);
+  if (e == cudaSuccess) e = launch_feature_scan(job.d_plans, 1, 0, ctx->stream);
+  if (e == cudaSuccess) e = launch_descriptor(job.d_plans, 1, n, dp, ctx->stream);
+  ctx->launches += 3;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "compute_descriptors");
+  uint32_t hc[2] = {0, 0};
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(pin, job.plans[0].feat_count, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(hc, pin, 8);
+  const uint32_t c = hc[0];
+  if (c > out->capacity) {
+    out->count = c;
+    return set_error(ctx, PSIFT_ERR_CAPACITY, "feature output capacity too small");
+  }
+  const ImagePlan& P = job.plans[0];
+  float* hp = (float*)pin;
+  if (c) {
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 0 * (size_t)c, P.fx, 4 * (size_t)c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 1 * (size_t)c, P.fy, 4 * (size_t)c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 2 * (size_t)c, P.fscale, 4 * (size_t)c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 3 * (size_t)c, P.fresp, 4 * (size_t)c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 4 * (size_t)c, P.fori, 4 * (size_t)c, cudaMemcpyDeviceToHost, ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hp + 5 * (size_t)c, P.fdesc, 4 * (size_t)c * kDescLen, cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!out->x || !out->y || !out->scale || !out->response || !out->orientation || !out->descriptors)
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null feature output array");
+    std::memcpy(out->x, hp + 0 * (size_t)c, 4 * (size_t)c);
+    std::memcpy(out->y, hp + 1 * (size_t)c, 4 * (size_t)c);
+    std::memcpy(out->scale, hp + 2 * (size_t)c, 4 * (size_t)c);
+    std::memcpy(out->response, hp + 3 * (size_t)c, 4 * (size_t)c);
+    std::memcpy(out->orientation, hp + 4 * (size_t)c, 4 * (size_t)c);
+    std::memcpy(out->descriptors, hp + 5 * (size_t)c, 4 * (size_t)c * kDescLen);
+  }
+  out->count = c;
+  return PSIFT_OK;
 }
 
 }  // extern "C"

@@ -2,6 +2,8 @@
 // Homography::estimate_similarity, RansacOptions::validate).
 //
 // Reference: src/pipeline.rs:177-247 (options, seeds), :2038-2049, :2635-2661.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -182,3 +184,70 @@ psift_status psift_ransac_batch_dev(psift_ctx* ctx, const psift_ransac_job* jobs
 }
 
 }  // extern "C"
+
+namespace psift {
+namespace {
+// Reference median_f32 (src/pipeline.rs:2195-2206).
+float median_f32(std::vector<float> v) {
+  if (v.empty()) return 0.0f;
+  std::stable_sort(v.begin(), v.end(), [](float a, float b) { return a < b; });
+  const size_t mid = v.size() / 2;
+  return v.size() % 2 == 1 ? v[mid] : 0.5f * (v[mid - 1] + v[mid]);
+}
+}  // namespace
+}  // namespace psift
+
+extern "C" psift_status psift_summarize_tracking(psift_ctx* ctx, const psift_match* m, uint32_t n,
+                                                 const float* q_scale, const float* q_ori, uint32_t nq,
+                                                 const float* t_scale, const float* t_ori, uint32_t nt,
+                                                 psift_tracking_summary* out) {
+  // summarize_tracking (src/pipeline.rs:2210-2272): the similarity RANSAC runs on the
+  // device; the O(n) summary below repeats the reference's f32 sums on the host.
+  if (!ctx || !out) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (n == 0) {
+    *out = psift_tracking_summary{0, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f};
+    return PSIFT_OK;
+  }
+  if (!m || !q_scale || !q_ori || !t_scale || !t_ori) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  for (uint32_t i = 0; i < n; ++i)
+    if (m[i].query_index >= nq || m[i].target_index >= nt)
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "match index outside the feature arrays");
+  std::vector<uint8_t> mask(n);
+  float model[9];
+  int32_t has = 0;
+  uint32_t cnt = 0;
+  psift_ransac_options opt;
+  psift_ransac_options_default(&opt);
+  psift_status st = psift_similarity_estimate(ctx, m, n, &opt, mask.data(), model, &has, &cnt);
+  if (st != PSIFT_OK) return st;
+  std::vector<const psift_match*> act;
+  for (uint32_t i = 0; i < n; ++i)
+    if (mask[i]) act.push_back(&m[i]);
+  if (act.empty())
+    for (uint32_t i = 0; i < n; ++i) act.push_back(&m[i]);
+  const float inv_n = 1.0f / (float)act.size();
+  float sdx = 0, sdy = 0, ssr = 0, ssin = 0, scos = 0;
+  std::vector<float> dxs, dys;
+  for (const psift_match* a : act) {
+    sdx += a->displacement_x;
+    sdy += a->displacement_y;
+    dxs.push_back(a->displacement_x);
+    dys.push_back(a->displacement_y);
+    const float qs = q_scale[a->query_index], ts = t_scale[a->target_index];
+    if (qs > 1e-6f) ssr += ts / qs;
+    const float dth = t_ori[a->target_index] - q_ori[a->query_index];
+    ssin += std::sin(dth);
+    scos += std::cos(dth);
+  }
+  const float mrot = std::atan2(ssin, scos);
+  out->raw_match_count = n;
+  out->match_count = (uint32_t)act.size();
+  out->inlier_ratio = (float)act.size() / (float)n;
+  out->mean_dx = sdx * inv_n;
+  out->mean_dy = sdy * inv_n;
+  out->median_dx = psift::median_f32(dxs);
+  out->median_dy = psift::median_f32(dys);
+  out->mean_scale_ratio = ssr * inv_n;
+  out->mean_rotation_deg = mrot * 57.2957795130823208767981548141051703f;
+  return PSIFT_OK;
+}

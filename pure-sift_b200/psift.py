@@ -96,6 +96,12 @@ class CRansacJob(C.Structure):
                 ("iterations", C.c_void_p)]
 
 
+class CTracking(C.Structure):
+    _fields_ = [("raw_match_count", C.c_uint32), ("match_count", C.c_uint32), ("inlier_ratio", C.c_float),
+                ("mean_dx", C.c_float), ("mean_dy", C.c_float), ("median_dx", C.c_float),
+                ("median_dy", C.c_float), ("mean_scale_ratio", C.c_float), ("mean_rotation_deg", C.c_float)]
+
+
 KEYPOINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("scale", "<f4"), ("response", "<f4"),
                            ("octave", "<u4"), ("layer", "<u4")])
 
@@ -145,6 +151,10 @@ _SIGS = {
                                   C.c_uint32, C.c_float, C.c_uint64, C.c_void_p]),
     "psift_mlp_train_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                       C.c_uint32, C.c_float, C.c_uint64, C.c_void_p]),
+    "psift_compute_descriptors": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p,
+                                            C.c_uint32, C.c_int32, C.POINTER(CFeatures)]),
+    "psift_summarize_tracking": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                           C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CTracking)]),
     "psift_quantize_u128": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "psift_quantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "psift_dequantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
@@ -636,3 +646,147 @@ def ransac_batch(match_sets, options: RansacOptions = RansacOptions(), homograph
         model = o[4:4 + (9 if homography else 6)].view(np.float32).copy()
         res.append((mask[:n].cpu().numpy().astype(bool), model if o[1] else None, (int(o[2]), int(o[3]))))
     return res
+
+
+def compute_sift_descriptors(img: np.ndarray, keypoints, kind: int = 0, ctx: Context | None = None) -> Features:
+    """``compute_sift_descriptors_with_kind`` (src/pipeline.rs:1585-1629): descriptors
+    for given keypoints; the pyramid is rebuilt from what the keypoints imply."""
+    ctx = ctx or default_context()
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    kps = np.ascontiguousarray(keypoints, dtype=KEYPOINT_DTYPE)
+    h, w = img.shape
+    cap = max(4 * len(kps), 1)
+    out = Features.empty(cap)
+    cf = _c_features(out)
+    ctx.check(ctx.lib.psift_compute_descriptors(ctx.handle, img.ctypes.data, h, w, w, kps.ctypes.data, len(kps),
+                                                int(kind), C.byref(cf)))
+    return out.head(int(cf.count))
+
+
+@dataclass
+class TrackingSummary:
+    """``TrackingSummary`` (src/pipeline.rs:1137-1152)."""
+    raw_match_count: int
+    match_count: int
+    inlier_ratio: float
+    mean_displacement: tuple
+    median_displacement: tuple
+    mean_scale_ratio: float
+    mean_rotation_deg: float
+
+
+def summarize_tracking(query: Features, target: Features, matches, ctx: Context | None = None) -> TrackingSummary:
+    """``summarize_tracking`` (src/pipeline.rs:2210-2272)."""
+    ctx = ctx or default_context()
+    m = _as_matches(matches)
+    out = CTracking()
+    ctx.check(ctx.lib.psift_summarize_tracking(ctx.handle, m.ctypes.data, len(m), query.scale.ctypes.data,
+                                               query.orientation.ctypes.data, len(query), target.scale.ctypes.data,
+                                               target.orientation.ctypes.data, len(target), C.byref(out)))
+    return TrackingSummary(out.raw_match_count, out.match_count, out.inlier_ratio, (out.mean_dx, out.mean_dy),
+                           (out.median_dx, out.median_dy), out.mean_scale_ratio, out.mean_rotation_deg)
+
+
+DEFAULT_CATALOG_SHORTLIST = 16
+DEFAULT_CATALOG_TOP_K = 5
+
+
+@dataclass
+class CatalogEntry:
+    """``CatalogEntry`` (src/catalog.rs:110-150)."""
+    id: str
+    width: int
+    height: int
+    features: Features
+    signatures: np.ndarray  # (n, 2) u64
+
+
+@dataclass
+class CatalogSearchHit:
+    """``CatalogSearchHit`` (src/catalog.rs:158-177)."""
+    id: str
+    width: int
+    height: int
+    feature_count: int
+    coarse_votes: int
+    tracking: TrackingSummary
+    transform: object
+    homography: object
+
+
+class FeatureCatalog:
+    """``FeatureCatalog`` (src/catalog.rs:182-702) with its search on the GPU.
+
+    The index (entries, id lookup) is host data as in the reference; the coarse
+    Hamming voting, Lowe matching, similarity / homography RANSAC and the tracking
+    summary's RANSAC run through the C ABI.  The multi-index-hashing semantics
+    apply above 32 entries, exactly where the reference switches to its tables.
+    """
+
+    def __init__(self, octaves: int = 3, scales: int = 3, threshold: float = DEFAULT_CONTRAST_THRESHOLD):
+        self.octaves, self.scales, self.threshold = octaves, scales, threshold
+        self.entries: list[CatalogEntry] = []
+        self._index: dict[str, int] = {}
+
+    def __len__(self):
+        return len(self.entries)
+
+    def upsert_entry(self, id: str, width: int, height: int, features: Features, ctx: Context | None = None):
+        sig = quantize_descriptor_u128(features.descriptors, ctx) if len(features) else np.zeros((0, 2), np.uint64)
+        e = CatalogEntry(id, width, height, features, sig)
+        if id in self._index:
+            self.entries[self._index[id]] = e
+        else:
+            self._index[id] = len(self.entries)
+            self.entries.append(e)
+
+    def remove(self, id: str) -> bool:
+        """``remove`` (src/catalog.rs:343-352): swap_remove then reindex."""
+        i = self._index.pop(id, None)
+        if i is None:
+            return False
+        last = self.entries.pop()
+        if i < len(self.entries):
+            self.entries[i] = last
+        self._index = {e.id: k for k, e in enumerate(self.entries)}
+        return True
+
+    def coarse_votes(self, query: Features, ctx: Context | None = None):
+        qs = quantize_descriptor_u128(query.descriptors, ctx)
+        sizes = [len(e.signatures) for e in self.entries]
+        off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        cat = np.concatenate([e.signatures for e in self.entries]) if off[-1] else np.zeros((0, 2), np.uint64)
+        mih = len(self.entries) > 32
+        return hamming_votes(qs, cat, off, mih, ctx), mih
+
+    def search_features(self, query: Features, top_k: int = DEFAULT_CATALOG_TOP_K,
+                        shortlist_k: int = DEFAULT_CATALOG_SHORTLIST, ratio_threshold: float = DEFAULT_MATCH_RATIO,
+                        ransac_threshold: float = DEFAULT_RANSAC_REPROJ_THRESHOLD,
+                        ctx: Context | None = None) -> list:
+        """``search_features`` (src/catalog.rs:576-702)."""
+        if not self.entries or len(query) == 0 or top_k == 0:
+            return []
+        votes, mih = self.coarse_votes(query, ctx)
+        cands = [(i, int(v)) for i, v in enumerate(votes) if (v > 0 or not mih)]
+        if len(cands) > max(shortlist_k, 1):
+            cands.sort(key=lambda c: (-c[1], self.entries[c[0]].id))
+            cands = cands[:max(shortlist_k, 1)]
+        hits = []
+        opt = RansacOptions(ransac_threshold)
+        for idx, v in cands:
+            e = self.entries[idx]
+            if len(e.features) < 2:
+                continue
+            raw = match_descriptors(query, e.features, ratio_threshold, ctx)
+            if len(raw) == 0:
+                continue
+            tracking = summarize_tracking(query, e.features, raw, ctx)
+            sim_in, sim_tf = Homography.estimate_similarity(raw, opt, ctx)
+            hom_in, hom_tf = Homography.estimate(raw, opt, ctx)
+            best = max(len(hom_in), len(sim_in))
+            tracking.match_count = best
+            if tracking.raw_match_count > 0:
+                tracking.inlier_ratio = float(np.float32(best) / np.float32(tracking.raw_match_count))
+            hits.append(CatalogSearchHit(e.id, e.width, e.height, len(e.features), v, tracking, sim_tf, hom_tf))
+        hits.sort(key=lambda h: (-h.tracking.match_count, -h.tracking.inlier_ratio, -h.coarse_votes, h.id))
+        return hits[:top_k]
