@@ -126,6 +126,21 @@ psift_status psift_detect_keypoints(psift_ctx* ctx, const float* image, uint32_t
                                     const psift_sift_config* cfg, psift_keypoint* out,
                                     uint32_t capacity, uint32_t* count);
 
+/* gaussian_blur (src/pipeline.rs:314-425): separable blur with the f32 weights of
+ * gaussian_kernel_1d (:275-311) and clamp-to-edge borders; `out` is a dense
+ * height x width host array.  Bit-identical to the reference.  Radii above 15
+ * (sigma > 5) are rejected; the pyramid never needs them. */
+psift_status psift_gaussian_blur(psift_ctx* ctx, const float* image, uint32_t height, uint32_t width,
+                                 size_t row_stride, float sigma, float* out);
+/* build_scale_space_pyramid_with_options (src/pipeline.rs:550-638): for each
+ * octave o < *n_octaves, its scales+3 Gaussian planes then its scales+2 DoG
+ * planes, each dims[2o] x dims[2o+1] dense row-major, octave after octave in
+ * `planes` (capacity in floats).  dims holds 2 * cfg->octaves entries.  With
+ * planes == NULL only the geometry is returned.  Bit-identical to the reference. */
+psift_status psift_build_pyramid(psift_ctx* ctx, const float* image, uint32_t height, uint32_t width,
+                                 size_t row_stride, const psift_sift_config* cfg, float* planes,
+                                 size_t capacity, uint32_t* dims, uint32_t* n_octaves);
+
 /* compute_sift_descriptors_with_kind (src/pipeline.rs:1585-1629): orientations
  * and descriptors for caller-given keypoints (the CLI extract path).  The pyramid
  * is rebuilt with scales / octaves / upsampling inferred from the keypoints as

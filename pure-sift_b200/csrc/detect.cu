@@ -576,6 +576,104 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
 // rebuilt with scales = max(max layer, 3), the first-octave upsampling inferred
 // from the first layered keypoint's scale, octaves = max octave + 1, and no
 // feature cap.
+psift_status psift_gaussian_blur(psift_ctx* ctx, const float* image, uint32_t h, uint32_t w, size_t stride,
+                                 float sigma, float* out) {
+  if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaSetDevice");
+  if (h == 0 || w == 0) return PSIFT_OK;
+  if (!image || !out || stride < w) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad image/output argument");
+  if (!(sigma == sigma)) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "sigma is NaN");
+  const std::vector<float> taps = gaussian_taps(sigma);
+  const int radius = (int)taps.size() / 2;
+  if (radius > kMaxTaps / 2 - 1)
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "sigma gives a radius above 15 (sigma > 5)");
+  HostOctave H{(int)h, (int)w, (long long)align_up((size_t)w, 32)};
+  const size_t img_bytes = sizeof(float) * (size_t)h * w;
+  psift_status st = arena_reserve(ctx, align_up(sizeof(ImagePlan), 256) + align_up(img_bytes, 256) +
+                                           align_up(plane_bytes(H), 256) + 256);
+  if (st != PSIFT_OK) return st;
+  ImagePlan* d_plan = (ImagePlan*)arena_alloc(ctx, sizeof(ImagePlan));
+  float* d_src = (float*)arena_alloc(ctx, img_bytes);
+  float* d_out = (float*)arena_alloc(ctx, plane_bytes(H));
+  ImagePlan P;
+  std::memset(&P, 0, sizeof P);
+  P.src = d_src;
+  P.src_stride = w;
+  P.src_h = (int)h;
+  P.src_w = (int)w;
+  P.src_kind = SRC_F32;
+  P.n_oct = 1;
+  P.oct[0].h = (int)h;
+  P.oct[0].w = (int)w;
+  P.oct[0].pitch = H.pitch;
+  P.oct[0].plane_stride = H.pitch * h;
+  P.oct[0].g = d_out;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpy2DAsync(d_src, sizeof(float) * w, image, sizeof(float) * stride, sizeof(float) * w, h,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_plan, &P, sizeof P, cudaMemcpyHostToDevice, ctx->stream));
+  cudaError_t e = launch_blur(1, taps.data(), radius, d_plan, 1, 0, 0, -1, (int)h, (int)w, ctx->stream);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "gaussian_blur");
+  PSIFT_CUDA_TRY(ctx, cudaMemcpy2DAsync(out, sizeof(float) * w, d_out, sizeof(float) * H.pitch, sizeof(float) * w, h,
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PSIFT_OK;
+}
+
+psift_status psift_build_pyramid(psift_ctx* ctx, const float* image, uint32_t h, uint32_t w, size_t stride,
+                                 const psift_sift_config* cfg, float* planes, size_t capacity, uint32_t* dims,
+                                 uint32_t* n_octaves) {
+  psift_status st = check_common(ctx, cfg);
+  if (st != PSIFT_OK) return st;
+  if (!n_octaves || !dims || (h && w && !image) || stride < w)
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad image/output argument");
+  const int S = (int)cfg->scales;
+  HostOctave oct[kMaxOctaves];
+  const int no = plan_octaves((int)h, (int)w, (int)cfg->octaves, cfg->upsample_first_octave != 0, oct);
+  *n_octaves = (uint32_t)no;
+  size_t need = 0;
+  for (int o = 0; o < no; ++o) {
+    dims[2 * o] = (uint32_t)oct[o].h;
+    dims[2 * o + 1] = (uint32_t)oct[o].w;
+    need += (size_t)(2 * S + 5) * oct[o].h * oct[o].w;
+  }
+  if (!planes || no == 0) return PSIFT_OK;  // geometry query
+  if (capacity < need) return set_error(ctx, PSIFT_ERR_CAPACITY, "plane buffer smaller than the pyramid");
+  ImageDesc d{};
+  d.stride = w;
+  d.h = (int)h;
+  d.w = (int)w;
+  d.kind = SRC_F32;
+  d.feat_cap = 1;
+  std::vector<ImageDesc> imgs{d};
+  DetectJob job;
+  const size_t img_bytes = sizeof(float) * (size_t)h * w;
+  void* extra = nullptr;
+  psift_sift_config c = *cfg;
+  c.max_features = 0;
+  st = build_job(ctx, imgs, c, job, img_bytes, &extra);
+  if (st != PSIFT_OK) return st;
+  job.plans[0].src = extra;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpy2DAsync(extra, sizeof(float) * w, image, sizeof(float) * stride, sizeof(float) * w, h,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+  st = launch_pyramid_only(ctx, job, c);
+  if (st != PSIFT_OK) return st;
+  float* dst = planes;
+  for (int o = 0; o < no; ++o) {
+    const OctaveDev& O = job.plans[0].oct[o];
+    const size_t hw = (size_t)O.h * O.w;
+    for (int i = 0; i < 2 * S + 5; ++i) {
+      const float* src = i < S + 3 ? O.g + (size_t)i * O.plane_stride : O.d + (size_t)(i - S - 3) * O.plane_stride;
+      PSIFT_CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, sizeof(float) * O.w, src, sizeof(float) * O.pitch,
+                                            sizeof(float) * O.w, O.h, cudaMemcpyDeviceToHost, ctx->stream));
+      dst += hw;
+    }
+  }
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PSIFT_OK;
+}
+
 psift_status psift_compute_descriptors(psift_ctx* ctx, const float* image, uint32_t h, uint32_t w, size_t stride,
                                        const psift_keypoint* kps, uint32_t n, int32_t kind, psift_features* out) {
   if (!ctx || !out) return PSIFT_ERR_INVALID_ARGUMENT;

@@ -12,12 +12,24 @@
 // like `(x + k).saturating_sub(r).min(w - 1)`, and the kernel weights are
 // computed on the host with the reference's f32 formula.
 //
-// Tiling: one CTA produces a 64x64 output tile.  The (64+2r)^2 input tile is
-// staged in shared memory, the horizontal pass writes (64+2r)x64 partial rows to
-// shared memory (4 outputs per thread from 128-bit loads), the vertical pass
-// produces 4 rows per thread and writes G_s and D_{s-1} = G_s - G_{s-1} with
-// coalesced 128-byte row segments.  Level `scales` also writes the even/even
-// samples that form the next octave's base (fused downsample_2x).
+// Tiling: one CTA of 256 threads produces a 64x64 output tile.
+//   1. Staging: the (64+2R) x (64+2R') input tile (R' = R rounded up to 4, so
+//      every interior chunk is one aligned 128-bit load) goes to shared memory
+//      with rows interleaved in pairs: element (2p+i, c) sits at s_in[p][c].i.
+//   2. Horizontal pass: each thread makes 4 (or 8) adjacent outputs of a row
+//      pair.  A 128-bit shared load yields two {row 2p, row 2p+1} pairs, so each
+//      tap is one packed multiply and one packed rounded add (see mul_add2_rn) for
+//      two outputs, with the scalar operations' rounding per component.
+//   3. Vertical pass: each thread makes a column pair x rows of outputs from the
+//      row-major intermediate, again with packed f32x2 operations.
+//   Taps are consumed in input order; for every output that is k = 0..2R, the
+//   reference's order.  The row-pair stride is 2 (mod 16) float2 and lanes are
+//   assigned so that the 8 lanes of a quarter-warp hit 8 distinct 16-byte bank
+//   groups.  Outputs: G_s and D_{s-1} = G_s - G_{s-1} as 64-bit stores; level
+//   `scales` also writes the even/even samples that form the next octave's base
+//   (fused downsample_2x).  Images alternate direction between consecutive
+//   levels (blockIdx.z reversed on odd levels) so the planes written last by
+//   one launch, still in L2, are read first by the next.
 #include "detect_plan.cuh"
 #include "psift_internal.cuh"
 
@@ -26,24 +38,50 @@ namespace psift {
 constexpr int kTileW = 64;
 constexpr int kTileH = 64;
 constexpr int kBlurThreads = 256;
+constexpr int kTmpStride = kTileW + 8;  // floats per intermediate row
 
-struct Taps {
-  float w[kMaxTaps];
+struct Taps2 {
+  float2 w[kMaxTaps];  // {w_k, w_k}
+  float2 one;          // {1, 1}: the multiplier of the packed add (see mul_add2_rn)
 };
 
 enum BlurMode : int { MODE_LEVEL = 0, MODE_INIT_F32 = 1, MODE_INIT_U8 = 2, MODE_INIT_F32_UP = 3, MODE_INIT_U8_UP = 4 };
 
 template <int R>
 struct BlurGeom {
-  static constexpr int NV = ((2 * R + 4) + 3) / 4 * 4;           // floats per thread in the H pass
-  static constexpr int IN_H = kTileH + 2 * R;
-  static constexpr int IN_WL = kTileW + 2 * R;                    // columns actually needed
-  static constexpr int IN_P0 = (IN_WL + 3) / 4 * 4;
-  static constexpr int IN_P = IN_P0 > (kTileW - 4 + NV) ? IN_P0 : (kTileW - 4 + NV);
-  static constexpr int SMEM_FLOATS = IN_H * IN_P + IN_H * kTileW;
+  static constexpr int RP = (R + 3) / 4 * 4;                          // column halo, whole float4 chunks
+  static constexpr int IN_W = kTileW + 2 * RP;                        // staged columns
+  static constexpr int IN_H = kTileH + 2 * R;                         // staged rows (even)
+  static constexpr int IN_PAIRS = IN_H / 2;
+  static constexpr int IN_S = IN_W + (((2 - IN_W) % 16) + 16) % 16;   // float2 per row pair, = 2 (mod 16)
+  static constexpr int C4 = IN_W / 4;
+  static constexpr int SMEM_BYTES = IN_PAIRS * IN_S * 8 + IN_H * kTmpStride * 4;
 };
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// acc + v * w per component with two roundings, never fused into one.
+// The packed multiply and add are each exact IEEE operations, but ptxas
+// contracts a single-use mul.rn.f32x2 feeding add.rn.f32x2 into a packed FMA
+// (even with explicit .rn and --fmad false), which changes about 6% of the
+// results by an ulp.  The add is therefore issued as fma.rn(p, one, acc) with
+// `one` = {1, 1} taken from the kernel parameters: p * 1 is exact, so this is
+// round(p + acc), and the compiler cannot fold a multiplier it does not know.
+// The bit-exact blur and pyramid tests guard this.
+__device__ __forceinline__ float2 mul_add2_rn(float2 acc, float2 v, float2 w, float2 one) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pv, pw, po, pp;\n\t"
+      "mov.b64 pa, {%2, %3};\n\t"
+      "mov.b64 pv, {%4, %5};\n\t"
+      "mov.b64 pw, {%6, %7};\n\t"
+      "mov.b64 po, {%8, %9};\n\t"
+      "mul.rn.f32x2 pp, pv, pw;\n\t"
+      "fma.rn.f32x2 pa, pp, po, pa;\n\t"
+      "mov.b64 {%0, %1}, pa;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(acc.x), "f"(acc.y), "f"(v.x), "f"(v.y), "f"(w.x), "f"(w.y), "f"(one.x), "f"(one.y));
+  return r;
+}
 
 // Source sample at octave-0 coordinates (gy, gx), already clamped to the plane.
 template <int MODE>
@@ -79,15 +117,18 @@ __device__ __forceinline__ float fetch_src(const ImagePlan& P, const OctaveDev& 
   }
 }
 
-// One blur level for every image of the batch (blockIdx.z = image).
+// One blur level for every image of the batch (blockIdx.z = image, reversed when zrev).
 //   MODE_LEVEL: G[s] = blur(G[s-1]); D[s-1] = G[s] - G[s-1]; level `down_level` also
 //               writes the next octave's G[0] (even rows/columns).
 //   MODE_INIT_*: G[0] of octave 0 from the input image.
-template <int R, int MODE>
+template <int R, int HC, int RV, int MODE>
 __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePlan* __restrict__ plans, int octave,
-                                                                   int level, int down_level, Taps taps) {
+                                                                   int level, int down_level, int zrev, Taps2 taps) {
   using Gm = BlurGeom<R>;
-  const ImagePlan& P = plans[blockIdx.z];
+  static_assert(HC == 4 || HC == 8, "horizontal outputs per thread");
+  static_assert(RV % 2 == 0 && kTileH % (RV * (kBlurThreads / 32)) == 0, "vertical rows per thread");
+  const int z = zrev ? (int)gridDim.z - 1 - (int)blockIdx.z : (int)blockIdx.z;
+  const ImagePlan& P = plans[z];
   if (octave >= P.n_oct) return;
   const OctaveDev& O = P.oct[octave];
   const int h = O.h, w = O.w;
@@ -95,101 +136,154 @@ __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePla
   if (tx0 >= w || ty0 >= h) return;
 
   extern __shared__ float4 smem4[];
-  float* s_in = reinterpret_cast<float*>(smem4);
-  float* s_tmp = s_in + Gm::IN_H * Gm::IN_P;
+  float2* s_in = reinterpret_cast<float2*>(smem4);                               // [IN_PAIRS][IN_S]
+  float* s_tmp = reinterpret_cast<float*>(s_in + Gm::IN_PAIRS * Gm::IN_S);       // [IN_H][kTmpStride]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  // Stage the clamped input tile.
-  for (int i = threadIdx.x; i < Gm::IN_H * Gm::IN_P; i += kBlurThreads) {
-    const int r = i / Gm::IN_P, c = i - r * Gm::IN_P;
-    float v = 0.0f;
-    if (c < Gm::IN_WL) {
-      const int gy = clampi(ty0 - R + r, 0, h - 1);
-      const int gx = clampi(tx0 - R + c, 0, w - 1);
-      v = fetch_src<MODE>(P, O, level - 1, gy, gx);
+  // 1. Stage the clamped input tile, rows interleaved in pairs.
+  const float* src_plane = O.g + (long long)(level - 1) * O.plane_stride;  // MODE_LEVEL only
+  for (int u = threadIdx.x; u < Gm::IN_PAIRS * Gm::C4; u += kBlurThreads) {
+    const int rp = u / Gm::C4, c4 = u - rp * Gm::C4;
+    const int gy0 = clampi(ty0 - R + 2 * rp, 0, h - 1);
+    const int gy1 = clampi(ty0 - R + 2 * rp + 1, 0, h - 1);
+    const int gx = tx0 - Gm::RP + 4 * c4;
+    float4 a, b;
+    if (MODE == MODE_LEVEL && gx >= 0 && gx + 3 < w) {
+      a = __ldg(reinterpret_cast<const float4*>(src_plane + (long long)gy0 * O.pitch + gx));
+      b = __ldg(reinterpret_cast<const float4*>(src_plane + (long long)gy1 * O.pitch + gx));
+    } else {
+      float av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int cx = clampi(gx + i, 0, w - 1);
+        av[i] = fetch_src<MODE>(P, O, level - 1, gy0, cx);
+        bv[i] = fetch_src<MODE>(P, O, level - 1, gy1, cx);
+      }
+      a = make_float4(av[0], av[1], av[2], av[3]);
+      b = make_float4(bv[0], bv[1], bv[2], bv[3]);
     }
-    s_in[i] = v;
+    float4* d = reinterpret_cast<float4*>(s_in + rp * Gm::IN_S + 4 * c4);
+    d[0] = make_float4(a.x, b.x, a.y, b.y);
+    d[1] = make_float4(a.z, b.z, a.w, b.w);
   }
   __syncthreads();
 
-  // Horizontal pass: 16 threads per row, 4 consecutive outputs each.
+  // 2. Horizontal pass over row pairs.
   {
-    const int x0 = (threadIdx.x & 15) * 4;
-    for (int row = threadIdx.x >> 4; row < Gm::IN_H; row += kBlurThreads / 16) {
-      float v[Gm::NV];
-      const float4* src4 = reinterpret_cast<const float4*>(s_in + row * Gm::IN_P + x0);
+    constexpr int QX = 16 / HC, QR = 8 / QX;  // a quarter-warp covers QR row pairs x QX column groups
+    constexpr int OFF = Gm::RP - R, SH = OFF & 1;
+    constexpr int NP = (HC + 2 * R + SH + 1) / 2;  // 128-bit loads per row pair
+    const int qi = lane & 7;
+    const int rsub = qi / QX;
+    const int xg = (lane >> 3) * QX + (qi % QX);
+    for (int rp = warp * QR + rsub; rp < Gm::IN_PAIRS; rp += (kBlurThreads / 32) * QR) {
+      const float4* src = reinterpret_cast<const float4*>(s_in + rp * Gm::IN_S + HC * xg + OFF - SH);
+      float2 acc[HC];
 #pragma unroll
-      for (int q = 0; q < Gm::NV / 4; ++q) {
-        const float4 t = src4[q];
-        v[4 * q + 0] = t.x;
-        v[4 * q + 1] = t.y;
-        v[4 * q + 2] = t.z;
-        v[4 * q + 3] = t.w;
+      for (int j = 0; j < HC; ++j) acc[j] = make_float2(0.0f, 0.0f);
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        const float4 t = src[q];
+        const float2 p0 = make_float2(t.x, t.y), p1 = make_float2(t.z, t.w);
+#pragma unroll
+        for (int j = 0; j < HC; ++j) {
+          const int k0 = 2 * q - SH - j;
+          if (k0 >= 0 && k0 <= 2 * R) acc[j] = mul_add2_rn(acc[j], p0, taps.w[k0], taps.one);
+          if (k0 + 1 >= 0 && k0 + 1 <= 2 * R) acc[j] = mul_add2_rn(acc[j], p1, taps.w[k0 + 1], taps.one);
+        }
       }
-      float o[4];
+      float* t0 = s_tmp + (2 * rp) * kTmpStride + HC * xg;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        float acc = 0.0f;
-#pragma unroll
-        for (int k = 0; k <= 2 * R; ++k) acc = __fadd_rn(acc, __fmul_rn(v[j + k], taps.w[k]));
-        o[j] = acc;
+      for (int jj = 0; jj < HC / 4; ++jj) {
+        *reinterpret_cast<float4*>(t0 + 4 * jj) =
+            make_float4(acc[4 * jj].x, acc[4 * jj + 1].x, acc[4 * jj + 2].x, acc[4 * jj + 3].x);
+        *reinterpret_cast<float4*>(t0 + kTmpStride + 4 * jj) =
+            make_float4(acc[4 * jj].y, acc[4 * jj + 1].y, acc[4 * jj + 2].y, acc[4 * jj + 3].y);
       }
-      *reinterpret_cast<float4*>(s_tmp + row * kTileW + x0) = make_float4(o[0], o[1], o[2], o[3]);
     }
   }
   __syncthreads();
 
-  // Vertical pass (row AXPY order of the reference): 4 consecutive rows per thread.
+  // 3. Vertical pass: a column pair x RV rows per thread.
   const long long gbase = (long long)level * O.plane_stride;
   float* gout = O.g + gbase;
   float* dout = (MODE == MODE_LEVEL) ? O.d + (long long)(level - 1) * O.plane_stride : nullptr;
   const bool do_down = (MODE == MODE_LEVEL) && level == down_level && octave + 1 < P.n_oct;
-  for (int item = threadIdx.x; item < kTileW * (kTileH / 4); item += kBlurThreads) {
-    const int x = item % kTileW;
-    const int y0 = (item / kTileW) * 4;
-    const int gx = tx0 + x;
-    float v[4 + 2 * R];
+  const int x = 2 * lane;
+  const int gx = tx0 + x;
+  for (int yb = warp * RV; yb < kTileH; yb += RV * (kBlurThreads / 32)) {
+    if (ty0 + yb >= h) break;
+    float2 acc[RV];
 #pragma unroll
-    for (int i = 0; i < 4 + 2 * R; ++i) v[i] = s_tmp[(y0 + i) * kTileW + x];
+    for (int j = 0; j < RV; ++j) acc[j] = make_float2(0.0f, 0.0f);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      float acc = 0.0f;
+    for (int i = 0; i < RV + 2 * R; ++i) {
+      const float2 v = *reinterpret_cast<const float2*>(s_tmp + (yb + i) * kTmpStride + x);
 #pragma unroll
-      for (int k = 0; k <= 2 * R; ++k) acc = __fadd_rn(acc, __fmul_rn(v[j + k], taps.w[k]));
-      const int gy = ty0 + y0 + j;
-      if (gy < h && gx < w) {
-        gout[(long long)gy * O.pitch + gx] = acc;
-        if constexpr (MODE == MODE_LEVEL) {
-          const float prev = s_in[(R + y0 + j) * Gm::IN_P + (R + x)];
-          dout[(long long)gy * O.pitch + gx] = __fsub_rn(acc, prev);
-          if (do_down && !(gy & 1) && !(gx & 1)) {
-            const OctaveDev& N = P.oct[octave + 1];
-            const int dy = gy >> 1, dx = gx >> 1;
-            if (dy < N.h && dx < N.w) N.g[(long long)dy * N.pitch + dx] = acc;
-          }
+      for (int j = 0; j < RV; ++j) {
+        const int k = i - j;
+        if (k >= 0 && k <= 2 * R) acc[j] = mul_add2_rn(acc[j], v, taps.w[k], taps.one);
+      }
+    }
+    if (gx >= w) continue;
+    const bool pair_ok = gx + 1 < w;
+    constexpr int NPR = ((R & 1) + RV + 1) / 2;
+    float4 prevp[MODE == MODE_LEVEL ? NPR : 1];
+    if constexpr (MODE == MODE_LEVEL) {
+      const float4* pp = reinterpret_cast<const float4*>(s_in + ((R >> 1) + (yb >> 1)) * Gm::IN_S + Gm::RP + x);
+#pragma unroll
+      for (int p = 0; p < NPR; ++p) prevp[p] = pp[p * (Gm::IN_S / 2)];
+    }
+#pragma unroll
+    for (int j = 0; j < RV; ++j) {
+      const int gy = ty0 + yb + j;
+      if (gy >= h) break;
+      float* grow = gout + (long long)gy * O.pitch + gx;
+      if (pair_ok) {
+        *reinterpret_cast<float2*>(grow) = acc[j];
+      } else {
+        grow[0] = acc[j].x;
+      }
+      if constexpr (MODE == MODE_LEVEL) {
+        const int idx = (R & 1) + j;
+        const float4 pv = prevp[idx >> 1];
+        const float px = (idx & 1) ? pv.y : pv.x;
+        const float py = (idx & 1) ? pv.w : pv.z;
+        float* drow = dout + (long long)gy * O.pitch + gx;
+        const float dx0 = __fsub_rn(acc[j].x, px);
+        if (pair_ok) {
+          __stcs(reinterpret_cast<float2*>(drow), make_float2(dx0, __fsub_rn(acc[j].y, py)));
+        } else {
+          __stcs(drow, dx0);
+        }
+        if (do_down && !(gy & 1)) {
+          const OctaveDev& N = P.oct[octave + 1];
+          const int dy = gy >> 1, dxn = gx >> 1;
+          if (dy < N.h && dxn < N.w) N.g[(long long)dy * N.pitch + dxn] = acc[j].x;
         }
       }
     }
   }
 }
 
-template <int R, int MODE>
+template <int R, int HC, int RV, int MODE>
 static cudaError_t launch_blur_r(const ImagePlan* plans, int n_images, int octave, int level, int down_level,
-                                 const Taps& taps, int max_h, int max_w, cudaStream_t st) {
+                                 int zrev, const Taps2& taps, int max_h, int max_w, cudaStream_t st) {
   using Gm = BlurGeom<R>;
-  const size_t smem = sizeof(float) * Gm::SMEM_FLOATS;
-  cudaError_t e = ensure_smem_attr((const void*)blur_level_kernel<R, MODE>, smem);
+  const size_t smem = Gm::SMEM_BYTES;
+  cudaError_t e = ensure_smem_attr((const void*)blur_level_kernel<R, HC, RV, MODE>, smem);
   if (e != cudaSuccess) return e;
   dim3 grid((max_w + kTileW - 1) / kTileW, (max_h + kTileH - 1) / kTileH, n_images);
-  blur_level_kernel<R, MODE><<<grid, kBlurThreads, smem, st>>>(plans, octave, level, down_level, taps);
+  blur_level_kernel<R, HC, RV, MODE><<<grid, kBlurThreads, smem, st>>>(plans, octave, level, down_level, zrev, taps);
   return cudaGetLastError();
 }
 
 template <int MODE>
 static cudaError_t launch_blur_mode(int radius, const ImagePlan* plans, int n, int octave, int level, int down_level,
-                                    const Taps& taps, int max_h, int max_w, cudaStream_t st) {
+                                    int zrev, const Taps2& taps, int max_h, int max_w, cudaStream_t st) {
   switch (radius) {
 #define PSIFT_R(RR) \
-  case RR: return launch_blur_r<RR, MODE>(plans, n, octave, level, down_level, taps, max_h, max_w, st);
+  case RR: return launch_blur_r<RR, 4, 8, MODE>(plans, n, octave, level, down_level, zrev, taps, max_h, max_w, st);
     PSIFT_R(1) PSIFT_R(2) PSIFT_R(3) PSIFT_R(4) PSIFT_R(5) PSIFT_R(6) PSIFT_R(7) PSIFT_R(8)
     PSIFT_R(9) PSIFT_R(10) PSIFT_R(11) PSIFT_R(12) PSIFT_R(13) PSIFT_R(14) PSIFT_R(15)
 #undef PSIFT_R
@@ -201,14 +295,19 @@ static cudaError_t launch_blur_mode(int radius, const ImagePlan* plans, int n, i
 // Host entry: mode 0 = level blur (octave, level >= 1); modes 1..4 = octave-0 base.
 cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
                         int level, int down_level, int max_h, int max_w, cudaStream_t st) {
-  Taps t;
-  for (int i = 0; i < kMaxTaps; ++i) t.w[i] = i <= 2 * radius ? taps_host[i] : 0.0f;
+  Taps2 t;
+  for (int i = 0; i < kMaxTaps; ++i) {
+    const float v = i <= 2 * radius ? taps_host[i] : 0.0f;
+    t.w[i] = make_float2(v, v);
+  }
+  t.one = make_float2(1.0f, 1.0f);
+  const int zrev = (octave * 8 + level) & 1;
   switch (mode) {
-    case MODE_LEVEL: return launch_blur_mode<MODE_LEVEL>(radius, plans, n, octave, level, down_level, t, max_h, max_w, st);
-    case MODE_INIT_F32: return launch_blur_mode<MODE_INIT_F32>(radius, plans, n, octave, level, down_level, t, max_h, max_w, st);
-    case MODE_INIT_U8: return launch_blur_mode<MODE_INIT_U8>(radius, plans, n, octave, level, down_level, t, max_h, max_w, st);
-    case MODE_INIT_F32_UP: return launch_blur_mode<MODE_INIT_F32_UP>(radius, plans, n, octave, level, down_level, t, max_h, max_w, st);
-    case MODE_INIT_U8_UP: return launch_blur_mode<MODE_INIT_U8_UP>(radius, plans, n, octave, level, down_level, t, max_h, max_w, st);
+    case MODE_LEVEL: return launch_blur_mode<MODE_LEVEL>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_INIT_F32: return launch_blur_mode<MODE_INIT_F32>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_INIT_U8: return launch_blur_mode<MODE_INIT_U8>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_INIT_F32_UP: return launch_blur_mode<MODE_INIT_F32_UP>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_INIT_U8_UP: return launch_blur_mode<MODE_INIT_U8_UP>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
     default: return cudaErrorInvalidValue;
   }
 }

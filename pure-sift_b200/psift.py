@@ -151,6 +151,10 @@ _SIGS = {
                                   C.c_uint32, C.c_float, C.c_uint64, C.c_void_p]),
     "psift_mlp_train_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                       C.c_uint32, C.c_float, C.c_uint64, C.c_void_p]),
+    "psift_gaussian_blur": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t, C.c_float,
+                                      C.c_void_p]),
+    "psift_build_pyramid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
+                                      C.POINTER(CSiftConfig), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
     "psift_compute_descriptors": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p,
                                             C.c_uint32, C.c_int32, C.POINTER(CFeatures)]),
     "psift_summarize_tracking": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
@@ -790,3 +794,41 @@ class FeatureCatalog:
             hits.append(CatalogSearchHit(e.id, e.width, e.height, len(e.features), v, tracking, sim_tf, hom_tf))
         hits.sort(key=lambda h: (-h.tracking.match_count, -h.tracking.inlier_ratio, -h.coarse_votes, h.id))
         return hits[:top_k]
+
+
+def gaussian_blur(img: np.ndarray, sigma: float, ctx: Context | None = None) -> np.ndarray:
+    """``gaussian_blur`` (src/pipeline.rs:314-425) on the GPU."""
+    ctx = ctx or default_context()
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    out = np.empty_like(img)
+    h, w = img.shape
+    ctx.check(ctx.lib.psift_gaussian_blur(ctx.handle, img.ctypes.data, h, w, w, float(sigma), out.ctypes.data))
+    return out
+
+
+def build_pyramid(img: np.ndarray, config: "SiftConfig" = None, ctx: Context | None = None):
+    """``build_scale_space_pyramid_with_options`` (src/pipeline.rs:550-638) on the GPU.
+
+    Returns a list of (gaussian, dog) per octave: arrays of shape
+    (scales+3, h, w) and (scales+2, h, w)."""
+    ctx = ctx or default_context()
+    config = config or SiftConfig()
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    h, w = img.shape
+    cc = config.to_c()
+    dims = np.zeros(2 * max(cc.octaves, 1), np.uint32)
+    n = C.c_uint32()
+    ctx.check(ctx.lib.psift_build_pyramid(ctx.handle, img.ctypes.data, h, w, w, C.byref(cc), None, 0,
+                                          dims.ctypes.data, C.byref(n)))
+    S = cc.scales
+    sizes = [(int(dims[2 * o]), int(dims[2 * o + 1])) for o in range(n.value)]
+    total = sum((2 * S + 5) * a * b for a, b in sizes)
+    buf = np.empty(max(total, 1), np.float32)
+    ctx.check(ctx.lib.psift_build_pyramid(ctx.handle, img.ctypes.data, h, w, w, C.byref(cc), buf.ctypes.data, total,
+                                          dims.ctypes.data, C.byref(n)))
+    out, off = [], 0
+    for a, b in sizes:
+        blk = buf[off: off + (2 * S + 5) * a * b].reshape(2 * S + 5, a, b)
+        out.append((blk[: S + 3], blk[S + 3:]))
+        off += (2 * S + 5) * a * b
+    return out
