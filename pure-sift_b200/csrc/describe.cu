@@ -243,18 +243,31 @@ __global__ void __launch_bounds__(1024) feature_scan_kernel(const ImagePlan* __r
 
 // Grid (ceil(sel_cap / 4), images), 128 threads: one warp per keypoint, one
 // descriptor per orientation.
+//
+// The window is walked in chunks of 256 pixels.  Phase 1: each lane tests 8
+// pixels against the rotated 4x4-cell square (the reference's r_bin/c_bin test,
+// about half of the window passes) and the passing ones are compacted into the
+// warp's queue.  Phase 2: full lanes take queued pixels for the gradient,
+// weight and trilinear binning.  Histograms: 16 private columns per warp
+// ([bin][16], 8 KB); lanes l and l + 16 share column l and add in two fixed
+// phases, so every bin's sum has one fixed order (deterministic).
+constexpr int kDescChunk = 256;
+constexpr int kHistCols = 16;
+constexpr int kDescSmemPerWarp = kDescLen * kHistCols * 4 + kDescChunk * 4;
+
 __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const ImagePlan* __restrict__ plans,
                                                                      DescribeParams prm) {
   const ImagePlan& P = plans[blockIdx.y];
-  extern __shared__ float s_dyn[];
+  extern __shared__ float4 s_dyn4[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t i = blockIdx.x * kDescWarps + warp;
   if (i >= *P.sel_count) return;
   const uint32_t fcount = *P.feat_count;
   const uint32_t f0 = P.feat_offsets[i];
   if (f0 >= fcount) return;
-  float (*hist)[32] = reinterpret_cast<float (*)[32]>(s_dyn + warp * (kDescLen * 32 + kDescLen));
-  float* desc = s_dyn + warp * (kDescLen * 32 + kDescLen) + kDescLen * 32;
+  char* wbase = reinterpret_cast<char*>(s_dyn4) + warp * kDescSmemPerWarp;
+  float (*hist)[kHistCols] = reinterpret_cast<float (*)[kHistCols]>(wbase);
+  uint32_t* queue = reinterpret_cast<uint32_t*>(wbase + kDescLen * kHistCols * 4);
 
   const psift_keypoint kp = P.sel[i];
   OctKp ok = to_octave(P, kp);
@@ -276,95 +289,164 @@ __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const Image
   const int x_min = max(cx - max_radius, 1);
   const int x_max = max(min(cx + max_radius, O.w - 2), 1);
   const int wx = x_max - x_min + 1;
-  const int n = (y_max >= y_min && x_max >= x_min) ? (y_max - y_min + 1) * wx : 0;
+  const int n = (y_max >= y_min && x_max >= x_min && O.h >= 3 && O.w >= 3) ? (y_max - y_min + 1) * wx : 0;
   const float bin_per_rad = 8.0f / two_pi;
-  const bool planes_ok = O.h >= 3 && O.w >= 3;
+  // the lane's first window pixel; later ones follow by stepping 32 pixels
+  const int y_first = y_min + (wx > 0 ? lane / wx : 0);
+  const int x_first = x_min + (wx > 0 ? lane % wx : 0);
+  const int col = lane & (kHistCols - 1), half = lane >> 4;
 
   for (uint32_t q = 0; q < nori; ++q) {
     const uint32_t f = f0 + q;
     if (f >= fcount) break;
     const float theta = P.oris[(size_t)i * 4 + q];
-    for (int b = 0; b < kDescLen; ++b) hist[b][lane] = 0.0f;
+#pragma unroll 4
+    for (int b = lane; b < kDescLen * kHistCols / 4; b += 32)
+      reinterpret_cast<float4*>(&hist[0][0])[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float cos_t = cosf(theta), sin_t = sinf(theta);
-    for (int t = lane; planes_ok && t < n; t += 32) {
-      const int yy = y_min + t / wx, xx = x_min + t % wx;
-      const float dy = (float)yy - ok.y;
-      const float dx = (float)xx - ok.x;
-      const float r_rot = (dx * cos_t + dy * sin_t) * inv_hw;
-      const float c_rot = (-dx * sin_t + dy * cos_t) * inv_hw;
-      const float r_bin = r_rot + 4.0f * 0.5f - 0.5f;
-      const float c_bin = c_rot + 4.0f * 0.5f - 0.5f;
-      if (r_bin <= -1.0f || r_bin >= 4.0f || c_bin <= -1.0f || c_bin >= 4.0f) continue;
-      float m, ang;
-      grad_at(g, O.pitch, xx, yy, m, ang, two_pi);
-      if (m <= 1e-7f) continue;
-      const float w_gauss = expf((r_rot * r_rot + c_rot * c_rot) * exp_scale);
-      const float wm = m * w_gauss;
-      const float rel = rem_2pi(ang - theta, two_pi);
-      const float o_bin = rel * bin_per_rad;
-      const int r0 = (int)floorf(r_bin), c0 = (int)floorf(c_bin), o0 = (int)floorf(o_bin);
-      const float dr = r_bin - (float)r0, dc = c_bin - (float)c0, dof = o_bin - (float)o0;
+    int yy = y_first, xx = x_first;
+    for (int base = 0; base < n; base += kDescChunk) {
+      // Phase 1: rotated-square test for 8 pixels per lane.
+      uint32_t m = 0, packed[8];
 #pragma unroll
-      for (int ir = 0; ir <= 1; ++ir) {
-        const int rb = r0 + ir;
-        if (rb < 0 || rb >= 4) continue;
-        const float wr = ir == 0 ? 1.0f - dr : dr;
+      for (int k = 0; k < 8; ++k) {
+        const int t = base + 32 * k + lane;
+        const int py = yy, px = xx;
+        packed[k] = ((uint32_t)py << 16) | (uint32_t)px;
+        xx += 32;
+        while (xx > x_max) {
+          xx -= wx;
+          ++yy;
+        }
+        if (t < n) {
+          const float dy = (float)py - ok.y;
+          const float dx = (float)px - ok.x;
+          const float r_bin = (dx * cos_t + dy * sin_t) * inv_hw + 4.0f * 0.5f - 0.5f;
+          const float c_bin = (-dx * sin_t + dy * cos_t) * inv_hw + 4.0f * 0.5f - 0.5f;
+          if (!(r_bin <= -1.0f || r_bin >= 4.0f || c_bin <= -1.0f || c_bin >= 4.0f)) m |= 1u << k;
+        }
+      }
+      const uint32_t c = __popc(m);
+      uint32_t incl = c;
 #pragma unroll
-        for (int ic = 0; ic <= 1; ++ic) {
-          const int cb = c0 + ic;
-          if (cb < 0 || cb >= 4) continue;
-          const float wc = ic == 0 ? 1.0f - dc : dc;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int total = (int)__shfl_sync(0xffffffffu, incl, 31);
+      uint32_t pos = incl - c;
 #pragma unroll
-          for (int io = 0; io <= 1; ++io) {
-            const int ob = (o0 + io) & 7;
-            const float wo = io == 0 ? 1.0f - dof : dof;
-            hist[(rb * 4 + cb) * 8 + ob][lane] += wm * wr * wc * wo;
+      for (int k = 0; k < 8; ++k)
+        if (m & (1u << k)) queue[pos++] = packed[k];
+      __syncwarp();
+      // Phase 2: queued pixels, all lanes busy.
+      for (int e0 = 0; e0 < total; e0 += 32) {
+        const int e = e0 + lane;
+        bool live = false;
+        int r0 = 0, c0 = 0, o0 = 0;
+        float dr = 0.0f, dc = 0.0f, dof = 0.0f, wm = 0.0f;
+        if (e < total) {
+          const uint32_t pk = queue[e];
+          const int py = (int)(pk >> 16), px = (int)(pk & 0xFFFFu);
+          const float dy = (float)py - ok.y;
+          const float dx = (float)px - ok.x;
+          const float r_rot = (dx * cos_t + dy * sin_t) * inv_hw;
+          const float c_rot = (-dx * sin_t + dy * cos_t) * inv_hw;
+          const float r_bin = r_rot + 4.0f * 0.5f - 0.5f;
+          const float c_bin = c_rot + 4.0f * 0.5f - 0.5f;
+          float mg, ang;
+          grad_at(g, O.pitch, px, py, mg, ang, two_pi);
+          if (mg > 1e-7f) {
+            live = true;
+            const float w_gauss = expf((r_rot * r_rot + c_rot * c_rot) * exp_scale);
+            wm = mg * w_gauss;
+            const float rel = rem_2pi(ang - theta, two_pi);
+            const float o_bin = rel * bin_per_rad;
+            r0 = (int)floorf(r_bin);
+            c0 = (int)floorf(c_bin);
+            o0 = (int)floorf(o_bin);
+            dr = r_bin - (float)r0;
+            dc = c_bin - (float)c0;
+            dof = o_bin - (float)o0;
           }
         }
+#pragma unroll
+        for (int hp = 0; hp < 2; ++hp) {
+          if (live && half == hp) {
+#pragma unroll
+            for (int ir = 0; ir <= 1; ++ir) {
+              const int rb = r0 + ir;
+              if (rb < 0 || rb >= 4) continue;
+              const float wr = ir == 0 ? 1.0f - dr : dr;
+#pragma unroll
+              for (int ic = 0; ic <= 1; ++ic) {
+                const int cb = c0 + ic;
+                if (cb < 0 || cb >= 4) continue;
+                const float wc = ic == 0 ? 1.0f - dc : dc;
+                float* cell = &hist[(rb * 4 + cb) * 8][col];
+                const float wrc = wm * wr * wc;
+                cell[(o0 & 7) * kHistCols] += wrc * (1.0f - dof);
+                cell[((o0 + 1) & 7) * kHistCols] += wrc * dof;
+              }
+            }
+          }
+          __syncwarp();
+        }
       }
     }
-    __syncwarp();
-    for (int b = lane; b < kDescLen; b += 32) {
-      float s = 0.0f;
-      for (int j = 0; j < 32; ++j) s += hist[b][j];
-      desc[b] = s;
+    // Bin b = lane + 32k: sum of the 16 columns, read rotated by b >> 1 so the
+    // 32 lanes hit 32 distinct banks (a fixed order per bin: deterministic).
+    float d[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int b = lane + 32 * k;
+      float acc = 0.0f;
+#pragma unroll
+      for (int j = 0; j < kHistCols; ++j) acc += hist[b][(j + (b >> 1)) & (kHistCols - 1)];
+      d[k] = acc;
     }
     __syncwarp();
+    // L2 -> clamp 0.2 -> L2 (src/pipeline.rs:1462-1477); sums as xor-butterfly
+    // reductions (same on every lane, deterministic).
+    float n1 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n1 += __shfl_xor_sync(0xffffffffu, n1, o);
+    n1 = sqrtf(n1);
+    if (n1 > 1e-7f) {
+      const float inv1 = 1.0f / n1;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) d[k] = fminf(d[k] * inv1, 0.2f);
+      float n2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+      n2 = sqrtf(n2);
+      if (n2 > 1e-7f) {
+        const float inv2 = 1.0f / n2;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) d[k] *= inv2;
+      }
+    }
+    if (prm.descriptor_kind == 1) {
+      // to_rootsift_descriptor (src/pipeline.rs:1012-1019)
+      float l1 = fmaxf(d[0], 0.0f) + fmaxf(d[1], 0.0f) + fmaxf(d[2], 0.0f) + fmaxf(d[3], 0.0f);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) l1 += __shfl_xor_sync(0xffffffffu, l1, o);
+      if (l1 > 1e-7f) {
+        const float inv = 1.0f / l1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) d[k] = sqrtf(fmaxf(d[k], 0.0f) * inv);
+      }
+    }
+    float* dst = P.fdesc + (size_t)f * kDescLen;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dst[lane + 32 * k] = d[k];
     if (lane == 0) {
-      // L2 -> clamp 0.2 -> L2 (src/pipeline.rs:1462-1477), sequential sums.
-      float n1 = 0.0f;
-      for (int b = 0; b < kDescLen; ++b) n1 += desc[b] * desc[b];
-      n1 = sqrtf(n1);
-      if (n1 > 1e-7f) {
-        const float inv1 = 1.0f / n1;
-        for (int b = 0; b < kDescLen; ++b) desc[b] = fminf(desc[b] * inv1, 0.2f);
-        float n2 = 0.0f;
-        for (int b = 0; b < kDescLen; ++b) n2 += desc[b] * desc[b];
-        n2 = sqrtf(n2);
-        if (n2 > 1e-7f) {
-          const float inv2 = 1.0f / n2;
-          for (int b = 0; b < kDescLen; ++b) desc[b] *= inv2;
-        }
-      }
-      if (prm.descriptor_kind == 1) {
-        // to_rootsift_descriptor (src/pipeline.rs:1012-1019)
-        float l1 = 0.0f;
-        for (int b = 0; b < kDescLen; ++b) l1 += fmaxf(desc[b], 0.0f);
-        if (l1 > 1e-7f) {
-          const float inv = 1.0f / l1;
-          for (int b = 0; b < kDescLen; ++b) desc[b] = sqrtf(fmaxf(desc[b], 0.0f) * inv);
-        }
-      }
       P.fx[f] = kp.x;
       P.fy[f] = kp.y;
       P.fscale[f] = kp.scale;
       P.fresp[f] = kp.response;
       P.fori[f] = theta;
     }
-    __syncwarp();
-    float4* dst = reinterpret_cast<float4*>(P.fdesc + (size_t)f * kDescLen);
-    dst[lane] = reinterpret_cast<const float4*>(desc)[lane];
-    __syncwarp();
   }
 }
 
@@ -382,7 +464,7 @@ cudaError_t launch_feature_scan(const ImagePlan* plans, int n, uint32_t max_feat
 
 cudaError_t launch_descriptor(const ImagePlan* plans, int n, uint32_t sel_cap, const DescribeParams& prm,
                               cudaStream_t st) {
-  const size_t smem = sizeof(float) * kDescWarps * (kDescLen * 32 + kDescLen);
+  const size_t smem = (size_t)kDescWarps * kDescSmemPerWarp;
   cudaError_t e = ensure_smem_attr((const void*)descriptor_kernel, smem);
   if (e != cudaSuccess) return e;
   dim3 grid((sel_cap + kDescWarps - 1) / kDescWarps, n);

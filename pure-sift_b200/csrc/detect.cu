@@ -162,6 +162,8 @@ psift_status build_job(psift_ctx* ctx, const std::vector<ImageDesc>& imgs, const
   for (int i = 0; i < n; ++i) {
     job.n_oct[i] = plan_octaves(imgs[i].h, imgs[i].w, (int)cfg.octaves, cfg.upsample_first_octave != 0,
                                 &job.oct[(size_t)i * kMaxOctaves]);
+    if (job.n_oct[i] > 0 && (job.oct[(size_t)i * kMaxOctaves].h > 65535 || job.oct[(size_t)i * kMaxOctaves].w > 65535))
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "octave-0 side above 65535 pixels is not supported");
     int rows = 0;
     for (int o = 0; o < job.n_oct[i]; ++o) {
       const HostOctave& O = job.oct[(size_t)i * kMaxOctaves + o];

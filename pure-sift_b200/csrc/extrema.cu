@@ -82,50 +82,46 @@ __device__ __forceinline__ void refine3d(const float* __restrict__ p, const floa
 }
 
 // Full acceptance test for pixel (x, y) of slice `c` (rows already offset to y).
+// The reference's comparison chain (is_greater/less_than_patch3x3 over the
+// current, previous and next slices) is evaluated on loads issued together: the
+// 8 same-slice neighbours first, then, only if they pass, the 18 of the other
+// two slices.  Short-circuiting does not change the outcome (all must hold).
 __device__ __forceinline__ bool accept_pixel(const float* __restrict__ p, const float* __restrict__ c,
                                              const float* __restrict__ n, long long pitch, int x, float thr) {
   const float v = c[x];
   if (fabsf(v) <= thr) return false;
   const float* ca = c - pitch;
   const float* cb = c + pitch;
-  bool ext;
-  if (v > 0.0f) {
-    ext = v > c[x - 1] && v > c[x + 1] && v > ca[x - 1] && v > ca[x] && v > ca[x + 1] && v > cb[x - 1] &&
-          v > cb[x] && v > cb[x + 1];
-    if (ext) {
-      const float* pa = p - pitch;
-      const float* pb = p + pitch;
-      ext = v > pa[x - 1] && v > pa[x] && v > pa[x + 1] && v > p[x - 1] && v > p[x] && v > p[x + 1] &&
-            v > pb[x - 1] && v > pb[x] && v > pb[x + 1];
-    }
-    if (ext) {
-      const float* na = n - pitch;
-      const float* nb = n + pitch;
-      ext = v > na[x - 1] && v > na[x] && v > na[x + 1] && v > n[x - 1] && v > n[x] && v > n[x + 1] &&
-            v > nb[x - 1] && v > nb[x] && v > nb[x + 1];
-    }
-  } else {
-    ext = v < c[x - 1] && v < c[x + 1] && v < ca[x - 1] && v < ca[x] && v < ca[x + 1] && v < cb[x - 1] &&
-          v < cb[x] && v < cb[x + 1];
-    if (ext) {
-      const float* pa = p - pitch;
-      const float* pb = p + pitch;
-      ext = v < pa[x - 1] && v < pa[x] && v < pa[x + 1] && v < p[x - 1] && v < p[x] && v < p[x + 1] &&
-            v < pb[x - 1] && v < pb[x] && v < pb[x + 1];
-    }
-    if (ext) {
-      const float* na = n - pitch;
-      const float* nb = n + pitch;
-      ext = v < na[x - 1] && v < na[x] && v < na[x + 1] && v < n[x - 1] && v < n[x] && v < n[x + 1] &&
-            v < nb[x - 1] && v < nb[x] && v < nb[x + 1];
-    }
+  float nb[9];
+  nb[0] = ca[x - 1]; nb[1] = ca[x]; nb[2] = ca[x + 1];
+  nb[3] = c[x - 1];  nb[4] = c[x + 1];
+  nb[5] = cb[x - 1]; nb[6] = cb[x]; nb[7] = cb[x + 1];
+  const bool pos = v > 0.0f;
+  bool ext = true;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) ext = ext && (pos ? v > nb[k] : v < nb[k]);
+  if (!ext) return false;
+  float pn[18];
+  {
+    const float* pa = p - pitch;
+    const float* pb = p + pitch;
+    const float* na = n - pitch;
+    const float* nbp = n + pitch;
+    pn[0] = pa[x - 1];  pn[1] = pa[x];  pn[2] = pa[x + 1];
+    pn[3] = p[x - 1];   pn[4] = p[x];   pn[5] = p[x + 1];
+    pn[6] = pb[x - 1];  pn[7] = pb[x];  pn[8] = pb[x + 1];
+    pn[9] = na[x - 1];  pn[10] = na[x]; pn[11] = na[x + 1];
+    pn[12] = n[x - 1];  pn[13] = n[x];  pn[14] = n[x + 1];
+    pn[15] = nbp[x - 1]; pn[16] = nbp[x]; pn[17] = nbp[x + 1];
   }
+#pragma unroll
+  for (int k = 0; k < 18; ++k) ext = ext && (pos ? v > pn[k] : v < pn[k]);
   if (!ext) return false;
   // passes_hessian_edge_test (src/pipeline.rs:664-687)
   {
-    const float dxx = c[x + 1] - 2.0f * v + c[x - 1];
-    const float dyy = cb[x] - 2.0f * v + ca[x];
-    const float dxy = 0.25f * ((cb[x + 1] - cb[x - 1]) - (ca[x + 1] - ca[x - 1]));
+    const float dxx = nb[4] - 2.0f * v + nb[3];
+    const float dyy = nb[6] - 2.0f * v + nb[1];
+    const float dxy = 0.25f * ((nb[7] - nb[5]) - (nb[2] - nb[0]));
     const float trace = dxx + dyy;
     const float det = dxx * dyy - dxy * dxy;
     const float ratio = (11.0f * 11.0f) / 10.0f;
@@ -136,13 +132,42 @@ __device__ __forceinline__ bool accept_pixel(const float* __restrict__ p, const 
   return fabsf(interp) > thr;
 }
 
-// Grid (max_h, scales, images), 256 threads: one block per (row, slice, image).
-__global__ void __launch_bounds__(256) extrema_mark_kernel(const ImagePlan* __restrict__ plans, int octave,
-                                                           ExtremaParams prm) {
+// Grid (ceil(max_h / 4), scales, images), 128 threads: one warp per (row,
+// slice, image), no block-wide barriers.  The warp walks its row in 256-pixel
+// spans (a lane reads 8 pixels as two 128-bit loads, 128 pixels apart; the
+// next span's loads are issued before the current span is processed); a span is
+// exactly 8 mask words.
+//   A. streaming: pixels with |v| > threshold (the reference's first test, a
+//      small fraction of the row) become candidates; a span without any writes
+//      zero words;
+//   B. otherwise the candidates are compacted into the warp's shared-memory
+//      queue and the warp runs the full 26-neighbour / Hessian / refinement
+//      test on them only, setting bits of the span's 8 mask words.
+constexpr int kMarkWarps = 4;
+constexpr int kMarkSpan = 256;  // pixels per warp step
+
+__device__ __forceinline__ void mark_load_span(const float* __restrict__ Dc, int xb, int lane, int w, float4 (&v)[2]) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int x0 = xb + h * 128 + 4 * lane;
+    if (x0 + 3 < w) {
+      v[h] = *reinterpret_cast<const float4*>(Dc + x0);
+    } else {
+      v[h] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (x0 + 0 < w) v[h].x = Dc[x0 + 0];
+      if (x0 + 1 < w) v[h].y = Dc[x0 + 1];
+      if (x0 + 2 < w) v[h].z = Dc[x0 + 2];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kMarkWarps * 32) extrema_mark_kernel(const ImagePlan* __restrict__ plans,
+                                                                       int octave, ExtremaParams prm) {
   const ImagePlan& P = plans[blockIdx.z];
   if (octave >= P.n_oct) return;
   const OctaveDev& O = P.oct[octave];
-  const int y = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int y = blockIdx.x * kMarkWarps + warp;
   if (y >= O.h) return;
   const int s = blockIdx.y + 1;
   const long long ps = O.plane_stride;
@@ -150,28 +175,70 @@ __global__ void __launch_bounds__(256) extrema_mark_kernel(const ImagePlan* __re
   const float* Dc = O.d + (long long)s * ps + (long long)y * O.pitch;
   const float* Dn = O.d + (long long)(s + 1) * ps + (long long)y * O.pitch;
   uint32_t* mrow = O.masks + ((long long)(s - 1) * O.h + y) * O.words;
-  const int lane = threadIdx.x & 31;
-  uint32_t cnt = 0;
+  const float thr = prm.threshold;
   const bool row_ok = y >= 1 && y < O.h - 1;
-  for (int xb = 0; xb < O.words * 32; xb += 256) {
-    const int x = xb + threadIdx.x;
-    bool acc = false;
-    if (row_ok && x >= 1 && x < O.w - 1) acc = accept_pixel(Dp, Dc, Dn, O.pitch, x, prm.threshold);
-    const unsigned bal = __ballot_sync(0xffffffffu, acc);
-    const int word = x >> 5;
-    if (lane == 0 && word < O.words) {
-      mrow[word] = bal;
-      cnt += __popc(bal);
+  const int w = O.w;
+  const int span_end = O.words * 32;
+
+  __shared__ uint16_t s_q[kMarkWarps][kMarkSpan];
+  __shared__ uint32_t s_mask[kMarkWarps][kMarkSpan / 32];
+  uint16_t* q = s_q[warp];
+  uint32_t* wm = s_mask[warp];
+  uint32_t cnt = 0;
+
+  float4 cur[2], nxt[2];
+  if (row_ok) mark_load_span(Dc, 0, lane, w, cur);
+  for (int xb = 0; xb < span_end; xb += kMarkSpan) {
+    if (row_ok && xb + kMarkSpan < span_end) mark_load_span(Dc, xb + kMarkSpan, lane, w, nxt);
+    uint32_t m = 0;  // bit 4h + i: pixel xb + 128 h + 4 lane + i
+    if (row_ok) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const float e[4] = {cur[h].x, cur[h].y, cur[h].z, cur[h].w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int x = xb + h * 128 + 4 * lane + i;
+          // the reference's first rejection is |v| <= threshold (NaN continues)
+          if (x >= 1 && x < w - 1 && !(fabsf(e[i]) <= thr)) m |= 1u << (4 * h + i);
+        }
+      }
     }
+    uint32_t word_bits = 0;  // lane < 8: mask word (xb >> 5) + lane
+    if (__any_sync(0xffffffffu, m != 0)) {
+      const uint32_t c = __popc(m);
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int total = (int)__shfl_sync(0xffffffffu, incl, 31);
+      uint32_t pos = incl - c;
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        if (m & (1u << b)) q[pos++] = (uint16_t)((b >> 2) * 128 + 4 * lane + (b & 3));
+      if (lane < 8) wm[lane] = 0;
+      __syncwarp();
+      for (int i = lane; i < total; i += 32) {
+        const int off = q[i];
+        if (accept_pixel(Dp, Dc, Dn, O.pitch, xb + off, thr)) atomicOr(&wm[off >> 5], 1u << (off & 31));
+      }
+      __syncwarp();
+      if (lane < 8) word_bits = wm[lane];
+      __syncwarp();
+    }
+    if (lane < 8) {
+      const int word = (xb >> 5) + lane;
+      if (word < O.words) {
+        mrow[word] = word_bits;
+        cnt += __popc(word_bits);
+      }
+    }
+    cur[0] = nxt[0];
+    cur[1] = nxt[1];
   }
-  __shared__ uint32_t s_cnt[8];
-  if (lane == 0) s_cnt[threadIdx.x >> 5] = cnt;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t t = 0;
-    for (int i = 0; i < 8; ++i) t += s_cnt[i];
-    P.row_counts[O.row_base + (s - 1) * O.h + y] = t;
-  }
+  cnt = __reduce_add_sync(0xffffffffu, cnt);
+  if (lane == 0) P.row_counts[O.row_base + (s - 1) * O.h + y] = cnt;
 }
 
 // Block-wide exclusive scan helper for 1024 threads; returns the block total.
@@ -371,8 +438,8 @@ __global__ void __launch_bounds__(1024) select_topk_kernel(const ImagePlan* __re
 
 cudaError_t launch_extrema_mark(const ImagePlan* plans, int n, int octave, int max_h, const ExtremaParams& prm,
                                 cudaStream_t st) {
-  dim3 grid(max_h, prm.scales, n);
-  extrema_mark_kernel<<<grid, 256, 0, st>>>(plans, octave, prm);
+  dim3 grid((max_h + kMarkWarps - 1) / kMarkWarps, prm.scales, n);
+  extrema_mark_kernel<<<grid, kMarkWarps * 32, 0, st>>>(plans, octave, prm);
   return cudaGetLastError();
 }
 
