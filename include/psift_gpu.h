@@ -154,13 +154,28 @@ psift_status psift_compute_descriptors(psift_ctx* ctx, const float* image, uint3
  * per-image feature counts written to the device array d_counts.  No host
  * synchronisation; work is queued on the context's stream. */
 typedef struct psift_image_u8 {
-  const uint8_t* data;   /* device pointer */
+  const uint8_t* data;   /* device pointer (host pointer for the host batch entry) */
   uint32_t height, width;
   size_t row_stride;     /* elements */
 } psift_image_u8;
 psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_image_u8* images,
                                                 uint32_t n, const psift_sift_config* cfg,
                                                 psift_features* outs, uint32_t* d_counts);
+
+/* Host-pointer batch of u8 images (psift_image_u8.data are host pointers,
+ * row_stride in bytes); features into the host arrays of outs[i] (capacity per
+ * image, count written back).  One launch per stage for the whole batch, two
+ * chunks on two streams so transfers overlap kernels, one final synchronisation.
+ * Page-locked inputs/outputs (psift_host_alloc, cudaMallocHost, cudaHostRegister)
+ * are transferred directly.  No counterpart in the reference (which handles one
+ * image per Sift::detect_and_compute call); per image, results equal
+ * psift_detect_and_compute_u8.  If any image's features exceed its capacity the
+ * call returns PSIFT_ERR_CAPACITY with that image's count set to the size needed. */
+psift_status psift_detect_and_compute_u8_batch(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
+                                               const psift_sift_config* cfg, psift_features* outs);
+/* Page-locked host memory for the batch entry's inputs and outputs. */
+psift_status psift_host_alloc(psift_ctx* ctx, size_t bytes, void** out);
+psift_status psift_host_free(psift_ctx* ctx, void* p);
 
 /* ---------------------------------------------------------------- matching */
 #define PSIFT_PRECISION_FP32 0        /* exact f32 distances, the reference's summation order */

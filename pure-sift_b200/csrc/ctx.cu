@@ -71,17 +71,19 @@ static cudaEvent_t take_event(psift_ctx* ctx) {
   return e;
 }
 
-StageScope::StageScope(psift_ctx* c, int s) : ctx(c), stage(s) {
+StageScope::StageScope(psift_ctx* c, int s) : StageScope(c, s, c ? c->stream : nullptr) {}
+
+StageScope::StageScope(psift_ctx* c, int s, cudaStream_t stream) : ctx(c), stage(s), st(stream) {
   if (ctx && ctx->timer.enabled) {
     start = take_event(ctx);
-    cudaEventRecord(start, ctx->stream);
+    cudaEventRecord(start, st);
   }
 }
 
 StageScope::~StageScope() {
   if (start) {
     cudaEvent_t end = take_event(ctx);
-    cudaEventRecord(end, ctx->stream);
+    cudaEventRecord(end, st);
     ctx->timer.pending.push_back({stage, {start, end}});
   }
 }
@@ -89,6 +91,7 @@ StageScope::~StageScope() {
 static void drain_timer(psift_ctx* ctx) {
   if (ctx->timer.pending.empty()) return;
   cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->stream2);
   for (auto& p : ctx->timer.pending) {
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
@@ -156,7 +159,19 @@ psift_status psift_ctx_create(int device, psift_ctx** out) {
     delete ctx;
     return PSIFT_ERR_CUDA;
   }
+  if (cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return PSIFT_ERR_CUDA;
+  }
   if (cudaMalloc(&ctx->d_error, 64) != cudaSuccess || cudaMemset(ctx->d_error, 0, 64) != cudaSuccess) {
+    cudaStreamDestroy(ctx->stream2);
+    cudaEventDestroy(ctx->ev_fork);
+    cudaEventDestroy(ctx->ev_join);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PSIFT_ERR_OUT_OF_MEMORY;
@@ -169,6 +184,7 @@ psift_status psift_ctx_destroy(psift_ctx* ctx) {
   if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->stream2);
   if (ctx->arena.base) cudaFree(ctx->arena.base);
   if (ctx->io.base) cudaFree(ctx->io.base);
   if (ctx->pinned.base) cudaFreeHost(ctx->pinned.base);
@@ -178,6 +194,9 @@ psift_status psift_ctx_destroy(psift_ctx* ctx) {
     cudaEventDestroy(p.second.second);
   }
   for (cudaEvent_t e : ctx->timer.pool) cudaEventDestroy(e);
+  cudaEventDestroy(ctx->ev_fork);
+  cudaEventDestroy(ctx->ev_join);
+  cudaStreamDestroy(ctx->stream2);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PSIFT_OK;

@@ -248,11 +248,13 @@ psift_status build_job(psift_ctx* ctx, const std::vector<ImageDesc>& imgs, const
 
 // Queue every stage of the path for the batch (no host synchronisation).
 // stop_after_keypoints: end after extrema_emit (Sift::detect_keypoints).
-psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_config& cfg, bool stop_after_keypoints) {
-  cudaStream_t st = ctx->stream;
+psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_config& cfg, bool stop_after_keypoints,
+                           cudaStream_t stream = nullptr, bool plans_uploaded = false) {
+  cudaStream_t st = stream ? stream : ctx->stream;
   const int n = job.n;
   const int S = (int)cfg.scales;
-  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice, st));
+  if (!plans_uploaded)
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice, st));
   const SigmaSchedule sc = make_schedule(S, cfg.upsample_first_octave != 0);
   int max_oct = 0;
   for (int i = 0; i < n; ++i) max_oct = std::max(max_oct, job.n_oct[i]);
@@ -274,7 +276,7 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
   };
   // Octave-0 base: luma -> f32 (+ 2x bilinear upsample) + initial blur.
   {
-    StageScope sc_pyr(ctx, STAGE_PYRAMID);
+    StageScope sc_pyr(ctx, STAGE_PYRAMID, st);
     int mh, mw;
     max_dims(0, mh, mw);
     const bool up = cfg.upsample_first_octave != 0;
@@ -298,21 +300,21 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
     int mh, mw;
     max_dims(o, mh, mw);
     {
-      StageScope sc_pyr(ctx, STAGE_PYRAMID);
+      StageScope sc_pyr(ctx, STAGE_PYRAMID, st);
       for (int s = 1; s <= S + 2; ++s) {
         cudaError_t e = launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, n, o, s, S, mh, mw, st);
         ctx->launches++;
         if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
       }
     }
-    StageScope sc_x(ctx, STAGE_EXTREMA);
+    StageScope sc_x(ctx, STAGE_EXTREMA, st);
     cudaError_t e = launch_extrema_mark(job.d_plans, n, o, mh, xp, st);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "extrema_mark");
   }
   cudaError_t e;
   {
-  StageScope sc_x2(ctx, STAGE_EXTREMA);
+  StageScope sc_x2(ctx, STAGE_EXTREMA, st);
   e = launch_row_scan(job.d_plans, n, job.kp_cap, ctx->d_error, st);
   ctx->launches++;
   if (e != cudaSuccess) return cuda_error(ctx, e, "row_scan");
@@ -326,20 +328,20 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
   }
   if (stop_after_keypoints) return PSIFT_OK;
   {
-    StageScope sc_s(ctx, STAGE_SELECT);
+    StageScope sc_s(ctx, STAGE_SELECT, st);
     e = launch_select_topk(job.d_plans, n, job.kp_cap, cfg.max_features, ctx->d_error, st);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "select_topk");
   }
   DescribeParams dp{S, cfg.max_features, cfg.descriptor_kind};
   {
-    StageScope sc_o(ctx, STAGE_ORIENTATION);
+    StageScope sc_o(ctx, STAGE_ORIENTATION, st);
     e = launch_orientation(job.d_plans, n, job.sel_cap, dp, st);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "orientation");
   }
   {
-    StageScope sc_d(ctx, STAGE_DESCRIPTOR);
+    StageScope sc_d(ctx, STAGE_DESCRIPTOR, st);
     e = launch_feature_scan(job.d_plans, n, cfg.max_features, st);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "feature_scan");
@@ -381,6 +383,16 @@ psift_status launch_pyramid_only(psift_ctx* ctx, DetectJob& job, const psift_sif
     }
   }
   return PSIFT_OK;
+}
+
+// True when p lies in page-locked host memory (cudaMallocHost / cudaHostRegister).
+bool is_host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
 }
 
 psift_status check_common(psift_ctx* ctx, const psift_sift_config* cfg) {
@@ -535,6 +547,172 @@ psift_status psift_detect_keypoints(psift_ctx* ctx, const float* image, uint32_t
     PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     std::memcpy(out, pin, sizeof(psift_keypoint) * n);
   }
+  return PSIFT_OK;
+}
+
+psift_status psift_host_alloc(psift_ctx* ctx, size_t bytes, void** out) {
+  if (!ctx || !out) return PSIFT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e == cudaSuccess) e = cudaMallocHost(out, bytes ? bytes : 1);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return cuda_error(ctx, e, "cudaMallocHost");
+  }
+  return PSIFT_OK;
+}
+
+psift_status psift_host_free(psift_ctx* ctx, void* p) {
+  if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (p) PSIFT_CUDA_TRY(ctx, cudaFreeHost(p));
+  return PSIFT_OK;
+}
+
+// Host-pointer batch.  Layout of the work:
+//   one workspace for all images (build_job) and one device copy of each image;
+//   the batch is split into two chunks on two streams: chunk c's uploads and
+//   kernels run on stream c, so chunk 1's upload overlaps chunk 0's kernels and
+//   chunk 0's feature download overlaps chunk 1's kernels;
+//   counts come back first (one small copy per image), then exactly the feature
+//   bytes, straight into the caller's arrays when they are page-locked, else
+//   through the context's pinned staging.
+psift_status psift_detect_and_compute_u8_batch(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
+                                               const psift_sift_config* cfg, psift_features* outs) {
+  psift_status st = check_common(ctx, cfg);
+  if (st != PSIFT_OK) return st;
+  if (!images || !outs || n == 0) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad batch argument");
+  std::vector<ImageDesc> imgs(n);
+  std::vector<size_t> dev_off(n), in_off(n), out_off(n);
+  std::vector<char> in_pin(n), out_pin(n);
+  size_t dev_total = 0, stage_in = 0, stage_out = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const psift_image_u8& im = images[i];
+    const psift_features& o = outs[i];
+    if ((im.height && im.width && !im.data) || im.row_stride < im.width)
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad batch image descriptor");
+    if (o.capacity && (!o.x || !o.y || !o.scale || !o.response || !o.orientation || !o.descriptors))
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null feature output array");
+    ImageDesc& d = imgs[i];
+    d.stride = im.width;
+    d.h = (int)im.height;
+    d.w = (int)im.width;
+    d.kind = SRC_U8;
+    d.feat_cap = cfg->max_features ? cfg->max_features
+                                   : std::min<uint32_t>(o.capacity ? o.capacity : 1, 4u * kDefaultKeypointCapacity);
+    const size_t px = (size_t)im.height * im.width;
+    dev_off[i] = dev_total;
+    dev_total += align_up(px, 256);
+    in_pin[i] = px ? (char)is_host_pinned(im.data) : 1;
+    in_off[i] = stage_in;
+    if (!in_pin[i]) stage_in += align_up(px, 64);
+    out_pin[i] = (char)(o.capacity && is_host_pinned(o.x) && is_host_pinned(o.y) && is_host_pinned(o.scale) &&
+                        is_host_pinned(o.response) && is_host_pinned(o.orientation) && is_host_pinned(o.descriptors));
+    out_off[i] = stage_out;
+    if (!out_pin[i]) stage_out += align_up((size_t)std::min(d.feat_cap, o.capacity) * sizeof(float) * (5 + kDescLen), 64);
+  }
+  DetectJob job;
+  void* extra = nullptr;
+  st = build_job(ctx, imgs, *cfg, job, dev_total, &extra);
+  if (st != PSIFT_OK) return st;
+  for (uint32_t i = 0; i < n; ++i) job.plans[i].src = (char*)extra + dev_off[i];
+  const size_t meta_bytes = align_up(16 * (size_t)n + 64, 64);
+  st = pinned_reserve(ctx, meta_bytes + stage_in + stage_out);
+  if (st != PSIFT_OK) return st;
+  uint32_t* meta = (uint32_t*)ctx->pinned.base;
+  char* pin_in = ctx->pinned.base + meta_bytes;
+  char* pin_out = pin_in + stage_in;
+
+  const uint32_t n_chunks = n >= 2 ? 2 : 1;
+  const uint32_t split = (n + 1) / 2;
+  cudaStream_t streams[2] = {ctx->stream, ctx->stream2};
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream));
+  // the device plan table is uploaded once for the whole batch; chunk views index into it
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream2, ctx->ev_fork, 0));
+  for (uint32_t c = 0; c < n_chunks; ++c) {
+    const uint32_t b = c == 0 ? 0 : split, e = c == 0 ? (n_chunks == 1 ? n : split) : n;
+    cudaStream_t sc = streams[c];
+    for (uint32_t i = b; i < e; ++i) {
+      const psift_image_u8& im = images[i];
+      const size_t px = (size_t)im.height * im.width;
+      if (!px) continue;
+      char* dst = (char*)extra + dev_off[i];
+      if (in_pin[i]) {
+        PSIFT_CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, im.width, im.data, im.row_stride, im.width, im.height,
+                                              cudaMemcpyHostToDevice, sc));
+      } else {
+        char* stg = pin_in + in_off[i];
+        for (uint32_t y = 0; y < im.height; ++y)
+          std::memcpy(stg + (size_t)y * im.width, im.data + (size_t)y * im.row_stride, im.width);
+        PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(dst, stg, px, cudaMemcpyHostToDevice, sc));
+      }
+    }
+    DetectJob v;
+    v.n = (int)(e - b);
+    v.plans.assign(job.plans.begin() + b, job.plans.begin() + e);
+    v.oct.assign(job.oct.begin() + (size_t)b * kMaxOctaves, job.oct.begin() + (size_t)e * kMaxOctaves);
+    v.n_oct.assign(job.n_oct.begin() + b, job.n_oct.begin() + e);
+    v.d_plans = job.d_plans + b;
+    v.kp_cap = job.kp_cap;
+    v.sel_cap = job.sel_cap;
+    st = launch_detect(ctx, v, *cfg, false, sc, /*plans_uploaded=*/true);
+    if (st != PSIFT_OK) return st;
+    for (uint32_t i = b; i < e; ++i)
+      PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(meta + 4 * i, job.plans[i].kp_count, 16, cudaMemcpyDeviceToHost, sc));
+  }
+  // Per chunk: wait for its counts, then queue its feature download on its stream.
+  bool capacity_short = false;
+  for (uint32_t c = 0; c < n_chunks; ++c) {
+    const uint32_t b = c == 0 ? 0 : split, e = c == 0 ? (n_chunks == 1 ? n : split) : n;
+    cudaStream_t sc = streams[c];
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(sc));
+    for (uint32_t i = b; i < e; ++i) {
+      psift_features& o = outs[i];
+      const uint32_t count = meta[4 * i + 2];
+      const uint32_t total = cfg->max_features ? count : meta[4 * i + 3];
+      if (total > o.capacity) {
+        o.count = total;
+        capacity_short = true;
+        continue;
+      }
+      o.count = count;
+      if (!count) continue;
+      const ImagePlan& P = job.plans[i];
+      const size_t cb = 4 * (size_t)count;
+      float* dsts[6];
+      if (out_pin[i]) {
+        dsts[0] = o.x; dsts[1] = o.y; dsts[2] = o.scale; dsts[3] = o.response; dsts[4] = o.orientation;
+        dsts[5] = o.descriptors;
+      } else {
+        float* hp = (float*)(pin_out + out_off[i]);
+        for (int k = 0; k < 6; ++k) dsts[k] = hp + (size_t)k * count;
+      }
+      const float* srcs[6] = {P.fx, P.fy, P.fscale, P.fresp, P.fori, P.fdesc};
+      for (int k = 0; k < 6; ++k)
+        PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(dsts[k], srcs[k], k == 5 ? cb * kDescLen : cb, cudaMemcpyDeviceToHost, sc));
+    }
+  }
+  PSIFT_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_join, ctx->stream2));
+  PSIFT_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(meta + 4 * n, ctx->d_error, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  st = error_from_word(ctx, meta[4 * n]);
+  if (st != PSIFT_OK) return st;
+  for (uint32_t i = 0; i < n; ++i) {
+    psift_features& o = outs[i];
+    if (out_pin[i] || o.count > o.capacity || !o.count) continue;
+    const float* hp = (const float*)(pin_out + out_off[i]);
+    const size_t c = o.count;
+    std::memcpy(o.x, hp + 0 * c, 4 * c);
+    std::memcpy(o.y, hp + 1 * c, 4 * c);
+    std::memcpy(o.scale, hp + 2 * c, 4 * c);
+    std::memcpy(o.response, hp + 3 * c, 4 * c);
+    std::memcpy(o.orientation, hp + 4 * c, 4 * c);
+    std::memcpy(o.descriptors, hp + 5 * c, 4 * c * kDescLen);
+  }
+  if (capacity_short) return set_error(ctx, PSIFT_ERR_CAPACITY, "feature output capacity too small");
   return PSIFT_OK;
 }
 

@@ -59,6 +59,11 @@ struct StageTimer {
 struct psift_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Second stream for the host-pointer batch entry (chunks of a batch overlap
+  // their uploads and downloads with the other chunk's kernels), and the events
+  // that fork it from and join it back to `stream`.
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string last_error;
   uint64_t launches = 0;
   psift::DeviceArena arena;   // per-call workspace
@@ -96,8 +101,10 @@ cudaError_t ensure_smem_attr(const void* func, size_t bytes);
 struct StageScope {
   psift_ctx* ctx;
   int stage;
+  cudaStream_t st;
   cudaEvent_t start = nullptr;
   StageScope(psift_ctx* c, int s);
+  StageScope(psift_ctx* c, int s, cudaStream_t stream);
   ~StageScope();
 };
 

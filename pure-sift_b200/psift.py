@@ -155,6 +155,10 @@ _SIGS = {
                                       C.c_void_p]),
     "psift_build_pyramid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
                                       C.POINTER(CSiftConfig), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "psift_detect_and_compute_u8_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CSiftConfig),
+                                                    C.c_void_p]),
+    "psift_host_alloc": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "psift_host_free": (C.c_int, [C.c_void_p, C.c_void_p]),
     "psift_compute_descriptors": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p,
                                             C.c_uint32, C.c_int32, C.POINTER(CFeatures)]),
     "psift_summarize_tracking": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
@@ -251,6 +255,32 @@ class Context:
         return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(self.STAGES)}
 
 
+class _PinnedBlock:
+    """Page-locked host allocation (psift_host_alloc), freed with the last array using it."""
+
+    def __init__(self, ctx: Context, nbytes: int):
+        self.ctx = ctx
+        p = C.c_void_p()
+        ctx.check(ctx.lib.psift_host_alloc(ctx.handle, nbytes, C.byref(p)))
+        self.ptr = int(p.value)
+        self.__array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (self.ptr, False), "version": 3}
+
+    def __del__(self):
+        if getattr(self, "ptr", 0) and getattr(self.ctx, "handle", None):
+            self.ctx.lib.psift_host_free(self.ctx.handle, C.c_void_p(self.ptr))
+            self.ptr = 0
+
+
+def pinned_empty(shape, dtype, ctx: Context | None = None) -> np.ndarray:
+    """An uninitialised numpy array in page-locked host memory."""
+    ctx = ctx or default_context()
+    dtype = np.dtype(dtype)
+    shape = tuple(shape) if isinstance(shape, (tuple, list)) else (int(shape),)
+    nbytes = int(np.prod(shape)) * dtype.itemsize
+    raw = np.asarray(_PinnedBlock(ctx, max(nbytes, 1)))
+    return raw[:nbytes].view(dtype).reshape(shape)
+
+
 _tls = threading.local()
 
 
@@ -318,6 +348,18 @@ class Features:
     def empty(n: int) -> "Features":
         return Features(*(np.zeros(n, np.float32) for _ in range(5)), np.zeros((n, 128), np.float32))
 
+    @staticmethod
+    def pinned(n: int, ctx: "Context | None" = None) -> "Features":
+        """Capacity-n feature arrays in one page-locked block (direct device->host copies)."""
+        blk = pinned_empty(((5 + 128) * max(n, 1),), np.float32, ctx)
+        cols = [blk[i * n:(i + 1) * n] for i in range(5)]
+        return Features(*cols, blk[5 * n:5 * n + 128 * n].reshape(n, 128))
+
+    def view(self, n: int) -> "Features":
+        """The first n features, without copying."""
+        return Features(self.x[:n], self.y[:n], self.scale[:n], self.response[:n], self.orientation[:n],
+                        self.descriptors[:n])
+
     def head(self, n: int) -> "Features":
         return Features(self.x[:n].copy(), self.y[:n].copy(), self.scale[:n].copy(), self.response[:n].copy(),
                         self.orientation[:n].copy(), self.descriptors[:n].copy())
@@ -360,6 +402,35 @@ class Sift:
 
     def detect_and_compute(self, img: np.ndarray, ctx: Context | None = None) -> Features:
         return self._run(img, False, ctx)
+
+    def detect_and_compute_batch_u8(self, images, outs: "list[Features] | None" = None,
+                                    ctx: Context | None = None) -> "list[Features]":
+        """Many u8 images in one call (psift_detect_and_compute_u8_batch): one launch
+        per stage for the batch, transfers overlapped with kernels.  Per image the
+        result equals ``detect_and_compute_u8``.  Returns views into ``outs``
+        (allocated here when not given; ``Features.pinned`` outputs and
+        ``pinned_empty`` images are transferred without staging copies)."""
+        ctx = ctx or default_context()
+        imgs = [np.ascontiguousarray(im, dtype=np.uint8) for im in images]
+        if any(im.ndim != 2 for im in imgs):
+            raise ValueError("images must be 2-D (H, W)")
+        n = len(imgs)
+        if n == 0:
+            return []
+        cfg = self.config.to_c()
+        cap = self.config.max_features_ or 16384
+        outs = list(outs) if outs is not None else [Features.empty(cap) for _ in range(n)]
+        cimgs = (CImageU8 * n)(*[CImageU8(im.ctypes.data, im.shape[0], im.shape[1], im.strides[0]) for im in imgs])
+        while True:
+            couts = (CFeatures * n)(*[_c_features(o) for o in outs])
+            st = ctx.lib.psift_detect_and_compute_u8_batch(ctx.handle, cimgs, n, C.byref(cfg), couts)
+            short = [i for i in range(n) if couts[i].count > len(outs[i])]
+            if st == PSIFT_ERR_CAPACITY and short:
+                for i in short:
+                    outs[i] = Features.empty(int(couts[i].count))
+                continue
+            ctx.check(st)
+            return [outs[i].view(int(couts[i].count)) for i in range(n)]
 
     def detect_and_compute_u8(self, img: np.ndarray, ctx: Context | None = None) -> Features:
         return self._run(img, True, ctx)
