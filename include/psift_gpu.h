@@ -101,6 +101,13 @@ psift_status psift_ctx_synchronize(psift_ctx* ctx);
  * emit), 2 top-K cap, 3 orientation, 4 descriptors, 5 matching, 6 Hamming,
  * 7 RANSAC, 8 MLP.  psift_ctx_stage_times synchronises the stream and returns
  * the accumulated milliseconds and the number of timed intervals per stage. */
+/* CUDA graphs for psift_detect_and_compute_batch_dev (on by default): the first
+ * call with a given launch geometry (image count and sizes, config) runs
+ * eagerly, the second is captured into a graph, later ones replay it.  The
+ * plan table of each call (image and output pointers) is uploaded before the
+ * replay, so pointers may change between calls.  Off while stage timing is on. */
+psift_status psift_ctx_enable_graphs(psift_ctx* ctx, int enable);
+uint64_t psift_ctx_graph_replays(const psift_ctx* ctx);
 psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
 psift_status psift_ctx_stage_times(psift_ctx* ctx, double* ms, uint64_t* counts, uint32_t n, int reset);
 

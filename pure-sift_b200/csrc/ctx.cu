@@ -194,6 +194,8 @@ psift_status psift_ctx_destroy(psift_ctx* ctx) {
     cudaEventDestroy(p.second.second);
   }
   for (cudaEvent_t e : ctx->timer.pool) cudaEventDestroy(e);
+  for (auto& g : ctx->graphs)
+    if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
   cudaEventDestroy(ctx->ev_fork);
   cudaEventDestroy(ctx->ev_join);
   cudaStreamDestroy(ctx->stream2);
@@ -215,6 +217,14 @@ psift_status psift_ctx_synchronize(psift_ctx* ctx) {
   PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return PSIFT_OK;
 }
+
+psift_status psift_ctx_enable_graphs(psift_ctx* ctx, int enable) {
+  if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  ctx->graphs_enabled = enable != 0;
+  return PSIFT_OK;
+}
+
+uint64_t psift_ctx_graph_replays(const psift_ctx* ctx) { return ctx ? ctx->graph_replays : 0; }
 
 psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable) {
   if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;

@@ -385,6 +385,12 @@ psift_status launch_pyramid_only(psift_ctx* ctx, DetectJob& job, const psift_sif
   return PSIFT_OK;
 }
 
+uint32_t float_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
 // True when p lies in page-locked host memory (cudaMallocHost / cudaHostRegister).
 bool is_host_pinned(const void* p) {
   cudaPointerAttributes a;
@@ -747,7 +753,52 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
   DetectJob job;
   st = build_job(ctx, imgs, *cfg, job, 0, nullptr);
   if (st != PSIFT_OK) return st;
-  return launch_detect(ctx, job, *cfg, false);
+  if (!ctx->graphs_enabled || ctx->timer.enabled) return launch_detect(ctx, job, *cfg, false);
+  // The plan table (image, output and workspace pointers) is data: it is uploaded
+  // before every run, so one graph serves every call with the same geometry.
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  std::string key;
+  {
+    char buf[160];
+    snprintf(buf, sizeof buf, "n%u o%u s%u t%08x u%d k%d m%u kc%u sc%u p%p e%p|", n, cfg->octaves, cfg->scales,
+             float_bits(cfg->contrast_threshold), cfg->upsample_first_octave, cfg->descriptor_kind, cfg->max_features,
+             job.kp_cap, job.sel_cap, (void*)job.d_plans, (void*)ctx->d_error);
+    key = buf;
+    for (uint32_t i = 0; i < n; ++i) {
+      snprintf(buf, sizeof buf, "%dx%d:%d,", job.plans[i].oct[0].h, job.plans[i].oct[0].w, job.n_oct[i]);
+      key += buf;
+    }
+  }
+  auto it = ctx->graphs.find(key);
+  if (it == ctx->graphs.end()) {
+    if (ctx->graph_seen[key]++ == 0) return launch_detect(ctx, job, *cfg, false, nullptr, true);
+    if (ctx->graphs.size() >= 32) {
+      for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
+      ctx->graphs.clear();
+    }
+    const uint64_t l0 = ctx->launches;
+    PSIFT_CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    st = launch_detect(ctx, job, *cfg, false, nullptr, true);
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st != PSIFT_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaStreamEndCapture");
+    psift_ctx::GraphEntry ent;
+    ce = cudaGraphInstantiate(&ent.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaGraphInstantiate");
+    ent.launches = ctx->launches - l0;
+    ctx->launches = l0;
+    it = ctx->graphs.emplace(key, ent).first;
+  }
+  PSIFT_CUDA_TRY(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
+  ctx->launches += it->second.launches;
+  ctx->graph_replays++;
+  return PSIFT_OK;
 }
 
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -73,6 +74,16 @@ struct psift_ctx {
   // Device status words: [0] error bits (kErr* below), [1] re-rank fallback rows.
   uint32_t* d_error = nullptr;
   psift::StageTimer timer;
+  // CUDA graphs of the device batch path, keyed by launch geometry: a key seen
+  // once runs eagerly, the second time it is captured, afterwards replayed.
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0;
+  };
+  bool graphs_enabled = true;
+  std::map<std::string, GraphEntry> graphs;
+  std::map<std::string, int> graph_seen;
+  uint64_t graph_replays = 0;
 };
 
 namespace psift {

@@ -157,6 +157,8 @@ _SIGS = {
                                       C.POINTER(CSiftConfig), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
     "psift_detect_and_compute_u8_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CSiftConfig),
                                                     C.c_void_p]),
+    "psift_ctx_enable_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "psift_ctx_graph_replays": (C.c_uint64, [C.c_void_p]),
     "psift_host_alloc": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]),
     "psift_host_free": (C.c_int, [C.c_void_p, C.c_void_p]),
     "psift_compute_descriptors": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p,
@@ -241,6 +243,13 @@ class Context:
 
     def synchronize(self):
         self.check(self.lib.psift_ctx_synchronize(self.handle))
+
+    def enable_graphs(self, on: bool = True):
+        self.check(self.lib.psift_ctx_enable_graphs(self.handle, int(on)))
+
+    @property
+    def graph_replays(self) -> int:
+        return int(self.lib.psift_ctx_graph_replays(self.handle))
 
     STAGES = ("pyramid", "extrema", "select", "orientation", "descriptor", "match", "hamming", "ransac", "mlp")
 
