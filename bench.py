@@ -40,9 +40,11 @@ METRIC = "1080p SIFT detect+describe images/s"
 WORKLOAD = ("1920x1080 u8 blob images (2000 blobs, sigma U(1.5,20), N(0,3) noise); "
             "SiftConfig octaves=4 scales=3 threshold=0.015 upsample=on, cap 4096")
 L2_NOTE = "no flush: per-step working set (~0.5 GB of scale-space planes per image) >> 126 MB L2"
-# DRAM bytes per blur_level_kernel launch from one ncu capture (octave 0, 1080p
-# image, radius-10 level); profiles/blur_level_1080p.md gives the command.
-NCU_TRAFFIC_BLUR_LEVEL = None
+# DRAM bytes per blur_level_kernel launch, averaged over the 21 launches of one step:
+# one ncu capture at batch 2 (826.2 MB read + written over 21 launches), scaled by 4 to
+# the 8 images of a step here (traffic grows with the images processed).  Writes of the
+# small octaves stay in L2 past the kernel's end, so this under-counts writes.
+NCU_TRAFFIC_BLUR_LEVEL = 4 * 826.17e6 / 21
 
 
 def peaks():
@@ -211,6 +213,125 @@ def match_bench(ctx, torch, n_pairs: int = 32, n: int = 4096, reps: int = 5):
     }
 
 
+def catalog_bench(ctx, torch, n_cat: int = 2_000_000, n_q: int = 4096, k: int = 64, reps: int = 5):
+    """Catalog search: 2M SIFT-like catalog descriptors (10,000 images x 200;
+    |N(0,1)| L2-normalised, clipped at 0.2, renormalised), binarised to 128-bit
+    codes by the reference's scheme (bit i = desc[i] > 0.065), 4096 queries
+    (perturbed catalog descriptors), XOR+POPCNT top-64 shortlist, exact FP32
+    L2 re-rank of the 64.  Device-resident inputs; CUDA events per stage."""
+    import psift
+    g = torch.Generator(device="cuda")
+    g.manual_seed(4)
+    cat = torch.randn((n_cat, 128), generator=g, device="cuda").abs_()
+    cat /= cat.norm(dim=1, keepdim=True)
+    cat.clamp_(max=0.2)
+    cat /= cat.norm(dim=1, keepdim=True)
+    pick = torch.randint(0, n_cat, (n_q,), generator=g, device="cuda")
+    q = cat[pick] + 0.02 * torch.randn((n_q, 128), generator=g, device="cuda").abs_()
+    q /= q.norm(dim=1, keepdim=True)
+    cat_codes = torch.empty((n_cat, 2), dtype=torch.int64, device="cuda")
+    q_codes = torch.empty((n_q, 2), dtype=torch.int64, device="cuda")
+    idx = torch.empty((n_q, k), dtype=torch.int32, device="cuda")
+    dist = torch.empty((n_q, k), dtype=torch.int32, device="cuda")
+    ridx = torch.empty((n_q, k), dtype=torch.int32, device="cuda")
+    rd2 = torch.empty((n_q, k), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    L = ctx.lib
+    steps = {
+        "quantize": lambda: ctx.check(L.psift_quantize_u128_dev(ctx.handle, C.c_void_p(cat.data_ptr()), n_cat,
+                                                                 C.c_void_p(cat_codes.data_ptr()))),
+        "topk": lambda: ctx.check(L.psift_hamming_topk_dev(ctx.handle, C.c_void_p(q_codes.data_ptr()), n_q,
+                                                           C.c_void_p(cat_codes.data_ptr()), n_cat, k,
+                                                           C.c_void_p(idx.data_ptr()), C.c_void_p(dist.data_ptr()))),
+        "rerank": lambda: ctx.check(L.psift_l2_rerank_dev(ctx.handle, C.c_void_p(q.data_ptr()), n_q,
+                                                          C.c_void_p(cat.data_ptr()), C.c_void_p(idx.data_ptr()), k,
+                                                          C.c_void_p(ridx.data_ptr()), C.c_void_p(rd2.data_ptr()))),
+    }
+    ctx.check(L.psift_quantize_u128_dev(ctx.handle, C.c_void_p(q.data_ptr()), n_q, C.c_void_p(q_codes.data_ptr())))
+    ms = {}
+    for name, fn in steps.items():
+        fn()
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        ctx.synchronize()
+        ms[name] = e0.elapsed_time(e1) / reps
+    peak = C.c_double()
+    ctx.check(L.psift_popc_throughput(ctx.handle, C.byref(peak)))
+    pairs = float(n_q) * n_cat
+    popc_s = pairs * 4 / (ms["topk"] * 1e-3)
+    # the query's own (perturbed) source descriptor should be found by the shortlist
+    hit = float((idx == pick[:, None].int()).any(dim=1).float().mean().item())
+    return {
+        "workload": f"{n_cat} catalog codes (10,000 images x 200), {n_q} queries, top-{k} XOR+POPCNT shortlist "
+                    f"+ exact FP32 L2 re-rank",
+        "ms": {"quantize_2M": ms["quantize"], "topk": ms["topk"], "l2_rerank": ms["rerank"],
+               "search_total": ms["topk"] + ms["rerank"]},
+        "topk_pairs_per_s": pairs / (ms["topk"] * 1e-3),
+        "roofline_topk": {"bound": "int (popc)", "achieved": popc_s, "peak": peak.value, "unit": "popc/s",
+                          "frac": popc_s / peak.value,
+                          "peak_source": "measured: psift_popc_throughput (popc+xor+add register chains)"},
+        "quantize_gbs": n_cat * 512 / (ms["quantize"] * 1e-3) / 1e9,
+        "source_in_shortlist": hit,
+    }
+
+
+def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int = 3):
+    """Learned RANSAC proposal: 1024 synthetic 1080p pairs with known perspective
+    homographies, 2k-8k putative matches each, outlier ratio U(0.1, 0.7).  The MLP
+    (8-64-64-1) is trained on the GPU on plain-RANSAC labels of 64 other pairs,
+    then plain (uniform) and guided (MLP-weighted) homography RANSAC run over the
+    1024 pairs in one launch each; iterations, ms, and inlier counts compared."""
+    import psift
+    train = [synth.c5_pair(k) for k in range(5000, 5000 + n_train)]
+    pairs = [synth.c5_pair(k) for k in range(n_pairs)]
+    labels = psift.ransac_batch([r for r, _, _ in train], ctx=ctx)
+    X = np.concatenate([f for _, f, _ in train])
+    Y = np.concatenate([m for m, _, _ in labels]).astype(np.float32)
+    mlp = psift.InlierMLP(seed=11)
+    t0 = time.perf_counter()
+    mlp.train(X, Y, steps=400, batch=4096, lr=3e-3, seed=12, ctx=ctx)
+    train_s = time.perf_counter() - t0
+    feats = np.concatenate([f for _, f, _ in pairs])
+    t0 = time.perf_counter()
+    probs_all = np.clip(mlp.predict(feats, ctx=ctx), 0.02, 1.0)
+    infer_s = time.perf_counter() - t0
+    offs = np.cumsum([0] + [len(f) for _, f, _ in pairs])
+    probs = [probs_all[offs[i]:offs[i + 1]] for i in range(n_pairs)]
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {}
+    for name, w in (("plain", None), ("guided", probs)):
+        jobs, keep = psift.ransac_jobs([r for r, _, _ in pairs], weights=w)
+        opt = psift.RansacOptions().to_c()
+        launch = lambda: ctx.check(ctx.lib.psift_ransac_batch_dev(ctx.handle, jobs, n_pairs, C.byref(opt), 1))
+        launch()
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            launch()
+        e1.record(stream)
+        ctx.synchronize()
+        res = psift.ransac_results(keep, homography=True)
+        out[name] = {"ms": e0.elapsed_time(e1) / reps,
+                     "inliers": np.array([m.sum() for m, _, _ in res]),
+                     "iters": np.array([it[1] for _, _, it in res])}
+    p, gd = out["plain"], out["guided"]
+    ok = gd["inliers"] >= np.floor(0.99 * p["inliers"])
+    return {
+        "workload": f"{n_pairs} pairs, 2k-8k matches, outlier ratio U(0.1,0.7); MLP trained on {n_train} other pairs",
+        "plain_ms": p["ms"], "guided_ms": gd["ms"], "speedup": p["ms"] / gd["ms"],
+        "plain_mean_iterations": float(p["iters"].mean()), "guided_mean_iterations": float(gd["iters"].mean()),
+        "plain_total_inliers": int(p["inliers"].sum()), "guided_total_inliers": int(gd["inliers"].sum()),
+        "pairs_guided_within_1pct_of_plain": float(ok.mean()),
+        "mlp_train_s_400_steps": train_s, "mlp_infer_ms_all_matches": infer_s * 1e3,
+        "matches_total": int(offs[-1]),
+    }
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -373,6 +494,13 @@ def run_ours(args):
             "stage_ms_per_step": {k: v[0] / reps for k, v in st.items() if v[1]},
             "clocks": clk.summary(),
         }
+        for key, fn in (("catalog", catalog_bench), ("learned_ransac", ransac_bench)):
+            if getattr(args, "no_" + key):
+                continue
+            try:
+                result[key] = fn(ctx, torch)
+            except Exception as exc:  # reported, not hidden
+                result[key] = {"error": repr(exc)}
         try:
             result["match"] = match_bench(ctx, torch)
             bf16_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
@@ -396,7 +524,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=8)
@@ -404,6 +532,8 @@ def main():
     ap.add_argument("--only-device", action="store_true", help="time the device path only (profiling case)")
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
+    ap.add_argument("--no-catalog", action="store_true")
+    ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

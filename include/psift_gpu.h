@@ -311,6 +311,10 @@ psift_status psift_mlp_train_dev(psift_ctx* ctx, float* params, const float* fea
 /* quantize_descriptor_u128 (src/catalog.rs:37-45): bit i set iff desc[i] > 0.065.
  * codes: 2 x u64 per descriptor, little endian (word 0 = bits 0..63). */
 psift_status psift_quantize_u128(psift_ctx* ctx, const float* desc, uint32_t n, uint64_t* codes);
+psift_status psift_quantize_u128_dev(psift_ctx* ctx, const float* desc, uint32_t n, uint64_t* codes);
+/* Diagnostic: measured 32-bit popcount throughput of this GPU (independent
+ * register chains, no memory traffic), the INT roofline of the Hamming kernels. */
+psift_status psift_popc_throughput(psift_ctx* ctx, double* popc_per_s);
 /* quantize_descriptor_u8 (src/pipeline.rs:1024-1030): round(v * 512) clamped to [0, 255]. */
 psift_status psift_quantize_u8(psift_ctx* ctx, const float* desc, uint32_t n, uint8_t* out);
 /* dequantize_descriptor_u8 (src/pipeline.rs:1034-1044): v / 512, then L2 renormalised. */

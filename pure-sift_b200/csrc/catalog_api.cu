@@ -11,6 +11,7 @@
 namespace psift {
 
 cudaError_t launch_quantize(const float* desc, int n, uint64_t* codes, uint8_t* u8, cudaStream_t st);
+cudaError_t launch_popc_probe(int blocks, int iters, uint32_t* out, cudaStream_t st);
 cudaError_t launch_dequantize(const uint8_t* q, int n, float* out, cudaStream_t st);
 cudaError_t launch_votes(const uint64_t* q, int nq, const uint64_t* cat, const long long* offsets, int n_entries,
                          int mih, uint32_t* votes, cudaStream_t st);
@@ -69,6 +70,47 @@ psift_status psift_quantize_u128(psift_ctx* ctx, const float* desc, uint32_t n, 
   ctx->launches++;
   if (e != cudaSuccess) return cuda_error(ctx, e, "quantize");
   return d2h_sync(ctx, codes, d_codes, (size_t)n * 16);
+}
+
+psift_status psift_quantize_u128_dev(psift_ctx* ctx, const float* desc, uint32_t n, uint64_t* codes) {
+  psift_status st = begin(ctx);
+  if (st != PSIFT_OK) return st;
+  if (n == 0) return PSIFT_OK;
+  if (!desc || !codes) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  StageScope sc(ctx, STAGE_HAMMING);
+  cudaError_t e = launch_quantize(desc, (int)n, codes, nullptr, ctx->stream);
+  ctx->launches++;
+  if (e != cudaSuccess) return cuda_error(ctx, e, "quantize");
+  return PSIFT_OK;
+}
+
+psift_status psift_popc_throughput(psift_ctx* ctx, double* popc_per_s) {
+  psift_status st = begin(ctx);
+  if (st != PSIFT_OK) return st;
+  if (!popc_per_s) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  const int blocks = ctx->num_sms * 8, iters = 4096;
+  st = io_reserve(ctx, (size_t)blocks * 256 * 4 + 1024);
+  if (st != PSIFT_OK) return st;
+  uint32_t* d_out = (uint32_t*)io_take(ctx, (size_t)blocks * 256 * 4);
+  cudaEvent_t a = nullptr, b = nullptr;
+  PSIFT_CUDA_TRY(ctx, cudaEventCreate(&a));
+  PSIFT_CUDA_TRY(ctx, cudaEventCreate(&b));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(a, ctx->stream);
+    cudaError_t e = launch_popc_probe(blocks, iters, d_out, ctx->stream);
+    cudaEventRecord(b, ctx->stream);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "popc probe");
+    PSIFT_CUDA_TRY(ctx, cudaEventSynchronize(b));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *popc_per_s = (double)blocks * 256.0 * iters * 8.0 / (best * 1e-3);
+  return PSIFT_OK;
 }
 
 psift_status psift_quantize_u8(psift_ctx* ctx, const float* desc, uint32_t n, uint8_t* out) {

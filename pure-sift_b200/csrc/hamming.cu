@@ -352,6 +352,34 @@ cudaError_t launch_topk(const uint64_t* q, int nq, const uint64_t* cat, long lon
   return cudaGetLastError();
 }
 
+// Throughput probe for the INT roofline of the Hamming kernels: every thread
+// keeps 8 independent 32-bit popcount chains in registers (no memory traffic in
+// the loop); the sum is stored so nothing is dead code.
+__global__ void __launch_bounds__(256) popc_probe_kernel(uint32_t seed, int iters, uint32_t* out) {
+  uint32_t v[8], acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    v[j] = seed * (threadIdx.x + 1u) + 0x9E3779B9u * (uint32_t)(j + 1) + blockIdx.x;
+    acc[j] = 0;
+  }
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      acc[j] += __popc(v[j]);
+      v[j] ^= acc[j];
+    }
+  }
+  uint32_t t = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) t += acc[j];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = t;
+}
+
+cudaError_t launch_popc_probe(int blocks, int iters, uint32_t* out, cudaStream_t st) {
+  popc_probe_kernel<<<blocks, 256, 0, st>>>(12345u, iters, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_l2_rerank(const float* qd, int nq, const float* cd, const uint32_t* cand, int k,
                              uint32_t* out_idx, float* out_d2, cudaStream_t st) {
   if (nq <= 0) return cudaSuccess;

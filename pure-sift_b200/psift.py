@@ -165,6 +165,8 @@ _SIGS = {
                                             C.c_uint32, C.c_int32, C.POINTER(CFeatures)]),
     "psift_summarize_tracking": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CTracking)]),
+    "psift_quantize_u128_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "psift_popc_throughput": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "psift_quantize_u128": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "psift_quantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "psift_dequantize_u8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
@@ -698,12 +700,9 @@ class InlierMLP:
         return losses
 
 
-def ransac_batch(match_sets, options: RansacOptions = RansacOptions(), homography: bool = True,
-                 weights=None, ctx: Context | None = None):
-    """Runs many estimations in one launch (device-resident); returns
-    [(inlier mask, model or None, (similarity iters, homography iters))]."""
+def ransac_jobs(match_sets, weights=None):
+    """Device-resident RANSAC jobs for psift_ransac_batch_dev (torch buffers)."""
     import torch
-    ctx = ctx or default_context()
     dev = []
     jobs = (CRansacJob * len(match_sets))()
     for i, m in enumerate(match_sets):
@@ -721,15 +720,28 @@ def ransac_batch(match_sets, options: RansacOptions = RansacOptions(), homograph
         # [3] homography iterations, [4..13) model floats
         jobs[i] = CRansacJob(d_m.data_ptr(), n, mask.data_ptr(), out.data_ptr() + 16, out.data_ptr() + 4,
                              out.data_ptr(), w.data_ptr() if w is not None else None, out.data_ptr() + 8)
-    c = options.to_c()
-    ctx.check(ctx.lib.psift_ransac_batch_dev(ctx.handle, jobs, len(match_sets), C.byref(c), int(homography)))
-    ctx.synchronize()
+    return jobs, dev
+
+
+def ransac_results(dev, homography: bool = True):
     res = []
     for d_m, mask, out, w, n in dev:
         o = out.cpu().numpy()
         model = o[4:4 + (9 if homography else 6)].view(np.float32).copy()
         res.append((mask[:n].cpu().numpy().astype(bool), model if o[1] else None, (int(o[2]), int(o[3]))))
     return res
+
+
+def ransac_batch(match_sets, options: RansacOptions = RansacOptions(), homography: bool = True,
+                 weights=None, ctx: Context | None = None):
+    """Runs many estimations in one launch (device-resident); returns
+    [(inlier mask, model or None, (similarity iters, homography iters))]."""
+    ctx = ctx or default_context()
+    jobs, dev = ransac_jobs(match_sets, weights)
+    c = options.to_c()
+    ctx.check(ctx.lib.psift_ransac_batch_dev(ctx.handle, jobs, len(match_sets), C.byref(c), int(homography)))
+    ctx.synchronize()
+    return ransac_results(dev, homography)
 
 
 def compute_sift_descriptors(img: np.ndarray, keypoints, kind: int = 0, ctx: Context | None = None) -> Features:
