@@ -241,33 +241,48 @@ __global__ void __launch_bounds__(1024) feature_scan_kernel(const ImagePlan* __r
   }
 }
 
-// Grid (ceil(sel_cap / 4), images), 128 threads: one warp per keypoint, one
+// Grid (sel_cap, images), 128 threads: one CTA (4 warps) per keypoint, one
 // descriptor per orientation.
 //
-// The window is walked in chunks of 256 pixels.  Phase 1: each lane tests 8
-// pixels against the rotated 4x4-cell square (the reference's r_bin/c_bin test,
-// about half of the window passes) and the passing ones are compacted into the
-// warp's queue.  Phase 2: full lanes take queued pixels for the gradient,
-// weight and trilinear binning.  Histograms: 16 private columns per warp
-// ([bin][16], 8 KB); lanes l and l + 16 share column l and add in two fixed
-// phases, so every bin's sum has one fixed order (deterministic).
+// The window is cut into chunks of 256 pixels dealt round-robin to the 4 warps.
+// Per chunk, phase 1: each lane tests 8 pixels against the rotated 4x4-cell
+// square (the reference's r_bin/c_bin test; about half of the window passes) and
+// the passing ones are compacted into the warp's queue; phase 2: full lanes take
+// queued pixels for the gradient, weight and trilinear binning.  Histograms: 16
+// private columns per warp ([bin][16], 8 KB); lanes l and l + 16 share column l
+// and add in two fixed phases.  Bin b's value is the sum over (warp, column) in a
+// fixed order, so the result does not depend on scheduling (deterministic).
 constexpr int kDescChunk = 256;
 constexpr int kHistCols = 16;
-constexpr int kDescSmemPerWarp = kDescLen * kHistCols * 4 + kDescChunk * 4;
+constexpr int kDescWarpSmem = kDescLen * kHistCols * 4 + kDescChunk * 4;
+constexpr int kDescSmem = kDescWarps * kDescWarpSmem + 64;
+
+// Block-wide sum of one value per thread (128 threads), same result on every thread.
+__device__ __forceinline__ float block_sum128(float v, float* s_red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  return (s_red[0] + s_red[1]) + (s_red[2] + s_red[3]);
+}
 
 __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const ImagePlan* __restrict__ plans,
                                                                      DescribeParams prm) {
+  static_assert(kDescWarps == 4, "one thread per bin in the final sums");
   const ImagePlan& P = plans[blockIdx.y];
   extern __shared__ float4 s_dyn4[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t i = blockIdx.x * kDescWarps + warp;
+  const uint32_t i = blockIdx.x;
   if (i >= *P.sel_count) return;
   const uint32_t fcount = *P.feat_count;
   const uint32_t f0 = P.feat_offsets[i];
   if (f0 >= fcount) return;
-  char* wbase = reinterpret_cast<char*>(s_dyn4) + warp * kDescSmemPerWarp;
+  char* base_smem = reinterpret_cast<char*>(s_dyn4);
+  char* wbase = base_smem + warp * kDescWarpSmem;
   float (*hist)[kHistCols] = reinterpret_cast<float (*)[kHistCols]>(wbase);
   uint32_t* queue = reinterpret_cast<uint32_t*>(wbase + kDescLen * kHistCols * 4);
+  float* s_red = reinterpret_cast<float*>(base_smem + kDescWarps * kDescWarpSmem);
 
   const psift_keypoint kp = P.sel[i];
   OctKp ok = to_octave(P, kp);
@@ -291,9 +306,6 @@ __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const Image
   const int wx = x_max - x_min + 1;
   const int n = (y_max >= y_min && x_max >= x_min && O.h >= 3 && O.w >= 3) ? (y_max - y_min + 1) * wx : 0;
   const float bin_per_rad = 8.0f / two_pi;
-  // the lane's first window pixel; later ones follow by stepping 32 pixels
-  const int y_first = y_min + (wx > 0 ? lane / wx : 0);
-  const int x_first = x_min + (wx > 0 ? lane % wx : 0);
   const int col = lane & (kHistCols - 1), half = lane >> 4;
 
   for (uint32_t q = 0; q < nori; ++q) {
@@ -304,13 +316,14 @@ __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const Image
     for (int b = lane; b < kDescLen * kHistCols / 4; b += 32)
       reinterpret_cast<float4*>(&hist[0][0])[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float cos_t = cosf(theta), sin_t = sinf(theta);
-    int yy = y_first, xx = x_first;
-    for (int base = 0; base < n; base += kDescChunk) {
+    for (int base = warp * kDescChunk; base < n; base += kDescWarps * kDescChunk) {
       // Phase 1: rotated-square test for 8 pixels per lane.
+      const int t0 = base + lane;
+      int yy = y_min + t0 / wx, xx = x_min + t0 % wx;
       uint32_t m = 0, packed[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        const int t = base + 32 * k + lane;
+        const int t = t0 + 32 * k;
         const int py = yy, px = xx;
         packed[k] = ((uint32_t)py << 16) | (uint32_t)px;
         xx += 32;
@@ -394,59 +407,40 @@ __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const Image
         }
       }
     }
-    // Bin b = lane + 32k: sum of the 16 columns, read rotated by b >> 1 so the
-    // 32 lanes hit 32 distinct banks (a fixed order per bin: deterministic).
-    float d[4];
+    __syncthreads();
+    // Bin b = threadIdx.x: sum over warps 0..3, each over its 16 columns read
+    // rotated by b >> 1 (the 32 lanes of a warp hit 32 distinct banks).
+    const int b = threadIdx.x;
+    float d = 0.0f;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int b = lane + 32 * k;
+    for (int w4 = 0; w4 < kDescWarps; ++w4) {
+      const float* row = reinterpret_cast<const float*>(base_smem + w4 * kDescWarpSmem) + b * kHistCols;
       float acc = 0.0f;
 #pragma unroll
-      for (int j = 0; j < kHistCols; ++j) acc += hist[b][(j + (b >> 1)) & (kHistCols - 1)];
-      d[k] = acc;
+      for (int j = 0; j < kHistCols; ++j) acc += row[(j + (b >> 1)) & (kHistCols - 1)];
+      d += acc;
     }
-    __syncwarp();
-    // L2 -> clamp 0.2 -> L2 (src/pipeline.rs:1462-1477); sums as xor-butterfly
-    // reductions (same on every lane, deterministic).
-    float n1 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n1 += __shfl_xor_sync(0xffffffffu, n1, o);
-    n1 = sqrtf(n1);
+    // L2 -> clamp 0.2 -> L2 (src/pipeline.rs:1462-1477); block sums in a fixed order.
+    float n1 = sqrtf(block_sum128(d * d, s_red));
     if (n1 > 1e-7f) {
-      const float inv1 = 1.0f / n1;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) d[k] = fminf(d[k] * inv1, 0.2f);
-      float n2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xffffffffu, n2, o);
-      n2 = sqrtf(n2);
-      if (n2 > 1e-7f) {
-        const float inv2 = 1.0f / n2;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) d[k] *= inv2;
-      }
+      d = fminf(d * (1.0f / n1), 0.2f);
+      const float n2 = sqrtf(block_sum128(d * d, s_red));
+      if (n2 > 1e-7f) d *= 1.0f / n2;
     }
     if (prm.descriptor_kind == 1) {
       // to_rootsift_descriptor (src/pipeline.rs:1012-1019)
-      float l1 = fmaxf(d[0], 0.0f) + fmaxf(d[1], 0.0f) + fmaxf(d[2], 0.0f) + fmaxf(d[3], 0.0f);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) l1 += __shfl_xor_sync(0xffffffffu, l1, o);
-      if (l1 > 1e-7f) {
-        const float inv = 1.0f / l1;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) d[k] = sqrtf(fmaxf(d[k], 0.0f) * inv);
-      }
+      const float l1 = block_sum128(fmaxf(d, 0.0f), s_red);
+      if (l1 > 1e-7f) d = sqrtf(fmaxf(d, 0.0f) * (1.0f / l1));
     }
-    float* dst = P.fdesc + (size_t)f * kDescLen;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) dst[lane + 32 * k] = d[k];
-    if (lane == 0) {
+    P.fdesc[(size_t)f * kDescLen + b] = d;
+    if (threadIdx.x == 0) {
       P.fx[f] = kp.x;
       P.fy[f] = kp.y;
       P.fscale[f] = kp.scale;
       P.fresp[f] = kp.response;
       P.fori[f] = theta;
     }
+    __syncthreads();  // histograms are cleared for the next orientation
   }
 }
 
@@ -464,10 +458,10 @@ cudaError_t launch_feature_scan(const ImagePlan* plans, int n, uint32_t max_feat
 
 cudaError_t launch_descriptor(const ImagePlan* plans, int n, uint32_t sel_cap, const DescribeParams& prm,
                               cudaStream_t st) {
-  const size_t smem = (size_t)kDescWarps * kDescSmemPerWarp;
+  const size_t smem = kDescSmem;
   cudaError_t e = ensure_smem_attr((const void*)descriptor_kernel, smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((sel_cap + kDescWarps - 1) / kDescWarps, n);
+  dim3 grid(sel_cap, n);
   descriptor_kernel<<<grid, kDescWarps * 32, smem, st>>>(plans, prm);
   return cudaGetLastError();
 }

@@ -140,6 +140,45 @@ __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePla
   float* s_tmp = reinterpret_cast<float*>(s_in + Gm::IN_PAIRS * Gm::IN_S);       // [IN_H][kTmpStride]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
+  // 0. Upsampling base modes: the half-resolution source tile the staged tile
+  //    needs (at most 32 + R + 2 rows, 32 + R' + 2 columns) goes to shared memory
+  //    once, already in f32 (u8 * (1/255), luma_to_array2), in the intermediate
+  //    buffer that the horizontal pass only fills later.
+  constexpr bool kUp = MODE == MODE_INIT_F32_UP || MODE == MODE_INIT_U8_UP;
+  constexpr int SRC_H = (Gm::IN_H + 1) / 2 + 2, SRC_W = (Gm::IN_W + 1) / 2 + 2;
+  static_assert(!kUp || SRC_H * SRC_W <= Gm::IN_H * kTmpStride, "source tile fits the intermediate buffer");
+  int sy_lo = 0, sx_lo = 0;
+  if constexpr (kUp) {
+    sy_lo = clampi(ty0 - R, 0, h - 1) >> 1;
+    sx_lo = clampi(tx0 - Gm::RP, 0, w - 1) >> 1;
+    const int sh = min(SRC_H, P.src_h - sy_lo), sw = min(SRC_W, P.src_w - sx_lo);
+    for (int i = threadIdx.x; i < SRC_H * SRC_W; i += kBlurThreads) {
+      const int r = i / SRC_W, c = i - r * SRC_W;
+      float v = 0.0f;
+      if (r < sh && c < sw) {
+        const long long off = (long long)(sy_lo + r) * P.src_stride + (sx_lo + c);
+        if constexpr (MODE == MODE_INIT_U8_UP) {
+          const float inv255 = 1.0f / 255.0f;
+          v = (float)((const uint8_t*)P.src)[off] * inv255;
+        } else {
+          v = ((const float*)P.src)[off];
+        }
+      }
+      s_tmp[i] = v;
+    }
+    __syncthreads();
+  }
+  // upsample_2x_bilinear sample at octave-0 (gy, gx), both already clamped
+  auto up_sample = [&](int gy, int gx) -> float {
+    const int y0 = gy >> 1, x0 = gx >> 1;
+    const int y1 = min(y0 + (gy & 1), P.src_h - 1);
+    const int x1 = min(x0 + (gx & 1), P.src_w - 1);
+    const float* r0 = s_tmp + (y0 - sy_lo) * SRC_W - sx_lo;
+    const float* r1 = s_tmp + (y1 - sy_lo) * SRC_W - sx_lo;
+    const float a = r0[x0], b = r0[x1], c = r1[x0], d = r1[x1];
+    return 0.25f * (((a + b) + c) + d);
+  };
+
   // 1. Stage the clamped input tile, rows interleaved in pairs.
   const float* src_plane = O.g + (long long)(level - 1) * O.plane_stride;  // MODE_LEVEL only
   for (int u = threadIdx.x; u < Gm::IN_PAIRS * Gm::C4; u += kBlurThreads) {
@@ -156,8 +195,13 @@ __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePla
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int cx = clampi(gx + i, 0, w - 1);
-        av[i] = fetch_src<MODE>(P, O, level - 1, gy0, cx);
-        bv[i] = fetch_src<MODE>(P, O, level - 1, gy1, cx);
+        if constexpr (kUp) {
+          av[i] = up_sample(gy0, cx);
+          bv[i] = up_sample(gy1, cx);
+        } else {
+          av[i] = fetch_src<MODE>(P, O, level - 1, gy0, cx);
+          bv[i] = fetch_src<MODE>(P, O, level - 1, gy1, cx);
+        }
       }
       a = make_float4(av[0], av[1], av[2], av[3]);
       b = make_float4(bv[0], bv[1], bv[2], bv[3]);
