@@ -226,6 +226,7 @@ psift_status psift_ctx_enable_graphs(psift_ctx* ctx, int enable) {
 
 uint64_t psift_ctx_graph_replays(const psift_ctx* ctx) { return ctx ? ctx->graph_replays : 0; }
 
+
 psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable) {
   if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
   ctx->timer.enabled = enable != 0;

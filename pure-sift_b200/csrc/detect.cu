@@ -246,6 +246,12 @@ psift_status build_job(psift_ctx* ctx, const std::vector<ImageDesc>& imgs, const
   return PSIFT_OK;
 }
 
+// One blur level (octave o, level s >= 1) of every image of the job.
+cudaError_t launch_level(const DetectJob& job, const SigmaSchedule& sc, int o, int s, int S, int mh, int mw,
+                         cudaStream_t st) {
+  return launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, job.n, o, s, S, mh, mw, st);
+}
+
 // Queue every stage of the path for the batch (no host synchronisation).
 // stop_after_keypoints: end after extrema_emit (Sift::detect_keypoints).
 psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_config& cfg, bool stop_after_keypoints,
@@ -302,7 +308,7 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
     {
       StageScope sc_pyr(ctx, STAGE_PYRAMID, st);
       for (int s = 1; s <= S + 2; ++s) {
-        cudaError_t e = launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, n, o, s, S, mh, mw, st);
+        cudaError_t e = launch_level(job, sc, o, s, S, mh, mw, st);
         ctx->launches++;
         if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
       }
@@ -377,7 +383,7 @@ psift_status launch_pyramid_only(psift_ctx* ctx, DetectJob& job, const psift_sif
       if (e != cudaSuccess) return cuda_error(ctx, e, "blur(init)");
     }
     for (int s = 1; s <= S + 2; ++s) {
-      cudaError_t e = launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, n, o, s, S, mh, mw, st);
+      cudaError_t e = launch_level(job, sc, o, s, S, mh, mw, st);
       ctx->launches++;
       if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
     }

@@ -126,6 +126,13 @@ __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePla
                                                                    int level, int down_level, int zrev, Taps2 taps) {
   using Gm = BlurGeom<R>;
   static_assert(HC == 4 || HC == 8, "horizontal outputs per thread");
+  // The Gaussian taps are bit-symmetric (gaussian_kernel_1d evaluates the same
+  // x^2 for +-x and normalises both by one sum), so w[k] = w[2R - k] exactly and
+  // R + 1 register pairs hold them all for the whole kernel.
+  float2 wv[R + 1];
+#pragma unroll
+  for (int k = 0; k <= R; ++k) wv[k] = taps.w[k];
+  const float2 one = taps.one;
   static_assert(RV % 2 == 0 && kTileH % (RV * (kBlurThreads / 32)) == 0, "vertical rows per thread");
   const int z = zrev ? (int)gridDim.z - 1 - (int)blockIdx.z : (int)blockIdx.z;
   const ImagePlan& P = plans[z];
@@ -232,8 +239,8 @@ __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePla
 #pragma unroll
         for (int j = 0; j < HC; ++j) {
           const int k0 = 2 * q - SH - j;
-          if (k0 >= 0 && k0 <= 2 * R) acc[j] = mul_add2_rn(acc[j], p0, taps.w[k0], taps.one);
-          if (k0 + 1 >= 0 && k0 + 1 <= 2 * R) acc[j] = mul_add2_rn(acc[j], p1, taps.w[k0 + 1], taps.one);
+          if (k0 >= 0 && k0 <= 2 * R) acc[j] = mul_add2_rn(acc[j], p0, wv[(k0) <= R ? (k0) : 2 * R - (k0)], one);
+          if (k0 + 1 >= 0 && k0 + 1 <= 2 * R) acc[j] = mul_add2_rn(acc[j], p1, wv[(k0 + 1) <= R ? (k0 + 1) : 2 * R - (k0 + 1)], one);
         }
       }
       float* t0 = s_tmp + (2 * rp) * kTmpStride + HC * xg;
@@ -266,7 +273,7 @@ __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePla
 #pragma unroll
       for (int j = 0; j < RV; ++j) {
         const int k = i - j;
-        if (k >= 0 && k <= 2 * R) acc[j] = mul_add2_rn(acc[j], v, taps.w[k], taps.one);
+        if (k >= 0 && k <= 2 * R) acc[j] = mul_add2_rn(acc[j], v, wv[(k) <= R ? (k) : 2 * R - (k)], one);
       }
     }
     if (gx >= w) continue;
