@@ -213,6 +213,87 @@ def match_bench(ctx, torch, n_pairs: int = 32, n: int = 4096, reps: int = 5):
     }
 
 
+def _uneven_pair(k):
+    sys.path.insert(0, os.path.join(ROOT, "pure-sift_b200"))
+    import synth as S
+    return S.uneven_pair(k)
+
+
+def uneven_bench(ctx, torch, n_pairs: int = 32, reps: int = 3):
+    """Uneven batch: 64 images (32 pairs A_i, B_i = perspective warp of A_i), widths
+    U(480, 3840), aspect U(0.5, 2), blobs in proportion to area; SiftConfig octaves 4,
+    threshold 0.015, upsampling, uncapped features.  All 64 images in one device
+    batch call (one launch per stage; CUDA-graph replay), then the 32 pairs matched
+    in one call with the exact FP32 kernel and with BF16 + certified re-rank."""
+    import multiprocessing as mp
+    import psift
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        pairs = pool.map(_uneven_pair, range(n_pairs))
+    imgs = [im for ab in pairs for im in ab]
+    B = len(imgs)
+    cap = 65536
+    d_imgs = [torch.from_numpy(im).cuda() for im in imgs]
+    outs = [{k: torch.empty(cap, dtype=torch.float32, device="cuda") for k in "xysro"} for _ in range(B)]
+    for o in outs:
+        o["d"] = torch.empty((cap, 128), dtype=torch.float32, device="cuda")
+    counts = torch.zeros(B, dtype=torch.int32, device="cuda")
+    ccfg = psift.SiftConfig().with_octaves(OCTAVES).with_scales(SCALES).with_contrast_threshold(THRESH) \
+        .max_features(0).to_c()
+    cimgs = (psift.CImageU8 * B)(*[psift.CImageU8(t.data_ptr(), t.shape[0], t.shape[1], t.shape[1]) for t in d_imgs])
+    couts = (psift.CFeatures * B)(*[psift.CFeatures(cap, 0, o["x"].data_ptr(), o["y"].data_ptr(), o["s"].data_ptr(),
+                                                    o["r"].data_ptr(), o["o"].data_ptr(), o["d"].data_ptr())
+                                    for o in outs])
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    run = lambda: ctx.check(ctx.lib.psift_detect_and_compute_batch_dev(ctx.handle, cimgs, B, C.byref(ccfg), couts,
+                                                                      C.c_void_p(counts.data_ptr())))
+    for _ in range(2):
+        run()
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    ctx.synchronize()
+    det_ms = e0.elapsed_time(e1) / reps
+    cnt = counts.cpu().numpy().astype(np.int64)
+    mpx = sum(im.size for im in imgs) / 1e6
+    # match A_i against B_i, all pairs in one call
+    mouts = [torch.zeros((int(max(cnt[2 * i], 1)), 10), dtype=torch.float32, device="cuda") for i in range(n_pairs)]
+    mcounts = [torch.zeros(1, dtype=torch.int32, device="cuda") for _ in range(n_pairs)]
+    xy = [torch.stack([o["x"], o["y"]], dim=1).contiguous() for o in outs]
+    jobs = (psift.CMatchJob * n_pairs)(*[psift.CMatchJob(outs[2 * i]["d"].data_ptr(), outs[2 * i + 1]["d"].data_ptr(),
+                                                         xy[2 * i].data_ptr(), xy[2 * i + 1].data_ptr(),
+                                                         int(cnt[2 * i]), int(cnt[2 * i + 1]),
+                                                         mouts[i].data_ptr(), mouts[i].shape[0],
+                                                         mcounts[i].data_ptr()) for i in range(n_pairs)])
+    res, lists = {}, {}
+    for name, prec in (("fp32", psift.PRECISION_FP32), ("bf16_rerank", psift.PRECISION_BF16_RERANK)):
+        opt = psift.MatchOptions(0.8, False, prec).to_c()
+        call = lambda: ctx.check(ctx.lib.psift_match_batch_dev(ctx.handle, jobs, n_pairs, C.byref(opt)))
+        call()
+        ctx.synchronize()
+        e0.record(stream)
+        call()
+        e1.record(stream)
+        ctx.synchronize()
+        res[name] = e0.elapsed_time(e1)
+        lists[name] = [mouts[i][: int(mcounts[i].item())].cpu().numpy().tobytes() for i in range(n_pairs)]
+    flops = sum(2.0 * cnt[2 * i] * cnt[2 * i + 1] * 128 for i in range(n_pairs))
+    return {
+        "workload": f"{B} images (widths U(480,3840), aspect U(0.5,2), {mpx:.0f} Mpx total), uncapped; "
+                    f"{n_pairs} pairs A_i vs warp(A_i), ratio 0.8",
+        "detect_ms_batch": det_ms, "detect_images_per_s": B / (det_ms * 1e-3),
+        "detect_mpx_per_s": mpx / (det_ms * 1e-3),
+        "features_per_image": {"min": int(cnt.min()), "median": int(np.median(cnt)), "max": int(cnt.max())},
+        "match_fp32_ms_32_pairs": res["fp32"], "match_bf16_rerank_ms_32_pairs": res["bf16_rerank"],
+        "match_speedup_bf16_vs_fp32": res["fp32"] / res["bf16_rerank"],
+        "identical_match_lists": lists["fp32"] == lists["bf16_rerank"],
+        "matches_total": int(sum(int(m.item()) for m in mcounts)),
+        "bf16_tflops_effective": flops / (res["bf16_rerank"] * 1e-3) / 1e12,
+    }
+
+
 def catalog_bench(ctx, torch, n_cat: int = 2_000_000, n_q: int = 4096, k: int = 64, reps: int = 5):
     """Catalog search: 2M SIFT-like catalog descriptors (10,000 images x 200;
     |N(0,1)| L2-normalised, clipped at 0.2, renormalised), binarised to 128-bit
@@ -494,7 +575,7 @@ def run_ours(args):
             "stage_ms_per_step": {k: v[0] / reps for k, v in st.items() if v[1]},
             "clocks": clk.summary(),
         }
-        for key, fn in (("catalog", catalog_bench), ("learned_ransac", ransac_bench)):
+        for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench), ("learned_ransac", ransac_bench)):
             if getattr(args, "no_" + key):
                 continue
             try:
@@ -533,6 +614,7 @@ def main():
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
     ap.add_argument("--no-catalog", action="store_true")
+    ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -50,6 +50,7 @@ struct RansacJob {
   int* has_model;
   int* count;
   int* iters;               // [0] similarity iterations, [1] homography iterations
+  double* pts;              // 4 per match: the current inlier list's coordinates, gathered
 };
 
 struct RShared {
@@ -82,6 +83,7 @@ struct RShared {
   double dres[16];
   double ata[9][9];
   int draw_ptr, draws_ready;
+  int draws_s[2 * kDrawChunk];  // draw t lives at [t % (2 * kDrawChunk)]
   int sim_count;
   float sim_model[6];
   int has_sim;
@@ -129,8 +131,20 @@ __device__ void build_cdf(const RansacJob& J, RShared& S) {
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    // running sum in order; 16 weights are loaded ahead of the dependent additions
     double acc = 0.0;
-    for (int i = 0; i < n; ++i) {
+    int i = 0;
+    for (; i + 16 <= n; i += 16) {
+      double w[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) w[u] = J.cdf[i + u];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        acc += w[u];
+        J.cdf[i + u] = acc;
+      }
+    }
+    for (; i < n; ++i) {
       acc += J.cdf[i];
       J.cdf[i] = acc;
     }
@@ -255,8 +269,19 @@ __device__ float sim_err(const RansacJob& J, RShared& S, float a, float b, float
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    // in order; 16 loads are issued ahead of the dependent additions
     float s = 0.0f;
-    for (int i = 0; i < S.n; ++i) {
+    const int n = S.n;
+    int i = 0;
+    for (; i + 16 <= n; i += 16) {
+      float e[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) e[u] = buf[i + u];
+#pragma unroll
+      for (int u = 0; u < 16; ++u)
+        if (e[u] >= 0.0f) s += e[u];
+    }
+    for (; i < n; ++i) {
       const float e = buf[i];
       if (e >= 0.0f) s += e;
     }
@@ -316,12 +341,21 @@ __device__ bool procrustes(const RansacJob& J, RShared& S, int k, float* out6) {
     return true;
   }
   const float inv_n = 1.0f / (float)k;
+  // Gather the inliers (list order): P[j] = (q.x, q.y, t.x, t.y); the sums stay
+  // sequential in list order, their loads contiguous and issued ahead.
+  float4* P = reinterpret_cast<float4*>(J.pts);
+  for (int j = threadIdx.x; j < k; j += kRThreads) {
+    const psift_match& m = J.m[J.list[j]];
+    P[j] = make_float4(m.query_x, m.query_y, m.target_x, m.target_y);
+  }
+  __syncthreads();
   if (threadIdx.x < 4) {
     float s = 0.0f;
+    const int c = threadIdx.x;
+#pragma unroll 8
     for (int j = 0; j < k; ++j) {
-      const psift_match& m = J.m[J.list[j]];
-      const float v = threadIdx.x == 0 ? m.query_x : threadIdx.x == 1 ? m.query_y : threadIdx.x == 2 ? m.target_x : m.target_y;
-      s += v;
+      const float4 p = P[j];
+      s += c == 0 ? p.x : c == 1 ? p.y : c == 2 ? p.z : p.w;
     }
     S.fres[threadIdx.x] = s * inv_n;
   }
@@ -329,9 +363,10 @@ __device__ bool procrustes(const RansacJob& J, RShared& S, int k, float* out6) {
   const float mqx = S.fres[0], mqy = S.fres[1], mtx = S.fres[2], mty = S.fres[3];
   if (threadIdx.x < 3) {
     float s = 0.0f;
+#pragma unroll 8
     for (int j = 0; j < k; ++j) {
-      const psift_match& m = J.m[J.list[j]];
-      const float qx = m.query_x - mqx, qy = m.query_y - mqy, tx = m.target_x - mtx, ty = m.target_y - mty;
+      const float4 p = P[j];
+      const float qx = p.x - mqx, qy = p.y - mqy, tx = p.z - mtx, ty = p.w - mty;
       const float v = threadIdx.x == 0 ? qx * qx + qy * qy : threadIdx.x == 1 ? qx * tx + qy * ty : qx * ty - qy * tx;
       s += v;
     }
@@ -608,8 +643,19 @@ __device__ double h_err(const RansacJob& J, RShared& S, const double* H) {
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    // in order; 16 loads are issued ahead of the dependent additions
     double s = 0.0;
-    for (int i = 0; i < S.n; ++i) {
+    const int n = S.n;
+    int i = 0;
+    for (; i + 16 <= n; i += 16) {
+      double e[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) e[u] = J.err[i + u];
+#pragma unroll
+      for (int u = 0; u < 16; ++u)
+        if (e[u] >= 0.0) s += e[u];
+    }
+    for (; i < n; ++i) {
       const double e = J.err[i];
       if (e >= 0.0) s += e;
     }
@@ -767,14 +813,24 @@ __device__ bool fit_dlt4(const psift_match* const* s, double* H) {
 // fit_homography_dlt_f64 over J.list[0..k) (k >= 4), whole CTA; result in S.dres[0..8], flag in S.flag.
 __device__ bool fit_dlt_list(const RansacJob& J, RShared& S, int k, double* H) {
   const double inv_n = 1.0 / (double)k;
+  // Gather the inliers (list order) as doubles: P[j] = (q.x, q.y, t.x, t.y).  The
+  // sums below stay sequential in list order (the reference's order); only the
+  // loads change: contiguous, issued ahead of the dependent additions.
+  double4* P = reinterpret_cast<double4*>(J.pts);
+  for (int j = threadIdx.x; j < k; j += kRThreads) {
+    const psift_match& m = J.m[J.list[j]];
+    P[j] = make_double4((double)m.query_x, (double)m.query_y, (double)m.target_x, (double)m.target_y);
+  }
+  __syncthreads();
   if (threadIdx.x < 4) {
     double s = 0.0;
     bool finite = true;
+    const int c = threadIdx.x;
+#pragma unroll 8
     for (int j = 0; j < k; ++j) {
-      const psift_match& m = J.m[J.list[j]];
-      const double v = threadIdx.x == 0 ? m.query_x : threadIdx.x == 1 ? m.query_y : threadIdx.x == 2 ? m.target_x : m.target_y;
-      const double qx = m.query_x, qy = m.query_y, tx = m.target_x, ty = m.target_y;
-      if (!isfinite(qx) || !isfinite(qy) || !isfinite(tx) || !isfinite(ty)) finite = false;
+      const double4 p = P[j];
+      const double v = c == 0 ? p.x : c == 1 ? p.y : c == 2 ? p.z : p.w;
+      if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(p.w)) finite = false;
       s += v;
     }
     S.dres[threadIdx.x] = s * inv_n;
@@ -787,16 +843,12 @@ __device__ bool fit_dlt_list(const RansacJob& J, RShared& S, int k, double* H) {
   if (!finite) return false;
   if (threadIdx.x < 2) {
     double s = 0.0;
+    const double cx = threadIdx.x == 0 ? cxq : cxt, cy = threadIdx.x == 0 ? cyq : cyt;
+#pragma unroll 8
     for (int j = 0; j < k; ++j) {
-      const psift_match& m = J.m[J.list[j]];
-      double dx, dy;
-      if (threadIdx.x == 0) {
-        dx = (double)m.query_x - cxq;
-        dy = (double)m.query_y - cyq;
-      } else {
-        dx = (double)m.target_x - cxt;
-        dy = (double)m.target_y - cyt;
-      }
+      const double4 p = P[j];
+      const double dx = (threadIdx.x == 0 ? p.x : p.z) - cx;
+      const double dy = (threadIdx.x == 0 ? p.y : p.w) - cy;
       s += sqrt(dx * dx + dy * dy);
     }
     S.dres[4 + threadIdx.x] = s * inv_n;
@@ -806,6 +858,12 @@ __device__ bool fit_dlt_list(const RansacJob& J, RShared& S, int k, double* H) {
   __syncthreads();
   if (!isfinite(mdq) || !isfinite(mdt) || mdq < 1e-6 || mdt < 1e-6) return false;
   const double sq = 1.41421356237309504880 / mdq, st = 1.41421356237309504880 / mdt;
+  // normalised coordinates in place: (x, y, x', y')
+  for (int j = threadIdx.x; j < k; j += kRThreads) {
+    const double4 p = P[j];
+    P[j] = make_double4((p.x - cxq) * sq, (p.y - cyq) * sq, (p.z - cxt) * st, (p.w - cyt) * st);
+  }
+  __syncthreads();
   // upper triangle of A^T A: entry (a, b), a <= b, one thread each, sequential over the list
   if (threadIdx.x < 45) {
     int a = 0, rem = threadIdx.x;
@@ -815,10 +873,10 @@ __device__ bool fit_dlt_list(const RansacJob& J, RShared& S, int k, double* H) {
     }
     const int b = a + rem;
     double s = 0.0;
+#pragma unroll 8
     for (int j = 0; j < k; ++j) {
-      const psift_match& m = J.m[J.list[j]];
-      const double x = ((double)m.query_x - cxq) * sq, y = ((double)m.query_y - cyq) * sq;
-      const double xp = ((double)m.target_x - cxt) * st, yp = ((double)m.target_y - cyt) * st;
+      const double4 p = P[j];
+      const double x = p.x, y = p.y, xp = p.z, yp = p.w;
       const double r1[9] = {-x, -y, -1.0, 0.0, 0.0, 0.0, x * xp, y * xp, xp};
       const double r2[9] = {0.0, 0.0, 0.0, -x, -y, -1.0, x * yp, y * yp, yp};
       s += r1[a] * r1[b] + r2[a] * r2[b];
@@ -959,7 +1017,7 @@ __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __re
       const int need = S.draw_ptr + kDrawChunk;
       for (int t0 = S.draws_ready; t0 < need && t0 < J.draw_cap; t0 += kRThreads) {
         const int t = t0 + threadIdx.x;
-        if (t < need && t < J.draw_cap) J.draws[t] = sample_at(J.cdf, n, seed, (uint64_t)t);
+        if (t < need && t < J.draw_cap) S.draws_s[t % (2 * kDrawChunk)] = sample_at(J.cdf, n, seed, (uint64_t)t);
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -970,7 +1028,7 @@ __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __re
           int q[4] = {0, 0, 0, 0};
           while (chosen < 4 && attempts < 16) {
             ++attempts;
-            const int c = J.draws[p++];
+            const int c = S.draws_s[(p++) % (2 * kDrawChunk)];
             bool dup = false;
             for (int j = 0; j < chosen; ++j) dup |= q[j] == c;
             if (!dup) q[chosen++] = c;

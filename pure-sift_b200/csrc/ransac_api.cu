@@ -29,6 +29,7 @@ struct RansacJob {
   int* has_model;
   int* count;
   int* iters;
+  double* pts;  // 4 per match: the current inlier list's coordinates, gathered
 };
 cudaError_t launch_ransac(const RansacJob* jobs, int n_jobs, cudaStream_t st);
 size_t ransac_job_bytes();
@@ -54,7 +55,7 @@ psift_status run_batch(psift_ctx* ctx, const psift_ransac_job* jobs, int n, cons
   size_t bytes = sizeof(RansacJob) * n + 4096;
   for (int i = 0; i < n; ++i) {
     const size_t m = jobs[i].n;
-    bytes += 8 * m + 8 * m + 4 * m + 4 * (size_t)kDrawCap + 4 * 256 + 4096;
+    bytes += 8 * m + 8 * m + 4 * m + 32 * m + 4 * (size_t)kDrawCap + 5 * 256 + 4096;
   }
   psift_status st = arena_reserve(ctx, bytes);
   if (st != PSIFT_OK) return st;
@@ -77,6 +78,7 @@ psift_status run_batch(psift_ctx* ctx, const psift_ransac_job* jobs, int n, cons
     R.cdf = (double*)arena_alloc(ctx, 8 * m + 8);
     R.err = (double*)arena_alloc(ctx, 8 * m + 8);
     R.list = (int*)arena_alloc(ctx, 4 * m + 4);
+    R.pts = (double*)arena_alloc(ctx, 32 * m + 32);
     R.draws = (int*)arena_alloc(ctx, 4 * (size_t)kDrawCap);
     R.draw_cap = kDrawCap;
     R.mask = J.inlier_mask;

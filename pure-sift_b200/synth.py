@@ -158,6 +158,18 @@ def uneven_batch_shapes(n: int, seed: int = 3):
     return shapes
 
 
+def uneven_pair(k: int, seed: int = 3):
+    """Pair k of the uneven batch: A of shape uneven_batch_shapes(...)[k] with blobs in
+    proportion to its area (2000 per 1920x1080), B = A under a 1080p-pair-style
+    perspective warp about its centre.  Returns (A, B)."""
+    h, w = uneven_batch_shapes(k + 1, seed)[k]
+    n_blobs = max(1, int(round(2000 * (w * h) / (1920 * 1080))))
+    a = blob_image(w, h, n_blobs, 1.5, 20.0, seed * 100003 + k)
+    u = SplitMix64((seed * 7919 + k) ^ 0xABCDEF).uniform(4)
+    H = perspective_h(w, h, -30 + 60 * u[0], 0.7 + 0.7 * u[1], -2e-4 + 4e-4 * u[2], -2e-4 + 4e-4 * u[3])
+    return a, warp_image(a, H)
+
+
 def sift_like_descriptors(n: int, seed: int) -> np.ndarray:
     """|N(0,1)| per element, L2-normalised, clipped at 0.2, renormalised (float32, n x 128)."""
     rng = SplitMix64(seed)
