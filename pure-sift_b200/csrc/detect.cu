@@ -397,6 +397,12 @@ uint32_t float_bits(float f) {
   return u;
 }
 
+// Queues the job as two chunk views, chunk c on stream c (images [0, n/2) and
+// [n/2, n)), forked from and joined back to the context's stream by events; the
+// two chunks' kernels fill each other's idle SMs (small octaves, launch tails,
+// serial stages).  The plan table must already be on the device.
+psift_status launch_detect_split(psift_ctx* ctx, DetectJob& job, const psift_sift_config& cfg);
+
 // True when p lies in page-locked host memory (cudaMallocHost / cudaHostRegister).
 bool is_host_pinned(const void* p) {
   cudaPointerAttributes a;
@@ -405,6 +411,31 @@ bool is_host_pinned(const void* p) {
     return false;
   }
   return a.type == cudaMemoryTypeHost;
+}
+
+psift_status launch_detect_split(psift_ctx* ctx, DetectJob& job, const psift_sift_config& cfg) {
+  const int n = job.n;
+  if (n < 2) return launch_detect(ctx, job, cfg, false, nullptr, true);
+  PSIFT_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream2, ctx->ev_fork, 0));
+  const int split = (n + 1) / 2;
+  cudaStream_t streams[2] = {ctx->stream, ctx->stream2};
+  for (int c = 0; c < 2; ++c) {
+    const int b = c == 0 ? 0 : split, e = c == 0 ? split : n;
+    DetectJob v;
+    v.n = e - b;
+    v.plans.assign(job.plans.begin() + b, job.plans.begin() + e);
+    v.oct.assign(job.oct.begin() + (size_t)b * kMaxOctaves, job.oct.begin() + (size_t)e * kMaxOctaves);
+    v.n_oct.assign(job.n_oct.begin() + b, job.n_oct.begin() + e);
+    v.d_plans = job.d_plans + b;
+    v.kp_cap = job.kp_cap;
+    v.sel_cap = job.sel_cap;
+    psift_status st = launch_detect(ctx, v, cfg, false, streams[c], true);
+    if (st != PSIFT_OK) return st;
+  }
+  PSIFT_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_join, ctx->stream2));
+  PSIFT_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+  return PSIFT_OK;
 }
 
 psift_status check_common(psift_ctx* ctx, const psift_sift_config* cfg) {
@@ -759,11 +790,12 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
   DetectJob job;
   st = build_job(ctx, imgs, *cfg, job, 0, nullptr);
   if (st != PSIFT_OK) return st;
-  if (!ctx->graphs_enabled || ctx->timer.enabled) return launch_detect(ctx, job, *cfg, false);
   // The plan table (image, output and workspace pointers) is data: it is uploaded
   // before every run, so one graph serves every call with the same geometry.
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice,
                                       ctx->stream));
+  if (ctx->timer.enabled) return launch_detect(ctx, job, *cfg, false, nullptr, true);
+  if (!ctx->graphs_enabled) return launch_detect_split(ctx, job, *cfg);
   std::string key;
   {
     char buf[160];
@@ -778,14 +810,14 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
   }
   auto it = ctx->graphs.find(key);
   if (it == ctx->graphs.end()) {
-    if (ctx->graph_seen[key]++ == 0) return launch_detect(ctx, job, *cfg, false, nullptr, true);
+    if (ctx->graph_seen[key]++ == 0) return launch_detect_split(ctx, job, *cfg);
     if (ctx->graphs.size() >= 32) {
       for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
       ctx->graphs.clear();
     }
     const uint64_t l0 = ctx->launches;
     PSIFT_CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    st = launch_detect(ctx, job, *cfg, false, nullptr, true);
+    st = launch_detect_split(ctx, job, *cfg);
     cudaGraph_t graph = nullptr;
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
     if (st != PSIFT_OK) {
