@@ -307,6 +307,7 @@ __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const Image
   const int n = (y_max >= y_min && x_max >= x_min && O.h >= 3 && O.w >= 3) ? (y_max - y_min + 1) * wx : 0;
   const float bin_per_rad = 8.0f / two_pi;
   const int col = lane & (kHistCols - 1), half = lane >> 4;
+  const int q32 = wx > 0 ? 32 / wx : 0, r32 = wx > 0 ? 32 - q32 * wx : 0;
 
   for (uint32_t q = 0; q < nori; ++q) {
     const uint32_t f = f0 + q;
@@ -326,8 +327,10 @@ __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const Image
         const int t = t0 + 32 * k;
         const int py = yy, px = xx;
         packed[k] = ((uint32_t)py << 16) | (uint32_t)px;
-        xx += 32;
-        while (xx > x_max) {
+        // advance 32 pixels: q32 whole rows plus r32 columns, at most one wrap
+        xx += r32;
+        yy += q32;
+        if (xx > x_max) {
           xx -= wx;
           ++yy;
         }
@@ -383,20 +386,25 @@ __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const Image
             dof = o_bin - (float)o0;
           }
         }
+        // Branch-free trilinear update: a cell outside the 4x4 grid (or a lane
+        // without a pixel) adds +0 to a valid bin.  Every contribution is >= +0
+        // and every bin starts at +0, so adding +0 leaves the bin unchanged and
+        // the real contributions keep their order.
+        if (!live) wm = 0.0f;
 #pragma unroll
         for (int hp = 0; hp < 2; ++hp) {
-          if (live && half == hp) {
+          if (half == hp) {
 #pragma unroll
             for (int ir = 0; ir <= 1; ++ir) {
               const int rb = r0 + ir;
-              if (rb < 0 || rb >= 4) continue;
-              const float wr = ir == 0 ? 1.0f - dr : dr;
+              const bool vr = (unsigned)rb < 4u;
+              const float wr = vr ? (ir == 0 ? 1.0f - dr : dr) : 0.0f;
 #pragma unroll
               for (int ic = 0; ic <= 1; ++ic) {
                 const int cb = c0 + ic;
-                if (cb < 0 || cb >= 4) continue;
-                const float wc = ic == 0 ? 1.0f - dc : dc;
-                float* cell = &hist[(rb * 4 + cb) * 8][col];
+                const bool vc = (unsigned)cb < 4u;
+                const float wc = vc ? (ic == 0 ? 1.0f - dc : dc) : 0.0f;
+                float* cell = &hist[((vr ? rb : 0) * 4 + (vc ? cb : 0)) * 8][col];
                 const float wrc = wm * wr * wc;
                 cell[(o0 & 7) * kHistCols] += wrc * (1.0f - dof);
                 cell[((o0 + 1) & 7) * kHistCols] += wrc * dof;
