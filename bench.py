@@ -641,6 +641,8 @@ def main():
     ap.add_argument("--only-device", action="store_true", help="time the device path only (profiling case)")
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
+    ap.add_argument("--only-section", choices=["match", "catalog", "learned_ransac", "uneven_batch"],
+                    help="run one section alone (profiling case)")
     ap.add_argument("--no-catalog", action="store_true")
     ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
@@ -648,10 +650,16 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.match_only:
+        args.only_section = "match"
+    if args.only_section:
+        # one section alone (profiling cases); sizes as in the full run
         import torch
         import psift
         ctx = psift.Context(int(os.environ.get("LOCAL_RANK", "0")))
-        print(json.dumps(match_bench(ctx, torch, n_pairs=args.match_pairs, reps=args.steps)), flush=True)
+        fns = {"match": lambda: match_bench(ctx, torch, n_pairs=args.match_pairs, reps=args.steps),
+               "catalog": lambda: catalog_bench(ctx, torch), "learned_ransac": lambda: ransac_bench(ctx, torch),
+               "uneven_batch": lambda: uneven_bench(ctx, torch)}
+        print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)
         ctx.close()
         return 0
     return run_ours(args)

@@ -38,6 +38,30 @@ __device__ __forceinline__ int ham128(uint32_t a0, uint32_t a1, uint32_t a2, uin
 
 __device__ __forceinline__ bool has_zero_byte(uint32_t x) { return ((x - 0x01010101u) & ~x & 0x80808080u) != 0; }
 
+// quantize_descriptor_u128 (src/catalog.rs:37-45): bit d = desc[d] > 0.065.
+// A warp handles kQDesc descriptors; lane l reads dims l, l + 32, l + 64, l + 96
+// of each (coalesced 128-byte rows, all loads issued first) and the ballot of
+// "dim 32 w + l > 0.065" over the lanes is code word w, bit l.
+constexpr int kQDesc = 4;
+__global__ void __launch_bounds__(256) quantize_codes_kernel(const float* __restrict__ desc, int n,
+                                                             uint64_t* __restrict__ codes) {
+  const int lane = threadIdx.x & 31;
+  const int row0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kQDesc;
+  float v[kQDesc][4];
+#pragma unroll
+  for (int d = 0; d < kQDesc; ++d)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) v[d][w] = row0 + d < n ? __ldcs(desc + (size_t)(row0 + d) * 128 + 32 * w + lane) : 0.0f;
+#pragma unroll
+  for (int d = 0; d < kQDesc; ++d) {
+    uint32_t word[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) word[w] = __ballot_sync(0xffffffffu, v[d][w] > 0.065f);
+    if (lane < 2 && row0 + d < n)
+      codes[2 * (size_t)(row0 + d) + lane] = (uint64_t)word[2 * lane] | ((uint64_t)word[2 * lane + 1] << 32);
+  }
+}
+
 // quantize_descriptor_u128 + quantize_descriptor_u8: one warp per descriptor.
 __global__ void quantize_kernel(const float* __restrict__ desc, int n, uint64_t* __restrict__ codes,
                                 uint8_t* __restrict__ u8) {
@@ -161,12 +185,16 @@ __global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4*
     qw[j][2] = v.z;
     qw[j][3] = v.w;
   }
-  unsigned long long maxkey[kQG];
+  // Within a chunk the codes come in increasing index, so every listed entry has
+  // a smaller index than the current code: key < max key is exactly
+  // distance < max distance (the empty entries have distance 2^32 - 1).  Only
+  // the distance is compared per pair; keys are built on insertion.
+  uint32_t maxd[kQG];
   int maxpos[kQG];
 #pragma unroll
   for (int j = 0; j < kQG; ++j) {
     for (int t = lane; t < kTopKMax; t += 32) list[j][t] = t < k ? ~0ull : 0ull;
-    maxkey[j] = ~0ull;
+    maxd[j] = 0xFFFFFFFFu;
     maxpos[j] = 0;
   }
   __syncwarp();
@@ -176,14 +204,14 @@ __global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4*
     const uint4 c = valid ? cat[idx] : make_uint4(0, 0, 0, 0);
 #pragma unroll
     for (int j = 0; j < kQG; ++j) {
-      const uint32_t d = valid ? (uint32_t)ham128(qw[j][0], qw[j][1], qw[j][2], qw[j][3], c) : 0x7fffffffu;
-      const unsigned long long key = ((unsigned long long)d << 32) | (unsigned long long)(uint32_t)idx;
-      unsigned m = __ballot_sync(0xffffffffu, valid && key < maxkey[j]);
+      const uint32_t d = (uint32_t)ham128(qw[j][0], qw[j][1], qw[j][2], qw[j][3], c);
+      unsigned m = __ballot_sync(0xffffffffu, valid && d < maxd[j]);
       while (m) {
         const int L = __ffs(m) - 1;
         m &= m - 1;
-        const unsigned long long kl = __shfl_sync(0xffffffffu, key, L);
-        if (kl < maxkey[j]) {
+        const uint32_t dl = __shfl_sync(0xffffffffu, d, L);
+        if (dl < maxd[j]) {
+          const unsigned long long kl = ((unsigned long long)dl << 32) | (unsigned long long)(uint32_t)(base + L);
           if (lane == 0) list[j][maxpos[j]] = kl;
           __syncwarp();
           // new maximum of the k entries (slots >= k hold 0 and never win)
@@ -194,7 +222,7 @@ __global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4*
           const unsigned who = __ballot_sync(0xffffffffu, mine == mx);
           const int src = __ffs(who) - 1;
           maxpos[j] = __shfl_sync(0xffffffffu, mine_pos, src);
-          maxkey[j] = mx;
+          maxd[j] = (uint32_t)(mx >> 32);
           __syncwarp();
         }
       }
@@ -309,7 +337,8 @@ __global__ void l2_rerank_kernel(const float* __restrict__ qd, int nq, const flo
 
 cudaError_t launch_quantize(const float* desc, int n, uint64_t* codes, uint8_t* u8, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  quantize_kernel<<<(n + 7) / 8, 256, 0, st>>>(desc, n, codes, u8);
+  if (codes) quantize_codes_kernel<<<(n + 8 * kQDesc - 1) / (8 * kQDesc), 256, 0, st>>>(desc, n, codes);
+  if (u8) quantize_kernel<<<(n + 7) / 8, 256, 0, st>>>(desc, n, nullptr, u8);
   return cudaGetLastError();
 }
 

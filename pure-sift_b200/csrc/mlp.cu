@@ -7,7 +7,8 @@
 // and accumulates in f32.  The backward pass is f32 on the same bf16-rounded
 // operands (straight-through rounding).  Training is deterministic:
 //   mlp_fwd_bwd_kernel   one thread per sample: forward, dL/dz for every layer;
-//   mlp_grad_kernel      one thread per parameter: the batch sum in sample order;
+//   mlp_grad_partial_kernel / mlp_grad_reduce_kernel: per-parameter sums over
+//                        chunks of samples in order, then over the chunks in order;
 //   mlp_adam_kernel      Adam update of the f32 masters.
 // Loss: mean binary cross-entropy over the minibatch.
 #include <algorithm>
@@ -136,32 +137,47 @@ __global__ void __launch_bounds__(128) mlp_fwd_bwd_kernel(const float* __restric
   loss_o[b] = l;
 }
 
-// One thread per parameter: sum over the batch in sample order.
-__global__ void mlp_grad_kernel(int B, const float* __restrict__ xb, const float* __restrict__ h1b,
-                                const float* __restrict__ h2b, const float* __restrict__ dz1,
-                                const float* __restrict__ dz2, const float* __restrict__ dz3,
-                                float* __restrict__ grad) {
+// Gradient sums, deterministic: the batch is cut into chunks of kGradChunk
+// samples; mlp_grad_partial_kernel (one thread per (parameter, chunk)) sums a
+// chunk in sample order, mlp_grad_reduce_kernel adds the chunks' sums in chunk
+// order.  Fixed order, so every run gives the same bits.
+constexpr int kGradChunk = 128;
+
+__global__ void mlp_grad_partial_kernel(int B, const float* __restrict__ xb, const float* __restrict__ h1b,
+                                        const float* __restrict__ h2b, const float* __restrict__ dz1,
+                                        const float* __restrict__ dz2, const float* __restrict__ dz3,
+                                        float* __restrict__ partial) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= kNP) return;
+  const int b0 = blockIdx.y * kGradChunk;
+  const int b1 = min(B, b0 + kGradChunk);
   float g = 0.0f;
   if (p < kOffB1) {
     const int j = (p - kOffW1) / kF, k = (p - kOffW1) % kF;
-    for (int b = 0; b < B; ++b) g = __fmaf_rn(dz1[(size_t)b * kH + j], xb[(size_t)b * kF + k], g);
+    for (int b = b0; b < b1; ++b) g = __fmaf_rn(dz1[(size_t)b * kH + j], xb[(size_t)b * kF + k], g);
   } else if (p < kOffW2) {
     const int j = p - kOffB1;
-    for (int b = 0; b < B; ++b) g += dz1[(size_t)b * kH + j];
+    for (int b = b0; b < b1; ++b) g += dz1[(size_t)b * kH + j];
   } else if (p < kOffB2) {
     const int j = (p - kOffW2) / kH, k = (p - kOffW2) % kH;
-    for (int b = 0; b < B; ++b) g = __fmaf_rn(dz2[(size_t)b * kH + j], h1b[(size_t)b * kH + k], g);
+    for (int b = b0; b < b1; ++b) g = __fmaf_rn(dz2[(size_t)b * kH + j], h1b[(size_t)b * kH + k], g);
   } else if (p < kOffW3) {
     const int j = p - kOffB2;
-    for (int b = 0; b < B; ++b) g += dz2[(size_t)b * kH + j];
+    for (int b = b0; b < b1; ++b) g += dz2[(size_t)b * kH + j];
   } else if (p < kOffB3) {
     const int j = p - kOffW3;
-    for (int b = 0; b < B; ++b) g = __fmaf_rn(dz3[b], h2b[(size_t)b * kH + j], g);
+    for (int b = b0; b < b1; ++b) g = __fmaf_rn(dz3[b], h2b[(size_t)b * kH + j], g);
   } else {
-    for (int b = 0; b < B; ++b) g += dz3[b];
+    for (int b = b0; b < b1; ++b) g += dz3[b];
   }
+  partial[(size_t)blockIdx.y * kNP + p] = g;
+}
+
+__global__ void mlp_grad_reduce_kernel(int chunks, const float* __restrict__ partial, float* __restrict__ grad) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kNP) return;
+  float g = 0.0f;
+  for (int c = 0; c < chunks; ++c) g += partial[(size_t)c * kNP + p];
   grad[p] = g;
 }
 
@@ -194,8 +210,11 @@ cudaError_t launch_mlp_infer(const float* params, const float* X, int n, float* 
   return cudaGetLastError();
 }
 
-// Workspace for a minibatch of B: (8 + 64*4 + 2) * B floats.
-size_t mlp_batch_floats(int B) { return (size_t)B * (kF + 4 * kH + 2); }
+// Workspace for a minibatch of B: (8 + 64*4 + 2) * B floats of per-sample
+// operands, then one row of kNP partial gradient sums per kGradChunk samples.
+size_t mlp_batch_floats(int B) {
+  return (size_t)B * (kF + 4 * kH + 2) + (size_t)((B + kGradChunk - 1) / kGradChunk) * kNP;
+}
 
 cudaError_t launch_mlp_step(float* params, const float* X, const float* Y, const int* idx, int B, float* work,
                             float* grad, float* m, float* v, float lr, int t, float* loss_out, bool update,
@@ -207,8 +226,11 @@ cudaError_t launch_mlp_step(float* params, const float* X, const float* Y, const
   float* dz2 = dz1 + (size_t)B * kH;
   float* dz3 = dz2 + (size_t)B * kH;
   float* lb = dz3 + B;
+  float* partial = lb + B;
+  const int chunks = (B + kGradChunk - 1) / kGradChunk;
   mlp_fwd_bwd_kernel<<<(B + 127) / 128, 128, 0, st>>>(params, X, Y, idx, B, xb, h1b, h2b, dz1, dz2, dz3, lb);
-  mlp_grad_kernel<<<(kNP + 127) / 128, 128, 0, st>>>(B, xb, h1b, h2b, dz1, dz2, dz3, grad);
+  mlp_grad_partial_kernel<<<dim3((kNP + 127) / 128, chunks), 128, 0, st>>>(B, xb, h1b, h2b, dz1, dz2, dz3, partial);
+  mlp_grad_reduce_kernel<<<(kNP + 127) / 128, 128, 0, st>>>(chunks, partial, grad);
   if (loss_out) mlp_loss_kernel<<<1, 32, 0, st>>>(lb, B, loss_out);
   if (update) {
     const float b1 = 0.9f, b2 = 0.999f;

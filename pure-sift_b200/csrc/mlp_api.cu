@@ -105,7 +105,7 @@ psift_status psift_mlp_train_dev(psift_ctx* ctx, float* params, const float* x, 
     const uint32_t start = (uint32_t)(((uint64_t)t * batch) % n);
     cudaError_t e = launch_mlp_step(params, x, y, d_perm + start, (int)batch, work, grad, m, v, lr, (int)t + 1,
                                     losses ? losses + t : nullptr, true, ctx->stream);
-    ctx->launches += losses ? 4 : 3;
+    ctx->launches += losses ? 5 : 4;
     if (e != cudaSuccess) return cuda_error(ctx, e, "mlp_train_step");
   }
   return PSIFT_OK;
@@ -122,7 +122,7 @@ psift_status psift_mlp_gradients_dev(psift_ctx* ctx, const float* params, const 
   float* work = (float*)arena_alloc(ctx, sizeof(float) * mlp_batch_floats((int)n));
   cudaError_t e = launch_mlp_step(const_cast<float*>(params), x, y, nullptr, (int)n, work, grad, nullptr, nullptr,
                                   0.0f, 1, loss, false, ctx->stream);
-  ctx->launches += loss ? 3 : 2;
+  ctx->launches += loss ? 4 : 3;
   if (e != cudaSuccess) return cuda_error(ctx, e, "mlp_gradients");
   return PSIFT_OK;
 }
