@@ -198,10 +198,13 @@ __global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4*
     maxpos[j] = 0;
   }
   __syncwarp();
+  // the next 32 codes are loaded while the current ones are compared
+  uint4 c_next = c_begin + lane < c_end ? cat[c_begin + lane] : make_uint4(0, 0, 0, 0);
   for (long long base = c_begin; base < c_end; base += 32) {
     const long long idx = base + lane;
     const bool valid = idx < c_end;
-    const uint4 c = valid ? cat[idx] : make_uint4(0, 0, 0, 0);
+    const uint4 c = c_next;
+    c_next = idx + 32 < c_end ? cat[idx + 32] : make_uint4(0, 0, 0, 0);
 #pragma unroll
     for (int j = 0; j < kQG; ++j) {
       const uint32_t d = (uint32_t)ham128(qw[j][0], qw[j][1], qw[j][2], qw[j][3], c);
