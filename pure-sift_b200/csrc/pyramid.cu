@@ -39,6 +39,7 @@ constexpr int kTileW = 64;
 constexpr int kTileH = 64;
 constexpr int kBlurThreads = 256;
 constexpr int kTmpStride = kTileW + 8;  // floats per intermediate row
+constexpr int kStageBatch = 4;          // staging units per thread with loads in flight
 
 struct Taps2 {
   float2 w[kMaxTaps];  // {w_k, w_k}
@@ -122,7 +123,7 @@ __device__ __forceinline__ float fetch_src(const ImagePlan& P, const OctaveDev& 
 //               writes the next octave's G[0] (even rows/columns).
 //   MODE_INIT_*: G[0] of octave 0 from the input image.
 template <int R, int HC, int RV, int MODE>
-__global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePlan* __restrict__ plans, int octave,
+__global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const ImagePlan* __restrict__ plans, int octave,
                                                                    int level, int down_level, int zrev, Taps2 taps) {
   using Gm = BlurGeom<R>;
   static_assert(HC == 4 || HC == 8, "horizontal outputs per thread");
@@ -186,14 +187,15 @@ __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePla
     return 0.25f * (((a + b) + c) + d);
   };
 
-  // 1. Stage the clamped input tile, rows interleaved in pairs.
+  // 1. Stage the clamped input tile, rows interleaved in pairs.  A thread's units
+  //    are taken kStageBatch at a time with all their loads issued before any
+  //    shared-memory store, so several loads are in flight per thread.
   const float* src_plane = O.g + (long long)(level - 1) * O.plane_stride;  // MODE_LEVEL only
-  for (int u = threadIdx.x; u < Gm::IN_PAIRS * Gm::C4; u += kBlurThreads) {
+  auto load_unit = [&](int u, float4& a, float4& b) {
     const int rp = u / Gm::C4, c4 = u - rp * Gm::C4;
     const int gy0 = clampi(ty0 - R + 2 * rp, 0, h - 1);
     const int gy1 = clampi(ty0 - R + 2 * rp + 1, 0, h - 1);
     const int gx = tx0 - Gm::RP + 4 * c4;
-    float4 a, b;
     if (MODE == MODE_LEVEL && gx >= 0 && gx + 3 < w) {
       a = __ldg(reinterpret_cast<const float4*>(src_plane + (long long)gy0 * O.pitch + gx));
       b = __ldg(reinterpret_cast<const float4*>(src_plane + (long long)gy1 * O.pitch + gx));
@@ -213,9 +215,23 @@ __global__ void __launch_bounds__(kBlurThreads) blur_level_kernel(const ImagePla
       a = make_float4(av[0], av[1], av[2], av[3]);
       b = make_float4(bv[0], bv[1], bv[2], bv[3]);
     }
-    float4* d = reinterpret_cast<float4*>(s_in + rp * Gm::IN_S + 4 * c4);
-    d[0] = make_float4(a.x, b.x, a.y, b.y);
-    d[1] = make_float4(a.z, b.z, a.w, b.w);
+  };
+  constexpr int kUnits = Gm::IN_PAIRS * Gm::C4;
+  for (int u0 = threadIdx.x; u0 < kUnits; u0 += kStageBatch * kBlurThreads) {
+    float4 a[kStageBatch], b[kStageBatch];
+#pragma unroll
+    for (int q = 0; q < kStageBatch; ++q)
+      if (u0 + q * kBlurThreads < kUnits) load_unit(u0 + q * kBlurThreads, a[q], b[q]);
+#pragma unroll
+    for (int q = 0; q < kStageBatch; ++q) {
+      const int u = u0 + q * kBlurThreads;
+      if (u < kUnits) {
+        const int rp = u / Gm::C4, c4 = u - rp * Gm::C4;
+        float4* d = reinterpret_cast<float4*>(s_in + rp * Gm::IN_S + 4 * c4);
+        d[0] = make_float4(a[q].x, b[q].x, a[q].y, b[q].y);
+        d[1] = make_float4(a[q].z, b[q].z, a[q].w, b[q].w);
+      }
+    }
   }
   __syncthreads();
 
