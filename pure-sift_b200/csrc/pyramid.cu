@@ -160,19 +160,28 @@ __global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const Image
     sy_lo = clampi(ty0 - R, 0, h - 1) >> 1;
     sx_lo = clampi(tx0 - Gm::RP, 0, w - 1) >> 1;
     const int sh = min(SRC_H, P.src_h - sy_lo), sw = min(SRC_W, P.src_w - sx_lo);
-    for (int i = threadIdx.x; i < SRC_H * SRC_W; i += kBlurThreads) {
+    // every load of the thread is issued before the first store
+    constexpr int kSrcIter = (SRC_H * SRC_W + kBlurThreads - 1) / kBlurThreads;
+    float v[kSrcIter];
+#pragma unroll
+    for (int q = 0; q < kSrcIter; ++q) {
+      const int i = threadIdx.x + q * kBlurThreads;
       const int r = i / SRC_W, c = i - r * SRC_W;
-      float v = 0.0f;
-      if (r < sh && c < sw) {
+      v[q] = 0.0f;
+      if (i < SRC_H * SRC_W && r < sh && c < sw) {
         const long long off = (long long)(sy_lo + r) * P.src_stride + (sx_lo + c);
         if constexpr (MODE == MODE_INIT_U8_UP) {
           const float inv255 = 1.0f / 255.0f;
-          v = (float)((const uint8_t*)P.src)[off] * inv255;
+          v[q] = (float)__ldg((const uint8_t*)P.src + off) * inv255;
         } else {
-          v = ((const float*)P.src)[off];
+          v[q] = __ldg((const float*)P.src + off);
         }
       }
-      s_tmp[i] = v;
+    }
+#pragma unroll
+    for (int q = 0; q < kSrcIter; ++q) {
+      const int i = threadIdx.x + q * kBlurThreads;
+      if (i < SRC_H * SRC_W) s_tmp[i] = v[q];
     }
     __syncthreads();
   }
@@ -196,6 +205,24 @@ __global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const Image
     const int gy0 = clampi(ty0 - R + 2 * rp, 0, h - 1);
     const int gy1 = clampi(ty0 - R + 2 * rp + 1, 0, h - 1);
     const int gx = tx0 - Gm::RP + 4 * c4;
+    if constexpr (kUp && R % 2 == 0) {
+      // Interior unit of an even-radius base: rows (gy0, gy0 + 1) = (2 y0, 2 y0 + 1)
+      // and columns 2 xs .. 2 xs + 3 need source rows y0, y1 and columns xs ..
+      // xs + 2 only; each output is the same four-term sum as up_sample.
+      if (gy0 == ty0 - R + 2 * rp && gy0 + 1 < h && gx >= 0 && gx + 3 < w) {
+        const int y0 = gy0 >> 1, y1 = min(y0 + 1, P.src_h - 1), xs = gx >> 1;
+        const int x2 = min(xs + 2, P.src_w - 1);
+        const float* r0 = s_tmp + (y0 - sy_lo) * SRC_W - sx_lo;
+        const float* r1 = s_tmp + (y1 - sy_lo) * SRC_W - sx_lo;
+        const float p0 = r0[xs], p1 = r0[xs + 1], p2 = r0[x2];
+        const float q0 = r1[xs], q1 = r1[xs + 1], q2 = r1[x2];
+        a = make_float4(0.25f * (((p0 + p0) + p0) + p0), 0.25f * (((p0 + p1) + p0) + p1),
+                        0.25f * (((p1 + p1) + p1) + p1), 0.25f * (((p1 + p2) + p1) + p2));
+        b = make_float4(0.25f * (((p0 + p0) + q0) + q0), 0.25f * (((p0 + p1) + q0) + q1),
+                        0.25f * (((p1 + p1) + q1) + q1), 0.25f * (((p1 + p2) + q1) + q2));
+        return;
+      }
+    }
     if (MODE == MODE_LEVEL && gx >= 0 && gx + 3 < w) {
       a = __ldg(reinterpret_cast<const float4*>(src_plane + (long long)gy0 * O.pitch + gx));
       b = __ldg(reinterpret_cast<const float4*>(src_plane + (long long)gy1 * O.pitch + gx));
