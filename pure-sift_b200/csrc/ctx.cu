@@ -3,6 +3,7 @@
 #include <cstring>
 #include <mutex>
 #include <map>
+#include <tuple>
 
 #include "psift_internal.cuh"
 
@@ -41,6 +42,27 @@ void* arena_alloc(psift_ctx* ctx, size_t bytes) {
   if (off + bytes > ctx->arena.capacity) return nullptr;
   ctx->arena.offset = off + bytes;
   return ctx->arena.base + off;
+}
+
+cudaError_t resident_ctas(const void* func, int threads, size_t smem, int* out) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_tuple(func, dev, threads, smem);
+  auto it = cache.find(key);
+  if (it != cache.end()) {
+    *out = it->second;
+    return cudaSuccess;
+  }
+  int per_sm = 0, sms = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  *out = cache[key] = per_sm * sms;
+  return cudaSuccess;
 }
 
 cudaError_t ensure_smem_attr(const void* func, size_t bytes) {

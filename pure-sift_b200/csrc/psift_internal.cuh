@@ -106,6 +106,8 @@ psift_status io_reserve(psift_ctx* ctx, size_t bytes);
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Raise a kernel's dynamic shared-memory limit once per (kernel, device).
 cudaError_t ensure_smem_attr(const void* func, size_t bytes);
+// CTAs of `func` resident on the whole device at once (occupancy x SMs), cached.
+cudaError_t resident_ctas(const void* func, int threads, size_t smem, int* out);
 
 // Stage timing: `StageScope sc(ctx, STAGE_X);` records events around the launches
 // issued while it is alive (no-op unless timing is enabled).

@@ -40,6 +40,7 @@ constexpr int kTileH = 64;
 constexpr int kBlurThreads = 256;
 constexpr int kTmpStride = kTileW + 8;  // floats per intermediate row
 constexpr int kStageBatch = 4;          // staging units per thread with loads in flight
+constexpr int kPrefetchWaves = 1;       // level blur: L2 prefetch distance in resident-CTA waves
 
 struct Taps2 {
   float2 w[kMaxTaps];  // {w_k, w_k}
@@ -118,14 +119,46 @@ __device__ __forceinline__ float fetch_src(const ImagePlan& P, const OctaveDev& 
   }
 }
 
+// L2 prefetch of the input rows of the tile `ahead` CTAs further in launch order
+// (one thread per staged row).  With `ahead` = the CTAs resident at once, that
+// tile is staged about one tile-time later and its loads hit L2, so the HBM
+// reads of the next wave overlap the arithmetic of this one.
+template <int R>
+__device__ __forceinline__ void prefetch_ahead_rows(const ImagePlan* __restrict__ plans, int octave, int level,
+                                                    int zrev, int ahead) {
+  using Gm = BlurGeom<R>;
+  const long long nxy = (long long)gridDim.x * gridDim.y;
+  const long long lin = blockIdx.x + (long long)gridDim.x * blockIdx.y + nxy * blockIdx.z + ahead;
+  if (lin >= nxy * gridDim.z) return;
+  const int bz = (int)(lin / nxy);
+  const int rem = (int)(lin - (long long)bz * nxy);
+  const int by = rem / (int)gridDim.x, bx = rem - by * (int)gridDim.x;
+  const ImagePlan& P = plans[zrev ? (int)gridDim.z - 1 - bz : bz];
+  if (octave >= P.n_oct) return;
+  const OctaveDev& O = P.oct[octave];
+  const int tx0 = bx * kTileW, ty0 = by * kTileH;
+  if (tx0 >= O.w || ty0 >= O.h) return;
+  // rows clamped like the staging; columns [c0, c1) are 16-byte aligned and end
+  // inside the row pitch (a multiple of 32 floats)
+  const int gy = clampi(ty0 - R + (int)threadIdx.x, 0, O.h - 1);
+  const int c0 = max(tx0 - Gm::RP, 0);
+  const int c1 = min(tx0 + kTileW + Gm::RP, (O.w + 3) & ~3);
+  const float* row = O.g + (long long)(level - 1) * O.plane_stride + (long long)gy * O.pitch + c0;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"((c1 - c0) * 4) : "memory");
+}
+
 // One blur level for every image of the batch (blockIdx.z = image, reversed when zrev).
 //   MODE_LEVEL: G[s] = blur(G[s-1]); D[s-1] = G[s] - G[s-1]; level `down_level` also
 //               writes the next octave's G[0] (even rows/columns).
 //   MODE_INIT_*: G[0] of octave 0 from the input image.
 template <int R, int HC, int RV, int MODE>
 __global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const ImagePlan* __restrict__ plans, int octave,
-                                                                   int level, int down_level, int zrev, Taps2 taps) {
+                                                                   int level, int down_level, int zrev, int pf_ahead,
+                                                                   Taps2 taps) {
   using Gm = BlurGeom<R>;
+  if constexpr (MODE == MODE_LEVEL) {
+    if (pf_ahead > 0 && threadIdx.x < Gm::IN_H) prefetch_ahead_rows<R>(plans, octave, level, zrev, pf_ahead);
+  }
   static_assert(HC == 4 || HC == 8, "horizontal outputs per thread");
   // The Gaussian taps are bit-symmetric (gaussian_kernel_1d evaluates the same
   // x^2 for +-x and normalises both by one sum), so w[k] = w[2R - k] exactly and
@@ -365,10 +398,18 @@ static cudaError_t launch_blur_r(const ImagePlan* plans, int n_images, int octav
                                  int zrev, const Taps2& taps, int max_h, int max_w, cudaStream_t st) {
   using Gm = BlurGeom<R>;
   const size_t smem = Gm::SMEM_BYTES;
-  cudaError_t e = ensure_smem_attr((const void*)blur_level_kernel<R, HC, RV, MODE>, smem);
+  const void* fn = (const void*)blur_level_kernel<R, HC, RV, MODE>;
+  cudaError_t e = ensure_smem_attr(fn, smem);
   if (e != cudaSuccess) return e;
+  int pf_ahead = 0;
+  if (MODE == MODE_LEVEL) {
+    e = resident_ctas(fn, kBlurThreads, smem, &pf_ahead);
+    if (e != cudaSuccess) return e;
+    pf_ahead *= kPrefetchWaves;
+  }
   dim3 grid((max_w + kTileW - 1) / kTileW, (max_h + kTileH - 1) / kTileH, n_images);
-  blur_level_kernel<R, HC, RV, MODE><<<grid, kBlurThreads, smem, st>>>(plans, octave, level, down_level, zrev, taps);
+  blur_level_kernel<R, HC, RV, MODE><<<grid, kBlurThreads, smem, st>>>(plans, octave, level, down_level, zrev,
+                                                                      pf_ahead, taps);
   return cudaGetLastError();
 }
 
