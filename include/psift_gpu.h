@@ -43,7 +43,9 @@ typedef enum psift_status {
   PSIFT_ERR_OUT_OF_MEMORY = 5,    /* device or pinned allocation failed */
   PSIFT_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up */
   PSIFT_ERR_NO_DEVICE = 7,        /* no usable sm_100 device */
-  PSIFT_ERR_INTERNAL = 8
+  PSIFT_ERR_INTERNAL = 8,
+  PSIFT_ERR_IO = 9,               /* a catalog file could not be opened, read, written or renamed */
+  PSIFT_ERR_FORMAT = 10           /* a PSIFTCAT file is malformed (magic, version, kind, truncation, UTF-8) */
 } psift_status;
 
 typedef struct psift_ctx psift_ctx;
@@ -345,6 +347,66 @@ psift_status psift_l2_rerank(psift_ctx* ctx, const float* query_desc, uint32_t n
 psift_status psift_l2_rerank_dev(psift_ctx* ctx, const float* query_desc, uint32_t nq,
                                  const float* catalog_desc, const uint32_t* candidates, uint32_t k,
                                  uint32_t* out_idx, float* out_d2);
+
+/* ---------------------------------------------------------------- device-resident catalog */
+/* FeatureCatalog (src/catalog.rs:182-702) with every entry's features, 128-bit
+ * codes and the entry table held in device memory, so that a search runs its
+ * votes, shortlist verification (Lowe matching, similarity and homography
+ * RANSAC) and tracking summaries as a few batched launches.  Entry order,
+ * upsert (replace in place or append), remove (swap_remove) and the PSIFTCAT v1
+ * file format follow the reference.  A catalog belongs to the context it was
+ * created with (its device and stream) and, like the context, is not
+ * thread-safe. */
+typedef struct psift_catalog psift_catalog;
+/* FeatureCatalog::new (src/catalog.rs:279-289) fields plus descriptor_kind. */
+typedef struct psift_catalog_params {
+  uint32_t octaves, scales;
+  float threshold;
+  int32_t descriptor_kind; /* 0 = Sift, 1 = RootSift */
+} psift_catalog_params;
+psift_status psift_catalog_create(psift_ctx* ctx, const psift_catalog_params* params, psift_catalog** out);
+psift_status psift_catalog_destroy(psift_catalog* cat);
+psift_status psift_catalog_params_get(const psift_catalog* cat, psift_catalog_params* out);
+uint32_t psift_catalog_size(const psift_catalog* cat);
+/* list_summaries (src/catalog.rs:355-366) for entry i: id copied NUL-terminated
+ * into id (truncated to id_capacity - 1 bytes; id_len receives the full length). */
+psift_status psift_catalog_entry(const psift_catalog* cat, uint32_t i, char* id, size_t id_capacity,
+                                 uint32_t* id_len, uint32_t* width, uint32_t* height, uint64_t* feature_count);
+/* Index of the entry with this id (the reference's id_index), or PSIFT_ERR_INVALID_ARGUMENT. */
+psift_status psift_catalog_find(const psift_catalog* cat, const char* id, uint32_t* index);
+/* upsert_entry (src/catalog.rs:324-342): host SoA features (count = features->count);
+ * the entry's codes are quantize_descriptor_u128 of its descriptors. */
+psift_status psift_catalog_upsert(psift_catalog* cat, const char* id, uint32_t width, uint32_t height,
+                                  const psift_features* features);
+/* remove (src/catalog.rs:345-353): swap_remove; removed = 0 when the id is absent. */
+psift_status psift_catalog_remove(psift_catalog* cat, const char* id, int32_t* removed);
+/* Entry i's features back to the host (out->capacity >= the entry's count) and,
+ * when codes is not NULL, its 2 x u64 codes. */
+psift_status psift_catalog_features(psift_catalog* cat, uint32_t i, psift_features* out, uint64_t* codes);
+/* load_binary (src/catalog.rs:447-540): the file's records go to device memory
+ * through pinned staging and are split into the feature arrays there; the u8
+ * descriptors are expanded by dequantize_descriptor_u8 and the stored codes are
+ * kept as they are.  save_binary (:401-445): written to "<name>.tmp.<pid>" in
+ * the same directory, then renamed over the target. */
+psift_status psift_catalog_load_binary(psift_ctx* ctx, const char* path, psift_catalog** out);
+psift_status psift_catalog_save_binary(psift_catalog* cat, const char* path);
+/* One ranked hit of search_features (src/catalog.rs:576-702).  tracking.match_count
+ * and tracking.inlier_ratio already hold the better of the two estimates, as in
+ * the reference. */
+typedef struct psift_catalog_hit {
+  uint32_t entry;         /* catalog index */
+  uint32_t coarse_votes;
+  psift_tracking_summary tracking;
+  float similarity[6];    /* a, b, tx, ty, scale, rotation_deg */
+  int32_t has_similarity;
+  float homography[9];
+  int32_t has_homography;
+} psift_catalog_hit;
+/* search_features: query features are host SoA (count = query->count).  At most
+ * top_k hits; *count receives their number (PSIFT_ERR_CAPACITY if > capacity). */
+psift_status psift_catalog_search(psift_catalog* cat, const psift_features* query, uint32_t top_k,
+                                  uint32_t shortlist_k, float ratio, float ransac_threshold,
+                                  psift_catalog_hit* hits, uint32_t capacity, uint32_t* count);
 
 /* Allocation-free variant of psift_detect_and_compute_batch_dev for one u8 image.
  * No counterpart in the reference: it exists for callers that cannot allocate

@@ -1,0 +1,883 @@
+// Device-resident FeatureCatalog: every entry's features, 128-bit codes and the
+// entry table in device memory; PSIFTCAT v1 load and save; search_features with
+// the shortlist verified as batched launches.
+//
+// Reference: FeatureCatalog (src/catalog.rs:182-702): upsert_entry (:324-342),
+// remove (:345-353), list_summaries (:355-366), atomic_write_bytes (:203-245),
+// save_binary (:401-445), load_binary (:447-540), search_features (:576-702);
+// CatalogEntry::new (:122-140) for the codes of an upserted entry.
+//
+// Layout in HBM: structure-of-arrays over all features of all entries in entry
+// order; entry e owns [offset_e, offset_e + count_e).  Descriptors are f32
+// (n x 128, row-major, 512 B rows), coordinates interleaved (x, y) as the
+// matcher reads them, codes 2 x u64 (word 0 = bits 0..63).  A replace or remove
+// rebuilds the arrays in the new entry order with device-to-device copies.
+//
+// A search: query upload + quantisation, coarse votes over the resident codes
+// (one launch), shortlist on the host (the reference's sort by votes, then id),
+// then Lowe matching of the query against every shortlisted entry (one batched
+// matcher call), similarity and homography RANSAC of every non-empty match list
+// (one CTA per list, one launch each), and the tracking statistics on the host.
+#include <algorithm>
+#include <cerrno>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include "psift_internal.cuh"
+
+namespace psift {
+cudaError_t launch_quantize(const float* desc, int n, uint64_t* codes, uint8_t* u8, cudaStream_t st);
+cudaError_t launch_dequantize(const uint8_t* q, int n, float* out, cudaStream_t st);
+cudaError_t launch_votes(const uint64_t* q, int nq, const uint64_t* cat, const long long* offsets, int n_entries,
+                         int mih, uint32_t* votes, cudaStream_t st);
+
+namespace {
+
+constexpr char kMagic[8] = {'P', 'S', 'I', 'F', 'T', 'C', 'A', 'T'};  // BINARY_CATALOG_MAGIC
+constexpr uint32_t kVersion = 1;                                        // BINARY_CATALOG_VERSION
+constexpr int kRecordBytes = 5 * 4 + 16 + 128;                          // x y scale response orientation, sig, q[128]
+constexpr uint64_t kMaxFeatures = 0x7FFFFFFFull;                        // int indexing of the kernels
+constexpr float kDefaultRansacThreshold = 3.0f;                         // DEFAULT_RANSAC_REPROJ_THRESHOLD
+
+// The six feature arrays of `cap` features.
+struct FeatureArrays {
+  uint64_t cap = 0;
+  float* desc = nullptr;
+  float2* xy = nullptr;
+  float* scale = nullptr;
+  float* resp = nullptr;
+  float* ori = nullptr;
+  uint64_t* codes = nullptr;
+};
+
+void free_arrays(FeatureArrays& a) {
+  cudaFree(a.desc);
+  cudaFree(a.xy);
+  cudaFree(a.scale);
+  cudaFree(a.resp);
+  cudaFree(a.ori);
+  cudaFree(a.codes);
+  a = FeatureArrays{};
+}
+
+cudaError_t alloc_arrays(FeatureArrays& a, uint64_t cap) {
+  a = FeatureArrays{};
+  a.cap = cap;
+  if (cap == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc(&a.desc, cap * 512);
+  if (e == cudaSuccess) e = cudaMalloc(&a.xy, cap * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&a.scale, cap * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&a.resp, cap * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&a.ori, cap * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&a.codes, cap * 16);
+  if (e != cudaSuccess) free_arrays(a);
+  return e;
+}
+
+// Copies features [src_off, src_off + n) of `s` to [dst_off, ...) of `d`.
+cudaError_t copy_range(FeatureArrays& d, uint64_t dst_off, const FeatureArrays& s, uint64_t src_off, uint64_t n,
+                       cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  cudaError_t e = cudaMemcpyAsync(d.desc + dst_off * 128, s.desc + src_off * 128, n * 512, k, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d.xy + dst_off, s.xy + src_off, n * 8, k, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d.scale + dst_off, s.scale + src_off, n * 4, k, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d.resp + dst_off, s.resp + src_off, n * 4, k, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d.ori + dst_off, s.ori + src_off, n * 4, k, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d.codes + dst_off * 2, s.codes + src_off * 2, n * 16, k, st);
+  return e;
+}
+
+// PSIFTCAT records -> feature arrays: one warp per record.  The records of
+// entry e start at byte file_off[e] of the uploaded file (any alignment) and
+// fill features [out_off[e], out_off[e + 1]).  Descriptor bytes go to q8 for
+// dequantize_descriptor_u8; the stored signature is kept as it is.
+constexpr int kSplitWarps = 8;
+__global__ void __launch_bounds__(kSplitWarps * 32)
+    psiftcat_split_kernel(const uint8_t* __restrict__ file, const long long* __restrict__ file_off,
+                          const long long* __restrict__ out_off, int n_entries, long long total, float2* xy,
+                          float* scale, float* resp, float* ori, uint64_t* codes, uint8_t* q8) {
+  __shared__ __align__(16) uint8_t rec[kSplitWarps][kRecordBytes + 12];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long i = (long long)blockIdx.x * kSplitWarps + warp;
+  if (i >= total) return;
+  int lo = 0, hi = n_entries - 1;  // last entry with out_off[e] <= i
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (out_off[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  const uint8_t* src = file + file_off[lo] + (i - out_off[lo]) * kRecordBytes;
+  uint8_t* r = rec[warp];
+  for (int b = lane; b < kRecordBytes; b += 32) r[b] = src[b];
+  __syncwarp();
+  auto u32_at = [&](int b) {
+    return (uint32_t)r[b] | ((uint32_t)r[b + 1] << 8) | ((uint32_t)r[b + 2] << 16) | ((uint32_t)r[b + 3] << 24);
+  };
+  if (lane == 0) xy[i] = make_float2(__uint_as_float(u32_at(0)), __uint_as_float(u32_at(4)));
+  if (lane == 1) scale[i] = __uint_as_float(u32_at(8));
+  if (lane == 2) resp[i] = __uint_as_float(u32_at(12));
+  if (lane == 3) ori[i] = __uint_as_float(u32_at(16));
+  if (lane == 4 || lane == 5) {
+    const int b = 20 + 8 * (lane - 4);
+    codes[2 * i + (lane - 4)] = (uint64_t)u32_at(b) | ((uint64_t)u32_at(b + 4) << 32);
+  }
+  reinterpret_cast<uint32_t*>(q8 + i * 128)[lane] = u32_at(36 + 4 * lane);
+}
+
+// Rust's str::from_utf8 acceptance rule (shortest forms, no surrogates, <= U+10FFFF).
+bool valid_utf8(const uint8_t* s, size_t n) {
+  size_t i = 0;
+  while (i < n) {
+    const uint8_t c = s[i];
+    if (c < 0x80) {
+      ++i;
+      continue;
+    }
+    int len;
+    uint32_t cp;
+    if ((c & 0xE0) == 0xC0) {
+      len = 2;
+      cp = c & 0x1F;
+    } else if ((c & 0xF0) == 0xE0) {
+      len = 3;
+      cp = c & 0x0F;
+    } else if ((c & 0xF8) == 0xF0) {
+      len = 4;
+      cp = c & 0x07;
+    } else {
+      return false;
+    }
+    if (i + len > n) return false;
+    for (int k = 1; k < len; ++k) {
+      if ((s[i + k] & 0xC0) != 0x80) return false;
+      cp = (cp << 6) | (s[i + k] & 0x3F);
+    }
+    if ((len == 2 && cp < 0x80) || (len == 3 && cp < 0x800) || (len == 4 && cp < 0x10000)) return false;
+    if (cp > 0x10FFFF || (cp >= 0xD800 && cp <= 0xDFFF)) return false;
+    i += len;
+  }
+  return true;
+}
+
+struct Reader {
+  const uint8_t* p;
+  size_t left;
+  bool take(void* dst, size_t n) {
+    if (left < n) return false;
+    std::memcpy(dst, p, n);
+    p += n;
+    left -= n;
+    return true;
+  }
+};
+
+template <typename T>
+void put(std::vector<uint8_t>& b, T v) {
+  const size_t o = b.size();
+  b.resize(o + sizeof(T));
+  std::memcpy(b.data() + o, &v, sizeof(T));  // little-endian host
+}
+
+// atomic_write_bytes (src/catalog.rs:203-245): parent directories, then
+// "<file name>.tmp.<pid>" beside the target, renamed over it.
+psift_status atomic_write(psift_ctx* ctx, const std::string& path, const std::vector<uint8_t>& bytes) {
+  const size_t slash = path.find_last_of('/');
+  const std::string dir = slash == std::string::npos ? std::string() : path.substr(0, slash);
+  std::string name = slash == std::string::npos ? path : path.substr(slash + 1);
+  if (name.empty() || name == "." || name == "..") name = "catalog";
+  if (!dir.empty()) {
+    for (size_t k = 1; k <= dir.size(); ++k) {
+      if (k == dir.size() || dir[k] == '/') {
+        const std::string part = dir.substr(0, k);
+        if (mkdir(part.c_str(), 0777) != 0 && errno != EEXIST)
+          return set_error(ctx, PSIFT_ERR_IO, "Failed to create catalog directory `" + dir + "`: " + strerror(errno));
+      }
+    }
+  }
+  const std::string tmp = (dir.empty() ? std::string() : dir + "/") + name + ".tmp." + std::to_string(getpid());
+  FILE* f = std::fopen(tmp.c_str(), "wb");
+  if (!f) return set_error(ctx, PSIFT_ERR_IO, "Failed to create temporary catalog `" + tmp + "`: " + strerror(errno));
+  const bool ok = (bytes.empty() || std::fwrite(bytes.data(), 1, bytes.size(), f) == bytes.size()) &&
+                  std::fflush(f) == 0;
+  const bool closed = std::fclose(f) == 0;
+  if (!ok || !closed) {
+    std::remove(tmp.c_str());
+    return set_error(ctx, PSIFT_ERR_IO, "Failed to write catalog `" + tmp + "`");
+  }
+  if (std::rename(tmp.c_str(), path.c_str()) != 0) {
+    const std::string why = strerror(errno);
+    std::remove(tmp.c_str());
+    return set_error(ctx, PSIFT_ERR_IO, "Failed to atomically replace catalog `" + path + "`: " + why);
+  }
+  return PSIFT_OK;
+}
+
+}  // namespace
+}  // namespace psift
+
+using namespace psift;
+
+struct psift_catalog {
+  psift_ctx* ctx = nullptr;
+  psift_catalog_params params{};
+  struct Entry {
+    std::string id;
+    uint32_t width = 0, height = 0;
+    uint64_t count = 0, offset = 0;
+  };
+  std::vector<Entry> entries;
+  std::unordered_map<std::string, uint32_t> index;  // id_index (last duplicate wins, as rebuild_indices)
+  FeatureArrays a;
+  uint64_t total = 0;
+  char* scratch = nullptr;  // grow-only search / load workspace
+  size_t scratch_cap = 0;
+
+  psift_status reserve_scratch(size_t bytes) {
+    if (bytes <= scratch_cap) return PSIFT_OK;
+    bytes = align_up(bytes, 1 << 20);
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(scratch);
+    scratch = nullptr;
+    scratch_cap = 0;
+    cudaError_t e = cudaMalloc(&scratch, bytes);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaMalloc(catalog scratch)");
+    scratch_cap = bytes;
+    return PSIFT_OK;
+  }
+
+  void reindex() {
+    index.clear();
+    uint64_t off = 0;
+    for (uint32_t i = 0; i < entries.size(); ++i) {
+      entries[i].offset = off;
+      off += entries[i].count;
+      index[entries[i].id] = i;
+    }
+    total = off;
+  }
+
+  // New arrays holding, in order, the old entries `order` (index into the old
+  // `entries`, or -1 for `fresh_count` features uploaded afterwards by the caller).
+  psift_status rebuild(const std::vector<long long>& order, uint64_t fresh_count, std::vector<Entry> next,
+                       uint64_t* fresh_offset) {
+    uint64_t need = 0;
+    for (long long o : order) need += o < 0 ? fresh_count : entries[(size_t)o].count;
+    if (need > kMaxFeatures) return set_error(ctx, PSIFT_ERR_CAPACITY, "catalog larger than 2^31-1 features");
+    FeatureArrays n;
+    cudaError_t e = alloc_arrays(n, std::max<uint64_t>(std::max(need, a.cap), 1024));
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaMalloc(catalog)");
+    uint64_t off = 0;
+    for (long long o : order) {
+      if (o < 0) {
+        *fresh_offset = off;
+        off += fresh_count;
+        continue;
+      }
+      const Entry& E = entries[(size_t)o];
+      e = copy_range(n, off, a, E.offset, E.count, ctx->stream);
+      if (e != cudaSuccess) {
+        free_arrays(n);
+        return cuda_error(ctx, e, "catalog reorder copy");
+      }
+      off += E.count;
+    }
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    free_arrays(a);
+    a = n;
+    entries = std::move(next);
+    reindex();
+    return PSIFT_OK;
+  }
+
+  psift_status grow(uint64_t need) {
+    if (need <= a.cap) return PSIFT_OK;
+    if (need > kMaxFeatures) return set_error(ctx, PSIFT_ERR_CAPACITY, "catalog larger than 2^31-1 features");
+    FeatureArrays n;
+    cudaError_t e = alloc_arrays(n, std::max<uint64_t>(std::max(need, 2 * a.cap), 1024));
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaMalloc(catalog)");
+    e = copy_range(n, 0, a, 0, total, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      free_arrays(n);
+      return cuda_error(ctx, e, "catalog grow copy");
+    }
+    free_arrays(a);
+    a = n;
+    return PSIFT_OK;
+  }
+
+  // Host SoA features -> [off, off + n); codes from the descriptors.
+  psift_status upload(uint64_t off, const psift_features* f) {
+    const uint64_t n = f->count;
+    if (n == 0) return PSIFT_OK;
+    std::vector<float2> xy(n);
+    for (uint64_t i = 0; i < n; ++i) xy[i] = make_float2(f->x[i], f->y[i]);
+    cudaStream_t st = ctx->stream;
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(a.desc + off * 128, f->descriptors, n * 512, cudaMemcpyHostToDevice, st));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(a.xy + off, xy.data(), n * 8, cudaMemcpyHostToDevice, st));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(a.scale + off, f->scale, n * 4, cudaMemcpyHostToDevice, st));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(a.resp + off, f->response, n * 4, cudaMemcpyHostToDevice, st));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(a.ori + off, f->orientation, n * 4, cudaMemcpyHostToDevice, st));
+    cudaError_t e = launch_quantize(a.desc + off * 128, (int)n, a.codes + off * 2, nullptr, st);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "quantize_u128");
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // xy lives on the host stack
+    return PSIFT_OK;
+  }
+};
+
+namespace {
+
+psift_status cat_begin(const psift_catalog* cat) {
+  if (!cat || !cat->ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaSetDevice(cat->ctx->device);
+  if (e != cudaSuccess) return cuda_error(cat->ctx, e, "cudaSetDevice");
+  return PSIFT_OK;
+}
+
+bool features_ok(const psift_features* f) {
+  return f && (f->count == 0 ||
+               (f->x && f->y && f->scale && f->response && f->orientation && f->descriptors));
+}
+
+}  // namespace
+
+extern "C" {
+
+psift_status psift_catalog_create(psift_ctx* ctx, const psift_catalog_params* params, psift_catalog** out) {
+  if (!ctx || !params || !out) return PSIFT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (params->descriptor_kind != 0 && params->descriptor_kind != 1)
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "descriptor_kind must be 0 (Sift) or 1 (RootSift)");
+  psift_catalog* c = new psift_catalog;
+  c->ctx = ctx;
+  c->params = *params;
+  *out = c;
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_destroy(psift_catalog* cat) {
+  if (!cat) return PSIFT_OK;
+  if (cat_begin(cat) == PSIFT_OK) cudaStreamSynchronize(cat->ctx->stream);
+  free_arrays(cat->a);
+  cudaFree(cat->scratch);
+  delete cat;
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_params_get(const psift_catalog* cat, psift_catalog_params* out) {
+  if (!cat || !out) return PSIFT_ERR_INVALID_ARGUMENT;
+  *out = cat->params;
+  return PSIFT_OK;
+}
+
+uint32_t psift_catalog_size(const psift_catalog* cat) { return cat ? (uint32_t)cat->entries.size() : 0u; }
+
+psift_status psift_catalog_entry(const psift_catalog* cat, uint32_t i, char* id, size_t id_capacity,
+                                 uint32_t* id_len, uint32_t* width, uint32_t* height, uint64_t* feature_count) {
+  if (!cat) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (i >= cat->entries.size()) return set_error(cat->ctx, PSIFT_ERR_INVALID_ARGUMENT, "entry index out of range");
+  const psift_catalog::Entry& E = cat->entries[i];
+  if (id && id_capacity) {
+    const size_t n = std::min(E.id.size(), id_capacity - 1);
+    std::memcpy(id, E.id.data(), n);
+    id[n] = 0;
+  }
+  if (id_len) *id_len = (uint32_t)E.id.size();
+  if (width) *width = E.width;
+  if (height) *height = E.height;
+  if (feature_count) *feature_count = E.count;
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_find(const psift_catalog* cat, const char* id, uint32_t* index) {
+  if (!cat || !id || !index) return PSIFT_ERR_INVALID_ARGUMENT;
+  auto it = cat->index.find(id);
+  if (it == cat->index.end()) return set_error(cat->ctx, PSIFT_ERR_INVALID_ARGUMENT, std::string("no entry `") + id + "`");
+  *index = it->second;
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_upsert(psift_catalog* cat, const char* id, uint32_t width, uint32_t height,
+                                  const psift_features* f) {
+  psift_status st = cat_begin(cat);
+  if (st != PSIFT_OK) return st;
+  if (!id || !features_ok(f)) return set_error(cat->ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  psift_catalog::Entry E;
+  E.id = id;
+  E.width = width;
+  E.height = height;
+  E.count = f->count;
+  auto it = cat->index.find(E.id);
+  if (it != cat->index.end()) {
+    // entries[existing] = entry; rebuild_indices(): same position, new features
+    const uint32_t at = it->second;
+    std::vector<long long> order;
+    std::vector<psift_catalog::Entry> next = cat->entries;
+    next[at] = E;
+    for (uint32_t k = 0; k < cat->entries.size(); ++k) order.push_back(k == at ? -1 : (long long)k);
+    uint64_t off = 0;
+    if ((st = cat->rebuild(order, E.count, std::move(next), &off)) != PSIFT_OK) return st;
+    return cat->upload(off, f);
+  }
+  if ((st = cat->grow(cat->total + E.count)) != PSIFT_OK) return st;
+  const uint64_t off = cat->total;
+  if ((st = cat->upload(off, f)) != PSIFT_OK) return st;
+  E.offset = off;
+  cat->index[E.id] = (uint32_t)cat->entries.size();
+  cat->entries.push_back(E);
+  cat->total += E.count;
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_remove(psift_catalog* cat, const char* id, int32_t* removed) {
+  psift_status st = cat_begin(cat);
+  if (st != PSIFT_OK) return st;
+  if (!id || !removed) return set_error(cat->ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  *removed = 0;
+  auto it = cat->index.find(id);
+  if (it == cat->index.end()) return PSIFT_OK;
+  // entries.swap_remove(idx): the last entry takes the removed one's place
+  const uint32_t at = it->second, last = (uint32_t)cat->entries.size() - 1;
+  std::vector<long long> order;
+  std::vector<psift_catalog::Entry> next;
+  for (uint32_t k = 0; k < last; ++k) {
+    const uint32_t src = k == at ? last : k;
+    order.push_back(src);
+    next.push_back(cat->entries[src]);
+  }
+  uint64_t unused = 0;
+  if ((st = cat->rebuild(order, 0, std::move(next), &unused)) != PSIFT_OK) return st;
+  *removed = 1;
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_features(psift_catalog* cat, uint32_t i, psift_features* out, uint64_t* codes) {
+  psift_status st = cat_begin(cat);
+  if (st != PSIFT_OK) return st;
+  psift_ctx* ctx = cat->ctx;
+  if (!out) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null output");
+  if (i >= cat->entries.size()) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "entry index out of range");
+  const psift_catalog::Entry& E = cat->entries[i];
+  out->count = (uint32_t)E.count;
+  if (E.count > out->capacity) return set_error(ctx, PSIFT_ERR_CAPACITY, "feature output capacity too small");
+  if (E.count == 0) return PSIFT_OK;
+  psift_features probe = *out;
+  probe.count = 1;
+  if (!features_ok(&probe)) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null feature array");
+  const uint64_t n = E.count, o = E.offset;
+  std::vector<float2> xy(n);
+  cudaStream_t s = ctx->stream;
+  const cudaMemcpyKind k = cudaMemcpyDeviceToHost;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(out->descriptors, cat->a.desc + o * 128, n * 512, k, s));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(xy.data(), cat->a.xy + o, n * 8, k, s));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(out->scale, cat->a.scale + o, n * 4, k, s));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(out->response, cat->a.resp + o, n * 4, k, s));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(out->orientation, cat->a.ori + o, n * 4, k, s));
+  if (codes) PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(codes, cat->a.codes + o * 2, n * 16, k, s));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  for (uint64_t j = 0; j < n; ++j) {
+    out->x[j] = xy[j].x;
+    out->y[j] = xy[j].y;
+  }
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_load_binary(psift_ctx* ctx, const char* path, psift_catalog** out) {
+  if (!ctx || !path || !out) return PSIFT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaSetDevice");
+  const std::string p = path;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`: " + strerror(errno));
+  std::vector<uint8_t> raw;
+  {
+    uint8_t buf[1 << 16];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) raw.insert(raw.end(), buf, buf + got);
+    const bool err = std::ferror(f) != 0;
+    std::fclose(f);
+    if (err) return set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`");
+  }
+  // Header and entry table on the host (the reference's read order and messages).
+  Reader r{raw.data(), raw.size()};
+  const std::string eof = "Unexpected EOF while reading binary catalog";
+  char magic[8];
+  if (!r.take(magic, 8)) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
+  if (std::memcmp(magic, kMagic, 8) != 0)
+    return set_error(ctx, PSIFT_ERR_FORMAT, "Invalid binary catalog magic header in `" + p + "`");
+  uint32_t version = 0, octaves = 0, scales = 0;
+  float threshold = 0.0f;
+  uint8_t kind = 0;
+  uint64_t n_entries = 0;
+  if (!r.take(&version, 4)) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
+  if (version != kVersion)
+    return set_error(ctx, PSIFT_ERR_FORMAT, "Unsupported binary catalog version " + std::to_string(version) + " in `" +
+                                                p + "` (expected 1)");
+  if (!r.take(&octaves, 4) || !r.take(&scales, 4) || !r.take(&threshold, 4) || !r.take(&kind, 1))
+    return set_error(ctx, PSIFT_ERR_FORMAT, eof);
+  if (kind > 1)
+    return set_error(ctx, PSIFT_ERR_FORMAT,
+                     "Unknown descriptor kind " + std::to_string(kind) + " in binary catalog `" + p + "`");
+  if (!r.take(&n_entries, 8)) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
+  std::vector<psift_catalog::Entry> entries;
+  std::vector<long long> file_off, out_off;
+  uint64_t total = 0;
+  for (uint64_t e = 0; e < n_entries; ++e) {
+    uint32_t id_len = 0, w = 0, h = 0;
+    uint64_t cnt = 0;
+    if (!r.take(&id_len, 4)) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
+    if (r.left < id_len) return set_error(ctx, PSIFT_ERR_FORMAT, "Truncated entry id in binary catalog");
+    if (!valid_utf8(r.p, id_len)) return set_error(ctx, PSIFT_ERR_FORMAT, "Invalid UTF-8 entry id in binary catalog");
+    psift_catalog::Entry E;
+    E.id.assign(reinterpret_cast<const char*>(r.p), id_len);
+    r.p += id_len;
+    r.left -= id_len;
+    if (!r.take(&w, 4) || !r.take(&h, 4) || !r.take(&cnt, 8)) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
+    // every record must be present before the next header (the reference's reads)
+    if (cnt > r.left / kRecordBytes) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
+    E.width = w;
+    E.height = h;
+    E.count = cnt;
+    E.offset = total;
+    file_off.push_back((long long)(r.p - raw.data()));
+    out_off.push_back((long long)total);
+    r.p += cnt * kRecordBytes;
+    r.left -= cnt * kRecordBytes;
+    total += cnt;
+    if (total > kMaxFeatures) return set_error(ctx, PSIFT_ERR_CAPACITY, "catalog larger than 2^31-1 features");
+    entries.push_back(std::move(E));
+  }
+  out_off.push_back((long long)total);
+
+  psift_catalog_params prm{octaves, scales, threshold, (int32_t)kind};
+  psift_catalog* cat = nullptr;
+  psift_status st = psift_catalog_create(ctx, &prm, &cat);
+  if (st != PSIFT_OK) return st;
+  auto fail = [&](psift_status s) {
+    psift_catalog_destroy(cat);
+    return s;
+  };
+  cat->entries = std::move(entries);
+  cat->reindex();
+  if (total > 0) {
+    ce = alloc_arrays(cat->a, std::max<uint64_t>(total, 1024));
+    if (ce != cudaSuccess) return fail(cuda_error(ctx, ce, "cudaMalloc(catalog)"));
+    // Device workspace: the file, the two offset tables and the u8 descriptors.
+    const size_t fb = align_up(raw.size(), 256), tb = align_up(8 * out_off.size(), 256);
+    if ((st = cat->reserve_scratch(fb + 2 * tb + total * 128)) != PSIFT_OK) return fail(st);
+    uint8_t* d_file = (uint8_t*)cat->scratch;
+    long long* d_foff = (long long*)(cat->scratch + fb);
+    long long* d_ooff = (long long*)(cat->scratch + fb + tb);
+    uint8_t* d_q8 = (uint8_t*)(cat->scratch + fb + 2 * tb);
+    // Upload through two pinned staging halves, the copy of one overlapping the
+    // host memcpy into the other.
+    constexpr size_t kChunk = 16u << 20;
+    if ((st = pinned_reserve(ctx, 2 * kChunk)) != PSIFT_OK) return fail(st);
+    cudaEvent_t ev[2];
+    for (auto& x : ev)
+      if ((ce = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess)
+        return fail(cuda_error(ctx, ce, "cudaEventCreate"));
+    bool used[2] = {false, false};
+    for (size_t off = 0, k = 0; off < raw.size(); off += kChunk, k ^= 1) {
+      const size_t n = std::min(kChunk, raw.size() - off);
+      if (used[k]) cudaEventSynchronize(ev[k]);
+      std::memcpy(ctx->pinned.base + k * kChunk, raw.data() + off, n);
+      ce = cudaMemcpyAsync(d_file + off, ctx->pinned.base + k * kChunk, n, cudaMemcpyHostToDevice, ctx->stream);
+      if (ce == cudaSuccess) ce = cudaEventRecord(ev[k], ctx->stream);
+      if (ce != cudaSuccess) break;
+      used[k] = true;
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_foff, file_off.data(), 8 * file_off.size(), cudaMemcpyHostToDevice, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_ooff, out_off.data(), 8 * out_off.size(), cudaMemcpyHostToDevice, ctx->stream);
+    if (ce == cudaSuccess) {
+      const long long blocks = ((long long)total + kSplitWarps - 1) / kSplitWarps;
+      psiftcat_split_kernel<<<(unsigned)blocks, kSplitWarps * 32, 0, ctx->stream>>>(
+          d_file, d_foff, d_ooff, (int)file_off.size(), (long long)total, cat->a.xy, cat->a.scale, cat->a.resp,
+          cat->a.ori, cat->a.codes, d_q8);
+      ctx->launches++;
+      ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) {
+      ce = launch_dequantize(d_q8, (int)total, cat->a.desc, ctx->stream);
+      ctx->launches++;
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (ce != cudaSuccess) return fail(cuda_error(ctx, ce, "PSIFTCAT upload"));
+  }
+  *out = cat;
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_save_binary(psift_catalog* cat, const char* path) {
+  psift_status st = cat_begin(cat);
+  if (st != PSIFT_OK) return st;
+  psift_ctx* ctx = cat->ctx;
+  if (!path) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null path");
+  const uint64_t n = cat->total;
+  std::vector<float2> xy(n);
+  std::vector<float> sc(n), rs(n), orr(n);
+  std::vector<uint64_t> codes(2 * n);
+  std::vector<uint8_t> q(128 * n);
+  if (n) {
+    // quantize_descriptor_u8 of the resident f32 descriptors, as the reference's save does
+    if ((st = cat->reserve_scratch(n * 128)) != PSIFT_OK) return st;
+    cudaError_t e = launch_quantize(cat->a.desc, (int)n, nullptr, (uint8_t*)cat->scratch, ctx->stream);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_error(ctx, e, "quantize_u8");
+    cudaStream_t s = ctx->stream;
+    const cudaMemcpyKind k = cudaMemcpyDeviceToHost;
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(q.data(), cat->scratch, n * 128, k, s));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(xy.data(), cat->a.xy, n * 8, k, s));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(sc.data(), cat->a.scale, n * 4, k, s));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(rs.data(), cat->a.resp, n * 4, k, s));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(orr.data(), cat->a.ori, n * 4, k, s));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(codes.data(), cat->a.codes, n * 16, k, s));
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  }
+  std::vector<uint8_t> b;
+  b.reserve(64 + cat->entries.size() * 64 + n * kRecordBytes);
+  b.insert(b.end(), kMagic, kMagic + 8);
+  put<uint32_t>(b, kVersion);
+  put<uint32_t>(b, cat->params.octaves);
+  put<uint32_t>(b, cat->params.scales);
+  put<float>(b, cat->params.threshold);
+  put<uint8_t>(b, (uint8_t)cat->params.descriptor_kind);
+  put<uint64_t>(b, (uint64_t)cat->entries.size());
+  for (const psift_catalog::Entry& E : cat->entries) {
+    put<uint32_t>(b, (uint32_t)E.id.size());
+    b.insert(b.end(), E.id.begin(), E.id.end());
+    put<uint32_t>(b, E.width);
+    put<uint32_t>(b, E.height);
+    put<uint64_t>(b, E.count);
+    for (uint64_t j = E.offset; j < E.offset + E.count; ++j) {
+      put<float>(b, xy[j].x);
+      put<float>(b, xy[j].y);
+      put<float>(b, sc[j]);
+      put<float>(b, rs[j]);
+      put<float>(b, orr[j]);
+      put<uint64_t>(b, codes[2 * j]);
+      put<uint64_t>(b, codes[2 * j + 1]);
+      b.insert(b.end(), q.begin() + 128 * j, q.begin() + 128 * (j + 1));
+    }
+  }
+  return atomic_write(ctx, path, b);
+}
+
+psift_status psift_catalog_search(psift_catalog* cat, const psift_features* query, uint32_t top_k,
+                                  uint32_t shortlist_k, float ratio, float ransac_threshold,
+                                  psift_catalog_hit* hits, uint32_t capacity, uint32_t* count) {
+  psift_status st = cat_begin(cat);
+  if (st != PSIFT_OK) return st;
+  psift_ctx* ctx = cat->ctx;
+  if (!count || !features_ok(query)) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  *count = 0;
+  const uint32_t nq = query->count;
+  const uint32_t n_entries = (uint32_t)cat->entries.size();
+  if (n_entries == 0 || nq == 0 || top_k == 0) return PSIFT_OK;
+  psift_match_options mopt{ratio, 0, PSIFT_PRECISION_BF16_RERANK};
+  char msg[160];
+  if ((st = psift_match_options_validate(&mopt, msg, sizeof msg)) != PSIFT_OK) return set_error(ctx, st, msg);
+  psift_ransac_options ropt;
+  psift_ransac_options_default(&ropt);
+  ropt.reproj_threshold = ransac_threshold;
+  if ((st = psift_ransac_options_validate(&ropt, msg, sizeof msg)) != PSIFT_OK) return set_error(ctx, st, msg);
+  const bool own_tracking = ransac_threshold != kDefaultRansacThreshold;
+  const uint32_t max_cands = std::min<uint32_t>(n_entries, std::max<uint32_t>(shortlist_k, 1));
+
+  // Workspace (device): query, codes, offsets, votes, then per candidate the
+  // match list, three masks and the model / flag / count words.
+  const size_t q_bytes = align_up((size_t)nq * 512, 256), xy_bytes = align_up((size_t)nq * 8, 256);
+  const size_t code_bytes = align_up((size_t)nq * 16, 256), off_bytes = align_up(8 * (size_t)(n_entries + 1), 256);
+  const size_t vote_bytes = align_up(4 * (size_t)n_entries, 256);
+  const size_t m_bytes = align_up(sizeof(psift_match) * nq, 256), mask_bytes = align_up(nq, 256);
+  constexpr size_t kWords = 64;  // [0] match count, [4..12) sim, [16..32) hom, [40..48) tracking sim
+  const size_t per_cand = m_bytes + 3 * mask_bytes + kWords * 4;
+  if ((st = cat->reserve_scratch(q_bytes + xy_bytes + code_bytes + off_bytes + vote_bytes +
+                                 per_cand * max_cands)) != PSIFT_OK)
+    return st;
+  char* w = cat->scratch;
+  float* d_q = (float*)w;
+  float2* d_qxy = (float2*)(w + q_bytes);
+  uint64_t* d_codes = (uint64_t*)(w + q_bytes + xy_bytes);
+  long long* d_off = (long long*)(w + q_bytes + xy_bytes + code_bytes);
+  uint32_t* d_votes = (uint32_t*)(w + q_bytes + xy_bytes + code_bytes + off_bytes);
+  char* cand_base = w + q_bytes + xy_bytes + code_bytes + off_bytes + vote_bytes;
+  cudaStream_t s = ctx->stream;
+
+  // Step 1: coarse votes (src/catalog.rs:588-633).
+  std::vector<float2> qxy(nq);
+  for (uint32_t i = 0; i < nq; ++i) qxy[i] = make_float2(query->x[i], query->y[i]);
+  std::vector<long long> off(n_entries + 1);
+  for (uint32_t e = 0; e < n_entries; ++e) off[e] = (long long)cat->entries[e].offset;
+  off[n_entries] = (long long)cat->total;
+  const int mih = n_entries > 32 ? 1 : 0;
+  std::vector<uint32_t> votes(n_entries);
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_q, query->descriptors, (size_t)nq * 512, cudaMemcpyHostToDevice, s));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_qxy, qxy.data(), (size_t)nq * 8, cudaMemcpyHostToDevice, s));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_off, off.data(), 8 * off.size(), cudaMemcpyHostToDevice, s));
+  {
+    StageScope sc(ctx, STAGE_HAMMING);
+    cudaError_t e = launch_quantize(d_q, (int)nq, d_codes, nullptr, s);
+    ctx->launches++;
+    if (e == cudaSuccess) {
+      e = launch_votes(d_codes, (int)nq, cat->a.codes, d_off, (int)n_entries, mih, d_votes, s);
+      ctx->launches++;
+    }
+    if (e != cudaSuccess) return cuda_error(ctx, e, "catalog votes");
+  }
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(votes.data(), d_votes, 4 * (size_t)n_entries, cudaMemcpyDeviceToHost, s));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+
+  // Shortlist: MIH keeps entries with votes > 0; sort (votes desc, id asc) when too many.
+  std::vector<std::pair<uint32_t, uint32_t>> cands;  // (entry, votes)
+  for (uint32_t e = 0; e < n_entries; ++e)
+    if (!mih || votes[e] > 0) cands.emplace_back(e, votes[e]);
+  if (cands.size() > max_cands) {
+    std::stable_sort(cands.begin(), cands.end(), [&](const auto& a, const auto& b) {
+      if (a.second != b.second) return a.second > b.second;
+      return cat->entries[a.first].id < cat->entries[b.first].id;
+    });
+    cands.resize(max_cands);
+  }
+
+  // Step 2: Lowe matching against every candidate with >= 2 features (one batched call).
+  std::vector<uint32_t> live;  // positions into cands
+  for (uint32_t c = 0; c < cands.size(); ++c)
+    if (cat->entries[cands[c].first].count >= 2) live.push_back(c);
+  struct Slot {
+    psift_match* m;
+    uint8_t* mask_sim;
+    uint8_t* mask_hom;
+    uint8_t* mask_trk;
+    uint32_t* words;
+  };
+  std::vector<Slot> slot(live.size());
+  std::vector<psift_match_job> mjobs;
+  for (size_t k = 0; k < live.size(); ++k) {
+    char* b = cand_base + per_cand * k;
+    slot[k] = Slot{(psift_match*)b, (uint8_t*)(b + m_bytes), (uint8_t*)(b + m_bytes + mask_bytes),
+                   (uint8_t*)(b + m_bytes + 2 * mask_bytes), (uint32_t*)(b + m_bytes + 3 * mask_bytes)};
+    const psift_catalog::Entry& E = cat->entries[cands[live[k]].first];
+    mjobs.push_back(psift_match_job{d_q, cat->a.desc + E.offset * 128, (const float*)d_qxy,
+                                    (const float*)(cat->a.xy + E.offset), nq, (uint32_t)E.count, slot[k].m, nq,
+                                    slot[k].words});
+  }
+  std::vector<uint32_t> n_raw(live.size(), 0);
+  if (!live.empty()) {
+    PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(cand_base, 0, per_cand * live.size(), s));
+    PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, sizeof(uint32_t), s));
+    if ((st = psift_match_batch_dev(ctx, mjobs.data(), (uint32_t)mjobs.size(), &mopt)) != PSIFT_OK) return st;
+    uint32_t err = 0;
+    for (size_t k = 0; k < live.size(); ++k)
+      PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(&n_raw[k], slot[k].words, 4, cudaMemcpyDeviceToHost, s));
+    PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(&err, ctx->d_error, 4, cudaMemcpyDeviceToHost, s));
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    if (err & kErrTimeout) return set_error(ctx, PSIFT_ERR_TIMEOUT, "tensor-core matcher wait timed out");
+  }
+
+  // Step 3: similarity + homography RANSAC of every non-empty list (and the
+  // tracking summary's own similarity RANSAC when the threshold differs from
+  // the default it uses).
+  std::vector<size_t> verified;  // indices into live with raw matches
+  std::vector<psift_ransac_job> sim, hom, trk;
+  for (size_t k = 0; k < live.size(); ++k) {
+    if (n_raw[k] == 0) continue;
+    verified.push_back(k);
+    uint32_t* W = slot[k].words;
+    sim.push_back(psift_ransac_job{slot[k].m, n_raw[k], slot[k].mask_sim, (float*)(W + 4), (int32_t*)(W + 1),
+                                   W + 2, nullptr, nullptr});
+    hom.push_back(psift_ransac_job{slot[k].m, n_raw[k], slot[k].mask_hom, (float*)(W + 16), (int32_t*)(W + 12),
+                                   W + 13, nullptr, nullptr});
+    if (own_tracking)
+      trk.push_back(psift_ransac_job{slot[k].m, n_raw[k], slot[k].mask_trk, (float*)(W + 40), (int32_t*)(W + 36),
+                                     W + 37, nullptr, nullptr});
+  }
+  if (!verified.empty()) {
+    if ((st = psift_ransac_batch_dev(ctx, sim.data(), (uint32_t)sim.size(), &ropt, 0)) != PSIFT_OK) return st;
+    if ((st = psift_ransac_batch_dev(ctx, hom.data(), (uint32_t)hom.size(), &ropt, 1)) != PSIFT_OK) return st;
+    if (own_tracking) {
+      psift_ransac_options dopt;
+      psift_ransac_options_default(&dopt);
+      if ((st = psift_ransac_batch_dev(ctx, trk.data(), (uint32_t)trk.size(), &dopt, 0)) != PSIFT_OK) return st;
+    }
+  }
+
+  // Step 4: results to the host; tracking statistics and the hit list.
+  std::vector<psift_catalog_hit> out;
+  std::vector<const psift_catalog::Entry*> out_entry;
+  if (!verified.empty()) {
+    const size_t nv = verified.size();
+    std::vector<std::vector<psift_match>> hm(nv);
+    std::vector<std::vector<uint8_t>> hmask(nv);
+    std::vector<std::vector<float>> tsc(nv), tor(nv);
+    std::vector<uint32_t> words(nv * kWords);
+    for (size_t v = 0; v < nv; ++v) {
+      const size_t k = verified[v];
+      const psift_catalog::Entry& E = cat->entries[cands[live[k]].first];
+      hm[v].resize(n_raw[k]);
+      hmask[v].resize(n_raw[k]);
+      tsc[v].resize(E.count);
+      tor[v].resize(E.count);
+      PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hm[v].data(), slot[k].m, sizeof(psift_match) * n_raw[k],
+                                          cudaMemcpyDeviceToHost, s));
+      PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hmask[v].data(), own_tracking ? slot[k].mask_trk : slot[k].mask_sim,
+                                          n_raw[k], cudaMemcpyDeviceToHost, s));
+      PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(words.data() + v * kWords, slot[k].words, kWords * 4,
+                                          cudaMemcpyDeviceToHost, s));
+      PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(tsc[v].data(), cat->a.scale + E.offset, 4 * E.count,
+                                          cudaMemcpyDeviceToHost, s));
+      PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(tor[v].data(), cat->a.ori + E.offset, 4 * E.count,
+                                          cudaMemcpyDeviceToHost, s));
+    }
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    for (size_t v = 0; v < nv; ++v) {
+      const size_t k = verified[v];
+      const uint32_t* W = words.data() + v * kWords;
+      psift_catalog_hit H;
+      std::memset(&H, 0, sizeof H);
+      H.entry = cands[live[k]].first;
+      H.coarse_votes = cands[live[k]].second;
+      tracking_stats(hm[v].data(), n_raw[k], hmask[v].data(), query->scale, query->orientation, tsc[v].data(),
+                     tor[v].data(), &H.tracking);
+      const uint32_t sim_in = W[2], hom_in = W[13];
+      const uint32_t best = std::max(hom_in, sim_in);
+      H.tracking.match_count = best;
+      H.tracking.inlier_ratio = (float)best / (float)H.tracking.raw_match_count;
+      H.has_similarity = (int32_t)W[1];
+      std::memcpy(H.similarity, W + 4, sizeof H.similarity);
+      H.has_homography = (int32_t)W[12];
+      std::memcpy(H.homography, W + 16, sizeof H.homography);
+      out.push_back(H);
+    }
+  }
+  // match_count desc, inlier_ratio desc (NaN compares equal), votes desc, id asc
+  std::vector<size_t> order(out.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t i, size_t j) {
+    const psift_catalog_hit &a = out[i], &b = out[j];
+    if (a.tracking.match_count != b.tracking.match_count) return a.tracking.match_count > b.tracking.match_count;
+    const float ra = a.tracking.inlier_ratio, rb = b.tracking.inlier_ratio;
+    if (ra > rb) return true;
+    if (ra < rb) return false;
+    if (a.coarse_votes != b.coarse_votes) return a.coarse_votes > b.coarse_votes;
+    return cat->entries[a.entry].id < cat->entries[b.entry].id;
+  });
+  const uint32_t n_out = (uint32_t)std::min<size_t>(order.size(), top_k);
+  *count = n_out;
+  if (n_out > capacity) return set_error(ctx, PSIFT_ERR_CAPACITY, "hit output capacity too small");
+  if (n_out && !hits) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null hit output");
+  for (uint32_t i = 0; i < n_out; ++i) hits[i] = out[order[i]];
+  return PSIFT_OK;
+}
+
+}  // extern "C"

@@ -106,6 +106,9 @@ psift_status io_reserve(psift_ctx* ctx, size_t bytes);
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Raise a kernel's dynamic shared-memory limit once per (kernel, device).
 cudaError_t ensure_smem_attr(const void* func, size_t bytes);
+// Statistics of summarize_tracking over the masked matches (ransac_api.cu).
+void tracking_stats(const psift_match* m, uint32_t n, const uint8_t* mask, const float* q_scale,
+                    const float* q_ori, const float* t_scale, const float* t_ori, psift_tracking_summary* out);
 // CTAs of `func` resident on the whole device at once (occupancy x SMs), cached.
 cudaError_t resident_ctas(const void* func, int threads, size_t smem, int* out);
 

@@ -197,31 +197,12 @@ float median_f32(std::vector<float> v) {
   return v.size() % 2 == 1 ? v[mid] : 0.5f * (v[mid - 1] + v[mid]);
 }
 }  // namespace
-}  // namespace psift
 
-extern "C" psift_status psift_summarize_tracking(psift_ctx* ctx, const psift_match* m, uint32_t n,
-                                                 const float* q_scale, const float* q_ori, uint32_t nq,
-                                                 const float* t_scale, const float* t_ori, uint32_t nt,
-                                                 psift_tracking_summary* out) {
-  // summarize_tracking (src/pipeline.rs:2210-2272): the similarity RANSAC runs on the
-  // device; the O(n) summary below repeats the reference's f32 sums on the host.
-  if (!ctx || !out) return PSIFT_ERR_INVALID_ARGUMENT;
-  if (n == 0) {
-    *out = psift_tracking_summary{0, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f};
-    return PSIFT_OK;
-  }
-  if (!m || !q_scale || !q_ori || !t_scale || !t_ori) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
-  for (uint32_t i = 0; i < n; ++i)
-    if (m[i].query_index >= nq || m[i].target_index >= nt)
-      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "match index outside the feature arrays");
-  std::vector<uint8_t> mask(n);
-  float model[9];
-  int32_t has = 0;
-  uint32_t cnt = 0;
-  psift_ransac_options opt;
-  psift_ransac_options_default(&opt);
-  psift_status st = psift_similarity_estimate(ctx, m, n, &opt, mask.data(), model, &has, &cnt);
-  if (st != PSIFT_OK) return st;
+// The statistics of summarize_tracking (src/pipeline.rs:2227-2271) over the
+// matches that `mask` marks (all of them when it marks none), in the reference's
+// f32 order.  n > 0.
+void tracking_stats(const psift_match* m, uint32_t n, const uint8_t* mask, const float* q_scale,
+                    const float* q_ori, const float* t_scale, const float* t_ori, psift_tracking_summary* out) {
   std::vector<const psift_match*> act;
   for (uint32_t i = 0; i < n; ++i)
     if (mask[i]) act.push_back(&m[i]);
@@ -230,6 +211,8 @@ extern "C" psift_status psift_summarize_tracking(psift_ctx* ctx, const psift_mat
   const float inv_n = 1.0f / (float)act.size();
   float sdx = 0, sdy = 0, ssr = 0, ssin = 0, scos = 0;
   std::vector<float> dxs, dys;
+  dxs.reserve(act.size());
+  dys.reserve(act.size());
   for (const psift_match* a : act) {
     sdx += a->displacement_x;
     sdy += a->displacement_y;
@@ -247,9 +230,36 @@ extern "C" psift_status psift_summarize_tracking(psift_ctx* ctx, const psift_mat
   out->inlier_ratio = (float)act.size() / (float)n;
   out->mean_dx = sdx * inv_n;
   out->mean_dy = sdy * inv_n;
-  out->median_dx = psift::median_f32(dxs);
-  out->median_dy = psift::median_f32(dys);
+  out->median_dx = median_f32(dxs);
+  out->median_dy = median_f32(dys);
   out->mean_scale_ratio = ssr * inv_n;
   out->mean_rotation_deg = mrot * 57.2957795130823208767981548141051703f;
+}
+}  // namespace psift
+
+extern "C" psift_status psift_summarize_tracking(psift_ctx* ctx, const psift_match* m, uint32_t n,
+                                                 const float* q_scale, const float* q_ori, uint32_t nq,
+                                                 const float* t_scale, const float* t_ori, uint32_t nt,
+                                                 psift_tracking_summary* out) {
+  // summarize_tracking (src/pipeline.rs:2210-2272): the similarity RANSAC runs on the
+  // device; the O(n) summary repeats the reference's f32 sums on the host.
+  if (!ctx || !out) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (n == 0) {
+    *out = psift_tracking_summary{0, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f};
+    return PSIFT_OK;
+  }
+  if (!m || !q_scale || !q_ori || !t_scale || !t_ori) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  for (uint32_t i = 0; i < n; ++i)
+    if (m[i].query_index >= nq || m[i].target_index >= nt)
+      return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "match index outside the feature arrays");
+  std::vector<uint8_t> mask(n);
+  float model[9];
+  int32_t has = 0;
+  uint32_t cnt = 0;
+  psift_ransac_options opt;
+  psift_ransac_options_default(&opt);
+  psift_status st = psift_similarity_estimate(ctx, m, n, &opt, mask.data(), model, &has, &cnt);
+  if (st != PSIFT_OK) return st;
+  psift::tracking_stats(m, n, mask.data(), q_scale, q_ori, t_scale, t_ori, out);
   return PSIFT_OK;
 }

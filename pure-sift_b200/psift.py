@@ -39,8 +39,10 @@ PSIFT_OK = 0
 PSIFT_ERR_INVALID_ARGUMENT = 1
 PSIFT_ERR_INVALID_CONFIG = 2
 PSIFT_ERR_CAPACITY = 3
+PSIFT_ERR_IO = 9
+PSIFT_ERR_FORMAT = 10
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "INVALID_CONFIG", 3: "CAPACITY", 4: "CUDA",
-                5: "OUT_OF_MEMORY", 6: "TIMEOUT", 7: "NO_DEVICE", 8: "INTERNAL"}
+                5: "OUT_OF_MEMORY", 6: "TIMEOUT", 7: "NO_DEVICE", 8: "INTERNAL", 9: "IO", 10: "FORMAT"}
 
 
 class PsiftError(RuntimeError):
@@ -100,6 +102,17 @@ class CTracking(C.Structure):
     _fields_ = [("raw_match_count", C.c_uint32), ("match_count", C.c_uint32), ("inlier_ratio", C.c_float),
                 ("mean_dx", C.c_float), ("mean_dy", C.c_float), ("median_dx", C.c_float),
                 ("median_dy", C.c_float), ("mean_scale_ratio", C.c_float), ("mean_rotation_deg", C.c_float)]
+
+
+class CCatalogParams(C.Structure):
+    _fields_ = [("octaves", C.c_uint32), ("scales", C.c_uint32), ("threshold", C.c_float),
+                ("descriptor_kind", C.c_int32)]
+
+
+class CCatalogHit(C.Structure):
+    _fields_ = [("entry", C.c_uint32), ("coarse_votes", C.c_uint32), ("tracking", CTracking),
+                ("similarity", C.c_float * 6), ("has_similarity", C.c_int32), ("homography", C.c_float * 9),
+                ("has_homography", C.c_int32)]
 
 
 KEYPOINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("scale", "<f4"), ("response", "<f4"),
@@ -183,6 +196,20 @@ _SIGS = {
     "psift_detect_and_compute_u8_noalloc_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
                                                           C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p,
                                                           C.c_void_p]),
+    "psift_catalog_create": (C.c_int, [C.c_void_p, C.POINTER(CCatalogParams), C.POINTER(C.c_void_p)]),
+    "psift_catalog_destroy": (C.c_int, [C.c_void_p]),
+    "psift_catalog_params_get": (C.c_int, [C.c_void_p, C.POINTER(CCatalogParams)]),
+    "psift_catalog_size": (C.c_uint32, [C.c_void_p]),
+    "psift_catalog_entry": (C.c_int, [C.c_void_p, C.c_uint32, C.c_char_p, C.c_size_t, C.POINTER(C.c_uint32),
+                                      C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    "psift_catalog_find": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_uint32)]),
+    "psift_catalog_upsert": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_uint32, C.POINTER(CFeatures)]),
+    "psift_catalog_remove": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32)]),
+    "psift_catalog_features": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(CFeatures), C.c_void_p]),
+    "psift_catalog_load_binary": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "psift_catalog_save_binary": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "psift_catalog_search": (C.c_int, [C.c_void_p, C.POINTER(CFeatures), C.c_uint32, C.c_uint32, C.c_float,
+                                       C.c_float, C.POINTER(CCatalogHit), C.c_uint32, C.POINTER(C.c_uint32)]),
 }
 
 _lib = None
@@ -886,6 +913,208 @@ class FeatureCatalog:
             hits.append(CatalogSearchHit(e.id, e.width, e.height, len(e.features), v, tracking, sim_tf, hom_tf))
         hits.sort(key=lambda h: (-h.tracking.match_count, -h.tracking.inlier_ratio, -h.coarse_votes, h.id))
         return hits[:top_k]
+
+
+@dataclass
+class CatalogEntrySummary:
+    """``CatalogEntrySummary`` (src/catalog.rs:47-58)."""
+    id: str
+    width: int
+    height: int
+    feature_count: int
+
+
+BINARY_CATALOG_MAGIC = b"PSIFTCAT"
+_KIND_NAMES = {0: "Sift", 1: "RootSift"}
+
+
+def _c_features_count(f: Features) -> tuple:
+    """CFeatures with count = capacity = len(f), and the contiguous f32 arrays it points into."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (f.x, f.y, f.scale, f.response, f.orientation)]
+    d = np.ascontiguousarray(f.descriptors, dtype=np.float32).reshape(len(f), 128)
+    n = len(f)
+    return CFeatures(n, n, *(a.ctypes.data for a in arrs), d.ctypes.data), (arrs, d)
+
+
+class DeviceCatalog:
+    """``FeatureCatalog`` (src/catalog.rs:182-702) resident in device memory.
+
+    Every entry's features, 128-bit codes and the entry table live on the GPU
+    (``psift_catalog_*``).  ``search_features`` runs the coarse votes, the
+    shortlist's Lowe matching and its similarity / homography RANSAC as batched
+    launches; ``load_binary`` / ``save_binary`` move PSIFTCAT v1 files to and from
+    device memory.  Entry order, upsert (replace in place or append) and remove
+    (swap_remove) follow the reference."""
+
+    def __init__(self, octaves: int = 3, scales: int = 3, threshold: float = DEFAULT_CONTRAST_THRESHOLD,
+                 descriptor_kind: int = 0, ctx: Context | None = None, _handle=None):
+        self.ctx = ctx or default_context()
+        if _handle is None:
+            prm = CCatalogParams(octaves, scales, threshold, descriptor_kind)
+            _handle = C.c_void_p()
+            self.ctx.check(self.ctx.lib.psift_catalog_create(self.ctx.handle, C.byref(prm), C.byref(_handle)))
+        self.handle = _handle
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.ctx.lib.psift_catalog_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return int(self.ctx.lib.psift_catalog_size(self.handle))
+
+    @property
+    def params(self) -> CCatalogParams:
+        p = CCatalogParams()
+        self.ctx.check(self.ctx.lib.psift_catalog_params_get(self.handle, C.byref(p)))
+        return p
+
+    def entry(self, i: int) -> CatalogEntrySummary:
+        lib = self.ctx.lib
+        cap = 256
+        while True:
+            buf = C.create_string_buffer(cap)
+            n, w, h, cnt = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint64()
+            self.ctx.check(lib.psift_catalog_entry(self.handle, i, buf, cap, C.byref(n), C.byref(w), C.byref(h),
+                                                   C.byref(cnt)))
+            if n.value < cap:
+                return CatalogEntrySummary(buf.raw[:n.value].decode("utf-8"), w.value, h.value, cnt.value)
+            cap = n.value + 1
+
+    def list_summaries(self) -> list:
+        """``list_summaries`` (src/catalog.rs:355-366)."""
+        return [self.entry(i) for i in range(len(self))]
+
+    def index_of(self, id: str) -> int | None:
+        i = C.c_uint32()
+        st = self.ctx.lib.psift_catalog_find(self.handle, id.encode("utf-8"), C.byref(i))
+        return int(i.value) if st == PSIFT_OK else None
+
+    def entry_features(self, i: int):
+        """Entry i's features and (n, 2) u64 codes, copied back from the device."""
+        n = self.entry(i).feature_count
+        f = Features.empty(n)
+        codes = np.zeros((max(n, 1), 2), np.uint64)
+        cf = CFeatures(n, 0, f.x.ctypes.data, f.y.ctypes.data, f.scale.ctypes.data, f.response.ctypes.data,
+                       f.orientation.ctypes.data, f.descriptors.ctypes.data)
+        self.ctx.check(self.ctx.lib.psift_catalog_features(self.handle, i, C.byref(cf), codes.ctypes.data))
+        return f, codes[:n]
+
+    def upsert_entry(self, id: str, width: int, height: int, features: Features):
+        """``upsert_entry`` (src/catalog.rs:324-342)."""
+        cf, keep = _c_features_count(features)
+        self.ctx.check(self.ctx.lib.psift_catalog_upsert(self.handle, id.encode("utf-8"), width, height,
+                                                         C.byref(cf)))
+        del keep
+
+    def remove(self, id: str) -> bool:
+        """``remove`` (src/catalog.rs:345-353): swap_remove."""
+        r = C.c_int32()
+        self.ctx.check(self.ctx.lib.psift_catalog_remove(self.handle, id.encode("utf-8"), C.byref(r)))
+        return bool(r.value)
+
+    def search_features(self, query: Features, top_k: int = DEFAULT_CATALOG_TOP_K,
+                        shortlist_k: int = DEFAULT_CATALOG_SHORTLIST, ratio_threshold: float = DEFAULT_MATCH_RATIO,
+                        ransac_threshold: float = DEFAULT_RANSAC_REPROJ_THRESHOLD) -> list:
+        """``search_features`` (src/catalog.rs:576-702)."""
+        cap = max(int(top_k), 1)
+        hits = (CCatalogHit * cap)()
+        cnt = C.c_uint32()
+        cf, keep = _c_features_count(query)
+        self.ctx.check(self.ctx.lib.psift_catalog_search(self.handle, C.byref(cf), top_k, shortlist_k,
+                                                         ratio_threshold, ransac_threshold, hits, cap,
+                                                         C.byref(cnt)))
+        del keep
+        out = []
+        for k in range(cnt.value):
+            h = hits[k]
+            e = self.entry(h.entry)
+            t = h.tracking
+            tr = TrackingSummary(t.raw_match_count, t.match_count, t.inlier_ratio, (t.mean_dx, t.mean_dy),
+                                 (t.median_dx, t.median_dy), t.mean_scale_ratio, t.mean_rotation_deg)
+            sim = np.array(h.similarity[:], np.float32) if h.has_similarity else None
+            hom = np.array(h.homography[:], np.float32).reshape(3, 3) if h.has_homography else None
+            out.append(CatalogSearchHit(e.id, e.width, e.height, e.feature_count, h.coarse_votes, tr, sim, hom))
+        return out
+
+    # ---- persistence (src/catalog.rs:378-574)
+    @classmethod
+    def load_binary(cls, path: str, ctx: Context | None = None) -> "DeviceCatalog":
+        """``load_binary`` (src/catalog.rs:447-540), straight into device memory."""
+        ctx = ctx or default_context()
+        h = C.c_void_p()
+        ctx.check(ctx.lib.psift_catalog_load_binary(ctx.handle, os.fsencode(path), C.byref(h)))
+        return cls(ctx=ctx, _handle=h)
+
+    def save_binary(self, path: str):
+        """``save_binary`` (src/catalog.rs:401-445), written atomically."""
+        self.ctx.check(self.ctx.lib.psift_catalog_save_binary(self.handle, os.fsencode(path)))
+
+    def to_json_obj(self) -> dict:
+        p = self.params
+        entries = []
+        for i in range(len(self)):
+            e = self.entry(i)
+            f, _ = self.entry_features(i)
+            feats = [{"x": float(f.x[j]), "y": float(f.y[j]), "scale": float(f.scale[j]),
+                      "response": float(f.response[j]), "orientation": float(f.orientation[j]),
+                      "descriptor": [float(v) for v in f.descriptors[j]]} for j in range(len(f))]
+            entries.append({"id": e.id, "width": e.width, "height": e.height, "features": feats})
+        return {"octaves": int(p.octaves), "scales": int(p.scales), "threshold": float(p.threshold),
+                "descriptor_kind": _KIND_NAMES[int(p.descriptor_kind)], "entries": entries}
+
+    def save_json(self, path: str, pretty: bool = False):
+        """``save_json`` (src/catalog.rs:378-388): serde field names; temp file + rename."""
+        import json
+        text = json.dumps(self.to_json_obj(), indent=2 if pretty else None,
+                          separators=None if pretty else (",", ":")) + "\n"
+        d = os.path.dirname(path)
+        if d:
+            os.makedirs(d, exist_ok=True)
+        tmp = os.path.join(d, f"{os.path.basename(path) or 'catalog'}.tmp.{os.getpid()}")
+        with open(tmp, "w") as fh:
+            fh.write(text)
+        os.replace(tmp, path)
+
+    @classmethod
+    def load_json(cls, path: str, ctx: Context | None = None) -> "DeviceCatalog":
+        """``load_json`` (src/catalog.rs:390-399): codes recomputed from the descriptors."""
+        import json
+        with open(path) as fh:
+            obj = json.load(fh)
+        kind = {"Sift": 0, "RootSift": 1}[obj.get("descriptor_kind", "Sift")]
+        cat = cls(int(obj["octaves"]), int(obj["scales"]), float(obj["threshold"]), kind, ctx)
+        for e in obj["entries"]:
+            fs = e["features"]
+            n = len(fs)
+            col = lambda k: np.array([f[k] for f in fs], np.float32).reshape(n)
+            desc = np.array([f["descriptor"] for f in fs], np.float32).reshape(n, 128) if n else \
+                np.zeros((0, 128), np.float32)
+            cat.upsert_entry(e["id"], int(e["width"]), int(e["height"]),
+                             Features(col("x"), col("y"), col("scale"), col("response"), col("orientation"), desc))
+        return cat
+
+    def save_auto(self, path: str, pretty: bool = False):
+        """``save_auto`` (src/catalog.rs:543-553): JSON for a .json extension, else binary."""
+        if os.path.splitext(path)[1].lower() == ".json":
+            self.save_json(path, pretty)
+        else:
+            self.save_binary(path)
+
+    @classmethod
+    def load_auto(cls, path: str, ctx: Context | None = None) -> "DeviceCatalog":
+        """``load_auto`` (src/catalog.rs:556-574): PSIFTCAT magic -> binary, else JSON."""
+        with open(path, "rb") as fh:
+            head = fh.read(8)
+        if head == BINARY_CATALOG_MAGIC:
+            return cls.load_binary(path, ctx)
+        return cls.load_json(path, ctx)
 
 
 def gaussian_blur(img: np.ndarray, sigma: float, ctx: Context | None = None) -> np.ndarray:
