@@ -360,6 +360,96 @@ def catalog_bench(ctx, torch, n_cat: int = 2_000_000, n_q: int = 4096, k: int = 
     }
 
 
+def _psiftcat_bytes(meta, codes, q, per_entry: int, w: int, h: int) -> bytes:
+    """PSIFTCAT v1 file (FeatureCatalog::save_binary layout, src/catalog.rs:401-445)
+    of len(meta) // per_entry entries named img00000, img00001, ..."""
+    import struct
+    n = len(meta)
+    rec = np.zeros(n, np.dtype([("m", "<f4", 5), ("c", "<u8", 2), ("q", "u1", 128)]))
+    rec["m"], rec["c"], rec["q"] = meta, codes, q
+    raw = rec.tobytes()
+    parts = [b"PSIFTCAT", struct.pack("<IIIfBQ", 1, 4, 3, 0.015, 0, n // per_entry)]
+    for e in range(n // per_entry):
+        ib = f"img{e:05d}".encode()
+        parts.append(struct.pack("<I", len(ib)) + ib + struct.pack("<IIQ", w, h, per_entry))
+        parts.append(raw[e * per_entry * 164:(e + 1) * per_entry * 164])
+    return b"".join(parts)
+
+
+def catalog_search_bench(ctx, torch, n_entries: int = 10_000, per_entry: int = 200, n_q: int = 4096,
+                         reps: int = 10):
+    """Device-resident catalog: a PSIFTCAT v1 file of 10,000 entries x 200 features
+    (C4-style descriptors stored as the reference's u8 quantisation, codes of the
+    f32 descriptors) is loaded into device memory, then search_features (top 5,
+    shortlist 16, ratio 0.75, RANSAC 3 px) runs for a 4096-feature query whose
+    first 200 features are the target entry's, perturbed and moved by a
+    similarity (the rest are random).  Host API timing (wall clock of the call)."""
+    import tempfile
+    import psift
+    rng = np.random.default_rng(21)
+    n = n_entries * per_entry
+    d = np.abs(rng.standard_normal((n, 128), dtype=np.float32))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    np.minimum(d, 0.2, out=d)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    q8 = np.clip(np.rint(d * 512.0), 0, 255).astype(np.uint8)
+    codes = np.zeros((n, 2), np.uint64)
+    bits = (d > 0.065)
+    for wd in range(2):
+        blk = bits[:, 64 * wd:64 * wd + 64].astype(np.uint64)
+        codes[:, wd] = (blk << np.arange(64, dtype=np.uint64)).sum(axis=1, dtype=np.uint64)
+    meta = np.zeros((n, 5), np.float32)
+    meta[:, 0] = rng.uniform(0, 1920, n)
+    meta[:, 1] = rng.uniform(0, 1080, n)
+    meta[:, 2] = rng.uniform(1.6, 12.0, n)
+    meta[:, 3] = rng.uniform(0.01, 0.1, n)
+    meta[:, 4] = rng.uniform(0, 2 * np.pi, n)
+    blob = _psiftcat_bytes(meta, codes, q8, per_entry, 1920, 1080)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "catalog.psiftcat")
+        with open(path, "wb") as fh:
+            fh.write(blob)
+        psift.DeviceCatalog.load_binary(path, ctx).close()  # warm: page cache, allocations
+        t0 = time.perf_counter()
+        cat = psift.DeviceCatalog.load_binary(path, ctx)
+        load_s = time.perf_counter() - t0
+    target = 1234
+    tf, _ = cat.entry_features(target)
+    th = np.deg2rad(10.0)
+    qx = 1.1 * (np.cos(th) * tf.x - np.sin(th) * tf.y) + 30.0
+    qy = 1.1 * (np.sin(th) * tf.x + np.cos(th) * tf.y) - 20.0
+    qd = np.abs(rng.standard_normal((n_q, 128), dtype=np.float32))
+    qd[:per_entry] = tf.descriptors + 0.01 * np.abs(rng.standard_normal((per_entry, 128), dtype=np.float32))
+    qd /= np.linalg.norm(qd, axis=1, keepdims=True)
+    query = psift.Features(np.r_[qx, rng.uniform(0, 1920, n_q - per_entry)].astype(np.float32),
+                           np.r_[qy, rng.uniform(0, 1080, n_q - per_entry)].astype(np.float32),
+                           np.r_[tf.scale * 1.1, rng.uniform(1.6, 12, n_q - per_entry)].astype(np.float32),
+                           np.full(n_q, 0.05, np.float32),
+                           np.r_[tf.orientation + th, rng.uniform(0, 6.28, n_q - per_entry)].astype(np.float32), qd)
+    hits = cat.search_features(query)
+    l0 = ctx.launch_count
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        hits = cat.search_features(query)
+    search_s = (time.perf_counter() - t0) / reps
+    launches = (ctx.launch_count - l0) / reps
+    ctx.enable_stage_timing(True)
+    ctx.stage_times(reset=True)
+    for _ in range(reps):
+        cat.search_features(query)
+    stages = {k: v[0] / reps for k, v in ctx.stage_times(reset=True).items() if v[1]}
+    ctx.enable_stage_timing(False)
+    cat.close()
+    return {
+        "workload": f"PSIFTCAT v1 catalog of {n_entries} entries x {per_entry} features ({len(blob) / 1e6:.0f} MB), "
+                    f"{n_q}-feature query, top-5 / shortlist 16, host API wall clock",
+        "load_binary_s": load_s, "load_binary_gbs": len(blob) / load_s / 1e9,
+        "search_ms": search_s * 1e3, "launches_per_search": launches, "device_stage_ms_per_search": stages,
+        "top_hit": hits[0].id if hits else None, "top_hit_inliers": hits[0].tracking.match_count if hits else 0,
+        "expected_top_hit": f"img{target:05d}",
+    }
+
+
 def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int = 3):
     """Learned RANSAC proposal: 1024 synthetic 1080p pairs with known perspective
     homographies, 2k-8k putative matches each, outlier ratio U(0.1, 0.7).  The MLP
@@ -602,7 +692,8 @@ def run_ours(args):
             "stage_ms_per_step": {k: v[0] / reps for k, v in st.items() if v[1]},
             "clocks": clk.summary(),
         }
-        for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench), ("learned_ransac", ransac_bench)):
+        for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench),
+                        ("catalog_search", catalog_search_bench), ("learned_ransac", ransac_bench)):
             if getattr(args, "no_" + key):
                 continue
             try:
@@ -641,9 +732,10 @@ def main():
     ap.add_argument("--only-device", action="store_true", help="time the device path only (profiling case)")
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
-    ap.add_argument("--only-section", choices=["match", "catalog", "learned_ransac", "uneven_batch"],
+    ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "learned_ransac", "uneven_batch"],
                     help="run one section alone (profiling case)")
     ap.add_argument("--no-catalog", action="store_true")
+    ap.add_argument("--no-catalog-search", dest="no_catalog_search", action="store_true")
     ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
     args = ap.parse_args()
@@ -658,6 +750,7 @@ def main():
         ctx = psift.Context(int(os.environ.get("LOCAL_RANK", "0")))
         fns = {"match": lambda: match_bench(ctx, torch, n_pairs=args.match_pairs, reps=args.steps),
                "catalog": lambda: catalog_bench(ctx, torch), "learned_ransac": lambda: ransac_bench(ctx, torch),
+               "catalog_search": lambda: catalog_search_bench(ctx, torch),
                "uneven_batch": lambda: uneven_bench(ctx, torch)}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)
         ctx.close()

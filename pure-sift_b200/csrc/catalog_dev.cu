@@ -166,14 +166,19 @@ bool valid_utf8(const uint8_t* s, size_t n) {
   return true;
 }
 
-struct Reader {
-  const uint8_t* p;
-  size_t left;
+// Sequential reads of a file of known size; a short read counts as EOF.
+struct FileReader {
+  FILE* f;
+  uint64_t pos, size;
+  uint64_t left() const { return size - pos; }
   bool take(void* dst, size_t n) {
-    if (left < n) return false;
-    std::memcpy(dst, p, n);
-    p += n;
-    left -= n;
+    if (left() < n || (n && std::fread(dst, 1, n, f) != n)) return false;
+    pos += n;
+    return true;
+  }
+  bool skip(uint64_t n) {
+    if (left() < n || fseeko(f, (off_t)n, SEEK_CUR) != 0) return false;
+    pos += n;
     return true;
   }
 };
@@ -498,17 +503,16 @@ psift_status psift_catalog_load_binary(psift_ctx* ctx, const char* path, psift_c
   const std::string p = path;
   FILE* f = std::fopen(path, "rb");
   if (!f) return set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`: " + strerror(errno));
-  std::vector<uint8_t> raw;
-  {
-    uint8_t buf[1 << 16];
-    size_t got;
-    while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) raw.insert(raw.end(), buf, buf + got);
-    const bool err = std::ferror(f) != 0;
-    std::fclose(f);
-    if (err) return set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`");
-  }
-  // Header and entry table on the host (the reference's read order and messages).
-  Reader r{raw.data(), raw.size()};
+  struct Closer {
+    FILE* f;
+    ~Closer() { std::fclose(f); }
+  } closer{f};
+  struct stat sb;
+  if (fstat(fileno(f), &sb) != 0)
+    return set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`: " + strerror(errno));
+  FileReader r{f, 0, (uint64_t)sb.st_size};
+  // Pass 1: header and entry table (the reference's read order and messages),
+  // seeking over the record blocks.
   const std::string eof = "Unexpected EOF while reading binary catalog";
   char magic[8];
   if (!r.take(magic, 8)) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
@@ -535,23 +539,22 @@ psift_status psift_catalog_load_binary(psift_ctx* ctx, const char* path, psift_c
     uint32_t id_len = 0, w = 0, h = 0;
     uint64_t cnt = 0;
     if (!r.take(&id_len, 4)) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
-    if (r.left < id_len) return set_error(ctx, PSIFT_ERR_FORMAT, "Truncated entry id in binary catalog");
-    if (!valid_utf8(r.p, id_len)) return set_error(ctx, PSIFT_ERR_FORMAT, "Invalid UTF-8 entry id in binary catalog");
+    if (r.left() < id_len) return set_error(ctx, PSIFT_ERR_FORMAT, "Truncated entry id in binary catalog");
     psift_catalog::Entry E;
-    E.id.assign(reinterpret_cast<const char*>(r.p), id_len);
-    r.p += id_len;
-    r.left -= id_len;
+    E.id.resize(id_len);
+    if (!r.take(&E.id[0], id_len)) return set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`");
+    if (!valid_utf8(reinterpret_cast<const uint8_t*>(E.id.data()), id_len))
+      return set_error(ctx, PSIFT_ERR_FORMAT, "Invalid UTF-8 entry id in binary catalog");
     if (!r.take(&w, 4) || !r.take(&h, 4) || !r.take(&cnt, 8)) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
     // every record must be present before the next header (the reference's reads)
-    if (cnt > r.left / kRecordBytes) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
+    if (cnt > r.left() / kRecordBytes) return set_error(ctx, PSIFT_ERR_FORMAT, eof);
     E.width = w;
     E.height = h;
     E.count = cnt;
     E.offset = total;
-    file_off.push_back((long long)(r.p - raw.data()));
+    file_off.push_back((long long)r.pos);
     out_off.push_back((long long)total);
-    r.p += cnt * kRecordBytes;
-    r.left -= cnt * kRecordBytes;
+    if (!r.skip(cnt * kRecordBytes)) return set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`");
     total += cnt;
     if (total > kMaxFeatures) return set_error(ctx, PSIFT_ERR_CAPACITY, "catalog larger than 2^31-1 features");
     entries.push_back(std::move(E));
@@ -571,48 +574,59 @@ psift_status psift_catalog_load_binary(psift_ctx* ctx, const char* path, psift_c
   if (total > 0) {
     ce = alloc_arrays(cat->a, std::max<uint64_t>(total, 1024));
     if (ce != cudaSuccess) return fail(cuda_error(ctx, ce, "cudaMalloc(catalog)"));
-    // Device workspace: the file, the two offset tables and the u8 descriptors.
-    const size_t fb = align_up(raw.size(), 256), tb = align_up(8 * out_off.size(), 256);
+    // Device workspace: the file up to its last record, the two offset tables
+    // and the u8 descriptors.
+    const uint64_t used = r.pos;
+    const size_t fb = align_up(used, 256), tb = align_up(8 * out_off.size(), 256);
     if ((st = cat->reserve_scratch(fb + 2 * tb + total * 128)) != PSIFT_OK) return fail(st);
     uint8_t* d_file = (uint8_t*)cat->scratch;
     long long* d_foff = (long long*)(cat->scratch + fb);
     long long* d_ooff = (long long*)(cat->scratch + fb + tb);
     uint8_t* d_q8 = (uint8_t*)(cat->scratch + fb + 2 * tb);
-    // Upload through two pinned staging halves, the copy of one overlapping the
-    // host memcpy into the other.
-    constexpr size_t kChunk = 16u << 20;
+    // Pass 2: the file streamed into two pinned staging halves; the copy of one
+    // half to the device overlaps the read into the other.
+    constexpr size_t kChunk = 32u << 20;
     if ((st = pinned_reserve(ctx, 2 * kChunk)) != PSIFT_OK) return fail(st);
-    cudaEvent_t ev[2];
+    if (std::fseek(f, 0, SEEK_SET) != 0) return fail(set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`"));
+    cudaEvent_t ev[2] = {nullptr, nullptr};
     for (auto& x : ev)
-      if ((ce = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess)
-        return fail(cuda_error(ctx, ce, "cudaEventCreate"));
-    bool used[2] = {false, false};
-    for (size_t off = 0, k = 0; off < raw.size(); off += kChunk, k ^= 1) {
-      const size_t n = std::min(kChunk, raw.size() - off);
-      if (used[k]) cudaEventSynchronize(ev[k]);
-      std::memcpy(ctx->pinned.base + k * kChunk, raw.data() + off, n);
-      ce = cudaMemcpyAsync(d_file + off, ctx->pinned.base + k * kChunk, n, cudaMemcpyHostToDevice, ctx->stream);
+      if ((ce = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) break;
+    bool used_buf[2] = {false, false}, short_read = false;
+    for (uint64_t off = 0, k = 0; ce == cudaSuccess && off < used; off += kChunk, k ^= 1) {
+      const size_t n = (size_t)std::min<uint64_t>(kChunk, used - off);
+      if (used_buf[k]) cudaEventSynchronize(ev[k]);
+      char* hbuf = ctx->pinned.base + k * kChunk;
+      if (std::fread(hbuf, 1, n, f) != n) {
+        short_read = true;
+        break;
+      }
+      ce = cudaMemcpyAsync(d_file + off, hbuf, n, cudaMemcpyHostToDevice, ctx->stream);
       if (ce == cudaSuccess) ce = cudaEventRecord(ev[k], ctx->stream);
-      if (ce != cudaSuccess) break;
-      used[k] = true;
+      used_buf[k] = true;
     }
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_foff, file_off.data(), 8 * file_off.size(), cudaMemcpyHostToDevice, ctx->stream);
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_ooff, out_off.data(), 8 * out_off.size(), cudaMemcpyHostToDevice, ctx->stream);
-    if (ce == cudaSuccess) {
-      const long long blocks = ((long long)total + kSplitWarps - 1) / kSplitWarps;
-      psiftcat_split_kernel<<<(unsigned)blocks, kSplitWarps * 32, 0, ctx->stream>>>(
-          d_file, d_foff, d_ooff, (int)file_off.size(), (long long)total, cat->a.xy, cat->a.scale, cat->a.resp,
-          cat->a.ori, cat->a.codes, d_q8);
-      ctx->launches++;
-      ce = cudaGetLastError();
+    if (ce == cudaSuccess && !short_read) {
+      ce = cudaMemcpyAsync(d_foff, file_off.data(), 8 * file_off.size(), cudaMemcpyHostToDevice, ctx->stream);
+      if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(d_ooff, out_off.data(), 8 * out_off.size(), cudaMemcpyHostToDevice, ctx->stream);
+      if (ce == cudaSuccess) {
+        const long long blocks = ((long long)total + kSplitWarps - 1) / kSplitWarps;
+        psiftcat_split_kernel<<<(unsigned)blocks, kSplitWarps * 32, 0, ctx->stream>>>(
+            d_file, d_foff, d_ooff, (int)file_off.size(), (long long)total, cat->a.xy, cat->a.scale, cat->a.resp,
+            cat->a.ori, cat->a.codes, d_q8);
+        ctx->launches++;
+        ce = cudaGetLastError();
+      }
+      if (ce == cudaSuccess) {
+        ce = launch_dequantize(d_q8, (int)total, cat->a.desc, ctx->stream);
+        ctx->launches++;
+      }
     }
-    if (ce == cudaSuccess) {
-      ce = launch_dequantize(d_q8, (int)total, cat->a.desc, ctx->stream);
-      ctx->launches++;
-    }
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
-    for (auto& x : ev) cudaEventDestroy(x);
+    const cudaError_t cs = cudaStreamSynchronize(ctx->stream);
+    if (ce == cudaSuccess) ce = cs;
+    for (auto& x : ev)
+      if (x) cudaEventDestroy(x);
     if (ce != cudaSuccess) return fail(cuda_error(ctx, ce, "PSIFTCAT upload"));
+    if (short_read) return fail(set_error(ctx, PSIFT_ERR_IO, "Failed to read binary catalog `" + p + "`"));
   }
   *out = cat;
   return PSIFT_OK;
