@@ -167,9 +167,9 @@ __global__ void __launch_bounds__(kMarkWarps * 32) extrema_mark_kernel(const Ima
   if (octave >= P.n_oct) return;
   const OctaveDev& O = P.oct[octave];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int y = blockIdx.x * kMarkWarps + warp;
+  const int y = blockIdx.y * kMarkWarps + warp;
   if (y >= O.h) return;
-  const int s = blockIdx.y + 1;
+  const int s = blockIdx.x + 1;  // slices fastest: the three slices of a row band share D rows in L2
   const long long ps = O.plane_stride;
   const float* Dp = O.d + (long long)(s - 1) * ps + (long long)y * O.pitch;
   const float* Dc = O.d + (long long)s * ps + (long long)y * O.pitch;
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(1024) select_topk_kernel(const ImagePlan* __re
 
 cudaError_t launch_extrema_mark(const ImagePlan* plans, int n, int octave, int max_h, const ExtremaParams& prm,
                                 cudaStream_t st) {
-  dim3 grid((max_h + kMarkWarps - 1) / kMarkWarps, prm.scales, n);
+  dim3 grid(prm.scales, (max_h + kMarkWarps - 1) / kMarkWarps, n);
   extrema_mark_kernel<<<grid, kMarkWarps * 32, 0, st>>>(plans, octave, prm);
   return cudaGetLastError();
 }
