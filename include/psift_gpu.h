@@ -408,6 +408,26 @@ psift_status psift_catalog_search(psift_catalog* cat, const psift_features* quer
                                   uint32_t shortlist_k, float ratio, float ransac_threshold,
                                   psift_catalog_hit* hits, uint32_t capacity, uint32_t* count);
 
+/* ---------------------------------------------------------------- warp and stitch */
+/* warp_and_stitch (src/visualize.rs:379-483): the query warped into the target's
+ * frame through the inverse of h9 (row-major, f32; bilinear inverse mapping in
+ * f64) and feather-blended with the target on the union canvas.  Images are RGBA8
+ * with row strides in bytes.  Call with canvas = NULL for the canvas size (and
+ * origin, 2 doubles, optional: the canvas corner in target coordinates), then
+ * with canvas_capacity >= width * height * 4 bytes.  Errors carry the reference's
+ * messages: singular homography, a corner projected to infinity or to a
+ * non-finite coordinate, a canvas over 8192 x 8192 or 25,000,000 px. */
+psift_status psift_warp_and_stitch(psift_ctx* ctx, const uint8_t* query, uint32_t qh, uint32_t qw,
+                                   size_t q_stride, const uint8_t* target, uint32_t th, uint32_t tw,
+                                   size_t t_stride, const float* h9, uint8_t* canvas, size_t canvas_capacity,
+                                   uint32_t* width, uint32_t* height, double* origin);
+/* Device-resident variant: query, target and canvas are device pointers (4-byte
+ * aligned, strides multiples of 4); queued on the context's stream. */
+psift_status psift_warp_and_stitch_dev(psift_ctx* ctx, const uint8_t* query, uint32_t qh, uint32_t qw,
+                                       size_t q_stride, const uint8_t* target, uint32_t th, uint32_t tw,
+                                       size_t t_stride, const float* h9, uint8_t* canvas,
+                                       size_t canvas_capacity, uint32_t* width, uint32_t* height);
+
 /* Allocation-free variant of psift_detect_and_compute_batch_dev for one u8 image.
  * No counterpart in the reference: it exists for callers that cannot allocate
  * device memory -- plugin hosts that hand out only a stream, real-time loops in

@@ -109,6 +109,9 @@ def lib():
             L.oracle_hamming_votes.argtypes = [_u64p, C.c_int, _u64p, _i64p, C.c_int, C.c_int, _u32p]
             L.oracle_hamming_topk.argtypes = [_u64p, C.c_int, _u64p, C.c_int64, C.c_int, _u32p, _u32p]
             L.oracle_l2_rerank.argtypes = [_fp, C.c_int, _fp, _u32p, C.c_int, _u32p, _fp]
+            L.oracle_warp_and_stitch.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_int,
+                                                 C.c_int, C.c_size_t, _fp, C.c_void_p, _ip, _ip, C.c_void_p]
+            L.oracle_warp_and_stitch.restype = C.c_int
             L.oracle_splitmix64_next.argtypes = [_u64p]
             L.oracle_splitmix64_next.restype = C.c_uint64
             _lib = L
@@ -334,3 +337,23 @@ def l2_rerank(q_desc, cat_desc, cand):
     lib().oracle_l2_rerank(_p(qd, _fp), qd.shape[0], _p(cd, _fp), _p(cand, _u32p), k, _p(out_idx, _u32p),
                            _p(out_d2, _fp))
     return out_idx, out_d2
+
+
+def warp_and_stitch(query, target, h9):
+    """warp_and_stitch (src/visualize.rs:379-483): (canvas, (origin_x, origin_y)), or
+    an int error code (-1 singular, -2 infinity, -3 non-finite, -4 too large)."""
+    q = np.ascontiguousarray(query, dtype=np.uint8)
+    t = np.ascontiguousarray(target, dtype=np.uint8)
+    h = _f32(h9).reshape(9)
+    w, hh = C.c_int(), C.c_int()
+    origin = np.zeros(2, np.float64)
+    rc = lib().oracle_warp_and_stitch(q.ctypes.data, q.shape[0], q.shape[1], q.shape[1] * 4, t.ctypes.data,
+                                      t.shape[0], t.shape[1], t.shape[1] * 4, _p(h, _fp), None, C.byref(w),
+                                      C.byref(hh), origin.ctypes.data)
+    if rc != 0:
+        return rc
+    canvas = np.zeros((hh.value, w.value, 4), np.uint8)
+    lib().oracle_warp_and_stitch(q.ctypes.data, q.shape[0], q.shape[1], q.shape[1] * 4, t.ctypes.data,
+                                 t.shape[0], t.shape[1], t.shape[1] * 4, _p(h, _fp), canvas.ctypes.data,
+                                 C.byref(w), C.byref(hh), origin.ctypes.data)
+    return canvas, (float(origin[0]), float(origin[1]))

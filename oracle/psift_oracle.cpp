@@ -1610,4 +1610,112 @@ void oracle_l2_rerank(const float* qd, int nq, const float* cat_desc, const uint
   }
 }
 
+// warp_and_stitch (src/visualize.rs:379-483) with invert_matrix_3x3 (:202-233),
+// project_f64 (:236-247), sample_bilinear_rgba (:250-287) and Homography2D::project
+// (src/pipeline.rs:1122-1132).  Returns 0 and the canvas geometry (canvas = NULL:
+// geometry only), or a negative code: -1 singular, -2 corner at infinity,
+// -3 non-finite corner, -4 canvas over the safety limits.
+static bool ow_sample(const uint8_t* img, int h, int w, size_t stride, double x, double y, double rgba[4],
+                      double* feather) {
+  const double wf = (double)w, hf = (double)h;
+  if (x < 0.0 || y < 0.0 || x > (wf - 1.0) || y > (hf - 1.0)) return false;
+  const uint32_t x0 = (uint32_t)std::floor(x), y0 = (uint32_t)std::floor(y);
+  const uint32_t x1 = std::min<uint32_t>(x0 + 1, (uint32_t)w - 1), y1 = std::min<uint32_t>(y0 + 1, (uint32_t)h - 1);
+  const double fx = x - (double)x0, fy = y - (double)y0;
+  const double w00 = (1.0 - fx) * (1.0 - fy), w10 = fx * (1.0 - fy), w01 = (1.0 - fx) * fy, w11 = fx * fy;
+  const uint8_t* p00 = img + y0 * stride + 4 * (size_t)x0;
+  const uint8_t* p10 = img + y0 * stride + 4 * (size_t)x1;
+  const uint8_t* p01 = img + y1 * stride + 4 * (size_t)x0;
+  const uint8_t* p11 = img + y1 * stride + 4 * (size_t)x1;
+  for (int c = 0; c < 4; ++c)
+    rgba[c] = (double)p00[c] * w00 + (double)p10[c] * w10 + (double)p01[c] * w01 + (double)p11[c] * w11;
+  auto fmin_ = [](double a, double b) { return std::isnan(a) ? b : (std::isnan(b) ? a : (a < b ? a : b)); };
+  const double dist_edge = fmin_(fmin_(fmin_(x, (wf - 1.0) - x), y), (hf - 1.0) - y);
+  double f = (dist_edge + 1.0) / 32.0;
+  f = f < 0.02 ? 0.02 : (f > 1.0 ? 1.0 : f);
+  *feather = f;
+  return true;
+}
+
+static uint8_t ow_u8(double v) {  // Rust `as u8`: saturating, NaN -> 0
+  if (!(v == v)) return 0;
+  return v <= 0.0 ? 0 : (v >= 255.0 ? 255 : (uint8_t)v);
+}
+
+int oracle_warp_and_stitch(const uint8_t* q, int qh, int qw, size_t qs, const uint8_t* t, int th, int tw, size_t ts,
+                           const float* h9, uint8_t* canvas, int* out_w, int* out_h, double* origin) {
+  double a[3][3];
+  for (int i = 0; i < 9; ++i) a[i / 3][i % 3] = (double)h9[i];
+  const double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+  const double c01 = -(a[1][0] * a[2][2] - a[1][2] * a[2][0]);
+  const double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+  const double c10 = -(a[0][1] * a[2][2] - a[0][2] * a[2][1]);
+  const double c11 = a[0][0] * a[2][2] - a[0][2] * a[2][0];
+  const double c12 = -(a[0][0] * a[2][1] - a[0][1] * a[2][0]);
+  const double c20 = a[0][1] * a[1][2] - a[0][2] * a[1][1];
+  const double c21 = -(a[0][0] * a[1][2] - a[0][2] * a[1][0]);
+  const double c22 = a[0][0] * a[1][1] - a[0][1] * a[1][0];
+  const double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+  if (std::fabs(det) < 1e-12 || !std::isfinite(det)) return -1;
+  const double id = 1.0 / det;
+  const double hi[3][3] = {{c00 * id, c10 * id, c20 * id}, {c01 * id, c11 * id, c21 * id}, {c02 * id, c12 * id, c22 * id}};
+  const double qwf = qw, qhf = qh, twf = tw, thf = th;
+  double min_x = 0.0, min_y = 0.0, max_x = std::max(twf - 1.0, 0.0), max_y = std::max(thf - 1.0, 0.0);
+  const double corners[4][2] = {{0.0, 0.0}, {qwf - 1.0, 0.0}, {0.0, qhf - 1.0}, {qwf - 1.0, qhf - 1.0}};
+  for (const auto& c : corners) {
+    const float x = (float)c[0], y = (float)c[1];
+    const float w = h9[6] * x + h9[7] * y + h9[8];
+    if (std::fabs(w) < 1e-6f) return -2;
+    const float iw = 1.0f / w;
+    const double px = (double)((h9[0] * x + h9[1] * y + h9[2]) * iw);
+    const double py = (double)((h9[3] * x + h9[4] * y + h9[5]) * iw);
+    if (!std::isfinite(px) || !std::isfinite(py)) return -3;
+    min_x = std::min(min_x, px);
+    min_y = std::min(min_y, py);
+    max_x = std::max(max_x, px);
+    max_y = std::max(max_y, py);
+  }
+  const double ox0 = std::floor(min_x), oy0 = std::floor(min_y);
+  const double wf = std::max(std::ceil(max_x) - ox0 + 1.0, 1.0), hf = std::max(std::ceil(max_y) - oy0 + 1.0, 1.0);
+  if (wf > 8192.0 || hf > 8192.0 || wf * hf > 25000000.0) return -4;
+  *out_w = (int)wf;
+  *out_h = (int)hf;
+  origin[0] = ox0;
+  origin[1] = oy0;
+  if (!canvas) return 0;
+  const int W = *out_w, H = *out_h;
+#pragma omp parallel for schedule(static)
+  for (int oy = 0; oy < H; ++oy) {
+    const double ty = (double)oy + oy0;
+    for (int ox = 0; ox < W; ++ox) {
+      const double tx = (double)ox + ox0;
+      double tc[4], qc[4], tw_ = 0, qw_ = 0;
+      const bool has_t = ow_sample(t, th, tw, ts, tx, ty, tc, &tw_);
+      bool has_q = false;
+      const double w = hi[2][0] * tx + hi[2][1] * ty + hi[2][2];
+      if (!(std::fabs(w) < 1e-7)) {
+        const double iw = 1.0 / w;
+        const double qx = (hi[0][0] * tx + hi[0][1] * ty + hi[0][2]) * iw;
+        const double qy = (hi[1][0] * tx + hi[1][1] * ty + hi[1][2]) * iw;
+        has_q = ow_sample(q, qh, qw, qs, qx, qy, qc, &qw_);
+      }
+      uint8_t* o = canvas + ((size_t)oy * W + ox) * 4;
+      if (has_t && has_q) {
+        const double den = tw_ + qw_, wt = tw_ / den, wq = qw_ / den;
+        for (int c = 0; c < 3; ++c) o[c] = ow_u8(std::round(tc[c] * wt + qc[c] * wq));
+        double al = std::round(tc[3] * wt + qc[3] * wq);
+        al = al < 0.0 ? 0.0 : (al > 255.0 ? 255.0 : al);
+        o[3] = ow_u8(al);
+      } else if (has_t) {
+        for (int c = 0; c < 4; ++c) o[c] = ow_u8(std::round(tc[c]));
+      } else if (has_q) {
+        for (int c = 0; c < 4; ++c) o[c] = ow_u8(std::round(qc[c]));
+      } else {
+        o[0] = o[1] = o[2] = o[3] = 0;
+      }
+    }
+  }
+  return 0;
+}
+
 }  // extern "C"

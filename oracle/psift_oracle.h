@@ -103,6 +103,14 @@ void oracle_l2_rerank(const float* qd, int nq, const float* cat_desc, const uint
 
 uint64_t oracle_splitmix64_next(uint64_t* state);
 
+/* warp_and_stitch (src/visualize.rs:379-483) on RGBA8 images (row strides in
+ * bytes): the canvas geometry (out_w, out_h, origin[2]) and, when canvas is not
+ * NULL, the out_w x out_h x 4 composite.  0 or a negative error code (-1 singular
+ * homography, -2 corner at infinity, -3 non-finite corner, -4 canvas too large). */
+int oracle_warp_and_stitch(const uint8_t* q, int qh, int qw, size_t qs, const uint8_t* t, int th, int tw,
+                           size_t ts, const float* h9, uint8_t* canvas, int* out_w, int* out_h,
+                           double* origin);
+
 #ifdef __cplusplus
 }
 #endif

@@ -196,6 +196,13 @@ _SIGS = {
     "psift_detect_and_compute_u8_noalloc_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
                                                           C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p,
                                                           C.c_void_p]),
+    "psift_warp_and_stitch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p,
+                                        C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t,
+                                        C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p]),
+    "psift_warp_and_stitch_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
+                                            C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p,
+                                            C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32),
+                                            C.POINTER(C.c_uint32)]),
     "psift_catalog_create": (C.c_int, [C.c_void_p, C.POINTER(CCatalogParams), C.POINTER(C.c_void_p)]),
     "psift_catalog_destroy": (C.c_int, [C.c_void_p]),
     "psift_catalog_params_get": (C.c_int, [C.c_void_p, C.POINTER(CCatalogParams)]),
@@ -1115,6 +1122,30 @@ class DeviceCatalog:
         if head == BINARY_CATALOG_MAGIC:
             return cls.load_binary(path, ctx)
         return cls.load_json(path, ctx)
+
+
+def warp_and_stitch(query: np.ndarray, target: np.ndarray, homography, ctx: Context | None = None):
+    """``warp_and_stitch`` (src/visualize.rs:379-483) on the GPU.
+
+    query, target: (h, w, 4) u8 RGBA; homography: 3x3 (query -> target).
+    Returns (canvas (H, W, 4) u8, (origin_x, origin_y)); raises ValueError with
+    the reference's message when it returns Err."""
+    ctx = ctx or default_context()
+    q = np.ascontiguousarray(query, dtype=np.uint8).reshape(query.shape[0], query.shape[1], 4)
+    t = np.ascontiguousarray(target, dtype=np.uint8).reshape(target.shape[0], target.shape[1], 4)
+    h9 = np.ascontiguousarray(homography, dtype=np.float32).reshape(9)
+    w, h = C.c_uint32(), C.c_uint32()
+    origin = np.zeros(2, np.float64)
+    args = (q.ctypes.data, q.shape[0], q.shape[1], q.shape[1] * 4, t.ctypes.data, t.shape[0], t.shape[1],
+            t.shape[1] * 4, h9.ctypes.data)
+    st = ctx.lib.psift_warp_and_stitch(ctx.handle, *args, None, 0, C.byref(w), C.byref(h), origin.ctypes.data)
+    if st == PSIFT_ERR_INVALID_ARGUMENT:
+        raise ValueError(ctx.lib.psift_last_error(ctx.handle).decode())
+    ctx.check(st)
+    canvas = np.empty((h.value, w.value, 4), np.uint8)
+    ctx.check(ctx.lib.psift_warp_and_stitch(ctx.handle, *args, canvas.ctypes.data, canvas.nbytes, C.byref(w),
+                                            C.byref(h), None))
+    return canvas, (float(origin[0]), float(origin[1]))
 
 
 def gaussian_blur(img: np.ndarray, sigma: float, ctx: Context | None = None) -> np.ndarray:
