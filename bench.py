@@ -450,6 +450,70 @@ def catalog_search_bench(ctx, torch, n_entries: int = 10_000, per_entry: int = 2
     }
 
 
+def warp_bench(ctx, torch, reps: int = 50):
+    """warp_and_stitch on a 1080p RGBA pair: the query warped by a C2-style
+    homography (rotation, scale, perspective about the centre) onto the target's
+    frame, feather-blended.  Device variant timed with CUDA events; host API
+    (uploads and canvas download included) by wall clock; the CPU restatement
+    (OpenMP, all host threads) on the same pair."""
+    import psift
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    rng = np.random.default_rng(31)
+    W, H = 1920, 1080
+    q = rng.integers(0, 256, (H, W, 4)).astype(np.uint8)
+    t = rng.integers(0, 256, (H, W, 4)).astype(np.uint8)
+    th = np.deg2rad(8.0)
+    A = np.array([[1.05 * np.cos(th), -1.05 * np.sin(th), 0], [1.05 * np.sin(th), 1.05 * np.cos(th), 0],
+                  [4e-5, -3e-5, 1]])
+    C0 = np.array([[1, 0, -W / 2], [0, 1, -H / 2], [0, 0, 1]])
+    C1 = np.array([[1, 0, W / 2 + 60], [0, 1, H / 2 - 40], [0, 0, 1]])
+    Hm = (C1 @ A @ C0).astype(np.float32)
+    h9 = np.ascontiguousarray(Hm.reshape(9))
+    canvas, origin = psift.warp_and_stitch(q, t, Hm, ctx)
+    dq, dt = torch.from_numpy(q).cuda(), torch.from_numpy(t).cuda()
+    out = torch.empty(canvas.size, dtype=torch.uint8, device="cuda")
+    w, h = C.c_uint32(), C.c_uint32()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def run():
+        ctx.check(ctx.lib.psift_warp_and_stitch_dev(ctx.handle, C.c_void_p(dq.data_ptr()), H, W, 4 * W,
+                                                    C.c_void_p(dt.data_ptr()), H, W, 4 * W, h9.ctypes.data,
+                                                    C.c_void_p(out.data_ptr()), out.numel(), C.byref(w),
+                                                    C.byref(h)))
+    torch.cuda.synchronize()
+    for _ in range(3):
+        run()
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    ctx.synchronize()
+    dev_ms = e0.elapsed_time(e1) / reps
+    same = bool(np.array_equal(out.cpu().numpy().reshape(canvas.shape), canvas))
+    t0 = time.perf_counter()
+    for _ in range(5):
+        psift.warp_and_stitch(q, t, Hm, ctx)
+    host_ms = (time.perf_counter() - t0) / 5 * 1e3
+    t0 = time.perf_counter()
+    ref, _ = O.warp_and_stitch(q, t, Hm)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    px = canvas.shape[0] * canvas.shape[1]
+    algo = 4 * px + 4 * q.shape[0] * q.shape[1] + 4 * t.shape[0] * t.shape[1]
+    peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    return {
+        "workload": f"1080p RGBA query warped onto a 1080p RGBA target, canvas {canvas.shape[1]}x{canvas.shape[0]}",
+        "device_ms": dev_ms, "canvas_mpx_per_s": px / (dev_ms * 1e-3) / 1e6,
+        "roofline": {"bound": "hbm", "achieved": algo / (dev_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": algo / (dev_ms * 1e-3) / 1e9 / peak,
+                     "algorithmic_bytes": algo, "note": "canvas write + each source texel once"},
+        "host_api_ms": host_ms, "cpu_restatement_ms": cpu_ms, "cpu_threads": os.cpu_count(),
+        "identical_to_restatement": same and bool(np.array_equal(ref, canvas)),
+    }
+
+
 def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int = 3):
     """Learned RANSAC proposal: 1024 synthetic 1080p pairs with known perspective
     homographies, 2k-8k putative matches each, outlier ratio U(0.1, 0.7).  The MLP
@@ -693,7 +757,8 @@ def run_ours(args):
             "clocks": clk.summary(),
         }
         for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench),
-                        ("catalog_search", catalog_search_bench), ("learned_ransac", ransac_bench)):
+                        ("catalog_search", catalog_search_bench), ("warp", warp_bench),
+                        ("learned_ransac", ransac_bench)):
             if getattr(args, "no_" + key):
                 continue
             try:
@@ -732,10 +797,12 @@ def main():
     ap.add_argument("--only-device", action="store_true", help="time the device path only (profiling case)")
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
-    ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "learned_ransac", "uneven_batch"],
+    ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "warp", "learned_ransac",
+                                               "uneven_batch"],
                     help="run one section alone (profiling case)")
     ap.add_argument("--no-catalog", action="store_true")
     ap.add_argument("--no-catalog-search", dest="no_catalog_search", action="store_true")
+    ap.add_argument("--no-warp", dest="no_warp", action="store_true")
     ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
     args = ap.parse_args()
@@ -750,7 +817,7 @@ def main():
         ctx = psift.Context(int(os.environ.get("LOCAL_RANK", "0")))
         fns = {"match": lambda: match_bench(ctx, torch, n_pairs=args.match_pairs, reps=args.steps),
                "catalog": lambda: catalog_bench(ctx, torch), "learned_ransac": lambda: ransac_bench(ctx, torch),
-               "catalog_search": lambda: catalog_search_bench(ctx, torch),
+               "catalog_search": lambda: catalog_search_bench(ctx, torch), "warp": lambda: warp_bench(ctx, torch),
                "uneven_batch": lambda: uneven_bench(ctx, torch)}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)
         ctx.close()

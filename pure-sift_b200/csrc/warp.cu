@@ -11,9 +11,10 @@
 // built with -fmad=false, so no product is fused into an add); floor / round
 // are exact; `as u8` saturates as Rust's cast does.  The canvas geometry
 // (inverse, projected corners in f32, bounds) is computed on the host with the
-// same expressions.  Each thread reads four RGBA8 texels of each image (32-bit
-// loads, neighbouring threads share rows through L1/L2) and writes one 32-bit
-// canvas pixel: bound by HBM for the canvas write plus the source reads.
+// same expressions.  Each thread reads one target texel and four query texels
+// (32-bit loads, neighbouring threads share rows through L1/L2) and writes one
+// 32-bit canvas pixel.  The f64 arithmetic (the query's projection and bilinear
+// weights, three IEEE divisions), not HBM, bounds the kernel.
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -78,7 +79,20 @@ __global__ void __launch_bounds__(256) warp_stitch_kernel(WarpImages im, WarpGeo
   if (ox >= g.width || oy >= g.height) return;
   const double tx = (double)ox + g.ox0, ty = (double)oy + g.oy0;
   double tc[4], qc[4], tw = 0.0, qw = 0.0;
-  const bool has_t = sample_rgba(im.t, im.th, im.tw, im.t_stride, tx, ty, tc, tw);
+  // The canvas origin is integral, so the target is sampled at whole pixels:
+  // sample_bilinear_rgba's weights are (1, 0, 0, 0) there and its sum is the
+  // texel itself (the zero-weight terms add +0), its feather weight
+  // ((min edge distance) + 1) / 32 clamped.
+  const bool has_t = tx >= 0.0 && ty >= 0.0 && tx <= (double)im.tw - 1.0 && ty <= (double)im.th - 1.0;
+  if (has_t) {
+    const int ix = (int)tx, iy = (int)ty;
+    const uint32_t p = __ldg(reinterpret_cast<const uint32_t*>(im.t + (long long)iy * im.t_stride) + ix);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) tc[c] = (double)((p >> (8 * c)) & 255u);
+    const double dist_edge = fmin(fmin(fmin(tx, ((double)im.tw - 1.0) - tx), ty), ((double)im.th - 1.0) - ty);
+    const double f = (dist_edge + 1.0) / 32.0;
+    tw = f < 0.02 ? 0.02 : (f > 1.0 ? 1.0 : f);
+  }
   bool has_q = false;
   const double w = g.hinv[6] * tx + g.hinv[7] * ty + g.hinv[8];
   if (!(fabs(w) < 1e-7)) {
