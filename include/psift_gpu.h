@@ -279,6 +279,35 @@ typedef struct psift_ransac_job {
 psift_status psift_ransac_batch_dev(psift_ctx* ctx, const psift_ransac_job* jobs, uint32_t n,
                                     const psift_ransac_options* opt, int32_t homography);
 
+/* Fundamental matrix.  FundamentalRansacOptions (src/geometry.rs:107-143). */
+typedef struct psift_fundamental_options {
+  double sampson_threshold; /* default 1.5 (px, Sampson distance; at least 0.25 is used) */
+  uint32_t max_iters;       /* default 2000 (at least 64 are allowed) */
+  double confidence;        /* default 0.999 */
+  uint64_t seed;            /* default 0xF00DCAFE12345678 */
+} psift_fundamental_options;
+void psift_fundamental_options_default(psift_fundamental_options* opt);
+/* estimate_fundamental_ransac_with_options (src/geometry.rs:868-1016): normalised
+ * 8-point LO-RANSAC with Sampson scoring (the 7-point solver for exactly 7 matches).
+ * f9 row-major f64 (x2^T F x1 = 0 with x1 the query point), has_f = 0 for None;
+ * inlier_mask[i] = 1 for the returned inliers; iterations (optional) the loop count. */
+psift_status psift_fundamental_estimate(psift_ctx* ctx, const psift_match* matches, uint32_t n,
+                                        const psift_fundamental_options* opt, uint8_t* inlier_mask,
+                                        double* f9, int32_t* has_f, uint32_t* inlier_count,
+                                        uint32_t* iterations);
+/* Device-resident batch, one CTA per match set.  Asynchronous. */
+typedef struct psift_fundamental_job {
+  const psift_match* matches;
+  uint32_t n;
+  uint8_t* inlier_mask;
+  double* f9;
+  int32_t* has_f;
+  uint32_t* inlier_count;
+  uint32_t* iterations; /* optional */
+} psift_fundamental_job;
+psift_status psift_fundamental_batch_dev(psift_ctx* ctx, const psift_fundamental_job* jobs, uint32_t n,
+                                         const psift_fundamental_options* opt);
+
 /* ---------------------------------------------------------------- learned sampler */
 /* A small MLP (8 -> 64 -> 64 -> 1, ReLU, ReLU, sigmoid; bf16 operands, f32
  * accumulation, f32 master weights) scoring each putative match's inlier

@@ -112,6 +112,16 @@ def lib():
             L.oracle_warp_and_stitch.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_int,
                                                  C.c_int, C.c_size_t, _fp, C.c_void_p, _ip, _ip, C.c_void_p]
             L.oracle_warp_and_stitch.restype = C.c_int
+            L.oracle_fundamental_ransac.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double,
+                                                    C.c_uint64, _u8p, C.POINTER(C.c_double), _ip, _ip]
+            L.oracle_fundamental_ransac.restype = C.c_int
+            L.oracle_fit_fundamental_8point.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+            L.oracle_fit_fundamental_8point.restype = C.c_int
+            L.oracle_fit_fundamental_7point.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+            L.oracle_fit_fundamental_7point.restype = C.c_int
+            L.oracle_sampson_distance_sq.argtypes = [C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double,
+                                                     C.c_double]
+            L.oracle_sampson_distance_sq.restype = C.c_double
             L.oracle_splitmix64_next.argtypes = [_u64p]
             L.oracle_splitmix64_next.restype = C.c_uint64
             _lib = L
@@ -357,3 +367,41 @@ def warp_and_stitch(query, target, h9):
                                  t.shape[0], t.shape[1], t.shape[1] * 4, _p(h, _fp), canvas.ctypes.data,
                                  C.byref(w), C.byref(hh), origin.ctypes.data)
     return canvas, (float(origin[0]), float(origin[1]))
+
+
+DEFAULT_FUNDAMENTAL_SEED = 0xF00DCAFE12345678
+
+
+def _as_oracle_matches(matches) -> np.ndarray:
+    m = np.ascontiguousarray(matches)
+    return m if m.dtype == MATCH_DTYPE else m.view(MATCH_DTYPE)
+
+
+def fundamental_ransac(matches, sampson_threshold=1.5, max_iters=2000, confidence=0.999,
+                       seed=DEFAULT_FUNDAMENTAL_SEED):
+    """estimate_fundamental_ransac_with_options (src/geometry.rs:868-1016):
+    (inlier mask, F (3, 3) f64 or None, iterations)."""
+    m = _as_oracle_matches(matches)
+    n = len(m)
+    mask = np.zeros(max(n, 1), np.uint8)
+    f9 = np.zeros(9, np.float64)
+    has, iters = C.c_int(), C.c_int()
+    lib().oracle_fundamental_ransac(m.ctypes.data, n, sampson_threshold, max_iters, confidence,
+                                    seed & 0xFFFFFFFFFFFFFFFF, _p(mask, _u8p), f9.ctypes.data_as(C.POINTER(C.c_double)),
+                                    C.byref(has), C.byref(iters))
+    return mask[:n].astype(bool), (f9.reshape(3, 3) if has.value else None), iters.value
+
+
+def fit_fundamental_8point(matches):
+    m = _as_oracle_matches(matches)
+    f9 = np.zeros(9, np.float64)
+    ok = lib().oracle_fit_fundamental_8point(m.ctypes.data, len(m), f9.ctypes.data_as(C.POINTER(C.c_double)))
+    return f9.reshape(3, 3) if ok else None
+
+
+def fit_fundamental_7point(matches):
+    """fit_fundamental_7point (src/geometry.rs:727-806) of the first 7 matches: list of F."""
+    m = _as_oracle_matches(matches)[:7]
+    out = np.zeros(36, np.float64)
+    k = lib().oracle_fit_fundamental_7point(m.ctypes.data, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return [out[9 * i:9 * i + 9].reshape(3, 3).copy() for i in range(k)]

@@ -1259,6 +1259,477 @@ inline bool has_zero_byte128(uint64_t x0, uint64_t x1) {
 
 }  // namespace
 
+namespace {
+
+// ------------------------------------------------- fundamental matrix (src/geometry.rs)
+struct M3 {
+  double v[3][3];
+};
+static M3 f_mul(const M3& a, const M3& b) {  // mul_mat3 (:145-154)
+  M3 o;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) o.v[r][c] = a.v[r][0] * b.v[0][c] + a.v[r][1] * b.v[1][c] + a.v[r][2] * b.v[2][c];
+  return o;
+}
+static M3 f_tr(const M3& m) {  // transpose_3x3 (:156-163)
+  M3 o;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) o.v[r][c] = m.v[c][r];
+  return o;
+}
+static double f_det(const M3& m) {  // det_3x3 (:165-170)
+  return m.v[0][0] * (m.v[1][1] * m.v[2][2] - m.v[1][2] * m.v[2][1]) -
+         m.v[0][1] * (m.v[1][0] * m.v[2][2] - m.v[1][2] * m.v[2][0]) +
+         m.v[0][2] * (m.v[1][0] * m.v[2][1] - m.v[1][1] * m.v[2][0]);
+}
+static bool f_norm_frob(M3& m) {  // normalize_frobenius (:172-185)
+  double s = 0.0;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) s += m.v[r][c] * m.v[r][c];
+  if (!std::isfinite(s) || s < 1e-24) return false;
+  const double inv = 1.0 / std::sqrt(s);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) m.v[r][c] *= inv;
+  return true;
+}
+static double f_dot(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static void f_cross(const double a[3], const double b[3], double o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+static bool f_normalize(const double v[3], double o[3]) {  // normalize_vec3 (:201-207)
+  const double n = std::sqrt(f_dot(v, v));
+  if (!std::isfinite(n) || n < 1e-12) return false;
+  o[0] = v[0] / n;
+  o[1] = v[1] / n;
+  o[2] = v[2] / n;
+  return true;
+}
+
+// One rotation step of the reference's classical Jacobi on an N x N symmetric
+// matrix (largest off-diagonal pivot, first in row-major order on ties).
+// Returns 1 to continue, 0 converged, -1 non-finite.
+template <int N>
+static int f_jacobi_step(double a[N][N], double v[N][N], double tol) {
+  int p = 0, q = 1;
+  double max_off = 0.0;
+  for (int i = 0; i < N; ++i)
+    for (int j = i + 1; j < N; ++j)
+      if (std::fabs(a[i][j]) > max_off) {
+        max_off = std::fabs(a[i][j]);
+        p = i;
+        q = j;
+      }
+  if (!std::isfinite(max_off)) return -1;
+  if (max_off < tol) return 0;
+  const double app = a[p][p], aqq = a[q][q], apq = a[p][q];
+  const double tau = (aqq - app) / (2.0 * apq);
+  const double t = tau >= 0.0 ? 1.0 / (tau + std::sqrt(1.0 + tau * tau)) : -1.0 / (-tau + std::sqrt(1.0 + tau * tau));
+  const double c = 1.0 / std::sqrt(1.0 + t * t);
+  const double s = t * c;
+  a[p][p] = app - t * apq;
+  a[q][q] = aqq + t * apq;
+  a[p][q] = 0.0;
+  a[q][p] = 0.0;
+  for (int r = 0; r < N; ++r) {
+    if (r != p && r != q) {
+      const double arp = a[r][p], arq = a[r][q];
+      const double nrp = c * arp - s * arq, nrq = s * arp + c * arq;
+      a[r][p] = nrp;
+      a[p][r] = nrp;
+      a[r][q] = nrq;
+      a[q][r] = nrq;
+    }
+  }
+  for (int r = 0; r < N; ++r) {
+    const double vrp = v[r][p], vrq = v[r][q];
+    v[r][p] = c * vrp - s * vrq;
+    v[r][q] = s * vrp + c * vrq;
+  }
+  return 1;
+}
+
+// jacobi_symmetric_eigen_9x9 (:209-295): eigenvectors as columns, ascending.
+static bool f_eigen9(double a[9][9], double vecs[9][9]) {
+  double v[9][9] = {};
+  for (int i = 0; i < 9; ++i) v[i][i] = 1.0;
+  for (int it = 0; it < 500; ++it) {
+    const int r = f_jacobi_step<9>(a, v, 1e-13);
+    if (r < 0) return false;
+    if (r == 0) break;
+  }
+  int order[9] = {0, 1, 2, 3, 4, 5, 6, 7, 8};
+  std::stable_sort(order, order + 9, [&](int i, int j) { return a[i][i] < a[j][j]; });
+  for (int dc = 0; dc < 9; ++dc)
+    for (int r = 0; r < 9; ++r) {
+      const double val = v[r][order[dc]];
+      if (!std::isfinite(val)) return false;
+      vecs[r][dc] = val;
+    }
+  return true;
+}
+
+// jacobi_symmetric_eigen_3x3 (:297-372): descending.
+static bool f_eigen3(double a[3][3], double vals[3], double vecs[3][3]) {
+  double v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int it = 0; it < 100; ++it) {
+    const int r = f_jacobi_step<3>(a, v, 1e-14);
+    if (r < 0) return false;
+    if (r == 0) break;
+  }
+  int order[3] = {0, 1, 2};
+  std::stable_sort(order, order + 3, [&](int i, int j) { return a[j][j] < a[i][i]; });
+  for (int dc = 0; dc < 3; ++dc) {
+    vals[dc] = a[order[dc]][order[dc]];
+    for (int r = 0; r < 3; ++r) vecs[r][dc] = v[r][order[dc]];
+  }
+  return true;
+}
+
+// svd_3x3 (:463-531) + rank2_project_f (:533-545).
+static bool f_rank2(M3& f) {
+  const M3 m = f;
+  M3 mtm = f_mul(f_tr(m), m);
+  double vals[3], vm[3][3];
+  if (!f_eigen3(mtm.v, vals, vm)) return false;
+  double s[3];
+  for (int i = 0; i < 3; ++i) s[i] = std::sqrt(std::fmax(vals[i], 0.0));
+  auto mul_mv = [&](const double x[3], double o[3]) {
+    for (int r = 0; r < 3; ++r) o[r] = m.v[r][0] * x[0] + m.v[r][1] * x[1] + m.v[r][2] * x[2];
+  };
+  const double v0[3] = {vm[0][0], vm[1][0], vm[2][0]}, v1[3] = {vm[0][1], vm[1][1], vm[2][1]},
+               v2[3] = {vm[0][2], vm[1][2], vm[2][2]};
+  double u0[3] = {1.0, 0.0, 0.0}, u1[3], u2[3], t[3];
+  if (s[0] > 1e-12) {
+    mul_mv(v0, t);
+    if (!f_normalize(t, u0)) u0[0] = 1.0, u0[1] = 0.0, u0[2] = 0.0;
+  }
+  auto fallback = [&](double o[3]) {
+    const double basis[3] = {std::fabs(u0[0]) < 0.9 ? 1.0 : 0.0, std::fabs(u0[0]) < 0.9 ? 0.0 : 1.0, 0.0};
+    double c[3];
+    f_cross(u0, basis, c);
+    if (!f_normalize(c, o)) o[0] = 0.0, o[1] = 1.0, o[2] = 0.0;
+  };
+  if (s[1] > 1e-12) {
+    double raw[3];
+    mul_mv(v1, raw);
+    const double proj = f_dot(raw, u0);
+    const double orth[3] = {raw[0] - proj * u0[0], raw[1] - proj * u0[1], raw[2] - proj * u0[2]};
+    if (!f_normalize(orth, u1)) fallback(u1);
+  } else {
+    fallback(u1);
+  }
+  f_cross(u0, u1, t);
+  if (!f_normalize(t, u2)) return false;
+  if (s[2] > 1e-12) {
+    double mv2[3];
+    mul_mv(v2, mv2);
+    if (f_dot(u2, mv2) < 0.0) u2[0] = -u2[0], u2[1] = -u2[1], u2[2] = -u2[2];
+  }
+  M3 u, d = {}, vt;
+  for (int r = 0; r < 3; ++r) u.v[r][0] = u0[r], u.v[r][1] = u1[r], u.v[r][2] = u2[r];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) vt.v[r][c] = vm[c][r];
+  d.v[0][0] = s[0];
+  d.v[1][1] = s[1];
+  f = f_mul(u, f_mul(d, vt));
+  return f_norm_frob(f);
+}
+
+// normalize_points_2d (:547-583).
+static bool f_norm_pts(const std::vector<double>& x, const std::vector<double>& y, std::vector<double>& nx,
+                       std::vector<double>& ny, M3& t) {
+  const size_t n = x.size();
+  if (n == 0) return false;
+  const double inv_n = 1.0 / (double)n;
+  double cx = 0.0, cy = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    if (!std::isfinite(x[i]) || !std::isfinite(y[i])) return false;
+    cx += x[i];
+    cy += y[i];
+  }
+  cx *= inv_n;
+  cy *= inv_n;
+  double md = 0.0;
+  for (size_t i = 0; i < n; ++i) md += std::hypot(x[i] - cx, y[i] - cy);
+  md *= inv_n;
+  if (!std::isfinite(md) || md < 1e-9) return false;
+  const double scale = 1.41421356237309504880 / md;
+  nx.resize(n);
+  ny.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    nx[i] = (x[i] - cx) * scale;
+    ny[i] = (y[i] - cy) * scale;
+  }
+  t = M3{{{scale, 0.0, -scale * cx}, {0.0, scale, -scale * cy}, {0.0, 0.0, 1.0}}};
+  return true;
+}
+
+// assemble_fundamental_ata (:586-604) -> jacobi -> the two smallest eigenvectors.
+static bool f_null2(const std::vector<oracle_match>& s, M3& tq, M3& tt, M3& f1, M3& f2) {
+  std::vector<double> qx, qy, tx, ty, nqx, nqy, ntx, nty;
+  for (const auto& m : s) {
+    qx.push_back((double)m.qx);
+    qy.push_back((double)m.qy);
+    tx.push_back((double)m.tx);
+    ty.push_back((double)m.ty);
+  }
+  if (!f_norm_pts(qx, qy, nqx, nqy, tq) || !f_norm_pts(tx, ty, ntx, nty, tt)) return false;
+  double ata[9][9] = {};
+  for (size_t k = 0; k < s.size(); ++k) {
+    const double x1 = nqx[k], y1 = nqy[k], x2 = ntx[k], y2 = nty[k];
+    const double r[9] = {x2 * x1, x2 * y1, x2, y2 * x1, y2 * y1, y2, x1, y1, 1.0};
+    for (int i = 0; i < 9; ++i)
+      for (int j = i; j < 9; ++j) ata[i][j] += r[i] * r[j];
+  }
+  for (int i = 0; i < 9; ++i)
+    for (int j = 0; j < i; ++j) ata[i][j] = ata[j][i];
+  double vecs[9][9];
+  if (!f_eigen9(ata, vecs)) return false;
+  for (int k = 0; k < 9; ++k) {
+    f1.v[k / 3][k % 3] = vecs[k][0];
+    f2.v[k / 3][k % 3] = vecs[k][1];
+  }
+  return true;
+}
+
+// fit_fundamental_8point (:638-665).
+static bool f_fit8(const std::vector<oracle_match>& s, M3& f) {
+  if (s.size() < 8) return false;
+  M3 tq, tt, f1, f2;
+  if (!f_null2(s, tq, tt, f1, f2)) return false;
+  if (!f_rank2(f1)) return false;
+  f = f_mul(f_tr(tt), f_mul(f1, tq));
+  return f_norm_frob(f);
+}
+
+// solve_cubic_real (:667-725).
+static std::vector<double> f_cubic(double c3, double c2, double c1, double c0) {
+  std::vector<double> roots;
+  if (std::fabs(c3) < 1e-12) {
+    if (std::fabs(c2) < 1e-12) {
+      if (std::fabs(c1) < 1e-12) return roots;
+      roots.push_back(-c0 / c1);
+      return roots;
+    }
+    const double disc = c1 * c1 - 4.0 * c2 * c0;
+    if (disc < 0.0) return roots;
+    const double sq = std::sqrt(disc);
+    roots.push_back((-c1 + sq) / (2.0 * c2));
+    roots.push_back((-c1 - sq) / (2.0 * c2));
+    return roots;
+  }
+  const double a = c2 / c3, b = c1 / c3, c = c0 / c3;
+  const double a3 = a / 3.0;
+  const double p = b - a * a3;
+  const double q = (2.0 * a * a * a) / 27.0 - (a * b) / 3.0 + c;
+  const double disc = (q * 0.5) * (q * 0.5) + powi_d(p / 3.0, 3);
+  if (disc > 1e-14) {
+    const double sq = std::sqrt(disc);
+    roots.push_back(std::cbrt(-0.5 * q + sq) + std::cbrt(-0.5 * q - sq) - a3);
+  } else if (disc >= -1e-14) {
+    const double u = std::cbrt(-0.5 * q);
+    roots.push_back(2.0 * u - a3);
+    roots.push_back(-u - a3);
+  } else {
+    const double r = std::sqrt(-p / 3.0);
+    double cp = (-0.5 * q) / (r * r * r);
+    cp = cp < -1.0 ? -1.0 : (cp > 1.0 ? 1.0 : cp);
+    const double phi = std::acos(cp);
+    const double two_r = 2.0 * r;
+    const double pi = 3.14159265358979323846;
+    roots.push_back(two_r * std::cos(phi / 3.0) - a3);
+    roots.push_back(two_r * std::cos((phi + 2.0 * pi) / 3.0) - a3);
+    roots.push_back(two_r * std::cos((phi + 4.0 * pi) / 3.0) - a3);
+  }
+  for (double& t : roots)
+    for (int k = 0; k < 3; ++k) {
+      const double fv = ((c3 * t + c2) * t + c1) * t + c0;
+      const double df = (3.0 * c3 * t + 2.0 * c2) * t + c1;
+      if (std::fabs(df) > 1e-14) t -= fv / df;
+    }
+  return roots;
+}
+
+// fit_fundamental_7point (:727-806).
+static std::vector<M3> f_fit7(const std::vector<oracle_match>& s) {
+  std::vector<M3> out;
+  M3 tq, tt, f1, f2;
+  if (!f_null2(s, tq, tt, f1, f2)) return out;
+  M3 b;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) b.v[r][c] = f1.v[r][c] - f2.v[r][c];
+  auto eval = [&](double t) {
+    M3 m;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) m.v[r][c] = f2.v[r][c] + t * b.v[r][c];
+    return m;
+  };
+  const double p0 = f_det(f2), p1 = f_det(eval(1.0)), pm1 = f_det(eval(-1.0)), p2 = f_det(eval(2.0));
+  const double c0 = p0;
+  const double c2 = 0.5 * (p1 + pm1) - c0;
+  const double s1 = 0.5 * (p1 - pm1);
+  const double s2 = p2 - c0 - 4.0 * c2;
+  const double c3 = (s2 - 2.0 * s1) / 6.0;
+  const double c1 = s1 - c3;
+  const M3 ttt = f_tr(tt);
+  for (double t : f_cubic(c3, c2, c1, c0)) {
+    if (!std::isfinite(t)) continue;
+    M3 f = f_mul(ttt, f_mul(eval(t), tq));
+    if (f_norm_frob(f)) out.push_back(f);
+  }
+  if (std::fabs(c3) < 1e-12 && std::fabs(f_det(b)) < 1e-10) {
+    M3 f = f_mul(ttt, f_mul(b, tq));
+    if (f_norm_frob(f)) out.push_back(f);
+  }
+  return out;
+}
+
+// sampson_distance_sq (:617-636).
+static double f_sampson(const M3& f, double x1, double y1, double x2, double y2) {
+  const auto& m = f.v;
+  const double a0 = m[0][0] * x1 + m[0][1] * y1 + m[0][2];
+  const double a1 = m[1][0] * x1 + m[1][1] * y1 + m[1][2];
+  const double a2 = m[2][0] * x1 + m[2][1] * y1 + m[2][2];
+  const double b0 = m[0][0] * x2 + m[1][0] * y2 + m[2][0];
+  const double b1 = m[0][1] * x2 + m[1][1] * y2 + m[2][1];
+  const double e = x2 * a0 + y2 * a1 + a2;
+  const double den = a0 * a0 + a1 * a1 + b0 * b0 + b1 * b1;
+  if (den < 1e-18 || !std::isfinite(den)) return std::numeric_limits<double>::infinity();
+  return (e * e) / den;
+}
+static double f_sampson_m(const M3& f, const oracle_match& m) {
+  return f_sampson(f, (double)m.qx, (double)m.qy, (double)m.tx, (double)m.ty);
+}
+
+// evaluate_fundamental_hypothesis (:808-829).
+static void f_eval(const oracle_match* m, int n, const M3& f, double tsq, int& count, double& err) {
+  count = 0;
+  err = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double d2 = f_sampson_m(f, m[i]);
+    if (d2 <= tsq) {
+      ++count;
+      err += d2;
+    } else {
+      err += tsq;
+    }
+  }
+}
+
+// adaptive_epipolar_iters (:831-855).
+static int f_adaptive(int best, int total, int ss, double conf, int min_it, int max_it) {
+  if (total <= ss || best == 0) return max_it;
+  const double w = (double)best / (double)total;
+  if (w >= 0.9999) return min_it;
+  const double pg = powi_d(w, ss);
+  if (pg <= 1e-12) return max_it;
+  const double den = std::log(std::fmax(1.0 - pg, 1e-15));
+  const double c = conf < 0.5 ? 0.5 : (conf > 0.999999 ? 0.999999 : conf);
+  const double num = std::log(1.0 - c);
+  const double est = std::ceil(num / den);
+  const unsigned long long e = d2u_sat(est);
+  return (int)std::min<unsigned long long>(std::max<unsigned long long>(e, (unsigned long long)min_it),
+                                           (unsigned long long)max_it);
+}
+
+// estimate_fundamental_ransac_with_options (:868-1016).
+static int f_ransac(const oracle_match* m, int n, double sampson_thr, int max_iters_opt, double conf, uint64_t seed,
+                    uint8_t* mask, M3& out_f, bool& has_f, int* iters_out) {
+  has_f = false;
+  for (int i = 0; i < n; ++i) mask[i] = 0;
+  if (iters_out) *iters_out = 0;
+  if (n < 7) return 0;
+  const double thr = std::fmax(sampson_thr, 0.25);
+  const double tsq = thr * thr;
+  M3 best_f{};
+  bool have = false;
+  int best_count = 0;
+  double best_err = std::numeric_limits<double>::infinity();
+  if (n == 7) {
+    std::vector<oracle_match> s(m, m + 7);
+    for (const M3& c : f_fit7(s)) {
+      int cnt;
+      double err;
+      f_eval(m, n, c, tsq, cnt, err);
+      if (cnt > best_count || (cnt == best_count && err < best_err)) {
+        best_count = cnt;
+        best_err = err;
+        best_f = c;
+        have = true;
+      }
+    }
+  } else {
+    const std::vector<double> cdf = ratio_cdf(m, n);
+    uint64_t rng = seed;
+    const int hard_cap = std::max(max_iters_opt, 64);
+    const int min_iters = std::min(64, hard_cap);
+    int max_iters = hard_cap;
+    int iter = 0;
+    while (iter < max_iters) {
+      ++iter;
+      size_t idx[8];
+      int chosen = 0, attempts = 0;
+      while (chosen < 8 && attempts < 32) {
+        ++attempts;
+        const size_t c = sample_weighted(cdf, rng);
+        bool dup = false;
+        for (int k = 0; k < chosen; ++k) dup = dup || idx[k] == c;
+        if (!dup) idx[chosen++] = c;
+      }
+      if (chosen < 8) continue;
+      std::vector<oracle_match> s;
+      for (int k = 0; k < 8; ++k) s.push_back(m[idx[k]]);
+      M3 f;
+      if (f_fit8(s, f)) {
+        int cnt;
+        double err;
+        f_eval(m, n, f, tsq, cnt, err);
+        if (cnt > best_count || (cnt == best_count && err < best_err)) {
+          best_count = cnt;
+          best_err = err;
+          best_f = f;
+          have = true;
+          max_iters = f_adaptive(best_count, n, 8, conf, min_iters, hard_cap);
+        }
+      }
+    }
+    if (iters_out) *iters_out = iter;
+    if (have) {
+      for (int r = 0; r < 2; ++r) {
+        std::vector<oracle_match> inl;
+        for (int i = 0; i < n; ++i)
+          if (f_sampson_m(best_f, m[i]) <= tsq) inl.push_back(m[i]);
+        if (inl.size() < 8) break;
+        M3 rf;
+        if (!f_fit8(inl, rf)) break;
+        int cnt;
+        double err;
+        f_eval(m, n, rf, tsq, cnt, err);
+        if (cnt > best_count || (cnt == best_count && err < best_err)) {
+          best_count = cnt;
+          best_err = err;
+          best_f = rf;
+        } else {
+          break;
+        }
+      }
+    }
+  }
+  if (!have) return 0;
+  int k = 0;
+  for (int i = 0; i < n; ++i) {
+    mask[i] = f_sampson_m(best_f, m[i]) <= tsq ? 1 : 0;
+    k += mask[i];
+  }
+  out_f = best_f;
+  has_f = true;
+  return k;
+}
+
+}  // namespace
+
 extern "C" {
 
 uint64_t oracle_splitmix64_next(uint64_t* state) { return splitmix64(*state); }
@@ -1716,6 +2187,38 @@ int oracle_warp_and_stitch(const uint8_t* q, int qh, int qw, size_t qs, const ui
     }
   }
   return 0;
+}
+
+int oracle_fundamental_ransac(const oracle_match* m, int n, double sampson_threshold, int max_iters,
+                              double confidence, uint64_t seed, uint8_t* mask, double* f9, int* has_f, int* iters) {
+  M3 f{};
+  bool has = false;
+  const int k = f_ransac(m, n, sampson_threshold, max_iters, confidence, seed, mask, f, has, iters);
+  *has_f = has ? 1 : 0;
+  for (int i = 0; i < 9; ++i) f9[i] = has ? f.v[i / 3][i % 3] : 0.0;
+  return k;
+}
+
+int oracle_fit_fundamental_7point(const oracle_match* m, double* f9s) {
+  std::vector<oracle_match> s(m, m + 7);
+  const std::vector<M3> c = f_fit7(s);
+  for (size_t k = 0; k < c.size(); ++k)
+    for (int i = 0; i < 9; ++i) f9s[9 * k + i] = c[k].v[i / 3][i % 3];
+  return (int)c.size();
+}
+
+int oracle_fit_fundamental_8point(const oracle_match* m, int n, double* f9) {
+  std::vector<oracle_match> s(m, m + n);
+  M3 f;
+  if (!f_fit8(s, f)) return 0;
+  for (int i = 0; i < 9; ++i) f9[i] = f.v[i / 3][i % 3];
+  return 1;
+}
+
+double oracle_sampson_distance_sq(const double* f9, double x1, double y1, double x2, double y2) {
+  M3 f;
+  for (int i = 0; i < 9; ++i) f.v[i / 3][i % 3] = f9[i];
+  return f_sampson(f, x1, y1, x2, y2);
 }
 
 }  // extern "C"

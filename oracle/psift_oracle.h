@@ -103,6 +103,18 @@ void oracle_l2_rerank(const float* qd, int nq, const float* cat_desc, const uint
 
 uint64_t oracle_splitmix64_next(uint64_t* state);
 
+/* estimate_fundamental_ransac_with_options (src/geometry.rs:868-1016): returns the
+ * inlier count; mask[i] = 1 for inliers; f9 row-major; iters (optional) the
+ * iterations run.  fit_fundamental_8point (:638-665) and sampson_distance_sq
+ * (:617-636) for direct checks. */
+int oracle_fundamental_ransac(const oracle_match* m, int n, double sampson_threshold, int max_iters,
+                              double confidence, uint64_t seed, uint8_t* mask, double* f9, int* has_f,
+                              int* iters);
+int oracle_fit_fundamental_8point(const oracle_match* m, int n, double* f9);
+/* fit_fundamental_7point (:727-806): up to 4 candidates (9 doubles each); returns their number. */
+int oracle_fit_fundamental_7point(const oracle_match* m, double* f9s);
+double oracle_sampson_distance_sq(const double* f9, double x1, double y1, double x2, double y2);
+
 /* warp_and_stitch (src/visualize.rs:379-483) on RGBA8 images (row strides in
  * bytes): the canvas geometry (out_w, out_h, origin[2]) and, when canvas is not
  * NULL, the out_w x out_h x 4 composite.  0 or a negative error code (-1 singular

@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include "psift_internal.cuh"
+#include "ransac_common.cuh"
 
 namespace psift {
 
@@ -90,26 +91,6 @@ struct RShared {
   uint32_t red_u[32];
   double red_d[32];
 };
-
-// ------------------------------------------------------------------ RNG / CDF
-__device__ __forceinline__ uint64_t sm64_draw(uint64_t seed, uint64_t t) {
-  uint64_t z = seed + (t + 1ull) * 0x9E3779B97F4A7C15ull;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-
-// sample_weighted_index: first index with cdf >= u, clamped to n-1.
-__device__ __forceinline__ int sample_at(const double* __restrict__ cdf, int n, uint64_t seed, uint64_t t) {
-  const double u = (double)(sm64_draw(seed, t) >> 11) * (1.0 / 9007199254740992.0);
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (cdf[mid] < u) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo < n - 1 ? lo : n - 1;
-}
 
 // build_ratio_weighted_cdf: weights in parallel, the running sum sequentially.
 __device__ void build_cdf(const RansacJob& J, RShared& S) {

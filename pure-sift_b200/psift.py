@@ -104,6 +104,16 @@ class CTracking(C.Structure):
                 ("median_dy", C.c_float), ("mean_scale_ratio", C.c_float), ("mean_rotation_deg", C.c_float)]
 
 
+class CFundamentalOptions(C.Structure):
+    _fields_ = [("sampson_threshold", C.c_double), ("max_iters", C.c_uint32), ("confidence", C.c_double),
+                ("seed", C.c_uint64)]
+
+
+class CFundamentalJob(C.Structure):
+    _fields_ = [("matches", C.c_void_p), ("n", C.c_uint32), ("inlier_mask", C.c_void_p), ("f9", C.c_void_p),
+                ("has_f", C.c_void_p), ("inlier_count", C.c_void_p), ("iterations", C.c_void_p)]
+
+
 class CCatalogParams(C.Structure):
     _fields_ = [("octaves", C.c_uint32), ("scales", C.c_uint32), ("threshold", C.c_float),
                 ("descriptor_kind", C.c_int32)]
@@ -196,6 +206,12 @@ _SIGS = {
     "psift_detect_and_compute_u8_noalloc_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
                                                           C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p,
                                                           C.c_void_p]),
+    "psift_fundamental_options_default": (None, [C.POINTER(CFundamentalOptions)]),
+    "psift_fundamental_estimate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CFundamentalOptions),
+                                             C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_uint32)]),
+    "psift_fundamental_batch_dev": (C.c_int, [C.c_void_p, C.POINTER(CFundamentalJob), C.c_uint32,
+                                              C.POINTER(CFundamentalOptions)]),
     "psift_warp_and_stitch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p,
                                         C.c_uint32, C.c_uint32, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t,
                                         C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p]),
@@ -776,6 +792,75 @@ def ransac_batch(match_sets, options: RansacOptions = RansacOptions(), homograph
     ctx.check(ctx.lib.psift_ransac_batch_dev(ctx.handle, jobs, len(match_sets), C.byref(c), int(homography)))
     ctx.synchronize()
     return ransac_results(dev, homography)
+
+
+@dataclass(frozen=True)
+class FundamentalRansacOptions:
+    """``FundamentalRansacOptions`` (src/geometry.rs:107-143)."""
+    sampson_threshold: float = 1.5
+    max_iters: int = 2000
+    confidence: float = 0.999
+    seed: int = 0xF00DCAFE12345678
+
+    def to_c(self) -> CFundamentalOptions:
+        return CFundamentalOptions(self.sampson_threshold, self.max_iters, self.confidence,
+                                   self.seed & 0xFFFFFFFFFFFFFFFF)
+
+
+def estimate_fundamental_ransac_with_options(matches, options: FundamentalRansacOptions = FundamentalRansacOptions(),
+                                             ctx: Context | None = None):
+    """``estimate_fundamental_ransac_with_options`` (src/geometry.rs:868-1016):
+    (inlier matches, F (3, 3) f64 or None)."""
+    ctx = ctx or default_context()
+    m = _as_matches(matches)
+    n = len(m)
+    mask = np.zeros(max(n, 1), np.uint8)
+    f9 = np.zeros(9, np.float64)
+    has, cnt, it = C.c_int32(), C.c_uint32(), C.c_uint32()
+    c = options.to_c()
+    ctx.check(ctx.lib.psift_fundamental_estimate(ctx.handle, m.ctypes.data, n, C.byref(c), mask.ctypes.data,
+                                                 f9.ctypes.data, C.byref(has), C.byref(cnt), C.byref(it)))
+    return m[mask[:n].astype(bool)], (f9.reshape(3, 3) if has.value else None)
+
+
+def estimate_fundamental_ransac(matches, sampson_threshold: float = 1.5, ctx: Context | None = None):
+    """``estimate_fundamental_ransac`` (src/geometry.rs:857-866)."""
+    return estimate_fundamental_ransac_with_options(matches, FundamentalRansacOptions(sampson_threshold), ctx)
+
+
+def fundamental_batch(match_sets, options: FundamentalRansacOptions = FundamentalRansacOptions(),
+                      ctx: Context | None = None, timing: bool = False):
+    """Many fundamental-matrix estimations in one launch (device-resident); returns
+    [(inlier mask, F or None, iterations)] and, with timing, the device ms."""
+    import torch
+    ctx = ctx or default_context()
+    sizes = [len(m) for m in match_sets]
+    allm = np.concatenate([_as_matches(m) for m in match_sets]) if sizes else np.zeros(0, MATCH_DTYPE)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    d_m = torch.from_numpy(allm.view(np.uint8)).cuda()
+    d_mask = torch.zeros(max(int(off[-1]), 1), dtype=torch.uint8, device="cuda")
+    d_f = torch.zeros((max(len(sizes), 1), 9), dtype=torch.float64, device="cuda")
+    d_i = torch.zeros((max(len(sizes), 1), 4), dtype=torch.int32, device="cuda")  # has, count, iters
+    jobs = (CFundamentalJob * max(len(sizes), 1))()
+    rec = allm.dtype.itemsize
+    for k, n in enumerate(sizes):
+        jobs[k] = CFundamentalJob(d_m.data_ptr() + int(off[k]) * rec, n, d_mask.data_ptr() + int(off[k]),
+                                  d_f.data_ptr() + 72 * k, d_i.data_ptr() + 16 * k, d_i.data_ptr() + 16 * k + 4,
+                                  d_i.data_ptr() + 16 * k + 8)
+    c = options.to_c()
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.check(ctx.lib.psift_fundamental_batch_dev(ctx.handle, jobs, len(sizes), C.byref(c)))
+    e1.record(stream)
+    ctx.synchronize()
+    masks = d_mask.cpu().numpy().astype(bool)
+    fs = d_f.cpu().numpy()
+    info = d_i.cpu().numpy()
+    out = [(masks[off[k]:off[k + 1]], fs[k].reshape(3, 3) if info[k, 0] else None, int(info[k, 2]))
+           for k in range(len(sizes))]
+    return (out, e0.elapsed_time(e1)) if timing else out
 
 
 def compute_sift_descriptors(img: np.ndarray, keypoints, kind: int = 0, ctx: Context | None = None) -> Features:

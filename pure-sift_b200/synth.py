@@ -259,6 +259,54 @@ def putative_matches(n: int, outlier_ratio: float, H: np.ndarray, width: int, he
     return rec, feats, inl
 
 
+def epipolar_matches(n: int, outlier_ratio: float, seed: int, width: int = 1920, height: int = 1080,
+                     noise_px: float = 0.5):
+    """Putative matches between two views of a 3-D scene (fundamental-matrix workload).
+
+    Camera 1 = K [I | 0], camera 2 = K [R | t] with K = (focal 1200 px, centred
+    principal point), R a rotation of up to 10 degrees about a random axis and t a
+    baseline of length 1 (mostly sideways).  Query points are uniform in image 1 at
+    depths U(4, 20); inliers are their projections in image 2 + N(0, noise_px);
+    outliers are uniform in image 2.  Ratios as `correspondences`.  Returns
+    (records with the match fields, is_inlier (n,) bool, F_true (3, 3))."""
+    rng = SplitMix64(seed)
+    u = rng.uniform(6)
+    axis = np.array([u[0] - 0.5, u[1] - 0.5, u[2] - 0.5])
+    axis /= max(np.linalg.norm(axis), 1e-9)
+    ang = np.deg2rad(10.0) * (2 * u[3] - 1)
+    Kx = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    R = np.eye(3) + np.sin(ang) * Kx + (1 - np.cos(ang)) * (Kx @ Kx)
+    t = np.array([1.0, 0.2 * (u[4] - 0.5), 0.2 * (u[5] - 0.5)])
+    t /= np.linalg.norm(t)
+    K = np.array([[1200.0, 0, width / 2], [0, 1200.0, height / 2], [0, 0, 1]])
+    q = rng.uniform(2 * n).reshape(n, 2) * np.array([width, height])
+    z = 4.0 + 16.0 * rng.uniform(n)
+    X = (np.linalg.inv(K) @ np.c_[q, np.ones(n)].T).T * z[:, None]
+    Y = (R @ X.T).T + t
+    p2 = (K @ Y.T).T
+    t_in = p2[:, :2] / p2[:, 2:3] + noise_px * rng.normal(2 * n).reshape(n, 2)
+    inl = rng.uniform(n) >= outlier_ratio
+    t_out = rng.uniform(2 * n).reshape(n, 2) * np.array([width, height])
+    tp = np.where(inl[:, None], t_in, t_out)
+    ru = rng.uniform(n)
+    ratio = np.where(inl, 0.2 + 0.6 * ru, 0.5 + 0.5 * ru)
+    rec = np.zeros(n, dtype=[("query_index", "<u4"), ("target_index", "<u4"), ("query_x", "<f4"),
+                             ("query_y", "<f4"), ("target_x", "<f4"), ("target_y", "<f4"), ("distance", "<f4"),
+                             ("ratio", "<f4"), ("displacement_x", "<f4"), ("displacement_y", "<f4")])
+    rec["query_index"] = np.arange(n)
+    rec["target_index"] = np.arange(n)
+    rec["query_x"], rec["query_y"] = q[:, 0], q[:, 1]
+    rec["target_x"], rec["target_y"] = tp[:, 0], tp[:, 1]
+    rec["distance"] = 0.3
+    rec["ratio"] = ratio
+    rec["displacement_x"] = rec["target_x"] - rec["query_x"]
+    rec["displacement_y"] = rec["target_y"] - rec["query_y"]
+    tx = np.array([[0, -t[2], t[1]], [t[2], 0, -t[0]], [-t[1], t[0], 0]])
+    Kinv = np.linalg.inv(K)
+    F = Kinv.T @ tx @ R @ Kinv
+    return rec, inl, F / np.linalg.norm(F)
+
+
 def c5_pair(k: int, seed0: int = 500):
     """Pair k of the learned-sampler workload: 1920x1080 geometry, random
     perspective homography (as for the 1080p pair), 2k-8k matches, outlier ratio U(0.1, 0.7)."""
