@@ -514,6 +514,36 @@ def warp_bench(ctx, torch, reps: int = 50):
     }
 
 
+def fundamental_bench(ctx, torch, n_sets: int = 256, cpu_sample: int = 8):
+    """Fundamental-matrix LO-RANSAC over 256 two-view match sets (1920x1080 views
+    of a 3-D scene, 2k-8k matches, outlier ratio U(0.1, 0.6)), one launch; the
+    CPU restatement (one thread per set, as the reference runs it) on the first
+    8 sets, scaled to the 256, and their inlier sets compared."""
+    import psift
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sets = []
+    for k in range(n_sets):
+        u = synth.SplitMix64(9000 + k).uniform(2)
+        sets.append(synth.epipolar_matches(int(2000 + 6000 * u[0]), 0.1 + 0.5 * u[1], seed=9100 + k)[0])
+    psift.fundamental_batch(sets[:4], ctx=ctx)  # warm-up
+    res, dev_ms = psift.fundamental_batch(sets, ctx=ctx, timing=True)
+    t0 = time.perf_counter()
+    ref = [O.fundamental_ransac(m) for m in sets[:cpu_sample]]
+    cpu_s = time.perf_counter() - t0
+    same = all(np.array_equal(r[0], g[0]) and r[2] == g[2] for r, g in zip(ref, res[:cpu_sample]))
+    n_matches = int(sum(len(m) for m in sets))
+    iters = [g[2] for g in res]
+    return {
+        "workload": f"{n_sets} two-view sets, 2k-8k matches ({n_matches} total), outliers U(0.1, 0.6), one launch",
+        "device_ms": dev_ms, "sets_per_s": n_sets / (dev_ms * 1e-3),
+        "mean_iterations": float(np.mean(iters)), "max_iterations": int(np.max(iters)),
+        "cpu_restatement_ms_per_set": cpu_s / cpu_sample * 1e3,
+        "cpu_restatement_ms_256_sets_one_thread": cpu_s / cpu_sample * n_sets * 1e3,
+        "identical_on_cpu_sample": same,
+    }
+
+
 def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int = 3):
     """Learned RANSAC proposal: 1024 synthetic 1080p pairs with known perspective
     homographies, 2k-8k putative matches each, outlier ratio U(0.1, 0.7).  The MLP
@@ -758,6 +788,7 @@ def run_ours(args):
         }
         for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench),
                         ("catalog_search", catalog_search_bench), ("warp", warp_bench),
+                        ("fundamental", fundamental_bench),
                         ("learned_ransac", ransac_bench)):
             if getattr(args, "no_" + key):
                 continue
@@ -797,12 +828,13 @@ def main():
     ap.add_argument("--only-device", action="store_true", help="time the device path only (profiling case)")
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
-    ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "warp", "learned_ransac",
-                                               "uneven_batch"],
+    ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "warp", "fundamental",
+                                               "learned_ransac", "uneven_batch"],
                     help="run one section alone (profiling case)")
     ap.add_argument("--no-catalog", action="store_true")
     ap.add_argument("--no-catalog-search", dest="no_catalog_search", action="store_true")
     ap.add_argument("--no-warp", dest="no_warp", action="store_true")
+    ap.add_argument("--no-fundamental", dest="no_fundamental", action="store_true")
     ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
     args = ap.parse_args()
@@ -818,6 +850,7 @@ def main():
         fns = {"match": lambda: match_bench(ctx, torch, n_pairs=args.match_pairs, reps=args.steps),
                "catalog": lambda: catalog_bench(ctx, torch), "learned_ransac": lambda: ransac_bench(ctx, torch),
                "catalog_search": lambda: catalog_search_bench(ctx, torch), "warp": lambda: warp_bench(ctx, torch),
+               "fundamental": lambda: fundamental_bench(ctx, torch),
                "uneven_batch": lambda: uneven_bench(ctx, torch)}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)
         ctx.close()

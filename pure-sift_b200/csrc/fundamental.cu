@@ -46,7 +46,7 @@ struct FundJob {
   uint64_t seed;
   double* cdf;    // n
   double* terms;  // n
-  int* list;      // n
+  double* pts;    // 4 per match: the ordered inlier list's coordinates, gathered
   uint8_t* mask;
   double* f9;
   int* has_f;
@@ -451,6 +451,23 @@ __device__ int block_sum(int v, FShared& S) {
   return t;
 }
 
+// Sequential sum of v[0..n) in order, the loads issued kSeqAhead at a time ahead
+// of the dependent adds (one thread).
+constexpr int kSeqAhead = 16;
+__device__ double seq_sum(const double* __restrict__ v, int n) {
+  double acc = 0.0;
+  int i = 0;
+  for (; i + kSeqAhead <= n; i += kSeqAhead) {
+    double w[kSeqAhead];
+#pragma unroll
+    for (int k = 0; k < kSeqAhead; ++k) w[k] = v[i + k];
+#pragma unroll
+    for (int k = 0; k < kSeqAhead; ++k) acc += w[k];
+  }
+  for (; i < n; ++i) acc += v[i];
+  return acc;
+}
+
 // evaluate_fundamental_hypothesis of f (shared): count (whole CTA) and the
 // truncated error sum in match order (terms in parallel, summed by thread 0).
 __device__ void evaluate(const FundJob& J, FShared& S, const double* f, int& count, double& err) {
@@ -462,17 +479,14 @@ __device__ void evaluate(const FundJob& J, FShared& S, const double* f, int& cou
     J.terms[i] = in ? d2 : J.tsq;
   }
   count = block_sum(c, S);  // its barriers also order the term stores before the sum
-  if (threadIdx.x == 0) {
-    double e = 0.0;
-    for (int i = 0; i < J.n; ++i) e += J.terms[i];
-    S.ev_err = e;
-  }
+  if (threadIdx.x == 0) S.ev_err = seq_sum(J.terms, J.n);
   __syncthreads();
   err = S.ev_err;
   __syncthreads();
 }
 
-// Ordered inlier list of S.best into J.list; returns its length (whole CTA).
+// Ordered inlier list of S.best, its coordinates gathered into J.pts; returns its
+// length (whole CTA).
 __device__ int collect(const FundJob& J, FShared& S) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int base = 0;
@@ -484,7 +498,12 @@ __device__ int collect(const FundJob& J, FShared& S) {
     __syncthreads();
     int off = base;
     for (int w = 0; w < warp; ++w) off += S.scan[w];
-    if (in) J.list[off + __popc(bal & ((1u << lane) - 1u))] = i;
+    if (in) {
+      const int pos = off + __popc(bal & ((1u << lane) - 1u));
+      const psift_match& a = J.m[i];
+      reinterpret_cast<double4*>(J.pts)[pos] =
+          make_double4((double)a.query_x, (double)a.query_y, (double)a.target_x, (double)a.target_y);
+    }
     int tot = 0;
     for (int w = 0; w < kFThreads / 32; ++w) tot += S.scan[w];
     base += tot;
@@ -493,31 +512,54 @@ __device__ int collect(const FundJob& J, FShared& S) {
   return base;
 }
 
-// fit_fundamental_8point over J.list[0..k) (k >= 8) into S.cand; S.fit_ok.
+// fit_fundamental_8point over the gathered inliers J.pts[0..k) (k >= 8) into
+// S.cand; S.fit_ok.  Every sum runs over the list in order, one thread each, with
+// the coordinates of kSeqAhead points loaded ahead of the dependent adds.
 __device__ void fit_list(const FundJob& J, FShared& S, int k) {
   const int t = threadIdx.x;
-  // normalisation sums, each sequential over the list in order
-  if (t < 4) {
+  const double4* P = reinterpret_cast<const double4*>(J.pts);
+  auto coord = [](const double4& p, int c) { return c == 0 ? p.x : c == 1 ? p.y : c == 2 ? p.z : p.w; };
+  if (t < 4) {  // normalisation sums: qx, qy, tx, ty
     double s = 0.0;
     bool fin = true;
-    for (int i = 0; i < k; ++i) {
-      const psift_match& a = J.m[J.list[i]];
-      const double v = t == 0 ? (double)a.query_x : t == 1 ? (double)a.query_y : t == 2 ? (double)a.target_x
-                                                                                        : (double)a.target_y;
-      fin = fin && isfinite(v);
-      s += v;
+    int i = 0;
+    for (; i + kSeqAhead <= k; i += kSeqAhead) {
+      double w[kSeqAhead];
+#pragma unroll
+      for (int q = 0; q < kSeqAhead; ++q) w[q] = coord(P[i + q], t);
+#pragma unroll
+      for (int q = 0; q < kSeqAhead; ++q) {
+        fin = fin && isfinite(w[q]);
+        s += w[q];
+      }
+    }
+    for (; i < k; ++i) {
+      const double w = coord(P[i], t);
+      fin = fin && isfinite(w);
+      s += w;
     }
     S.sums[t] = fin ? s : __longlong_as_double(0x7ff8000000000000ll);
   }
   __syncthreads();
   const double inv_n = 1.0 / (double)k;
   const double qcx = S.sums[0] * inv_n, qcy = S.sums[1] * inv_n, tcx = S.sums[2] * inv_n, tcy = S.sums[3] * inv_n;
-  if (t < 2) {
+  if (t < 2) {  // mean distances to the centroid: query, target
+    const double cx = t == 0 ? qcx : tcx, cy = t == 0 ? qcy : tcy;
     double md = 0.0;
-    for (int i = 0; i < k; ++i) {
-      const psift_match& a = J.m[J.list[i]];
-      md += t == 0 ? hypot((double)a.query_x - qcx, (double)a.query_y - qcy)
-                   : hypot((double)a.target_x - tcx, (double)a.target_y - tcy);
+    int i = 0;
+    for (; i + kSeqAhead <= k; i += kSeqAhead) {
+      double w[kSeqAhead];
+#pragma unroll
+      for (int q = 0; q < kSeqAhead; ++q) {
+        const double4 p = P[i + q];
+        w[q] = t == 0 ? hypot(p.x - cx, p.y - cy) : hypot(p.z - cx, p.w - cy);
+      }
+#pragma unroll
+      for (int q = 0; q < kSeqAhead; ++q) md += w[q];
+    }
+    for (; i < k; ++i) {
+      const double4 p = P[i];
+      md += t == 0 ? hypot(p.x - cx, p.y - cy) : hypot(p.z - cx, p.w - cy);
     }
     S.sums[4 + t] = md * inv_n;
   }
@@ -534,14 +576,21 @@ __device__ void fit_list(const FundJob& J, FShared& S, int k) {
       ++i;
     }
     const int j = i + rem;
-    double s = 0.0;
-    for (int p = 0; p < k; ++p) {
-      const psift_match& a = J.m[J.list[p]];
+    auto term = [&](const double4& p) {
       double r[9];
-      ata_row(((double)a.query_x - qcx) * qs, ((double)a.query_y - qcy) * qs, ((double)a.target_x - tcx) * ts,
-              ((double)a.target_y - tcy) * ts, r);
-      s += r[i] * r[j];
+      ata_row((p.x - qcx) * qs, (p.y - qcy) * qs, (p.z - tcx) * ts, (p.w - tcy) * ts, r);
+      return r[i] * r[j];
+    };
+    double s = 0.0;
+    int p0 = 0;
+    for (; p0 + kSeqAhead <= k; p0 += kSeqAhead) {
+      double w[kSeqAhead];
+#pragma unroll
+      for (int q = 0; q < kSeqAhead; ++q) w[q] = term(P[p0 + q]);
+#pragma unroll
+      for (int q = 0; q < kSeqAhead; ++q) s += w[q];
     }
+    for (; p0 < k; ++p0) s += term(P[p0]);
     S.ata[i][j] = s;
     S.ata[j][i] = s;
   }
@@ -649,7 +698,18 @@ __global__ void __launch_bounds__(kFThreads) fundamental_kernel(const FundJob* _
     __syncthreads();
     if (t == 0) {
       double acc = 0.0;
-      for (int i = 0; i < n; ++i) {
+      int i = 0;
+      for (; i + kSeqAhead <= n; i += kSeqAhead) {
+        double w[kSeqAhead];
+#pragma unroll
+        for (int q = 0; q < kSeqAhead; ++q) w[q] = J.cdf[i + q];
+#pragma unroll
+        for (int q = 0; q < kSeqAhead; ++q) {
+          acc += w[q];
+          J.cdf[i + q] = acc;
+        }
+      }
+      for (; i < n; ++i) {
         acc += J.cdf[i];
         J.cdf[i] = acc;
       }
@@ -839,7 +899,7 @@ psift_status validate_fundamental_options(psift_ctx* ctx, const psift_fundamenta
 psift_status run_fundamental(psift_ctx* ctx, const psift_fundamental_job* jobs, int n,
                              const psift_fundamental_options& o) {
   size_t bytes = sizeof(FundJob) * (size_t)n + 4096;
-  for (int i = 0; i < n; ++i) bytes += 20 * (size_t)jobs[i].n + 3 * 256;
+  for (int i = 0; i < n; ++i) bytes += 48 * (size_t)jobs[i].n + 3 * 256;
   psift_status st = arena_reserve(ctx, bytes);
   if (st != PSIFT_OK) return st;
   FundJob* d_jobs = (FundJob*)arena_alloc(ctx, sizeof(FundJob) * n);
@@ -858,13 +918,13 @@ psift_status run_fundamental(psift_ctx* ctx, const psift_fundamental_job* jobs, 
     F.seed = o.seed;
     F.cdf = (double*)arena_alloc(ctx, 8 * (size_t)J.n + 8);
     F.terms = (double*)arena_alloc(ctx, 8 * (size_t)J.n + 8);
-    F.list = (int*)arena_alloc(ctx, 4 * (size_t)J.n + 4);
+    F.pts = (double*)arena_alloc(ctx, 32 * (size_t)J.n + 32);
     F.mask = J.inlier_mask;
     F.f9 = J.f9;
     F.has_f = J.has_f;
     F.count = (int*)J.inlier_count;
     F.iters = (int*)J.iterations;
-    if (!F.list) return set_error(ctx, PSIFT_ERR_INTERNAL, "fundamental workspace carve overflow");
+    if (!F.pts) return set_error(ctx, PSIFT_ERR_INTERNAL, "fundamental workspace carve overflow");
   }
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_jobs, hj.data(), sizeof(FundJob) * n, cudaMemcpyHostToDevice, ctx->stream));
   StageScope sc(ctx, STAGE_RANSAC);
