@@ -15,7 +15,7 @@
 // The reference's loop is replayed exactly: its draws are resolved in parallel
 // (ransac_common.cuh), thread 0 walks them to form the same 8-index samples
 // (distinct indices, at most 32 attempts), 64 samples are fitted at a time (one
-// thread each, the reference's f64 operations in its order), each warp counts
+// quad of lanes each, the reference's f64 operations in its order), each warp counts
 // the inliers of 8 of them, and thread 0 takes every decision in order: count,
 // the tie-break on the truncated error sum (the reference's sequential sum over
 // the matches, evaluated only when a tie needs it), the adaptive iteration
@@ -135,15 +135,30 @@ __device__ bool normalize3(const double v[3], double o[3]) {
 // first in row-major order on ties): 1 continue, 0 converged, -1 non-finite.
 template <int N>
 __device__ int jacobi_step(double (&a)[N][N], double (&v)[N][N], double tol) {
+  // the N(N-1)/2 magnitudes are loaded together, then scanned in row-major order
+  constexpr int kOff = N * (N - 1) / 2;
+  double mag[kOff];
+  {
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = i + 1; j < N; ++j) mag[k++] = fabs(a[i][j]);
+  }
   int p = 0, q = 1;
   double max_off = 0.0;
-  for (int i = 0; i < N; ++i)
-    for (int j = i + 1; j < N; ++j)
-      if (fabs(a[i][j]) > max_off) {
-        max_off = fabs(a[i][j]);
-        p = i;
-        q = j;
-      }
+  {
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int j = i + 1; j < N; ++j, ++k)
+        if (mag[k] > max_off) {
+          max_off = mag[k];
+          p = i;
+          q = j;
+        }
+  }
   if (!isfinite(max_off)) return -1;
   if (max_off < tol) return 0;
   const double app = a[p][p], aqq = a[q][q], apq = a[p][q];
@@ -155,6 +170,7 @@ __device__ int jacobi_step(double (&a)[N][N], double (&v)[N][N], double tol) {
   a[q][q] = aqq + t * apq;
   a[p][q] = 0.0;
   a[q][p] = 0.0;
+#pragma unroll
   for (int r = 0; r < N; ++r) {
     if (r != p && r != q) {
       const double arp = a[r][p], arq = a[r][q];
@@ -165,6 +181,7 @@ __device__ int jacobi_step(double (&a)[N][N], double (&v)[N][N], double tol) {
       a[q][r] = nrq;
     }
   }
+#pragma unroll
   for (int r = 0; r < N; ++r) {
     const double vrp = v[r][p], vrq = v[r][q];
     v[r][p] = c * vrp - s * vrq;
@@ -174,7 +191,8 @@ __device__ int jacobi_step(double (&a)[N][N], double (&v)[N][N], double tol) {
 }
 
 // jacobi_symmetric_eigen_9x9: the eigenvectors of the two smallest eigenvalues
-// (ascending, stable order) as 3x3 matrices.
+// (ascending, stable order) as 3x3 matrices (one thread: the 7-point solver and
+// the LO refits).
 __device__ bool null2_of_ata(double (&a)[9][9], M3& f1, M3& f2) {
   double v[9][9];
   for (int i = 0; i < 9; ++i)
@@ -337,15 +355,158 @@ __device__ bool small_ata(const psift_match* __restrict__ m, const int* idx, int
   return true;
 }
 
-// Eigenvector -> rank 2 -> de-normalised, Frobenius-normalised F (fit_fundamental_8point tail).
-__device__ bool finish8(double (&ata)[9][9], const M3& tq, const M3& tt, double* out) {
-  M3 f1, f2;
-  if (!null2_of_ata(ata, f1, f2)) return false;
+// jacobi_symmetric_eigen_9x9's rotations on A (eigenvectors accumulated in V),
+// shared by a quad of lanes (see quad_fit8); false on a non-finite pivot.
+// A and V are complete and visible to the quad on entry and on return.
+__device__ bool quad_jacobi(double* A, double* V, int ql, unsigned qmask) {
+  // this lane's 9 pivot candidates: upper-triangle entries 9 ql .. 9 ql + 8 in row-major order
+  int ki[9], kj[9];
+  {
+    int i = 0, rem = 9 * ql;
+    while (rem >= 8 - i) {
+      rem -= 8 - i;
+      ++i;
+    }
+    int j = i + 1 + rem;
+#pragma unroll
+    for (int s = 0; s < 9; ++s) {
+      ki[s] = i;
+      kj[s] = j;
+      if (++j == 9) {
+        ++i;
+        j = i + 1;
+      }
+    }
+  }
+  bool finite = true;
+  for (int it = 0; it < 500; ++it) {
+    double mx = -1.0;
+    int mk = 99;
+#pragma unroll
+    for (int s = 0; s < 9; ++s) {
+      const double v = fabs(A[ki[s] * 9 + kj[s]]);
+      if (v > mx) {
+        mx = v;
+        mk = 9 * ql + s;
+      }
+    }
+#pragma unroll
+    for (int o = 1; o <= 2; o <<= 1) {
+      const double om = __shfl_xor_sync(qmask, mx, o);
+      const int ok = __shfl_xor_sync(qmask, mk, o);
+      if (om > mx || (om == mx && ok < mk)) {
+        mx = om;
+        mk = ok;
+      }
+    }
+    if (!isfinite(mx)) {
+      finite = false;
+      break;
+    }
+    if (mx < 1e-13) break;
+    int p = 0, rem = mk;
+    while (rem >= 8 - p) {
+      rem -= 8 - p;
+      ++p;
+    }
+    const int q = p + 1 + rem;
+    const double app = A[p * 9 + p], aqq = A[q * 9 + q], apq = A[p * 9 + q];
+    const double tau = (aqq - app) / (2.0 * apq);
+    const double t = tau >= 0.0 ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
+    const double c = 1.0 / sqrt(1.0 + t * t);
+    const double s = t * c;
+    __syncwarp(qmask);  // every pivot read precedes the writes
+    if (ql == 0) {
+      A[p * 9 + p] = app - t * apq;
+      A[q * 9 + q] = aqq + t * apq;
+      A[p * 9 + q] = 0.0;
+      A[q * 9 + p] = 0.0;
+    }
+    for (int r = ql; r < 9; r += 4) {
+      if (r != p && r != q) {
+        const double arp = A[r * 9 + p], arq = A[r * 9 + q];
+        const double nrp = c * arp - s * arq, nrq = s * arp + c * arq;
+        A[r * 9 + p] = nrp;
+        A[p * 9 + r] = nrp;
+        A[r * 9 + q] = nrq;
+        A[q * 9 + r] = nrq;
+      }
+      const double vrp = V[r * 9 + p], vrq = V[r * 9 + q];
+      V[r * 9 + p] = c * vrp - s * vrq;
+      V[r * 9 + q] = s * vrp + c * vrq;
+    }
+    __syncwarp(qmask);
+  }
+  return finite;
+}
+
+// The leader's tail of jacobi_symmetric_eigen_9x9 (stable ascending order,
+// finite eigenvectors) and of fit_fundamental_8point (rank 2, de-normalisation).
+__device__ bool finish_from_eigen(const double* A, const double* V, const M3& tq, const M3& tt, double* out) {
+  int order[9];
+  for (int i = 0; i < 9; ++i) order[i] = i;
+  for (int i = 1; i < 9; ++i) {
+    const int k = order[i];
+    int j = i - 1;
+    while (j >= 0 && A[k * 9 + k] < A[order[j] * 9 + order[j]]) {
+      order[j + 1] = order[j];
+      --j;
+    }
+    order[j + 1] = k;
+  }
+  for (int dc = 0; dc < 9; ++dc)
+    for (int r = 0; r < 9; ++r)
+      if (!isfinite(V[r * 9 + order[dc]])) return false;
+  M3 f1;
+  for (int k = 0; k < 9; ++k) f1.v[k / 3][k % 3] = V[k * 9 + order[0]];
   if (!rank2(f1)) return false;
   M3 f = m3_mul(m3_tr(tt), m3_mul(f1, tq));
   if (!norm_frob(f)) return false;
   for (int i = 0; i < 9; ++i) out[i] = f.v[i / 3][i % 3];
   return true;
+}
+
+// fit_fundamental_8point of one sample by a quad of lanes (ql = 0..3, converged,
+// qmask their lane mask); A and V (81 doubles each, shared memory) hold the
+// Jacobi matrix and eigenvectors.  Every lane computes the normalisation; the 45
+// A^T A entries and the rotations' row updates are split over the lanes; each
+// lane scans 9 of the 36 pivot candidates in row-major order and the quad keeps
+// the first largest, so every value and decision is the sequential solver's.
+// The result (out, return value) is the leader's (ql == 0).
+__device__ bool quad_fit8(const psift_match* __restrict__ m, const int* idx, double* A, double* V, int ql,
+                          unsigned qmask, double* out) {
+  double qx[8], qy[8], tx[8], ty[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const psift_match& a = m[idx[i]];
+    qx[i] = (double)a.query_x, qy[i] = (double)a.query_y, tx[i] = (double)a.target_x, ty[i] = (double)a.target_y;
+  }
+  double qcx, qcy, qs, tcx, tcy, ts;
+  if (!norm_pts(qx, qy, 8, qcx, qcy, qs) || !norm_pts(tx, ty, 8, tcx, tcy, ts)) return false;
+  for (int e = ql; e < 45; e += 4) {
+    int i = 0, rem = e;
+    while (rem >= 9 - i) {
+      rem -= 9 - i;
+      ++i;
+    }
+    const int j = i + rem;
+    double sum = 0.0;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      double r[9];
+      ata_row((qx[p] - qcx) * qs, (qy[p] - qcy) * qs, (tx[p] - tcx) * ts, (ty[p] - tcy) * ts, r);
+      sum += r[i] * r[j];
+    }
+    A[i * 9 + j] = sum;
+    A[j * 9 + i] = sum;
+  }
+  for (int r = ql; r < 9; r += 4)
+#pragma unroll
+    for (int c = 0; c < 9; ++c) V[r * 9 + c] = r == c ? 1.0 : 0.0;
+  __syncwarp(qmask);
+  const bool finite = quad_jacobi(A, V, ql, qmask);
+  if (ql != 0 || !finite) return false;
+  return finish_from_eigen(A, V, norm_T(qs, qcx, qcy), norm_T(ts, tcx, tcy), out);
 }
 
 __device__ __forceinline__ double sampson(const double* f, const psift_match& a) {
@@ -515,7 +676,7 @@ __device__ int collect(const FundJob& J, FShared& S) {
 // fit_fundamental_8point over the gathered inliers J.pts[0..k) (k >= 8) into
 // S.cand; S.fit_ok.  Every sum runs over the list in order, one thread each, with
 // the coordinates of kSeqAhead points loaded ahead of the dependent adds.
-__device__ void fit_list(const FundJob& J, FShared& S, int k) {
+__device__ void fit_list(const FundJob& J, FShared& S, double* jac, int k) {
   const int t = threadIdx.x;
   const double4* P = reinterpret_cast<const double4*>(J.pts);
   auto coord = [](const double4& p, int c) { return c == 0 ? p.x : c == 1 ? p.y : c == 2 ? p.z : p.w; };
@@ -576,10 +737,15 @@ __device__ void fit_list(const FundJob& J, FShared& S, int k) {
       ++i;
     }
     const int j = i + rem;
+    // row entry k of assemble_fundamental_ata is U[k / 3] * W[k % 3] with
+    // U = (x2, y2, 1), W = (x1, y1, 1) (the 1 factors are exact): r_i * r_j
+    // without a per-point array
+    const int ui = i / 3, wi = i % 3, uj = j / 3, wj = j % 3;
     auto term = [&](const double4& p) {
-      double r[9];
-      ata_row((p.x - qcx) * qs, (p.y - qcy) * qs, (p.z - tcx) * ts, (p.w - tcy) * ts, r);
-      return r[i] * r[j];
+      const double x1 = (p.x - qcx) * qs, y1 = (p.y - qcy) * qs, x2 = (p.z - tcx) * ts, y2 = (p.w - tcy) * ts;
+      const double u_i = ui == 0 ? x2 : (ui == 1 ? y2 : 1.0), w_i = wi == 0 ? x1 : (wi == 1 ? y1 : 1.0);
+      const double u_j = uj == 0 ? x2 : (uj == 1 ? y2 : 1.0), w_j = wj == 0 ? x1 : (wj == 1 ? y1 : 1.0);
+      return (u_i * w_i) * (u_j * w_j);
     };
     double s = 0.0;
     int p0 = 0;
@@ -595,15 +761,21 @@ __device__ void fit_list(const FundJob& J, FShared& S, int k) {
     S.ata[j][i] = s;
   }
   __syncthreads();
-  if (t == 0) {
+  if (t < 4) {  // the eigen-decomposition by the first quad, in the (now free) slot of sample 0
+    const unsigned qmask = 0xFu;
+    double* A = jac;
+    double* V = jac + 81;
     bool good = ok;
     if (good) {
-      double a[9][9];
-      for (int i = 0; i < 9; ++i)
-        for (int j = 0; j < 9; ++j) a[i][j] = S.ata[i][j];
-      good = finish8(a, norm_T(qs, qcx, qcy), norm_T(ts, tcx, tcy), S.cand);
+      for (int e = t; e < 81; e += 4) {
+        A[e] = S.ata[e / 9][e % 9];
+        V[e] = e / 9 == e % 9 ? 1.0 : 0.0;
+      }
+      __syncwarp(qmask);
+      const bool fin = quad_jacobi(A, V, t, qmask);
+      if (t == 0) good = fin && finish_from_eigen(A, V, norm_T(qs, qcx, qcy), norm_T(ts, tcx, tcy), S.cand);
     }
-    S.fit_ok = good ? 1 : 0;
+    if (t == 0) S.fit_ok = good ? 1 : 0;
   }
   __syncthreads();
 }
@@ -672,8 +844,11 @@ __device__ void seven_point(const FundJob& J, FShared& S) {
   }
 }
 
+constexpr size_t kJacSmem = sizeof(double) * 162 * kFB;  // A and V of every sample of a batch
+
 __global__ void __launch_bounds__(kFThreads) fundamental_kernel(const FundJob* __restrict__ jobs) {
   __shared__ FShared S;
+  extern __shared__ double jac[];
   const FundJob& J = jobs[blockIdx.x];
   const int n = J.n, t = threadIdx.x;
   if (t == 0) {
@@ -768,29 +943,45 @@ __global__ void __launch_bounds__(kFThreads) fundamental_kernel(const FundJob* _
         __syncthreads();
       }
       const int nb = S.nb;
-      // 2. fits, one thread per sample
-      if (t < nb) {
-        int ok = 0;
-        if (S.sok[t]) {
-          M3 tq, tt;
-          double ata[9][9];
-          if (small_ata(J.m, S.samp[t], 8, tq, tt, ata)) ok = finish8(ata, tq, tt, S.F[t]) ? 1 : 0;
+      // 2. fits, a quad of lanes per sample
+      {
+        const int h = t >> 2, ql = t & 3;
+        const unsigned qmask = 0xFu << (t & 28);
+        if (h < nb) {
+          bool ok = false;
+          if (S.sok[h]) ok = quad_fit8(J.m, S.samp[h], jac + h * 162, jac + h * 162 + 81, ql, qmask, S.F[h]);
+          if (ql == 0) S.fok[h] = ok ? 1 : 0;
         }
-        S.fok[t] = ok;
       }
       __syncthreads();
       // 3. inlier counts: warp w takes hypotheses w, w + 8, ...
       {
         const int lane = t & 31, warp = t >> 5;
-        for (int h = warp; h < nb; h += kFThreads / 32) {
-          int c = 0;
-          if (S.fok[h]) {
-            double f[9];
-            for (int i = 0; i < 9; ++i) f[i] = S.F[h][i];
-            for (int i = lane; i < n; i += 32) c += sampson(f, J.m[i]) <= J.tsq;
+        // two hypotheses per pass over the matches (one load, two independent evaluations)
+        for (int h = warp; h < nb; h += 2 * (kFThreads / 32)) {
+          const int h2 = h + kFThreads / 32;
+          const bool v1 = S.fok[h] != 0, v2 = h2 < nb && S.fok[h2] != 0;
+          int c1 = 0, c2 = 0;
+          if (v1 || v2) {
+            double f1[9], f2[9];
+            for (int i = 0; i < 9; ++i) {
+              f1[i] = S.F[h][i];
+              f2[i] = h2 < nb ? S.F[h2][i] : 0.0;
+            }
+            for (int i = lane; i < n; i += 32) {
+              const psift_match& a = J.m[i];
+              c1 += v1 && sampson(f1, a) <= J.tsq;
+              c2 += v2 && sampson(f2, a) <= J.tsq;
+            }
           }
-          for (int o = 16; o >= 1; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-          if (lane == 0) S.cnt[h] = c;
+          for (int o = 16; o >= 1; o >>= 1) {
+            c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+            c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+          }
+          if (lane == 0) {
+            S.cnt[h] = c1;
+            if (h2 < nb) S.cnt[h2] = c2;
+          }
         }
       }
       __syncthreads();
@@ -846,7 +1037,7 @@ __global__ void __launch_bounds__(kFThreads) fundamental_kernel(const FundJob* _
       for (int round = 0; round < 2; ++round) {
         const int k = collect(J, S);
         if (k < 8) break;
-        fit_list(J, S, k);
+        fit_list(J, S, jac, k);
         if (!S.fit_ok) break;
         int c;
         double e;
@@ -928,7 +1119,9 @@ psift_status run_fundamental(psift_ctx* ctx, const psift_fundamental_job* jobs, 
   }
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_jobs, hj.data(), sizeof(FundJob) * n, cudaMemcpyHostToDevice, ctx->stream));
   StageScope sc(ctx, STAGE_RANSAC);
-  fundamental_kernel<<<n, kFThreads, 0, ctx->stream>>>(d_jobs);
+  cudaError_t ea = ensure_smem_attr((const void*)fundamental_kernel, kJacSmem);
+  if (ea != cudaSuccess) return cuda_error(ctx, ea, "cudaFuncSetAttribute(fundamental_kernel)");
+  fundamental_kernel<<<n, kFThreads, kJacSmem, ctx->stream>>>(d_jobs);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(ctx, e, "fundamental_ransac");
