@@ -57,7 +57,7 @@ struct FundJob {
 struct FShared {
   double F[kFB][9];
   int samp[kFB][8];
-  int sok[kFB], fok[kFB], cnt[kFB];
+  int sok[kFB], fok[kFB], cnt[kFB], sdup[kFB];
   int draws[kFWin];
   double best[9], cand[9];
   double best_err;
@@ -522,6 +522,28 @@ __device__ __forceinline__ double sampson(const double* f, const psift_match& a)
   return (e * e) / den;
 }
 
+// sampson(f, a) <= tsq without the division where the comparison is clear:
+// with ee = e * e and p = tsq * den (both rounded), ee / den <= tsq when
+// ee <= p (1 - 2^-50) and round(ee / den) > tsq when ee >= p (1 + 2^-50) (the
+// margins cover the roundings of p, of the margin product and of the quotient);
+// in between, and for NaN, the reference's quotient decides.
+__device__ __forceinline__ bool sampson_in(const double* f, const psift_match& a, double tsq) {
+  const double x1 = (double)a.query_x, y1 = (double)a.query_y, x2 = (double)a.target_x, y2 = (double)a.target_y;
+  const double a0 = f[0] * x1 + f[1] * y1 + f[2];
+  const double a1 = f[3] * x1 + f[4] * y1 + f[5];
+  const double a2 = f[6] * x1 + f[7] * y1 + f[8];
+  const double b0 = f[0] * x2 + f[3] * y2 + f[6];
+  const double b1 = f[1] * x2 + f[4] * y2 + f[7];
+  const double e = x2 * a0 + y2 * a1 + a2;
+  const double den = a0 * a0 + a1 * a1 + b0 * b0 + b1 * b1;
+  if (den < 1e-18 || !isfinite(den)) return false;  // infinite distance
+  const double ee = e * e;
+  const double p = tsq * den;
+  if (ee <= p * (1.0 - 0x1p-50)) return true;
+  if (ee >= p * (1.0 + 0x1p-50)) return false;
+  return ee / den <= tsq;
+}
+
 // powi as the compiler runtime evaluates it (square-and-multiply, low bit first).
 __device__ double powi_d(double a, int b) {
   double r = 1.0;
@@ -913,6 +935,38 @@ __global__ void __launch_bounds__(kFThreads) fundamental_kernel(const FundJob* _
       if (t == 0) S.nb = 0;
       __syncthreads();
       while (true) {
+        // Speculation: almost every iteration's first 8 draws are distinct, so
+        // iteration nb0 + k uses draws tp0 + 8k .. tp0 + 8k + 7 until the first one
+        // holding a repeat; thread 0 walks on from there as the reference does.
+        {
+          const int nb0 = S.nb;
+          const long long tp0 = S.tpos;
+          const long long room = S.wb + kFWin - 32 - tp0;  // iteration k needs tp0 + 8k + 32 <= wb + kFWin
+          const int K = room < 0 ? 0 : (int)min((long long)(want - nb0), room / 8 + 1);
+          if (t < K) {
+            int d[8];
+            const int base = (int)(tp0 - S.wb) + 8 * t;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) d[q] = S.draws[base + q];
+            bool dup = false;
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+              for (int b = a + 1; b < 8; ++b) dup = dup || d[a] == d[b];
+            S.sdup[t] = dup ? 1 : 0;
+            if (!dup)
+#pragma unroll
+              for (int q = 0; q < 8; ++q) S.samp[nb0 + t][q] = d[q];
+          }
+          __syncthreads();
+          if (t == 0) {
+            int k = 0;
+            while (k < K && !S.sdup[k]) S.sok[nb0 + k++] = 1;
+            S.nb = nb0 + k;
+            S.tpos = tp0 + 8ll * k;
+          }
+          __syncthreads();
+        }
         if (t == 0) {
           int nb = S.nb;
           long long tp = S.tpos;
@@ -970,8 +1024,8 @@ __global__ void __launch_bounds__(kFThreads) fundamental_kernel(const FundJob* _
             }
             for (int i = lane; i < n; i += 32) {
               const psift_match& a = J.m[i];
-              c1 += v1 && sampson(f1, a) <= J.tsq;
-              c2 += v2 && sampson(f2, a) <= J.tsq;
+              c1 += v1 && sampson_in(f1, a, J.tsq);
+              c2 += v2 && sampson_in(f2, a, J.tsq);
             }
           }
           for (int o = 16; o >= 1; o >>= 1) {
