@@ -103,8 +103,9 @@ psift_status psift_ctx_synchronize(psift_ctx* ctx);
  * emit), 2 top-K cap, 3 orientation, 4 descriptors, 5 matching, 6 Hamming,
  * 7 RANSAC, 8 MLP.  psift_ctx_stage_times synchronises the stream and returns
  * the accumulated milliseconds and the number of timed intervals per stage. */
-/* CUDA graphs for psift_detect_and_compute_batch_dev (on by default): the first
- * call with a given launch geometry (image count and sizes, config) runs
+/* CUDA graphs for psift_detect_and_compute_batch_dev and the one-image host
+ * entries psift_detect_and_compute[_u8] (on by default): the first call with a
+ * given launch geometry (image count and sizes, input type, config) runs
  * eagerly, the second is captured into a graph, later ones replay it.  The
  * plan table of each call (image and output pointers) is uploaded before the
  * replay, so pointers may change between calls.  Off while stage timing is on. */

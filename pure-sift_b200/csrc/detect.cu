@@ -462,6 +462,57 @@ psift_status error_from_word(psift_ctx* ctx, uint32_t w) {
 }
 
 // Host-pointer detect_and_compute for one image (f32 or u8 source).
+// Runs the detection work of a job whose plan table is already uploaded: the
+// first call with a launch geometry runs eagerly, the second captures a CUDA graph
+// (keyed by the geometry, the configuration and the workspace addresses the
+// kernels take as arguments), later ones replay it.
+psift_status run_detect_cached(psift_ctx* ctx, DetectJob& job, const psift_sift_config& cfg, const char* tag) {
+  if (!ctx->graphs_enabled) return launch_detect_split(ctx, job, cfg);
+  const int n = job.n;
+  std::string key;
+  {
+    char buf[192];
+    snprintf(buf, sizeof buf, "%s n%d o%u s%u t%08x u%d k%d m%u kc%u sc%u p%p e%p|", tag, n, cfg.octaves, cfg.scales,
+             float_bits(cfg.contrast_threshold), cfg.upsample_first_octave, cfg.descriptor_kind, cfg.max_features,
+             job.kp_cap, job.sel_cap, (void*)job.d_plans, (void*)ctx->d_error);
+    key = buf;
+    for (int i = 0; i < n; ++i) {
+      snprintf(buf, sizeof buf, "%dx%d:%d:%d,", job.plans[i].oct[0].h, job.plans[i].oct[0].w, job.n_oct[i],
+               job.plans[i].src_kind);
+      key += buf;
+    }
+  }
+  auto it = ctx->graphs.find(key);
+  if (it == ctx->graphs.end()) {
+    if (ctx->graph_seen[key]++ == 0) return launch_detect_split(ctx, job, cfg);
+    if (ctx->graphs.size() >= 32) {
+      for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
+      ctx->graphs.clear();
+    }
+    const uint64_t l0 = ctx->launches;
+    PSIFT_CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    psift_status st = launch_detect_split(ctx, job, cfg);
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st != PSIFT_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaStreamEndCapture");
+    psift_ctx::GraphEntry ent;
+    ce = cudaGraphInstantiate(&ent.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaGraphInstantiate");
+    ent.launches = ctx->launches - l0;
+    ctx->launches = l0;
+    it = ctx->graphs.emplace(key, ent).first;
+  }
+  PSIFT_CUDA_TRY(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
+  ctx->launches += it->second.launches;
+  ctx->graph_replays++;
+  return PSIFT_OK;
+}
+
 psift_status detect_host(psift_ctx* ctx, const void* image, int kind, uint32_t h, uint32_t w, size_t stride,
                          const psift_sift_config* cfg, psift_features* out) {
   psift_status st = check_common(ctx, cfg);
@@ -487,11 +538,22 @@ psift_status detect_host(psift_ctx* ctx, const void* image, int kind, uint32_t h
   st = pinned_reserve(ctx, std::max(img_bytes, (size_t)feat_cap * sizeof(float) * (5 + kDescLen)) + meta_bytes);
   if (st != PSIFT_OK) return st;
   char* pin = ctx->pinned.base;
-  for (uint32_t y = 0; y < h; ++y)
-    std::memcpy(pin + (size_t)y * w * esz, (const char*)image + (size_t)y * stride * esz, (size_t)w * esz);
+  // rows staged in bands: the upload of one band overlaps the host copy of the next
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream));
-  if (img_bytes) PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_img, pin, img_bytes, cudaMemcpyHostToDevice, ctx->stream));
-  st = launch_detect(ctx, job, *cfg, false);
+  if (img_bytes) {
+    const uint32_t band = std::max<uint32_t>(1, (uint32_t)((256u << 10) / std::max<size_t>((size_t)w * esz, 1)));
+    for (uint32_t y0 = 0; y0 < h; y0 += band) {
+      const uint32_t y1 = std::min(h, y0 + band);
+      for (uint32_t y = y0; y < y1; ++y)
+        std::memcpy(pin + (size_t)y * w * esz, (const char*)image + (size_t)y * stride * esz, (size_t)w * esz);
+      PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync((char*)d_img + (size_t)y0 * w * esz, pin + (size_t)y0 * w * esz,
+                                          (size_t)(y1 - y0) * w * esz, cudaMemcpyHostToDevice, ctx->stream));
+    }
+  }
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * job.n,
+                                      cudaMemcpyHostToDevice, ctx->stream));
+  st = ctx->timer.enabled ? launch_detect(ctx, job, *cfg, false, nullptr, true)
+                          : run_detect_cached(ctx, job, *cfg, "host");
   if (st != PSIFT_OK) return st;
   uint32_t* hmeta = (uint32_t*)(pin + ctx->pinned.capacity - meta_bytes);
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hmeta, job.plans[0].kp_count, 16, cudaMemcpyDeviceToHost, ctx->stream));
@@ -795,48 +857,7 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice,
                                       ctx->stream));
   if (ctx->timer.enabled) return launch_detect(ctx, job, *cfg, false, nullptr, true);
-  if (!ctx->graphs_enabled) return launch_detect_split(ctx, job, *cfg);
-  std::string key;
-  {
-    char buf[160];
-    snprintf(buf, sizeof buf, "n%u o%u s%u t%08x u%d k%d m%u kc%u sc%u p%p e%p|", n, cfg->octaves, cfg->scales,
-             float_bits(cfg->contrast_threshold), cfg->upsample_first_octave, cfg->descriptor_kind, cfg->max_features,
-             job.kp_cap, job.sel_cap, (void*)job.d_plans, (void*)ctx->d_error);
-    key = buf;
-    for (uint32_t i = 0; i < n; ++i) {
-      snprintf(buf, sizeof buf, "%dx%d:%d,", job.plans[i].oct[0].h, job.plans[i].oct[0].w, job.n_oct[i]);
-      key += buf;
-    }
-  }
-  auto it = ctx->graphs.find(key);
-  if (it == ctx->graphs.end()) {
-    if (ctx->graph_seen[key]++ == 0) return launch_detect_split(ctx, job, *cfg);
-    if (ctx->graphs.size() >= 32) {
-      for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
-      ctx->graphs.clear();
-    }
-    const uint64_t l0 = ctx->launches;
-    PSIFT_CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    st = launch_detect_split(ctx, job, *cfg);
-    cudaGraph_t graph = nullptr;
-    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
-    if (st != PSIFT_OK) {
-      if (graph) cudaGraphDestroy(graph);
-      return st;
-    }
-    if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaStreamEndCapture");
-    psift_ctx::GraphEntry ent;
-    ce = cudaGraphInstantiate(&ent.exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaGraphInstantiate");
-    ent.launches = ctx->launches - l0;
-    ctx->launches = l0;
-    it = ctx->graphs.emplace(key, ent).first;
-  }
-  PSIFT_CUDA_TRY(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
-  ctx->launches += it->second.launches;
-  ctx->graph_replays++;
-  return PSIFT_OK;
+  return run_detect_cached(ctx, job, *cfg, "dev");
 }
 
 

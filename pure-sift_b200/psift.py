@@ -410,6 +410,11 @@ class Features:
         return Features(*(np.zeros(n, np.float32) for _ in range(5)), np.zeros((n, 128), np.float32))
 
     @staticmethod
+    def uninitialized(n: int) -> "Features":
+        """Capacity-n output arrays without a zero fill (the library writes them)."""
+        return Features(*(np.empty(n, np.float32) for _ in range(5)), np.empty((n, 128), np.float32))
+
+    @staticmethod
     def pinned(n: int, ctx: "Context | None" = None) -> "Features":
         """Capacity-n feature arrays in one page-locked block (direct device->host copies)."""
         blk = pinned_empty(((5 + 128) * max(n, 1),), np.float32, ctx)
@@ -452,14 +457,16 @@ class Sift:
         cap = self.config.max_features_ or 16384
         fn = ctx.lib.psift_detect_and_compute_u8 if u8 else ctx.lib.psift_detect_and_compute
         while True:
-            out = Features.empty(cap)
+            out = Features.uninitialized(cap)
             cf = _c_features(out)
             st = fn(ctx.handle, img.ctypes.data, h, w, w, C.byref(cfg), C.byref(cf))
             if st == PSIFT_ERR_CAPACITY and cf.count > cap:
                 cap = int(cf.count)
                 continue
             ctx.check(st)
-            return out.head(int(cf.count))
+            n = int(cf.count)
+            # views when most of the block is used, else compact copies
+            return out.view(n) if 2 * n >= cap else out.head(n)
 
     def detect_and_compute(self, img: np.ndarray, ctx: Context | None = None) -> Features:
         return self._run(img, False, ctx)

@@ -67,3 +67,29 @@ def test_graph_replay_equals_eager():
     assert ctx.graph_replays == 5
     ctx.close()
     eager.close()
+
+
+def test_single_image_host_path_replays_graphs():
+    # psift_detect_and_compute_u8 / psift_detect_and_compute (one image per call, host
+    # buffers) share the geometry-keyed graph cache; u8 and f32 inputs get separate graphs
+    cfg = psift.SiftConfig().with_octaves(4)
+    sift = psift.Sift.new(cfg)
+    imgs = [synth.blob_image(320, 240, 90, 2.0, 10.0, seed=300 + i) for i in range(3)]
+    eager = psift.Context(0)
+    eager.enable_graphs(False)
+    ctx = psift.Context(0)
+    ref = [sift.detect_and_compute_u8(im, ctx=eager) for im in imgs]
+    ref_f = sift.detect_and_compute(imgs[0].astype(np.float32) / 255.0, ctx=eager)
+    for _ in range(2):
+        for im, r in zip(imgs, ref):
+            got = sift.detect_and_compute_u8(im, ctx=ctx)
+            for k in ("x", "y", "scale", "response", "orientation", "descriptors"):
+                np.testing.assert_array_equal(getattr(got, k), getattr(r, k), err_msg=k)
+    assert eager.graph_replays == 0 and ctx.graph_replays == 5
+    for _ in range(3):
+        got = sift.detect_and_compute(imgs[0].astype(np.float32) / 255.0, ctx=ctx)
+        np.testing.assert_array_equal(got.descriptors, ref_f.descriptors)
+        np.testing.assert_array_equal(got.x, ref_f.x)
+    assert ctx.graph_replays == 7
+    ctx.close()
+    eager.close()
