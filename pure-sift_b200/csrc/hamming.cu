@@ -32,8 +32,18 @@ constexpr int kQG = 16;       // queries per warp
 constexpr int kTopKMax = 64;  // shortlist length upper bound
 constexpr int kHamWarps = 4;
 
+// popc(x0) + popc(x1) + popc(x2) + popc(x3) with three popcounts: a carry-save
+// step gives, bit by bit, x0 + x1 + x2 = s + 2c (s = x0 ^ x1 ^ x2, c = majority),
+// so the sum is popc(s) + 2 popc(c) + popc(x3), the same integer.  The popcount
+// pipe bounds the Hamming scans; s and c are one LOP3 each on the ALU pipe.
+__device__ __forceinline__ int popc4(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
+  const uint32_t s = x0 ^ x1 ^ x2;
+  const uint32_t c = (x0 & x1) | (x2 & (x0 ^ x1));
+  return __popc(s) + 2 * __popc(c) + __popc(x3);
+}
+
 __device__ __forceinline__ int ham128(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint4 c) {
-  return __popc(a0 ^ c.x) + __popc(a1 ^ c.y) + __popc(a2 ^ c.z) + __popc(a3 ^ c.w);
+  return popc4(a0 ^ c.x, a1 ^ c.y, a2 ^ c.z, a3 ^ c.w);
 }
 
 __device__ __forceinline__ bool has_zero_byte(uint32_t x) { return ((x - 0x01010101u) & ~x & 0x80808080u) != 0; }
@@ -135,7 +145,7 @@ __global__ void __launch_bounds__(256) votes_kernel(const uint4* __restrict__ q,
     for (long long s = s0; s < s1; ++s) {
       const uint4 c = cat[s];
       const uint32_t x0 = qq.x ^ c.x, x1 = qq.y ^ c.y, x2 = qq.z ^ c.z, x3 = qq.w ^ c.w;
-      const int d = __popc(x0) + __popc(x1) + __popc(x2) + __popc(x3);
+      const int d = popc4(x0, x1, x2, x3);
       if (d <= 24 && (!mih || has_zero_byte(x0) || has_zero_byte(x1) || has_zero_byte(x2) || has_zero_byte(x3))) {
         ++hits;
         break;
