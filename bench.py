@@ -644,6 +644,11 @@ def run_ours(args):
     ctx = psift.Context(local)
     cfg = psift.SiftConfig().with_octaves(OCTAVES).with_scales(SCALES).with_contrast_threshold(THRESH)
     ccfg = cfg.to_c()
+    # tile shapes: the library's autotuner on this geometry (one chunk of the batch;
+    # the matcher on 4096 x 4096 problems), before any timing
+    t_tune = time.perf_counter()
+    tune = None if args.no_autotune else ctx.autotune(HEIGHT, WIDTH, (B + 1) // 2, cfg, n_desc=4096, n_pairs=8)
+    tune_s = time.perf_counter() - t_tune
     cimgs = (psift.CImageU8 * B)(*[psift.CImageU8(t.data_ptr(), HEIGHT, WIDTH, WIDTH) for t in d_imgs])
     couts = (psift.CFeatures * B)(*[psift.CFeatures(cap, 0, o["x"].data_ptr(), o["y"].data_ptr(),
                                                     o["s"].data_ptr(), o["r"].data_ptr(), o["o"].data_ptr(),
@@ -723,6 +728,12 @@ def run_ours(args):
         return ims, [psift.Features.pinned(MAX_FEATURES, c) for _ in range(B)]
 
     ctx2 = psift.Context(local)
+    if tune is not None:  # the second host thread's context runs the same tile shapes
+        t = ctx.tuning()
+        for r, v in t["blur"].items():
+            ctx2.set_tuning(ctx2.TUNE_BLUR, r, v)
+        ctx2.set_tuning(ctx2.TUNE_MATCH_FP32, 0, t["match_fp32_per_sm"])
+        ctx2.set_tuning(ctx2.TUNE_MATCH_TC, 0, t["match_tc_per_sm"])
     workers = [(ctx,) + pinned_set(ctx), (ctx2,) + pinned_set(ctx2)]
     for c, ims, fo in workers:
         for _ in range(2):
@@ -773,7 +784,14 @@ def run_ours(args):
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "batch_per_gpu": B, "global_batch": world * B, "l2": L2_NOTE,
-                       "features_per_image": [int(c) for c in counts[:4]]},
+                       "features_per_image": [int(c) for c in counts[:4]],
+                       "autotune": None if tune is None else {
+                           "seconds": tune_s,
+                           "blur_variant_per_radius": {r: e["variant"] for r, e in tune["blur"].items()},
+                           "blur_ms_per_variant": {r: e["ms"] for r, e in tune["blur"].items()},
+                           "match_fp32_items_per_sm": tune["match_fp32"]["per_sm"],
+                           "match_tc_items_per_sm": tune["match_tc"]["per_sm"],
+                           "variants": "blur outputs per thread 0: 4x8, 1: 8x8, 2: 4x4 (columns x rows)"}},
             "gpu_launches": int(launches),
             "e2e": {"value": e2e_value, "unit": "images/s", "h2d_bytes_per_step": B * WIDTH * HEIGHT,
                     "d2h_bytes_per_step": int(d2h),
@@ -837,6 +855,8 @@ def main():
     ap.add_argument("--no-catalog", action="store_true")
     ap.add_argument("--no-catalog-search", dest="no_catalog_search", action="store_true")
     ap.add_argument("--no-warp", dest="no_warp", action="store_true")
+    ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
+                    help="run the default tile shapes instead of the autotuner's")
     ap.add_argument("--no-fundamental", dest="no_fundamental", action="store_true")
     ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")

@@ -112,6 +112,29 @@ psift_status psift_ctx_synchronize(psift_ctx* ctx);
 psift_status psift_ctx_enable_graphs(psift_ctx* ctx, int enable);
 uint64_t psift_ctx_graph_replays(const psift_ctx* ctx);
 psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
+
+/* Tile shapes, chosen by the library's autotuner.  No counterpart in the
+ * reference.  Every choice computes identical results; only time differs.
+ *  - PSIFT_TUNE_BLUR, index = radius 1..15: the level blur's outputs per thread
+ *    (0: 4 columns x 8 rows, the default; 1: 8 x 8; 2: 4 x 4).
+ *  - PSIFT_TUNE_MATCH_FP32 / PSIFT_TUNE_MATCH_TC, index 0: the matchers' work items
+ *    per SM (default 2); a query tile's target tiles are split into that many
+ *    ranges overall, which sets each CTA's target extent.
+ * psift_ctx_autotune times every candidate on synthetic inputs of the caller's
+ * geometry (n_images u8 images of height x width with cfg's blur schedule;
+ * n_pairs matching problems of n_desc x n_desc descriptors, both matcher paths)
+ * and keeps the fastest in the context.  report (optional, report_capacity
+ * doubles; report_count = the doubles written): per blur radius (radius, ms of
+ * variants 0..2, chosen), then -1, then per matcher path (path 0 FP32 / 1 tensor
+ * core, ms for 1, 2, 4, 8 work items per SM, chosen). */
+#define PSIFT_TUNE_BLUR 0
+#define PSIFT_TUNE_MATCH_FP32 1
+#define PSIFT_TUNE_MATCH_TC 2
+psift_status psift_ctx_autotune(psift_ctx* ctx, uint32_t height, uint32_t width, uint32_t n_images,
+                                const psift_sift_config* cfg, uint32_t n_desc, uint32_t n_pairs, double* report,
+                                uint32_t report_capacity, uint32_t* report_count);
+psift_status psift_ctx_tuning_get(const psift_ctx* ctx, int32_t what, int32_t index, int32_t* value);
+psift_status psift_ctx_tuning_set(psift_ctx* ctx, int32_t what, int32_t index, int32_t value);
 psift_status psift_ctx_stage_times(psift_ctx* ctx, double* ms, uint64_t* counts, uint32_t n, int reset);
 
 /* ---------------------------------------------------------------- config */

@@ -24,7 +24,7 @@ namespace psift {
 
 // Declared in pyramid.cu / extrema.cu / describe.cu.
 cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
-                        int level, int down_level, int max_h, int max_w, cudaStream_t st);
+                        int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant = 0);
 cudaError_t launch_extrema_mark(const ImagePlan* plans, int n, int octave, int max_h, const ExtremaParams& prm,
                                 cudaStream_t st);
 cudaError_t launch_row_scan(const ImagePlan* plans, int n, uint32_t kp_cap, uint32_t* err, cudaStream_t st);
@@ -133,6 +133,7 @@ struct DetectJob {
   std::vector<int> n_oct;
   ImagePlan* d_plans = nullptr;
   uint32_t kp_cap = 0, sel_cap = 0;
+  int8_t blur_variant[16] = {0};     // level-blur variant per radius (the context's tuning)
 };
 
 struct ImageDesc {
@@ -156,6 +157,7 @@ psift_status build_job(psift_ctx* ctx, const std::vector<ImageDesc>& imgs, const
   job.n = n;
   job.kp_cap = kDefaultKeypointCapacity;
   job.sel_cap = cfg.max_features ? cfg.max_features : job.kp_cap;
+  std::memcpy(job.blur_variant, ctx->tune.blur, sizeof job.blur_variant);
   job.oct.assign((size_t)n * kMaxOctaves, HostOctave{0, 0, 0});
   job.n_oct.assign(n, 0);
   size_t total = align_up(sizeof(ImagePlan) * n, 256) + align_up(extra_bytes, 256);
@@ -249,7 +251,9 @@ psift_status build_job(psift_ctx* ctx, const std::vector<ImageDesc>& imgs, const
 // One blur level (octave o, level s >= 1) of every image of the job.
 cudaError_t launch_level(const DetectJob& job, const SigmaSchedule& sc, int o, int s, int S, int mh, int mw,
                          cudaStream_t st) {
-  return launch_blur(0, sc.level_taps[s].data(), sc.level_radius[s], job.d_plans, job.n, o, s, S, mh, mw, st);
+  const int r = sc.level_radius[s];
+  return launch_blur(0, sc.level_taps[s].data(), r, job.d_plans, job.n, o, s, S, mh, mw, st,
+                     r >= 0 && r < 16 ? job.blur_variant[r] : 0);
 }
 
 // Queue every stage of the path for the batch (no host synchronisation).
@@ -472,9 +476,9 @@ psift_status run_detect_cached(psift_ctx* ctx, DetectJob& job, const psift_sift_
   std::string key;
   {
     char buf[192];
-    snprintf(buf, sizeof buf, "%s n%d o%u s%u t%08x u%d k%d m%u kc%u sc%u p%p e%p|", tag, n, cfg.octaves, cfg.scales,
-             float_bits(cfg.contrast_threshold), cfg.upsample_first_octave, cfg.descriptor_kind, cfg.max_features,
-             job.kp_cap, job.sel_cap, (void*)job.d_plans, (void*)ctx->d_error);
+    snprintf(buf, sizeof buf, "%s n%d o%u s%u t%08x u%d k%d m%u kc%u sc%u p%p e%p g%u|", tag, n, cfg.octaves,
+             cfg.scales, float_bits(cfg.contrast_threshold), cfg.upsample_first_octave, cfg.descriptor_kind,
+             cfg.max_features, job.kp_cap, job.sel_cap, (void*)job.d_plans, (void*)ctx->d_error, ctx->tune.gen);
     key = buf;
     for (int i = 0; i < n; ++i) {
       snprintf(buf, sizeof buf, "%dx%d:%d:%d,", job.plans[i].oct[0].h, job.plans[i].oct[0].w, job.n_oct[i],
@@ -592,12 +596,135 @@ psift_status detect_host(psift_ctx* ctx, const void* image, int kind, uint32_t h
   return PSIFT_OK;
 }
 
+// Autotuner, level blur: every variant of every level radius of cfg's schedule,
+// timed on octave 0 of n synthetic u8 images of h x w (pseudo-random bytes, the
+// pyramid built once first); the fastest variant per radius is kept.  report:
+// per distinct radius (radius, ms of each variant, chosen).
+constexpr int kBlurVariantCount = 3;
+psift_status autotune_blur(psift_ctx* ctx, uint32_t h, uint32_t w, uint32_t n, const psift_sift_config& cfg,
+                           std::vector<double>& report) {
+  if (h == 0 || w == 0 || n == 0) return PSIFT_OK;
+  const size_t img = (size_t)h * w;
+  ImageDesc d{};
+  d.stride = w;
+  d.h = (int)h;
+  d.w = (int)w;
+  d.kind = SRC_U8;
+  d.feat_cap = 1;
+  std::vector<ImageDesc> imgs(n, d);
+  DetectJob job;
+  void* d_img = nullptr;
+  psift_status st = build_job(ctx, imgs, cfg, job, img * n, &d_img);
+  if (st != PSIFT_OK) return st;
+  if (job.n_oct[0] == 0) return PSIFT_OK;
+  std::vector<uint8_t> bytes(img * n);
+  uint64_t x = 0x9E3779B97F4A7C15ull;
+  for (size_t i = 0; i < bytes.size(); ++i) {
+    x ^= x << 13;
+    x ^= x >> 7;
+    x ^= x << 17;
+    bytes[i] = (uint8_t)(x >> 24);
+  }
+  for (uint32_t i = 0; i < n; ++i) job.plans[i].src = (uint8_t*)d_img + img * i;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_img, bytes.data(), bytes.size(), cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  if ((st = launch_detect(ctx, job, cfg, true, nullptr, true)) != PSIFT_OK) return st;
+  const int S = (int)cfg.scales;
+  const SigmaSchedule sc = make_schedule(S, cfg.upsample_first_octave != 0);
+  const int mh = job.oct[0].h, mw = job.oct[0].w;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  PSIFT_CUDA_TRY(ctx, cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_error(ctx, ce, "cudaEventCreate");
+  }
+  bool seen[16] = {false};
+  for (int s = 1; s <= S + 2 && st == PSIFT_OK; ++s) {
+    const int r = sc.level_radius[s];
+    if (r < 1 || r > 15 || seen[r]) continue;
+    seen[r] = true;
+    report.push_back(r);
+    double best_ms = 1e30;
+    int best = 0;
+    for (int v = 0; v < kBlurVariantCount; ++v) {
+      float ms = 1e30f;
+      for (int rep = 0; rep < 4 && ce == cudaSuccess; ++rep) {  // rep 0 warms up
+        if (rep > 0) ce = cudaEventRecord(e0, ctx->stream);
+        if (ce == cudaSuccess) ce = launch_blur(0, sc.level_taps[s].data(), r, job.d_plans, (int)n, 0, s, -1, mh, mw,
+                                                ctx->stream, v);
+        ctx->launches++;
+        if (rep == 0 || ce != cudaSuccess) continue;
+        ce = cudaEventRecord(e1, ctx->stream);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        float t = 0.0f;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&t, e0, e1);
+        ms = std::min(ms, t);
+      }
+      if (ce != cudaSuccess) {
+        st = cuda_error(ctx, ce, "autotune blur");
+        break;
+      }
+      report.push_back(ms);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = v;
+      }
+    }
+    if (st != PSIFT_OK) break;
+    ctx->tune.blur[r] = (int8_t)best;
+    report.push_back(best);
+  }
+  ctx->tune.gen++;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
+
 }  // namespace
 }  // namespace psift
 
 using namespace psift;
 
 extern "C" {
+
+psift_status psift_ctx_autotune(psift_ctx* ctx, uint32_t height, uint32_t width, uint32_t n_images,
+                                const psift_sift_config* cfg, uint32_t n_desc, uint32_t n_pairs, double* report,
+                                uint32_t report_capacity, uint32_t* report_count) {
+  psift_status st = check_common(ctx, cfg);
+  if (st != PSIFT_OK) return st;
+  std::vector<double> rep;
+  if ((st = autotune_blur(ctx, height, width, n_images, *cfg, rep)) != PSIFT_OK) return st;
+  rep.push_back(-1.0);  // separator between the blur and the matcher entries
+  if ((st = autotune_match(ctx, n_desc, n_pairs, rep)) != PSIFT_OK) return st;
+  if (report_count) *report_count = (uint32_t)rep.size();
+  if (report) std::memcpy(report, rep.data(), sizeof(double) * std::min<size_t>(rep.size(), report_capacity));
+  if (report && rep.size() > report_capacity) return set_error(ctx, PSIFT_ERR_CAPACITY, "report capacity too small");
+  return PSIFT_OK;
+}
+
+psift_status psift_ctx_tuning_get(const psift_ctx* ctx, int32_t what, int32_t index, int32_t* value) {
+  if (!ctx || !value) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (what == PSIFT_TUNE_BLUR && index >= 1 && index <= 15) *value = ctx->tune.blur[index];
+  else if (what == PSIFT_TUNE_MATCH_FP32 && index == 0) *value = ctx->tune.match_per_sm[0];
+  else if (what == PSIFT_TUNE_MATCH_TC && index == 0) *value = ctx->tune.match_per_sm[1];
+  else return PSIFT_ERR_INVALID_ARGUMENT;
+  return PSIFT_OK;
+}
+
+psift_status psift_ctx_tuning_set(psift_ctx* ctx, int32_t what, int32_t index, int32_t value) {
+  if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (what == PSIFT_TUNE_BLUR && index >= 1 && index <= 15 && value >= 0 && value < kBlurVariantCount)
+    ctx->tune.blur[index] = (int8_t)value;
+  else if ((what == PSIFT_TUNE_MATCH_FP32 || what == PSIFT_TUNE_MATCH_TC) && index == 0 && value >= 1 && value <= 64)
+    ctx->tune.match_per_sm[what == PSIFT_TUNE_MATCH_TC ? 1 : 0] = (int8_t)value;
+  else
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "tuning entry or value out of range");
+  ctx->tune.gen++;
+  return PSIFT_OK;
+}
+
 
 psift_status psift_detect_and_compute(psift_ctx* ctx, const float* image, uint32_t height, uint32_t width,
                                       size_t row_stride, const psift_sift_config* cfg, psift_features* out) {

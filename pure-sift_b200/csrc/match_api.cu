@@ -84,7 +84,7 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   long long cand_f = 0, cand_r = 0;
   std::vector<int> tc_split_f(na), tc_split_r(na);
   int n_items_f = 0, n_items_r = 0;
-  const int target_ctas = 2 * ctx->num_sms;
+  const int target_ctas = ctx->tune.match_per_sm[tc ? 1 : 0] * ctx->num_sms;
   for (int k = 0; k < na; ++k) {
     const psift_match_job& J = jobs[active[k]];
     const int qt = (int)((J.nq + kTile - 1) / kTile);
@@ -321,6 +321,101 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
 }
 
 }  // namespace
+
+// Autotuner, matchers: work items per SM in {1, 2, 4, 8} (how many ranges of
+// 256-wide target tiles each query tile is split into follows) for the FP32 and
+// the tensor-core paths, timed on n_pairs problems of n_desc x n_desc SIFT-like
+// descriptors (|N(0,1)|, L2-normalised, clipped at 0.2, renormalised; seeded);
+// the fastest is kept.  report: per path (path, ms for 1, 2, 4, 8, chosen).
+psift_status autotune_match(psift_ctx* ctx, uint32_t n_desc, uint32_t n_pairs, std::vector<double>& report) {
+  if (n_desc < 2 || n_pairs == 0) return PSIFT_OK;
+  const size_t nd = n_desc;
+  std::vector<float> host(2 * nd * 130);
+  uint64_t sm = 0x5EED1234ABCDull;
+  auto next = [&]() {
+    uint64_t z = (sm += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return (double)((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+  };
+  for (size_t r = 0; r < 2 * nd; ++r) {
+    float* d = host.data() + r * 128;
+    double ss = 0.0;
+    for (int k = 0; k < 128; ++k) {
+      const double u1 = next() + 1e-12, u2 = next();
+      d[k] = (float)std::fabs(std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2));
+      ss += (double)d[k] * d[k];
+    }
+    double s2 = 0.0;
+    for (int k = 0; k < 128; ++k) {
+      d[k] = std::min((float)(d[k] / std::sqrt(ss)), 0.2f);
+      s2 += (double)d[k] * d[k];
+    }
+    for (int k = 0; k < 128; ++k) d[k] = (float)(d[k] / std::sqrt(s2));
+  }
+  float* xy = host.data() + 2 * nd * 128;
+  for (size_t i = 0; i < 4 * nd; ++i) xy[i] = (float)(1000.0 * next());
+  float* d_in = nullptr;
+  psift_match* d_out = nullptr;
+  uint32_t* d_cnt = nullptr;
+  cudaError_t e = cudaMalloc(&d_in, host.size() * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(psift_match) * nd * n_pairs);
+  if (e == cudaSuccess) e = cudaMalloc(&d_cnt, 4 * (size_t)n_pairs);
+  auto release = [&]() {
+    cudaFree(d_in);
+    cudaFree(d_out);
+    cudaFree(d_cnt);
+  };
+  if (e != cudaSuccess) {
+    release();
+    return cuda_error(ctx, e, "cudaMalloc(autotune match)");
+  }
+  e = cudaMemcpyAsync(d_in, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  std::vector<psift_match_job> jobs(n_pairs);
+  for (uint32_t k = 0; k < n_pairs; ++k)
+    jobs[k] = psift_match_job{d_in, d_in + nd * 128, d_in + 2 * nd * 128, d_in + 2 * nd * 128 + 2 * nd,
+                              (uint32_t)nd, (uint32_t)nd, d_out + nd * k, (uint32_t)nd, d_cnt + k};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  psift_status st = e == cudaSuccess ? PSIFT_OK : cuda_error(ctx, e, "autotune match setup");
+  const int cands[4] = {1, 2, 4, 8};
+  for (int path = 0; path < 2 && st == PSIFT_OK; ++path) {
+    psift_match_options opt{0.8f, 0, path ? PSIFT_PRECISION_BF16_RERANK : PSIFT_PRECISION_FP32};
+    double best_ms = 1e30;
+    int best = ctx->tune.match_per_sm[path];
+    report.push_back(path);
+    for (int c = 0; c < 4 && st == PSIFT_OK; ++c) {
+      ctx->tune.match_per_sm[path] = (int8_t)cands[c];
+      float ms = 1e30f;
+      for (int rep = 0; rep < 3 && st == PSIFT_OK; ++rep) {
+        if ((st = match_batch(ctx, jobs.data(), (int)n_pairs, opt)) != PSIFT_OK) break;  // warm-up on rep 0
+        if (rep == 0) continue;
+        cudaEventRecord(e0, ctx->stream);
+        if ((st = match_batch(ctx, jobs.data(), (int)n_pairs, opt)) != PSIFT_OK) break;
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms = std::min(ms, t);
+      }
+      report.push_back(ms);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = cands[c];
+      }
+    }
+    ctx->tune.match_per_sm[path] = (int8_t)best;
+    report.push_back(best);
+  }
+  ctx->tune.gen++;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaStreamSynchronize(ctx->stream);
+  release();
+  return st;
+}
+
 }  // namespace psift
 
 using namespace psift;

@@ -80,6 +80,14 @@ struct psift_ctx {
     cudaGraphExec_t exec = nullptr;
     uint64_t launches = 0;
   };
+  // Tile shapes chosen by the autotuner (psift_ctx_autotune, tune.cu): the
+  // level-blur variant per radius and the matchers' work items per SM (FP32,
+  // tensor-core path).  gen changes with them (part of the graph cache key).
+  struct Tuning {
+    int8_t blur[16] = {0};
+    int8_t match_per_sm[2] = {2, 2};
+    uint32_t gen = 0;
+  } tune;
   bool graphs_enabled = true;
   std::map<std::string, GraphEntry> graphs;
   std::map<std::string, int> graph_seen;
@@ -106,6 +114,9 @@ psift_status io_reserve(psift_ctx* ctx, size_t bytes);
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Raise a kernel's dynamic shared-memory limit once per (kernel, device).
 cudaError_t ensure_smem_attr(const void* func, size_t bytes);
+// Autotuner of the matchers' work decomposition (match_api.cu); appends
+// (path, ms per candidate, chosen) per path to report.
+psift_status autotune_match(psift_ctx* ctx, uint32_t n_desc, uint32_t n_pairs, std::vector<double>& report);
 // Statistics of summarize_tracking over the masked matches (ransac_api.cu).
 void tracking_stats(const psift_match* m, uint32_t n, const uint8_t* mask, const float* q_scale,
                     const float* q_ori, const float* t_scale, const float* t_ori, psift_tracking_summary* out);

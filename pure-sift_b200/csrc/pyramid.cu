@@ -40,6 +40,8 @@ constexpr int kTileH = 64;
 constexpr int kBlurThreads = 256;
 constexpr int kTmpStride = kTileW + 8;  // floats per intermediate row
 constexpr int kStageBatch = 4;          // staging units per thread with loads in flight
+// Level-blur variants (outputs per thread: columns x rows), chosen per radius by
+// the context's tuning table (psift_ctx_autotune): 0 = 4 x 8, 1 = 8 x 8, 2 = 4 x 4.
 constexpr int kPrefetchWaves = 1;       // level blur: L2 prefetch distance in resident-CTA waves
 
 struct Taps2 {
@@ -413,12 +415,12 @@ static cudaError_t launch_blur_r(const ImagePlan* plans, int n_images, int octav
   return cudaGetLastError();
 }
 
-template <int MODE>
+template <int MODE, int HC, int RV>
 static cudaError_t launch_blur_mode(int radius, const ImagePlan* plans, int n, int octave, int level, int down_level,
                                     int zrev, const Taps2& taps, int max_h, int max_w, cudaStream_t st) {
   switch (radius) {
 #define PSIFT_R(RR) \
-  case RR: return launch_blur_r<RR, 4, 8, MODE>(plans, n, octave, level, down_level, zrev, taps, max_h, max_w, st);
+  case RR: return launch_blur_r<RR, HC, RV, MODE>(plans, n, octave, level, down_level, zrev, taps, max_h, max_w, st);
     PSIFT_R(1) PSIFT_R(2) PSIFT_R(3) PSIFT_R(4) PSIFT_R(5) PSIFT_R(6) PSIFT_R(7) PSIFT_R(8)
     PSIFT_R(9) PSIFT_R(10) PSIFT_R(11) PSIFT_R(12) PSIFT_R(13) PSIFT_R(14) PSIFT_R(15)
 #undef PSIFT_R
@@ -428,8 +430,10 @@ static cudaError_t launch_blur_mode(int radius, const ImagePlan* plans, int n, i
 }
 
 // Host entry: mode 0 = level blur (octave, level >= 1); modes 1..4 = octave-0 base.
+// variant (level blur only) picks the outputs per thread (see above); every
+// variant computes the same values.
 cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
-                        int level, int down_level, int max_h, int max_w, cudaStream_t st) {
+                        int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant) {
   Taps2 t;
   for (int i = 0; i < kMaxTaps; ++i) {
     const float v = i <= 2 * radius ? taps_host[i] : 0.0f;
@@ -438,11 +442,17 @@ cudaError_t launch_blur(int mode, const float* taps_host, int radius, const Imag
   t.one = make_float2(1.0f, 1.0f);
   const int zrev = (octave * 8 + level) & 1;
   switch (mode) {
-    case MODE_LEVEL: return launch_blur_mode<MODE_LEVEL>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-    case MODE_INIT_F32: return launch_blur_mode<MODE_INIT_F32>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-    case MODE_INIT_U8: return launch_blur_mode<MODE_INIT_U8>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-    case MODE_INIT_F32_UP: return launch_blur_mode<MODE_INIT_F32_UP>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-    case MODE_INIT_U8_UP: return launch_blur_mode<MODE_INIT_U8_UP>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_LEVEL:
+      switch (variant) {
+        case 0: return launch_blur_mode<MODE_LEVEL, 4, 8>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+        case 1: return launch_blur_mode<MODE_LEVEL, 8, 8>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+        case 2: return launch_blur_mode<MODE_LEVEL, 4, 4>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+        default: return cudaErrorInvalidValue;
+      }
+    case MODE_INIT_F32: return launch_blur_mode<MODE_INIT_F32, 4, 8>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_INIT_U8: return launch_blur_mode<MODE_INIT_U8, 4, 8>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_INIT_F32_UP: return launch_blur_mode<MODE_INIT_F32_UP, 4, 8>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_INIT_U8_UP: return launch_blur_mode<MODE_INIT_U8_UP, 4, 8>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -206,6 +206,10 @@ _SIGS = {
     "psift_detect_and_compute_u8_noalloc_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
                                                           C.POINTER(CSiftConfig), C.POINTER(CFeatures), C.c_void_p,
                                                           C.c_void_p]),
+    "psift_ctx_autotune": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(CSiftConfig),
+                                     C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "psift_ctx_tuning_get": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "psift_ctx_tuning_set": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "psift_fundamental_options_default": (None, [C.POINTER(CFundamentalOptions)]),
     "psift_fundamental_estimate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CFundamentalOptions),
                                              C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
@@ -307,6 +311,47 @@ class Context:
 
     def enable_stage_timing(self, on: bool = True):
         self.check(self.lib.psift_ctx_enable_stage_timing(self.handle, int(on)))
+
+    TUNE_BLUR, TUNE_MATCH_FP32, TUNE_MATCH_TC = 0, 1, 2
+
+    def autotune(self, height: int, width: int, n_images: int, config: "SiftConfig" = None, n_desc: int = 4096,
+                 n_pairs: int = 8) -> dict:
+        """Times the candidate tile shapes (level-blur outputs per thread per radius,
+        matcher work items per SM) on synthetic inputs of this geometry and keeps the
+        fastest; returns {"blur": {radius: {"ms": [...], "variant": v}},
+        "match_fp32" / "match_tc": {"ms": {items: ms}, "per_sm": m}}."""
+        config = config or SiftConfig()
+        c = config.to_c()
+        rep = np.zeros(1024, np.float64)
+        cnt = C.c_uint32()
+        self.check(self.lib.psift_ctx_autotune(self.handle, height, width, n_images, C.byref(c), n_desc, n_pairs,
+                                               rep.ctypes.data, len(rep), C.byref(cnt)))
+        r = rep[:cnt.value].tolist()
+        out = {"blur": {}}
+        i = 0
+        while i < len(r) and r[i] != -1.0:
+            out["blur"][int(r[i])] = {"ms": r[i + 1:i + 4], "variant": int(r[i + 4])}
+            i += 5
+        i += 1
+        while i + 6 <= len(r):
+            key = "match_tc" if r[i] == 1.0 else "match_fp32"
+            out[key] = {"ms": dict(zip((1, 2, 4, 8), r[i + 1:i + 5])), "per_sm": int(r[i + 5])}
+            i += 6
+        return out
+
+    def tuning(self) -> dict:
+        v = C.c_int32()
+        blur = {}
+        for rr in range(1, 16):
+            self.check(self.lib.psift_ctx_tuning_get(self.handle, self.TUNE_BLUR, rr, C.byref(v)))
+            blur[rr] = v.value
+        self.check(self.lib.psift_ctx_tuning_get(self.handle, self.TUNE_MATCH_FP32, 0, C.byref(v)))
+        fp32 = v.value
+        self.check(self.lib.psift_ctx_tuning_get(self.handle, self.TUNE_MATCH_TC, 0, C.byref(v)))
+        return {"blur": blur, "match_fp32_per_sm": fp32, "match_tc_per_sm": v.value}
+
+    def set_tuning(self, what: int, index: int, value: int):
+        self.check(self.lib.psift_ctx_tuning_set(self.handle, what, index, value))
 
     def stage_times(self, reset: bool = True) -> dict:
         """{stage: (total_ms, intervals)} accumulated since the last reset."""
