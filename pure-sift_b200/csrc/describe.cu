@@ -16,12 +16,15 @@
 // Per-bin sums therefore differ from the reference's raster-order sums only by
 // f32 rounding; all selection logic (peak tests, sort, truncation) and the final
 // normalisation repeat the reference's sequence exactly.
+#include <algorithm>
+
 #include "detect_plan.cuh"
 #include "psift_internal.cuh"
 
 namespace psift {
 
 constexpr int kOriBins = 36;
+constexpr uint32_t kKpPerLaunchRow = 4096;  // keypoints per image covered by one grid row
 constexpr int kOriWarps = 8;
 constexpr int kDescWarps = 4;
 
@@ -79,15 +82,11 @@ __device__ __forceinline__ void grad_at(const float* __restrict__ g, long long p
   ang = a < 0.0f ? a + two_pi : a;  // rem_euclid(2pi) of a value in [-pi, pi]
 }
 
-// Grid (ceil(sel_cap / 8), images), 256 threads: one warp per selected keypoint.
-__global__ void __launch_bounds__(kOriWarps * 32) orientation_kernel(const ImagePlan* __restrict__ plans,
-                                                                     DescribeParams prm) {
-  const ImagePlan& P = plans[blockIdx.y];
-  __shared__ float s_hist[kOriWarps][kOriBins][32];
-  __shared__ float s_bins[kOriWarps][kOriBins];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t i = blockIdx.x * kOriWarps + warp;
-  if (i >= *P.sel_count) return;
+// Orientations of selected keypoint i of image P, one warp (hist, bins: the
+// warp's shared-memory histograms).
+__device__ void orient_one(const ImagePlan& P, const DescribeParams& prm, uint32_t i, float (*hist)[32],
+                           float* bins_w) {
+  const int lane = threadIdx.x & 31;
   const psift_keypoint kp = P.sel[i];
   OctKp ok = to_octave(P, kp);
   ok.l = resolve_layer(kp, ok.o, prm.scales);
@@ -95,7 +94,6 @@ __global__ void __launch_bounds__(kOriWarps * 32) orientation_kernel(const Image
   const float* g = O.g + (long long)ok.l * O.plane_stride;
   const float two_pi = 2.0f * kPiF;
 
-  float (*hist)[32] = s_hist[warp];
   for (int b = 0; b < kOriBins; ++b) hist[b][lane] = 0.0f;
 
   const float sigma_ori = fmaxf(1.5f * ok.scale, 1.0f);
@@ -128,11 +126,11 @@ __global__ void __launch_bounds__(kOriWarps * 32) orientation_kernel(const Image
   for (int b = lane; b < kOriBins; b += 32) {
     float s = 0.0f;
     for (int j = 0; j < 32; ++j) s += hist[b][j];
-    s_bins[warp][b] = s;
+    bins_w[b] = s;
   }
   __syncwarp();
   if (lane != 0) return;
-  const float* hb = s_bins[warp];
+  const float* hb = bins_w;
   float sm[kOriBins];
   for (int b = 0; b < kOriBins; ++b) {
     const float prev = hb[(b + kOriBins - 1) % kOriBins];
@@ -196,6 +194,24 @@ __global__ void __launch_bounds__(kOriWarps * 32) orientation_kernel(const Image
     out[q] = rem_2pi(th, two_pi);
   }
   P.ori_count[i] = (uint32_t)np;
+}
+
+// Grid (min(keypoint capacity, kKpPerLaunchRow) / 8, images): warp w of CTA b
+// takes selected keypoints 8b + w, then a grid-width further on, of image
+// blockIdx.y.  Capacity-sized rows keep one warp per keypoint when the cap is
+// small; an uncapped batch (capacity 2^18) gets bounded rows instead of
+// millions of empty CTAs.
+__global__ void __launch_bounds__(kOriWarps * 32) orientation_kernel(const ImagePlan* __restrict__ plans,
+                                                                     DescribeParams prm) {
+  __shared__ float s_hist[kOriWarps][kOriBins][32];
+  __shared__ float s_bins[kOriWarps][kOriBins];
+  const int warp = threadIdx.x >> 5;
+  const ImagePlan& P = plans[blockIdx.y];
+  const uint32_t cnt = *P.sel_count, stride = gridDim.x * kOriWarps;
+  for (uint32_t i = blockIdx.x * kOriWarps + warp; i < cnt; i += stride) {
+    orient_one(P, prm, i, s_hist[warp], s_bins[warp]);
+    __syncwarp();
+  }
 }
 
 // Exclusive offsets of orientations per keypoint; feature count = min(total, cap).
@@ -267,18 +283,14 @@ __device__ __forceinline__ float block_sum128(float v, float* s_red) {
   return (s_red[0] + s_red[1]) + (s_red[2] + s_red[3]);
 }
 
-__global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const ImagePlan* __restrict__ plans,
-                                                                     DescribeParams prm) {
+// Descriptors of selected keypoint i of image P, the whole CTA (base_smem: the
+// CTA's dynamic shared memory); returns with the CTA converged.
+__device__ void describe_one(const ImagePlan& P, const DescribeParams& prm, uint32_t i, char* base_smem) {
   static_assert(kDescWarps == 4, "one thread per bin in the final sums");
-  const ImagePlan& P = plans[blockIdx.y];
-  extern __shared__ float4 s_dyn4[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t i = blockIdx.x;
-  if (i >= *P.sel_count) return;
   const uint32_t fcount = *P.feat_count;
   const uint32_t f0 = P.feat_offsets[i];
   if (f0 >= fcount) return;
-  char* base_smem = reinterpret_cast<char*>(s_dyn4);
   char* wbase = base_smem + warp * kDescWarpSmem;
   float (*hist)[kHistCols] = reinterpret_cast<float (*)[kHistCols]>(wbase);
   uint32_t* queue = reinterpret_cast<uint32_t*>(wbase + kDescLen * kHistCols * 4);
@@ -452,9 +464,23 @@ __global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const Image
   }
 }
 
+// Grid (min(keypoint capacity, kKpPerLaunchRow), images): CTA b takes selected
+// keypoint b, then a grid-width further on, of image blockIdx.y (see
+// orientation_kernel); every output slot is fixed by the keypoint's feature
+// offset, so the result does not depend on which CTA computes it.
+__global__ void __launch_bounds__(kDescWarps * 32) descriptor_kernel(const ImagePlan* __restrict__ plans,
+                                                                     DescribeParams prm) {
+  extern __shared__ float4 s_dyn4[];
+  char* base_smem = reinterpret_cast<char*>(s_dyn4);
+  const ImagePlan& P = plans[blockIdx.y];
+  const uint32_t cnt = *P.sel_count;
+  for (uint32_t i = blockIdx.x; i < cnt; i += gridDim.x) describe_one(P, prm, i, base_smem);
+}
+
 cudaError_t launch_orientation(const ImagePlan* plans, int n, uint32_t sel_cap, const DescribeParams& prm,
                                cudaStream_t st) {
-  dim3 grid((sel_cap + kOriWarps - 1) / kOriWarps, n);
+  const uint32_t row = std::min<uint32_t>(std::max<uint32_t>(sel_cap, 1), kKpPerLaunchRow);
+  dim3 grid((row + kOriWarps - 1) / kOriWarps, n);
   orientation_kernel<<<grid, kOriWarps * 32, 0, st>>>(plans, prm);
   return cudaGetLastError();
 }
@@ -469,7 +495,7 @@ cudaError_t launch_descriptor(const ImagePlan* plans, int n, uint32_t sel_cap, c
   const size_t smem = kDescSmem;
   cudaError_t e = ensure_smem_attr((const void*)descriptor_kernel, smem);
   if (e != cudaSuccess) return e;
-  dim3 grid(sel_cap, n);
+  dim3 grid(std::min<uint32_t>(std::max<uint32_t>(sel_cap, 1), kKpPerLaunchRow), n);
   descriptor_kernel<<<grid, kDescWarps * 32, smem, st>>>(plans, prm);
   return cudaGetLastError();
 }
