@@ -89,6 +89,13 @@ def lib():
             L.oracle_detect_keypoints.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                                   C.c_int, C.c_void_p, C.c_int]
             L.oracle_detect_keypoints.restype = C.c_int
+            _dp = C.POINTER(C.c_double)
+            L.oracle_detect_and_compute_f64.argtypes = [_u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                                        C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_int]
+            L.oracle_detect_and_compute_f64.restype = C.c_int
+            L.oracle_detect_keypoints_f64.argtypes = [_u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                                      C.c_int, _dp, C.c_int]
+            L.oracle_detect_keypoints_f64.restype = C.c_int
             L.oracle_compute_descriptors.argtypes = [_fp, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                                      _fp, _fp, C.c_int]
             L.oracle_compute_descriptors.restype = C.c_int
@@ -229,6 +236,38 @@ def detect_and_compute(img, octaves=3, scales=3, threshold=0.015, upsample=True,
         n = lib().oracle_detect_and_compute(_p(img, _fp), img.shape[0], img.shape[1], octaves, scales,
                                             threshold, int(bool(upsample)), int(kind), int(max_features),
                                             _p(meta, _fp), _p(desc, _fp), cap)
+        if n <= cap:
+            return meta[:n].copy(), desc[:n].copy()
+        cap = n
+
+
+def detect_keypoints_f64(luma_u8, octaves=3, scales=3, threshold=0.015, upsample=True) -> np.ndarray:
+    """The keypoints of the pipeline run in f64 from the u8 luma: (n, 6) float64
+    rows (x, y, scale, response, octave, layer)."""
+    u8 = np.ascontiguousarray(luma_u8, dtype=np.uint8)
+    dp = C.POINTER(C.c_double)
+    cap = 1 << 16
+    while True:
+        out = np.zeros((cap, 6), np.float64)
+        n = lib().oracle_detect_keypoints_f64(_p(u8, _u8p), u8.shape[0], u8.shape[1], octaves, scales,
+                                              threshold, int(bool(upsample)), _p(out, dp), cap)
+        if n <= cap:
+            return out[:n].copy()
+        cap = n
+
+
+def detect_and_compute_f64(luma_u8, octaves=3, scales=3, threshold=0.015, upsample=True, kind=0,
+                           max_features=4096):
+    """The pipeline run in f64 from the u8 luma: (meta[n,5], desc[n,128]) float64."""
+    u8 = np.ascontiguousarray(luma_u8, dtype=np.uint8)
+    dp = C.POINTER(C.c_double)
+    cap = max(max_features, 1) if max_features > 0 else 1 << 15
+    while True:
+        meta = np.zeros((cap, 5), np.float64)
+        desc = np.zeros((cap, 128), np.float64)
+        n = lib().oracle_detect_and_compute_f64(_p(u8, _u8p), u8.shape[0], u8.shape[1], octaves, scales,
+                                                threshold, int(bool(upsample)), int(kind), int(max_features),
+                                                _p(meta, dp), _p(desc, dp), cap)
         if n <= cap:
             return meta[:n].copy(), desc[:n].copy()
         cap = n

@@ -22,122 +22,143 @@
 namespace {
 
 constexpr float BASE_SIGMA = 1.6f;            // src/pipeline.rs:10
-constexpr float ASSUMED_INPUT_SIGMA = 0.5f;   // src/pipeline.rs:13
 constexpr float PI_F = 3.14159265358979323846f;
-constexpr float SQRT_2_F = 1.41421356237309504880f;
 constexpr size_t DESC_LEN = 128;              // src/pipeline.rs:1000
-constexpr float SECONDARY_ORI_PEAK_RATIO = 0.80f;  // src/pipeline.rs:1155
 constexpr float RAD_TO_DEG_F = 57.2957795130823208767981548141051703f;
 constexpr int PAR_MIN_PIXELS = 16384;         // src/pipeline.rs:381,:410,:901
 
-struct Plane {
+// The detection path (pyramid, extrema, orientations, descriptors) is written
+// once over the arithmetic type T.  T = float is the restatement of the
+// reference's f32 arithmetic; T = double runs the same algorithm with every
+// value, constant and libm call in f64, the yardstick that the f32 results
+// (the reference's and the GPU's) state their error against.  lit<T>(f, d)
+// picks the f32 literal as written in the reference for float and the same
+// decimal constant in f64 for double.
+template <typename T> constexpr T lit(float f, double d);
+template <> constexpr float lit<float>(float f, double) { return f; }
+template <> constexpr double lit<double>(float, double d) { return d; }
+#define K(x) lit<T>(x##f, x)
+
+template <typename T> constexpr T base_sigma() { return K(1.6); }           // src/pipeline.rs:10
+template <typename T> constexpr T assumed_input_sigma() { return K(0.5); }  // src/pipeline.rs:13
+template <typename T> constexpr T pi_t() { return K(3.14159265358979323846); }
+template <typename T> constexpr T sqrt_2_t() { return K(1.41421356237309504880); }
+template <typename T> constexpr T secondary_ori_peak_ratio() { return K(0.80); }  // src/pipeline.rs:1155
+
+template <typename T>
+struct PlaneT {
   int h = 0, w = 0;
-  std::vector<float> d;
-  Plane() = default;
-  Plane(int hh, int ww) : h(hh), w(ww), d((size_t)hh * ww, 0.0f) {}
-  float* row(int y) { return d.data() + (size_t)y * w; }
-  const float* row(int y) const { return d.data() + (size_t)y * w; }
+  std::vector<T> d;
+  PlaneT() = default;
+  PlaneT(int hh, int ww) : h(hh), w(ww), d((size_t)hh * ww, T(0)) {}
+  T* row(int y) { return d.data() + (size_t)y * w; }
+  const T* row(int y) const { return d.data() + (size_t)y * w; }
 };
+using Plane = PlaneT<float>;
 
-struct Octave {
-  std::vector<Plane> g, dog;
-  float scale_factor = 1.0f;
+template <typename T>
+struct OctaveT {
+  std::vector<PlaneT<T>> g, dog;
+  T scale_factor = T(1);
 };
+using Octave = OctaveT<float>;
 
-// Rust `f32::rem_euclid`: r = a % b; if r < 0 { r + |b| } else { r }.
-inline float rem_euclid_f(float a, float b) {
-  float r = std::fmod(a, b);
-  return r < 0.0f ? r + std::fabs(b) : r;
+// Keypoint record: the C struct for f32, the same fields in f64 otherwise.
+struct keypoint_f64 {
+  double x, y, scale, response;
+  uint32_t octave, layer;
+};
+template <typename T> struct KpOf { using type = oracle_keypoint; };
+template <> struct KpOf<double> { using type = keypoint_f64; };
+template <typename T> using KpT = typename KpOf<T>::type;
+
+// Rust `f32::rem_euclid` / `f64::rem_euclid`: r = a % b; if r < 0 { r + |b| } else { r }.
+template <typename T> inline T rem_euclid(T a, T b) {
+  T r = std::fmod(a, b);
+  return r < T(0) ? r + std::fabs(b) : r;
 }
+inline float rem_euclid_f(float a, float b) { return rem_euclid<float>(a, b); }
 
-// Rust `f32::clamp(lo, hi)`.
-inline float clampf(float x, float lo, float hi) {
+// Rust `clamp(lo, hi)`.
+template <typename T> inline T clampt(T x, T lo, T hi) {
   if (x < lo) x = lo;
   if (x > hi) x = hi;
   return x;
 }
+inline float clampf(float x, float lo, float hi) { return clampt<float>(x, lo, hi); }
 
-// Rust `f32 as isize` / `as usize`: saturating, NaN -> 0.
-inline long long f2i_sat(float v) {
+// Rust `as isize` / `as usize` from a float: saturating, NaN -> 0.
+template <typename T> inline long long to_i_sat(T v) {
   if (std::isnan(v)) return 0;
-  if (v >= 9.2233720368547758e18f) return std::numeric_limits<long long>::max();
-  if (v <= -9.2233720368547758e18f) return std::numeric_limits<long long>::min();
+  if (v >= T(9.2233720368547758e18)) return std::numeric_limits<long long>::max();
+  if (v <= T(-9.2233720368547758e18)) return std::numeric_limits<long long>::min();
   return (long long)v;
 }
-inline unsigned long long f2u_sat(float v) {
-  if (std::isnan(v) || v <= 0.0f) return 0;
-  if (v >= 1.8446744073709552e19f) return std::numeric_limits<unsigned long long>::max();
+template <typename T> inline unsigned long long to_u_sat(T v) {
+  if (std::isnan(v) || v <= T(0)) return 0;
+  if (v >= T(1.8446744073709552e19)) return std::numeric_limits<unsigned long long>::max();
   return (unsigned long long)v;
 }
-inline unsigned long long d2u_sat(double v) {
-  if (std::isnan(v) || v <= 0.0) return 0;
-  if (v >= 1.8446744073709552e19) return std::numeric_limits<unsigned long long>::max();
-  return (unsigned long long)v;
-}
+inline long long f2i_sat(float v) { return to_i_sat<float>(v); }
+inline unsigned long long f2u_sat(float v) { return to_u_sat<float>(v); }
+inline unsigned long long d2u_sat(double v) { return to_u_sat<double>(v); }
 
-// `f32::powi(i32)` lowers to the compiler runtime's binary exponentiation
-// (square-and-multiply, low bit first); restated here.
-inline float powi_f(float a, int b) {
+// `f32::powi(i32)` / `f64::powi` lower to the compiler runtime's binary
+// exponentiation (square-and-multiply, low bit first); restated here.
+template <typename T> inline T powi_t(T a, int b) {
   const bool recip = b < 0;
-  float r = 1.0f;
+  T r = T(1);
   for (;;) {
     if (b & 1) r *= a;
     b /= 2;
     if (b == 0) break;
     a *= a;
   }
-  return recip ? 1.0f / r : r;
+  return recip ? T(1) / r : r;
 }
-inline double powi_d(double a, int b) {
-  const bool recip = b < 0;
-  double r = 1.0;
-  for (;;) {
-    if (b & 1) r *= a;
-    b /= 2;
-    if (b == 0) break;
-    a *= a;
-  }
-  return recip ? 1.0 / r : r;
-}
+inline float powi_f(float a, int b) { return powi_t<float>(a, b); }
+inline double powi_d(double a, int b) { return powi_t<double>(a, b); }
 
 // src/pipeline.rs:275-296
-std::vector<float> gaussian_kernel_1d(float sigma) {
-  const float cs = std::fmax(sigma, 1e-3f);
-  long long radius = f2i_sat(std::ceil(3.0f * cs));
+template <typename T>
+std::vector<T> gaussian_kernel_1d(T sigma) {
+  const T cs = std::fmax(sigma, K(1e-3));
+  long long radius = to_i_sat<T>(std::ceil(K(3.0) * cs));
   if (radius < 1) radius = 1;
-  const float two_sigma_sq = 2.0f * cs * cs;
-  const float norm_factor = 1.0f / (std::sqrt(2.0f * PI_F) * cs);
-  std::vector<float> k;
+  const T two_sigma_sq = K(2.0) * cs * cs;
+  const T norm_factor = K(1.0) / (std::sqrt(K(2.0) * pi_t<T>()) * cs);
+  std::vector<T> k;
   k.reserve((size_t)(2 * radius + 1));
   for (long long x = -radius; x <= radius; ++x) {
-    const float xf = (float)x;
+    const T xf = (T)x;
     k.push_back(norm_factor * std::exp(-((xf * xf) / two_sigma_sq)));
   }
-  float sum = 0.0f;
-  for (float v : k) sum += v;
-  if (sum > 0.0f) {
-    const float inv = 1.0f / sum;
-    for (float& v : k) v *= inv;
+  T sum = T(0);
+  for (T v : k) sum += v;
+  if (sum > T(0)) {
+    const T inv = K(1.0) / sum;
+    for (T& v : k) v *= inv;
   }
   return k;
 }
 
 // src/pipeline.rs:314-425 (horizontal pass :329-377, vertical AXPY pass :395-406).
-Plane gaussian_blur(const Plane& img, float sigma) {
+template <typename T>
+PlaneT<T> gaussian_blur(const PlaneT<T>& img, T sigma) {
   const int h = img.h, w = img.w;
-  if (h == 0 || w == 0) return Plane(h, w);
-  const std::vector<float> kernel = gaussian_kernel_1d(sigma);
+  if (h == 0 || w == 0) return PlaneT<T>(h, w);
+  const std::vector<T> kernel = gaussian_kernel_1d<T>(sigma);
   const int klen = (int)kernel.size();
   const int radius = klen / 2;
   const bool par = (long long)h * w >= PAR_MIN_PIXELS;
 
-  Plane temp(h, w);
+  PlaneT<T> temp(h, w);
 #pragma omp parallel for schedule(static) if (par)
   for (int y = 0; y < h; ++y) {
-    const float* in_row = img.row(y);
-    float* out_row = temp.row(y);
+    const T* in_row = img.row(y);
+    T* out_row = temp.row(y);
     for (int x = 0; x < w; ++x) {
-      float acc = 0.0f;
+      T acc = T(0);
       for (int k = 0; k < klen; ++k) {
         int sx = x + k - radius;            // (x + k).saturating_sub(r).min(w-1)
         if (sx < 0) sx = 0;
@@ -148,16 +169,16 @@ Plane gaussian_blur(const Plane& img, float sigma) {
     }
   }
 
-  Plane dst(h, w);
+  PlaneT<T> dst(h, w);
 #pragma omp parallel for schedule(static) if (par)
   for (int y = 0; y < h; ++y) {
-    float* out_row = dst.row(y);
+    T* out_row = dst.row(y);
     for (int k = 0; k < klen; ++k) {
       int sy = y + k - radius;
       if (sy < 0) sy = 0;
       if (sy > h - 1) sy = h - 1;
-      const float* in_row = temp.row(sy);
-      const float wgt = kernel[k];
+      const T* in_row = temp.row(sy);
+      const T wgt = kernel[k];
       for (int x = 0; x < w; ++x) out_row[x] += in_row[x] * wgt;
     }
   }
@@ -165,70 +186,74 @@ Plane gaussian_blur(const Plane& img, float sigma) {
 }
 
 // src/pipeline.rs:429-449
-Plane downsample_2x(const Plane& img) {
+template <typename T>
+PlaneT<T> downsample_2x(const PlaneT<T>& img) {
   const int nh = img.h / 2, nw = img.w / 2;
-  if (nh == 0 || nw == 0) return Plane(0, 0);
-  Plane out(nh, nw);
+  if (nh == 0 || nw == 0) return PlaneT<T>(0, 0);
+  PlaneT<T> out(nh, nw);
   for (int y = 0; y < nh; ++y)
     for (int x = 0; x < nw; ++x) out.row(y)[x] = img.row(2 * y)[2 * x];
   return out;
 }
 
 // src/pipeline.rs:455-483
-Plane upsample_2x_bilinear(const Plane& img) {
+template <typename T>
+PlaneT<T> upsample_2x_bilinear(const PlaneT<T>& img) {
   const int h = img.h, w = img.w;
   const int nh = h * 2, nw = w * 2;
-  if (nh == 0 || nw == 0) return Plane(0, 0);
-  Plane out(nh, nw);
+  if (nh == 0 || nw == 0) return PlaneT<T>(0, 0);
+  PlaneT<T> out(nh, nw);
   for (int uy = 0; uy < nh; ++uy) {
     const int y0 = uy / 2;
     const int y1 = std::min(y0 + (uy & 1), h - 1);
-    const float* r0 = img.row(y0);
-    const float* r1 = img.row(y1);
-    float* o = out.row(uy);
+    const T* r0 = img.row(y0);
+    const T* r1 = img.row(y1);
+    T* o = out.row(uy);
     for (int ux = 0; ux < nw; ++ux) {
       const int x0 = ux / 2;
       const int x1 = std::min(x0 + (ux & 1), w - 1);
-      o[ux] = 0.25f * (r0[x0] + r0[x1] + r1[x0] + r1[x1]);
+      o[ux] = K(0.25) * (r0[x0] + r0[x1] + r1[x0] + r1[x1]);
     }
   }
   return out;
 }
 
 // src/pipeline.rs:550-638
-std::vector<Octave> build_pyramid(const Plane& img, int octaves, int scales, bool upsample) {
-  std::vector<Octave> pyr;
+template <typename T>
+std::vector<OctaveT<T>> build_pyramid(const PlaneT<T>& img, int octaves, int scales, bool upsample) {
+  std::vector<OctaveT<T>> pyr;
   if (img.h == 0 || img.w == 0 || octaves == 0 || scales == 0) return pyr;
   const int dog_slices = scales + 2;
-  const float k = std::pow(2.0f, 1.0f / (float)scales);
+  const T k = std::pow(K(2.0), K(1.0) / (T)scales);
+  const T bs = base_sigma<T>();
 
-  Plane base;
-  float base_mult;
+  PlaneT<T> base;
+  T base_mult;
   if (upsample) {
-    Plane up = upsample_2x_bilinear(img);
-    const float sigma_in = 2.0f * ASSUMED_INPUT_SIGMA;
-    const float init_sigma = std::sqrt(std::fmax(BASE_SIGMA * BASE_SIGMA - sigma_in * sigma_in, 1e-4f));
+    PlaneT<T> up = upsample_2x_bilinear(img);
+    const T sigma_in = K(2.0) * assumed_input_sigma<T>();
+    const T init_sigma = std::sqrt(std::fmax(bs * bs - sigma_in * sigma_in, K(1e-4)));
     base = gaussian_blur(up, init_sigma);
-    base_mult = 0.5f;
+    base_mult = K(0.5);
   } else {
-    const float sigma_in = ASSUMED_INPUT_SIGMA;
-    const float init_sigma = std::sqrt(std::fmax(BASE_SIGMA * BASE_SIGMA - sigma_in * sigma_in, 1e-4f));
+    const T sigma_in = assumed_input_sigma<T>();
+    const T init_sigma = std::sqrt(std::fmax(bs * bs - sigma_in * sigma_in, K(1e-4)));
     base = gaussian_blur(img, init_sigma);
-    base_mult = 1.0f;
+    base_mult = K(1.0);
   }
 
   for (int o = 0; o < octaves; ++o) {
     const int h = base.h, w = base.w;
     if (h < 3 || w < 3) break;
-    Octave oct;
+    OctaveT<T> oct;
     oct.g.push_back(base);
-    float prev_sigma = BASE_SIGMA;
+    T prev_sigma = bs;
     for (int s = 1; s <= dog_slices; ++s) {
-      const float target = BASE_SIGMA * powi_f(k, s);
-      const float delta = std::sqrt(std::fmax(target * target - prev_sigma * prev_sigma, 1e-4f));
-      Plane next = gaussian_blur(oct.g.back(), delta);
-      Plane dog(h, w);
-      const Plane& prev = oct.g.back();
+      const T target = bs * powi_t<T>(k, s);
+      const T delta = std::sqrt(std::fmax(target * target - prev_sigma * prev_sigma, K(1e-4)));
+      PlaneT<T> next = gaussian_blur(oct.g.back(), delta);
+      PlaneT<T> dog(h, w);
+      const PlaneT<T>& prev = oct.g.back();
       for (size_t i = 0; i < dog.d.size(); ++i) dog.d[i] = next.d[i] - prev.d[i];
       oct.dog.push_back(std::move(dog));
       oct.g.push_back(std::move(next));
@@ -236,132 +261,137 @@ std::vector<Octave> build_pyramid(const Plane& img, int octaves, int scales, boo
     }
     if (o + 1 < octaves) base = downsample_2x(oct.g[scales]);
     else base = oct.g.back();
-    oct.scale_factor = base_mult * (float)(1ull << o);
+    oct.scale_factor = base_mult * (T)(1ull << o);
     pyr.push_back(std::move(oct));
   }
   return pyr;
 }
 
 // src/pipeline.rs:664-687
-bool passes_hessian_edge_test(const Plane& c, int x, int y, float center) {
-  const float* rp = c.row(y - 1);
-  const float* rc = c.row(y);
-  const float* rn = c.row(y + 1);
-  const float dxx = rc[x + 1] - 2.0f * center + rc[x - 1];
-  const float dyy = rn[x] - 2.0f * center + rp[x];
-  const float dxy = 0.25f * ((rn[x + 1] - rn[x - 1]) - (rp[x + 1] - rp[x - 1]));
-  const float trace = dxx + dyy;
-  const float det = dxx * dyy - dxy * dxy;
-  const float threshold_ratio = (11.0f * 11.0f) / 10.0f;
-  return det > 1e-9f && (trace * trace) < threshold_ratio * det;
+template <typename T>
+bool passes_hessian_edge_test(const PlaneT<T>& c, int x, int y, T center) {
+  const T* rp = c.row(y - 1);
+  const T* rc = c.row(y);
+  const T* rn = c.row(y + 1);
+  const T dxx = rc[x + 1] - K(2.0) * center + rc[x - 1];
+  const T dyy = rn[x] - K(2.0) * center + rp[x];
+  const T dxy = K(0.25) * ((rn[x + 1] - rn[x - 1]) - (rp[x + 1] - rp[x - 1]));
+  const T trace = dxx + dyy;
+  const T det = dxx * dyy - dxy * dxy;
+  const T threshold_ratio = (K(11.0) * K(11.0)) / K(10.0);
+  return det > K(1e-9) && (trace * trace) < threshold_ratio * det;
 }
 
 // src/pipeline.rs:697-770
-void refine_extremum_3d(const Plane& p, const Plane& c, const Plane& n, int x, int y, float& ox_out,
-                        float& oy_out, float& os_out, float& interp_out) {
-  const float* c_prev = c.row(y - 1);
-  const float* c_curr = c.row(y);
-  const float* c_next = c.row(y + 1);
-  const float* p_prev = p.row(y - 1);
-  const float* p_curr = p.row(y);
-  const float* p_next = p.row(y + 1);
-  const float* n_prev = n.row(y - 1);
-  const float* n_curr = n.row(y);
-  const float* n_next = n.row(y + 1);
-  const float center = c_curr[x];
+template <typename T>
+void refine_extremum_3d(const PlaneT<T>& p, const PlaneT<T>& c, const PlaneT<T>& n, int x, int y, T& ox_out,
+                        T& oy_out, T& os_out, T& interp_out) {
+  const T* c_prev = c.row(y - 1);
+  const T* c_curr = c.row(y);
+  const T* c_next = c.row(y + 1);
+  const T* p_prev = p.row(y - 1);
+  const T* p_curr = p.row(y);
+  const T* p_next = p.row(y + 1);
+  const T* n_prev = n.row(y - 1);
+  const T* n_curr = n.row(y);
+  const T* n_next = n.row(y + 1);
+  const T center = c_curr[x];
 
-  const float gx = 0.5f * (c_curr[x + 1] - c_curr[x - 1]);
-  const float gy = 0.5f * (c_next[x] - c_prev[x]);
-  const float gs = 0.5f * (n_curr[x] - p_curr[x]);
+  const T gx = K(0.5) * (c_curr[x + 1] - c_curr[x - 1]);
+  const T gy = K(0.5) * (c_next[x] - c_prev[x]);
+  const T gs = K(0.5) * (n_curr[x] - p_curr[x]);
 
-  const float dxx = c_curr[x + 1] - 2.0f * center + c_curr[x - 1];
-  const float dyy = c_next[x] - 2.0f * center + c_prev[x];
-  const float dss = n_curr[x] - 2.0f * center + p_curr[x];
+  const T dxx = c_curr[x + 1] - K(2.0) * center + c_curr[x - 1];
+  const T dyy = c_next[x] - K(2.0) * center + c_prev[x];
+  const T dss = n_curr[x] - K(2.0) * center + p_curr[x];
 
-  const float dxy = 0.25f * ((c_next[x + 1] - c_next[x - 1]) - (c_prev[x + 1] - c_prev[x - 1]));
-  const float dxs = 0.25f * ((n_curr[x + 1] - n_curr[x - 1]) - (p_curr[x + 1] - p_curr[x - 1]));
-  const float dys = 0.25f * ((n_next[x] - n_prev[x]) - (p_next[x] - p_prev[x]));
+  const T dxy = K(0.25) * ((c_next[x + 1] - c_next[x - 1]) - (c_prev[x + 1] - c_prev[x - 1]));
+  const T dxs = K(0.25) * ((n_curr[x + 1] - n_curr[x - 1]) - (p_curr[x + 1] - p_curr[x - 1]));
+  const T dys = K(0.25) * ((n_next[x] - n_prev[x]) - (p_next[x] - p_prev[x]));
 
-  const float c00 = dyy * dss - dys * dys;
-  const float c01 = dys * dxs - dxy * dss;
-  const float c02 = dxy * dys - dyy * dxs;
-  const float c11 = dxx * dss - dxs * dxs;
-  const float c12 = dxy * dxs - dxx * dys;
-  const float c22 = dxx * dyy - dxy * dxy;
+  const T c00 = dyy * dss - dys * dys;
+  const T c01 = dys * dxs - dxy * dss;
+  const T c02 = dxy * dys - dyy * dxs;
+  const T c11 = dxx * dss - dxs * dxs;
+  const T c12 = dxy * dxs - dxx * dys;
+  const T c22 = dxx * dyy - dxy * dxy;
 
-  const float det3 = dxx * c00 + dxy * c01 + dxs * c02;
-  if (std::fabs(det3) > 1e-9f) {
-    const float inv_det = -1.0f / det3;
-    const float ox = (c00 * gx + c01 * gy + c02 * gs) * inv_det;
-    const float oy = (c01 * gx + c11 * gy + c12 * gs) * inv_det;
-    const float os = (c02 * gx + c12 * gy + c22 * gs) * inv_det;
-    if (std::fabs(ox) <= 0.5f && std::fabs(oy) <= 0.5f && std::fabs(os) <= 0.5f) {
+  const T det3 = dxx * c00 + dxy * c01 + dxs * c02;
+  if (std::fabs(det3) > K(1e-9)) {
+    const T inv_det = K(-1.0) / det3;
+    const T ox = (c00 * gx + c01 * gy + c02 * gs) * inv_det;
+    const T oy = (c01 * gx + c11 * gy + c12 * gs) * inv_det;
+    const T os = (c02 * gx + c12 * gy + c22 * gs) * inv_det;
+    if (std::fabs(ox) <= K(0.5) && std::fabs(oy) <= K(0.5) && std::fabs(os) <= K(0.5)) {
       ox_out = ox;
       oy_out = oy;
       os_out = os;
-      interp_out = center + 0.5f * (gx * ox + gy * oy + gs * os);
+      interp_out = center + K(0.5) * (gx * ox + gy * oy + gs * os);
       return;
     }
   }
-  if (std::fabs(c22) > 1e-9f) {
-    const float inv_det2 = -1.0f / c22;
-    const float ox = clampf((dyy * gx - dxy * gy) * inv_det2, -0.5f, 0.5f);
-    const float oy = clampf((-dxy * gx + dxx * gy) * inv_det2, -0.5f, 0.5f);
-    const float os = std::fabs(dss) > 1e-6f ? clampf(-gs / dss, -0.5f, 0.5f) : 0.0f;
+  if (std::fabs(c22) > K(1e-9)) {
+    const T inv_det2 = K(-1.0) / c22;
+    const T ox = clampt<T>((dyy * gx - dxy * gy) * inv_det2, K(-0.5), K(0.5));
+    const T oy = clampt<T>((-dxy * gx + dxx * gy) * inv_det2, K(-0.5), K(0.5));
+    const T os = std::fabs(dss) > K(1e-6) ? clampt<T>(-gs / dss, K(-0.5), K(0.5)) : T(0);
     ox_out = ox;
     oy_out = oy;
     os_out = os;
-    interp_out = center + 0.5f * (gx * ox + gy * oy + gs * os);
+    interp_out = center + K(0.5) * (gx * ox + gy * oy + gs * os);
     return;
   }
-  ox_out = oy_out = os_out = 0.0f;
+  ox_out = oy_out = os_out = T(0);
   interp_out = center;
 }
 
-inline bool gt_patch(const Plane& pl, int x, int y, float v) {
-  const float* r0 = pl.row(y - 1);
-  const float* r1 = pl.row(y);
-  const float* r2 = pl.row(y + 1);
+template <typename T>
+inline bool gt_patch(const PlaneT<T>& pl, int x, int y, T v) {
+  const T* r0 = pl.row(y - 1);
+  const T* r1 = pl.row(y);
+  const T* r2 = pl.row(y + 1);
   return v > r0[x - 1] && v > r0[x] && v > r0[x + 1] && v > r1[x - 1] && v > r1[x] &&
          v > r1[x + 1] && v > r2[x - 1] && v > r2[x] && v > r2[x + 1];
 }
-inline bool lt_patch(const Plane& pl, int x, int y, float v) {
-  const float* r0 = pl.row(y - 1);
-  const float* r1 = pl.row(y);
-  const float* r2 = pl.row(y + 1);
+template <typename T>
+inline bool lt_patch(const PlaneT<T>& pl, int x, int y, T v) {
+  const T* r0 = pl.row(y - 1);
+  const T* r1 = pl.row(y);
+  const T* r2 = pl.row(y + 1);
   return v < r0[x - 1] && v < r0[x] && v < r0[x + 1] && v < r1[x - 1] && v < r1[x] &&
          v < r1[x + 1] && v < r2[x - 1] && v < r2[x] && v < r2[x + 1];
 }
 
 // src/pipeline.rs:810-916
-void extract_extrema_in_octave(int octave_idx, const std::vector<Plane>& dogs, float mult,
-                               float threshold, std::vector<oracle_keypoint>& out) {
+template <typename T>
+void extract_extrema_in_octave(int octave_idx, const std::vector<PlaneT<T>>& dogs, T mult,
+                               T threshold, std::vector<KpT<T>>& out) {
   if (dogs.size() < 3) return;
   const int h = dogs[0].h, w = dogs[0].w;
   if (h < 3 || w < 3) return;
   const int searchable = std::max((int)dogs.size() - 2, 1);
-  const float k = std::pow(2.0f, 1.0f / (float)searchable);
+  const T k = std::pow(K(2.0), K(1.0) / (T)searchable);
   const int nslices = (int)dogs.size() - 2;
-  std::vector<std::vector<oracle_keypoint>> per_slice(nslices);
+  std::vector<std::vector<KpT<T>>> per_slice(nslices);
   const bool par = (long long)h * w >= PAR_MIN_PIXELS;
 
 #pragma omp parallel for schedule(dynamic, 1) if (par)
   for (int si = 0; si < nslices; ++si) {
     const int s = si + 1;
-    const Plane& prev = dogs[s - 1];
-    const Plane& curr = dogs[s];
-    const Plane& next = dogs[s + 1];
-    const float eff_scale = BASE_SIGMA * mult * powi_f(k, s);
+    const PlaneT<T>& prev = dogs[s - 1];
+    const PlaneT<T>& curr = dogs[s];
+    const PlaneT<T>& next = dogs[s + 1];
+    const T eff_scale = base_sigma<T>() * mult * powi_t<T>(k, s);
     auto& kps = per_slice[si];
     for (int y = 1; y < h - 1; ++y) {
-      const float* ra = curr.row(y - 1);
-      const float* rc = curr.row(y);
-      const float* rb = curr.row(y + 1);
+      const T* ra = curr.row(y - 1);
+      const T* rc = curr.row(y);
+      const T* rb = curr.row(y + 1);
       for (int x = 1; x < w - 1; ++x) {
-        const float v = rc[x];
+        const T v = rc[x];
         if (std::fabs(v) <= threshold) continue;
         bool ext;
-        if (v > 0.0f) {
+        if (v > T(0)) {
           ext = v > rc[x - 1] && v > rc[x + 1] && v > ra[x - 1] && v > ra[x] && v > ra[x + 1] &&
                 v > rb[x - 1] && v > rb[x] && v > rb[x + 1] && gt_patch(prev, x, y, v) &&
                 gt_patch(next, x, y, v);
@@ -371,18 +401,18 @@ void extract_extrema_in_octave(int octave_idx, const std::vector<Plane>& dogs, f
                 lt_patch(next, x, y, v);
         }
         if (ext && passes_hessian_edge_test(curr, x, y, v)) {
-          float dx, dy, ds, interp;
+          T dx, dy, ds, interp;
           refine_extremum_3d(prev, curr, next, x, y, dx, dy, ds, interp);
           if (std::fabs(interp) > threshold) {
-            const float refined_scale = eff_scale * std::pow(k, ds);
-            const float lf = clampf(std::round((float)s + ds), 1.0f, (float)searchable);
-            oracle_keypoint kp;
-            kp.x = ((float)x + dx) * mult;
-            kp.y = ((float)y + dy) * mult;
-            kp.scale = std::fmax(refined_scale, 0.25f * BASE_SIGMA);
+            const T refined_scale = eff_scale * std::pow(k, ds);
+            const T lf = clampt<T>(std::round((T)s + ds), K(1.0), (T)searchable);
+            KpT<T> kp;
+            kp.x = ((T)x + dx) * mult;
+            kp.y = ((T)y + dy) * mult;
+            kp.scale = std::fmax(refined_scale, K(0.25) * base_sigma<T>());
             kp.response = interp;
             kp.octave = (uint32_t)octave_idx;
-            kp.layer = (uint32_t)f2u_sat(lf);
+            kp.layer = (uint32_t)to_u_sat<T>(lf);
             kps.push_back(kp);
           }
         }
@@ -393,37 +423,40 @@ void extract_extrema_in_octave(int octave_idx, const std::vector<Plane>& dogs, f
 }
 
 // src/pipeline.rs:535-547
-std::vector<oracle_keypoint> pyramid_extract(const std::vector<Octave>& pyr, float thr) {
-  std::vector<oracle_keypoint> kps;
+template <typename T>
+std::vector<KpT<T>> pyramid_extract(const std::vector<OctaveT<T>>& pyr, T thr) {
+  std::vector<KpT<T>> kps;
   for (size_t o = 0; o < pyr.size(); ++o)
-    extract_extrema_in_octave((int)o, pyr[o].dog, pyr[o].scale_factor, thr, kps);
+    extract_extrema_in_octave<T>((int)o, pyr[o].dog, pyr[o].scale_factor, thr, kps);
   return kps;
 }
 
 // src/pipeline.rs:1158-1203
-struct GradPlanes {
+template <typename T>
+struct GradPlanesT {
   int octave, layer, w, h;
-  std::vector<float> mag, ang;
+  std::vector<T> mag, ang;
 };
-GradPlanes gradient_planes(int octave, int layer, const Plane& g) {
-  GradPlanes gp;
+template <typename T>
+GradPlanesT<T> gradient_planes(int octave, int layer, const PlaneT<T>& g) {
+  GradPlanesT<T> gp;
   gp.octave = octave;
   gp.layer = layer;
   gp.w = g.w;
   gp.h = g.h;
-  gp.mag.assign((size_t)g.h * g.w, 0.0f);
-  gp.ang.assign((size_t)g.h * g.w, 0.0f);
-  const float two_pi = 2.0f * PI_F;
+  gp.mag.assign((size_t)g.h * g.w, T(0));
+  gp.ang.assign((size_t)g.h * g.w, T(0));
+  const T two_pi = K(2.0) * pi_t<T>();
   if (g.h >= 3 && g.w >= 3) {
     for (int y = 1; y < g.h - 1; ++y) {
-      const float* ra = g.row(y - 1);
-      const float* rc = g.row(y);
-      const float* rb = g.row(y + 1);
+      const T* ra = g.row(y - 1);
+      const T* rc = g.row(y);
+      const T* rb = g.row(y + 1);
       for (int x = 1; x < g.w - 1; ++x) {
-        const float dx = rc[x + 1] - rc[x - 1];
-        const float dy = rb[x] - ra[x];
+        const T dx = rc[x + 1] - rc[x - 1];
+        const T dy = rb[x] - ra[x];
         gp.mag[(size_t)y * g.w + x] = std::sqrt(dx * dx + dy * dy);
-        gp.ang[(size_t)y * g.w + x] = rem_euclid_f(std::atan2(dy, dx), two_pi);
+        gp.ang[(size_t)y * g.w + x] = rem_euclid<T>(std::atan2(dy, dx), two_pi);
       }
     }
   }
@@ -431,8 +464,8 @@ GradPlanes gradient_planes(int octave, int layer, const Plane& g) {
 }
 
 // src/pipeline.rs:1206-1227
-void resolve_octave_and_layer(const oracle_keypoint& kp, const std::vector<Octave>& pyr, int& oct,
-                              int& layer) {
+template <typename T>
+void resolve_octave_and_layer(const KpT<T>& kp, const std::vector<OctaveT<T>>& pyr, int& oct, int& layer) {
   if (pyr.empty()) {
     oct = layer = 0;
     return;
@@ -441,76 +474,78 @@ void resolve_octave_and_layer(const oracle_keypoint& kp, const std::vector<Octav
   if (kp.layer > 0) {
     oct = std::min((int)kp.octave, nocts - 1);
   } else {
-    const float ratio = std::fmax(kp.scale / BASE_SIGMA, 1.0f);
-    oct = (int)std::min<unsigned long long>(f2u_sat(std::floor(std::log2(ratio))), (unsigned long long)(nocts - 1));
+    const T ratio = std::fmax(kp.scale / base_sigma<T>(), K(1.0));
+    oct = (int)std::min<unsigned long long>(to_u_sat<T>(std::floor(std::log2(ratio))),
+                                            (unsigned long long)(nocts - 1));
   }
   const int g_len = (int)pyr[oct].g.size();
   const int searchable = std::max(g_len - 3, 1);
   if (kp.layer > 0) {
     layer = std::min((int)kp.layer, g_len - 1);
   } else {
-    const float oct_mult = (float)(1ull << oct);
-    const float local_sigma = std::fmax(kp.scale / (BASE_SIGMA * oct_mult), 1.0f);
-    const unsigned long long l = f2u_sat(std::round(std::log2(local_sigma) * (float)searchable));
+    const T oct_mult = (T)(1ull << oct);
+    const T local_sigma = std::fmax(kp.scale / (base_sigma<T>() * oct_mult), K(1.0));
+    const unsigned long long l = to_u_sat<T>(std::round(std::log2(local_sigma) * (T)searchable));
     const int hi = std::max(g_len - 2, 1);
     layer = (int)std::min<unsigned long long>(std::max<unsigned long long>(l, 1ull), (unsigned long long)hi);
   }
 }
 
 // src/pipeline.rs:1233-1347
-std::vector<float> keypoint_orientations(const GradPlanes& gp, const oracle_keypoint& kp) {
+template <typename T>
+std::vector<T> keypoint_orientations(const GradPlanesT<T>& gp, const KpT<T>& kp) {
   const int NB = 36;
-  const float two_pi = 2.0f * PI_F;
-  const float sigma_ori = std::fmax(1.5f * kp.scale, 1.0f);
-  const float two_sigma_sq = 2.0f * sigma_ori * sigma_ori;
-  long long radius = f2i_sat(std::ceil(3.0f * sigma_ori));
+  const T two_pi = K(2.0) * pi_t<T>();
+  const T sigma_ori = std::fmax(K(1.5) * kp.scale, K(1.0));
+  const T two_sigma_sq = K(2.0) * sigma_ori * sigma_ori;
+  long long radius = to_i_sat<T>(std::ceil(K(3.0) * sigma_ori));
   if (radius < 2) radius = 2;
-  const long long cx = f2i_sat(std::round(kp.x));
-  const long long cy = f2i_sat(std::round(kp.y));
-  float hist[NB] = {0};
-  const float bin_scale = (float)NB / two_pi;
+  const long long cx = to_i_sat<T>(std::round(kp.x));
+  const long long cy = to_i_sat<T>(std::round(kp.y));
+  T hist[NB] = {0};
+  const T bin_scale = (T)NB / two_pi;
   const long long H = gp.h, W = gp.w;
   const long long y_min = std::max(cy - radius, 1ll);
   const long long y_max = std::max(std::min(cy + radius, H - 2), 1ll);
   const long long x_min = std::max(cx - radius, 1ll);
   const long long x_max = std::max(std::min(cx + radius, W - 2), 1ll);
-  const float r_sq_max = (float)(radius * radius);
+  const T r_sq_max = (T)(radius * radius);
   for (long long y = y_min; y <= y_max; ++y) {
-    const float dy = (float)(y - cy);
+    const T dy = (T)(y - cy);
     for (long long x = x_min; x <= x_max; ++x) {
-      const float dx = (float)(x - cx);
-      const float r_sq = dx * dx + dy * dy;
+      const T dx = (T)(x - cx);
+      const T r_sq = dx * dx + dy * dy;
       if (r_sq > r_sq_max) continue;
-      const float m = gp.mag[(size_t)(y * W + x)];
-      if (m <= 1e-7f) continue;
-      const float weight = std::exp(-r_sq / two_sigma_sq);
-      const float ang = gp.ang[(size_t)(y * W + x)];
-      const int bin = (int)(f2u_sat(std::floor(ang * bin_scale)) % NB);
+      const T m = gp.mag[(size_t)(y * W + x)];
+      if (m <= K(1e-7)) continue;
+      const T weight = std::exp(-r_sq / two_sigma_sq);
+      const T ang = gp.ang[(size_t)(y * W + x)];
+      const int bin = (int)(to_u_sat<T>(std::floor(ang * bin_scale)) % NB);
       hist[bin] += m * weight;
     }
   }
-  float sm[NB];
+  T sm[NB];
   for (int b = 0; b < NB; ++b) {
-    const float prev = hist[(b + NB - 1) % NB];
-    const float curr = hist[b];
-    const float next = hist[(b + 1) % NB];
-    sm[b] = (prev + curr + next) * (1.0f / 3.0f);
+    const T prev = hist[(b + NB - 1) % NB];
+    const T curr = hist[b];
+    const T next = hist[(b + 1) % NB];
+    sm[b] = (prev + curr + next) * (K(1.0) / K(3.0));
   }
   int best_bin = 0;
-  float best_val = sm[0];
+  T best_val = sm[0];
   for (int b = 1; b < NB; ++b)
     if (sm[b] > best_val) {
       best_val = sm[b];
       best_bin = b;
     }
-  if (best_val <= 1e-7f) return {0.0f};
-  const float split = SECONDARY_ORI_PEAK_RATIO * best_val;
-  std::vector<std::pair<int, float>> peaks;
+  if (best_val <= K(1e-7)) return {T(0)};
+  const T split = secondary_ori_peak_ratio<T>() * best_val;
+  std::vector<std::pair<int, T>> peaks;
   for (int b = 0; b < NB; ++b) {
-    const float v = sm[b];
+    const T v = sm[b];
     if (v < split) continue;
-    const float l = sm[(b + NB - 1) % NB];
-    const float r = sm[(b + 1) % NB];
+    const T l = sm[(b + NB - 1) % NB];
+    const T r = sm[(b + 1) % NB];
     if (v > l && v >= r) peaks.push_back({b, v});
   }
   if (peaks.empty()) {
@@ -523,74 +558,75 @@ std::vector<float> keypoint_orientations(const GradPlanes& gp, const oracle_keyp
     });
     if (peaks.size() > 4) peaks.resize(4);
   }
-  std::vector<float> oris;
+  std::vector<T> oris;
   for (const auto& pk : peaks) {
     const int bin = pk.first;
-    const float val = pk.second;
-    const float l = sm[(bin + NB - 1) % NB];
-    const float r = sm[(bin + 1) % NB];
-    const float denom = l - 2.0f * val + r;
-    float off = std::fabs(denom) > 1e-6f ? 0.5f * (l - r) / denom : 0.0f;
-    off = clampf(off, -0.5f, 0.5f);
-    oris.push_back(rem_euclid_f((((float)bin + 0.5f) + off) * (two_pi / (float)NB), two_pi));
+    const T val = pk.second;
+    const T l = sm[(bin + NB - 1) % NB];
+    const T r = sm[(bin + 1) % NB];
+    const T denom = l - K(2.0) * val + r;
+    T off = std::fabs(denom) > K(1e-6) ? K(0.5) * (l - r) / denom : T(0);
+    off = clampt<T>(off, K(-0.5), K(0.5));
+    oris.push_back(rem_euclid<T>((((T)bin + K(0.5)) + off) * (two_pi / (T)NB), two_pi));
   }
   return oris;
 }
 
 // src/pipeline.rs:1352-1480
-void descriptor_128(const GradPlanes& gp, const oracle_keypoint& kp, float orientation, float* desc) {
+template <typename T>
+void descriptor_128(const GradPlanesT<T>& gp, const KpT<T>& kp, T orientation, T* desc) {
   const int GW = 4;
-  const float two_pi = 2.0f * PI_F;
-  std::fill(desc, desc + DESC_LEN, 0.0f);
+  const T two_pi = K(2.0) * pi_t<T>();
+  std::fill(desc, desc + DESC_LEN, T(0));
   if (gp.w < 3 || gp.h < 3) return;
-  const float cos_t = std::cos(orientation);
-  const float sin_t = std::sin(orientation);
-  const float hist_width = std::fmax(3.0f * kp.scale, 1.5f);
-  const float inv_hw = 1.0f / hist_width;
-  const float exp_scale = -1.0f / (2.0f * 2.0f * 2.0f);
-  long long max_radius = f2i_sat(std::ceil(hist_width * SQRT_2_F * ((float)GW + 1.0f) * 0.5f));
+  const T cos_t = std::cos(orientation);
+  const T sin_t = std::sin(orientation);
+  const T hist_width = std::fmax(K(3.0) * kp.scale, K(1.5));
+  const T inv_hw = K(1.0) / hist_width;
+  const T exp_scale = K(-1.0) / (K(2.0) * K(2.0) * K(2.0));
+  long long max_radius = to_i_sat<T>(std::ceil(hist_width * sqrt_2_t<T>() * ((T)GW + K(1.0)) * K(0.5)));
   if (max_radius < 4) max_radius = 4;
-  const long long cx = f2i_sat(std::round(kp.x));
-  const long long cy = f2i_sat(std::round(kp.y));
+  const long long cx = to_i_sat<T>(std::round(kp.x));
+  const long long cy = to_i_sat<T>(std::round(kp.y));
   const long long H = gp.h, W = gp.w;
   const long long y_min = std::max(cy - max_radius, 1ll);
   const long long y_max = std::max(std::min(cy + max_radius, H - 2), 1ll);
   const long long x_min = std::max(cx - max_radius, 1ll);
   const long long x_max = std::max(std::min(cx + max_radius, W - 2), 1ll);
-  const float bin_per_rad = 8.0f / two_pi;
+  const T bin_per_rad = K(8.0) / two_pi;
   for (long long y = y_min; y <= y_max; ++y) {
-    const float dy = (float)y - kp.y;
+    const T dy = (T)y - kp.y;
     for (long long x = x_min; x <= x_max; ++x) {
-      const float dx = (float)x - kp.x;
-      const float r_rot = (dx * cos_t + dy * sin_t) * inv_hw;
-      const float c_rot = (-dx * sin_t + dy * cos_t) * inv_hw;
-      const float r_bin = r_rot + (float)GW * 0.5f - 0.5f;
-      const float c_bin = c_rot + (float)GW * 0.5f - 0.5f;
-      if (r_bin <= -1.0f || r_bin >= (float)GW || c_bin <= -1.0f || c_bin >= (float)GW) continue;
-      const float m = gp.mag[(size_t)(y * W + x)];
-      if (m <= 1e-7f) continue;
-      const float w_gauss = std::exp((r_rot * r_rot + c_rot * c_rot) * exp_scale);
-      const float wm = m * w_gauss;
-      const float rel = rem_euclid_f(gp.ang[(size_t)(y * W + x)] - orientation, two_pi);
-      const float o_bin = rel * bin_per_rad;
-      const long long r0 = f2i_sat(std::floor(r_bin));
-      const long long c0 = f2i_sat(std::floor(c_bin));
-      const long long o0 = f2i_sat(std::floor(o_bin));
-      const float dr = r_bin - (float)r0;
-      const float dc = c_bin - (float)c0;
-      const float dof = o_bin - (float)o0;
+      const T dx = (T)x - kp.x;
+      const T r_rot = (dx * cos_t + dy * sin_t) * inv_hw;
+      const T c_rot = (-dx * sin_t + dy * cos_t) * inv_hw;
+      const T r_bin = r_rot + (T)GW * K(0.5) - K(0.5);
+      const T c_bin = c_rot + (T)GW * K(0.5) - K(0.5);
+      if (r_bin <= K(-1.0) || r_bin >= (T)GW || c_bin <= K(-1.0) || c_bin >= (T)GW) continue;
+      const T m = gp.mag[(size_t)(y * W + x)];
+      if (m <= K(1e-7)) continue;
+      const T w_gauss = std::exp((r_rot * r_rot + c_rot * c_rot) * exp_scale);
+      const T wm = m * w_gauss;
+      const T rel = rem_euclid<T>(gp.ang[(size_t)(y * W + x)] - orientation, two_pi);
+      const T o_bin = rel * bin_per_rad;
+      const long long r0 = to_i_sat<T>(std::floor(r_bin));
+      const long long c0 = to_i_sat<T>(std::floor(c_bin));
+      const long long o0 = to_i_sat<T>(std::floor(o_bin));
+      const T dr = r_bin - (T)r0;
+      const T dc = c_bin - (T)c0;
+      const T dof = o_bin - (T)o0;
       for (int ir = 0; ir <= 1; ++ir) {
         const long long rb = r0 + ir;
         if (rb < 0 || rb >= GW) continue;
-        const float wr = ir == 0 ? 1.0f - dr : dr;
+        const T wr = ir == 0 ? K(1.0) - dr : dr;
         for (int ic = 0; ic <= 1; ++ic) {
           const long long cb = c0 + ic;
           if (cb < 0 || cb >= GW) continue;
-          const float wc = ic == 0 ? 1.0f - dc : dc;
+          const T wc = ic == 0 ? K(1.0) - dc : dc;
           for (int io = 0; io <= 1; ++io) {
             long long ob = (o0 + io) % 8;
             if (ob < 0) ob += 8;
-            const float wo = io == 0 ? 1.0f - dof : dof;
+            const T wo = io == 0 ? K(1.0) - dof : dof;
             const size_t idx = (size_t)((rb * GW + cb) * 8 + ob);
             desc[idx] += wm * wr * wc * wo;
           }
@@ -598,88 +634,91 @@ void descriptor_128(const GradPlanes& gp, const oracle_keypoint& kp, float orien
       }
     }
   }
-  float n1 = 0.0f;
+  T n1 = T(0);
   for (size_t i = 0; i < DESC_LEN; ++i) n1 += desc[i] * desc[i];
   n1 = std::sqrt(n1);
-  if (n1 > 1e-7f) {
-    const float inv1 = 1.0f / n1;
-    for (size_t i = 0; i < DESC_LEN; ++i) desc[i] = std::fmin(desc[i] * inv1, 0.2f);
-    float n2 = 0.0f;
+  if (n1 > K(1e-7)) {
+    const T inv1 = K(1.0) / n1;
+    for (size_t i = 0; i < DESC_LEN; ++i) desc[i] = std::fmin(desc[i] * inv1, K(0.2));
+    T n2 = T(0);
     for (size_t i = 0; i < DESC_LEN; ++i) n2 += desc[i] * desc[i];
     n2 = std::sqrt(n2);
-    if (n2 > 1e-7f) {
-      const float inv2 = 1.0f / n2;
+    if (n2 > K(1e-7)) {
+      const T inv2 = K(1.0) / n2;
       for (size_t i = 0; i < DESC_LEN; ++i) desc[i] *= inv2;
     }
   }
 }
 
 // src/pipeline.rs:1012-1019
-void rootsift(const float* d, float* out) {
-  float l1 = 0.0f;
-  for (size_t i = 0; i < DESC_LEN; ++i) l1 += std::fmax(d[i], 0.0f);
-  if (l1 <= 1e-7f) {
-    std::memmove(out, d, DESC_LEN * sizeof(float));
+template <typename T>
+void rootsift(const T* d, T* out) {
+  T l1 = T(0);
+  for (size_t i = 0; i < DESC_LEN; ++i) l1 += std::fmax(d[i], T(0));
+  if (l1 <= K(1e-7)) {
+    std::memmove(out, d, DESC_LEN * sizeof(T));
     return;
   }
-  const float inv = 1.0f / l1;
-  for (size_t i = 0; i < DESC_LEN; ++i) out[i] = std::sqrt(std::fmax(d[i], 0.0f) * inv);
+  const T inv = K(1.0) / l1;
+  for (size_t i = 0; i < DESC_LEN; ++i) out[i] = std::sqrt(std::fmax(d[i], T(0)) * inv);
 }
 
-struct Feature {
-  float x, y, scale, response, orientation;
-  float desc[DESC_LEN];
+template <typename T>
+struct FeatureT {
+  T x, y, scale, response, orientation;
+  T desc[DESC_LEN];
 };
 
 // src/pipeline.rs:1482-1577
-std::vector<Feature> describe_from_pyramid(const std::vector<Octave>& pyr,
-                                           const std::vector<oracle_keypoint>& kps, int kind) {
-  std::vector<Feature> feats;
+template <typename T>
+std::vector<FeatureT<T>> describe_from_pyramid(const std::vector<OctaveT<T>>& pyr,
+                                               const std::vector<KpT<T>>& kps, int kind) {
+  std::vector<FeatureT<T>> feats;
   if (pyr.empty() || kps.empty()) return feats;
   std::vector<std::pair<int, int>> levels;
   for (const auto& kp : kps) {
     int o, l;
-    resolve_octave_and_layer(kp, pyr, o, l);
+    resolve_octave_and_layer<T>(kp, pyr, o, l);
     if (std::find(levels.begin(), levels.end(), std::make_pair(o, l)) == levels.end())
       levels.push_back({o, l});
   }
-  std::vector<GradPlanes> cache(levels.size());
+  std::vector<GradPlanesT<T>> cache(levels.size());
 #pragma omp parallel for schedule(dynamic, 1)
   for (int i = 0; i < (int)levels.size(); ++i)
-    cache[i] = gradient_planes(levels[i].first, levels[i].second, pyr[levels[i].first].g[levels[i].second]);
+    cache[i] = gradient_planes<T>(levels[i].first, levels[i].second, pyr[levels[i].first].g[levels[i].second]);
 
-  std::vector<std::vector<Feature>> per_kp(kps.size());
+  std::vector<std::vector<FeatureT<T>>> per_kp(kps.size());
 #pragma omp parallel for schedule(dynamic, 16)
   for (long long i = 0; i < (long long)kps.size(); ++i) {
-    const oracle_keypoint& kp = kps[i];
+    const KpT<T>& kp = kps[i];
     int o, l;
-    resolve_octave_and_layer(kp, pyr, o, l);
-    const GradPlanes* gp = nullptr;
+    resolve_octave_and_layer<T>(kp, pyr, o, l);
+    const GradPlanesT<T>* gp = nullptr;
     for (const auto& c : cache)
       if (c.octave == o && c.layer == l) {
         gp = &c;
         break;
       }
-    const float oct_mult = pyr[o].scale_factor;
-    const float inv = 1.0f / oct_mult;
-    oracle_keypoint okp;
+    const T oct_mult = pyr[o].scale_factor;
+    const T inv = K(1.0) / oct_mult;
+    KpT<T> okp;
     okp.x = kp.x * inv;
     okp.y = kp.y * inv;
-    okp.scale = std::fmax(kp.scale * inv, 0.5f * BASE_SIGMA);
+    okp.scale = std::fmax(kp.scale * inv, K(0.5) * base_sigma<T>());
     okp.response = kp.response;
     okp.octave = (uint32_t)o;
     okp.layer = (uint32_t)l;
-    const std::vector<float> oris = keypoint_orientations(*gp, okp);
-    for (float ori : oris) {
-      Feature f;
+    const std::vector<T> oris = keypoint_orientations<T>(*gp, okp);
+    for (T ori : oris) {
+      FeatureT<T> f;
       f.x = kp.x;
       f.y = kp.y;
       f.scale = kp.scale;
       f.response = kp.response;
       f.orientation = ori;
-      float raw[DESC_LEN];
-      descriptor_128(*gp, okp, ori, raw);
-      if (kind == 1) rootsift(raw, f.desc);
+      T raw[DESC_LEN];
+      descriptor_128<T>(*gp, okp, ori, raw);
+      if (kind == 1) rootsift<T>(raw, f.desc);
       else std::memcpy(f.desc, raw, sizeof(raw));
       per_kp[i].push_back(f);
     }
@@ -688,13 +727,15 @@ std::vector<Feature> describe_from_pyramid(const std::vector<Octave>& pyr,
   return feats;
 }
 
-Plane make_plane(const float* img, int h, int w) {
-  Plane p(h, w);
-  std::memcpy(p.d.data(), img, sizeof(float) * (size_t)h * w);
+template <typename T>
+PlaneT<T> make_plane(const T* img, int h, int w) {
+  PlaneT<T> p(h, w);
+  std::memcpy(p.d.data(), img, sizeof(T) * (size_t)h * w);
   return p;
 }
 
-int write_features(const std::vector<Feature>& f, float* meta, float* desc, int cap) {
+template <typename T>
+int write_features(const std::vector<FeatureT<T>>& f, T* meta, T* desc, int cap) {
   const int n = (int)f.size();
   for (int i = 0; i < n && i < cap; ++i) {
     if (meta) {
@@ -704,10 +745,30 @@ int write_features(const std::vector<Feature>& f, float* meta, float* desc, int 
       meta[5 * i + 3] = f[i].response;
       meta[5 * i + 4] = f[i].orientation;
     }
-    if (desc) std::memcpy(desc + (size_t)i * DESC_LEN, f[i].desc, sizeof(float) * DESC_LEN);
+    if (desc) std::memcpy(desc + (size_t)i * DESC_LEN, f[i].desc, sizeof(T) * DESC_LEN);
   }
   return n;
 }
+
+// src/pipeline.rs:1633-1658.  max_features = 0 disables the cap (the reference
+// always caps at MAX_FEATURES_PER_IMAGE = 4096, src/pipeline.rs:1054).
+template <typename T>
+int detect_and_compute_t(const PlaneT<T>& img, int octaves, int scales, T thr, int upsample, int kind,
+                         int max_features, T* meta, T* desc, int cap) {
+  const auto pyr = build_pyramid<T>(img, octaves, scales, upsample != 0);
+  auto kps = pyramid_extract<T>(pyr, thr);
+  if (max_features > 0 && (int)kps.size() > max_features) {
+    std::stable_sort(kps.begin(), kps.end(), [](const KpT<T>& a, const KpT<T>& b) {
+      return std::fabs(b.response) < std::fabs(a.response);
+    });
+    kps.resize(max_features);
+  }
+  auto feats = describe_from_pyramid<T>(pyr, kps, kind);
+  if (max_features > 0 && (int)feats.size() > max_features) feats.resize(max_features);
+  return write_features<T>(feats, meta, desc, cap);
+}
+
+#undef K
 
 // ---------------------------------------------------------------- matching
 // src/pipeline.rs:1700-1717
@@ -1786,22 +1847,44 @@ int oracle_detect_keypoints(const float* img, int h, int w, int octaves, int sca
   return (int)kps.size();
 }
 
-// src/pipeline.rs:1633-1658.  max_features = 0 disables the cap (the reference
-// always caps at MAX_FEATURES_PER_IMAGE = 4096, src/pipeline.rs:1054).
+// src/pipeline.rs:1633-1658 (see detect_and_compute_t).
 int oracle_detect_and_compute(const float* img, int h, int w, int octaves, int scales, float thr,
                               int upsample, int kind, int max_features, float* meta, float* desc,
                               int cap) {
-  const auto pyr = build_pyramid(make_plane(img, h, w), octaves, scales, upsample != 0);
-  auto kps = pyramid_extract(pyr, thr);
-  if (max_features > 0 && (int)kps.size() > max_features) {
-    std::stable_sort(kps.begin(), kps.end(), [](const oracle_keypoint& a, const oracle_keypoint& b) {
-      return std::fabs(b.response) < std::fabs(a.response);
-    });
-    kps.resize(max_features);
+  return detect_and_compute_t<float>(make_plane(img, h, w), octaves, scales, thr, upsample, kind, max_features,
+                                     meta, desc, cap);
+}
+
+// The same pipeline in f64 from the u8 luma (src/pipeline.rs:957-966 with
+// `px as f64 * (1.0 / 255.0)`): the yardstick for the f32 results' error.
+int oracle_detect_and_compute_f64(const uint8_t* luma, int h, int w, int octaves, int scales, double thr,
+                                  int upsample, int kind, int max_features, double* meta, double* desc,
+                                  int cap) {
+  PlaneT<double> img(h, w);
+  const double inv_255 = 1.0 / 255.0;
+  for (size_t i = 0; i < img.d.size(); ++i) img.d[i] = (double)luma[i] * inv_255;
+  return detect_and_compute_t<double>(img, octaves, scales, thr, upsample, kind, max_features, meta, desc, cap);
+}
+
+// Keypoints of the f64 pipeline: 6 doubles each (x, y, scale, response, octave, layer).
+int oracle_detect_keypoints_f64(const uint8_t* luma, int h, int w, int octaves, int scales, double thr,
+                                int upsample, double* out, int cap) {
+  PlaneT<double> img(h, w);
+  const double inv_255 = 1.0 / 255.0;
+  for (size_t i = 0; i < img.d.size(); ++i) img.d[i] = (double)luma[i] * inv_255;
+  const auto pyr = build_pyramid<double>(img, octaves, scales, upsample != 0);
+  const auto kps = pyramid_extract<double>(pyr, thr);
+  for (int i = 0; i < (int)kps.size() && i < cap; ++i) {
+    const keypoint_f64& k = kps[i];
+    double* o = out + 6 * (size_t)i;
+    o[0] = k.x;
+    o[1] = k.y;
+    o[2] = k.scale;
+    o[3] = k.response;
+    o[4] = (double)k.octave;
+    o[5] = (double)k.layer;
   }
-  auto feats = describe_from_pyramid(pyr, kps, kind);
-  if (max_features > 0 && (int)feats.size() > max_features) feats.resize(max_features);
-  return write_features(feats, meta, desc, cap);
+  return (int)kps.size();
 }
 
 // src/pipeline.rs:1581-1629

@@ -66,6 +66,15 @@ void oracle_pyramid_free(void* pyr);
 int oracle_detect_and_compute(const float* img, int h, int w, int octaves, int scales,
                               float threshold, int upsample, int kind, int max_features,
                               float* meta, float* desc, int cap);
+/* The same pipeline run in f64 (values, constants and libm calls), from the u8
+ * luma: the yardstick that f32 results state their error against.
+ * meta: 5 doubles per feature; keypoints: 6 doubles (x, y, scale, response,
+ * octave, layer). */
+int oracle_detect_and_compute_f64(const uint8_t* luma, int h, int w, int octaves, int scales,
+                                  double threshold, int upsample, int kind, int max_features,
+                                  double* meta, double* desc, int cap);
+int oracle_detect_keypoints_f64(const uint8_t* luma, int h, int w, int octaves, int scales,
+                                double threshold, int upsample, double* out, int cap);
 int oracle_detect_keypoints(const float* img, int h, int w, int octaves, int scales,
                             float threshold, int upsample, oracle_keypoint* out, int cap);
 int oracle_compute_descriptors(const float* img, int h, int w, const oracle_keypoint* kps, int n,
