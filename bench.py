@@ -428,7 +428,13 @@ def catalog_search_bench(ctx, torch, n_entries: int = 10_000, per_entry: int = 2
                            np.r_[tf.scale * 1.1, rng.uniform(1.6, 12, n_q - per_entry)].astype(np.float32),
                            np.full(n_q, 0.05, np.float32),
                            np.r_[tf.orientation + th, rng.uniform(0, 6.28, n_q - per_entry)].astype(np.float32), qd)
+    t0 = time.perf_counter()
+    hits = cat.search_features(query)  # first search after the load builds the MIH tables
+    build_s = time.perf_counter() - t0
     hits = cat.search_features(query)
+    t0 = time.perf_counter()
+    hits = cat.search_features(query)
+    build_s -= time.perf_counter() - t0
     l0 = ctx.launch_count
     t0 = time.perf_counter()
     for _ in range(reps):
@@ -440,13 +446,37 @@ def catalog_search_bench(ctx, torch, n_entries: int = 10_000, per_entry: int = 2
     for _ in range(reps):
         cat.search_features(query)
     stages = {k: v[0] / reps for k, v in ctx.stage_times(reset=True).items() if v[1]}
+    # Coarse votes alone (device time of the votes launches, query codes given):
+    # the MIH rule through the device tables vs every code scanned; the search
+    # with the scan path for comparison.
+    qcodes = psift.quantize_descriptor_u128(qd, ctx)
+    votes_ms = {}
+    for name, path in (("mih_index", psift.VOTES_MIH_INDEX), ("mih_scan", psift.VOTES_MIH_SCAN)):
+        ref = cat.votes(qcodes, path)
+        ctx.stage_times(reset=True)
+        for _ in range(reps):
+            got = cat.votes(qcodes, path)
+        votes_ms[name] = ctx.stage_times(reset=True)["hamming"][0] / reps
+        assert np.array_equal(got, ref)
+    same_votes = bool(np.array_equal(cat.votes(qcodes, psift.VOTES_MIH_INDEX), cat.votes(qcodes, psift.VOTES_MIH_SCAN)))
     ctx.enable_stage_timing(False)
+    cat.set_search_votes(psift.VOTES_MIH_SCAN)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        hits_scan = cat.search_features(query)
+    search_scan_s = (time.perf_counter() - t0) / reps
+    cat.set_search_votes(psift.VOTES_AUTO)
+    same_hits = [(h.id, h.coarse_votes, h.tracking.match_count) for h in hits_scan] == \
+                [(h.id, h.coarse_votes, h.tracking.match_count) for h in hits]
     cat.close()
     return {
         "workload": f"PSIFTCAT v1 catalog of {n_entries} entries x {per_entry} features ({len(blob) / 1e6:.0f} MB), "
                     f"{n_q}-feature query, top-5 / shortlist 16, host API wall clock",
         "load_binary_s": load_s, "load_binary_gbs": len(blob) / load_s / 1e9,
         "search_ms": search_s * 1e3, "launches_per_search": launches, "device_stage_ms_per_search": stages,
+        "search_ms_votes_by_scan": search_scan_s * 1e3, "same_hits_either_votes_path": same_hits,
+        "votes_device_ms": votes_ms, "same_votes_index_vs_scan": same_votes,
+        "mih_tables_build_s": build_s,
         "top_hit": hits[0].id if hits else None, "top_hit_inliers": hits[0].tracking.match_count if hits else 0,
         "expected_top_hit": f"img{target:05d}",
     }

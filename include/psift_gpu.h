@@ -460,6 +460,26 @@ typedef struct psift_catalog_hit {
 psift_status psift_catalog_search(psift_catalog* cat, const psift_features* query, uint32_t top_k,
                                   uint32_t shortlist_k, float ratio, float ransac_threshold,
                                   psift_catalog_hit* hits, uint32_t capacity, uint32_t* count);
+/* How the coarse votes of search_features (src/catalog.rs:588-633) are computed.
+ * AUTO is the reference's choice: for at most 32 entries the exhaustive rule
+ * (count_coarse_hamming_votes, :707-728: some signature within 24 bits); beyond,
+ * the multi-index-hashing rule (:596-621: some signature within 24 bits that
+ * shares one of the query's 16 bytes), answered through the device MIH tables
+ * (FeatureCatalog's 16 x 256 inverted tables, :291-321) when the query's
+ * (query, entry) bitmap fits in 128 MB, else by scanning every code.  The other
+ * values force one computation; all give the votes of their rule exactly. */
+#define PSIFT_VOTES_AUTO 0
+#define PSIFT_VOTES_MIH_SCAN 1  /* MIH rule, every code scanned */
+#define PSIFT_VOTES_MIH_INDEX 2 /* MIH rule through the tables (PSIFT_ERR_CAPACITY when they cannot serve the query) */
+#define PSIFT_VOTES_EXHAUSTIVE 3
+/* Votes for host query codes (2 x u64 each, quantize_descriptor_u128) against the
+ * resident codes; votes: host, psift_catalog_size(cat) words.  The MIH tables
+ * are built on the device by the first index use after the catalog changed. */
+psift_status psift_catalog_votes(psift_catalog* cat, const uint64_t* query_codes, uint32_t nq, int32_t path,
+                                 uint32_t* votes);
+/* The votes computation psift_catalog_search uses: PSIFT_VOTES_AUTO (default) or
+ * PSIFT_VOTES_MIH_SCAN (for comparison; the same votes, the same hits). */
+psift_status psift_catalog_set_search_votes(psift_catalog* cat, int32_t path);
 
 /* ---------------------------------------------------------------- warp and stitch */
 /* warp_and_stitch (src/visualize.rs:379-483): the query warped into the target's

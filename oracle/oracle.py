@@ -114,6 +114,7 @@ def lib():
             L.oracle_summarize_tracking.argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp,
                                                     C.POINTER(Tracking)]
             L.oracle_hamming_votes.argtypes = [_u64p, C.c_int, _u64p, _i64p, C.c_int, C.c_int, _u32p]
+            L.oracle_mih_votes_tables.argtypes = [_u64p, C.c_int, _u64p, _i64p, C.c_int, _u32p]
             L.oracle_hamming_topk.argtypes = [_u64p, C.c_int, _u64p, C.c_int64, C.c_int, _u32p, _u32p]
             L.oracle_l2_rerank.argtypes = [_fp, C.c_int, _fp, _u32p, C.c_int, _u32p, _fp]
             L.oracle_warp_and_stitch.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_int,
@@ -364,6 +365,17 @@ def hamming_votes(q_codes, cat_codes, offsets, mih: bool) -> np.ndarray:
     votes = np.zeros(len(off) - 1, np.uint32)
     lib().oracle_hamming_votes(_p(q, _u64p), q.shape[0], _p(c, _u64p), _p(off, _i64p), len(off) - 1,
                                int(bool(mih)), _p(votes, _u32p))
+    return votes
+
+
+def mih_votes_tables(q_codes, cat_codes, offsets) -> np.ndarray:
+    """MIH votes by the reference's own table walk (inverted tables + seen_stamp)."""
+    q = np.ascontiguousarray(q_codes, dtype=np.uint64).reshape(-1, 2)
+    c = np.ascontiguousarray(cat_codes, dtype=np.uint64).reshape(-1, 2)
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    votes = np.zeros(len(off) - 1, np.uint32)
+    lib().oracle_mih_votes_tables(_p(q, _u64p), q.shape[0], _p(c, _u64p), _p(off, _i64p), len(off) - 1,
+                                  _p(votes, _u32p))
     return votes
 
 

@@ -2114,6 +2114,42 @@ void oracle_hamming_votes(const uint64_t* q, int nq, const uint64_t* cat, const 
   }
 }
 
+// The MIH branch as the reference runs it: the 16 x 256 inverted tables of
+// (entry, signature) pairs (src/catalog.rs:291-306, filled in entry and
+// signature order) and, per query, the walk over the 16 buckets its bytes
+// select with seen_stamp deduplication (:596-615).  Sequential, for small
+// cases: the pin of the zero-byte rule that oracle_hamming_votes evaluates.
+void oracle_mih_votes_tables(const uint64_t* q, int nq, const uint64_t* cat, const int64_t* offsets, int ne,
+                             uint32_t* votes) {
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> tables((size_t)16 * 256);
+  for (int e = 0; e < ne; ++e)
+    for (int64_t s = offsets[e]; s < offsets[e + 1]; ++s) {
+      const uint64_t w[2] = {cat[2 * s], cat[2 * s + 1]};
+      for (int band = 0; band < 16; ++band) {
+        const unsigned key = (unsigned)((w[band / 8] >> (8 * (band % 8))) & 0xFF);
+        tables[(size_t)band * 256 + key].emplace_back((uint32_t)e, (uint32_t)(s - offsets[e]));
+      }
+    }
+  std::vector<size_t> seen(ne, 0);
+  for (int e = 0; e < ne; ++e) votes[e] = 0;
+  for (int qi = 0; qi < nq; ++qi) {
+    const size_t stamp = (size_t)qi + 1;
+    const uint64_t qw[2] = {q[2 * qi], q[2 * qi + 1]};
+    for (int band = 0; band < 16; ++band) {
+      const unsigned key = (unsigned)((qw[band / 8] >> (8 * (band % 8))) & 0xFF);
+      for (const auto& es : tables[(size_t)band * 256 + key]) {
+        if (seen[es.first] == stamp) continue;
+        const int64_t s = offsets[es.first] + es.second;
+        const int d = __builtin_popcountll(qw[0] ^ cat[2 * s]) + __builtin_popcountll(qw[1] ^ cat[2 * s + 1]);
+        if (d <= 24) {
+          seen[es.first] = stamp;
+          votes[es.first] += 1;
+        }
+      }
+    }
+  }
+}
+
 void oracle_hamming_topk(const uint64_t* q, int nq, const uint64_t* cat, int64_t ncat, int k, uint32_t* idx,
                          uint32_t* dist) {
 #pragma omp parallel for schedule(dynamic, 1)

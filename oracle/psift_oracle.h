@@ -103,6 +103,9 @@ void oracle_summarize_tracking(const oracle_match* m, int n, const float* q_scal
  * semantics, else the exhaustive scan. */
 void oracle_hamming_votes(const uint64_t* q, int nq, const uint64_t* cat, const int64_t* offsets,
                           int n_entries, int mih, uint32_t* votes);
+/* The MIH votes through the reference's inverted tables and seen_stamp walk (src/catalog.rs:291-306, :596-615). */
+void oracle_mih_votes_tables(const uint64_t* q, int nq, const uint64_t* cat, const int64_t* offsets, int ne,
+                             uint32_t* votes);
 /* Per-query top-k nearest codes by (Hamming distance, global index). */
 void oracle_hamming_topk(const uint64_t* q, int nq, const uint64_t* cat, int64_t ncat, int k,
                          uint32_t* idx, uint32_t* dist);

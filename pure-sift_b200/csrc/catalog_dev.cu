@@ -29,6 +29,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include "mih.cuh"
 #include "psift_internal.cuh"
 
 namespace psift {
@@ -243,6 +244,11 @@ struct psift_catalog {
   uint64_t total = 0;
   char* scratch = nullptr;  // grow-only search / load workspace
   size_t scratch_cap = 0;
+  // Multi-index hashing tables (src/catalog.rs:291-321), rebuilt on the first
+  // votes after a change of contents (version counts upserts, removals).
+  MihIndex mih;
+  uint64_t version = 0;
+  int32_t search_votes = PSIFT_VOTES_AUTO;
 
   psift_status reserve_scratch(size_t bytes) {
     if (bytes <= scratch_cap) return PSIFT_OK;
@@ -352,6 +358,50 @@ bool features_ok(const psift_features* f) {
                (f->x && f->y && f->scale && f->response && f->orientation && f->descriptors));
 }
 
+// Whether the MIH tables can answer nq queries: the (query, entry) bitmap, the
+// grouped query lists and the tables within their limits.
+bool mih_index_fits(const psift_catalog* cat, uint32_t nq) {
+  return (uint64_t)nq * cat->entries.size() <= kMihBitmapMaxBits && nq <= (1u << 26) &&
+         cat->total <= (1ull << 28);
+}
+
+// The tables of the catalog's current contents (built on first use after a change).
+psift_status ensure_mih(psift_catalog* cat) {
+  if (cat->mih.valid && cat->mih.version == cat->version) return PSIFT_OK;
+  std::vector<long long> off(cat->entries.size() + 1);
+  for (size_t e = 0; e < cat->entries.size(); ++e) off[e] = (long long)cat->entries[e].offset;
+  off[cat->entries.size()] = (long long)cat->total;
+  const psift_status st = mih_build(cat->ctx, cat->mih, cat->a.codes, cat->total, off);
+  if (st == PSIFT_OK) cat->mih.version = cat->version;
+  return st;
+}
+
+enum ResolvedVotes { kExhaustiveScan, kMihScan, kMihIndex };
+
+ResolvedVotes resolve_votes(const psift_catalog* cat, uint32_t nq, int32_t path) {
+  switch (path) {
+    case PSIFT_VOTES_MIH_SCAN: return kMihScan;
+    case PSIFT_VOTES_MIH_INDEX: return kMihIndex;
+    case PSIFT_VOTES_EXHAUSTIVE: return kExhaustiveScan;
+    default:
+      if (cat->entries.size() <= 32) return kExhaustiveScan;
+      return mih_index_fits(cat, nq) ? kMihIndex : kMihScan;
+  }
+}
+
+// Device votes for device query codes: the scan kernel (d_off: device entry
+// offsets) or the tables (mih_scratch: mih_votes_scratch_bytes).
+cudaError_t launch_catalog_votes(psift_catalog* cat, ResolvedVotes how, const uint64_t* d_codes, uint32_t nq,
+                                 const long long* d_off, void* mih_scratch, uint32_t* d_votes, cudaStream_t s) {
+  const uint32_t n_entries = (uint32_t)cat->entries.size();
+  if (how == kMihIndex) {
+    cat->ctx->launches += 2;
+    return mih_votes(cat->mih, cat->a.codes, d_codes, nq, d_votes, mih_scratch, s);
+  }
+  cat->ctx->launches++;
+  return launch_votes(d_codes, (int)nq, cat->a.codes, d_off, (int)n_entries, how == kMihScan ? 1 : 0, d_votes, s);
+}
+
 }  // namespace
 
 extern "C" {
@@ -373,6 +423,7 @@ psift_status psift_catalog_destroy(psift_catalog* cat) {
   if (cat_begin(cat) == PSIFT_OK) cudaStreamSynchronize(cat->ctx->stream);
   free_arrays(cat->a);
   cudaFree(cat->scratch);
+  mih_free(cat->mih);
   delete cat;
   return PSIFT_OK;
 }
@@ -415,6 +466,7 @@ psift_status psift_catalog_upsert(psift_catalog* cat, const char* id, uint32_t w
   psift_status st = cat_begin(cat);
   if (st != PSIFT_OK) return st;
   if (!id || !features_ok(f)) return set_error(cat->ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  ++cat->version;
   psift_catalog::Entry E;
   E.id = id;
   E.width = width;
@@ -459,6 +511,7 @@ psift_status psift_catalog_remove(psift_catalog* cat, const char* id, int32_t* r
     next.push_back(cat->entries[src]);
   }
   uint64_t unused = 0;
+  ++cat->version;
   if ((st = cat->rebuild(order, 0, std::move(next), &unused)) != PSIFT_OK) return st;
   *removed = 1;
   return PSIFT_OK;
@@ -707,18 +760,22 @@ psift_status psift_catalog_search(psift_catalog* cat, const psift_features* quer
   if ((st = psift_ransac_options_validate(&ropt, msg, sizeof msg)) != PSIFT_OK) return set_error(ctx, st, msg);
   const bool own_tracking = ransac_threshold != kDefaultRansacThreshold;
   const uint32_t max_cands = std::min<uint32_t>(n_entries, std::max<uint32_t>(shortlist_k, 1));
+  const ResolvedVotes how = n_entries <= 32 ? kExhaustiveScan : resolve_votes(cat, nq, cat->search_votes);
+  if (how == kMihIndex && (st = ensure_mih(cat)) != PSIFT_OK) return st;
+  const size_t mih_bytes = how == kMihIndex ? mih_votes_scratch_bytes(nq, n_entries) : 0;
 
   // Workspace (device): query, codes, offsets, votes, then per candidate the
-  // match list, three masks and the model / flag / count words.
+  // match list, three masks and the model / flag / count words, then the MIH
+  // votes' scratch.
   const size_t q_bytes = align_up((size_t)nq * 512, 256), xy_bytes = align_up((size_t)nq * 8, 256);
   const size_t code_bytes = align_up((size_t)nq * 16, 256), off_bytes = align_up(8 * (size_t)(n_entries + 1), 256);
   const size_t vote_bytes = align_up(4 * (size_t)n_entries, 256);
   const size_t m_bytes = align_up(sizeof(psift_match) * nq, 256), mask_bytes = align_up(nq, 256);
   constexpr size_t kWords = 64;  // [0] match count, [4..12) sim, [16..32) hom, [40..48) tracking sim
   const size_t per_cand = m_bytes + 3 * mask_bytes + kWords * 4;
-  if ((st = cat->reserve_scratch(q_bytes + xy_bytes + code_bytes + off_bytes + vote_bytes +
-                                 per_cand * max_cands)) != PSIFT_OK)
-    return st;
+  const size_t search_bytes = align_up(q_bytes + xy_bytes + code_bytes + off_bytes + vote_bytes +
+                                      per_cand * max_cands, 256);
+  if ((st = cat->reserve_scratch(search_bytes + mih_bytes)) != PSIFT_OK) return st;
   char* w = cat->scratch;
   float* d_q = (float*)w;
   float2* d_qxy = (float2*)(w + q_bytes);
@@ -744,8 +801,7 @@ psift_status psift_catalog_search(psift_catalog* cat, const psift_features* quer
     cudaError_t e = launch_quantize(d_q, (int)nq, d_codes, nullptr, s);
     ctx->launches++;
     if (e == cudaSuccess) {
-      e = launch_votes(d_codes, (int)nq, cat->a.codes, d_off, (int)n_entries, mih, d_votes, s);
-      ctx->launches++;
+      e = launch_catalog_votes(cat, how, d_codes, nq, d_off, w + search_bytes, d_votes, s);
     }
     if (e != cudaSuccess) return cuda_error(ctx, e, "catalog votes");
   }
@@ -891,6 +947,54 @@ psift_status psift_catalog_search(psift_catalog* cat, const psift_features* quer
   if (n_out > capacity) return set_error(ctx, PSIFT_ERR_CAPACITY, "hit output capacity too small");
   if (n_out && !hits) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null hit output");
   for (uint32_t i = 0; i < n_out; ++i) hits[i] = out[order[i]];
+  return PSIFT_OK;
+}
+
+
+psift_status psift_catalog_votes(psift_catalog* cat, const uint64_t* query_codes, uint32_t nq, int32_t path,
+                                 uint32_t* votes) {
+  psift_status st = cat_begin(cat);
+  if (st != PSIFT_OK) return st;
+  psift_ctx* ctx = cat->ctx;
+  if (path < PSIFT_VOTES_AUTO || path > PSIFT_VOTES_EXHAUSTIVE)
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "votes path must be one of PSIFT_VOTES_*");
+  const uint32_t n_entries = (uint32_t)cat->entries.size();
+  if (n_entries == 0) return PSIFT_OK;
+  if (!votes || (nq && !query_codes)) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
+  const ResolvedVotes how = resolve_votes(cat, nq, path);
+  if (how == kMihIndex && !mih_index_fits(cat, nq))
+    return set_error(ctx, PSIFT_ERR_CAPACITY, "MIH tables cannot serve this query: (query, entry) bitmap above 2^30 bits");
+  if (how == kMihIndex && (st = ensure_mih(cat)) != PSIFT_OK) return st;
+  const size_t code_bytes = align_up((size_t)nq * 16 + 16, 256), off_bytes = align_up(8 * (size_t)(n_entries + 1), 256);
+  const size_t vote_bytes = align_up(4 * (size_t)n_entries, 256);
+  const size_t mih_bytes = how == kMihIndex ? mih_votes_scratch_bytes(nq, n_entries) : 0;
+  if ((st = cat->reserve_scratch(code_bytes + off_bytes + vote_bytes + mih_bytes)) != PSIFT_OK) return st;
+  char* w = cat->scratch;
+  uint64_t* d_codes = (uint64_t*)w;
+  long long* d_off = (long long*)(w + code_bytes);
+  uint32_t* d_votes = (uint32_t*)(w + code_bytes + off_bytes);
+  cudaStream_t s = ctx->stream;
+  std::vector<long long> off(n_entries + 1);
+  for (uint32_t e = 0; e < n_entries; ++e) off[e] = (long long)cat->entries[e].offset;
+  off[n_entries] = (long long)cat->total;
+  if (nq) PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_codes, query_codes, (size_t)nq * 16, cudaMemcpyHostToDevice, s));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_off, off.data(), 8 * off.size(), cudaMemcpyHostToDevice, s));
+  {
+    StageScope sc(ctx, STAGE_HAMMING);
+    const cudaError_t e = launch_catalog_votes(cat, how, d_codes, nq, d_off, w + code_bytes + off_bytes + vote_bytes,
+                                               d_votes, s);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "catalog votes");
+  }
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(votes, d_votes, 4 * (size_t)n_entries, cudaMemcpyDeviceToHost, s));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  return PSIFT_OK;
+}
+
+psift_status psift_catalog_set_search_votes(psift_catalog* cat, int32_t path) {
+  if (!cat) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (path != PSIFT_VOTES_AUTO && path != PSIFT_VOTES_MIH_SCAN)
+    return set_error(cat->ctx, PSIFT_ERR_INVALID_ARGUMENT, "search votes must be PSIFT_VOTES_AUTO or PSIFT_VOTES_MIH_SCAN");
+  cat->search_votes = path;
   return PSIFT_OK;
 }
 

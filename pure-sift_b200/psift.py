@@ -235,6 +235,8 @@ _SIGS = {
     "psift_catalog_features": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(CFeatures), C.c_void_p]),
     "psift_catalog_load_binary": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
     "psift_catalog_save_binary": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "psift_catalog_votes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p]),
+    "psift_catalog_set_search_votes": (C.c_int, [C.c_void_p, C.c_int32]),
     "psift_catalog_search": (C.c_int, [C.c_void_p, C.POINTER(CFeatures), C.c_uint32, C.c_uint32, C.c_float,
                                        C.c_float, C.POINTER(CCatalogHit), C.c_uint32, C.POINTER(C.c_uint32)]),
 }
@@ -955,6 +957,8 @@ def summarize_tracking(query: Features, target: Features, matches, ctx: Context 
 
 
 DEFAULT_CATALOG_SHORTLIST = 16
+# Coarse-vote computations of the device catalog (PSIFT_VOTES_*).
+VOTES_AUTO, VOTES_MIH_SCAN, VOTES_MIH_INDEX, VOTES_EXHAUSTIVE = 0, 1, 2, 3
 DEFAULT_CATALOG_TOP_K = 5
 
 
@@ -1186,6 +1190,21 @@ class DeviceCatalog:
             hom = np.array(h.homography[:], np.float32).reshape(3, 3) if h.has_homography else None
             out.append(CatalogSearchHit(e.id, e.width, e.height, e.feature_count, h.coarse_votes, tr, sim, hom))
         return out
+
+    def votes(self, query_codes, path: int = 0) -> np.ndarray:
+        """Coarse votes of ``search_features`` (src/catalog.rs:588-633) for u128
+        query codes ((n, 2) u64) against the resident codes.  path: VOTES_AUTO
+        (the search's choice), VOTES_MIH_SCAN, VOTES_MIH_INDEX (the device MIH
+        tables, src/catalog.rs:291-321) or VOTES_EXHAUSTIVE."""
+        q = np.ascontiguousarray(query_codes, dtype=np.uint64).reshape(-1, 2)
+        out = np.zeros(len(self), np.uint32)
+        self.ctx.check(self.ctx.lib.psift_catalog_votes(self.handle, q.ctypes.data, q.shape[0], int(path),
+                                                        out.ctypes.data))
+        return out
+
+    def set_search_votes(self, path: int):
+        """Votes computation of ``search_features``: VOTES_AUTO or VOTES_MIH_SCAN."""
+        self.ctx.check(self.ctx.lib.psift_catalog_set_search_votes(self.handle, int(path)))
 
     # ---- persistence (src/catalog.rs:378-574)
     @classmethod
