@@ -459,6 +459,12 @@ def catalog_search_bench(ctx, torch, n_entries: int = 10_000, per_entry: int = 2
         votes_ms[name] = ctx.stage_times(reset=True)["hamming"][0] / reps
         assert np.array_equal(got, ref)
     same_votes = bool(np.array_equal(cat.votes(qcodes, psift.VOTES_MIH_INDEX), cat.votes(qcodes, psift.VOTES_MIH_SCAN)))
+    # Pairs the MIH votes test: per band, queries x listed codes summed over the 256 keys.
+    mih_pairs = 0
+    for b in range(16):
+        kc = ((codes[:, b // 8] >> np.uint64(8 * (b % 8))) & np.uint64(0xFF)).astype(np.int64)
+        kq = ((qcodes[:, b // 8] >> np.uint64(8 * (b % 8))) & np.uint64(0xFF)).astype(np.int64)
+        mih_pairs += int(np.dot(np.bincount(kc, minlength=256), np.bincount(kq, minlength=256)))
     ctx.enable_stage_timing(False)
     cat.set_search_votes(psift.VOTES_MIH_SCAN)
     t0 = time.perf_counter()
@@ -476,6 +482,9 @@ def catalog_search_bench(ctx, torch, n_entries: int = 10_000, per_entry: int = 2
         "search_ms": search_s * 1e3, "launches_per_search": launches, "device_stage_ms_per_search": stages,
         "search_ms_votes_by_scan": search_scan_s * 1e3, "same_hits_either_votes_path": same_hits,
         "votes_device_ms": votes_ms, "same_votes_index_vs_scan": same_votes,
+        "mih_pairs": mih_pairs, "scan_pairs": n_q * n,
+        "mih_pairs_per_s": mih_pairs / (votes_ms["mih_index"] * 1e-3),
+        "scan_pairs_per_s": n_q * n / (votes_ms["mih_scan"] * 1e-3),
         "mih_tables_build_s": build_s,
         "top_hit": hits[0].id if hits else None, "top_hit_inliers": hits[0].tracking.match_count if hits else 0,
         "expected_top_hit": f"img{target:05d}",
