@@ -638,6 +638,55 @@ def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int =
     }
 
 
+def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
+    """Input step: 8 colour 1920x1080 JPEGs (three independent 2000-blob fields as
+    R, G, B; 4:2:0, quality 90) in host memory -> features in host memory through
+    psift_detect_and_compute_jpeg_batch (nvJPEG decode on the GPU into the batch's
+    inputs), against the host u8 batch entry given the already decoded luma, and the
+    CPU decode (PIL + the image crate's luma formula, one thread) per image."""
+    import io
+    from PIL import Image
+    import psift
+    rgbs = [np.stack([synth.blob_image(WIDTH, HEIGHT, 2000, 1.5, 20.0, seed=900 + 3 * i + k) for k in range(3)],
+                     axis=2) for i in range(n)]
+    blobs = []
+    for im in rgbs:
+        buf = io.BytesIO()
+        Image.fromarray(im).save(buf, format="JPEG", quality=90, subsampling=2)
+        blobs.append(buf.getvalue())
+    sift = psift.Sift.new(psift.SiftConfig().with_octaves(4).with_contrast_threshold(0.015))
+    outs = [psift.Features.pinned(4096, ctx) for _ in range(n)]
+    for _ in range(3):
+        sift.detect_and_compute_jpeg_batch(blobs, outs=outs, ctx=ctx)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        feats = sift.detect_and_compute_jpeg_batch(blobs, outs=outs, ctx=ctx)
+    jpeg_s = (time.perf_counter() - t0) / reps
+    lumas = [psift.decode_jpeg_luma(b, ctx=ctx) for b in blobs]
+    pin = [psift.pinned_empty(l.shape, np.uint8, ctx) for l in lumas]
+    for d, l in zip(pin, lumas):
+        d[...] = l
+    for _ in range(3):
+        sift.detect_and_compute_batch_u8(pin, outs=outs, ctx=ctx)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        sift.detect_and_compute_batch_u8(pin, outs=outs, ctx=ctx)
+    u8_s = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    for b in blobs:
+        rgb = np.asarray(Image.open(io.BytesIO(b)).convert("RGB"))
+        r, g, bl = (rgb[..., k].astype(np.uint32) for k in range(3))
+        _ = ((2126 * r + 7152 * g + 722 * bl) // 10000).astype(np.uint8)
+    cpu_decode_ms = (time.perf_counter() - t0) / n * 1e3
+    return {
+        "workload": f"{n} colour {WIDTH}x{HEIGHT} JPEGs (4:2:0, q90, {sum(map(len, blobs)) / n / 1e3:.0f} KB each), "
+                    "host bytes -> pinned host features, host API wall clock",
+        "jpeg_images_per_s": n / jpeg_s, "u8_batch_images_per_s": n / u8_s,
+        "jpeg_minus_u8_input_ms_per_batch": (jpeg_s - u8_s) * 1e3, "cpu_decode_ms_per_image_1_thread": cpu_decode_ms,
+        "nvjpeg_backend": ctx.jpeg_backend, "features_per_image": [len(f) for f in feats[:4]],
+    }
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -851,7 +900,7 @@ def run_ours(args):
         for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench),
                         ("catalog_search", catalog_search_bench), ("warp", warp_bench),
                         ("fundamental", fundamental_bench),
-                        ("learned_ransac", ransac_bench)):
+                        ("learned_ransac", ransac_bench), ("jpeg", jpeg_bench)):
             if getattr(args, "no_" + key):
                 continue
             try:
@@ -891,7 +940,7 @@ def main():
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
     ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "warp", "fundamental",
-                                               "learned_ransac", "uneven_batch"],
+                                               "learned_ransac", "uneven_batch", "jpeg"],
                     help="run one section alone (profiling case)")
     ap.add_argument("--no-catalog", action="store_true")
     ap.add_argument("--no-catalog-search", dest="no_catalog_search", action="store_true")
@@ -901,6 +950,7 @@ def main():
     ap.add_argument("--no-fundamental", dest="no_fundamental", action="store_true")
     ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
+    ap.add_argument("--no-jpeg", dest="no_jpeg", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -915,7 +965,7 @@ def main():
                "catalog": lambda: catalog_bench(ctx, torch), "learned_ransac": lambda: ransac_bench(ctx, torch),
                "catalog_search": lambda: catalog_search_bench(ctx, torch), "warp": lambda: warp_bench(ctx, torch),
                "fundamental": lambda: fundamental_bench(ctx, torch),
-               "uneven_batch": lambda: uneven_bench(ctx, torch)}
+               "uneven_batch": lambda: uneven_bench(ctx, torch), "jpeg": lambda: jpeg_bench(ctx, torch)}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)
         ctx.close()
         return 0

@@ -206,6 +206,33 @@ psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_imag
  * call returns PSIFT_ERR_CAPACITY with that image's count set to the size needed. */
 psift_status psift_detect_and_compute_u8_batch(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
                                                const psift_sift_config* cfg, psift_features* outs);
+/* ---------------------------------------------------------------- JPEG input */
+/* decode_validated_dynamic_image / decode_validated_luma8 (src/cli.rs:129-170)
+ * for JPEG bytes, decoded on the GPU by nvJPEG (hardware JPEG engines when
+ * available, else its GPU-assisted backend; loaded on first use) and converted
+ * with the image crate's rgb_to_luma ((2126 R + 7152 G + 722 B) / 10000, u32,
+ * truncating).  Header checks as the reference: width and height >= 8
+ * (MIN_IMAGE_DIM), and with enforce_pixel_cap <= 8192 each and <= 25,000,000
+ * pixels (MAX_IMAGE_DIM, MAX_IMAGE_PIXELS); violations return
+ * PSIFT_ERR_INVALID_ARGUMENT with the reference's message, undecodable bytes
+ * PSIFT_ERR_FORMAT, a missing nvJPEG PSIFT_ERR_INTERNAL.  Decoded pixels follow
+ * nvJPEG's IDCT and chroma upsampling (not the image crate's decoder). */
+psift_status psift_jpeg_info(psift_ctx* ctx, const uint8_t* data, size_t length, int32_t enforce_pixel_cap,
+                             uint32_t* width, uint32_t* height, uint32_t* components);
+/* One JPEG to host u8 luma (width x height, dense rows; capacity in bytes). */
+psift_status psift_decode_jpeg_luma(psift_ctx* ctx, const uint8_t* data, size_t length, int32_t enforce_pixel_cap,
+                                    uint8_t* luma, size_t capacity, uint32_t* width, uint32_t* height);
+/* The extract path from bytes (run_extract_from_bytes, src/cli.rs:173-185, with
+ * Sift::detect_and_compute's features): n JPEG buffers (host) decoded on the GPU
+ * straight into the batch's device inputs, then as psift_detect_and_compute_u8_batch
+ * (features into the host arrays of outs[i]).  Per image, the features equal
+ * psift_detect_and_compute_u8 of the luma psift_decode_jpeg_luma returns. */
+psift_status psift_detect_and_compute_jpeg_batch(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths,
+                                                 uint32_t n, int32_t enforce_pixel_cap,
+                                                 const psift_sift_config* cfg, psift_features* outs);
+/* nvJPEG backend of the context's last decoded batch: 3 = hardware, 2 = GPU-assisted, -1 = none yet. */
+psift_status psift_ctx_jpeg_backend(psift_ctx* ctx, int32_t* backend);
+
 /* Page-locked host memory for the batch entry's inputs and outputs. */
 psift_status psift_host_alloc(psift_ctx* ctx, size_t bytes, void** out);
 psift_status psift_host_free(psift_ctx* ctx, void* p);

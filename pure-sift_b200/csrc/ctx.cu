@@ -211,6 +211,7 @@ psift_status psift_ctx_destroy(psift_ctx* ctx) {
   if (ctx->io.base) cudaFree(ctx->io.base);
   if (ctx->pinned.base) cudaFreeHost(ctx->pinned.base);
   if (ctx->d_error) cudaFree(ctx->d_error);
+  psift::jpeg_release(ctx);
   for (auto& p : ctx->timer.pending) {
     cudaEventDestroy(p.second.first);
     cudaEventDestroy(p.second.second);

@@ -1,0 +1,310 @@
+// Input step of the extract path: JPEG bytes -> u8 luma in device memory -> features.
+//
+// Reference: decode_validated_dynamic_image / decode_validated_luma8
+// (src/cli.rs:129-170): the header's size is checked (MIN_IMAGE_DIM, and
+// MAX_IMAGE_DIM / MAX_IMAGE_PIXELS when the pixel cap is enforced, :46-48), the
+// bytes are decoded by the image crate (0.25.10) and converted by
+// DynamicImage::into_luma8.  For RGB the crate's rgb_to_luma computes, in u32,
+// (2126 R + 7152 G + 722 B) / 10000 with truncation (Rec. 709 weights); a
+// grayscale JPEG's plane is its luma, and (w R + w G + w B) / 10000 of a gray
+// pixel returns it unchanged, so one conversion serves both.
+//
+// Here the JPEG is decoded on the GPU by nvJPEG into interleaved RGB — with the
+// hardware backend (the B200's JPEG engines) when it is present and accepts the
+// batch, else with its GPU-assisted backend — and rgb_to_luma_kernel writes the
+// luma straight into the detection batch's input slots.  nvJPEG is loaded with
+// dlopen on first use: the library loads without it, and these entries then
+// report PSIFT_ERR_INTERNAL.  The decoded pixels come from nvJPEG's IDCT and
+// chroma upsampling, not the image crate's decoder, so they can differ from the
+// reference's by a few levels; the luma conversion itself is exact.  PNG stays
+// on the host (inflate and the row filters are sequential).
+#include <dlfcn.h>
+#include <nvjpeg.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "psift_internal.cuh"
+
+namespace psift {
+namespace {
+
+constexpr uint32_t kMinImageDim = 8;            // MIN_IMAGE_DIM, src/cli.rs:46
+constexpr uint32_t kMaxImageDim = 8192;         // MAX_IMAGE_DIM, src/cli.rs:47
+constexpr uint64_t kMaxImagePixels = 25000000;  // MAX_IMAGE_PIXELS, src/cli.rs:48
+
+struct NvjpegApi {
+  bool tried = false, ok = false;
+  void* lib = nullptr;
+  decltype(&nvjpegCreateEx) create_ex = nullptr;
+  decltype(&nvjpegDestroy) destroy = nullptr;
+  decltype(&nvjpegJpegStateCreate) state_create = nullptr;
+  decltype(&nvjpegJpegStateDestroy) state_destroy = nullptr;
+  decltype(&nvjpegGetImageInfo) image_info = nullptr;
+  decltype(&nvjpegDecodeBatchedInitialize) batched_init = nullptr;
+  decltype(&nvjpegDecodeBatched) batched = nullptr;
+};
+
+NvjpegApi& nvjpeg() {
+  static NvjpegApi a;
+  static std::mutex m;
+  std::lock_guard<std::mutex> lock(m);
+  if (a.tried) return a;
+  a.tried = true;
+  for (const char* name : {"libnvjpeg.so.12", "libnvjpeg.so"}) {
+    a.lib = dlopen(name, RTLD_NOW | RTLD_LOCAL);
+    if (a.lib) break;
+  }
+  if (!a.lib) return a;
+  bool ok = true;
+  auto sym = [&](auto& fp, const char* name) {
+    fp = reinterpret_cast<std::remove_reference_t<decltype(fp)>>(dlsym(a.lib, name));
+    ok = ok && fp != nullptr;
+  };
+  sym(a.create_ex, "nvjpegCreateEx");
+  sym(a.destroy, "nvjpegDestroy");
+  sym(a.state_create, "nvjpegJpegStateCreate");
+  sym(a.state_destroy, "nvjpegJpegStateDestroy");
+  sym(a.image_info, "nvjpegGetImageInfo");
+  sym(a.batched_init, "nvjpegDecodeBatchedInitialize");
+  sym(a.batched, "nvjpegDecodeBatched");
+  a.ok = ok;
+  return a;
+}
+
+struct Backend {
+  nvjpegBackend_t kind;
+  nvjpegHandle_t h = nullptr;
+  nvjpegJpegState_t st = nullptr;
+  int batch = 0;        // batch size the state is initialised for
+  bool unusable = false;
+  explicit Backend(nvjpegBackend_t k) : kind(k) {}
+};
+
+// Per context: the hardware backend, the GPU-assisted one (created when the
+// hardware one is missing or refuses a batch), the RGB staging buffer.
+struct Decoder {
+  Backend hw{NVJPEG_BACKEND_HARDWARE};
+  Backend gpu{NVJPEG_BACKEND_GPU_HYBRID};
+  uint8_t* rgb = nullptr;
+  size_t rgb_cap = 0;
+  int last = -1;  // backend of the last successful batch
+};
+
+Decoder* decoder(psift_ctx* ctx) {
+  if (!ctx->jpeg) ctx->jpeg = new Decoder;
+  return static_cast<Decoder*>(ctx->jpeg);
+}
+
+bool backend_ready(Backend& b) {
+  if (b.unusable) return false;
+  if (b.h) return true;
+  NvjpegApi& A = nvjpeg();
+  if (A.create_ex(b.kind, nullptr, nullptr, 0, &b.h) != NVJPEG_STATUS_SUCCESS) {
+    b.h = nullptr;
+    b.unusable = true;
+    return false;
+  }
+  if (A.state_create(b.h, &b.st) != NVJPEG_STATUS_SUCCESS) {
+    A.destroy(b.h);
+    b.h = nullptr;
+    b.unusable = true;
+    return false;
+  }
+  return true;
+}
+
+void backend_release(Backend& b) {
+  NvjpegApi& A = nvjpeg();
+  if (b.st) A.state_destroy(b.st);
+  if (b.h) A.destroy(b.h);
+  b.st = nullptr;
+  b.h = nullptr;
+}
+
+// rgb_to_luma of the image crate for u8 (see the file comment), one pixel per thread.
+__global__ void rgb_to_luma_kernel(const uint8_t* __restrict__ rgb, uint8_t* __restrict__ luma, uint32_t n_px) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_px) return;
+  const uint32_t r = rgb[3 * (size_t)i], g = rgb[3 * (size_t)i + 1], b = rgb[3 * (size_t)i + 2];
+  luma[i] = (uint8_t)((2126u * r + 7152u * g + 722u * b) / 10000u);
+}
+
+struct JpegDims {
+  uint32_t w = 0, h = 0, comps = 0;
+};
+
+// Header read and the reference's size checks (src/cli.rs:137-158).
+psift_status read_header(psift_ctx* ctx, const uint8_t* data, size_t len, bool enforce_cap, JpegDims* d) {
+  NvjpegApi& A = nvjpeg();
+  if (!A.ok) return set_error(ctx, PSIFT_ERR_INTERNAL, "nvJPEG (libnvjpeg.so.12) could not be loaded");
+  Decoder* dec = decoder(ctx);
+  Backend& b = backend_ready(dec->hw) ? dec->hw : dec->gpu;
+  if (!backend_ready(b)) return set_error(ctx, PSIFT_ERR_INTERNAL, "no nvJPEG backend could be created");
+  if (!data || len == 0) return set_error(ctx, PSIFT_ERR_FORMAT, "Invalid or unsupported image header: empty buffer");
+  int nc = 0, ws[NVJPEG_MAX_COMPONENT] = {0}, hs[NVJPEG_MAX_COMPONENT] = {0};
+  nvjpegChromaSubsampling_t sub;
+  const nvjpegStatus_t s = A.image_info(b.h, data, len, &nc, &sub, ws, hs);
+  if (s != NVJPEG_STATUS_SUCCESS)
+    return set_error(ctx, PSIFT_ERR_FORMAT,
+                     "Invalid or unsupported image header (nvJPEG status " + std::to_string((int)s) + ")");
+  d->w = (uint32_t)ws[0];
+  d->h = (uint32_t)hs[0];
+  d->comps = (uint32_t)nc;
+  if (d->w < kMinImageDim || d->h < kMinImageDim)
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
+                     "Image dimensions " + std::to_string(d->w) + "x" + std::to_string(d->h) +
+                         " are too small (minimum 8x8)");
+  const uint64_t total = (uint64_t)d->w * d->h;
+  if (total > (1ull << 31))
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
+                     "Image dimensions " + std::to_string(d->w) + "x" + std::to_string(d->h) +
+                         " exceed 2^31 pixels");
+  if (enforce_cap && (d->w > kMaxImageDim || d->h > kMaxImageDim || total > kMaxImagePixels))
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
+                     "Image dimensions " + std::to_string(d->w) + "x" + std::to_string(d->h) + " (" +
+                         std::to_string(total) + " px) exceed maximum allowed (8192x8192, 25000000 px)");
+  return PSIFT_OK;
+}
+
+// Decodes n JPEGs (host bytes) and writes their luma to luma[i] (dense rows) on st.
+psift_status decode_to_luma(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths, uint32_t n,
+                            const std::vector<JpegDims>& dims, uint8_t* const* luma, cudaStream_t st) {
+  NvjpegApi& A = nvjpeg();
+  Decoder* dec = decoder(ctx);
+  std::vector<size_t> off(n);
+  size_t total = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    off[i] = total;
+    total += align_up(3 * (size_t)dims[i].w * dims[i].h, 256);
+  }
+  if (total > dec->rgb_cap) {
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    cudaFree(dec->rgb);
+    dec->rgb = nullptr;
+    dec->rgb_cap = 0;
+    const size_t cap = align_up(total, 1 << 20);
+    cudaError_t e = cudaMalloc(&dec->rgb, cap);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaMalloc(jpeg rgb)");
+    dec->rgb_cap = cap;
+  }
+  std::vector<nvjpegImage_t> dst(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    std::memset(&dst[i], 0, sizeof(nvjpegImage_t));
+    dst[i].channel[0] = dec->rgb + off[i];
+    dst[i].pitch[0] = 3 * (size_t)dims[i].w;
+  }
+  nvjpegStatus_t s = NVJPEG_STATUS_NOT_INITIALIZED;
+  int used = -1;
+  for (Backend* b : {&dec->hw, &dec->gpu}) {
+    if (!backend_ready(*b)) continue;
+    if (b->batch != (int)n) {
+      s = A.batched_init(b->h, b->st, (int)n, 1, NVJPEG_OUTPUT_RGBI);
+      if (s != NVJPEG_STATUS_SUCCESS) continue;
+      b->batch = (int)n;
+    }
+    s = A.batched(b->h, b->st, data, lengths, dst.data(), st);
+    if (s == NVJPEG_STATUS_SUCCESS) {
+      used = (int)b->kind;
+      break;
+    }
+  }
+  if (used < 0)
+    return set_error(ctx, PSIFT_ERR_FORMAT,
+                     "Failed to decode image payload (nvJPEG status " + std::to_string((int)s) + ")");
+  dec->last = used;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t px = dims[i].w * dims[i].h;
+    rgb_to_luma_kernel<<<(px + 255) / 256, 256, 0, st>>>(dec->rgb + off[i], luma[i], px);
+    ctx->launches++;
+  }
+  PSIFT_CUDA_TRY(ctx, cudaGetLastError());
+  return PSIFT_OK;
+}
+
+}  // namespace
+
+void jpeg_release(psift_ctx* ctx) {
+  if (!ctx->jpeg) return;
+  Decoder* dec = static_cast<Decoder*>(ctx->jpeg);
+  if (nvjpeg().ok) {
+    backend_release(dec->hw);
+    backend_release(dec->gpu);
+  }
+  cudaFree(dec->rgb);
+  delete dec;
+  ctx->jpeg = nullptr;
+}
+
+}  // namespace psift
+
+using namespace psift;
+
+extern "C" {
+
+psift_status psift_jpeg_info(psift_ctx* ctx, const uint8_t* data, size_t length, int32_t enforce_pixel_cap,
+                             uint32_t* width, uint32_t* height, uint32_t* components) {
+  if (!ctx || !width || !height) return PSIFT_ERR_INVALID_ARGUMENT;
+  PSIFT_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  JpegDims d;
+  psift_status st = read_header(ctx, data, length, enforce_pixel_cap != 0, &d);
+  *width = d.w;
+  *height = d.h;
+  if (components) *components = d.comps;
+  return st;
+}
+
+psift_status psift_decode_jpeg_luma(psift_ctx* ctx, const uint8_t* data, size_t length, int32_t enforce_pixel_cap,
+                                    uint8_t* luma, size_t capacity, uint32_t* width, uint32_t* height) {
+  if (!ctx || !width || !height) return PSIFT_ERR_INVALID_ARGUMENT;
+  PSIFT_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  std::vector<JpegDims> dims(1);
+  psift_status st = read_header(ctx, data, length, enforce_pixel_cap != 0, &dims[0]);
+  *width = dims[0].w;
+  *height = dims[0].h;
+  if (st != PSIFT_OK) return st;
+  const size_t px = (size_t)dims[0].w * dims[0].h;
+  if (px > capacity) return set_error(ctx, PSIFT_ERR_CAPACITY, "luma output capacity too small");
+  if (!luma) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null luma output");
+  if ((st = io_reserve(ctx, px)) != PSIFT_OK) return st;
+  uint8_t* d_luma = (uint8_t*)ctx->io.base;
+  const uint8_t* const bufs[1] = {data};
+  const size_t lens[1] = {length};
+  uint8_t* const outs[1] = {d_luma};
+  if ((st = decode_to_luma(ctx, bufs, lens, 1, dims, outs, ctx->stream)) != PSIFT_OK) return st;
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(luma, d_luma, px, cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PSIFT_OK;
+}
+
+psift_status psift_detect_and_compute_jpeg_batch(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths,
+                                                 uint32_t n, int32_t enforce_pixel_cap,
+                                                 const psift_sift_config* cfg, psift_features* outs) {
+  if (!ctx || !data || !lengths || !outs || n == 0) return PSIFT_ERR_INVALID_ARGUMENT;
+  PSIFT_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  std::vector<JpegDims> dims(n);
+  std::vector<psift_image_u8> imgs(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const psift_status st = read_header(ctx, data[i], lengths[i], enforce_pixel_cap != 0, &dims[i]);
+    if (st != PSIFT_OK) return st;
+    imgs[i] = psift_image_u8{nullptr, dims[i].h, dims[i].w, dims[i].w};
+  }
+  const DeviceFill fill = [&](char* extra, const std::vector<size_t>& dev_off, cudaStream_t st) {
+    std::vector<uint8_t*> luma(n);
+    for (uint32_t i = 0; i < n; ++i) luma[i] = (uint8_t*)extra + dev_off[i];
+    return decode_to_luma(ctx, data, lengths, n, dims, luma.data(), st);
+  };
+  return detect_batch_host_out(ctx, imgs.data(), n, cfg, outs, &fill);
+}
+
+psift_status psift_ctx_jpeg_backend(psift_ctx* ctx, int32_t* backend) {
+  if (!ctx || !backend) return PSIFT_ERR_INVALID_ARGUMENT;
+  *backend = ctx->jpeg ? static_cast<Decoder*>(ctx->jpeg)->last : -1;
+  return PSIFT_OK;
+}
+
+}  // extern "C"

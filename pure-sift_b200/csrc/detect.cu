@@ -810,6 +810,20 @@ psift_status psift_host_free(psift_ctx* ctx, void* p) {
 //   through the context's pinned staging.
 psift_status psift_detect_and_compute_u8_batch(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
                                                const psift_sift_config* cfg, psift_features* outs) {
+  return psift::detect_batch_host_out(ctx, images, n, cfg, outs, nullptr);
+}
+
+}  // extern "C"
+
+namespace psift {
+
+// The host-output batch: features of n u8 images into host arrays, one launch
+// per stage, two chunks on two streams.  Inputs come from host memory
+// (images[i].data, copied per chunk), or, with `fill`, are written into their
+// device slots by fill (on ctx->stream, before the chunks fork; images[i].data
+// is then unused and the slots are dense rows of width bytes).
+psift_status detect_batch_host_out(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
+                                   const psift_sift_config* cfg, psift_features* outs, const DeviceFill* fill) {
   psift_status st = check_common(ctx, cfg);
   if (st != PSIFT_OK) return st;
   if (!images || !outs || n == 0) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad batch argument");
@@ -820,7 +834,7 @@ psift_status psift_detect_and_compute_u8_batch(psift_ctx* ctx, const psift_image
   for (uint32_t i = 0; i < n; ++i) {
     const psift_image_u8& im = images[i];
     const psift_features& o = outs[i];
-    if ((im.height && im.width && !im.data) || im.row_stride < im.width)
+    if (!fill && ((im.height && im.width && !im.data) || im.row_stride < im.width))
       return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "bad batch image descriptor");
     if (o.capacity && (!o.x || !o.y || !o.scale || !o.response || !o.orientation || !o.descriptors))
       return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null feature output array");
@@ -834,7 +848,7 @@ psift_status psift_detect_and_compute_u8_batch(psift_ctx* ctx, const psift_image
     const size_t px = (size_t)im.height * im.width;
     dev_off[i] = dev_total;
     dev_total += align_up(px, 256);
-    in_pin[i] = px ? (char)is_host_pinned(im.data) : 1;
+    in_pin[i] = (fill || !px) ? 1 : (char)is_host_pinned(im.data);
     in_off[i] = stage_in;
     if (!in_pin[i]) stage_in += align_up(px, 64);
     out_pin[i] = (char)(o.capacity && is_host_pinned(o.x) && is_host_pinned(o.y) && is_host_pinned(o.scale) &&
@@ -861,12 +875,13 @@ psift_status psift_detect_and_compute_u8_batch(psift_ctx* ctx, const psift_image
   // the device plan table is uploaded once for the whole batch; chunk views index into it
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice,
                                       ctx->stream));
+  if (fill && (st = (*fill)((char*)extra, dev_off, ctx->stream)) != PSIFT_OK) return st;
   PSIFT_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
   PSIFT_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream2, ctx->ev_fork, 0));
   for (uint32_t c = 0; c < n_chunks; ++c) {
     const uint32_t b = c == 0 ? 0 : split, e = c == 0 ? (n_chunks == 1 ? n : split) : n;
     cudaStream_t sc = streams[c];
-    for (uint32_t i = b; i < e; ++i) {
+    for (uint32_t i = b; i < e && !fill; ++i) {
       const psift_image_u8& im = images[i];
       const size_t px = (size_t)im.height * im.width;
       if (!px) continue;
@@ -947,6 +962,10 @@ psift_status psift_detect_and_compute_u8_batch(psift_ctx* ctx, const psift_image
   if (capacity_short) return set_error(ctx, PSIFT_ERR_CAPACITY, "feature output capacity too small");
   return PSIFT_OK;
 }
+
+}  // namespace psift
+
+extern "C" {
 
 psift_status psift_detect_and_compute_batch_dev(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
                                                 const psift_sift_config* cfg, psift_features* outs,

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -92,6 +93,8 @@ struct psift_ctx {
   std::map<std::string, GraphEntry> graphs;
   std::map<std::string, int> graph_seen;
   uint64_t graph_replays = 0;
+  // nvJPEG decoder of the JPEG entries (decode.cu), created on first use.
+  void* jpeg = nullptr;
 };
 
 namespace psift {
@@ -122,6 +125,12 @@ void tracking_stats(const psift_match* m, uint32_t n, const uint8_t* mask, const
                     const float* q_ori, const float* t_scale, const float* t_ori, psift_tracking_summary* out);
 // CTAs of `func` resident on the whole device at once (occupancy x SMs), cached.
 cudaError_t resident_ctas(const void* func, int threads, size_t smem, int* out);
+// Writes the batch's u8 inputs into their device slots (extra + dev_off[i], dense
+// rows of the image's width) on stream st.
+using DeviceFill = std::function<psift_status(char* extra, const std::vector<size_t>& dev_off, cudaStream_t st)>;
+psift_status detect_batch_host_out(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
+                                   const psift_sift_config* cfg, psift_features* outs, const DeviceFill* fill);
+void jpeg_release(psift_ctx* ctx);
 
 // Stage timing: `StageScope sc(ctx, STAGE_X);` records events around the launches
 // issued while it is alive (no-op unless timing is enabled).

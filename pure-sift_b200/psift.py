@@ -178,6 +178,13 @@ _SIGS = {
                                       C.c_void_p]),
     "psift_build_pyramid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_size_t,
                                       C.POINTER(CSiftConfig), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "psift_jpeg_info": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32, C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "psift_decode_jpeg_luma": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32, C.c_void_p, C.c_size_t,
+                                         C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "psift_detect_and_compute_jpeg_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32,
+                                                      C.POINTER(CSiftConfig), C.c_void_p]),
+    "psift_ctx_jpeg_backend": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "psift_detect_and_compute_u8_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CSiftConfig),
                                                     C.c_void_p]),
     "psift_ctx_enable_graphs": (C.c_int, [C.c_void_p, C.c_int]),
@@ -290,6 +297,13 @@ class Context:
     def check(self, st: int):
         if st != PSIFT_OK:
             raise PsiftError(st, self.lib.psift_last_error(self.handle).decode())
+
+    @property
+    def jpeg_backend(self) -> int:
+        """nvJPEG backend of the last decoded JPEG batch (3 hardware, 2 GPU-assisted, -1 none)."""
+        b = C.c_int32()
+        self.check(self.lib.psift_ctx_jpeg_backend(self.handle, C.byref(b)))
+        return int(b.value)
 
     @property
     def launch_count(self) -> int:
@@ -547,6 +561,33 @@ class Sift:
             ctx.check(st)
             return [outs[i].view(int(couts[i].count)) for i in range(n)]
 
+    def detect_and_compute_jpeg_batch(self, blobs, enforce_pixel_cap: bool = False, outs=None,
+                                      ctx: Context | None = None) -> "list[Features]":
+        """JPEG bytes -> features (psift_detect_and_compute_jpeg_batch): decoded on the
+        GPU into the batch's inputs (decode_validated_luma8, src/cli.rs:164-170), then
+        as ``detect_and_compute_batch_u8``."""
+        ctx = ctx or default_context()
+        bufs = [bytes(b) for b in blobs]
+        n = len(bufs)
+        if n == 0:
+            return []
+        ptrs = (C.c_char_p * n)(*bufs)
+        lens = (C.c_size_t * n)(*[len(b) for b in bufs])
+        cfg = self.config.to_c()
+        cap = self.config.max_features_ or 16384
+        outs = list(outs) if outs is not None else [Features.empty(cap) for _ in range(n)]
+        while True:
+            couts = (CFeatures * n)(*[_c_features(o) for o in outs])
+            st = ctx.lib.psift_detect_and_compute_jpeg_batch(ctx.handle, ptrs, lens, n, int(bool(enforce_pixel_cap)),
+                                                             C.byref(cfg), couts)
+            short = [i for i in range(n) if couts[i].count > len(outs[i])]
+            if st == PSIFT_ERR_CAPACITY and short:
+                for i in short:
+                    outs[i] = Features.empty(int(couts[i].count))
+                continue
+            ctx.check(st)
+            return [outs[i].view(int(couts[i].count)) for i in range(n)]
+
     def detect_and_compute_u8(self, img: np.ndarray, ctx: Context | None = None) -> Features:
         return self._run(img, True, ctx)
 
@@ -622,6 +663,27 @@ def match_arrays(q_desc, t_desc, q_xy, t_xy, options: MatchOptions = MatchOption
 def match_descriptors(query: Features, target: Features, ratio_threshold: float, ctx: Context | None = None):
     """``match_descriptors`` (src/pipeline.rs:1845-1858)."""
     return Matcher.new(MatchOptions(ratio=ratio_threshold)).match_(query, target, ctx)
+
+
+# ---------------------------------------------------------------- JPEG input
+def jpeg_info(blob: bytes, enforce_pixel_cap: bool = False, ctx: Context | None = None):
+    """(width, height, components) of a JPEG, with the reference's size checks."""
+    ctx = ctx or default_context()
+    w, h, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    ctx.check(ctx.lib.psift_jpeg_info(ctx.handle, blob, len(blob), int(bool(enforce_pixel_cap)), C.byref(w),
+                                      C.byref(h), C.byref(c)))
+    return int(w.value), int(h.value), int(c.value)
+
+
+def decode_jpeg_luma(blob: bytes, enforce_pixel_cap: bool = False, ctx: Context | None = None) -> np.ndarray:
+    """``decode_validated_luma8`` (src/cli.rs:164-170) for a JPEG, decoded on the GPU."""
+    ctx = ctx or default_context()
+    w, h, _ = jpeg_info(blob, enforce_pixel_cap, ctx)
+    out = np.zeros((h, w), np.uint8)
+    ww, hh = C.c_uint32(), C.c_uint32()
+    ctx.check(ctx.lib.psift_decode_jpeg_luma(ctx.handle, blob, len(blob), int(bool(enforce_pixel_cap)),
+                                             out.ctypes.data, out.size, C.byref(ww), C.byref(hh)))
+    return out
 
 
 # ---------------------------------------------------------------- catalog codes
