@@ -608,6 +608,22 @@ def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int =
     offs = np.cumsum([0] + [len(f) for _, f, _ in pairs])
     probs = [probs_all[offs[i]:offs[i + 1]] for i in range(n_pairs)]
     stream = torch.cuda.ExternalStream(ctx.stream)
+    # device-resident inference (psift_mlp_infer_dev), CUDA events on the context's stream
+    feats_d = torch.from_numpy(feats).cuda()
+    params_d = torch.from_numpy(np.ascontiguousarray(mlp.params, dtype=np.float32)).cuda()
+    prob_d = torch.empty(feats.shape[0], device="cuda", dtype=torch.float32)
+    torch.cuda.synchronize()
+    infer = lambda: ctx.check(ctx.lib.psift_mlp_infer_dev(ctx.handle, params_d.data_ptr(), feats_d.data_ptr(),
+                                                           feats.shape[0], prob_d.data_ptr()))
+    infer()
+    ctx.synchronize()
+    i0, i1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    i0.record(stream)
+    for _ in range(reps):
+        infer()
+    i1.record(stream)
+    ctx.synchronize()
+    infer_dev_ms = i0.elapsed_time(i1) / reps
     out = {}
     for name, w in (("plain", None), ("guided", probs)):
         jobs, keep = psift.ransac_jobs([r for r, _, _ in pairs], weights=w)
@@ -633,7 +649,10 @@ def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int =
         "plain_mean_iterations": float(p["iters"].mean()), "guided_mean_iterations": float(gd["iters"].mean()),
         "plain_total_inliers": int(p["inliers"].sum()), "guided_total_inliers": int(gd["inliers"].sum()),
         "pairs_guided_within_1pct_of_plain": float(ok.mean()),
-        "mlp_train_s_400_steps": train_s, "mlp_infer_ms_all_matches": infer_s * 1e3,
+        "mlp_train_s_400_steps": train_s, "mlp_infer_host_api_ms_all_matches": infer_s * 1e3,
+        "mlp_infer_device_ms_all_matches": infer_dev_ms,
+        "guided_plus_device_inference_ms": gd["ms"] + infer_dev_ms,
+        "speedup_with_inference": p["ms"] / (gd["ms"] + infer_dev_ms),
         "matches_total": int(offs[-1]),
     }
 
@@ -678,10 +697,20 @@ def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
         r, g, bl = (rgb[..., k].astype(np.uint32) for k in range(3))
         _ = ((2126 * r + 7152 * g + 722 * bl) // 10000).astype(np.uint8)
     cpu_decode_ms = (time.perf_counter() - t0) / n * 1e3
+    # 64 images (the same files repeated): nvJPEG's GPU-assisted backend decodes the
+    # Huffman stage on the GPU only for batches of more than 50 images
+    blobs8 = blobs * 8
+    outs8 = outs + [psift.Features.pinned(4096, ctx) for _ in range(7 * n)]
+    sift.detect_and_compute_jpeg_batch(blobs8, outs=outs8, ctx=ctx)
+    t0 = time.perf_counter()
+    for _ in range(reps // 4 or 1):
+        sift.detect_and_compute_jpeg_batch(blobs8, outs=outs8, ctx=ctx)
+    jpeg8_s = (time.perf_counter() - t0) / (reps // 4 or 1)
     return {
         "workload": f"{n} colour {WIDTH}x{HEIGHT} JPEGs (4:2:0, q90, {sum(map(len, blobs)) / n / 1e3:.0f} KB each), "
                     "host bytes -> pinned host features, host API wall clock",
         "jpeg_images_per_s": n / jpeg_s, "u8_batch_images_per_s": n / u8_s,
+        "jpeg_images_per_s_batch_of_64": 8 * n / jpeg8_s,
         "jpeg_minus_u8_input_ms_per_batch": (jpeg_s - u8_s) * 1e3, "cpu_decode_ms_per_image_1_thread": cpu_decode_ms,
         "nvjpeg_backend": ctx.jpeg_backend, "features_per_image": [len(f) for f in feats[:4]],
     }
