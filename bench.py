@@ -660,9 +660,10 @@ def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int =
 def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
     """Input step: 8 colour 1920x1080 JPEGs (three independent 2000-blob fields as
     R, G, B; 4:2:0, quality 90) in host memory -> features in host memory through
-    psift_detect_and_compute_jpeg_batch (nvJPEG decode on the GPU into the batch's
-    inputs), against the host u8 batch entry given the already decoded luma, and the
-    CPU decode (PIL + the image crate's luma formula, one thread) per image."""
+    psift_detect_and_compute_jpeg_batch (nvJPEG: Huffman stage on host threads, the
+    rest on the GPU, into the batch's inputs), against the host u8 batch entry given
+    the already decoded luma, and the CPU decode (PIL + the image crate's luma
+    formula, one thread) per image; also 64-image batches and the single-call mode."""
     import io
     from PIL import Image
     import psift
@@ -681,6 +682,7 @@ def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
     for _ in range(reps):
         feats = sift.detect_and_compute_jpeg_batch(blobs, outs=outs, ctx=ctx)
     jpeg_s = (time.perf_counter() - t0) / reps
+    backend = ctx.jpeg_backend
     lumas = [psift.decode_jpeg_luma(b, ctx=ctx) for b in blobs]
     pin = [psift.pinned_empty(l.shape, np.uint8, ctx) for l in lumas]
     for d, l in zip(pin, lumas):
@@ -697,22 +699,34 @@ def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
         r, g, bl = (rgb[..., k].astype(np.uint32) for k in range(3))
         _ = ((2126 * r + 7152 * g + 722 * bl) // 10000).astype(np.uint8)
     cpu_decode_ms = (time.perf_counter() - t0) / n * 1e3
-    # 64 images (the same files repeated): nvJPEG's GPU-assisted backend decodes the
-    # Huffman stage on the GPU only for batches of more than 50 images
+    # 64 images (the same files repeated); and both batch sizes with one batched
+    # call on the calling thread (nvJPEG's GPU-assisted backend, whose Huffman
+    # stage runs on the GPU only for batches of more than 50 images)
     blobs8 = blobs * 8
     outs8 = outs + [psift.Features.pinned(4096, ctx) for _ in range(7 * n)]
-    sift.detect_and_compute_jpeg_batch(blobs8, outs=outs8, ctx=ctx)
-    t0 = time.perf_counter()
-    for _ in range(reps // 4 or 1):
-        sift.detect_and_compute_jpeg_batch(blobs8, outs=outs8, ctx=ctx)
-    jpeg8_s = (time.perf_counter() - t0) / (reps // 4 or 1)
+
+    def timed(bl, ou, r):
+        sift.detect_and_compute_jpeg_batch(bl, outs=ou, ctx=ctx)
+        t = time.perf_counter()
+        for _ in range(r):
+            sift.detect_and_compute_jpeg_batch(bl, outs=ou, ctx=ctx)
+        return (time.perf_counter() - t) / r
+    jpeg8_s = timed(blobs8, outs8, reps // 4 or 1)
+    ctx.set_jpeg_threads(1)
+    single8_s = timed(blobs, outs, reps // 2 or 1)
+    single64_s = timed(blobs8, outs8, reps // 4 or 1)
+    single_backend = ctx.jpeg_backend
+    ctx.set_jpeg_threads(0)
     return {
         "workload": f"{n} colour {WIDTH}x{HEIGHT} JPEGs (4:2:0, q90, {sum(map(len, blobs)) / n / 1e3:.0f} KB each), "
                     "host bytes -> pinned host features, host API wall clock",
         "jpeg_images_per_s": n / jpeg_s, "u8_batch_images_per_s": n / u8_s,
         "jpeg_images_per_s_batch_of_64": 8 * n / jpeg8_s,
+        "single_call_images_per_s": {"batch_8": n / single8_s, "batch_64": 8 * n / single64_s,
+                                     "nvjpeg_backend": single_backend},
+        "host_decode_threads": min(os.cpu_count() or 1, 16),
         "jpeg_minus_u8_input_ms_per_batch": (jpeg_s - u8_s) * 1e3, "cpu_decode_ms_per_image_1_thread": cpu_decode_ms,
-        "nvjpeg_backend": ctx.jpeg_backend, "features_per_image": [len(f) for f in feats[:4]],
+        "nvjpeg_backend": backend, "features_per_image": [len(f) for f in feats[:4]],
     }
 
 

@@ -230,7 +230,16 @@ psift_status psift_decode_jpeg_luma(psift_ctx* ctx, const uint8_t* data, size_t 
 psift_status psift_detect_and_compute_jpeg_batch(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths,
                                                  uint32_t n, int32_t enforce_pixel_cap,
                                                  const psift_sift_config* cfg, psift_features* outs);
-/* nvJPEG backend of the context's last decoded batch: 3 = hardware, 2 = GPU-assisted, -1 = none yet. */
+/* How a context decodes a JPEG batch.  threads = 0 (default): the batch is split
+ * into contiguous shares of at most 50 images over up to 16 host threads (the
+ * hardware concurrency), each share decoded by nvJPEG's hybrid backend (Huffman
+ * stage on its thread, the rest on its own stream; the context's stream waits
+ * for all); threads = k > 1: k threads; threads = 1: one batched call on the
+ * calling thread (the hardware backend when available, else the GPU-assisted
+ * one, which moves the Huffman stage to the GPU for batches above 50 images). */
+psift_status psift_ctx_set_jpeg_threads(psift_ctx* ctx, int32_t threads);
+/* nvJPEG backend of the context's last decoded batch: 3 = hardware, 2 = GPU-assisted,
+ * 1 = hybrid on host threads, -1 = none yet. */
 psift_status psift_ctx_jpeg_backend(psift_ctx* ctx, int32_t* backend);
 
 /* Page-locked host memory for the batch entry's inputs and outputs. */

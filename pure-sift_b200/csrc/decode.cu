@@ -25,6 +25,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -87,9 +88,21 @@ struct Backend {
 
 // Per context: the hardware backend, the GPU-assisted one (created when the
 // hardware one is missing or refuses a batch), the RGB staging buffer.
+// A host thread's share of a batch: its own handle and state (only the header
+// query is documented thread-safe), CUDA stream and completion event.
+struct Worker {
+  Backend b{NVJPEG_BACKEND_HYBRID};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  nvjpegStatus_t status = NVJPEG_STATUS_SUCCESS;
+};
+
 struct Decoder {
   Backend hw{NVJPEG_BACKEND_HARDWARE};
   Backend gpu{NVJPEG_BACKEND_GPU_HYBRID};
+  std::vector<Worker> workers;
+  cudaEvent_t start = nullptr;
+  int threads = 0;  // 0: automatic; 1: one batched call on the calling thread
   uint8_t* rgb = nullptr;
   size_t rgb_cap = 0;
   int last = -1;  // backend of the last successful batch
@@ -125,6 +138,93 @@ void backend_release(Backend& b) {
   b.st = nullptr;
   b.h = nullptr;
 }
+
+constexpr int kMaxJpegThreads = 16;
+constexpr uint32_t kWorkerBatchMax = 50;  // the hybrid stage stays on the host up to 50 images
+
+bool worker_ready(psift_ctx* ctx, Worker& w) {
+  if (!backend_ready(w.b)) return false;
+  if (!w.stream && cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    w.stream = nullptr;
+    return false;
+  }
+  if (!w.done && cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming) != cudaSuccess) {
+    w.done = nullptr;
+    return false;
+  }
+  (void)ctx;
+  return true;
+}
+
+// Decodes images [b, e) of the batch with worker w: the Huffman stage on this
+// host thread, the rest on w.stream; w.done is recorded after it.
+void worker_decode(const psift_ctx* ctx, Worker& w, const uint8_t* const* data, const size_t* lengths,
+                   nvjpegImage_t* dst, uint32_t b, uint32_t e) {
+  NvjpegApi& A = nvjpeg();
+  w.status = NVJPEG_STATUS_SUCCESS;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) {
+    w.status = NVJPEG_STATUS_EXECUTION_FAILED;
+    return;
+  }
+  const int n = (int)(e - b);
+  if (w.b.batch != n) {
+    w.status = A.batched_init(w.b.h, w.b.st, n, 1, NVJPEG_OUTPUT_RGBI);
+    if (w.status != NVJPEG_STATUS_SUCCESS) return;
+    w.b.batch = n;
+  }
+  w.status = A.batched(w.b.h, w.b.st, data + b, lengths + b, dst + b, w.stream);
+  if (w.status == NVJPEG_STATUS_SUCCESS && cudaEventRecord(w.done, w.stream) != cudaSuccess)
+    w.status = NVJPEG_STATUS_EXECUTION_FAILED;
+}
+
+// The batch over T host threads (the calling one included), contiguous shares.
+// Returns false when the workers cannot be set up or one of them failed.
+bool decode_threaded(psift_ctx* ctx, Decoder* dec, const uint8_t* const* data, const size_t* lengths, uint32_t n,
+                     nvjpegImage_t* dst, cudaStream_t st) {
+  const unsigned hc = std::max(1u, std::thread::hardware_concurrency());
+  int T = dec->threads > 1 ? dec->threads : (int)std::min<unsigned>(hc, kMaxJpegThreads);
+  T = std::max(1, std::min<int>(T, (int)n));
+  while ((n + T - 1) / T > kWorkerBatchMax && T < (int)n) ++T;
+  if ((int)dec->workers.size() < T) dec->workers.resize(T);
+  for (int t = 0; t < T; ++t)
+    if (!worker_ready(ctx, dec->workers[t])) return false;
+  if (!dec->start && cudaEventCreateWithFlags(&dec->start, cudaEventDisableTiming) != cudaSuccess) return false;
+  // The RGB staging buffer is free once the work queued before on st is done.
+  if (cudaEventRecord(dec->start, st) != cudaSuccess) return false;
+  for (int t = 0; t < T; ++t)
+    if (cudaStreamWaitEvent(dec->workers[t].stream, dec->start, 0) != cudaSuccess) return false;
+  std::vector<std::thread> pool;
+  const uint32_t per = n / T, extra = n % T;
+  uint32_t b = 0;
+  std::vector<std::pair<uint32_t, uint32_t>> range(T);
+  for (int t = 0; t < T; ++t) {
+    const uint32_t e = b + per + ((uint32_t)t < extra ? 1 : 0);
+    range[t] = {b, e};
+    b = e;
+  }
+  for (int t = 1; t < T; ++t) {
+    try {
+      pool.emplace_back(worker_decode, ctx, std::ref(dec->workers[t]), data, lengths, dst, range[t].first,
+                        range[t].second);
+    } catch (...) {  // no thread available: this share runs on the calling thread
+      worker_decode(ctx, dec->workers[t], data, lengths, dst, range[t].first, range[t].second);
+    }
+  }
+  worker_decode(ctx, dec->workers[0], data, lengths, dst, range[0].first, range[0].second);
+  for (auto& th : pool) th.join();
+  bool ok = true;
+  for (int t = 0; t < T; ++t) {
+    Worker& w = dec->workers[t];
+    if (w.status == NVJPEG_STATUS_SUCCESS) {
+      ok = ok && cudaStreamWaitEvent(st, w.done, 0) == cudaSuccess;
+    } else {
+      ok = false;
+      cudaStreamSynchronize(w.stream);  // nothing of a failed share may still write the staging buffer
+    }
+  }
+  return ok;
+}
+
 
 // rgb_to_luma of the image crate for u8 (see the file comment), one pixel per thread.
 __global__ void rgb_to_luma_kernel(const uint8_t* __restrict__ rgb, uint8_t* __restrict__ luma, uint32_t n_px) {
@@ -200,7 +300,12 @@ psift_status decode_to_luma(psift_ctx* ctx, const uint8_t* const* data, const si
   }
   nvjpegStatus_t s = NVJPEG_STATUS_NOT_INITIALIZED;
   int used = -1;
+  if (dec->threads != 1 && decode_threaded(ctx, dec, data, lengths, n, dst.data(), st)) {
+    used = (int)NVJPEG_BACKEND_HYBRID;
+    s = NVJPEG_STATUS_SUCCESS;
+  }
   for (Backend* b : {&dec->hw, &dec->gpu}) {
+    if (used >= 0) break;
     if (!backend_ready(*b)) continue;
     if (b->batch != (int)n) {
       s = A.batched_init(b->h, b->st, (int)n, 1, NVJPEG_OUTPUT_RGBI);
@@ -234,7 +339,13 @@ void jpeg_release(psift_ctx* ctx) {
   if (nvjpeg().ok) {
     backend_release(dec->hw);
     backend_release(dec->gpu);
+    for (Worker& w : dec->workers) backend_release(w.b);
   }
+  for (Worker& w : dec->workers) {
+    if (w.done) cudaEventDestroy(w.done);
+    if (w.stream) cudaStreamDestroy(w.stream);
+  }
+  if (dec->start) cudaEventDestroy(dec->start);
   cudaFree(dec->rgb);
   delete dec;
   ctx->jpeg = nullptr;
@@ -299,6 +410,12 @@ psift_status psift_detect_and_compute_jpeg_batch(psift_ctx* ctx, const uint8_t* 
     return decode_to_luma(ctx, data, lengths, n, dims, luma.data(), st);
   };
   return detect_batch_host_out(ctx, imgs.data(), n, cfg, outs, &fill);
+}
+
+psift_status psift_ctx_set_jpeg_threads(psift_ctx* ctx, int32_t threads) {
+  if (!ctx || threads < 0 || threads > 256) return PSIFT_ERR_INVALID_ARGUMENT;
+  decoder(ctx)->threads = threads;
+  return PSIFT_OK;
 }
 
 psift_status psift_ctx_jpeg_backend(psift_ctx* ctx, int32_t* backend) {

@@ -185,6 +185,7 @@ _SIGS = {
     "psift_detect_and_compute_jpeg_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32,
                                                       C.POINTER(CSiftConfig), C.c_void_p]),
     "psift_ctx_jpeg_backend": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "psift_ctx_set_jpeg_threads": (C.c_int, [C.c_void_p, C.c_int32]),
     "psift_detect_and_compute_u8_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CSiftConfig),
                                                     C.c_void_p]),
     "psift_ctx_enable_graphs": (C.c_int, [C.c_void_p, C.c_int]),
@@ -298,9 +299,14 @@ class Context:
         if st != PSIFT_OK:
             raise PsiftError(st, self.lib.psift_last_error(self.handle).decode())
 
+    def set_jpeg_threads(self, threads: int):
+        """JPEG batch decode: 0 = shares over host threads (default), 1 = one batched call."""
+        self.check(self.lib.psift_ctx_set_jpeg_threads(self.handle, int(threads)))
+
     @property
     def jpeg_backend(self) -> int:
-        """nvJPEG backend of the last decoded JPEG batch (3 hardware, 2 GPU-assisted, -1 none)."""
+        """nvJPEG backend of the last decoded JPEG batch (3 hardware, 2 GPU-assisted, 1 hybrid
+        on host threads, -1 none)."""
         b = C.c_int32()
         self.check(self.lib.psift_ctx_jpeg_backend(self.handle, C.byref(b)))
         return int(b.value)

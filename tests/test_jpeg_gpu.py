@@ -45,6 +45,29 @@ def test_decoded_luma_against_cpu_decoder(label, make, sub, mean_tol, max_tol):
     assert mean <= mean_tol and mx <= max_tol
 
 
+def test_single_call_mode_against_cpu_decoder():
+    # threads = 1: one batched call (GPU-assisted backend) instead of shares on host threads
+    ctx = psift.Context(0)
+    try:
+        ctx.set_jpeg_threads(1)
+        img = J.color_image(800, 600, 41)
+        blob = J.encode(img, 90, 2)
+        one = psift.decode_jpeg_luma(blob, ctx=ctx)
+        assert ctx.jpeg_backend in (2, 3)
+        mean, mx = _stats(one, J.cpu_luma(blob))
+        ctx.set_jpeg_threads(0)
+        shared = psift.decode_jpeg_luma(blob, ctx=ctx)
+        assert ctx.jpeg_backend == 1
+        m2, x2 = _stats(one, shared)
+        print(f"single call vs CPU decoder: mean {mean:.3f}, max {mx}; single call vs host-thread shares: "
+              f"mean {m2:.3f}, max {x2}")
+        assert mean <= 1.0 and mx <= 24
+        with pytest.raises(psift.PsiftError):
+            ctx.set_jpeg_threads(-1)
+    finally:
+        ctx.close()
+
+
 def test_gray_rgb_pixels_keep_their_level():
     # a gray image stored as 4:4:4 colour: R = G = B up to the codec, luma = that level
     g = J.gray_image(320, 240, 5)
