@@ -683,6 +683,25 @@ def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
         feats = sift.detect_and_compute_jpeg_batch(blobs, outs=outs, ctx=ctx)
     jpeg_s = (time.perf_counter() - t0) / reps
     backend = ctx.jpeg_backend
+    # two host threads with a context each, alternate batches: one thread's Huffman
+    # stage overlaps the other's GPU work
+    ctx2 = psift.Context(ctx.device)
+    outs2 = [psift.Features.pinned(4096, ctx2) for _ in range(n)]
+    sift.detect_and_compute_jpeg_batch(blobs, outs=outs2, ctx=ctx2)
+    pairs = [(ctx, outs), (ctx2, outs2)]
+
+    def worker(wi):
+        c, o = pairs[wi]
+        for _ in range(wi, reps, 2):
+            sift.detect_and_compute_jpeg_batch(blobs, outs=o, ctx=c)
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=worker, args=(wi,)) for wi in range(2)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    jpeg2_s = (time.perf_counter() - t0) / reps
+    ctx2.close()
     lumas = [psift.decode_jpeg_luma(b, ctx=ctx) for b in blobs]
     pin = [psift.pinned_empty(l.shape, np.uint8, ctx) for l in lumas]
     for d, l in zip(pin, lumas):
@@ -722,6 +741,7 @@ def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
                     "host bytes -> pinned host features, host API wall clock",
         "jpeg_images_per_s": n / jpeg_s, "u8_batch_images_per_s": n / u8_s,
         "jpeg_images_per_s_batch_of_64": 8 * n / jpeg8_s,
+        "jpeg_images_per_s_2_host_threads": n / jpeg2_s,
         "single_call_images_per_s": {"batch_8": n / single8_s, "batch_64": 8 * n / single64_s,
                                      "nvjpeg_backend": single_backend},
         "host_decode_threads": min(os.cpu_count() or 1, 16),
@@ -904,6 +924,27 @@ def run_ours(args):
         for im in ims:
             sift.detect_and_compute_u8(im, ctx=ctx)
     single_s = (time.perf_counter() - t1) / single_rounds
+    # one call per image from 4 host threads with a context each (a drop-in wrapper
+    # holding one context per rayon worker)
+    n_callers = 4
+    callers = [psift.Context(local) for _ in range(n_callers)]
+    for c in callers:
+        for _ in range(3):
+            sift.detect_and_compute_u8(ims[0], ctx=c)
+
+    def caller(ci):
+        for _ in range(single_rounds):
+            for k in range(ci, B, n_callers):
+                sift.detect_and_compute_u8(ims[k], ctx=callers[ci])
+    t1 = time.perf_counter()
+    ths = [threading.Thread(target=caller, args=(ci,)) for ci in range(n_callers)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    single4_s = (time.perf_counter() - t1) / single_rounds
+    for c in callers:
+        c.close()
     if dist:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -931,7 +972,8 @@ def run_ours(args):
                     "api": "psift_detect_and_compute_u8_batch (8 pinned host images -> pinned host features), "
                            "2 host threads with a context each, alternate steps",
                     "one_thread_images_per_s": e2e_single,
-                    "single_image_api_images_per_s": B / single_s},
+                    "single_image_api_images_per_s": B / single_s,
+                    "single_image_api_4_host_threads_images_per_s": B / single4_s},
             "roofline": {"kernel": "blur_level_kernel (pyramid: blur + DoG + decimation)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": NCU_TRAFFIC_BLUR_LEVEL,

@@ -283,6 +283,7 @@ class Context:
         if st != PSIFT_OK:
             raise PsiftError(st, "psift_ctx_create failed (no usable sm_100 device?)")
         self.handle = h
+        self.device = device
 
     def close(self):
         if getattr(self, "handle", None):

@@ -83,3 +83,41 @@ def test_gpu_batch_vs_f64_uneven():
         k64 = O.detect_keypoints_f64(u8, 4, 3, 0.015, True)
         kp = _gpu_keypoint_error(u8, k64)
         _check(f"GPU batch image {k} ({u8.shape[1]}x{u8.shape[0]})", kp, ft)
+
+
+def test_match_distances_and_decisions_vs_f64():
+    """Lowe matching stated against f64: every returned match's distance and ratio
+    against the f64 values of the same f32 descriptors (relative error within 1e-5:
+    128 f32 products summed in order), and the f64 ratio test taking the same
+    decisions for every query whose f64 ratio lies more than 1e-5 from the threshold."""
+    rng = np.random.default_rng(5)
+    t_desc = synth.sift_like_descriptors(3000, 71)
+    q_desc = np.concatenate([synth.perturbed_queries(t_desc, 1500, 72, 0.05)[0], synth.sift_like_descriptors(1500, 73)])
+    q_xy = rng.uniform(0, 1000, (len(q_desc), 2)).astype(np.float32)
+    t_xy = rng.uniform(0, 1000, (len(t_desc), 2)).astype(np.float32)
+    ratio = 0.8
+    got = psift.match_arrays(q_desc, t_desc, q_xy, t_xy, psift.MatchOptions(ratio=ratio))
+    # f64 nearest / second-nearest of every query
+    q64, t64 = q_desc.astype(np.float64), t_desc.astype(np.float64)
+    d2 = (q64 ** 2).sum(1)[:, None] + (t64 ** 2).sum(1)[None, :] - 2.0 * q64 @ t64.T
+    d2 = np.maximum(d2, 0.0)
+    order = np.argsort(d2, axis=1)[:, :2]
+    best = np.sqrt(d2[np.arange(len(q64)), order[:, 0]])
+    second = np.sqrt(d2[np.arange(len(q64)), order[:, 1]])
+    r64 = best / second
+    qi = got["query_index"].astype(np.int64)
+    ti = got["target_index"].astype(np.int64)
+    exact = np.sqrt(((q64[qi] - t64[ti]) ** 2).sum(1))
+    rel_d = np.abs(got["distance"].astype(np.float64) - exact) / exact
+    rel_r = np.abs(got["ratio"].astype(np.float64) - r64[qi]) / r64[qi]
+    accepted64 = r64 < ratio
+    clear = np.abs(r64 - ratio) > 1e-5
+    gpu_acc = np.zeros(len(q64), bool)
+    gpu_acc[qi] = True
+    print(f"matching vs f64: {len(got)} matches, distance rel. error max {rel_d.max():.2e}, ratio rel. error max "
+          f"{rel_r.max():.2e}; decisions equal on {int((gpu_acc == accepted64)[clear].sum())} of {int(clear.sum())} "
+          f"queries clear of the threshold by 1e-5 ({int((~clear).sum())} within)")
+    assert len(got) > 1000
+    assert rel_d.max() <= 1e-5 and rel_r.max() <= 1e-5
+    assert np.array_equal(gpu_acc[clear], accepted64[clear])
+    assert (order[qi[clear[qi]], 0] == ti[clear[qi]]).all()
