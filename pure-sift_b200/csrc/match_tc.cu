@@ -18,10 +18,11 @@
 // one split is matched by an exact scan of all targets.
 //
 // Kernel structure (one CTA = one 128-row A tile x a range of 256-row B tiles,
-// 192 threads): warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
+// 320 threads): warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
 // operand tile, double-buffered B), warp 1 owns TMEM (512 columns = two 128x256
 // f32 accumulators) and issues tcgen05.mma (M=128, N=256, K=16) from one thread,
-// warps 2-5 read the accumulators with tcgen05.ld and maintain the top-8 lists.
+// warps 2-9 read the accumulators with tcgen05.ld (two warps per TMEM lane quarter,
+// one per 128-column half of the tile; the halves are merged per row at the end).
 // All waits are bounded: on timeout the CTA records kErrTimeout, stops issuing,
 // drains what it issued and frees its TMEM.
 #include <cuda.h>
@@ -31,7 +32,8 @@
 
 namespace psift {
 
-constexpr int kTcThreads = 192;
+constexpr int kTcThreads = 320;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int kEpiWarps = 8;     // two per TMEM lane quarter, one per 128-column half
 constexpr int kBM = 128;
 constexpr int kBN = 256;
 constexpr uint32_t kSpinLimit = 1u << 25;
@@ -123,7 +125,10 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 constexpr uint32_t kSmA = 0;                      // 2 halves x 128 rows x 128 B = 32 KB
 constexpr uint32_t kSmB = 32768;                  // 2 stages x 2 halves x 256 rows x 128 B = 128 KB
 constexpr uint32_t kSmBar = kSmB + 2 * 65536;     // barriers
-constexpr uint32_t kSmTotal = kSmBar + 256 + 1024;  // + alignment slack
+// epilogue exchange, per row: pass 1 the second half's two smallest values, pass 2
+// its count and up to kColl indices
+constexpr uint32_t kSmX = kSmBar + 256;
+constexpr uint32_t kSmTotal = kSmX + kBM * (kColl + 2) * 4 + 1024;  // + alignment slack
 
 __global__ void __launch_bounds__(kTcThreads, 1)
     match_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -150,8 +155,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     mbar_init(afull, 1);
     mbar_init(&accf[0], 1);
     mbar_init(&accf[1], 1);
-    mbar_init(&acce[0], 4);
-    mbar_init(&acce[1], 4);
+    mbar_init(&acce[0], kEpiWarps);
+    mbar_init(&acce[1], kEpiWarps);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -168,6 +173,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *taddr_slot;
   const int nt = it.n_tiles;
+  // epilogue row state (warps 2..9)
+  const int quarter = warp & 3;
+  const int half = warp >= 2 ? (warp - 2) >> 2 : 0;
+  const int row = quarter * 32 + lane;
+  const int a_local = it.a_local + row;
+  const bool row_ok = a_local < PR.na;
+  const float inf = __int_as_float(0x7f800000);
+  float v0 = inf, v1 = inf;  // mode 0: the two smallest values of the row
+  int cnt = 0;               // mode 1: indices with a <= thr (the row's window)
+  int* xrow = reinterpret_cast<int*>(smem + kSmX) + row * (kColl + 2);
 
   if (warp == 0) {
     if (lane == 0) {
@@ -228,18 +243,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
     }
   } else {
-    // epilogue: warps 2..5 -> TMEM lane quarter (warp % 4)
-    const int quarter = warp & 3;
-    const int row = quarter * 32 + lane;
-    const int a_local = it.a_local + row;
-    const bool row_ok = a_local < PR.na;
+    // epilogue: warps 2..9 -> TMEM lane quarter (warp % 4) and column half (warp - 2) / 4
     const float an = row_ok ? PR.an[a_local] : 0.0f;
-    const float inf = __int_as_float(0x7f800000);
-    // mode 0: the two smallest values; mode 1: indices with a <= thr (the row's window)
-    float v0 = inf, v1 = inf;
     const float thr = (mode == 1 && row_ok) ? PR.thr[a_local] : -inf;
-    int cnt = 0;
-    int* coll = PR.coll_idx + ((long long)it.split * PR.na + (row_ok ? a_local : 0)) * kColl;
+    // half 0 collects into the row's list, half 1 into its exchange slot
+    int* coll = half == 0 ? PR.coll_idx + ((long long)it.split * PR.na + (row_ok ? a_local : 0)) * kColl
+                          : xrow + 2;
     for (int j = 0; j < nt; ++j) {
       const int s = j & 1;
       const uint32_t use = (uint32_t)(j >> 1);
@@ -252,7 +261,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(s * kBN);
       const int col0 = it.b_local + j * kBN;
 #pragma unroll 1
-      for (int c = 0; c < kBN / 32; ++c) {
+      for (int c = half * (kBN / 64); c < (half + 1) * (kBN / 64); ++c) {
         uint32_t r[32];
         __syncwarp();
         tmem_ld32(taddr + (uint32_t)(c * 32), r);
@@ -281,18 +290,34 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce[s]);
     }
-    if (row_ok) {
-      const long long o = (long long)it.split * PR.na + a_local;
+    if (half == 1) {
       if (mode == 0) {
-        PR.top2[2 * o] = v0;
-        PR.top2[2 * o + 1] = v1;
+        xrow[0] = __float_as_int(v0);
+        xrow[1] = __float_as_int(v1);
       } else {
-        PR.coll_cnt[o] = cnt;
+        xrow[0] = cnt;
       }
     }
   }
   tc_fence_before();
   __syncthreads();
+  // Half 0 merges the second half into its row: the two smallest values of both
+  // (pass 1), or the concatenated index lists with the summed count (pass 2; a
+  // count above kColl sends the row to the exact scan, as before).
+  if (warp >= 2 && half == 0 && row_ok) {
+    const long long o = (long long)it.split * PR.na + a_local;
+    if (mode == 0) {
+      const float w0 = __int_as_float(xrow[0]), w1 = __int_as_float(xrow[1]);
+      PR.top2[2 * o] = fminf(v0, w0);
+      PR.top2[2 * o + 1] = fminf(fmaxf(v0, w0), fminf(v1, w1));
+    } else {
+      const int c1 = xrow[0], total = cnt + c1;
+      int* coll0 = PR.coll_idx + o * kColl;
+      if (total <= kColl)
+        for (int k = 0; k < c1; ++k) coll0[cnt + k] = xrow[2 + k];
+      PR.coll_cnt[o] = total;
+    }
+  }
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
