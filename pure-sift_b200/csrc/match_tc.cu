@@ -18,11 +18,11 @@
 // one split is matched by an exact scan of all targets.
 //
 // Kernel structure (one CTA = one 128-row A tile x a range of 256-row B tiles,
-// 320 threads): warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
+// 576 threads): warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
 // operand tile, double-buffered B), warp 1 owns TMEM (512 columns = two 128x256
 // f32 accumulators) and issues tcgen05.mma (M=128, N=256, K=16) from one thread,
-// warps 2-9 read the accumulators with tcgen05.ld (two warps per TMEM lane quarter,
-// one per 128-column half of the tile; the halves are merged per row at the end).
+// warps 2-17 read the accumulators with tcgen05.ld (four warps per TMEM lane quarter,
+// one per 64-column part of the tile; the parts are merged per row at the end).
 // All waits are bounded: on timeout the CTA records kErrTimeout, stops issuing,
 // drains what it issued and frees its TMEM.
 #include <cuda.h>
@@ -32,8 +32,9 @@
 
 namespace psift {
 
-constexpr int kTcThreads = 320;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
-constexpr int kEpiWarps = 8;     // two per TMEM lane quarter, one per 128-column half
+constexpr int kEpiParts = 4;                    // epilogue warps per TMEM lane quarter (column parts)
+constexpr int kEpiWarps = 4 * kEpiParts;        // warps 2 .. 2 + kEpiWarps - 1
+constexpr int kTcThreads = 32 * (2 + kEpiWarps);  // warp 0 TMA, warp 1 MMA, then the epilogue
 constexpr int kBM = 128;
 constexpr int kBN = 256;
 constexpr uint32_t kSpinLimit = 1u << 25;
@@ -125,10 +126,10 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 constexpr uint32_t kSmA = 0;                      // 2 halves x 128 rows x 128 B = 32 KB
 constexpr uint32_t kSmB = 32768;                  // 2 stages x 2 halves x 256 rows x 128 B = 128 KB
 constexpr uint32_t kSmBar = kSmB + 2 * 65536;     // barriers
-// epilogue exchange, per row: pass 1 the second half's two smallest values, pass 2
-// its count and up to kColl indices
+// epilogue exchange, per row and column part 1..kEpiParts-1: pass 1 the part's two
+// smallest values, pass 2 its count and up to kColl indices
 constexpr uint32_t kSmX = kSmBar + 256;
-constexpr uint32_t kSmTotal = kSmX + kBM * (kColl + 2) * 4 + 1024;  // + alignment slack
+constexpr uint32_t kSmTotal = kSmX + (kEpiParts - 1) * kBM * (kColl + 2) * 4 + 1024;  // + alignment slack
 
 __global__ void __launch_bounds__(kTcThreads, 1)
     match_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -175,14 +176,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const int nt = it.n_tiles;
   // epilogue row state (warps 2..9)
   const int quarter = warp & 3;
-  const int half = warp >= 2 ? (warp - 2) >> 2 : 0;
+  const int part = warp >= 2 ? (warp - 2) >> 2 : 0;  // column part of the tile
   const int row = quarter * 32 + lane;
   const int a_local = it.a_local + row;
   const bool row_ok = a_local < PR.na;
   const float inf = __int_as_float(0x7f800000);
   float v0 = inf, v1 = inf;  // mode 0: the two smallest values of the row
   int cnt = 0;               // mode 1: indices with a <= thr (the row's window)
-  int* xrow = reinterpret_cast<int*>(smem + kSmX) + row * (kColl + 2);
+  // exchange slot of (part, row) for parts >= 1
+  int* xrow = reinterpret_cast<int*>(smem + kSmX) + ((part > 0 ? part - 1 : 0) * kBM + row) * (kColl + 2);
 
   if (warp == 0) {
     if (lane == 0) {
@@ -243,11 +245,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
     }
   } else {
-    // epilogue: warps 2..9 -> TMEM lane quarter (warp % 4) and column half (warp - 2) / 4
+    // epilogue: TMEM lane quarter warp % 4, column part (warp - 2) / 4
     const float an = row_ok ? PR.an[a_local] : 0.0f;
     const float thr = (mode == 1 && row_ok) ? PR.thr[a_local] : -inf;
-    // half 0 collects into the row's list, half 1 into its exchange slot
-    int* coll = half == 0 ? PR.coll_idx + ((long long)it.split * PR.na + (row_ok ? a_local : 0)) * kColl
+    // part 0 collects into the row's list, the other parts into their exchange slots
+    int* coll = part == 0 ? PR.coll_idx + ((long long)it.split * PR.na + (row_ok ? a_local : 0)) * kColl
                           : xrow + 2;
     for (int j = 0; j < nt; ++j) {
       const int s = j & 1;
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(s * kBN);
       const int col0 = it.b_local + j * kBN;
 #pragma unroll 1
-      for (int c = half * (kBN / 64); c < (half + 1) * (kBN / 64); ++c) {
+      for (int c = part * (kBN / 32 / kEpiParts); c < (part + 1) * (kBN / 32 / kEpiParts); ++c) {
         uint32_t r[32];
         __syncwarp();
         tmem_ld32(taddr + (uint32_t)(c * 32), r);
@@ -276,13 +278,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             v1 = fminf(v1, hi);
           }
         } else {
+          // the tests branch-free into a mask, then the (rare) hits in column order
+          uint32_t hits = 0;
 #pragma unroll
           for (int q = 0; q < 32; ++q) {
             const float a = __fmaf_rn(-2.0f, __uint_as_float(r[q]), an + __shfl_sync(0xffffffffu, bnl, q));
-            if (a <= thr) {
-              if (cnt < kColl) coll[cnt] = cb + q;
-              ++cnt;
-            }
+            hits |= (a <= thr ? 1u : 0u) << q;
+          }
+          while (hits) {
+            const int q = __ffs(hits) - 1;
+            hits &= hits - 1;
+            if (cnt < kColl) coll[cnt] = cb + q;
+            ++cnt;
           }
         }
       }
@@ -290,7 +297,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce[s]);
     }
-    if (half == 1) {
+    if (part > 0) {
       if (mode == 0) {
         xrow[0] = __float_as_int(v0);
         xrow[1] = __float_as_int(v1);
@@ -301,21 +308,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   tc_fence_before();
   __syncthreads();
-  // Half 0 merges the second half into its row: the two smallest values of both
-  // (pass 1), or the concatenated index lists with the summed count (pass 2; a
-  // count above kColl sends the row to the exact scan, as before).
-  if (warp >= 2 && half == 0 && row_ok) {
+  // Part 0 merges the other parts into its row, in part order: the two smallest
+  // values of all (pass 1), or the concatenated index lists with the summed count
+  // (pass 2; a count above kColl sends the row to the exact scan, as before).
+  if (warp >= 2 && part == 0 && row_ok) {
     const long long o = (long long)it.split * PR.na + a_local;
+    int* coll0 = PR.coll_idx + o * kColl;
+    for (int p = 1; p < kEpiParts; ++p) {
+      const int* x = reinterpret_cast<const int*>(smem + kSmX) + ((p - 1) * kBM + row) * (kColl + 2);
+      if (mode == 0) {
+        const float w0 = __int_as_float(x[0]), w1 = __int_as_float(x[1]);
+        const float m1 = fminf(fmaxf(v0, w0), fminf(v1, w1));
+        v0 = fminf(v0, w0);
+        v1 = m1;
+      } else {
+        const int c1 = x[0];
+        for (int k = 0; k < c1 && cnt + k < kColl; ++k) coll0[cnt + k] = x[2 + k];
+        cnt += c1;
+      }
+    }
     if (mode == 0) {
-      const float w0 = __int_as_float(xrow[0]), w1 = __int_as_float(xrow[1]);
-      PR.top2[2 * o] = fminf(v0, w0);
-      PR.top2[2 * o + 1] = fminf(fmaxf(v0, w0), fminf(v1, w1));
+      PR.top2[2 * o] = v0;
+      PR.top2[2 * o + 1] = v1;
     } else {
-      const int c1 = xrow[0], total = cnt + c1;
-      int* coll0 = PR.coll_idx + o * kColl;
-      if (total <= kColl)
-        for (int k = 0; k < c1; ++k) coll0[cnt + k] = xrow[2 + k];
-      PR.coll_cnt[o] = total;
+      PR.coll_cnt[o] = cnt;
     }
   }
   if (warp == 1) {
