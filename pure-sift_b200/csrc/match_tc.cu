@@ -35,6 +35,7 @@ namespace psift {
 constexpr int kEpiParts = 4;                    // epilogue warps per TMEM lane quarter (column parts)
 constexpr int kEpiWarps = 4 * kEpiParts;        // warps 2 .. 2 + kEpiWarps - 1
 constexpr int kTcThreads = 32 * (2 + kEpiWarps);  // warp 0 TMA, warp 1 MMA, then the epilogue
+static_assert(256 / kEpiParts == 64, "the epilogue folds four 16-column TMEM loads per part");
 constexpr int kBM = 128;
 constexpr int kBN = 256;
 constexpr uint32_t kSpinLimit = 1u << 25;
@@ -120,6 +121,22 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 16 columns of a TMEM lane quarter, without waiting: the registers are valid
+// only after tmem_wait16 on them.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+               : "r"(taddr));
+}
+// Waits for this thread's outstanding TMEM loads; r is tied so that no read of
+// it moves above the wait.
+__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
 }
 
 // Smem map (offsets from a 1024-aligned base).
@@ -262,17 +279,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tc_fence_after();
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(s * kBN);
       const int col0 = it.b_local + j * kBN;
-#pragma unroll 1
-      for (int c = part * (kBN / 32 / kEpiParts); c < (part + 1) * (kBN / 32 / kEpiParts); ++c) {
-        uint32_t r[32];
-        __syncwarp();
-        tmem_ld32(taddr + (uint32_t)(c * 32), r);
-        const int cb = col0 + c * 32;
-        const float bnl = (cb + lane < PR.nb) ? PR.bn[cb + lane] : inf;
+      // This warp's 64 columns as four 16-column TMEM loads, double-buffered: the
+      // next load is in flight while the current 16 values are folded in.
+      const int cbase = col0 + part * (kBN / kEpiParts);
+      const float bnl0 = (cbase + lane < PR.nb) ? PR.bn[cbase + lane] : inf;
+      const float bnl1 = (cbase + 32 + lane < PR.nb) ? PR.bn[cbase + 32 + lane] : inf;
+      const uint32_t tbase = taddr + (uint32_t)(part * (kBN / kEpiParts));
+      auto fold16 = [&](const uint32_t(&rr)[16], float bnl, int qoff, int cstart) {
         if (mode == 0) {
 #pragma unroll
-          for (int q = 0; q < 32; ++q) {
-            const float a = __fmaf_rn(-2.0f, __uint_as_float(r[q]), an + __shfl_sync(0xffffffffu, bnl, q));
+          for (int q = 0; q < 16; ++q) {
+            const float a = __fmaf_rn(-2.0f, __uint_as_float(rr[q]), an + __shfl_sync(0xffffffffu, bnl, qoff + q));
             const float hi = fmaxf(v0, a);
             v0 = fminf(v0, a);
             v1 = fminf(v1, hi);
@@ -281,18 +298,32 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           // the tests branch-free into a mask, then the (rare) hits in column order
           uint32_t hits = 0;
 #pragma unroll
-          for (int q = 0; q < 32; ++q) {
-            const float a = __fmaf_rn(-2.0f, __uint_as_float(r[q]), an + __shfl_sync(0xffffffffu, bnl, q));
+          for (int q = 0; q < 16; ++q) {
+            const float a = __fmaf_rn(-2.0f, __uint_as_float(rr[q]), an + __shfl_sync(0xffffffffu, bnl, qoff + q));
             hits |= (a <= thr ? 1u : 0u) << q;
           }
           while (hits) {
             const int q = __ffs(hits) - 1;
             hits &= hits - 1;
-            if (cnt < kColl) coll[cnt] = cb + q;
+            if (cnt < kColl) coll[cnt] = cstart + q;
             ++cnt;
           }
         }
-      }
+      };
+      uint32_t ra[16], rb[16];
+      __syncwarp();
+      tmem_ld16(tbase, ra);
+      tmem_wait16(ra);
+      tmem_ld16(tbase + 16, rb);
+      fold16(ra, bnl0, 0, cbase);
+      tmem_wait16(rb);
+      tmem_ld16(tbase + 32, ra);
+      fold16(rb, bnl0, 16, cbase + 16);
+      tmem_wait16(ra);
+      tmem_ld16(tbase + 48, rb);
+      fold16(ra, bnl1, 0, cbase + 32);
+      tmem_wait16(rb);
+      fold16(rb, bnl1, 16, cbase + 48);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce[s]);
