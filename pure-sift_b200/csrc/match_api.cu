@@ -35,6 +35,7 @@ cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, cons
                             const TcPair* pairs, uint32_t* err, int mode, cudaStream_t st);
 cudaError_t launch_window(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
+cudaError_t launch_gather_rows(const GatherJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 
 namespace {
 
@@ -134,6 +135,9 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
              sizeof(TcItem) * (n_items_f + n_items_r) +
              sizeof(TcPair) * 2 * na + sizeof(RerankJob) * 2 * na + 8192 + (size_t)t_rows * 4 +
              sizeof(Bf16Job) * 2 * na + 512;
+    // pass 2's compacted operands, row maps, counts and gather jobs
+    bytes += (size_t)(q_rows + t_rows) * 256 + (size_t)(q_rows + t_rows) * 4 + sizeof(int) * 2 * na +
+             sizeof(GatherJob) * 2 * na + 5 * 256;
   }
   psift_status s = arena_reserve(ctx, bytes);
   if (s != PSIFT_OK) return s;
@@ -210,8 +214,17 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   int* flags = mutual ? (int*)arena_alloc(ctx, sizeof(int) * t_rows) : nullptr;  // matched-target marks
   Bf16Job* d_bj = (Bf16Job*)arena_alloc(ctx, sizeof(Bf16Job) * 2 * na);
   std::vector<Bf16Job> bj(2 * na);
-  if (!qb || !tb || !thr || !coll_cnt || !d_rj || !d_bj || (mutual && !flags))
+  // pass 2 runs over the rows window_kernel keeps, gathered into these operands
+  uint16_t* qbc = (uint16_t*)arena_alloc(ctx, (size_t)q_rows * 256);
+  uint16_t* tbc = (uint16_t*)arena_alloc(ctx, (size_t)t_rows * 256);
+  int* rowmap = (int*)arena_alloc(ctx, sizeof(int) * (q_rows + t_rows));
+  int* ccount = (int*)arena_alloc(ctx, sizeof(int) * 2 * na);
+  GatherJob* d_gj = (GatherJob*)arena_alloc(ctx, sizeof(GatherJob) * 2 * na);
+  std::vector<GatherJob> gj(2 * na);
+  if (!qb || !tb || !thr || !coll_cnt || !d_rj || !d_bj || (mutual && !flags) || !qbc || !tbc || !rowmap ||
+      !ccount || !d_gj)
     return set_error(ctx, PSIFT_ERR_INTERNAL, "match workspace carve overflow");
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ccount, 0, sizeof(int) * 2 * na, st));
   if (mutual) PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * t_rows, st));
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(qb, 0, (size_t)q_rows * 256, st));
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(tb, 0, (size_t)t_rows * 256, st));
@@ -226,9 +239,11 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
       b += pad_rows(pairs[k].nt);
     }
   }
-  CUtensorMap tmQA, tmTB, tmTA, tmQB;
+  CUtensorMap tmQA, tmTB, tmTA, tmQB, tmQAc, tmTAc;
   if (!make_operand_map(&tmQA, qb, q_rows, kTcBM) || !make_operand_map(&tmTB, tb, t_rows, kTcBN) ||
-      (mutual && (!make_operand_map(&tmTA, tb, t_rows, kTcBM) || !make_operand_map(&tmQB, qb, q_rows, kTcBN))))
+      !make_operand_map(&tmQAc, qbc, q_rows, kTcBM) ||
+      (mutual && (!make_operand_map(&tmTA, tb, t_rows, kTcBM) || !make_operand_map(&tmQB, qb, q_rows, kTcBN) ||
+                  !make_operand_map(&tmTAc, tbc, t_rows, kTcBM))))
     return set_error(ctx, PSIFT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   std::vector<TcItem> items;
   std::vector<TcPair> tcp(2 * na);
@@ -236,8 +251,10 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   long long cf = 0;
   // one direction: A rows matched against B rows
   auto add_problem = [&](int slot, int pair_k, int nA, int nB, const float* an, const float* bn, int splits,
-                         long long a_row0, long long b_row0, float* thr_rows) {
+                         long long a_row0, long long b_row0, float* thr_rows, int* rowmap_rows) {
     TcPair& T = tcp[slot];
+    T.ccount = ccount + slot;
+    T.rowmap = rowmap_rows;
     T.na = nA;
     T.nb = nB;
     T.an = an;
@@ -264,27 +281,36 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     P.tn = tn + t0[k];
     P.tn_max = maxes + k;
     P.qn_max = maxes + na + k;
-    add_problem(k, k, P.nq, P.nt, P.qn, P.tn, tc_split_f[k], q0[k], t0[k], thr + q0[k]);
+    add_problem(k, k, P.nq, P.nt, P.qn, P.tn, tc_split_f[k], q0[k], t0[k], thr + q0[k], rowmap + q0[k]);
     const TcPair& T = tcp[k];
     rj[k] = RerankJob{P.q, P.t, P.nq, P.nt, P.qn, P.tn_max, T.top2, thr + q0[k], T.coll_idx, T.coll_cnt,
                       T.splits, P.best, P.second, P.best_idx, ctx->d_error + 1, opt.ratio,
                       mutual ? flags + t0[k] : nullptr};
+    rj[k].ccount = ccount + k;
+    rj[k].rowmap = rowmap + q0[k];
+    gj[k] = GatherJob{qb + (size_t)q0[k] * 128, qbc + (size_t)q0[k] * 128, rowmap + q0[k], ccount + k};
   }
   const int n_f = (int)items.size();
   if (mutual) {
     for (int k = 0; k < na; ++k) {
       MatchPair& P = pairs[k];
-      add_problem(na + k, k, P.nt, P.nq, P.tn, P.qn, tc_split_r[k], t0[k], q0[k], thr + q_rows + t0[k]);
+      add_problem(na + k, k, P.nt, P.nq, P.tn, P.qn, tc_split_r[k], t0[k], q0[k], thr + q_rows + t0[k],
+                  rowmap + q_rows + t0[k]);
       const TcPair& T = tcp[na + k];
       rj[na + k] = RerankJob{P.t, P.q, P.nt, P.nq, P.tn, P.qn_max, T.top2, thr + q_rows + t0[k], T.coll_idx,
                              T.coll_cnt, T.splits, P.col_best, nullptr, P.col_idx, ctx->d_error + 1, opt.ratio,
                              flags + t0[k]};
+      rj[na + k].ccount = ccount + na + k;
+      rj[na + k].rowmap = rowmap + q_rows + t0[k];
+      gj[na + k] = GatherJob{tb + (size_t)t0[k] * 128, tbc + (size_t)t0[k] * 128, rowmap + q_rows + t0[k],
+                             ccount + na + k};
     }
   }
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(MatchPair) * na, cudaMemcpyHostToDevice, st));
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(TcItem) * items.size(), cudaMemcpyHostToDevice, st));
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_tcp, tcp.data(), sizeof(TcPair) * tcp.size(), cudaMemcpyHostToDevice, st));
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_rj, rj.data(), sizeof(RerankJob) * rj.size(), cudaMemcpyHostToDevice, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_gj, gj.data(), sizeof(GatherJob) * gj.size(), cudaMemcpyHostToDevice, st));
   StageScope sc(ctx, STAGE_MATCH);
   int max_a = 0, max_b = 0;
   {
@@ -302,6 +328,7 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   // forward: queries vs targets; reverse (mutual): matched targets vs queries
   for (int dir = 0; dir < (mutual ? 2 : 1); ++dir) {
     const CUtensorMap& A = dir == 0 ? tmQA : tmTA;
+    const CUtensorMap& Ac = dir == 0 ? tmQAc : tmTAc;
     const CUtensorMap& B = dir == 0 ? tmTB : tmQB;
     const TcItem* it0 = d_items + (dir == 0 ? 0 : n_f);
     const int n_it = dir == 0 ? n_f : (int)items.size() - n_f;
@@ -309,9 +336,10 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     const int rows = dir == 0 ? max_a : max_b;
     cudaError_t e = launch_match_tc(A, B, it0, n_it, d_tcp, ctx->d_error, 0, st);
     if (e == cudaSuccess) e = launch_window(jobs_dir, na, rows, st);
-    if (e == cudaSuccess) e = launch_match_tc(A, B, it0, n_it, d_tcp, ctx->d_error, 1, st);
+    if (e == cudaSuccess) e = launch_gather_rows(d_gj + dir * na, na, rows, st);
+    if (e == cudaSuccess) e = launch_match_tc(Ac, B, it0, n_it, d_tcp, ctx->d_error, 1, st);
     if (e == cudaSuccess) e = launch_rerank(jobs_dir, na, rows, st);
-    ctx->launches += 4;
+    ctx->launches += 5;
     if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc / window / rerank");
   }
   cudaError_t e = launch_match_emit(d_pairs, na, opt.ratio, mutual, st);

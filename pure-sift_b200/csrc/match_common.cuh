@@ -53,6 +53,19 @@ struct TcPair {
   int* coll_idx;     // pass 2 output: [splits][na][kColl] window indices
   int* coll_cnt;     // [splits][na] window sizes (may exceed kColl = overflow)
   int splits;
+  // Pass 2 over the compacted A operand (null: pass 2 runs over every row): the
+  // number of rows window_kernel kept and, per compacted row, its row in the pair.
+  const int* ccount;
+  const int* rowmap;
+};
+
+// Copies the kept rows' bf16 descriptors into the compacted operand (one per
+// problem and direction).
+struct GatherJob {
+  const uint16_t* src;  // the pair's A rows (bf16, 128 per row)
+  uint16_t* dst;        // its compacted rows
+  const int* rowmap;
+  const int* count;
 };
 
 // Certified re-rank job (one per problem and direction).
@@ -74,6 +87,8 @@ struct RerankJob {
   float ratio;          // Lowe ratio (forward pass: rows certified to fail it are skipped)
   int* flags;           // forward: set flags[best] = 1 for accepted matches (mutual);
                         // reverse: only rows with flags[row] != 0 are ranked (null = all)
+  int* ccount;          // window_kernel: rows kept for pass 2 (null: no compaction)
+  int* rowmap;          // [na] their rows, in the order they were kept
 };
 
 // Merge of two (best, idx, second) triples over disjoint target sets where ties

@@ -164,6 +164,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const TcItem it = items[blockIdx.x];
   const TcPair& PR = pairs[it.pair];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // pass 2 over the compacted rows: a tile past the kept rows has nothing to do
+  const bool compact = mode == 1 && PR.ccount != nullptr;
+  const int n_rows = compact ? *PR.ccount : PR.na;
+  if (it.a_local >= n_rows) return;
 
   if (threadIdx.x == 0) {
     mbar_init(&full[0], 1);
@@ -195,8 +199,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const int quarter = warp & 3;
   const int part = warp >= 2 ? (warp - 2) >> 2 : 0;  // column part of the tile
   const int row = quarter * 32 + lane;
-  const int a_local = it.a_local + row;
-  const bool row_ok = a_local < PR.na;
+  // the row's index in the pair (through the row map when the operand is compacted)
+  const bool row_ok = it.a_local + row < n_rows;
+  const int a_local = compact ? (row_ok ? PR.rowmap[it.a_local + row] : 0) : it.a_local + row;
   const float inf = __int_as_float(0x7f800000);
   float v0 = inf, v1 = inf;  // mode 0: the two smallest values of the row
   int cnt = 0;               // mode 1: indices with a <= thr (the row's window)
@@ -302,6 +307,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const float a = __fmaf_rn(-2.0f, __uint_as_float(rr[q]), an + __shfl_sync(0xffffffffu, bnl, qoff + q));
             hits |= (a <= thr ? 1u : 0u) << q;
           }
+          // a row past the kept ones reads stale operand rows (possibly inf: a = -inf
+          // passes even thr = -inf): it collects nothing
+          if (!row_ok) hits = 0;
           while (hits) {
             const int q = __ffs(hits) - 1;
             hits &= hits - 1;
@@ -466,6 +474,19 @@ __global__ void window_kernel(const RerankJob* __restrict__ jobs) {
     if (lo1 > 0.0 && lo1 >= r * r * hi2 * (1.0 + 1e-5)) thr = -inf;
   }
   J.thr[row] = thr;
+  // rows with a window go to pass 2 (compacted; the order does not matter: every
+  // row's collection depends on that row alone and lands in its own slot)
+  if (J.ccount && thr != -inf) J.rowmap[atomicAdd(J.ccount, 1)] = row;
+}
+
+// One warp per compacted row: its 256 bytes of bf16 descriptor, coalesced.
+__global__ void gather_rows_kernel(const GatherJob* __restrict__ jobs) {
+  const GatherJob& G = jobs[blockIdx.y];
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= *G.count) return;
+  const int r = G.rowmap[c];
+  reinterpret_cast<uint2*>(G.dst + (size_t)c * 128)[lane] = reinterpret_cast<const uint2*>(G.src + (size_t)r * 128)[lane];
 }
 
 // One warp per A row: exact reference distances over the window candidates
@@ -565,6 +586,13 @@ cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, cons
 cudaError_t launch_window(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st) {
   dim3 grid((max_rows + 255) / 256, n_jobs);
   window_kernel<<<grid, 256, 0, st>>>(jobs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const GatherJob* jobs, int n_jobs, int max_rows, cudaStream_t st) {
+  if (n_jobs <= 0 || max_rows <= 0) return cudaSuccess;
+  dim3 grid((max_rows + 7) / 8, n_jobs);
+  gather_rows_kernel<<<grid, 256, 0, st>>>(jobs);
   return cudaGetLastError();
 }
 

@@ -118,3 +118,35 @@ def test_header_checks_and_errors():
     # the context stays usable after the errors
     ok = sift.detect_and_compute_jpeg_batch([J.encode(J.gray_image(200, 150, 9))])
     assert len(ok) == 1
+
+
+def test_large_batch_shares_and_thread_setting():
+    # 60 JPEGs of 8 sizes: shares over host threads (automatic count, and 3) give,
+    # per image, the features of the one-image path on the same decoded luma; one
+    # batched call gives nearly the same feature counts.
+    shapes = [(96, 128), (120, 160), (77, 203), (64, 64), (150, 100), (33, 250), (128, 96), (99, 101)]
+    blobs = [J.encode(J.color_image(w, h, 500 + i) if i % 3 else J.gray_image(w, h, 500 + i), 90, i % 2 * 2)
+             for i, (h, w) in enumerate(shapes[k % 8] for k in range(60))]
+    ctx = psift.Context(0)
+    try:
+        sift = psift.Sift.new(psift.SiftConfig().with_octaves(3).with_contrast_threshold(0.015))
+        counts = {}
+        for threads in (0, 3):
+            ctx.set_jpeg_threads(threads)
+            got = sift.detect_and_compute_jpeg_batch(blobs, ctx=ctx)
+            assert len(got) == 60 and ctx.jpeg_backend == 1
+            counts[threads] = [len(f) for f in got]
+            for k in (0, 7, 23, 59):
+                ref = sift.detect_and_compute_u8(psift.decode_jpeg_luma(blobs[k], ctx=ctx), ctx=ctx)
+                assert len(got[k]) == len(ref)
+                np.testing.assert_array_equal(got[k].descriptors, ref.descriptors)
+                np.testing.assert_array_equal(got[k].x, ref.x)
+        assert counts[0] == counts[3]
+        # one batched call (above 50 images nvJPEG decodes the Huffman stage on the GPU)
+        ctx.set_jpeg_threads(1)
+        one = sift.detect_and_compute_jpeg_batch(blobs, ctx=ctx)
+        assert ctx.jpeg_backend in (2, 3)
+        for a, b in zip(one, counts[0]):
+            assert abs(len(a) - b) <= max(2, 0.1 * b)
+    finally:
+        ctx.close()
