@@ -102,6 +102,7 @@ struct Decoder {
   Backend gpu{NVJPEG_BACKEND_GPU_HYBRID};
   std::vector<Worker> workers;
   cudaEvent_t start = nullptr;
+  cudaEvent_t all_done = nullptr;  // the whole batch decoded with chunk 0
   int threads = 0;  // 0: automatic; 1: one batched call on the calling thread
   uint8_t* rgb = nullptr;
   size_t rgb_cap = 0;
@@ -272,19 +273,18 @@ psift_status read_header(psift_ctx* ctx, const uint8_t* data, size_t len, bool e
 }
 
 // Decodes n JPEGs (host bytes) and writes their luma to luma[i] (dense rows) on st.
-psift_status decode_to_luma(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths, uint32_t n,
-                            const std::vector<JpegDims>& dims, uint8_t* const* luma, cudaStream_t st) {
-  NvjpegApi& A = nvjpeg();
+// RGB staging offsets of every image of a batch (each image its own region, so
+// chunks decoded on different streams never share one); grows the buffer.
+psift_status reserve_rgb(psift_ctx* ctx, const std::vector<JpegDims>& dims, std::vector<size_t>& off) {
   Decoder* dec = decoder(ctx);
-  std::vector<size_t> off(n);
+  off.assign(dims.size(), 0);
   size_t total = 0;
-  for (uint32_t i = 0; i < n; ++i) {
+  for (size_t i = 0; i < dims.size(); ++i) {
     off[i] = total;
     total += align_up(3 * (size_t)dims[i].w * dims[i].h, 256);
   }
   if (total > dec->rgb_cap) {
-    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    cudaFree(dec->rgb);
+    cudaFree(dec->rgb);  // synchronises the device: no earlier decode still writes it
     dec->rgb = nullptr;
     dec->rgb_cap = 0;
     const size_t cap = align_up(total, 1 << 20);
@@ -292,29 +292,40 @@ psift_status decode_to_luma(psift_ctx* ctx, const uint8_t* const* data, const si
     if (e != cudaSuccess) return cuda_error(ctx, e, "cudaMalloc(jpeg rgb)");
     dec->rgb_cap = cap;
   }
+  return PSIFT_OK;
+}
+
+// Decodes images [b, e) of the batch (host bytes) and writes their luma to
+// luma[i - b] (dense rows) on st.
+psift_status decode_range(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths,
+                          const std::vector<JpegDims>& dims, const std::vector<size_t>& off, uint32_t b, uint32_t e,
+                          uint8_t* const* luma, cudaStream_t st) {
+  NvjpegApi& A = nvjpeg();
+  Decoder* dec = decoder(ctx);
+  const uint32_t n = e - b;
   std::vector<nvjpegImage_t> dst(n);
   for (uint32_t i = 0; i < n; ++i) {
     std::memset(&dst[i], 0, sizeof(nvjpegImage_t));
-    dst[i].channel[0] = dec->rgb + off[i];
-    dst[i].pitch[0] = 3 * (size_t)dims[i].w;
+    dst[i].channel[0] = dec->rgb + off[b + i];
+    dst[i].pitch[0] = 3 * (size_t)dims[b + i].w;
   }
   nvjpegStatus_t s = NVJPEG_STATUS_NOT_INITIALIZED;
   int used = -1;
-  if (dec->threads != 1 && decode_threaded(ctx, dec, data, lengths, n, dst.data(), st)) {
+  if (dec->threads != 1 && decode_threaded(ctx, dec, data + b, lengths + b, n, dst.data(), st)) {
     used = (int)NVJPEG_BACKEND_HYBRID;
     s = NVJPEG_STATUS_SUCCESS;
   }
-  for (Backend* b : {&dec->hw, &dec->gpu}) {
+  for (Backend* bk : {&dec->hw, &dec->gpu}) {
     if (used >= 0) break;
-    if (!backend_ready(*b)) continue;
-    if (b->batch != (int)n) {
-      s = A.batched_init(b->h, b->st, (int)n, 1, NVJPEG_OUTPUT_RGBI);
+    if (!backend_ready(*bk)) continue;
+    if (bk->batch != (int)n) {
+      s = A.batched_init(bk->h, bk->st, (int)n, 1, NVJPEG_OUTPUT_RGBI);
       if (s != NVJPEG_STATUS_SUCCESS) continue;
-      b->batch = (int)n;
+      bk->batch = (int)n;
     }
-    s = A.batched(b->h, b->st, data, lengths, dst.data(), st);
+    s = A.batched(bk->h, bk->st, data + b, lengths + b, dst.data(), st);
     if (s == NVJPEG_STATUS_SUCCESS) {
-      used = (int)b->kind;
+      used = (int)bk->kind;
       break;
     }
   }
@@ -323,8 +334,8 @@ psift_status decode_to_luma(psift_ctx* ctx, const uint8_t* const* data, const si
                      "Failed to decode image payload (nvJPEG status " + std::to_string((int)s) + ")");
   dec->last = used;
   for (uint32_t i = 0; i < n; ++i) {
-    const uint32_t px = dims[i].w * dims[i].h;
-    rgb_to_luma_kernel<<<(px + 255) / 256, 256, 0, st>>>(dec->rgb + off[i], luma[i], px);
+    const uint32_t px = dims[b + i].w * dims[b + i].h;
+    rgb_to_luma_kernel<<<(px + 255) / 256, 256, 0, st>>>(dec->rgb + off[b + i], luma[i], px);
     ctx->launches++;
   }
   PSIFT_CUDA_TRY(ctx, cudaGetLastError());
@@ -346,6 +357,7 @@ void jpeg_release(psift_ctx* ctx) {
     if (w.stream) cudaStreamDestroy(w.stream);
   }
   if (dec->start) cudaEventDestroy(dec->start);
+  if (dec->all_done) cudaEventDestroy(dec->all_done);
   cudaFree(dec->rgb);
   delete dec;
   ctx->jpeg = nullptr;
@@ -386,7 +398,9 @@ psift_status psift_decode_jpeg_luma(psift_ctx* ctx, const uint8_t* data, size_t 
   const uint8_t* const bufs[1] = {data};
   const size_t lens[1] = {length};
   uint8_t* const outs[1] = {d_luma};
-  if ((st = decode_to_luma(ctx, bufs, lens, 1, dims, outs, ctx->stream)) != PSIFT_OK) return st;
+  std::vector<size_t> off;
+  if ((st = reserve_rgb(ctx, dims, off)) != PSIFT_OK) return st;
+  if ((st = decode_range(ctx, bufs, lens, dims, off, 0, 1, outs, ctx->stream)) != PSIFT_OK) return st;
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(luma, d_luma, px, cudaMemcpyDeviceToHost, ctx->stream));
   PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return PSIFT_OK;
@@ -404,10 +418,36 @@ psift_status psift_detect_and_compute_jpeg_batch(psift_ctx* ctx, const uint8_t* 
     if (st != PSIFT_OK) return st;
     imgs[i] = psift_image_u8{nullptr, dims[i].h, dims[i].w, dims[i].w};
   }
-  const DeviceFill fill = [&](char* extra, const std::vector<size_t>& dev_off, cudaStream_t st) {
-    std::vector<uint8_t*> luma(n);
-    for (uint32_t i = 0; i < n; ++i) luma[i] = (uint8_t*)extra + dev_off[i];
-    return decode_to_luma(ctx, data, lengths, n, dims, luma.data(), st);
+  std::vector<size_t> rgb_off;
+  psift_status rs = reserve_rgb(ctx, dims, rgb_off);
+  if (rs != PSIFT_OK) return rs;
+  Decoder* dec = decoder(ctx);
+  if (!dec->all_done && cudaEventCreateWithFlags(&dec->all_done, cudaEventDisableTiming) != cudaSuccess)
+    return set_error(ctx, PSIFT_ERR_CUDA, "cudaEventCreate(jpeg)");
+  // Per chunk: its images decoded on its stream, so that the host part of chunk
+  // 1's decode overlaps chunk 0's kernels -- when a chunk has at least as many
+  // images as there are decode threads (fewer would leave threads idle for longer
+  // than the overlap gains).  Otherwise, and for one batched call (threads = 1;
+  // above 50 images its Huffman stage then runs on the GPU), chunk 0 decodes the
+  // whole batch and chunk 1's stream waits for it.
+  const unsigned hc = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t decode_threads = dec->threads > 1 ? (uint32_t)dec->threads : std::min<unsigned>(hc, kMaxJpegThreads);
+  const bool whole = dec->threads == 1 || (n + 1) / 2 < decode_threads;
+  const DeviceFill fill = [&](char* extra, const std::vector<size_t>& dev_off, uint32_t b, uint32_t e,
+                              cudaStream_t st) -> psift_status {
+    if (whole) {
+      if (b > 0) return cudaStreamWaitEvent(st, dec->all_done, 0) == cudaSuccess
+                            ? PSIFT_OK
+                            : set_error(ctx, PSIFT_ERR_CUDA, "cudaStreamWaitEvent(jpeg)");
+      b = 0;
+      e = n;
+    }
+    std::vector<uint8_t*> luma(e - b);
+    for (uint32_t i = b; i < e; ++i) luma[i - b] = (uint8_t*)extra + dev_off[i];
+    psift_status r = decode_range(ctx, data, lengths, dims, rgb_off, b, e, luma.data(), st);
+    if (r == PSIFT_OK && whole && cudaEventRecord(dec->all_done, st) != cudaSuccess)
+      r = set_error(ctx, PSIFT_ERR_CUDA, "cudaEventRecord(jpeg)");
+    return r;
   };
   return detect_batch_host_out(ctx, imgs.data(), n, cfg, outs, &fill);
 }

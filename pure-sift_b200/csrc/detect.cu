@@ -820,8 +820,8 @@ namespace psift {
 // The host-output batch: features of n u8 images into host arrays, one launch
 // per stage, two chunks on two streams.  Inputs come from host memory
 // (images[i].data, copied per chunk), or, with `fill`, are written into their
-// device slots by fill (on ctx->stream, before the chunks fork; images[i].data
-// is then unused and the slots are dense rows of width bytes).
+// device slots by fill, per chunk on the chunk's stream just before its stages
+// (images[i].data is then unused and the slots are dense rows of width bytes).
 psift_status detect_batch_host_out(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
                                    const psift_sift_config* cfg, psift_features* outs, const DeviceFill* fill) {
   psift_status st = check_common(ctx, cfg);
@@ -875,7 +875,6 @@ psift_status detect_batch_host_out(psift_ctx* ctx, const psift_image_u8* images,
   // the device plan table is uploaded once for the whole batch; chunk views index into it
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(job.d_plans, job.plans.data(), sizeof(ImagePlan) * n, cudaMemcpyHostToDevice,
                                       ctx->stream));
-  if (fill && (st = (*fill)((char*)extra, dev_off, ctx->stream)) != PSIFT_OK) return st;
   PSIFT_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
   PSIFT_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream2, ctx->ev_fork, 0));
   for (uint32_t c = 0; c < n_chunks; ++c) {
@@ -896,6 +895,9 @@ psift_status detect_batch_host_out(psift_ctx* ctx, const psift_image_u8* images,
         PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(dst, stg, px, cudaMemcpyHostToDevice, sc));
       }
     }
+    // device-filled inputs: this chunk's, on its stream (the host part of the fill
+    // for chunk 1 overlaps chunk 0's kernels)
+    if (fill && (st = (*fill)((char*)extra, dev_off, b, e, sc)) != PSIFT_OK) return st;
     DetectJob v;
     v.n = (int)(e - b);
     v.plans.assign(job.plans.begin() + b, job.plans.begin() + e);

@@ -125,9 +125,11 @@ void tracking_stats(const psift_match* m, uint32_t n, const uint8_t* mask, const
                     const float* q_ori, const float* t_scale, const float* t_ori, psift_tracking_summary* out);
 // CTAs of `func` resident on the whole device at once (occupancy x SMs), cached.
 cudaError_t resident_ctas(const void* func, int threads, size_t smem, int* out);
-// Writes the batch's u8 inputs into their device slots (extra + dev_off[i], dense
-// rows of the image's width) on stream st.
-using DeviceFill = std::function<psift_status(char* extra, const std::vector<size_t>& dev_off, cudaStream_t st)>;
+// Writes the u8 inputs of images [b, e) of the batch into their device slots
+// (extra + dev_off[i], dense rows of the image's width) on stream st, the stream
+// that then runs those images' stages; called once per chunk, just before it.
+using DeviceFill = std::function<psift_status(char* extra, const std::vector<size_t>& dev_off, uint32_t b,
+                                              uint32_t e, cudaStream_t st)>;
 psift_status detect_batch_host_out(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
                                    const psift_sift_config* cfg, psift_features* outs, const DeviceFill* fill);
 void jpeg_release(psift_ctx* ctx);
