@@ -127,3 +127,32 @@ def test_search_same_hits_with_either_votes_path():
     with pytest.raises(psift.PsiftError):
         cat.set_search_votes(psift.VOTES_MIH_INDEX)
     cat.close()
+
+
+def test_reference_mih_indexed_search_and_remove():
+    # tests/pipeline_tests.rs:1439-1489 through the device catalog: 40 entries, the
+    # sample image's features at entry 17 among two synthetic scenes; the search
+    # (MIH tables) ranks item_17 first; remove is a swap_remove.
+    import scene_cases
+    import sweep_cases
+    sift = psift.Sift.new(psift.SiftConfig().with_octaves(3).with_scales(3).with_contrast_threshold(0.015))
+    target = sift.detect_and_compute_u8(sweep_cases.aerial_west_luma())
+    d1 = sift.detect_and_compute_u8(scene_cases.render_synthetic_scene(1))
+    d2 = sift.detect_and_compute_u8(scene_cases.render_synthetic_scene(2))
+    feats = [target if i == 17 else (d1 if i % 2 == 0 else d2) for i in range(40)]
+    cat = psift.DeviceCatalog()
+    for i, f in enumerate(feats):
+        cat.upsert_entry(f"item_{i:02d}.png", 220, 220, f)
+    hits = cat.search_features(target, top_k=3, shortlist_k=8)
+    assert hits and hits[0].id == "item_17.png"
+    qcodes = psift.quantize_descriptor_u128(target.descriptors)
+
+    def walk(fs):
+        sigs = [O.quantize_u128(f.descriptors) for f in fs]
+        off = np.concatenate([[0], np.cumsum([len(s) for s in sigs])]).astype(np.int64)
+        return O.mih_votes_tables(qcodes, np.concatenate(sigs), off)
+    np.testing.assert_array_equal(cat.votes(qcodes, psift.VOTES_AUTO), walk(feats))
+    assert cat.remove("item_17.png") and not cat.remove("item_17.png") and len(cat) == 39
+    feats[17] = feats.pop()  # swap_remove
+    np.testing.assert_array_equal(cat.votes(qcodes, psift.VOTES_AUTO), walk(feats))
+    cat.close()
