@@ -1,4 +1,10 @@
-"""Catalog top-k search sharded over ranks (one process per GPU).
+"""Work split over ranks (one process per GPU).
+
+Extraction and matching: images and pairs are independent, so each rank takes
+its own share (``rank_items``) with no exchange on the data path, and a timed
+region is reported as the slowest rank's (``max_over_ranks``).
+
+Catalog top-k search: sharded over ranks.
 
 Each rank owns the contiguous code range ``shard_range(ncat, rank, world)`` and
 computes the per-query top-k of its shard (``psift.hamming_topk`` on its GPU by
@@ -12,6 +18,32 @@ the shards' top-k lists.  Only the 4096 x k lists cross the interconnect
 from __future__ import annotations
 
 import numpy as np
+
+
+def rank_items(n_items: int, rank: int, world: int) -> list[int]:
+    """Round-robin share of `rank` among n_items independent images or pairs:
+    item i belongs to rank i mod world (shares differ in size by at most 1)."""
+    return list(range(int(rank), int(n_items), int(world)))
+
+
+def rank_image_seeds(batch: int, rank: int) -> list[int]:
+    """Seeds of the `batch` synthetic images rank `rank` detects per step when the
+    work scales weakly (every rank a full batch of its own, no image shared)."""
+    return [1000 * int(rank) + 1 + i for i in range(int(batch))]
+
+
+def max_over_ranks(value: float, group=None) -> float:
+    """The largest of every rank's `value` (a timed region's milliseconds), on
+    every rank; `value` itself when no process group is initialised."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(value)
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
 
 
 def shard_range(ncat: int, rank: int, world: int) -> tuple[int, int]:

@@ -9,10 +9,12 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def _run(env_extra):
+def _run(env_extra, gpus=None):
     env = dict(os.environ, **env_extra)
+    gpus = gpus if gpus is not None else int(env_extra.get("WORLD_SIZE", "1"))
     return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                           "--warmup", "0"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+                           "--warmup", "0", "--gpus", str(gpus)], cwd=ROOT, env=env, capture_output=True, text=True,
+                          timeout=600)
 
 
 def test_reference_arm_line():
@@ -34,4 +36,11 @@ def test_reference_arm_line():
 def test_reference_arm_other_ranks_exit_quietly():
     r = _run({"RANK": "1", "WORLD_SIZE": "2"})
     assert r.returncode == 0
+    assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_gpus_must_match_the_launch():
+    """--gpus N without N ranks is refused: the bench runs one process per GPU."""
+    r = _run({"WORLD_SIZE": "1"}, gpus=8)
+    assert r.returncode != 0 and "WORLD_SIZE" in r.stderr
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]

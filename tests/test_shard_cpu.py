@@ -71,3 +71,45 @@ def test_merge_handles_short_lists():
                                                                          np.array([[5, 7]], np.uint32), 0)], axis=1)
     i, d = shard.merge_keys(keys, 3)
     assert i.tolist() == [[1, 103, 2]] and d.tolist() == [[5, 5, 7]]
+
+
+def _split_worker(rank, world, port, n_items, ms, out):
+    import datetime
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        items = shard.rank_items(n_items, rank, world)
+        seeds = shard.rank_image_seeds(4, rank)
+        slowest = shard.max_over_ranks(ms[rank])
+        out[rank] = (items, seeds, slowest)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,n_items", [(2, 64), (2, 7), (3, 32)])
+def test_extraction_split_and_max_over_ranks(world, n_items):
+    """Images (and pairs) are split round-robin with no exchange: every item on
+    exactly one rank, shares within one item of each other; the weak-scaling
+    bench gives every rank its own images (disjoint seeds); the timed region is
+    the slowest rank's on every rank."""
+    ms = [10.0 + 7.5 * r for r in range(world)][::-1]
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_split_worker, args=(world, port, n_items, ms, out), nprocs=world, start_method="spawn",
+                       join=True)
+    got = [out[r] for r in range(world)]
+    every = sorted(i for items, _, _ in got for i in items)
+    assert every == list(range(n_items))
+    sizes = [len(items) for items, _, _ in got]
+    assert max(sizes) - min(sizes) <= 1
+    seeds = [s for _, ss, _ in got for s in ss]
+    assert len(set(seeds)) == len(seeds) == 4 * world
+    assert all(slowest == max(ms) for _, _, slowest in got)
+
+
+def test_max_over_ranks_without_a_group():
+    assert shard.max_over_ranks(3.25) == 3.25
