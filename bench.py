@@ -32,6 +32,7 @@ sys.path.insert(0, os.path.join(ROOT, "pure-sift_b200"))
 
 import numpy as np  # noqa: E402
 
+import shard  # noqa: E402
 import synth  # noqa: E402
 
 WIDTH, HEIGHT = 1920, 1080
@@ -115,11 +116,9 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_images(n: int, seed0: int):
-    imgs = []
-    for i in range(n):
-        imgs.append(synth.blob_image(WIDTH, HEIGHT, 2000, 1.5, 20.0, seed=seed0 + i))
-    return imgs
+def make_images(n: int, seed0: int = 1, seeds=None):
+    seeds = list(seeds) if seeds is not None else [seed0 + i for i in range(n)]
+    return [synth.blob_image(WIDTH, HEIGHT, 2000, 1.5, 20.0, seed=sd) for sd in seeds[:n]]
 
 
 def pyramid_bytes_per_image(h: int, w: int) -> tuple[float, int]:
@@ -348,17 +347,34 @@ def catalog_bench(ctx, torch, n_cat: int = 2_000_000, n_q: int = 4096, k: int = 
     popc_s = pairs * 3 / (ms["topk"] * 1e-3)  # three popcounts per pair (carry-save step)
     # the query's own (perturbed) source descriptor should be found by the shortlist
     hit = float((idx == pick[:, None].int()).any(dim=1).float().mean().item())
+    # outside the timed region: the whole top-64 and the re-rank against the CPU
+    # restatement (OpenMP), bit for bit
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    hq = q_codes.cpu().numpy().view(np.uint64)
+    hc = cat_codes.cpu().numpy().view(np.uint64)
+    t_cpu = time.perf_counter()
+    ci, cd = O.hamming_topk(hq, hc, k)
+    cpu_topk_s = time.perf_counter() - t_cpu
+    gi, gd = idx.cpu().numpy().view(np.uint32), dist.cpu().numpy().view(np.uint32)
+    topk_exact = bool(np.array_equal(ci, gi) and np.array_equal(cd, gd))
+    ri, rd = O.l2_rerank(q.cpu().numpy(), cat.cpu().numpy(), ci)
+    rerank_exact = bool(np.array_equal(ri, ridx.cpu().numpy().view(np.uint32)) and
+                        np.array_equal(rd.view(np.uint32), rd2.cpu().numpy().view(np.uint32)))
     return {
-        "workload": f"{n_cat} catalog codes (10,000 images x 200), {n_q} queries, top-{k} XOR+POPCNT shortlist "
+        "workload": f"{n_cat} catalog codes ({n_cat // 200:,} images x 200), {n_q} queries, top-{k} XOR+POPCNT shortlist "
                     f"+ exact FP32 L2 re-rank",
         "ms": {"quantize_2M": ms["quantize"], "topk": ms["topk"], "l2_rerank": ms["rerank"],
                "search_total": ms["topk"] + ms["rerank"]},
         "topk_pairs_per_s": pairs / (ms["topk"] * 1e-3),
         "roofline_topk": {"bound": "int (popc)", "achieved": popc_s, "peak": peak.value, "unit": "popc/s",
                           "frac": popc_s / peak.value, "popc_per_pair": 3,
-                          "peak_source": "measured: psift_popc_throughput (popc+xor+add register chains)"},
+                          "peak_source": "this library's own probe kernel psift_popc_throughput (popc+xor+add register "
+                                         "chains); the measured-peaks file has no integer peak"},
         "quantize_gbs": n_cat * 512 / (ms["quantize"] * 1e-3) / 1e9,
         "source_in_shortlist": hit,
+        "bit_exact_vs_cpu": {"topk": topk_exact, "l2_rerank": rerank_exact,
+                             "cpu": f"CPU restatement, OpenMP {os.cpu_count()} threads, {cpu_topk_s:.1f} s for the top-k"},
     }
 
 
@@ -786,7 +802,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     B = args.batch
-    host_imgs = make_images(B, seed0=1000 * rank + 1)
+    host_imgs = make_images(B, seeds=shard.rank_image_seeds(B, rank))
     d_imgs = [torch.from_numpy(im).cuda() for im in host_imgs]
     cap = MAX_FEATURES
     outs = [{k: torch.empty(cap, dtype=torch.float32, device="cuda") for k in ("x", "y", "s", "r", "o")}
@@ -830,10 +846,8 @@ def run_ours(args):
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launch_count - launches0
+    ms = shard.max_over_ranks(ms)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     ms_per_step = ms / args.steps
     value = world * B * args.steps / (ms / 1e3)
@@ -945,10 +959,7 @@ def run_ours(args):
     single4_s = (time.perf_counter() - t1) / single_rounds
     for c in callers:
         c.close()
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = shard.max_over_ranks(e2e_s)
     e2e_value = world * B * e2e_steps / e2e_s
 
     result = None
@@ -1027,6 +1038,9 @@ def main():
     ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "warp", "fundamental",
                                                "learned_ransac", "uneven_batch", "jpeg"],
                     help="run one section alone (profiling case)")
+    ap.add_argument("--ransac-pairs", type=int, default=1024, help="learned-RANSAC section: match sets")
+    ap.add_argument("--catalog-codes", type=int, default=2_000_000, help="catalog section: catalog codes")
+    ap.add_argument("--catalog-entries", type=int, default=10_000, help="catalog-search section: entries")
     ap.add_argument("--no-catalog", action="store_true")
     ap.add_argument("--no-catalog-search", dest="no_catalog_search", action="store_true")
     ap.add_argument("--no-warp", dest="no_warp", action="store_true")
@@ -1037,6 +1051,11 @@ def main():
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
     ap.add_argument("--no-jpeg", dest="no_jpeg", action="store_true")
     args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        # one process per GPU: --gpus N runs under torchrun with N ranks
+        sys.exit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch N>1 with "
+                 f"`python -m torch.distributed.run --nproc-per-node {args.gpus} bench.py --gpus {args.gpus}`")
     if args.impl == "reference":
         return run_reference(args)
     if args.match_only:
@@ -1047,8 +1066,9 @@ def main():
         import psift
         ctx = psift.Context(int(os.environ.get("LOCAL_RANK", "0")))
         fns = {"match": lambda: match_bench(ctx, torch, n_pairs=args.match_pairs, reps=args.steps),
-               "catalog": lambda: catalog_bench(ctx, torch), "learned_ransac": lambda: ransac_bench(ctx, torch),
-               "catalog_search": lambda: catalog_search_bench(ctx, torch), "warp": lambda: warp_bench(ctx, torch),
+               "catalog": lambda: catalog_bench(ctx, torch, n_cat=args.catalog_codes),
+               "learned_ransac": lambda: ransac_bench(ctx, torch, n_pairs=args.ransac_pairs),
+               "catalog_search": lambda: catalog_search_bench(ctx, torch, n_entries=args.catalog_entries), "warp": lambda: warp_bench(ctx, torch),
                "fundamental": lambda: fundamental_bench(ctx, torch),
                "uneven_batch": lambda: uneven_bench(ctx, torch), "jpeg": lambda: jpeg_bench(ctx, torch)}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)

@@ -4,7 +4,7 @@
  *
  * The reference exposes this path as a Rust API (src/lib.rs:26-52) with no FFI
  * of its own.  Each entry point below names the reference function it replaces;
- * a Rust binding crate (see INTEGRATION.md) maps the reference's structs onto
+ * a Rust binding crate maps the reference's structs onto
  * these plain-pointer signatures so `Sift::detect_and_compute`, `Matcher::match_`,
  * `Homography::estimate` and the catalog search keep their signatures.
  *
@@ -544,12 +544,20 @@ psift_status psift_warp_and_stitch_dev(psift_ctx* ctx, const uint8_t* query, uin
  * scratch lives in a 32 MiB file-scope device array inside this library (held by
  * every GPU that loads it until exit); the call makes no cudaMalloc/cudaFree or
  * other allocating call.  Enough for a 320x240 image at the reference defaults
- * (octaves <= 4, scales 3, first-octave upsampling); a request needing more
- * scratch returns PSIFT_ERR_CAPACITY without touching the GPU.
+ * (octaves <= 4, scales 3, first-octave upsampling) with at most 65536 DoG
+ * extrema (the regular entries hold 262144); a request needing more scratch
+ * returns PSIFT_ERR_CAPACITY without touching the GPU, and more extrema than
+ * 65536 returns PSIFT_ERR_CAPACITY after the run.
  *  - luma, out->x..descriptors (capacity out->capacity) and d_count are device
- *    pointers; cuda_stream is a cudaStream_t (NULL = legacy default stream).
+ *    pointers; cuda_stream is a cudaStream_t (NULL = legacy default stream)
+ *    that must belong to the current device (else PSIFT_ERR_INVALID_ARGUMENT).
+ *  - More features than out->capacity: the first out->capacity are written,
+ *    *d_count is set to the number needed and the call returns
+ *    PSIFT_ERR_CAPACITY, as the regular entries do.
  *  - The first call on a device looks up the scratch array's device address
- *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *    (cudaGetSymbolAddress) and keeps it for the life of the process; make that
+ *    first call before any stream capture.  After cudaDeviceReset the kept
+ *    address is stale: the entry does not support a device reset.
  *  - The call queues the work on cuda_stream and waits for it to finish.
  *  - Every call shares the one scratch array: calls that overlap on the GPU
  *    (other streams, other host threads) race and corrupt each other. */

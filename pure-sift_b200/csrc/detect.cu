@@ -1357,6 +1357,13 @@ extern "C" psift_status psift_detect_and_compute_u8_noalloc_dev(const uint8_t* l
   if (!out || !d_count || (height && width && !luma) || row_stride < width || !out->x || !out->y || !out->scale ||
       !out->response || !out->orientation || !out->descriptors || out->capacity == 0)
     return PSIFT_ERR_INVALID_ARGUMENT;
+  if (local.stream) {
+    // the stream must belong to the current device, whose scratch address is used
+    int cur = 0, sdev = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess || cudaStreamGetDevice(local.stream, &sdev) != cudaSuccess)
+      return PSIFT_ERR_CUDA;
+    if (sdev != cur) return PSIFT_ERR_INVALID_ARGUMENT;
+  }
   void* scratch = nullptr;
   st = noalloc_scratch_address(&local, &scratch);
   if (st != PSIFT_OK) return st;
@@ -1384,11 +1391,25 @@ extern "C" psift_status psift_detect_and_compute_u8_noalloc_dev(const uint8_t* l
   if (e != cudaSuccess) return PSIFT_ERR_CUDA;
   st = launch_detect(&local, job, *cfg, false);
   if (st != PSIFT_OK) return st;
-  uint32_t h_err = 0;
+  // the error word and the number of features found (before the output cut)
+  uint32_t h_err = 0, h_total = 0;
   e = cudaMemcpyAsync(&h_err, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, local.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&h_total, job.plans[0].feat_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, local.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(local.stream);
   if (e != cudaSuccess) return PSIFT_ERR_CUDA;
+  // same mapping as the regular entries: capacity, timeout, internal
   if (h_err & kErrKeypointCapacity) return PSIFT_ERR_CAPACITY;
+  if (h_err & kErrSortCapacity) return PSIFT_ERR_INTERNAL;
+  if (h_err & kErrTimeout) return PSIFT_ERR_TIMEOUT;
   if (h_err) return PSIFT_ERR_INTERNAL;
+  const uint32_t needed = cfg->max_features && h_total > cfg->max_features ? cfg->max_features : h_total;
+  if (needed > out->capacity) {
+    // the kernels cut the list at the capacity; report the size that was needed
+    e = cudaMemcpyAsync(d_count, &needed, sizeof(uint32_t), cudaMemcpyHostToDevice, local.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(local.stream);
+    if (e != cudaSuccess) return PSIFT_ERR_CUDA;
+    return PSIFT_ERR_CAPACITY;
+  }
   return PSIFT_OK;
 }
