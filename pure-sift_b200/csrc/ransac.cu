@@ -13,14 +13,21 @@
 // Identical results for the same seed.  The random stream does not depend on
 // the data except through the CDF, so samples are drawn ahead: splitmix64's
 // state advances by a constant, draw t is a pure function of (seed, t).
-// Hypotheses are generated and fitted 64 at a time (one thread each; f64 DLT with
-// the reference's cyclic Jacobi, same operation order), their inlier counts are
-// computed by the whole CTA, and thread 0 replays the reference's loop in order:
-// every decision (count, tie on the sequential error sum, adaptive iteration
-// budget, LO refinement) is taken exactly as the reference takes it.  Error sums
-// that decide something are the reference's sequential sums over the matches in
-// input order (computed in parallel per match, summed serially); LO refits
-// accumulate A^T A per entry sequentially over the inliers in order (45 threads).
+// Hypotheses are generated and fitted 64 at a time: a quad of lanes per
+// homography fit (f64 DLT; the cyclic Jacobi's rotations shared by the quad in
+// shared memory, each lane updating rows ql, ql + 4, ql + 8, so every value is
+// the sequential solver's), then counted by warps (two hypotheses per pass over
+// the packed match coordinates, no block barrier), and the reference's loop is
+// replayed in order by every thread on identical shared values: every decision
+// (count, tie on the sequential error sum, adaptive iteration budget, LO
+// refinement) is taken exactly as the reference takes it.  Error sums are needed
+// only to break a tie on the count, so they are computed when a tie occurs (for
+// the incumbent too, if its sum is not known yet): an error sum is a function of
+// the model alone, so the deferred value is the one the reference computed.
+// Error sums are the reference's sequential sums over the matches in input order
+// (terms computed in parallel, summed serially); LO refits accumulate A^T A per
+// entry sequentially over the inliers in order (45 threads) and solve it with one
+// quad.
 #include <stdint.h>
 
 #include "psift_internal.cuh"
@@ -29,57 +36,28 @@
 namespace psift {
 
 constexpr int kRThreads = 256;
+constexpr int kRWarps = kRThreads / 32;
 constexpr int kBatch = 64;
 constexpr int kDrawChunk = kBatch * 16;
-
-struct RansacJob {
-  const psift_match* m;
-  int n;
-  float thr;
-  uint64_t sim_seed, hom_seed;
-  int homography;           // 0: similarity only, 1: homography (similarity seed first)
-  const float* weights;     // optional sampling weights replacing 1/clamp(ratio) (guided sampling)
-  // scratch (n entries each, draws: draw_cap)
-  double* cdf;
-  double* err;
-  int* list;
-  int* draws;
-  int draw_cap;
-  // outputs
-  uint8_t* mask;
-  float* model;             // similarity: a, b, tx, ty, scale, rotation_deg; homography: 9 (row-major)
-  int* has_model;
-  int* count;
-  int* iters;               // [0] similarity iterations, [1] homography iterations
-  double* pts;              // 4 per match: the current inlier list's coordinates, gathered
-};
+// Jacobi matrix and eigenvectors (81 doubles each) of every hypothesis of a batch
+constexpr size_t kJacSmem = sizeof(double) * 162 * kBatch;
+// LO refits stage row values (10 doubles per point) in the same buffer
+constexpr int kRowChunk = (int)(kJacSmem / (sizeof(double) * 10));
 
 struct RShared {
   int n;
   float tsq_f;
   double tsq_d;
-  // similarity state
-  float ba, bb, btx, bty;
-  int best_count;
-  float best_err_f;
-  double best_err_d;
-  int max_iters;
-  int stop;
   int top32[32];
-  int ntop;
   // batch of hypotheses
   float ha[kBatch], hb[kBatch], htx[kBatch], hty[kBatch];
   double H[kBatch][9];
   int hvalid[kBatch];
   int hcnt[kBatch];
   int quad[kBatch][4];
-  // homography state
-  double BH[9];
-  int has_bh;
   // scratch scalars
   unsigned long long key_min;
   int flag;
-  int ires[4];
   float fres[8];
   double dres[16];
   double ata[9][9];
@@ -168,7 +146,7 @@ __device__ __forceinline__ int block_sum_int(int v, RShared& S) {
   if ((threadIdx.x & 31) == 0) S.red_u[threadIdx.x >> 5] = (uint32_t)v;
   __syncthreads();
   int t = 0;
-  for (int w = 0; w < kRThreads / 32; ++w) t += (int)S.red_u[w];
+  for (int w = 0; w < kRWarps; ++w) t += (int)S.red_u[w];
   __syncthreads();
   return t;
 }
@@ -179,7 +157,7 @@ __device__ __forceinline__ double block_sum_double(double v, RShared& S) {
   if ((threadIdx.x & 31) == 0) S.red_d[threadIdx.x >> 5] = v;
   __syncthreads();
   double t = 0.0;
-  for (int w = 0; w < kRThreads / 32; ++w) t += S.red_d[w];
+  for (int w = 0; w < kRWarps; ++w) t += S.red_d[w];
   __syncthreads();
   return t;
 }
@@ -205,25 +183,67 @@ __device__ int adaptive_iters_w(double w, int ss, int min_it, int cap) {
   return (int)c;
 }
 
+// Sequential sum of v[0..n) in order (one thread); the loads are issued 16 ahead
+// of the dependent additions.  Terms of matches that are not inliers are zero,
+// which leaves the running sum unchanged (x + 0 == x for the finite, non-negative
+// partial sums), so this equals the reference's sum over the inliers alone.
+template <typename T>
+__device__ T seq_sum(const T* __restrict__ v, int n) {
+  T s = T(0);
+  int i = 0;
+  for (; i + 16 <= n; i += 16) {
+    T e[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) e[u] = v[i + u];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) s += e[u];
+  }
+  for (; i < n; ++i) s += v[i];
+  return s;
+}
+
 // ------------------------------------------------------------- similarity
-__device__ __forceinline__ bool sim_inlier(const psift_match& m, float a, float b, float tx, float ty, float tsq,
-                                           float& e) {
-  const float px = a * m.query_x - b * m.query_y + tx;
-  const float py = b * m.query_x + a * m.query_y + ty;
-  const float dx = px - m.target_x;
-  const float dy = py - m.target_y;
+// evaluate_similarity_hypothesis's per-match test (src/pipeline.rs:1884-1893).
+__device__ __forceinline__ bool sim_inlier(const float4 p, float a, float b, float tx, float ty, float tsq, float& e) {
+  const float px = a * p.x - b * p.y + tx;
+  const float py = b * p.x + a * p.y + ty;
+  const float dx = px - p.z;
+  const float dy = py - p.w;
   e = dx * dx + dy * dy;
   return e <= tsq;
 }
 
-// Count of a similarity hypothesis (whole CTA).
-__device__ int sim_count(const RansacJob& J, RShared& S, float a, float b, float tx, float ty) {
-  int c = 0;
-  for (int i = threadIdx.x; i < S.n; i += kRThreads) {
-    float e;
-    c += sim_inlier(J.m[i], a, b, tx, ty, S.tsq_f, e) ? 1 : 0;
+// Inlier counts of the similarity hypotheses h < nh of the batch (S.ha.. /
+// S.hvalid -> S.hcnt): warp w takes h = w, w + 8, ..., two per pass over the
+// matches.  Ends with a block barrier.
+__device__ void sim_count_batch(const RansacJob& J, RShared& S, int nh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float tsq = S.tsq_f;
+  for (int h = warp; h < nh; h += 2 * kRWarps) {
+    const int h2 = h + kRWarps;
+    const bool v1 = S.hvalid[h] != 0, v2 = h2 < nh && S.hvalid[h2] != 0;
+    int c1 = 0, c2 = 0;
+    if (v1 || v2) {
+      const float a1 = S.ha[h], b1 = S.hb[h], x1 = S.htx[h], y1 = S.hty[h];
+      const float a2 = v2 ? S.ha[h2] : 0.f, b2 = v2 ? S.hb[h2] : 0.f, x2 = v2 ? S.htx[h2] : 0.f,
+                  y2 = v2 ? S.hty[h2] : 0.f;
+      for (int i = lane; i < S.n; i += 32) {
+        const float4 p = J.xy[i];
+        float e;
+        c1 += (v1 && sim_inlier(p, a1, b1, x1, y1, tsq, e)) ? 1 : 0;
+        c2 += (v2 && sim_inlier(p, a2, b2, x2, y2, tsq, e)) ? 1 : 0;
+      }
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+      c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+      c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+    }
+    if (lane == 0) {
+      S.hcnt[h] = c1;
+      if (h2 < nh) S.hcnt[h2] = c2;
+    }
   }
-  return block_sum_int(c, S);
+  __syncthreads();
 }
 
 __device__ double weight_total(const RansacJob& J, RShared& S) {
@@ -236,7 +256,7 @@ __device__ double sim_mass(const RansacJob& J, RShared& S, float a, float b, flo
   double t = 0.0;
   for (int i = threadIdx.x; i < S.n; i += kRThreads) {
     float e;
-    if (sim_inlier(J.m[i], a, b, tx, ty, S.tsq_f, e)) t += (double)J.weights[i];
+    if (sim_inlier(J.xy[i], a, b, tx, ty, S.tsq_f, e)) t += (double)J.weights[i];
   }
   return block_sum_double(t, S);
 }
@@ -246,28 +266,10 @@ __device__ float sim_err(const RansacJob& J, RShared& S, float a, float b, float
   float* buf = reinterpret_cast<float*>(J.err);
   for (int i = threadIdx.x; i < S.n; i += kRThreads) {
     float e;
-    buf[i] = sim_inlier(J.m[i], a, b, tx, ty, S.tsq_f, e) ? e : -1.0f;
+    buf[i] = sim_inlier(J.xy[i], a, b, tx, ty, S.tsq_f, e) ? e : 0.0f;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    // in order; 16 loads are issued ahead of the dependent additions
-    float s = 0.0f;
-    const int n = S.n;
-    int i = 0;
-    for (; i + 16 <= n; i += 16) {
-      float e[16];
-#pragma unroll
-      for (int u = 0; u < 16; ++u) e[u] = buf[i + u];
-#pragma unroll
-      for (int u = 0; u < 16; ++u)
-        if (e[u] >= 0.0f) s += e[u];
-    }
-    for (; i < n; ++i) {
-      const float e = buf[i];
-      if (e >= 0.0f) s += e;
-    }
-    S.fres[0] = s;
-  }
+  if (threadIdx.x == 0) S.fres[0] = seq_sum(buf, S.n);
   __syncthreads();
   const float r = S.fres[0];
   __syncthreads();
@@ -281,10 +283,10 @@ __device__ int sim_collect(const RansacJob& J, RShared& S, float a, float b, flo
     const int i = c0 + threadIdx.x;
     bool in = false;
     if (i < S.n) {
-      const psift_match& m = J.m[i];
+      const float4 p = J.xy[i];
       // the collection expression of src/pipeline.rs:2161-2166 / :2172-2178
-      const float dx = (a * m.query_x - b * m.query_y + tx) - m.target_x;
-      const float dy = (b * m.query_x + a * m.query_y + ty) - m.target_y;
+      const float dx = (a * p.x - b * p.y + tx) - p.z;
+      const float dy = (b * p.x + a * p.y + ty) - p.w;
       in = dx * dx + dy * dy <= S.tsq_f;
     }
     const unsigned bal = __ballot_sync(0xffffffffu, in);
@@ -292,7 +294,7 @@ __device__ int sim_collect(const RansacJob& J, RShared& S, float a, float b, flo
     if ((threadIdx.x & 31) == 0) S.red_u[threadIdx.x >> 5] = __popc(bal);
     __syncthreads();
     int pre = 0, tot = 0;
-    for (int w = 0; w < kRThreads / 32; ++w) {
+    for (int w = 0; w < kRWarps; ++w) {
       if (w < (int)(threadIdx.x >> 5)) pre += (int)S.red_u[w];
       tot += (int)S.red_u[w];
     }
@@ -325,10 +327,7 @@ __device__ bool procrustes(const RansacJob& J, RShared& S, int k, float* out6) {
   // Gather the inliers (list order): P[j] = (q.x, q.y, t.x, t.y); the sums stay
   // sequential in list order, their loads contiguous and issued ahead.
   float4* P = reinterpret_cast<float4*>(J.pts);
-  for (int j = threadIdx.x; j < k; j += kRThreads) {
-    const psift_match& m = J.m[J.list[j]];
-    P[j] = make_float4(m.query_x, m.query_y, m.target_x, m.target_y);
-  }
+  for (int j = threadIdx.x; j < k; j += kRThreads) P[j] = J.xy[J.list[j]];
   __syncthreads();
   if (threadIdx.x < 4) {
     float s = 0.0f;
@@ -375,6 +374,45 @@ __device__ bool procrustes(const RansacJob& J, RShared& S, int k, float* out6) {
   __syncthreads();
   for (int i = 0; i < 6; ++i) out6[i] = (float)S.dres[i];
   __syncthreads();
+  return true;
+}
+
+// The incumbent of a replay: every thread holds the same copy (the replay reads
+// only shared values that stay fixed while it runs, so every thread takes the
+// same decisions); err is valid when err_known.
+struct SimBest {
+  float a, b, tx, ty;
+  int count;
+  float err;
+  bool err_known;
+};
+
+// Replays hypothesis h of the batch against the incumbent (count first, the
+// sequential error sum on a tie): true if it replaces the incumbent.
+__device__ bool sim_consider(const RansacJob& J, RShared& S, SimBest& B, int h) {
+  const int c = S.hcnt[h];
+  if (c < B.count) return false;
+  const float a = S.ha[h], b = S.hb[h], tx = S.htx[h], ty = S.hty[h];
+  if (c > B.count) {
+    B.count = c;
+    B.err_known = false;
+  } else {
+    // the same parameters as the incumbent give the same error sum: not below it
+    if (__float_as_uint(a) == __float_as_uint(B.a) && __float_as_uint(b) == __float_as_uint(B.b) &&
+        __float_as_uint(tx) == __float_as_uint(B.tx) && __float_as_uint(ty) == __float_as_uint(B.ty))
+      return false;
+    if (!B.err_known) {
+      B.err = sim_err(J, S, B.a, B.b, B.tx, B.ty);
+      B.err_known = true;
+    }
+    const float e = sim_err(J, S, a, b, tx, ty);
+    if (!(e < B.err)) return false;
+    B.err = e;
+  }
+  B.a = a;
+  B.b = b;
+  B.tx = tx;
+  B.ty = ty;
   return true;
 }
 
@@ -427,7 +465,7 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
     __syncthreads();
     if (threadIdx.x == 0) {
       unsigned long long b = ~0ull;
-      for (int w = 0; w < kRThreads / 32; ++w) {
+      for (int w = 0; w < kRWarps; ++w) {
         const unsigned long long v = (unsigned long long)__double_as_longlong(S.dres[w]);
         b = v < b ? v : b;
       }
@@ -436,75 +474,52 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
     }
     __syncthreads();
   }
-  // initial model: translation of the lowest-ratio match
-  {
-    const psift_match& m0 = J.m[S.top32[0]];
-    const float a = 1.0f, b = 0.0f, tx = m0.displacement_x, ty = m0.displacement_y;
-    const int c = sim_count(J, S, a, b, tx, ty);
-    const float e = sim_err(J, S, a, b, tx, ty);
-    if (threadIdx.x == 0) {
-      S.ba = a;
-      S.bb = b;
-      S.btx = tx;
-      S.bty = ty;
-      S.best_count = c;
-      S.best_err_f = e;
-    }
-    __syncthreads();
+  // Phase A: the initial model (translation of the lowest-ratio match) and the 32
+  // one-point translations, counted together, replayed in order.  The initial
+  // model is translation 0: its evaluation is hypothesis 0's.
+  if (threadIdx.x < ntop) {
+    const psift_match& mr = J.m[S.top32[threadIdx.x]];
+    S.ha[threadIdx.x] = 1.0f;
+    S.hb[threadIdx.x] = 0.0f;
+    S.htx[threadIdx.x] = mr.displacement_x;
+    S.hty[threadIdx.x] = mr.displacement_y;
+    S.hvalid[threadIdx.x] = 1;
   }
-  // Phase A: the 32 one-point translations, in order
-  for (int r = 0; r < ntop; ++r) {
-    const psift_match& mr = J.m[S.top32[r]];
-    const float tx = mr.displacement_x, ty = mr.displacement_y;
-    const int c = sim_count(J, S, 1.0f, 0.0f, tx, ty);
-    if (c >= S.best_count) {
-      const float e = sim_err(J, S, 1.0f, 0.0f, tx, ty);
-      if (threadIdx.x == 0 && (c > S.best_count || e < S.best_err_f)) {
-        S.best_count = c;
-        S.best_err_f = e;
-        S.ba = 1.0f;
-        S.bb = 0.0f;
-        S.btx = tx;
-        S.bty = ty;
-      }
-    }
-    __syncthreads();
-  }
+  __syncthreads();
+  sim_count_batch(J, S, ntop);
+  SimBest B{1.0f, 0.0f, S.htx[0], S.hty[0], S.hcnt[0], 0.0f, false};
+  for (int r = 0; r < ntop; ++r) sim_consider(J, S, B, r);
+  __syncthreads();  // the batch slots are rewritten below
   // Phase B: adaptive 2-point hypotheses
   build_cdf(J, S);
   const bool guided = J.weights != nullptr;
   const double wtot = guided ? weight_total(J, S) : 1.0;
-  {
-    const double mass = guided ? sim_mass(J, S, S.ba, S.bb, S.btx, S.bty) : 0.0;
-    if (threadIdx.x == 0) {
-      S.max_iters = guided ? adaptive_iters_w(mass / wtot, 2, 64, 1000) : adaptive_iters(S.best_count, n, 2, 64, 1000);
-      S.stop = 0;
-    }
-  }
-  __syncthreads();
+  int max_iters = guided ? adaptive_iters_w(sim_mass(J, S, B.a, B.b, B.tx, B.ty) / wtot, 2, 64, 1000)
+                         : adaptive_iters(B.count, n, 2, 64, 1000);
   int iters_done = 0;
-  for (int base = 0; !S.stop && base < 1000; base += kBatch) {
-    if (base >= S.max_iters) break;
+  bool stop = false;
+  for (int base = 0; !stop && base < 1000; base += kBatch) {
+    if (base >= max_iters) break;
     const int t = threadIdx.x;
     if (t < kBatch) {
       const int it = base + t;  // 0-based iteration; draws 2it, 2it+1
       int i1 = sample_at(J.cdf, n, seed, 2ull * it);
       int i2 = sample_at(J.cdf, n, seed, 2ull * it + 1ull);
       if (i2 == i1) i2 = (i1 + 1) % n;
-      const psift_match& m1 = J.m[i1];
-      const psift_match& m2 = J.m[i2];
-      const float dxq = m2.query_x - m1.query_x, dyq = m2.query_y - m1.query_y;
+      const float4 m1 = J.xy[i1];
+      const float4 m2 = J.xy[i2];
+      const float dxq = m2.x - m1.x, dyq = m2.y - m1.y;
       const float dq = dxq * dxq + dyq * dyq;
       int valid = 0;
       float a = 0.f, b = 0.f, tx = 0.f, ty = 0.f;
       if (!(dq < 16.0f)) {
-        const float dxt = m2.target_x - m1.target_x, dyt = m2.target_y - m1.target_y;
+        const float dxt = m2.z - m1.z, dyt = m2.w - m1.w;
         a = (dxq * dxt + dyq * dyt) / dq;
         b = (dxq * dyt - dyq * dxt) / dq;
         const float s2 = a * a + b * b;
         if (s2 >= 0.04f && s2 <= 25.0f) {
-          tx = m1.target_x - (a * m1.query_x - b * m1.query_y);
-          ty = m1.target_y - (b * m1.query_x + a * m1.query_y);
+          tx = m1.z - (a * m1.x - b * m1.y);
+          ty = m1.w - (b * m1.x + a * m1.y);
           valid = 1;
         }
       }
@@ -513,59 +528,36 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
       S.htx[t] = tx;
       S.hty[t] = ty;
       S.hvalid[t] = valid;
-      S.hcnt[t] = 0;
     }
     __syncthreads();
-    for (int h = 0; h < kBatch; ++h) {
-      if (!S.hvalid[h]) continue;
-      const int c = sim_count(J, S, S.ha[h], S.hb[h], S.htx[h], S.hty[h]);
-      if (threadIdx.x == 0) S.hcnt[h] = c;
-    }
-    __syncthreads();
+    sim_count_batch(J, S, kBatch);
     // replay in order
     for (int h = 0; h < kBatch; ++h) {
       const int it = base + h;
-      if (it >= S.max_iters) {
-        if (threadIdx.x == 0) S.stop = 1;
-        __syncthreads();
+      if (it >= max_iters) {
+        stop = true;
         break;
       }
       iters_done = it + 1;
       if (!S.hvalid[h]) continue;
-      const int c = S.hcnt[h];
-      if (c < S.best_count) continue;
-      const float e = sim_err(J, S, S.ha[h], S.hb[h], S.htx[h], S.hty[h]);
-      const bool improved = c > S.best_count || e < S.best_err_f;
-      __syncthreads();
-      if (improved) {
-        const double mass = guided ? sim_mass(J, S, S.ha[h], S.hb[h], S.htx[h], S.hty[h]) : 0.0;
-        if (threadIdx.x == 0) {
-          S.best_count = c;
-          S.best_err_f = e;
-          S.ba = S.ha[h];
-          S.bb = S.hb[h];
-          S.btx = S.htx[h];
-          S.bty = S.hty[h];
-          S.max_iters = guided ? adaptive_iters_w(mass / wtot, 2, 64, 1000) : adaptive_iters(c, n, 2, 64, 1000);
-        }
-      }
-      __syncthreads();
+      if (sim_consider(J, S, B, h))
+        max_iters = guided ? adaptive_iters_w(sim_mass(J, S, B.a, B.b, B.tx, B.ty) / wtot, 2, 64, 1000)
+                           : adaptive_iters(B.count, n, 2, 64, 1000);
     }
     __syncthreads();
   }
   if (threadIdx.x == 0 && J.iters) J.iters[0] = iters_done;
   // consensus, Procrustes refit, re-collection
-  const float a0 = S.ba, b0 = S.bb, tx0 = S.btx, ty0 = S.bty;
-  int k = sim_collect(J, S, a0, b0, tx0, ty0);
+  int k = sim_collect(J, S, B.a, B.b, B.tx, B.ty);
   float refined[6];
   const bool has_ref = procrustes(J, S, k, refined);
   if (has_ref) {
     // count of the refined model's consensus (same expression as the collection)
     int c = 0;
     for (int i = threadIdx.x; i < n; i += kRThreads) {
-      const psift_match& m = J.m[i];
-      const float dx = (refined[0] * m.query_x - refined[1] * m.query_y + refined[2]) - m.target_x;
-      const float dy = (refined[1] * m.query_x + refined[0] * m.query_y + refined[3]) - m.target_y;
+      const float4 p = J.xy[i];
+      const float dx = (refined[0] * p.x - refined[1] * p.y + refined[2]) - p.z;
+      const float dy = (refined[1] * p.x + refined[0] * p.y + refined[3]) - p.w;
       c += dx * dx + dy * dy <= S.tsq_f ? 1 : 0;
     }
     c = block_sum_int(c, S);
@@ -587,23 +579,59 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
 }
 
 // ------------------------------------------------------------- homography
-__device__ __forceinline__ bool h_inlier(const psift_match& m, const double* H, double tsq, double& e) {
-  const double qx = m.query_x, qy = m.query_y;
+// evaluate_homography_hypothesis_f64's per-match test (src/pipeline.rs:2557-2573).
+__device__ __forceinline__ bool h_inlier(const float4 p, const double* H, double tsq, double& e) {
+  const double qx = p.x, qy = p.y;
   const double w = H[6] * qx + H[7] * qy + H[8];
   if (fabs(w) < 1e-9) return false;
   const double iw = 1.0 / w;
   const double px = (H[0] * qx + H[1] * qy + H[2]) * iw;
   const double py = (H[3] * qx + H[4] * qy + H[5]) * iw;
-  const double dx = px - (double)m.target_x, dy = py - (double)m.target_y;
+  const double dx = px - (double)p.z, dy = py - (double)p.w;
   e = dx * dx + dy * dy;
   return e <= tsq;
+}
+
+// Inlier counts of the homographies h < nh of the batch (S.H / S.hvalid ->
+// S.hcnt): warp w takes h = w, w + 8, ..., two per pass.  Ends with a barrier.
+__device__ void h_count_batch(const RansacJob& J, RShared& S, int nh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double tsq = S.tsq_d;
+  for (int h = warp; h < nh; h += 2 * kRWarps) {
+    const int h2 = h + kRWarps;
+    const bool v1 = S.hvalid[h] != 0, v2 = h2 < nh && S.hvalid[h2] != 0;
+    int c1 = 0, c2 = 0;
+    if (v1 || v2) {
+      double H1[9], H2[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        H1[i] = S.H[h][i];
+        H2[i] = v2 ? S.H[h2][i] : 0.0;
+      }
+      for (int i = lane; i < S.n; i += 32) {
+        const float4 p = J.xy[i];
+        double e;
+        c1 += (v1 && h_inlier(p, H1, tsq, e)) ? 1 : 0;
+        c2 += (v2 && h_inlier(p, H2, tsq, e)) ? 1 : 0;
+      }
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+      c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+      c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+    }
+    if (lane == 0) {
+      S.hcnt[h] = c1;
+      if (h2 < nh) S.hcnt[h2] = c2;
+    }
+  }
+  __syncthreads();
 }
 
 __device__ int h_count(const RansacJob& J, RShared& S, const double* H) {
   int c = 0;
   for (int i = threadIdx.x; i < S.n; i += kRThreads) {
     double e;
-    c += h_inlier(J.m[i], H, S.tsq_d, e) ? 1 : 0;
+    c += h_inlier(J.xy[i], H, S.tsq_d, e) ? 1 : 0;
   }
   return block_sum_int(c, S);
 }
@@ -612,36 +640,19 @@ __device__ double h_mass(const RansacJob& J, RShared& S, const double* H) {
   double t = 0.0;
   for (int i = threadIdx.x; i < S.n; i += kRThreads) {
     double e;
-    if (h_inlier(J.m[i], H, S.tsq_d, e)) t += (double)J.weights[i];
+    if (h_inlier(J.xy[i], H, S.tsq_d, e)) t += (double)J.weights[i];
   }
   return block_sum_double(t, S);
 }
 
+// Sequential f64 error sum over the inliers in input order (whole CTA).
 __device__ double h_err(const RansacJob& J, RShared& S, const double* H) {
   for (int i = threadIdx.x; i < S.n; i += kRThreads) {
     double e;
-    J.err[i] = h_inlier(J.m[i], H, S.tsq_d, e) ? e : -1.0;
+    J.err[i] = h_inlier(J.xy[i], H, S.tsq_d, e) ? e : 0.0;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    // in order; 16 loads are issued ahead of the dependent additions
-    double s = 0.0;
-    const int n = S.n;
-    int i = 0;
-    for (; i + 16 <= n; i += 16) {
-      double e[16];
-#pragma unroll
-      for (int u = 0; u < 16; ++u) e[u] = J.err[i + u];
-#pragma unroll
-      for (int u = 0; u < 16; ++u)
-        if (e[u] >= 0.0) s += e[u];
-    }
-    for (; i < n; ++i) {
-      const double e = J.err[i];
-      if (e >= 0.0) s += e;
-    }
-    S.dres[15] = s;
-  }
+  if (threadIdx.x == 0) S.dres[15] = seq_sum(J.err, S.n);
   __syncthreads();
   const double r = S.dres[15];
   __syncthreads();
@@ -655,14 +666,14 @@ __device__ int h_collect(const RansacJob& J, RShared& S, const double* H) {
     bool in = false;
     if (i < S.n) {
       double e;
-      in = h_inlier(J.m[i], H, S.tsq_d, e);
+      in = h_inlier(J.xy[i], H, S.tsq_d, e);
     }
     const unsigned bal = __ballot_sync(0xffffffffu, in);
     __syncthreads();
     if ((threadIdx.x & 31) == 0) S.red_u[threadIdx.x >> 5] = __popc(bal);
     __syncthreads();
     int pre = 0, tot = 0;
-    for (int w = 0; w < kRThreads / 32; ++w) {
+    for (int w = 0; w < kRWarps; ++w) {
       if (w < (int)(threadIdx.x >> 5)) pre += (int)S.red_u[w];
       tot += (int)S.red_u[w];
     }
@@ -673,65 +684,101 @@ __device__ int h_collect(const RansacJob& J, RShared& S, const double* H) {
   return base;
 }
 
-// smallest_eigenvector_9x9 (src/pipeline.rs:2276-2353), one thread.
-__device__ bool smallest_eigvec9(double (&a)[9][9], double* h) {
-  double v[9][9];
-  for (int i = 0; i < 9; ++i)
-    for (int j = 0; j < 9; ++j) v[i][j] = i == j ? 1.0 : 0.0;
+// Offset i * 9 + j of strict upper-triangle entry k (row-major, 36 entries).
+__device__ __forceinline__ int strict_upper_offset(int k) {
+  int i = 0;
+  while (k >= 8 - i) {
+    k -= 8 - i;
+    ++i;
+  }
+  return i * 9 + i + 1 + k;
+}
+
+// (a, b), a <= b, of upper-triangle entry e (row-major, 45 entries).
+__device__ __forceinline__ void upper_entry(int e, int& a, int& b) {
+  a = 0;
+  while (e >= 9 - a) {
+    e -= 9 - a;
+    ++a;
+  }
+  b = a + e;
+}
+
+// smallest_eigenvector_9x9 (src/pipeline.rs:2276-2353), the cyclic Jacobi shared
+// by a quad of lanes (ql = 0..3, converged, qmask their lane mask).  A (81
+// doubles, shared memory, symmetric and complete) is diagonalised in place; V
+// (81 doubles) accumulates the eigenvectors.  Every lane computes each
+// rotation's parameters from the same values; lane ql updates rows ql, ql + 4,
+// ql + 8 (a rotation's row updates touch disjoint entries), so every value and
+// decision is the sequential solver's.  Returns the column of the smallest
+// diagonal entry (the first on ties), or -1 if that eigenvector is not finite.
+// A and V are complete and visible to the quad on return.
+__device__ int quad_cyclic_jacobi(double* A, double* V, int ql, unsigned qmask) {
+  for (int r = ql; r < 9; r += 4)
+#pragma unroll
+    for (int c = 0; c < 9; ++c) V[r * 9 + c] = r == c ? 1.0 : 0.0;
+  // this lane's 9 of the 36 upper-triangle entries (row-major entries ql, ql + 4, ...)
+  int off[9];
+#pragma unroll
+  for (int s = 0; s < 9; ++s) off[s] = strict_upper_offset(ql + 4 * s);
+  __syncwarp(qmask);
   for (int sweep = 0; sweep < 20; ++sweep) {
-    double max_off = 0.0;
-    for (int p = 0; p < 9; ++p)
-      for (int q = p + 1; q < 9; ++q) {
-        const double av = fabs(a[p][q]);
-        if (av > max_off) max_off = av;
-      }
-    if (max_off < 1e-13) break;
+    double mx = 0.0;
+#pragma unroll
+    for (int s = 0; s < 9; ++s) {
+      const double v = fabs(A[off[s]]);
+      if (v > mx) mx = v;
+    }
+    mx = fmax(mx, __shfl_xor_sync(qmask, mx, 1));
+    mx = fmax(mx, __shfl_xor_sync(qmask, mx, 2));
+    if (mx < 1e-13) break;
     for (int p = 0; p < 8; ++p)
       for (int q = p + 1; q < 9; ++q) {
-        const double apq = a[p][q];
+        const double apq = A[p * 9 + q];
         if (fabs(apq) < 1e-15) continue;
-        const double app = a[p][p], aqq = a[q][q];
+        const double app = A[p * 9 + p], aqq = A[q * 9 + q];
         const double tau = (aqq - app) / (2.0 * apq);
         const double t = tau >= 0.0 ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
         const double c = 1.0 / sqrt(1.0 + t * t);
         const double s = t * c;
-        a[p][p] = app - t * apq;
-        a[q][q] = aqq + t * apq;
-        a[p][q] = 0.0;
-        a[q][p] = 0.0;
-        for (int r = 0; r < 9; ++r) {
-          if (r != p && r != q) {
-            const double arp = a[r][p], arq = a[r][q];
-            a[r][p] = c * arp - s * arq;
-            a[p][r] = a[r][p];
-            a[r][q] = s * arp + c * arq;
-            a[q][r] = a[r][q];
-          }
-          const double vrp = v[r][p], vrq = v[r][q];
-          v[r][p] = c * vrp - s * vrq;
-          v[r][q] = s * vrp + c * vrq;
+        __syncwarp(qmask);  // every pivot read precedes the writes
+        if (ql == 0) {
+          A[p * 9 + p] = app - t * apq;
+          A[q * 9 + q] = aqq + t * apq;
+          A[p * 9 + q] = 0.0;
+          A[q * 9 + p] = 0.0;
         }
+        for (int r = ql; r < 9; r += 4) {
+          if (r != p && r != q) {
+            const double arp = A[r * 9 + p], arq = A[r * 9 + q];
+            const double nrp = c * arp - s * arq, nrq = s * arp + c * arq;
+            A[r * 9 + p] = nrp;
+            A[p * 9 + r] = nrp;
+            A[r * 9 + q] = nrq;
+            A[q * 9 + r] = nrq;
+          }
+          const double vrp = V[r * 9 + p], vrq = V[r * 9 + q];
+          V[r * 9 + p] = c * vrp - s * vrq;
+          V[r * 9 + q] = s * vrp + c * vrq;
+        }
+        __syncwarp(qmask);
       }
   }
   int mi = 0;
-  double me = a[0][0];
+  double me = A[0];
   for (int i = 1; i < 9; ++i)
-    if (a[i][i] < me) {
-      me = a[i][i];
+    if (A[i * 10] < me) {
+      me = A[i * 10];
       mi = i;
     }
-  for (int r = 0; r < 9; ++r) {
-    h[r] = v[r][mi];
-    if (!isfinite(h[r])) return false;
-  }
-  return true;
+  for (int r = 0; r < 9; ++r)
+    if (!isfinite(V[r * 9 + mi])) return -1;
+  return mi;
 }
 
-// Normalisation + eigenvector -> de-normalised H (src/pipeline.rs:2482-2528).
-__device__ bool finish_dlt(double (&ata)[9][9], double sq, double st, double cxq, double cyq, double cxt, double cyt,
-                           double* H) {
-  double hv[9];
-  if (!smallest_eigvec9(ata, hv)) return false;
+// De-normalisation of the null vector hv (src/pipeline.rs:2500-2528).
+__device__ void denormalise(const double* hv, double sq, double st, double cxq, double cyq, double cxt, double cyt,
+                            double* H) {
   const double hn[3][3] = {{hv[0], hv[1], hv[2]}, {hv[3], hv[4], hv[5]}, {hv[6], hv[7], hv[8]}};
   const double tq[3][3] = {{sq, 0.0, -sq * cxq}, {0.0, sq, -sq * cyq}, {0.0, 0.0, 1.0}};
   const double ist = 1.0 / st;
@@ -745,29 +792,55 @@ __device__ bool finish_dlt(double (&ata)[9][9], double sq, double st, double cxq
     const double inv = 1.0 / H[8];
     for (int i = 0; i < 9; ++i) H[i] *= inv;
   }
-  return true;
 }
 
-// fit_homography_dlt_f64 on 4 matches, one thread.
-__device__ bool fit_dlt4(const psift_match* const* s, double* H) {
+// The two A^T A rows of one normalised correspondence (x, y) -> (x', y')
+// (src/pipeline.rs:2466-2479) take 10 distinct values, kept as one row:
+//   [-x, -y, -1, 0, x x', y x', x', x y', y y', y']
+// Row 1's entry a is row[(kSlot1 >> 4a) & 15], row 2's row[(kSlot2 >> 4a) & 15];
+// every value is the reference's (negation is exact, the products are the same
+// rounded products), so a sum of r1[a] r1[b] + r2[a] r2[b] terms is unchanged.
+constexpr int kRowVals = 10;
+constexpr unsigned long long kSlot1 = 0x654333210ull;  // -x -y -1 0 0 0 xx' yx' x'
+constexpr unsigned long long kSlot2 = 0x987210333ull;  // 0 0 0 -x -y -1 xy' yy' y'
+
+__device__ __forceinline__ void dlt_row_values(double x, double y, double xp, double yp, double* r) {
+  r[0] = -x, r[1] = -y, r[2] = -1.0, r[3] = 0.0, r[4] = x * xp, r[5] = y * xp, r[6] = xp, r[7] = x * yp,
+  r[8] = y * yp, r[9] = yp;
+}
+
+// fit_homography_dlt_f64 on 4 correspondences by a quad of lanes: every lane
+// normalises; lane i writes point i's row values (in V, free until the Jacobi
+// starts); the 45 A^T A entries are split over the lanes, each summed over the 4
+// points in order; the quad runs the Jacobi.  The result (H, return value) is
+// the leader's (ql == 0).
+__device__ bool quad_fit4(const float4* __restrict__ xy, const int* idx, double* A, double* V, int ql,
+                          unsigned qmask, double* H) {
+  double qx[4], qy[4], tx[4], ty[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float4 p = xy[idx[i]];
+    qx[i] = p.x, qy[i] = p.y, tx[i] = p.z, ty[i] = p.w;
+  }
   const double inv_n = 1.0 / 4.0;
   double cxq = 0, cyq = 0, cxt = 0, cyt = 0;
+#pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const double qx = s[i]->query_x, qy = s[i]->query_y, tx = s[i]->target_x, ty = s[i]->target_y;
-    if (!isfinite(qx) || !isfinite(qy) || !isfinite(tx) || !isfinite(ty)) return false;
-    cxq += qx;
-    cyq += qy;
-    cxt += tx;
-    cyt += ty;
+    if (!isfinite(qx[i]) || !isfinite(qy[i]) || !isfinite(tx[i]) || !isfinite(ty[i])) return false;
+    cxq += qx[i];
+    cyq += qy[i];
+    cxt += tx[i];
+    cyt += ty[i];
   }
   cxq *= inv_n;
   cyq *= inv_n;
   cxt *= inv_n;
   cyt *= inv_n;
   double mdq = 0, mdt = 0;
+#pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const double dxq = (double)s[i]->query_x - cxq, dyq = (double)s[i]->query_y - cyq;
-    const double dxt = (double)s[i]->target_x - cxt, dyt = (double)s[i]->target_y - cyt;
+    const double dxq = qx[i] - cxq, dyq = qy[i] - cyq;
+    const double dxt = tx[i] - cxt, dyt = ty[i] - cyt;
     mdq += sqrt(dxq * dxq + dyq * dyq);
     mdt += sqrt(dxt * dxt + dyt * dyt);
   }
@@ -775,32 +848,47 @@ __device__ bool fit_dlt4(const psift_match* const* s, double* H) {
   mdt *= inv_n;
   if (!isfinite(mdq) || !isfinite(mdt) || mdq < 1e-6 || mdt < 1e-6) return false;
   const double sq = 1.41421356237309504880 / mdq, st = 1.41421356237309504880 / mdt;
-  double ata[9][9];
-  for (int a = 0; a < 9; ++a)
-    for (int b = 0; b < 9; ++b) ata[a][b] = 0.0;
-  for (int i = 0; i < 4; ++i) {
-    const double x = ((double)s[i]->query_x - cxq) * sq, y = ((double)s[i]->query_y - cyq) * sq;
-    const double xp = ((double)s[i]->target_x - cxt) * st, yp = ((double)s[i]->target_y - cyt) * st;
-    const double r1[9] = {-x, -y, -1.0, 0.0, 0.0, 0.0, x * xp, y * xp, xp};
-    const double r2[9] = {0.0, 0.0, 0.0, -x, -y, -1.0, x * yp, y * yp, yp};
-    for (int a = 0; a < 9; ++a)
-      for (int b = a; b < 9; ++b) ata[a][b] += r1[a] * r1[b] + r2[a] * r2[b];
+  {
+    const float4 p = xy[idx[ql]];
+    dlt_row_values(((double)p.x - cxq) * sq, ((double)p.y - cyq) * sq, ((double)p.z - cxt) * st,
+                   ((double)p.w - cyt) * st, V + ql * kRowVals);
   }
-  for (int a = 0; a < 9; ++a)
-    for (int b = 0; b < a; ++b) ata[a][b] = ata[b][a];
-  return finish_dlt(ata, sq, st, cxq, cyq, cxt, cyt, H);
+  __syncwarp(qmask);
+  for (int e = ql; e < 45; e += 4) {
+    int a, b;
+    upper_entry(e, a, b);
+    const int s1a = (int)(kSlot1 >> (4 * a)) & 15, s1b = (int)(kSlot1 >> (4 * b)) & 15;
+    const int s2a = (int)(kSlot2 >> (4 * a)) & 15, s2b = (int)(kSlot2 >> (4 * b)) & 15;
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double* r = V + i * kRowVals;
+      s += r[s1a] * r[s1b] + r[s2a] * r[s2b];
+    }
+    A[a * 9 + b] = s;
+    A[b * 9 + a] = s;
+  }
+  __syncwarp(qmask);  // rows read, A complete
+  const int mi = quad_cyclic_jacobi(A, V, ql, qmask);
+  if (mi < 0 || ql != 0) return mi >= 0;
+  double hv[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) hv[r] = V[r * 9 + mi];
+  denormalise(hv, sq, st, cxq, cyq, cxt, cyt, H);
+  return true;
 }
 
-// fit_homography_dlt_f64 over J.list[0..k) (k >= 4), whole CTA; result in S.dres[0..8], flag in S.flag.
-__device__ bool fit_dlt_list(const RansacJob& J, RShared& S, int k, double* H) {
+// fit_homography_dlt_f64 over J.list[0..k) (k >= 4), whole CTA; jac holds one
+// free A / V pair.  Result in H (every thread); false if the fit fails.
+__device__ bool fit_dlt_list(const RansacJob& J, RShared& S, double* jac, int k, double* H) {
   const double inv_n = 1.0 / (double)k;
   // Gather the inliers (list order) as doubles: P[j] = (q.x, q.y, t.x, t.y).  The
   // sums below stay sequential in list order (the reference's order); only the
   // loads change: contiguous, issued ahead of the dependent additions.
   double4* P = reinterpret_cast<double4*>(J.pts);
   for (int j = threadIdx.x; j < k; j += kRThreads) {
-    const psift_match& m = J.m[J.list[j]];
-    P[j] = make_double4((double)m.query_x, (double)m.query_y, (double)m.target_x, (double)m.target_y);
+    const float4 p = J.xy[J.list[j]];
+    P[j] = make_double4((double)p.x, (double)p.y, (double)p.z, (double)p.w);
   }
   __syncthreads();
   if (threadIdx.x < 4) {
@@ -845,34 +933,52 @@ __device__ bool fit_dlt_list(const RansacJob& J, RShared& S, int k, double* H) {
     P[j] = make_double4((p.x - cxq) * sq, (p.y - cyq) * sq, (p.z - cxt) * st, (p.w - cyt) * st);
   }
   __syncthreads();
-  // upper triangle of A^T A: entry (a, b), a <= b, one thread each, sequential over the list
-  if (threadIdx.x < 45) {
-    int a = 0, rem = threadIdx.x;
-    while (rem >= 9 - a) {
-      rem -= 9 - a;
-      ++a;
-    }
-    const int b = a + rem;
+  // upper triangle of A^T A: entry (a, b), a <= b, one thread each, sequential
+  // over the list; the points' row values staged through jac a chunk at a time
+  {
+    int a = 0, b = 0;
+    if (threadIdx.x < 45) upper_entry(threadIdx.x, a, b);
+    const int s1a = (int)(kSlot1 >> (4 * a)) & 15, s1b = (int)(kSlot1 >> (4 * b)) & 15;
+    const int s2a = (int)(kSlot2 >> (4 * a)) & 15, s2b = (int)(kSlot2 >> (4 * b)) & 15;
     double s = 0.0;
+    for (int c0 = 0; c0 < k; c0 += kRowChunk) {
+      const int cn = min(kRowChunk, k - c0);
+      for (int j = threadIdx.x; j < cn; j += kRThreads) {
+        const double4 p = P[c0 + j];
+        dlt_row_values(p.x, p.y, p.z, p.w, jac + j * kRowVals);
+      }
+      __syncthreads();
+      if (threadIdx.x < 45) {
 #pragma unroll 8
-    for (int j = 0; j < k; ++j) {
-      const double4 p = P[j];
-      const double x = p.x, y = p.y, xp = p.z, yp = p.w;
-      const double r1[9] = {-x, -y, -1.0, 0.0, 0.0, 0.0, x * xp, y * xp, xp};
-      const double r2[9] = {0.0, 0.0, 0.0, -x, -y, -1.0, x * yp, y * yp, yp};
-      s += r1[a] * r1[b] + r2[a] * r2[b];
+        for (int j = 0; j < cn; ++j) {
+          const double* r = jac + j * kRowVals;
+          s += r[s1a] * r[s1b] + r[s2a] * r[s2b];
+        }
+      }
+      __syncthreads();
     }
-    S.ata[a][b] = s;
+    if (threadIdx.x < 45) {
+      S.ata[a][b] = s;
+      S.ata[b][a] = s;
+    }
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double ata[9][9];
-    for (int a = 0; a < 9; ++a)
-      for (int b = 0; b < 9; ++b) ata[a][b] = a <= b ? S.ata[a][b] : S.ata[b][a];
-    double Hl[9];
-    const bool ok = finish_dlt(ata, sq, st, cxq, cyq, cxt, cyt, Hl);
-    S.flag = ok ? 1 : 0;
-    for (int i = 0; i < 9; ++i) S.dres[i] = Hl[i];
+  if (threadIdx.x < 4) {  // the eigen-decomposition by the first quad
+    const int ql = threadIdx.x;
+    double* A = jac;
+    double* V = jac + 81;
+    for (int e = ql; e < 81; e += 4) A[e] = S.ata[e / 9][e % 9];
+    __syncwarp(0xFu);
+    const int mi = quad_cyclic_jacobi(A, V, ql, 0xFu);
+    if (ql == 0) {
+      S.flag = mi >= 0 ? 1 : 0;
+      if (mi >= 0) {
+        double hv[9], Hl[9];
+        for (int r = 0; r < 9; ++r) hv[r] = V[r * 9 + mi];
+        denormalise(hv, sq, st, cxq, cyq, cxt, cyt, Hl);
+        for (int i = 0; i < 9; ++i) S.dres[i] = Hl[i];
+      }
+    }
   }
   __syncthreads();
   const bool ok = S.flag != 0;
@@ -896,32 +1002,45 @@ __device__ bool degenerate4(const double (&p)[4][2]) {
   return false;
 }
 
-// local_optimize_homography (src/pipeline.rs:2605-2631); updates H/count/err in place.
-__device__ void local_optimize(const RansacJob& J, RShared& S, double* H, int& count, double& err) {
+// local_optimize_homography (src/pipeline.rs:2605-2631); updates H / count /
+// err in place (err valid when err_known; computed only for a tie).
+__device__ void local_optimize(const RansacJob& J, RShared& S, double* jac, double* H, int& count, double& err,
+                               bool& err_known) {
   for (int round = 0; round < 2; ++round) {
     const int k = h_collect(J, S, H);
     if (k < 4) break;
     double R[9];
-    if (!fit_dlt_list(J, S, k, R)) break;
+    if (!fit_dlt_list(J, S, jac, k, R)) break;
     const int rc = h_count(J, S, R);
-    const double re = h_err(J, S, R);
-    if (rc > count || (rc == count && re < err)) {
-      for (int i = 0; i < 9; ++i) H[i] = R[i];
-      count = rc;
+    if (rc < count) break;
+    if (rc == count) {
+      if (!err_known) {
+        err = h_err(J, S, H);
+        err_known = true;
+      }
+      const double re = h_err(J, S, R);
+      if (!(re < err)) break;
       err = re;
     } else {
-      break;
+      err_known = false;
     }
+    for (int i = 0; i < 9; ++i) H[i] = R[i];
+    count = rc;
   }
 }
 
 __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __restrict__ jobs) {
   __shared__ RShared S;
+  extern __shared__ double jac[];
   const RansacJob& J = jobs[blockIdx.x];
   const int n = J.n;
   if (threadIdx.x == 0) S.n = n;
+  for (int i = threadIdx.x; i < n; i += kRThreads) {
+    J.mask[i] = 0;
+    const psift_match& m = J.m[i];
+    J.xy[i] = make_float4(m.query_x, m.query_y, m.target_x, m.target_y);
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += kRThreads) J.mask[i] = 0;
   similarity_ransac(J, S, J.sim_seed, J.thr);
   if (!J.homography) {
     const int k = S.sim_count;
@@ -935,74 +1054,63 @@ __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __re
   }
   // ---- homography (src/pipeline.rs:2663-2755)
   const double thresh = (double)fmaxf(J.thr, 0.5f);
-  if (threadIdx.x == 0) {
-    S.tsq_d = thresh * thresh;
-    S.has_bh = S.has_sim;
-    if (S.has_sim) {
-      const double a = S.sim_model[0], b = S.sim_model[1];
-      S.BH[0] = a;
-      S.BH[1] = -b;
-      S.BH[2] = S.sim_model[2];
-      S.BH[3] = b;
-      S.BH[4] = a;
-      S.BH[5] = S.sim_model[3];
-      S.BH[6] = 0.0;
-      S.BH[7] = 0.0;
-      S.BH[8] = 1.0;
-    }
-  }
+  if (threadIdx.x == 0) S.tsq_d = thresh * thresh;
   __syncthreads();
+  // The incumbent, held identically by every thread.
+  bool has_bh = S.has_sim != 0;
+  double BH[9];
+  {
+    const double a = S.sim_model[0], b = S.sim_model[1];
+    BH[0] = a, BH[1] = -b, BH[2] = S.sim_model[2];
+    BH[3] = b, BH[4] = a, BH[5] = S.sim_model[3];
+    BH[6] = 0.0, BH[7] = 0.0, BH[8] = 1.0;
+  }
   int best_count = 0;
   double best_err = __longlong_as_double(0x7ff0000000000000ll);
-  double BH[9];
-  for (int i = 0; i < 9; ++i) BH[i] = S.BH[i];
-  if (S.has_bh) {
+  bool err_known = true;
+  if (has_bh) {
     best_count = h_count(J, S, BH);
-    best_err = h_err(J, S, BH);
+    err_known = false;
   }
   auto finish_sim = [&]() {
     const int k = S.sim_count;
     for (int j = threadIdx.x; j < k; j += kRThreads) J.mask[J.list[j]] = 1;
     if (threadIdx.x == 0) {
       *J.count = k;
-      *J.has_model = S.has_bh;
-      for (int i = 0; i < 9; ++i) J.model[i] = S.has_bh ? (float)BH[i] : 0.0f;
+      *J.has_model = has_bh ? 1 : 0;
+      for (int i = 0; i < 9; ++i) J.model[i] = has_bh ? (float)BH[i] : 0.0f;
     }
   };
   if (n < 4) {
     finish_sim();
     return;
   }
-  // keep the similarity inliers for the no-model exit: they are in J.list only until
-  // the first collection below, so record the flag now
   build_cdf(J, S);
   const bool guided = J.weights != nullptr;
   const double wtot = guided ? weight_total(J, S) : 1.0;
-  {
-    const double mass = (guided && S.has_bh) ? h_mass(J, S, BH) : 0.0;
-    if (threadIdx.x == 0) {
-      S.max_iters = guided ? adaptive_iters_w(mass / wtot, 4, 64, 2000) : adaptive_iters(best_count, n, 4, 64, 2000);
-      S.stop = 0;
-      S.draw_ptr = 0;
-      S.draws_ready = 0;
-    }
+  int max_iters = guided ? adaptive_iters_w((has_bh ? h_mass(J, S, BH) : 0.0) / wtot, 4, 64, 2000)
+                         : adaptive_iters(best_count, n, 4, 64, 2000);
+  if (threadIdx.x == 0) {
+    S.draw_ptr = 0;
+    S.draws_ready = 0;
   }
   __syncthreads();
   const uint64_t seed = J.hom_seed;
+  const int draw_cap = 2000 * 16;  // at most 16 draws per iteration
   int iters_done = 0;
-  bool list_is_sim = true;
-  for (int base = 0; !S.stop && base < 2000; base += kBatch) {
-    if (base >= S.max_iters) break;
+  bool stop = false;
+  for (int base = 0; !stop && base < 2000; base += kBatch) {
+    if (base >= max_iters) break;
     // draws for this batch: at most 16 per iteration
     {
       const int need = S.draw_ptr + kDrawChunk;
-      for (int t0 = S.draws_ready; t0 < need && t0 < J.draw_cap; t0 += kRThreads) {
+      for (int t0 = S.draws_ready; t0 < need && t0 < draw_cap; t0 += kRThreads) {
         const int t = t0 + threadIdx.x;
-        if (t < need && t < J.draw_cap) S.draws_s[t % (2 * kDrawChunk)] = sample_at(J.cdf, n, seed, (uint64_t)t);
+        if (t < need && t < draw_cap) S.draws_s[t % (2 * kDrawChunk)] = sample_at(J.cdf, n, seed, (uint64_t)t);
       }
       __syncthreads();
       if (threadIdx.x == 0) {
-        S.draws_ready = need < J.draw_cap ? need : J.draw_cap;
+        S.draws_ready = need < draw_cap ? need : draw_cap;
         int p = S.draw_ptr;
         for (int h = 0; h < kBatch; ++h) {
           int chosen = 0, attempts = 0;
@@ -1024,76 +1132,77 @@ __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __re
       }
       __syncthreads();
     }
-    if (threadIdx.x < kBatch) {
-      const int h = threadIdx.x;
-      int valid = S.hvalid[h];
+    // fits: a quad of lanes per hypothesis
+    {
+      const int h = threadIdx.x >> 2, ql = threadIdx.x & 3;
+      const unsigned qmask = 0xFu << (threadIdx.x & 28);
+      bool valid = S.hvalid[h] != 0;
       if (valid) {
-        const psift_match* quad[4] = {&J.m[S.quad[h][0]], &J.m[S.quad[h][1]], &J.m[S.quad[h][2]], &J.m[S.quad[h][3]]};
         double qp[4][2], tp[4][2];
         for (int i = 0; i < 4; ++i) {
-          qp[i][0] = quad[i]->query_x;
-          qp[i][1] = quad[i]->query_y;
-          tp[i][0] = quad[i]->target_x;
-          tp[i][1] = quad[i]->target_y;
+          const float4 p = J.xy[S.quad[h][i]];
+          qp[i][0] = p.x;
+          qp[i][1] = p.y;
+          tp[i][0] = p.z;
+          tp[i][1] = p.w;
         }
         if (degenerate4(qp) || degenerate4(tp)) {
-          valid = 0;
+          valid = false;
         } else {
           double Hh[9];
-          if (fit_dlt4(quad, Hh)) {
+          valid = quad_fit4(J.xy, S.quad[h], jac + h * 162, jac + h * 162 + 81, ql, qmask, Hh);
+          if (valid && ql == 0)
             for (int i = 0; i < 9; ++i) S.H[h][i] = Hh[i];
-          } else {
-            valid = 0;
-          }
         }
       }
-      S.hvalid[h] = valid;
-      S.hcnt[h] = 0;
+      __syncwarp();  // every lane of the quad has read S.hvalid[h]
+      if (ql == 0) S.hvalid[h] = valid ? 1 : 0;
     }
     __syncthreads();
-    for (int h = 0; h < kBatch; ++h) {
-      if (!S.hvalid[h]) continue;
-      const int c = h_count(J, S, S.H[h]);
-      if (threadIdx.x == 0) S.hcnt[h] = c;
-    }
-    __syncthreads();
+    h_count_batch(J, S, kBatch);
+    // replay in order
     for (int h = 0; h < kBatch; ++h) {
       const int it = base + h;
-      if (it >= S.max_iters) {
-        if (threadIdx.x == 0) S.stop = 1;
-        __syncthreads();
+      if (it >= max_iters) {
+        stop = true;
         break;
       }
       iters_done = it + 1;
       if (!S.hvalid[h]) continue;
       int c = S.hcnt[h];
       if (c < best_count) continue;
-      double e = h_err(J, S, S.H[h]);
-      if (c > best_count || e < best_err) {
-        double Hc[9];
-        for (int i = 0; i < 9; ++i) Hc[i] = S.H[h][i];
-        local_optimize(J, S, Hc, c, e);
-        list_is_sim = false;
-        best_count = c;
-        best_err = e;
-        for (int i = 0; i < 9; ++i) BH[i] = Hc[i];
-        const double mass = guided ? h_mass(J, S, BH) : 0.0;
-        if (threadIdx.x == 0) {
-          S.has_bh = 1;
-          S.max_iters = guided ? adaptive_iters_w(mass / wtot, 4, 64, 2000) : adaptive_iters(best_count, n, 4, 64, 2000);
+      double e = 0.0;
+      bool e_known = false;
+      if (c == best_count) {
+        if (!err_known) {
+          best_err = h_err(J, S, BH);
+          err_known = true;
         }
+        e = h_err(J, S, S.H[h]);
+        e_known = true;
+        if (!(e < best_err)) continue;
       }
-      __syncthreads();
+      double Hc[9];
+      for (int i = 0; i < 9; ++i) Hc[i] = S.H[h][i];
+      local_optimize(J, S, jac, Hc, c, e, e_known);
+      best_count = c;
+      best_err = e;
+      err_known = e_known;
+      for (int i = 0; i < 9; ++i) BH[i] = Hc[i];
+      has_bh = true;
+      max_iters = guided ? adaptive_iters_w(h_mass(J, S, BH) / wtot, 4, 64, 2000)
+                         : adaptive_iters(best_count, n, 4, 64, 2000);
     }
     __syncthreads();
   }
   if (threadIdx.x == 0 && J.iters) J.iters[1] = iters_done;
-  if (!S.has_bh) {
-    // no model at all: the similarity inliers (still in J.list when no LO ran)
-    if (list_is_sim) finish_sim();
+  if (!has_bh) {
+    // no model at all: no hypothesis was accepted, so no LO ran and J.list still
+    // holds the similarity inliers
+    finish_sim();
     return;
   }
-  local_optimize(J, S, BH, best_count, best_err);
+  local_optimize(J, S, jac, BH, best_count, best_err, err_known);
   const int k = h_collect(J, S, BH);
   for (int j = threadIdx.x; j < k; j += kRThreads) J.mask[J.list[j]] = 1;
   if (threadIdx.x == 0) {
@@ -1105,10 +1214,10 @@ __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __re
 
 cudaError_t launch_ransac(const RansacJob* jobs, int n_jobs, cudaStream_t st) {
   if (n_jobs <= 0) return cudaSuccess;
-  ransac_kernel<<<n_jobs, kRThreads, 0, st>>>(jobs);
+  cudaError_t e = ensure_smem_attr((const void*)ransac_kernel, kJacSmem);
+  if (e != cudaSuccess) return e;
+  ransac_kernel<<<n_jobs, kRThreads, kJacSmem, st>>>(jobs);
   return cudaGetLastError();
 }
-
-size_t ransac_job_bytes() { return sizeof(RansacJob); }
 
 }  // namespace psift

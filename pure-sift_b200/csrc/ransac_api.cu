@@ -9,35 +9,15 @@
 #include <vector>
 
 #include "psift_internal.cuh"
+#include "ransac_common.cuh"
 
 namespace psift {
 
-struct RansacJob {
-  const psift_match* m;
-  int n;
-  float thr;
-  uint64_t sim_seed, hom_seed;
-  int homography;
-  const float* weights;
-  double* cdf;
-  double* err;
-  int* list;
-  int* draws;
-  int draw_cap;
-  uint8_t* mask;
-  float* model;
-  int* has_model;
-  int* count;
-  int* iters;
-  double* pts;  // 4 per match: the current inlier list's coordinates, gathered
-};
 cudaError_t launch_ransac(const RansacJob* jobs, int n_jobs, cudaStream_t st);
-size_t ransac_job_bytes();
 
 namespace {
 constexpr uint64_t kSimSeed = 0xD1B54A32D192ED03ull;   // DEFAULT_SIMILARITY_RANSAC_SEED, src/pipeline.rs:172
 constexpr uint64_t kHomSeed = 0x517CC1B727220A95ull;   // DEFAULT_HOMOGRAPHY_RANSAC_SEED, src/pipeline.rs:174
-constexpr int kDrawCap = 2000 * 16;
 
 void seeds_for(const psift_ransac_options& o, bool homography, uint64_t& s1, uint64_t& s2) {
   if (!o.has_seed) {
@@ -51,11 +31,10 @@ void seeds_for(const psift_ransac_options& o, bool homography, uint64_t& s1, uin
 
 psift_status run_batch(psift_ctx* ctx, const psift_ransac_job* jobs, int n, const psift_ransac_options& opt,
                        bool homography) {
-  if (ransac_job_bytes() != sizeof(RansacJob)) return set_error(ctx, PSIFT_ERR_INTERNAL, "RansacJob layout mismatch");
   size_t bytes = sizeof(RansacJob) * n + 4096;
   for (int i = 0; i < n; ++i) {
     const size_t m = jobs[i].n;
-    bytes += 8 * m + 8 * m + 4 * m + 32 * m + 4 * (size_t)kDrawCap + 5 * 256 + 4096;
+    bytes += 8 * m + 8 * m + 4 * m + 16 * m + 32 * m + 6 * 256;
   }
   psift_status st = arena_reserve(ctx, bytes);
   if (st != PSIFT_OK) return st;
@@ -78,15 +57,14 @@ psift_status run_batch(psift_ctx* ctx, const psift_ransac_job* jobs, int n, cons
     R.cdf = (double*)arena_alloc(ctx, 8 * m + 8);
     R.err = (double*)arena_alloc(ctx, 8 * m + 8);
     R.list = (int*)arena_alloc(ctx, 4 * m + 4);
+    R.xy = (float4*)arena_alloc(ctx, 16 * m + 16);
     R.pts = (double*)arena_alloc(ctx, 32 * m + 32);
-    R.draws = (int*)arena_alloc(ctx, 4 * (size_t)kDrawCap);
-    R.draw_cap = kDrawCap;
     R.mask = J.inlier_mask;
     R.model = J.model;
     R.has_model = J.has_model;
     R.count = (int*)J.inlier_count;
     R.iters = (int*)J.iterations;
-    if (!R.draws) return set_error(ctx, PSIFT_ERR_INTERNAL, "ransac workspace carve overflow");
+    if (!R.pts) return set_error(ctx, PSIFT_ERR_INTERNAL, "ransac workspace carve overflow");
   }
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_jobs, hj.data(), sizeof(RansacJob) * n, cudaMemcpyHostToDevice, ctx->stream));
   StageScope sc(ctx, STAGE_RANSAC);

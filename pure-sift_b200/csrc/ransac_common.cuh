@@ -8,7 +8,32 @@
 #pragma once
 #include <stdint.h>
 
+#include "psift_gpu.h"
+
 namespace psift {
+
+// One match set of the homography / similarity kernel (ransac.cu), filled by the
+// host entry points (ransac_api.cu).
+struct RansacJob {
+  const psift_match* m;
+  int n;
+  float thr;
+  uint64_t sim_seed, hom_seed;
+  int homography;           // 0: similarity only, 1: homography (similarity seed first)
+  const float* weights;     // optional sampling weights replacing 1/clamp(ratio) (guided sampling)
+  // scratch (n entries each)
+  double* cdf;
+  double* err;
+  int* list;
+  float4* xy;               // (query x, query y, target x, target y) per match
+  double* pts;              // 4 per match: the current inlier list's coordinates, gathered
+  // outputs
+  uint8_t* mask;
+  float* model;             // similarity: a, b, tx, ty, scale, rotation_deg; homography: 9 (row-major)
+  int* has_model;
+  int* count;
+  int* iters;               // [0] similarity iterations, [1] homography iterations
+};
 
 __device__ __forceinline__ uint64_t sm64_draw(uint64_t seed, uint64_t t) {
   uint64_t z = seed + (t + 1ull) * 0x9E3779B97F4A7C15ull;
