@@ -134,6 +134,17 @@ psift_status psift_ctx_autotune(psift_ctx* ctx, uint32_t height, uint32_t width,
                                 const psift_sift_config* cfg, uint32_t n_desc, uint32_t n_pairs, double* report,
                                 uint32_t report_capacity, uint32_t* report_count);
 psift_status psift_ctx_tuning_get(const psift_ctx* ctx, int32_t what, int32_t index, int32_t* value);
+/* Blur rounding of the detection entries on this context.  No counterpart in
+ * the reference.  PSIFT_BLUR_REFERENCE (default): every tap a rounded multiply
+ * and a rounded add, bit-equal to gaussian_blur (src/pipeline.rs:314-425).
+ * PSIFT_BLUR_FUSED: every tap one fused multiply-add (one rounding), which halves
+ * the blur's arithmetic; results are no longer bit-equal to the reference's, and
+ * their error against an f64 run of the pipeline is held to the f32 path's
+ * tolerances (keypoints within 0.01 px and 0.01 scale, descriptors within 1e-4
+ * relative L2).  psift_gaussian_blur always uses the reference's rounding. */
+#define PSIFT_BLUR_REFERENCE 0
+#define PSIFT_BLUR_FUSED 1
+psift_status psift_ctx_set_blur_rounding(psift_ctx* ctx, int32_t mode);
 psift_status psift_ctx_tuning_set(psift_ctx* ctx, int32_t what, int32_t index, int32_t value);
 psift_status psift_ctx_stage_times(psift_ctx* ctx, double* ms, uint64_t* counts, uint32_t n, int reset);
 

@@ -24,7 +24,8 @@ namespace psift {
 
 // Declared in pyramid.cu / extrema.cu / describe.cu.
 cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
-                        int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant = 0);
+                        int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant = 0,
+                        bool fused = false);
 cudaError_t launch_extrema_mark(const ImagePlan* plans, int n, int octave, int max_h, const ExtremaParams& prm,
                                 cudaStream_t st);
 cudaError_t launch_row_scan(const ImagePlan* plans, int n, uint32_t kp_cap, uint32_t* err, cudaStream_t st);
@@ -134,6 +135,7 @@ struct DetectJob {
   ImagePlan* d_plans = nullptr;
   uint32_t kp_cap = 0, sel_cap = 0;
   int8_t blur_variant[16] = {0};     // level-blur variant per radius (the context's tuning)
+  bool blur_fused = false;           // single-rounding blur mode (the context's setting)
 };
 
 struct ImageDesc {
@@ -158,6 +160,7 @@ psift_status build_job(psift_ctx* ctx, const std::vector<ImageDesc>& imgs, const
   job.kp_cap = kDefaultKeypointCapacity;
   job.sel_cap = cfg.max_features ? cfg.max_features : job.kp_cap;
   std::memcpy(job.blur_variant, ctx->tune.blur, sizeof job.blur_variant);
+  job.blur_fused = ctx->blur_fused;
   job.oct.assign((size_t)n * kMaxOctaves, HostOctave{0, 0, 0});
   job.n_oct.assign(n, 0);
   size_t total = align_up(sizeof(ImagePlan) * n, 256) + align_up(extra_bytes, 256);
@@ -253,7 +256,7 @@ cudaError_t launch_level(const DetectJob& job, const SigmaSchedule& sc, int o, i
                          cudaStream_t st) {
   const int r = sc.level_radius[s];
   return launch_blur(0, sc.level_taps[s].data(), r, job.d_plans, job.n, o, s, S, mh, mw, st,
-                     r >= 0 && r < 16 ? job.blur_variant[r] : 0);
+                     r >= 0 && r < 16 ? job.blur_variant[r] : 0, job.blur_fused);
 }
 
 // Queue every stage of the path for the batch (no host synchronisation).
@@ -292,7 +295,8 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
     const bool up = cfg.upsample_first_octave != 0;
     const int kind = job.plans[0].src_kind;
     const int mode = kind == SRC_U8 ? (up ? 4 : 2) : (up ? 3 : 1);
-    cudaError_t e = launch_blur(mode, sc.init_taps.data(), sc.init_radius, job.d_plans, n, 0, 0, -1, mh, mw, st);
+    cudaError_t e = launch_blur(mode, sc.init_taps.data(), sc.init_radius, job.d_plans, n, 0, 0, -1, mh, mw, st, 0,
+                                job.blur_fused);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "blur(init)");
   }
@@ -382,7 +386,8 @@ psift_status launch_pyramid_only(psift_ctx* ctx, DetectJob& job, const psift_sif
     if (o == 0) {
       const bool up = cfg.upsample_first_octave != 0;
       const int mode = job.plans[0].src_kind == SRC_U8 ? (up ? 4 : 2) : (up ? 3 : 1);
-      cudaError_t e = launch_blur(mode, sc.init_taps.data(), sc.init_radius, job.d_plans, n, 0, 0, -1, mh, mw, st);
+      cudaError_t e = launch_blur(mode, sc.init_taps.data(), sc.init_radius, job.d_plans, n, 0, 0, -1, mh, mw, st, 0,
+                                job.blur_fused);
       ctx->launches++;
       if (e != cudaSuccess) return cuda_error(ctx, e, "blur(init)");
     }
@@ -725,6 +730,14 @@ psift_status psift_ctx_tuning_set(psift_ctx* ctx, int32_t what, int32_t index, i
   return PSIFT_OK;
 }
 
+psift_status psift_ctx_set_blur_rounding(psift_ctx* ctx, int32_t mode) {
+  if (!ctx) return PSIFT_ERR_INVALID_ARGUMENT;
+  if (mode != PSIFT_BLUR_REFERENCE && mode != PSIFT_BLUR_FUSED)
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "blur rounding must be PSIFT_BLUR_REFERENCE or PSIFT_BLUR_FUSED");
+  ctx->blur_fused = mode == PSIFT_BLUR_FUSED;
+  ctx->tune.gen++;  // captured graphs hold the other mode's kernels
+  return PSIFT_OK;
+}
 
 psift_status psift_detect_and_compute(psift_ctx* ctx, const float* image, uint32_t height, uint32_t width,
                                       size_t row_stride, const psift_sift_config* cfg, psift_features* out) {

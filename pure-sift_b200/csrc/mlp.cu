@@ -203,8 +203,202 @@ __global__ void mlp_loss_kernel(const float* __restrict__ l, int B, float* __res
   }
 }
 
-cudaError_t launch_mlp_infer(const float* params, const float* X, int n, float* prob, int num_sms, cudaStream_t st) {
+// ------------------------------------------------------------ tensor-core inference
+// mlp_infer_tc_kernel: the same network on bf16 tensor-core tiles
+// (mma.sync m16n8k16, f32 accumulation).  A warp evaluates 16 samples per tile:
+// layer 1 (K = 8 features, padded to 16) and layer 2 (K = 64) are MMAs whose f32
+// accumulators start at the biases; the layer-1 accumulator fragment, ReLU'd and
+// rounded to bf16, is exactly the layer-2 A fragment (rows g / g + 8, columns
+// 2t, 2t + 1 of consecutive 8-column tiles), so activations never leave the
+// registers; layer 3 is a per-row dot product reduced over the 4 lanes of a
+// quad.  The bf16-rounded weights live in registers for the whole kernel.
+// Operand rounding is the scalar kernel's (bf16, round to nearest even); only
+// the f32 summation order inside a product differs.
+//
+// Input staging: persistent CTAs (one per SM) take chunks of kMlpChunk samples
+// (32 KB) round-robin; thread 0 streams them into a kMlpStages-deep shared-memory
+// ring with 1-D bulk async copies (cp.async.bulk, mbarrier completion), so the
+// HBM reads run ahead of the tensor work.  Every wait is bounded: on timeout the
+// CTA records kErrTimeout in err and returns once its issued copies have landed.
+constexpr int kMlpThreads = 256;
+constexpr int kMlpWarps = kMlpThreads / 32;
+constexpr int kMlpChunk = 1024;  // samples per ring stage
+constexpr int kMlpStages = 4;
+constexpr uint32_t kMlpSpin = 1u << 24;
+constexpr size_t kMlpSmem = (size_t)kMlpStages * kMlpChunk * kF * sizeof(float) + 128;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// {lo, hi} -> bf16x2 (round to nearest even), lo in the low half.
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ bool mlp_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kMlpSpin; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kMlpThreads, 1) mlp_infer_tc_kernel(const float* __restrict__ params,
+                                                                      const float* __restrict__ X, int n,
+                                                                      float* __restrict__ prob, uint32_t* err) {
+  extern __shared__ __align__(128) uint8_t mlp_smem[];
+  float* xs = reinterpret_cast<float*>(mlp_smem);
+  uint64_t* full = reinterpret_cast<uint64_t*>(mlp_smem + (size_t)kMlpStages * kMlpChunk * kF * sizeof(float));
+  uint64_t* empty = full + kMlpStages;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int n_chunks = (n + kMlpChunk - 1) / kMlpChunk;
+  if ((int)blockIdx.x >= n_chunks) return;
+  const int my_chunks = (n_chunks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  auto chunk_samples = [&](int i) {
+    const int base = ((int)blockIdx.x + i * (int)gridDim.x) * kMlpChunk;
+    return min(kMlpChunk, n - base);
+  };
+  auto issue = [&](int i) {  // thread 0: chunk i of this CTA into stage i % kMlpStages
+    const int s = i % kMlpStages;
+    const long long base = ((long long)blockIdx.x + (long long)i * gridDim.x) * kMlpChunk;
+    const uint32_t bytes = (uint32_t)chunk_samples(i) * kF * sizeof(float);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(xs + (size_t)s * kMlpChunk * kF)),
+        "l"(X + base * kF), "r"(bytes), "r"(smem_addr(&full[s]))
+        : "memory");
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kMlpStages; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[s])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])), "r"(kMlpWarps) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    for (int i = 0; i < kMlpStages && i < my_chunks; ++i) issue(i);
+  }
+  // bf16 weight fragments (B operands: column n = output g of the 8-column tile,
+  // rows k = 2t, 2t + 1 and 2t + 8, 2t + 9 of the 16-deep K step) and biases for
+  // the accumulator columns 2t, 2t + 1 of each 8-column tile
+  uint32_t w1r[8], w2r[4][8][2];
+  float b1v[8][2], b2v[8][2], w3v[8][2];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    const int j = nt * 8 + g;
+    w1r[nt] = pack_bf16(params[kOffW1 + j * kF + 2 * t], params[kOffW1 + j * kF + 2 * t + 1]);
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const float* w = params + kOffW2 + j * kH + kk * 16 + 2 * t;
+      w2r[kk][nt][0] = pack_bf16(w[0], w[1]);
+      w2r[kk][nt][1] = pack_bf16(w[8], w[9]);
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      b1v[nt][c] = params[kOffB1 + nt * 8 + 2 * t + c];
+      b2v[nt][c] = params[kOffB2 + nt * 8 + 2 * t + c];
+      w3v[nt][c] = bf16r(params[kOffW3 + nt * 8 + 2 * t + c]);
+    }
+  }
+  const float b3 = params[kOffB3];
+  __syncthreads();  // barriers initialised
+  bool ok = true;
+  for (int i = 0; i < my_chunks; ++i) {
+    const int s = i % kMlpStages;
+    const uint32_t par = (uint32_t)(i / kMlpStages) & 1u;
+    if (!mlp_wait(&full[s], par)) {
+      ok = false;
+      break;
+    }
+    const float* xc = xs + (size_t)s * kMlpChunk * kF;
+    const int cnt = chunk_samples(i);
+    const long long base = ((long long)blockIdx.x + (long long)i * gridDim.x) * kMlpChunk;
+    for (int tile = warp; tile * 16 < cnt; tile += kMlpWarps) {
+      // layer 1: A = the tile's 16 x 8 features (K padded with zeros)
+      const float2 xa = *reinterpret_cast<const float2*>(xc + (tile * 16 + g) * kF + 2 * t);
+      const float2 xb = *reinterpret_cast<const float2*>(xc + (tile * 16 + g + 8) * kF + 2 * t);
+      const uint32_t a1[4] = {pack_bf16(xa.x, xa.y), pack_bf16(xb.x, xb.y), 0u, 0u};
+      uint32_t a2[4][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        float c[4] = {b1v[nt][0], b1v[nt][1], b1v[nt][0], b1v[nt][1]};
+        mma_bf16_16816(c, a1, w1r[nt], 0u);
+        // ReLU, bf16: this tile is K columns 8 (nt & 1) .. of layer 2's K step nt / 2
+        a2[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(fmaxf(c[0], 0.0f), fmaxf(c[1], 0.0f));
+        a2[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(fmaxf(c[2], 0.0f), fmaxf(c[3], 0.0f));
+      }
+      // layer 2 and the layer-3 dot products of rows g and g + 8
+      float z_lo = 0.0f, z_hi = 0.0f;
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        float c[4] = {b2v[nt][0], b2v[nt][1], b2v[nt][0], b2v[nt][1]};
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) mma_bf16_16816(c, a2[kk], w2r[kk][nt][0], w2r[kk][nt][1]);
+        z_lo = __fmaf_rn(w3v[nt][0], bf16r(fmaxf(c[0], 0.0f)), z_lo);
+        z_lo = __fmaf_rn(w3v[nt][1], bf16r(fmaxf(c[1], 0.0f)), z_lo);
+        z_hi = __fmaf_rn(w3v[nt][0], bf16r(fmaxf(c[2], 0.0f)), z_hi);
+        z_hi = __fmaf_rn(w3v[nt][1], bf16r(fmaxf(c[3], 0.0f)), z_hi);
+      }
+      z_lo += __shfl_xor_sync(0xffffffffu, z_lo, 1);
+      z_hi += __shfl_xor_sync(0xffffffffu, z_hi, 1);
+      z_lo += __shfl_xor_sync(0xffffffffu, z_lo, 2);
+      z_hi += __shfl_xor_sync(0xffffffffu, z_hi, 2);
+      if (t == 0) {
+        const int r0 = tile * 16 + g, r1 = r0 + 8;
+        if (r0 < cnt) prob[base + r0] = sigmoidf_(b3 + z_lo);
+        if (r1 < cnt) prob[base + r1] = sigmoidf_(b3 + z_hi);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
+    if (threadIdx.x == 0 && i + kMlpStages < my_chunks) {
+      // refill this stage once every warp is done with it
+      if (!mlp_wait(&empty[s], par)) {
+        ok = false;
+        break;
+      }
+      issue(i + kMlpStages);
+    }
+  }
+  if (!ok) {
+    atomicOr(err, kErrTimeout);
+    // wait (bounded) for this CTA's copies still in flight before the CTA exits
+    if (threadIdx.x == 0) {
+      const int issued = min(my_chunks, kMlpStages);
+      for (int i = 0; i < issued; ++i) mlp_wait(&full[i % kMlpStages], (uint32_t)(i / kMlpStages) & 1u);
+    }
+  }
+}
+
+cudaError_t launch_mlp_infer(const float* params, const float* X, int n, float* prob, int num_sms, uint32_t* err,
+                             cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
+  if ((reinterpret_cast<uintptr_t>(X) & 15u) == 0) {
+    // tensor-core path: the bulk copies need 16-byte aligned rows (32 B per sample)
+    cudaError_t e = ensure_smem_attr((const void*)mlp_infer_tc_kernel, kMlpSmem);
+    if (e != cudaSuccess) return e;
+    const int chunks = (n + kMlpChunk - 1) / kMlpChunk;
+    mlp_infer_tc_kernel<<<std::min(chunks, num_sms), kMlpThreads, kMlpSmem, st>>>(params, X, n, prob, err);
+    return cudaGetLastError();
+  }
   const int blocks = std::min((n + 255) / 256, num_sms * 8);
   mlp_infer_kernel<<<blocks, 256, 0, st>>>(params, X, n, prob);
   return cudaGetLastError();

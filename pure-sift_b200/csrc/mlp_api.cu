@@ -7,7 +7,8 @@
 
 namespace psift {
 
-cudaError_t launch_mlp_infer(const float* params, const float* X, int n, float* prob, int num_sms, cudaStream_t st);
+cudaError_t launch_mlp_infer(const float* params, const float* X, int n, float* prob, int num_sms, uint32_t* err,
+                             cudaStream_t st);
 size_t mlp_batch_floats(int B);
 cudaError_t launch_mlp_step(float* params, const float* X, const float* Y, const int* idx, int B, float* work,
                             float* grad, float* m, float* v, float lr, int t, float* loss_out, bool update,
@@ -74,7 +75,7 @@ psift_status psift_mlp_infer_dev(psift_ctx* ctx, const float* params, const floa
   if (n == 0) return PSIFT_OK;
   if (!params || !x || !prob) return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT, "null argument");
   StageScope sc(ctx, STAGE_MLP);
-  cudaError_t e = launch_mlp_infer(params, x, (int)n, prob, ctx->num_sms, ctx->stream);
+  cudaError_t e = launch_mlp_infer(params, x, (int)n, prob, ctx->num_sms, ctx->d_error, ctx->stream);
   ctx->launches++;
   if (e != cudaSuccess) return cuda_error(ctx, e, "mlp_infer");
   return PSIFT_OK;
@@ -140,10 +141,15 @@ psift_status psift_mlp_infer(psift_ctx* ctx, const float* params, const float* x
   float* dprob = dx + (size_t)n * kFeat;
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(dp, params, sizeof(float) * kNumParams, cudaMemcpyHostToDevice, ctx->stream));
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(dx, x, sizeof(float) * n * kFeat, cudaMemcpyHostToDevice, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream));
   st = psift_mlp_infer_dev(ctx, dp, dx, n, dprob);
   if (st != PSIFT_OK) return st;
+  if ((st = pinned_reserve(ctx, 64)) != PSIFT_OK) return st;
+  uint32_t* hword = (uint32_t*)ctx->pinned.base;
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(prob, dprob, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(hword, ctx->d_error, 4, cudaMemcpyDeviceToHost, ctx->stream));
   PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (*hword & kErrTimeout) return set_error(ctx, PSIFT_ERR_TIMEOUT, "mlp_infer: device wait timed out");
   return PSIFT_OK;
 }
 

@@ -89,6 +89,9 @@ struct psift_ctx {
     int8_t match_per_sm[2] = {2, 2};
     uint32_t gen = 0;
   } tune;
+  // Single-rounding blur mode (psift_ctx_set_blur_rounding); part of the graph
+  // cache key through tune.gen.
+  bool blur_fused = false;
   bool graphs_enabled = true;
   std::map<std::string, GraphEntry> graphs;
   std::map<std::string, int> graph_seen;

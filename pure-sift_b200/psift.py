@@ -218,6 +218,7 @@ _SIGS = {
                                      C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "psift_ctx_tuning_get": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "psift_ctx_tuning_set": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    "psift_ctx_set_blur_rounding": (C.c_int, [C.c_void_p, C.c_int32]),
     "psift_fundamental_options_default": (None, [C.POINTER(CFundamentalOptions)]),
     "psift_fundamental_estimate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CFundamentalOptions),
                                              C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
@@ -375,6 +376,14 @@ class Context:
 
     def set_tuning(self, what: int, index: int, value: int):
         self.check(self.lib.psift_ctx_tuning_set(self.handle, what, index, value))
+
+    BLUR_REFERENCE, BLUR_FUSED = 0, 1
+
+    def set_blur_rounding(self, mode: int):
+        """BLUR_REFERENCE (default): the reference's two roundings per blur tap,
+        bit-equal results.  BLUR_FUSED: one fused multiply-add per tap (faster; held
+        to the f32 path's tolerances against an f64 run, not bit-equal)."""
+        self.check(self.lib.psift_ctx_set_blur_rounding(self.handle, int(mode)))
 
     def stage_times(self, reset: bool = True) -> dict:
         """{stage: (total_ms, intervals)} accumulated since the last reset."""
