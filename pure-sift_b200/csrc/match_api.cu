@@ -23,16 +23,20 @@ cudaError_t launch_match_merge(const MatchPair* d_pairs, int n_pairs, int max_n,
                                const long long* part_off, const long long* cpart_off, bool mutual, cudaStream_t st);
 cudaError_t launch_match_emit(const MatchPair* d_pairs, int n_pairs, float ratio, bool mutual, cudaStream_t st);
 bool make_operand_map(CUtensorMap* tm, const void* base, long long rows, int box_rows);
+bool make_ext_map(CUtensorMap* tm, const void* base, long long rows, int box_rows);
 struct Bf16Job {
   const float* x;
   int n;
   uint16_t* out;
   float* norms;
   float* norm_max;
+  uint16_t* ext;
+  int n_pad;
 };
 cudaError_t launch_to_bf16(const void* jobs, int n_jobs, int max_rows, cudaStream_t st);
-cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcItem* items, int n_items,
-                            const TcPair* pairs, uint32_t* err, int mode, cudaStream_t st);
+cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const CUtensorMap& tmAx,
+                            const CUtensorMap& tmBx, const TcItem* items, int n_items, const TcPair* pairs,
+                            uint32_t* err, int mode, cudaStream_t st);
 cudaError_t launch_window(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 cudaError_t launch_gather_rows(const GatherJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
@@ -131,6 +135,7 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     bytes += (size_t)part_total * 12 + (size_t)cpart_total * 8 + 2 * sizeof(long long) * na + 1024;
   } else {
     bytes += (size_t)(q_rows + t_rows) * 256 + (size_t)(q_rows + t_rows) * 4 + 4096;
+    bytes += (size_t)(q_rows + t_rows) * 32 + (size_t)kTcBM * 32 + 3 * 256;  // GEMM norm extensions
     bytes += (size_t)(cand_f + cand_r) * (8 + 4 * kCollRows + 4) + (size_t)(q_rows + t_rows) * 4 +
              sizeof(TcItem) * (n_items_f + n_items_r) +
              sizeof(TcPair) * 2 * na + sizeof(RerankJob) * 2 * na + 8192 + (size_t)t_rows * 4 +
@@ -212,8 +217,13 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   TcPair* d_tcp = (TcPair*)arena_alloc(ctx, sizeof(TcPair) * 2 * na);
   RerankJob* d_rj = (RerankJob*)arena_alloc(ctx, sizeof(RerankJob) * 2 * na);
   int* flags = mutual ? (int*)arena_alloc(ctx, sizeof(int) * t_rows) : nullptr;  // matched-target marks
-  Bf16Job* d_bj = (Bf16Job*)arena_alloc(ctx, sizeof(Bf16Job) * 2 * na);
-  std::vector<Bf16Job> bj(2 * na);
+  Bf16Job* d_bj = (Bf16Job*)arena_alloc(ctx, sizeof(Bf16Job) * (2 * na + 1));
+  std::vector<Bf16Job> bj(2 * na + 1);
+  // GEMM norm extensions (16 bf16 per row): the rows' own [h, l, 0, ...] when
+  // they are the B operand, the constant [1, 1, 0, ...] tile for the A operand
+  uint16_t* qx = (uint16_t*)arena_alloc(ctx, (size_t)q_rows * 32);
+  uint16_t* tx = (uint16_t*)arena_alloc(ctx, (size_t)t_rows * 32);
+  uint16_t* ones = (uint16_t*)arena_alloc(ctx, (size_t)kTcBM * 32);
   // pass 2 runs over the rows window_kernel keeps, gathered into these operands
   uint16_t* qbc = (uint16_t*)arena_alloc(ctx, (size_t)q_rows * 256);
   uint16_t* tbc = (uint16_t*)arena_alloc(ctx, (size_t)t_rows * 256);
@@ -222,7 +232,7 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   GatherJob* d_gj = (GatherJob*)arena_alloc(ctx, sizeof(GatherJob) * 2 * na);
   std::vector<GatherJob> gj(2 * na);
   if (!qb || !tb || !thr || !coll_cnt || !d_rj || !d_bj || (mutual && !flags) || !qbc || !tbc || !rowmap ||
-      !ccount || !d_gj)
+      !ccount || !d_gj || !qx || !tx || !ones)
     return set_error(ctx, PSIFT_ERR_INTERNAL, "match workspace carve overflow");
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ccount, 0, sizeof(int) * 2 * na, st));
   if (mutual) PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * t_rows, st));
@@ -239,11 +249,12 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
       b += pad_rows(pairs[k].nt);
     }
   }
-  CUtensorMap tmQA, tmTB, tmTA, tmQB, tmQAc, tmTAc;
+  CUtensorMap tmQA, tmTB, tmTA, tmQB, tmQAc, tmTAc, tmOnes, tmTBx, tmQBx;
   if (!make_operand_map(&tmQA, qb, q_rows, kTcBM) || !make_operand_map(&tmTB, tb, t_rows, kTcBN) ||
-      !make_operand_map(&tmQAc, qbc, q_rows, kTcBM) ||
+      !make_operand_map(&tmQAc, qbc, q_rows, kTcBM) || !make_ext_map(&tmOnes, ones, kTcBM, kTcBM) ||
+      !make_ext_map(&tmTBx, tx, t_rows, kTcBN) ||
       (mutual && (!make_operand_map(&tmTA, tb, t_rows, kTcBM) || !make_operand_map(&tmQB, qb, q_rows, kTcBN) ||
-                  !make_operand_map(&tmTAc, tbc, t_rows, kTcBM))))
+                  !make_operand_map(&tmTAc, tbc, t_rows, kTcBM) || !make_ext_map(&tmQBx, qx, q_rows, kTcBN))))
     return set_error(ctx, PSIFT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   std::vector<TcItem> items;
   std::vector<TcPair> tcp(2 * na);
@@ -315,13 +326,17 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   int max_a = 0, max_b = 0;
   {
     for (int k = 0; k < na; ++k) {
-      bj[2 * k] = Bf16Job{pairs[k].q, pairs[k].nq, qb + (size_t)q0[k] * 128, qn + q0[k], maxes + na + k};
-      bj[2 * k + 1] = Bf16Job{pairs[k].t, pairs[k].nt, tb + (size_t)t0[k] * 128, tn + t0[k], maxes + k};
+      bj[2 * k] = Bf16Job{pairs[k].q, pairs[k].nq, qb + (size_t)q0[k] * 128, qn + q0[k], maxes + na + k,
+                          qx + (size_t)q0[k] * 16, (int)pad_rows(pairs[k].nq)};
+      bj[2 * k + 1] = Bf16Job{pairs[k].t, pairs[k].nt, tb + (size_t)t0[k] * 128, tn + t0[k], maxes + k,
+                              tx + (size_t)t0[k] * 16, (int)pad_rows(pairs[k].nt)};
       max_a = std::max(max_a, pairs[k].nq);
       max_b = std::max(max_b, pairs[k].nt);
     }
+    bj[2 * na] = Bf16Job{nullptr, 0, nullptr, nullptr, nullptr, ones, kTcBM};
     PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_bj, bj.data(), sizeof(Bf16Job) * bj.size(), cudaMemcpyHostToDevice, st));
-    cudaError_t e = launch_to_bf16(d_bj, 2 * na, std::max(max_a, max_b), st);
+    const int ext_rows = (int)std::max(pad_rows(std::max(max_a, max_b)), (long long)kTcBM);
+    cudaError_t e = launch_to_bf16(d_bj, 2 * na + 1, ext_rows, st);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "to_bf16");
   }
@@ -330,14 +345,15 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     const CUtensorMap& A = dir == 0 ? tmQA : tmTA;
     const CUtensorMap& Ac = dir == 0 ? tmQAc : tmTAc;
     const CUtensorMap& B = dir == 0 ? tmTB : tmQB;
+    const CUtensorMap& Bx = dir == 0 ? tmTBx : tmQBx;
     const TcItem* it0 = d_items + (dir == 0 ? 0 : n_f);
     const int n_it = dir == 0 ? n_f : (int)items.size() - n_f;
     const RerankJob* jobs_dir = d_rj + dir * na;
     const int rows = dir == 0 ? max_a : max_b;
-    cudaError_t e = launch_match_tc(A, B, it0, n_it, d_tcp, ctx->d_error, 0, st);
+    cudaError_t e = launch_match_tc(A, B, tmOnes, Bx, it0, n_it, d_tcp, ctx->d_error, 0, st);
     if (e == cudaSuccess) e = launch_window(jobs_dir, na, rows, st);
     if (e == cudaSuccess) e = launch_gather_rows(d_gj + dir * na, na, rows, st);
-    if (e == cudaSuccess) e = launch_match_tc(Ac, B, it0, n_it, d_tcp, ctx->d_error, 1, st);
+    if (e == cudaSuccess) e = launch_match_tc(Ac, B, tmOnes, Bx, it0, n_it, d_tcp, ctx->d_error, 1, st);
     if (e == cudaSuccess) e = launch_rerank(jobs_dir, na, rows, st);
     ctx->launches += 5;
     if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc / window / rerank");

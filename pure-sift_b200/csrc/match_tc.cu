@@ -3,28 +3,37 @@
 //
 // Reference: match_descriptors_with_options (src/pipeline.rs:1744-1841).
 //
-// Scheme.  a_ij = |q_i|^2 + |t_j|^2 - 2 <bf16(q_i), bf16(t_j)> (f32 accumulate in
-// TMEM) approximates the reference's f32 squared distance d_ij with
-//   |a_ij - d_ij| <= eps_i = 0.008 |q_i| max_j|t_j| + 5e-5 (|q_i|^2 + max_j|t_j|^2) + 1e-6
-// (bf16 rounding of both operands <= 2^-8 relative per product, tensor-core f32
-// accumulation, the f32 norms and the reference's own sequential f32 rounding, all
-// bounded with margin).  Every target that can be the exact best or second has
-// a_ij <= a_(2) + 2 eps_i.  Pass 1 of the GEMM keeps each row's two smallest a_ij;
-// window_kernel either certifies that the row fails the ratio test (then no exact
-// work is needed) or sets the row's window thr = a_(2) + 2 eps_i; pass 2 (same
-// GEMM, deterministic) collects every index with a_ij <= thr, and the exact
-// reference distances of those candidates give best/second/index equal to the
-// FP32 path bit for bit.  A row whose window holds more than kColl indices in
-// one split is matched by an exact scan of all targets.
+// Scheme.  The GEMM carries the target norms in one extra K step: the A
+// operand's extension is [1, 1, 0, ...] and the B operand's [h_j, l_j, 0, ...]
+// with h_j + l_j the bf16 hi/lo split of -|t_j|^2 / 2, so the accumulator is
+//   D_ij = <bf16(q_i), bf16(t_j)> + h_j + l_j  (f32 accumulation in TMEM)
+// and a_ij = |q_i|^2 - 2 D_ij (one f32 rounding) approximates the reference's
+// f32 squared distance d_ij with
+//   |a_ij - d_ij| <= eps_i = 0.008 |q_i| max_j|t_j| + 7e-5 (|q_i|^2 + max_j|t_j|^2) + 1e-6
+// (bf16 rounding of both operands <= 2^-8 relative per product, the hi/lo split
+// of the norm <= 2^-18 relative, tensor-core f32 accumulation, the f32 norms and
+// the reference's own sequential f32 rounding, all bounded with margin).  a_ij
+// is a non-increasing function of D_ij, so a row's two smallest a are the
+// images of its two largest D, and the epilogue works on D alone.  Every target
+// that can be the exact best or second has a_ij <= a_(2) + 2 eps_i.  Pass 1 of
+// the GEMM keeps each row's two largest D; window_kernel either certifies that
+// the row fails the ratio test (then no exact work is needed) or sets the row's
+// window thr = a_(2) + 2 eps_i; pass 2 (same GEMM, deterministic) collects every
+// index whose D is at least (|q_i|^2 - thr) / 2 less a margin that covers the
+// rounding of a (a superset of {a_ij <= thr}), and the exact reference distances
+// of those candidates give best/second/index equal to the FP32 path bit for bit.
+// A row whose window holds more than kColl indices in one split (or more than
+// kXColl in one column part) is matched by an exact scan of all targets.
 //
 // Kernel structure (one CTA = one 128-row A tile x a range of 256-row B tiles,
 // 576 threads): warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
-// operand tile, double-buffered B), warp 1 owns TMEM (512 columns = two 128x256
-// f32 accumulators) and issues tcgen05.mma (M=128, N=256, K=16) from one thread,
-// warps 2-17 read the accumulators with tcgen05.ld (four warps per TMEM lane quarter,
-// one per 64-column part of the tile; the parts are merged per row at the end).
-// All waits are bounded: on timeout the CTA records kErrTimeout, stops issuing,
-// drains what it issued and frees its TMEM.
+// operand tile plus the 16-column norm extension with SWIZZLE_32B,
+// double-buffered B), warp 1 owns TMEM (512 columns = two 128x256 f32
+// accumulators) and issues tcgen05.mma (M=128, N=256, K=16; nine per tile) from
+// one thread, warps 2-17 read the accumulators with tcgen05.ld (four warps per
+// TMEM lane quarter, one per 64-column part of the tile; the parts are merged per
+// row at the end).  All waits are bounded: on timeout the CTA records
+// kErrTimeout, stops issuing, drains what it issued and frees its TMEM.
 #include <cuda.h>
 
 #include "match_common.cuh"
@@ -39,7 +48,8 @@ static_assert(256 / kEpiParts == 64, "the epilogue folds four 16-column TMEM loa
 constexpr int kBM = 128;
 constexpr int kBN = 256;
 constexpr uint32_t kSpinLimit = 1u << 25;
-constexpr int kColl = 32;  // window indices kept per (split, row)
+constexpr int kColl = 32;   // window indices kept per (split, row)
+constexpr int kXColl = 16;  // window indices a column part 1..3 hands to part 0 (more: exact scan)
 
 // ---------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -93,6 +103,17 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 
+// K-major, 32-byte-swizzled 16-column extension tile: rows of 32 B, 8-row atoms 256 B apart.
+__device__ __forceinline__ uint64_t sw32_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);  // start address
+  d |= (uint64_t)1 << 16;                    // leading byte offset (unused: one swizzle atom wide)
+  d |= (uint64_t)(256u >> 4) << 32;          // stride byte offset: 8 rows x 32 B
+  d |= (uint64_t)1 << 46;                    // descriptor version (sm_100)
+  d |= (uint64_t)6 << 61;                    // SWIZZLE_32B
+  return d;
+}
+
 // kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=256.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
                             ((uint32_t)(kBM >> 4) << 24);
@@ -141,15 +162,19 @@ __device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
 
 // Smem map (offsets from a 1024-aligned base).
 constexpr uint32_t kSmA = 0;                      // 2 halves x 128 rows x 128 B = 32 KB
-constexpr uint32_t kSmB = 32768;                  // 2 stages x 2 halves x 256 rows x 128 B = 128 KB
-constexpr uint32_t kSmBar = kSmB + 2 * 65536;     // barriers
+constexpr uint32_t kSmAx = 32768;                 // A norm extension: 128 rows x 32 B
+constexpr uint32_t kSmB = 36864;                  // 2 stages of: 2 halves x 256 rows x 128 B, then 256 x 32 B
+constexpr uint32_t kSmBStage = 65536 + 8192;
+constexpr uint32_t kSmBar = kSmB + 2 * kSmBStage;  // barriers
 // epilogue exchange, per row and column part 1..kEpiParts-1: pass 1 the part's two
-// smallest values, pass 2 its count and up to kColl indices
+// largest values, pass 2 its count and up to kXColl indices
 constexpr uint32_t kSmX = kSmBar + 256;
-constexpr uint32_t kSmTotal = kSmX + (kEpiParts - 1) * kBM * (kColl + 2) * 4 + 1024;  // + alignment slack
+constexpr uint32_t kSmTotal = kSmX + (kEpiParts - 1) * kBM * (kXColl + 2) * 4 + 1024;  // + alignment slack
+static_assert(kSmTotal <= 227 * 1024, "shared memory per CTA");
 
 __global__ void __launch_bounds__(kTcThreads, 1)
     match_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    const __grid_constant__ CUtensorMap tmAx, const __grid_constant__ CUtensorMap tmBx,
                     const TcItem* __restrict__ items, const TcPair* __restrict__ pairs, uint32_t* err, int mode) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -203,17 +228,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const bool row_ok = it.a_local + row < n_rows;
   const int a_local = compact ? (row_ok ? PR.rowmap[it.a_local + row] : 0) : it.a_local + row;
   const float inf = __int_as_float(0x7f800000);
-  float v0 = inf, v1 = inf;  // mode 0: the two smallest values of the row
-  int cnt = 0;               // mode 1: indices with a <= thr (the row's window)
+  float u0 = -inf, u1 = -inf;  // mode 0: the two largest D of the row
+  int cnt = 0;                 // mode 1: indices with D >= the row's window bound
   // exchange slot of (part, row) for parts >= 1
-  int* xrow = reinterpret_cast<int*>(smem + kSmX) + ((part > 0 ? part - 1 : 0) * kBM + row) * (kColl + 2);
+  int* xrow = reinterpret_cast<int*>(smem + kSmX) + ((part > 0 ? part - 1 : 0) * kBM + row) * (kXColl + 2);
 
   if (warp == 0) {
     if (lane == 0) {
-      // A tile: two 64-column boxes of 128 rows
-      mbar_expect_tx(afull, 2u * kBM * 128u);
+      // A tile: two 64-column boxes of 128 rows and the constant norm extension
+      mbar_expect_tx(afull, 2u * kBM * 128u + kBM * 32u);
       tma_load_2d(&tmA, afull, smem + kSmA, 0, it.a_row);
       tma_load_2d(&tmA, afull, smem + kSmA + kBM * 128, 64, it.a_row);
+      tma_load_2d(&tmAx, afull, smem + kSmAx, 0, 0);
       for (int j = 0; j < nt; ++j) {
         const int s = j & 1;
         const uint32_t use = (uint32_t)(j >> 1);
@@ -222,10 +248,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           *abort_flag = 1;
           break;
         }
-        uint8_t* bst = smem + kSmB + s * 65536;
-        mbar_expect_tx(&full[s], 2u * kBN * 128u);
+        uint8_t* bst = smem + kSmB + s * kSmBStage;
+        mbar_expect_tx(&full[s], 2u * kBN * 128u + kBN * 32u);
         tma_load_2d(&tmB, &full[s], bst, 0, it.b_row + j * kBN);
         tma_load_2d(&tmB, &full[s], bst + kBN * 128, 64, it.b_row + j * kBN);
+        tma_load_2d(&tmBx, &full[s], bst + 2 * kBN * 128, 0, it.b_row + j * kBN);
       }
     }
   } else if (warp == 1) {
@@ -241,7 +268,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         tc_fence_after();
         const uint32_t a_base = smem_u32(smem + kSmA);
-        const uint32_t b_base = smem_u32(smem + kSmB + s * 65536);
+        const uint32_t b_base = smem_u32(smem + kSmB + s * kSmBStage);
         const uint32_t d = tmem + (uint32_t)(s * kBN);
 #pragma unroll
         for (int kk = 0; kk < 8; ++kk) {
@@ -249,6 +276,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           umma_bf16(d, sw128_desc(a_base + half * (kBM * 128) + koff), sw128_desc(b_base + half * (kBN * 128) + koff),
                     kk > 0 ? 1u : 0u);
         }
+        // the norm extension: D += h_j + l_j
+        umma_bf16(d, sw32_desc(smem_u32(smem + kSmAx)), sw32_desc(b_base + 2 * kBN * 128), 1u);
         umma_commit(&empty[s]);
         umma_commit(&accf[s]);
         ++issued;
@@ -270,9 +299,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // epilogue: TMEM lane quarter warp % 4, column part (warp - 2) / 4
     const float an = row_ok ? PR.an[a_local] : 0.0f;
     const float thr = (mode == 1 && row_ok) ? PR.thr[a_local] : -inf;
+    // pass 2 window in D: every D with |q|^2 - 2 D <= thr (one f32 rounding) has
+    // D >= (|q|^2 - thr) / 2 - 2^-24 (|q|^2 + |thr|); the margin below is larger
+    const float dthr = thr == -inf ? inf : 0.5f * (an - thr) - 1e-6f * (fabsf(an) + fabsf(thr));
     // part 0 collects into the row's list, the other parts into their exchange slots
     int* coll = part == 0 ? PR.coll_idx + ((long long)it.split * PR.na + (row_ok ? a_local : 0)) * kColl
                           : xrow + 2;
+    const int ccap = part == 0 ? kColl : kXColl;
     for (int j = 0; j < nt; ++j) {
       const int s = j & 1;
       const uint32_t use = (uint32_t)(j >> 1);
@@ -287,33 +320,27 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // This warp's 64 columns as four 16-column TMEM loads, double-buffered: the
       // next load is in flight while the current 16 values are folded in.
       const int cbase = col0 + part * (kBN / kEpiParts);
-      const float bnl0 = (cbase + lane < PR.nb) ? PR.bn[cbase + lane] : inf;
-      const float bnl1 = (cbase + 32 + lane < PR.nb) ? PR.bn[cbase + 32 + lane] : inf;
       const uint32_t tbase = taddr + (uint32_t)(part * (kBN / kEpiParts));
-      auto fold16 = [&](const uint32_t(&rr)[16], float bnl, int qoff, int cstart) {
+      auto fold16 = [&](const uint32_t(&rr)[16], int cstart) {
         if (mode == 0) {
 #pragma unroll
           for (int q = 0; q < 16; ++q) {
-            const float a = __fmaf_rn(-2.0f, __uint_as_float(rr[q]), an + __shfl_sync(0xffffffffu, bnl, qoff + q));
-            const float hi = fmaxf(v0, a);
-            v0 = fminf(v0, a);
-            v1 = fminf(v1, hi);
+            const float d = __uint_as_float(rr[q]);
+            const float lo = fminf(u0, d);
+            u0 = fmaxf(u0, d);
+            u1 = fmaxf(u1, lo);
           }
         } else {
           // the tests branch-free into a mask, then the (rare) hits in column order
           uint32_t hits = 0;
 #pragma unroll
-          for (int q = 0; q < 16; ++q) {
-            const float a = __fmaf_rn(-2.0f, __uint_as_float(rr[q]), an + __shfl_sync(0xffffffffu, bnl, qoff + q));
-            hits |= (a <= thr ? 1u : 0u) << q;
-          }
-          // a row past the kept ones reads stale operand rows (possibly inf: a = -inf
-          // passes even thr = -inf): it collects nothing
+          for (int q = 0; q < 16; ++q) hits |= (__uint_as_float(rr[q]) >= dthr ? 1u : 0u) << q;
+          // a row past the kept ones reads stale operand rows: it collects nothing
           if (!row_ok) hits = 0;
           while (hits) {
             const int q = __ffs(hits) - 1;
             hits &= hits - 1;
-            if (cnt < kColl) coll[cnt] = cstart + q;
+            if (cnt < ccap) coll[cnt] = cstart + q;
             ++cnt;
           }
         }
@@ -323,23 +350,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tmem_ld16(tbase, ra);
       tmem_wait16(ra);
       tmem_ld16(tbase + 16, rb);
-      fold16(ra, bnl0, 0, cbase);
+      fold16(ra, cbase);
       tmem_wait16(rb);
       tmem_ld16(tbase + 32, ra);
-      fold16(rb, bnl0, 16, cbase + 16);
+      fold16(rb, cbase + 16);
       tmem_wait16(ra);
       tmem_ld16(tbase + 48, rb);
-      fold16(ra, bnl1, 0, cbase + 32);
+      fold16(ra, cbase + 32);
       tmem_wait16(rb);
-      fold16(rb, bnl1, 16, cbase + 48);
+      fold16(rb, cbase + 48);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce[s]);
     }
     if (part > 0) {
       if (mode == 0) {
-        xrow[0] = __float_as_int(v0);
-        xrow[1] = __float_as_int(v1);
+        xrow[0] = __float_as_int(u0);
+        xrow[1] = __float_as_int(u1);
       } else {
         xrow[0] = cnt;
       }
@@ -347,30 +374,34 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   tc_fence_before();
   __syncthreads();
-  // Part 0 merges the other parts into its row, in part order: the two smallest
-  // values of all (pass 1), or the concatenated index lists with the summed count
-  // (pass 2; a count above kColl sends the row to the exact scan, as before).
+  // Part 0 merges the other parts into its row, in part order: the two largest D
+  // of all, mapped to the two smallest a = |q|^2 - 2 D (pass 1), or the
+  // concatenated index lists with the summed count (pass 2; a count above kColl,
+  // or a part that overflowed its kXColl slots, sends the row to the exact scan).
   if (warp >= 2 && part == 0 && row_ok) {
     const long long o = (long long)it.split * PR.na + a_local;
     int* coll0 = PR.coll_idx + o * kColl;
+    bool part_overflow = false;
     for (int p = 1; p < kEpiParts; ++p) {
-      const int* x = reinterpret_cast<const int*>(smem + kSmX) + ((p - 1) * kBM + row) * (kColl + 2);
+      const int* x = reinterpret_cast<const int*>(smem + kSmX) + ((p - 1) * kBM + row) * (kXColl + 2);
       if (mode == 0) {
         const float w0 = __int_as_float(x[0]), w1 = __int_as_float(x[1]);
-        const float m1 = fminf(fmaxf(v0, w0), fminf(v1, w1));
-        v0 = fminf(v0, w0);
-        v1 = m1;
+        const float m1 = fmaxf(fminf(u0, w0), fmaxf(u1, w1));
+        u0 = fmaxf(u0, w0);
+        u1 = m1;
       } else {
         const int c1 = x[0];
-        for (int k = 0; k < c1 && cnt + k < kColl; ++k) coll0[cnt + k] = x[2 + k];
+        part_overflow |= c1 > kXColl;
+        for (int k = 0; k < c1 && k < kXColl && cnt + k < kColl; ++k) coll0[cnt + k] = x[2 + k];
         cnt += c1;
       }
     }
     if (mode == 0) {
-      PR.top2[2 * o] = v0;
-      PR.top2[2 * o + 1] = v1;
+      const float an = PR.an[a_local];
+      PR.top2[2 * o] = __fmaf_rn(-2.0f, u0, an);
+      PR.top2[2 * o + 1] = __fmaf_rn(-2.0f, u1, an);
     } else {
-      PR.coll_cnt[o] = cnt;
+      PR.coll_cnt[o] = part_overflow ? max(cnt, kColl + 1) : cnt;
     }
   }
   if (warp == 1) {
@@ -381,14 +412,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
 // ------------------------------------------------------------ bf16 operands
 // One warp per row: bf16 copy (zero rows for padding are pre-cleared), exact f32
-// squared norm (sequential), running max of the norms.
+// squared norm (sequential), running max of the norms, and the row's GEMM norm
+// extension [h, l, 0, ...] with h = bf16(-|x|^2 / 2), l = bf16(-|x|^2 / 2 - h);
+// padding rows up to n_pad get [-inf, 0, ...], which no window or top-2 takes.
+// A job with x = null writes n_pad rows of the A operand's extension [1, 1, 0, ...].
 struct Bf16Job {
   const float* x;
   int n;
   uint16_t* out;
   float* norms;
   float* norm_max;
+  uint16_t* ext;  // n_pad rows x 16
+  int n_pad;
 };
+
+__device__ __forceinline__ uint16_t bf16_rne(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+}
 
 __global__ void to_bf16_kernel(const Bf16Job* __restrict__ jobs) {
   const Bf16Job& J = jobs[blockIdx.y];
@@ -396,17 +437,22 @@ __global__ void to_bf16_kernel(const Bf16Job* __restrict__ jobs) {
   uint16_t* __restrict__ out = J.out;
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (row >= J.n) return;
+  if (!x) {
+    // the A operand's constant extension rows [1, 1, 0, ...]
+    if (row < J.n_pad && lane < 4)
+      reinterpret_cast<uint2*>(J.ext + (size_t)row * 16)[lane] = make_uint2(lane == 0 ? 0x3F803F80u : 0u, 0u);
+    return;
+  }
+  if (row >= J.n) {
+    if (row < J.n_pad && lane < 4)
+      reinterpret_cast<uint2*>(J.ext + (size_t)row * 16)[lane] = make_uint2(lane == 0 ? 0xFF80u : 0u, 0u);
+    return;
+  }
   const float4 v = reinterpret_cast<const float4*>(x + (size_t)row * 128)[lane];
   const float e[4] = {v.x, v.y, v.z, v.w};
   unsigned short b[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    // round to nearest even
-    const uint32_t u = __float_as_uint(e[i]);
-    const uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
-    b[i] = (unsigned short)(r >> 16);
-  }
+  for (int i = 0; i < 4; ++i) b[i] = bf16_rne(e[i]);  // round to nearest even
   uint2 packed;
   packed.x = (uint32_t)b[0] | ((uint32_t)b[1] << 16);
   packed.y = (uint32_t)b[2] | ((uint32_t)b[3] << 16);
@@ -420,6 +466,16 @@ __global__ void to_bf16_kernel(const Bf16Job* __restrict__ jobs) {
   if (lane == 0) {
     J.norms[row] = s;
     atomicMax(reinterpret_cast<unsigned int*>(J.norm_max), __float_as_uint(s));
+  }
+  if (lane < 4) {
+    uint2 w = make_uint2(0u, 0u);
+    if (lane == 0) {
+      const float half = -0.5f * s;  // exact
+      const uint16_t hi = bf16_rne(half);
+      const uint16_t lo = bf16_rne(half - __uint_as_float((uint32_t)hi << 16));
+      w.x = (uint32_t)hi | ((uint32_t)lo << 16);
+    }
+    reinterpret_cast<uint2*>(J.ext + (size_t)row * 16)[lane] = w;
   }
 }
 
@@ -461,7 +517,7 @@ __global__ void window_kernel(const RerankJob* __restrict__ jobs) {
   }
   const float an = J.an[row];
   const float bmax = *J.bn_max;
-  const float eps = 0.008f * sqrtf(an) * sqrtf(bmax) + 5e-5f * (an + bmax) + 1e-6f;
+  const float eps = 0.008f * sqrtf(an) * sqrtf(bmax) + 7e-5f * (an + bmax) + 1e-6f;
   float thr = (forward ? v1 : v0) + 2.0f * eps;
   if (!forward && J.flags && J.flags[row] == 0) thr = -inf;
   if (forward && v1 < inf) {
@@ -568,6 +624,20 @@ bool make_operand_map(CUtensorMap* tm, const void* base, long long rows, int box
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2D bf16 tensor map over `rows` x 16 (the norm extension), box = 16 columns x
+// box_rows, 32B swizzle.
+bool make_ext_map(CUtensorMap* tm, const void* base, long long rows, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {16, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {32};
+  cuuint32_t box[2] = {16, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 cudaError_t launch_to_bf16(const void* jobs, int n_jobs, int max_rows, cudaStream_t st) {
   if (n_jobs <= 0 || max_rows <= 0) return cudaSuccess;
   dim3 grid((max_rows + 7) / 8, n_jobs);
@@ -575,11 +645,12 @@ cudaError_t launch_to_bf16(const void* jobs, int n_jobs, int max_rows, cudaStrea
   return cudaGetLastError();
 }
 
-cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcItem* items, int n_items,
-                            const TcPair* pairs, uint32_t* err, int mode, cudaStream_t st) {
+cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const CUtensorMap& tmAx,
+                            const CUtensorMap& tmBx, const TcItem* items, int n_items, const TcPair* pairs,
+                            uint32_t* err, int mode, cudaStream_t st) {
   cudaError_t e = ensure_smem_attr((const void*)match_tc_kernel, kSmTotal);
   if (e != cudaSuccess) return e;
-  match_tc_kernel<<<n_items, kTcThreads, kSmTotal, st>>>(tmA, tmB, items, pairs, err, mode);
+  match_tc_kernel<<<n_items, kTcThreads, kSmTotal, st>>>(tmA, tmB, tmAx, tmBx, items, pairs, err, mode);
   return cudaGetLastError();
 }
 
