@@ -130,6 +130,16 @@ def lib():
             L.oracle_sampson_distance_sq.argtypes = [C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double,
                                                      C.c_double]
             L.oracle_sampson_distance_sq.restype = C.c_double
+            L.oracle_warp_cylindrical.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_float, C.c_void_p]
+            L.oracle_panorama_register.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                                   C.POINTER(PanoramaOptions), _ip, C.c_void_p, _fp,
+                                                   C.c_void_p, C.c_void_p, C.c_void_p, _ip, _ip]
+            L.oracle_panorama_register.restype = C.c_int
+            L.oracle_panorama_composite.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, _fp,
+                                                    C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                    C.c_int, C.c_void_p]
+            L.oracle_solve_exposure_gains.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                                      C.c_double, _fp]
             L.oracle_splitmix64_next.argtypes = [_u64p]
             L.oracle_splitmix64_next.restype = C.c_uint64
             _lib = L
@@ -456,3 +466,93 @@ def fit_fundamental_7point(matches):
     out = np.zeros(36, np.float64)
     k = lib().oracle_fit_fundamental_7point(m.ctypes.data, out.ctypes.data_as(C.POINTER(C.c_double)))
     return [out[9 * i:9 * i + 9].reshape(3, 3).copy() for i in range(k)]
+
+
+# ---------------------------------------------------------------- stitch_panorama
+class PanoramaOptions(C.Structure):
+    """PanoramaOptions (src/stitch.rs:45-89); projection 0 planar / 1 cylindrical,
+    blend 0 feather / 1 multi-band."""
+    _fields_ = [("octaves", C.c_int), ("scales", C.c_int), ("threshold", C.c_float), ("ratio", C.c_float),
+                ("ransac_threshold", C.c_float), ("projection", C.c_int), ("focal_px", C.c_float),
+                ("blend", C.c_int), ("levels", C.c_int), ("exposure_compensation", C.c_int),
+                ("max_canvas_dim", C.c_int), ("max_canvas_pixels", C.c_longlong), ("tile_size", C.c_int)]
+
+    @classmethod
+    def default(cls, **kw):
+        o = cls(3, 3, 0.015, 0.75, 3.0, 0, 0.0, 1, 4, 1, 8192, 25_000_000, 512)
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+
+def warp_cylindrical(rgba, focal_px: float) -> np.ndarray:
+    """warp_image_cylindrical (src/stitch.rs:166-201) on an H x W x 4 u8 image."""
+    img = np.ascontiguousarray(rgba, dtype=np.uint8)
+    h, w = img.shape[:2]
+    out = np.zeros_like(img)
+    lib().oracle_warp_cylindrical(img.ctypes.data, h, w, w * 4, float(focal_px), out.ctypes.data)
+    return out
+
+
+def _img_ptrs(imgs):
+    imgs = [np.ascontiguousarray(im, dtype=np.uint8) for im in imgs]
+    ptrs = (C.c_void_p * len(imgs))(*[im.ctypes.data for im in imgs])
+    hs = np.array([im.shape[0] for im in imgs], np.int32)
+    ws = np.array([im.shape[1] for im in imgs], np.int32)
+    return imgs, ptrs, hs, ws
+
+
+def panorama_register(prepared, opt: PanoramaOptions):
+    """The registration half of stitch_panorama on prepared RGBA images: a dict with
+    ref, registered, gains, h_to_ref (n, 3, 3), inv (n, 3, 3), origin, width, height,
+    or an int error code (< 0)."""
+    imgs, ptrs, hs, ws = _img_ptrs(prepared)
+    n = len(imgs)
+    ref = C.c_int()
+    reg = np.zeros(n, np.uint8)
+    gains = np.zeros(n, np.float32)
+    H = np.zeros((n, 9), np.float64)
+    inv = np.zeros((n, 9), np.float64)
+    origin = np.zeros(2, np.float64)
+    w, h = C.c_int(), C.c_int()
+    rc = lib().oracle_panorama_register(ptrs, hs.ctypes.data, ws.ctypes.data, n, C.byref(opt), C.byref(ref),
+                                        reg.ctypes.data, _p(gains, _fp), H.ctypes.data, inv.ctypes.data,
+                                        origin.ctypes.data, C.byref(w), C.byref(h))
+    if rc != 0:
+        return rc
+    return {"ref": ref.value, "registered": reg.astype(bool), "gains": gains, "h_to_ref": H.reshape(n, 3, 3),
+            "inv": inv.reshape(n, 3, 3), "origin": origin, "width": w.value, "height": h.value}
+
+
+def panorama_composite(prepared, reg: dict, blend: int, levels: int = 4, tile_size: int = 512) -> np.ndarray:
+    """The blending half of stitch_panorama: the canvas (height, width, 4) u8."""
+    imgs, ptrs, hs, ws = _img_ptrs(prepared)
+    canvas = np.zeros((reg["height"], reg["width"], 4), np.uint8)
+    regm = np.ascontiguousarray(reg["registered"], dtype=np.uint8)
+    inv = np.ascontiguousarray(reg["inv"], dtype=np.float64)
+    lib().oracle_panorama_composite(ptrs, hs.ctypes.data, ws.ctypes.data, len(imgs), regm.ctypes.data,
+                                    _p(_f32(reg["gains"]), _fp), inv.ctypes.data,
+                                    np.ascontiguousarray(reg["origin"], dtype=np.float64).ctypes.data,
+                                    reg["width"], reg["height"], int(blend), int(levels), int(tile_size),
+                                    canvas.ctypes.data)
+    return canvas
+
+
+def stitch_panorama(images, opt: PanoramaOptions):
+    """stitch_panorama (src/stitch.rs:472-948) on H x W x 4 u8 images: (canvas, reg)
+    or an int error code."""
+    prepared = [np.ascontiguousarray(im, dtype=np.uint8) for im in images]
+    if opt.projection == 1:
+        prepared = [warp_cylindrical(im, opt.focal_px) for im in prepared]
+    reg = panorama_register(prepared, opt)
+    if isinstance(reg, int):
+        return reg
+    return panorama_composite(prepared, reg, opt.blend, opt.levels, opt.tile_size), reg
+
+
+def solve_exposure_gains(pairs, n_images: int, ref_idx: int, sigma_n=10.0, sigma_g=0.25) -> np.ndarray:
+    pr = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1, 5)
+    out = np.zeros(n_images, np.float32)
+    lib().oracle_solve_exposure_gains(pr.ctypes.data, pr.shape[0], n_images, ref_idx, sigma_n, sigma_g,
+                                      _p(out, _fp))
+    return out

@@ -16,6 +16,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <array>
+#include <deque>
+#include <map>
 #include <limits>
 #include <vector>
 
@@ -2338,6 +2341,613 @@ double oracle_sampson_distance_sq(const double* f9, double x1, double y1, double
   M3 f;
   for (int i = 0; i < 9; ++i) f.v[i / 3][i % 3] = f9[i];
   return f_sampson(f, x1, y1, x2, y2);
+}
+
+// ---------------------------------------------------------------- stitch_panorama
+// src/stitch.rs.  Helpers from src/visualize.rs: invert_matrix_3x3 (:202-233),
+// project_f64 (:236-247), sample_bilinear_rgba (:250-287, ow_sample above),
+// is_sane_homography_for_dims (:303-357), resolve_safe_alignment_homography
+// (:361-375).
+static bool pano_invert_f32(const float* m, double out[9]) {  // invert_matrix_3x3
+  double a[3][3];
+  for (int i = 0; i < 9; ++i) a[i / 3][i % 3] = (double)m[i];
+  const double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+  const double c01 = -(a[1][0] * a[2][2] - a[1][2] * a[2][0]);
+  const double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+  const double c10 = -(a[0][1] * a[2][2] - a[0][2] * a[2][1]);
+  const double c11 = a[0][0] * a[2][2] - a[0][2] * a[2][0];
+  const double c12 = -(a[0][0] * a[2][1] - a[0][1] * a[2][0]);
+  const double c20 = a[0][1] * a[1][2] - a[0][2] * a[1][1];
+  const double c21 = -(a[0][0] * a[1][2] - a[0][2] * a[1][0]);
+  const double c22 = a[0][0] * a[1][1] - a[0][1] * a[1][0];
+  const double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+  if (std::fabs(det) < 1e-12 || !std::isfinite(det)) return false;
+  const double id = 1.0 / det;
+  const double r[9] = {c00 * id, c10 * id, c20 * id, c01 * id, c11 * id, c21 * id, c02 * id, c12 * id, c22 * id};
+  for (int i = 0; i < 9; ++i) out[i] = r[i];
+  return true;
+}
+
+static bool pano_project(const double* m, double x, double y, double& px, double& py) {  // project_f64
+  const double w = m[6] * x + m[7] * y + m[8];
+  if (std::fabs(w) < 1e-7) return false;
+  const double iw = 1.0 / w;
+  px = (m[0] * x + m[1] * y + m[2]) * iw;
+  py = (m[3] * x + m[4] * y + m[5]) * iw;
+  return true;
+}
+
+static bool pano_sane(const float* m, int src_w, int src_h) {  // is_sane_homography_for_dims
+  if (src_w < 2 || src_h < 2) return false;
+  const double w = (double)(src_w - 1), ht = (double)(src_h - 1);
+  const double corners[4][2] = {{0.0, 0.0}, {w, 0.0}, {w, ht}, {0.0, ht}};
+  const double wc = (double)m[6] * (w * 0.5) + (double)m[7] * (ht * 0.5) + (double)m[8];
+  if (!std::isfinite(wc) || std::fabs(wc) < 1e-6) return false;
+  double P[4][2];
+  for (int i = 0; i < 4; ++i) {
+    const double cx = corners[i][0], cy = corners[i][1];
+    const double wi = (double)m[6] * cx + (double)m[7] * cy + (double)m[8];
+    if (!std::isfinite(wi) || wi * wc <= 0.0 || std::fabs(wi) < 0.1 * std::fabs(wc)) return false;
+    const double px = ((double)m[0] * cx + (double)m[1] * cy + (double)m[2]) / wi;
+    const double py = ((double)m[3] * cx + (double)m[4] * cy + (double)m[5]) / wi;
+    if (!std::isfinite(px) || !std::isfinite(py)) return false;
+    P[i][0] = px;
+    P[i][1] = py;
+  }
+  int pos = 0, neg = 0;
+  double shoelace = 0.0;
+  for (int i = 0; i < 4; ++i) {
+    const double* a = P[i];
+    const double* b = P[(i + 1) % 4];
+    const double* c = P[(i + 2) % 4];
+    shoelace += a[0] * b[1] - b[0] * a[1];
+    const double cross = (b[0] - a[0]) * (c[1] - b[1]) - (b[1] - a[1]) * (c[0] - b[0]);
+    if (cross > 1e-3) ++pos;
+    else if (cross < -1e-3) ++neg;
+    else return false;
+  }
+  if (!(pos == 4 || neg == 4)) return false;
+  const double area = 0.5 * std::fabs(shoelace), src_area = w * ht;
+  return area >= 0.04 * src_area && area <= 25.0 * src_area;
+}
+
+// sample_patch_intensity (src/stitch.rs:203-229) on the f32 luma plane.
+static double pano_patch(const std::vector<float>& g, int h, int w, float x, float y) {
+  if (h == 0 || w == 0 || !std::isfinite(x) || !std::isfinite(y)) return 0.0;
+  auto clampi = [](long long v, long long lo, long long hi) { return v < lo ? lo : (v > hi ? hi : v); };
+  const long long cx = clampi(f2i_sat(std::round(x)), 0, w - 1), cy = clampi(f2i_sat(std::round(y)), 0, h - 1);
+  const long long y0 = cy > 0 ? cy - 1 : 0, y1 = std::min(cy + 1, (long long)h - 1);
+  const long long x0 = cx > 0 ? cx - 1 : 0, x1 = std::min(cx + 1, (long long)w - 1);
+  double sum = 0.0;
+  long long cnt = 0;
+  for (long long yy = y0; yy <= y1; ++yy)
+    for (long long xx = x0; xx <= x1; ++xx) {
+      sum += (double)g[(size_t)yy * w + xx];
+      ++cnt;
+    }
+  return cnt == 0 ? 0.0 : (sum / (double)cnt) * 255.0;
+}
+
+// compose_mat3 (src/stitch.rs:115-132)
+static void pano_compose(const double* a, const double* b, double* out) {
+  double o[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) o[3 * r + c] = a[3 * r] * b[c] + a[3 * r + 1] * b[3 + c] + a[3 * r + 2] * b[6 + c];
+  if (std::fabs(o[8]) > 1e-12) {
+    const double inv = 1.0 / o[8];
+    for (int i = 0; i < 9; ++i) o[i] *= inv;
+  }
+  for (int i = 0; i < 9; ++i) out[i] = o[i];
+}
+
+void oracle_warp_cylindrical(const uint8_t* img, int h, int w, size_t stride, float focal_px, uint8_t* out) {
+  const double f = std::fmax(std::fmax((double)focal_px, (double)std::max(w, h) * 0.25), 16.0);
+  const double cx = ((double)w - 1.0) * 0.5, cy = ((double)h - 1.0) * 0.5;
+  std::memset(out, 0, (size_t)w * h * 4);
+  for (int y = 0; y < h; ++y) {
+    const double dy = (double)y - cy;
+    for (int x = 0; x < w; ++x) {
+      const double theta = ((double)x - cx) / f;
+      if (std::fabs(theta) >= 1.45) continue;
+      const double cos_t = std::cos(theta);
+      const double sx = f * std::tan(theta) + cx;
+      const double sy = dy / cos_t + cy;
+      double px[4], fw;
+      if (ow_sample(img, h, w, stride, sx, sy, px, &fw)) {
+        uint8_t* o = out + ((size_t)y * w + x) * 4;
+        for (int c = 0; c < 3; ++c) o[c] = ow_u8(std::round(px[c]));
+        o[3] = 255;
+      }
+    }
+  }
+}
+
+void oracle_solve_exposure_gains(const double* pairs, int n_pairs, int n, int ref_idx, double sigma_n,
+                                 double sigma_g, float* out) {
+  if (n == 0) return;
+  std::vector<std::vector<double>> a(n, std::vector<double>(n, 0.0));
+  std::vector<double> b(n, 0.0);
+  const double sn = std::fmax(sigma_n, 1e-3), sg = std::fmax(sigma_g, 1e-3);
+  const double inv_sn2 = 1.0 / (sn * sn), prior_w = 1.0 / (sg * sg);
+  for (int i = 0; i < n; ++i) {
+    a[i][i] += prior_w;
+    b[i] += prior_w;
+  }
+  for (int p = 0; p < n_pairs; ++p) {
+    const double* e = pairs + 5 * p;
+    const long long i = (long long)e[0], j = (long long)e[1];
+    const double nij = e[2], mi = e[3], mj = e[4];
+    if (i >= n || j >= n || i == j || nij <= 0.0) continue;
+    const double w = nij * inv_sn2;
+    a[i][i] += w * mi * mi;
+    a[j][j] += w * mj * mj;
+    const double cross = -w * mi * mj;
+    a[i][j] += cross;
+    a[j][i] += cross;
+  }
+  std::vector<double> g(n, 1.0);
+  for (int col = 0; col < n; ++col) {
+    int piv = col;
+    double mx = std::fabs(a[col][col]);
+    for (int r = col + 1; r < n; ++r)
+      if (std::fabs(a[r][col]) > mx) {
+        mx = std::fabs(a[r][col]);
+        piv = r;
+      }
+    if (mx < 1e-12) {
+      for (int i = 0; i < n; ++i) out[i] = 1.0f;
+      return;
+    }
+    std::swap(a[col], a[piv]);
+    std::swap(b[col], b[piv]);
+    const double diag = a[col][col];
+    for (int r = col + 1; r < n; ++r) {
+      const double factor = a[r][col] / diag;
+      a[r][col] = 0.0;
+      for (int c = col + 1; c < n; ++c) a[r][c] -= factor * a[col][c];
+      b[r] -= factor * b[col];
+    }
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int c = i + 1; c < n; ++c) s -= a[i][c] * g[c];
+    g[i] = s / a[i][i];
+  }
+  const double rg = ref_idx < n ? g[ref_idx] : 1.0;
+  const double norm = (std::isfinite(rg) && rg > 0.1) ? 1.0 / rg : 1.0;
+  for (int i = 0; i < n; ++i) {
+    const double sc = std::isfinite(g[i]) ? g[i] * norm : 1.0;
+    out[i] = clampf((float)sc, 0.4f, 2.5f);
+  }
+}
+
+namespace {
+struct PanoEdge {
+  int from, to;
+  double h[9];
+  int inliers;
+  double mean_from, mean_to;
+};
+}  // namespace
+
+int oracle_panorama_register(const uint8_t* const* imgs, const int* hs, const int* ws, int n,
+                             const oracle_panorama_options* opt, int* ref_index, uint8_t* registered, float* gains,
+                             double* h_to_ref, double* inv_out, double* origin, int* out_w, int* out_h) {
+  if (n < 2) return -1;
+  // gray planes and features (extract_sift_features: upsampling on, the 4096 cap)
+  std::vector<std::vector<float>> gray(n);
+  std::vector<std::vector<float>> meta(n), desc(n);
+  std::vector<int> nf(n);
+  for (int i = 0; i < n; ++i) {
+    const size_t np = (size_t)hs[i] * ws[i];
+    gray[i].resize(np);
+    for (size_t p = 0; p < np; ++p) {
+      const uint8_t* px = imgs[i] + 4 * p;
+      const uint32_t l = (2126u * px[0] + 7152u * px[1] + 722u * px[2]) / 10000u;
+      gray[i][p] = (float)l * (1.0f / 255.0f);
+    }
+    meta[i].resize(5 * 4096);
+    desc[i].resize(128 * 4096);
+    nf[i] = std::min(4096, oracle_detect_and_compute(gray[i].data(), hs[i], ws[i], opt->octaves, opt->scales,
+                                                     opt->threshold, 1, 0, 4096, meta[i].data(), desc[i].data(),
+                                                     4096));
+  }
+  std::vector<PanoEdge> edges;
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      std::vector<float> xi(2 * (size_t)nf[i]), xj(2 * (size_t)nf[j]);
+      for (int k = 0; k < nf[i]; ++k) xi[2 * k] = meta[i][5 * k], xi[2 * k + 1] = meta[i][5 * k + 1];
+      for (int k = 0; k < nf[j]; ++k) xj[2 * k] = meta[j][5 * k], xj[2 * k + 1] = meta[j][5 * k + 1];
+      std::vector<oracle_match> raw(std::max(nf[i], 1));
+      const int nr = oracle_match_descriptors(desc[i].data(), nf[i], desc[j].data(), nf[j], xi.data(), xj.data(),
+                                              opt->ratio, 0, raw.data(), (int)raw.size());
+      if (nr < 6) continue;
+      std::vector<uint8_t> sm(nr), hm(nr);
+      float sim[6], h9[9];
+      int has_s = 0, has_h = 0;
+      const int ns = oracle_similarity_ransac(raw.data(), nr, opt->ransac_threshold, 0xD1B54A32D192ED03ull,
+                                              sm.data(), sim, &has_s);
+      const int nh = oracle_homography_ransac(raw.data(), nr, opt->ransac_threshold, 0xD1B54A32D192ED03ull,
+                                              0x517CC1B727220A95ull, hm.data(), h9, &has_h);
+      const std::vector<uint8_t>& best = nh >= ns ? hm : sm;
+      const int nb = nh >= ns ? nh : ns;
+      if (nb < 6) continue;
+      float hij[9];
+      if (has_h && nh >= 6 && pano_sane(h9, ws[i], hs[i])) {
+        std::memcpy(hij, h9, sizeof hij);
+      } else if (has_s) {
+        const float r[9] = {sim[0], -sim[1], sim[2], sim[1], sim[0], sim[3], 0.0f, 0.0f, 1.0f};
+        std::memcpy(hij, r, sizeof hij);
+      } else {
+        continue;
+      }
+      double hji[9];
+      if (!pano_invert_f32(hij, hji)) continue;
+      double si = 0.0, sj = 0.0;
+      for (int k = 0; k < nr; ++k)
+        if (best[k]) {
+          si += pano_patch(gray[i], hs[i], ws[i], raw[k].qx, raw[k].qy);
+          sj += pano_patch(gray[j], hs[j], ws[j], raw[k].tx, raw[k].ty);
+        }
+      const double ic = 1.0 / (double)nb;
+      const double mi = std::fmax(si * ic, 1.0), mj = std::fmax(sj * ic, 1.0);
+      PanoEdge e1{i, j, {}, nb, mi, mj}, e2{j, i, {}, nb, mj, mi};
+      for (int k = 0; k < 9; ++k) e1.h[k] = (double)hij[k], e2.h[k] = hji[k];
+      edges.push_back(e1);
+      edges.push_back(e2);
+    }
+  if (edges.empty()) return -2;
+  std::vector<std::vector<PanoEdge>> adj(n);
+  for (const PanoEdge& e : edges) adj[e.from].push_back(e);
+  // largest connected component (first of the largest), BFS order
+  std::vector<char> visited(n, 0);
+  std::vector<int> best_comp;
+  for (int s0 = 0; s0 < n; ++s0) {
+    if (visited[s0] || adj[s0].empty()) continue;
+    std::vector<int> comp;
+    std::deque<int> q;
+    visited[s0] = 1;
+    q.push_back(s0);
+    while (!q.empty()) {
+      const int u = q.front();
+      q.pop_front();
+      comp.push_back(u);
+      for (const PanoEdge& e : adj[u])
+        if (!visited[e.to]) {
+          visited[e.to] = 1;
+          q.push_back(e.to);
+        }
+    }
+    if (comp.size() > best_comp.size()) best_comp = comp;
+  }
+  if (best_comp.size() < 2) return -3;
+  // reference: the largest (total inliers, index)
+  int ref = -1;
+  long long best_w = -1;
+  for (int u : best_comp) {
+    long long wsum = 0;
+    for (const PanoEdge& e : adj[u]) wsum += e.inliers;
+    if (wsum > best_w || (wsum == best_w && u > ref)) {
+      best_w = wsum;
+      ref = u;
+    }
+  }
+  // Prim's maximum spanning tree from the reference
+  std::vector<char> has(n, 0);
+  std::vector<double> H(9 * (size_t)n, 0.0);
+  has[ref] = 1;
+  const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  std::memcpy(&H[9 * (size_t)ref], I, sizeof I);
+  for (size_t it = 1; it < best_comp.size(); ++it) {
+    const PanoEdge* be = nullptr;
+    for (int u : best_comp) {
+      if (!has[u]) continue;
+      for (const PanoEdge& e : adj[u])
+        if (!has[e.to] && (!be || e.inliers > be->inliers)) be = &e;
+    }
+    if (!be) break;
+    const int parent = be->from, child = be->to;
+    const PanoEdge* rev = nullptr;
+    for (const PanoEdge& e : adj[child])
+      if (e.to == parent) {
+        rev = &e;
+        break;
+      }
+    pano_compose(&H[9 * (size_t)parent], rev->h, &H[9 * (size_t)child]);
+    has[child] = 1;
+  }
+  std::vector<int> reg;
+  for (int i = 0; i < n; ++i)
+    if (has[i]) reg.push_back(i);
+  // exposure gains over the registered component's edges
+  std::vector<float> g(n, 1.0f);
+  if (opt->exposure_compensation) {
+    std::map<std::pair<int, int>, std::array<double, 3>> seen;
+    for (int u : reg)
+      for (const PanoEdge& e : adj[u])
+        if (has[e.to]) {
+          const bool lt = e.from < e.to;
+          const std::pair<int, int> key = lt ? std::make_pair(e.from, e.to) : std::make_pair(e.to, e.from);
+          seen[key] = {(double)e.inliers, lt ? e.mean_from : e.mean_to, lt ? e.mean_to : e.mean_from};
+        }
+    std::vector<double> pairs;
+    for (const auto& kv : seen) {
+      pairs.push_back(kv.first.first);
+      pairs.push_back(kv.first.second);
+      pairs.push_back(kv.second[0]);
+      pairs.push_back(kv.second[1]);
+      pairs.push_back(kv.second[2]);
+    }
+    oracle_solve_exposure_gains(pairs.data(), (int)(pairs.size() / 5), n, ref, 10.0, 0.25, g.data());
+  }
+  // union bounding box in reference coordinates
+  double min_x = INFINITY, min_y = INFINITY, max_x = -INFINITY, max_y = -INFINITY;
+  std::vector<double> inv(9 * (size_t)n, 0.0);
+  for (int idx : reg) {
+    const double* hm = &H[9 * (size_t)idx];
+    float h2[9];
+    for (int k = 0; k < 9; ++k) h2[k] = (float)hm[k];
+    if (!pano_invert_f32(h2, &inv[9 * (size_t)idx])) return -4;
+    const double w = std::fmax((double)ws[idx] - 1.0, 0.0), hh = std::fmax((double)hs[idx] - 1.0, 0.0);
+    const double cs[4][2] = {{0.0, 0.0}, {w, 0.0}, {0.0, hh}, {w, hh}};
+    for (const auto& c : cs) {
+      double px, py;
+      if (!pano_project(hm, c[0], c[1], px, py)) return -5;
+      if (!std::isfinite(px) || !std::isfinite(py)) return -6;
+      min_x = std::fmin(min_x, px);
+      min_y = std::fmin(min_y, py);
+      max_x = std::fmax(max_x, px);
+      max_y = std::fmax(max_y, py);
+    }
+  }
+  const double ox = std::floor(min_x), oy = std::floor(min_y);
+  const double wf = std::fmax(std::ceil(max_x) - ox + 1.0, 1.0), hf = std::fmax(std::ceil(max_y) - oy + 1.0, 1.0);
+  if (wf > (double)opt->max_canvas_dim || hf > (double)opt->max_canvas_dim ||
+      wf * hf > (double)opt->max_canvas_pixels)
+    return -7;
+  *ref_index = ref;
+  for (int i = 0; i < n; ++i) {
+    registered[i] = has[i];
+    gains[i] = g[i];
+  }
+  std::memcpy(h_to_ref, H.data(), sizeof(double) * 9 * n);
+  std::memcpy(inv_out, inv.data(), sizeof(double) * 9 * n);
+  origin[0] = ox;
+  origin[1] = oy;
+  *out_w = (int)wf;
+  *out_h = (int)hf;
+  return 0;
+}
+
+namespace {
+using Rgb = std::array<float, 3>;
+const float kPyrK[5] = {1.0f / 16.0f, 4.0f / 16.0f, 6.0f / 16.0f, 4.0f / 16.0f, 1.0f / 16.0f};
+
+// downsample_half_rgba_weighted (src/stitch.rs:318-393)
+void pano_down_rgb(const std::vector<Rgb>& src, const std::vector<float>& mask, int w, int h, std::vector<Rgb>& dst,
+                   std::vector<float>& dmask, int& nw, int& nh) {
+  nw = std::max((w + 1) / 2, 1);
+  nh = std::max((h + 1) / 2, 1);
+  std::vector<Rgb> trgb((size_t)h * nw, Rgb{0, 0, 0});
+  std::vector<float> tm((size_t)h * nw, 0.0f);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < nw; ++x) {
+      Rgb acc{0, 0, 0};
+      float m = 0.0f, vw = 0.0f;
+      for (int k = 0; k < 5; ++k) {
+        const int sx = std::min(std::max(2 * x + k - 2, 0), w - 1);
+        const float mw = mask[(size_t)y * w + sx];
+        m += kPyrK[k] * mw;
+        if (mw > 0.0f) {
+          const float v = kPyrK[k] * mw;
+          vw += v;
+          for (int c = 0; c < 3; ++c) acc[c] += v * src[(size_t)y * w + sx][c];
+        }
+      }
+      tm[(size_t)y * nw + x] = m;
+      if (vw > 1e-6f) {
+        const float inv = 1.0f / vw;
+        trgb[(size_t)y * nw + x] = Rgb{acc[0] * inv, acc[1] * inv, acc[2] * inv};
+      }
+    }
+  dst.assign((size_t)nw * nh, Rgb{0, 0, 0});
+  dmask.assign((size_t)nw * nh, 0.0f);
+  for (int y = 0; y < nh; ++y)
+    for (int x = 0; x < nw; ++x) {
+      Rgb acc{0, 0, 0};
+      float m = 0.0f, vw = 0.0f;
+      for (int k = 0; k < 5; ++k) {
+        const int sy = std::min(std::max(2 * y + k - 2, 0), h - 1);
+        const size_t i = (size_t)sy * nw + x;
+        const float mw = tm[i];
+        m += kPyrK[k] * mw;
+        if (mw > 0.0f) {
+          const float v = kPyrK[k] * mw;
+          vw += v;
+          for (int c = 0; c < 3; ++c) acc[c] += v * trgb[i][c];
+        }
+      }
+      dmask[(size_t)y * nw + x] = m;
+      if (vw > 1e-6f) {
+        const float inv = 1.0f / vw;
+        dst[(size_t)y * nw + x] = Rgb{acc[0] * inv, acc[1] * inv, acc[2] * inv};
+      }
+    }
+}
+
+// downsample_half_scalar (src/stitch.rs:436-470)
+void pano_down_scalar(const std::vector<float>& src, int w, int h, std::vector<float>& dst) {
+  const int nw = std::max((w + 1) / 2, 1), nh = std::max((h + 1) / 2, 1);
+  std::vector<float> t((size_t)h * nw, 0.0f);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < nw; ++x) {
+      float acc = 0.0f;
+      for (int k = 0; k < 5; ++k) acc += kPyrK[k] * src[(size_t)y * w + std::min(std::max(2 * x + k - 2, 0), w - 1)];
+      t[(size_t)y * nw + x] = acc;
+    }
+  dst.assign((size_t)nw * nh, 0.0f);
+  for (int y = 0; y < nh; ++y)
+    for (int x = 0; x < nw; ++x) {
+      float acc = 0.0f;
+      for (int k = 0; k < 5; ++k) acc += kPyrK[k] * t[(size_t)std::min(std::max(2 * y + k - 2, 0), h - 1) * nw + x];
+      dst[(size_t)y * nw + x] = acc;
+    }
+}
+
+// upsample_to_size_rgb (src/stitch.rs:395-434)
+void pano_up_rgb(const std::vector<Rgb>& src, int sw, int sh, int dw, int dh, std::vector<Rgb>& out) {
+  out.assign((size_t)dw * dh, Rgb{0, 0, 0});
+  for (int y = 0; y < dh; ++y) {
+    const float fy = clampf((float)y * 0.5f, 0.0f, (float)(sh > 0 ? sh - 1 : 0));
+    const int y0 = std::min((int)std::floor(fy), sh - 1), y1 = std::min(y0 + 1, sh - 1);
+    const float wy1 = fy - (float)y0, wy0 = 1.0f - wy1;
+    for (int x = 0; x < dw; ++x) {
+      const float fx = clampf((float)x * 0.5f, 0.0f, (float)(sw > 0 ? sw - 1 : 0));
+      const int x0 = std::min((int)std::floor(fx), sw - 1), x1 = std::min(x0 + 1, sw - 1);
+      const float wx1 = fx - (float)x0, wx0 = 1.0f - wx1;
+      const Rgb& p00 = src[(size_t)y0 * sw + x0];
+      const Rgb& p10 = src[(size_t)y0 * sw + x1];
+      const Rgb& p01 = src[(size_t)y1 * sw + x0];
+      const Rgb& p11 = src[(size_t)y1 * sw + x1];
+      const float w00 = wx0 * wy0, w10 = wx1 * wy0, w01 = wx0 * wy1, w11 = wx1 * wy1;
+      for (int c = 0; c < 3; ++c) out[(size_t)y * dw + x][c] = p00[c] * w00 + p10[c] * w10 + p01[c] * w01 + p11[c] * w11;
+    }
+  }
+}
+}  // namespace
+
+void oracle_panorama_composite(const uint8_t* const* imgs, const int* hs, const int* ws, int n,
+                               const uint8_t* registered, const float* gains, const double* inv,
+                               const double* origin, int W, int Hh, int blend, int levels, int tile_size,
+                               uint8_t* canvas) {
+  (void)tile_size;  // the tiling does not change a pixel's value
+  std::memset(canvas, 0, (size_t)W * Hh * 4);
+  std::vector<int> reg;
+  for (int i = 0; i < n; ++i)
+    if (registered[i]) reg.push_back(i);
+  const double ox = origin[0], oy = origin[1];
+  if (blend == 0) {
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < Hh; ++y) {
+      const double ry = oy + (double)y;
+      for (int x = 0; x < W; ++x) {
+        const double rx = ox + (double)x;
+        double acc[3] = {0, 0, 0}, aw = 0.0;
+        for (int idx : reg) {
+          double sx, sy, px[4], fw;
+          if (!pano_project(inv + 9 * (size_t)idx, rx, ry, sx, sy)) continue;
+          if (!ow_sample(imgs[idx], hs[idx], ws[idx], (size_t)ws[idx] * 4, sx, sy, px, &fw)) continue;
+          const double g = (double)gains[idx], wt = std::fmax(fw, 1e-4);
+          for (int c = 0; c < 3; ++c) acc[c] += wt * clampt<double>(px[c] * g, 0.0, 255.0);
+          aw += wt;
+        }
+        if (aw > 0.0) {
+          const double iw = 1.0 / aw;
+          uint8_t* o = canvas + ((size_t)y * W + x) * 4;
+          for (int c = 0; c < 3; ++c) o[c] = ow_u8(std::round(acc[c] * iw));
+          o[3] = 255;
+        }
+      }
+    }
+    return;
+  }
+  const size_t np = (size_t)W * Hh;
+  const int k_reg = (int)reg.size();
+  std::vector<std::vector<Rgb>> warped(k_reg, std::vector<Rgb>(np, Rgb{0, 0, 0}));
+  std::vector<std::vector<float>> valid(k_reg, std::vector<float>(np, 0.0f));
+  std::vector<float> best_w(np, -1.0f);
+  std::vector<int> owner(np, -1);
+  for (int pos = 0; pos < k_reg; ++pos) {
+    const int idx = reg[pos];
+    const float gain = gains[idx];
+    for (int y = 0; y < Hh; ++y) {
+      const double ry = oy + (double)y;
+      for (int x = 0; x < W; ++x) {
+        const double rx = ox + (double)x;
+        double sx, sy, px[4], fw;
+        if (!pano_project(inv + 9 * (size_t)idx, rx, ry, sx, sy)) continue;
+        if (!ow_sample(imgs[idx], hs[idx], ws[idx], (size_t)ws[idx] * 4, sx, sy, px, &fw)) continue;
+        const size_t p = (size_t)y * W + x;
+        for (int c = 0; c < 3; ++c) warped[pos][p][c] = clampf((float)px[c] * gain, 0.0f, 255.0f);
+        valid[pos][p] = 1.0f;
+        const float f32 = (float)fw;
+        if (f32 > best_w[p]) {
+          best_w[p] = f32;
+          owner[p] = pos;
+        }
+      }
+    }
+  }
+  const int maxl = std::max((int)std::floor(std::log2((double)std::min(W, Hh))), 1);
+  const int nl = std::min(std::min(std::max(levels, 1), 6), maxl);
+  std::vector<std::pair<int, int>> dims;
+  std::vector<std::vector<Rgb>> bl;
+  std::vector<std::vector<float>> ms;
+  {
+    int cw = W, ch = Hh;
+    for (int l = 0; l < nl; ++l) {
+      dims.push_back({cw, ch});
+      bl.push_back(std::vector<Rgb>((size_t)cw * ch, Rgb{0, 0, 0}));
+      ms.push_back(std::vector<float>((size_t)cw * ch, 0.0f));
+      cw = std::max((cw + 1) / 2, 1);
+      ch = std::max((ch + 1) / 2, 1);
+    }
+  }
+  for (int pos = 0; pos < k_reg; ++pos) {
+    std::vector<std::vector<Rgb>> gi(nl);
+    std::vector<std::vector<float>> gv(nl), gm(nl);
+    gi[0].swap(warped[pos]);
+    gv[0].swap(valid[pos]);
+    gm[0].assign(np, 0.0f);
+    for (size_t p = 0; p < np; ++p) gm[0][p] = owner[p] == pos ? 1.0f : 0.0f;
+    for (int l = 1; l < nl; ++l) {
+      int nw, nh;
+      pano_down_rgb(gi[l - 1], gv[l - 1], dims[l - 1].first, dims[l - 1].second, gi[l], gv[l], nw, nh);
+      pano_down_scalar(gm[l - 1], dims[l - 1].first, dims[l - 1].second, gm[l]);
+    }
+    const int top = nl - 1;
+    for (size_t i = 0; i < gm[top].size(); ++i) {
+      const float w = gm[top][i];
+      if (w > 0.0f && gv[top][i] > 1e-3f) {
+        for (int c = 0; c < 3; ++c) bl[top][i][c] += w * gi[top][i][c];
+        ms[top][i] += w;
+      }
+    }
+    for (int l = 0; l < top; ++l) {
+      std::vector<Rgb> ex;
+      pano_up_rgb(gi[l + 1], dims[l + 1].first, dims[l + 1].second, dims[l].first, dims[l].second, ex);
+      const size_t cnt = (size_t)dims[l].first * dims[l].second;
+      for (size_t i = 0; i < cnt; ++i) {
+        const float w = gm[l][i];
+        if (w > 0.0f && gv[l][i] > 1e-3f) {
+          for (int c = 0; c < 3; ++c) bl[l][i][c] += w * (gi[l][i][c] - ex[i][c]);
+          ms[l][i] += w;
+        }
+      }
+    }
+  }
+  for (int l = 0; l < nl; ++l)
+    for (size_t i = 0; i < bl[l].size(); ++i) {
+      const float m = ms[l][i];
+      if (m > 1e-6f && std::fabs(m - 1.0f) > 1e-5f) {
+        const float iv = 1.0f / m;
+        for (int c = 0; c < 3; ++c) bl[l][i][c] *= iv;
+      }
+    }
+  std::vector<Rgb> recon = bl[nl - 1];
+  for (int l = nl - 2; l >= 0; --l) {
+    std::vector<Rgb> up;
+    pano_up_rgb(recon, dims[l + 1].first, dims[l + 1].second, dims[l].first, dims[l].second, up);
+    for (size_t i = 0; i < up.size(); ++i)
+      for (int c = 0; c < 3; ++c) up[i][c] = up[i][c] + bl[l][i][c];
+    recon.swap(up);
+  }
+  for (size_t p = 0; p < np; ++p)
+    if (owner[p] >= 0) {
+      uint8_t* o = canvas + p * 4;
+      for (int c = 0; c < 3; ++c) o[c] = ow_u8(std::round((double)recon[p][c]));
+      o[3] = 255;
+    }
 }
 
 }  // extern "C"

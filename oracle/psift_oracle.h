@@ -135,6 +135,43 @@ int oracle_warp_and_stitch(const uint8_t* q, int qh, int qw, size_t qs, const ui
                            size_t ts, const float* h9, uint8_t* canvas, int* out_w, int* out_h,
                            double* origin);
 
+/* stitch_panorama (src/stitch.rs:472-948) and its parts. */
+typedef struct {
+  int octaves, scales;
+  float threshold, ratio, ransac_threshold;
+  int projection;   /* 0 planar, 1 cylindrical */
+  float focal_px;
+  int blend;        /* 0 feather, 1 multi-band */
+  int levels;
+  int exposure_compensation;
+  int max_canvas_dim;
+  long long max_canvas_pixels;
+  int tile_size;
+} oracle_panorama_options;
+
+/* warp_image_cylindrical (:166-201): RGBA8 in (row stride in bytes), RGBA8 out (w*4 per row). */
+void oracle_warp_cylindrical(const uint8_t* img, int h, int w, size_t stride, float focal_px, uint8_t* out);
+/* The registration half of stitch_panorama (:472-788) on n prepared RGBA8 images
+ * (tight rows): features, pairwise matching + RANSAC, the largest component, the
+ * reference, the maximum spanning tree, exposure gains, the canvas.  Outputs:
+ * ref_index, registered[n] (0/1), gains[n], h_to_ref[n*9] (f64, row-major, zero
+ * when unregistered), inv[n*9] (f64 inverse of the f32-cast matrix), origin[2],
+ * out_w, out_h.  Returns 0 or a negative error: -1 fewer than 2 images, -2 no
+ * pair matched, -3 no connected pair, -4 singular registered homography, -5
+ * projected corner at infinity, -6 non-finite corner, -7 canvas over the limits. */
+int oracle_panorama_register(const uint8_t* const* imgs, const int* hs, const int* ws, int n,
+                             const oracle_panorama_options* opt, int* ref_index, uint8_t* registered,
+                             float* gains, double* h_to_ref, double* inv, double* origin, int* out_w, int* out_h);
+/* The blending half (:790-940): the out_w x out_h RGBA8 canvas of the registered
+ * images (tight rows) through their inverse matrices, with their gains. */
+void oracle_panorama_composite(const uint8_t* const* imgs, const int* hs, const int* ws, int n,
+                               const uint8_t* registered, const float* gains, const double* inv,
+                               const double* origin, int out_w, int out_h, int blend, int levels, int tile_size,
+                               uint8_t* canvas);
+/* solve_exposure_gains (:232-316): pairs are (i, j, n_ij, mean_i, mean_j) as 5 doubles. */
+void oracle_solve_exposure_gains(const double* pairs, int n_pairs, int n_images, int ref_idx, double sigma_n,
+                                 double sigma_g, float* gains);
+
 #ifdef __cplusplus
 }
 #endif
