@@ -548,6 +548,69 @@ psift_status psift_warp_and_stitch_dev(psift_ctx* ctx, const uint8_t* query, uin
                                        size_t t_stride, const float* h9, uint8_t* canvas,
                                        size_t canvas_capacity, uint32_t* width, uint32_t* height);
 
+/* ---------------------------------------------------------------- panorama */
+/* stitch_panorama (src/stitch.rs:472-948): two or more overlapping RGBA8 images
+ * registered by SIFT features (the batch detection entry), pairwise Lowe
+ * matching and similarity + homography RANSAC (default seeds), chained to the
+ * best-connected image through a maximum spanning tree of inlier counts,
+ * exposure-compensated (Brown & Lowe gains) and composited on the union canvas
+ * by feather or multi-band (Laplacian pyramid over Voronoi seams) blending.
+ * Images are host RGBA8 with row strides in bytes.  The canvas is host RGBA8,
+ * width x height x 4 bytes, tight rows; call with canvas = NULL (or too small a
+ * capacity: PSIFT_ERR_CAPACITY) to learn the size from info.  registered (n
+ * bytes), gains (n floats) and homographies (n x 9 floats, row-major, image ->
+ * reference; zero when not registered) are optional.  The reference's errors
+ * come back as PSIFT_ERR_INVALID_ARGUMENT with its message (fewer than 2
+ * images, no pair matched, no connected pair, singular homography, corner at
+ * infinity or non-finite, canvas over the limits). */
+typedef struct psift_rgba_image {
+  const uint8_t* data;
+  uint32_t height, width;
+  size_t row_stride;  /* bytes, >= 4 x width */
+} psift_rgba_image;
+#define PSIFT_PROJECTION_PLANAR 0
+#define PSIFT_PROJECTION_CYLINDRICAL 1
+#define PSIFT_BLEND_FEATHER 0
+#define PSIFT_BLEND_MULTIBAND 1
+/* PanoramaOptions (src/stitch.rs:45-89). */
+typedef struct psift_panorama_options {
+  uint32_t octaves, scales;   /* default 3, 3 */
+  float threshold;            /* default 0.015 */
+  float ratio;                /* default 0.75 */
+  float ransac_threshold;     /* default 3.0 */
+  int32_t projection;         /* default planar */
+  float focal_px;             /* cylindrical projection's focal length */
+  int32_t blend;              /* default multi-band */
+  uint32_t levels;            /* multi-band levels, default 4 (clamped to 1..=6) */
+  int32_t exposure_compensation;  /* default 1 */
+  uint32_t max_canvas_dim;    /* default 8192 */
+  uint64_t max_canvas_pixels; /* default 25,000,000 */
+  uint32_t tile_size;         /* feather tiles, default 512 (does not change results) */
+} psift_panorama_options;
+void psift_panorama_options_default(psift_panorama_options* opt);
+/* PanoramaResult's geometry (src/stitch.rs:91-103) and the canvas origin in
+ * reference coordinates. */
+typedef struct psift_panorama_info {
+  uint32_t width, height;
+  int32_t reference_index;
+  int32_t registered_count;
+  double origin_x, origin_y;
+} psift_panorama_info;
+psift_status psift_stitch_panorama(psift_ctx* ctx, const psift_rgba_image* images, uint32_t n,
+                                   const psift_panorama_options* opt, uint8_t* canvas, size_t canvas_capacity,
+                                   psift_panorama_info* info, uint8_t* registered, float* gains,
+                                   float* homographies);
+/* warp_image_cylindrical (src/stitch.rs:166-201): out is height x width x 4 bytes. */
+psift_status psift_warp_cylindrical(psift_ctx* ctx, const psift_rgba_image* image, float focal_px, uint8_t* out);
+/* The compositing half of stitch_panorama (src/stitch.rs:790-940) on given
+ * registration results: for each registered image its inverse homography
+ * (reference -> image, 9 doubles, row-major) and gain; the canvas origin and
+ * size; blend and levels as in the options.  canvas: width x height x 4 bytes. */
+psift_status psift_panorama_composite(psift_ctx* ctx, const psift_rgba_image* images, uint32_t n,
+                                      const uint8_t* registered, const float* gains, const double* inverses,
+                                      double origin_x, double origin_y, uint32_t width, uint32_t height,
+                                      int32_t blend, uint32_t levels, uint8_t* canvas);
+
 /* Allocation-free variant of psift_detect_and_compute_batch_dev for one u8 image.
  * No counterpart in the reference: it exists for callers that cannot allocate
  * device memory -- plugin hosts that hand out only a stream, real-time loops in

@@ -144,6 +144,24 @@ psift_status io_reserve(psift_ctx* ctx, size_t bytes) {
   return PSIFT_OK;
 }
 
+psift_status stitch_reserve(psift_ctx* ctx, size_t bytes) {
+  bytes = align_up(bytes + 4096, 1 << 20);
+  if (bytes > ctx->stitch.capacity) {
+    PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->stitch.base) cudaFree(ctx->stitch.base);
+    ctx->stitch.base = nullptr;
+    ctx->stitch.capacity = 0;
+    cudaError_t e = cudaMalloc(&ctx->stitch.base, bytes);
+    if (e != cudaSuccess) {
+      ctx->stitch.base = nullptr;
+      return cuda_error(ctx, e, "cudaMalloc(panorama)");
+    }
+    ctx->stitch.capacity = bytes;
+  }
+  ctx->stitch.offset = 0;
+  return PSIFT_OK;
+}
+
 psift_status pinned_reserve(psift_ctx* ctx, size_t bytes) {
   if (bytes <= ctx->pinned.capacity) return PSIFT_OK;
   bytes = align_up(bytes, 1 << 20);
@@ -209,6 +227,7 @@ psift_status psift_ctx_destroy(psift_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream2);
   if (ctx->arena.base) cudaFree(ctx->arena.base);
   if (ctx->io.base) cudaFree(ctx->io.base);
+  if (ctx->stitch.base) cudaFree(ctx->stitch.base);
   if (ctx->pinned.base) cudaFreeHost(ctx->pinned.base);
   if (ctx->d_error) cudaFree(ctx->d_error);
   psift::jpeg_release(ctx);

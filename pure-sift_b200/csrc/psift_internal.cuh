@@ -70,6 +70,7 @@ struct psift_ctx {
   uint64_t launches = 0;
   psift::DeviceArena arena;   // per-call workspace
   psift::DeviceArena io;      // device copies of host-pointer inputs/outputs
+  psift::DeviceArena stitch;  // panorama: images, features, matches (held across the entries it calls)
   psift::PinnedBuffer pinned;
   int num_sms = 148;
   // Device status words: [0] error bits (kErr* below), [1] re-rank fallback rows.
@@ -117,6 +118,8 @@ void* arena_alloc(psift_ctx* ctx, size_t bytes);
 psift_status pinned_reserve(psift_ctx* ctx, size_t bytes);
 // Grow-only device buffer for the host-pointer entry points' inputs/outputs.
 psift_status io_reserve(psift_ctx* ctx, size_t bytes);
+// Grow-only device buffer of the panorama entries (not used by the entries they call).
+psift_status stitch_reserve(psift_ctx* ctx, size_t bytes);
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Raise a kernel's dynamic shared-memory limit once per (kernel, device).
 cudaError_t ensure_smem_attr(const void* func, size_t bytes);

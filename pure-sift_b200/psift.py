@@ -219,6 +219,13 @@ _SIGS = {
     "psift_ctx_tuning_get": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "psift_ctx_tuning_set": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "psift_ctx_set_blur_rounding": (C.c_int, [C.c_void_p, C.c_int32]),
+    "psift_panorama_options_default": (None, [C.c_void_p]),
+    "psift_stitch_panorama": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_size_t,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "psift_warp_cylindrical": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]),
+    "psift_panorama_composite": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_double, C.c_double, C.c_uint32, C.c_uint32, C.c_int32, C.c_uint32,
+                                           C.c_void_p]),
     "psift_fundamental_options_default": (None, [C.POINTER(CFundamentalOptions)]),
     "psift_fundamental_estimate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CFundamentalOptions),
                                              C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
@@ -1418,3 +1425,107 @@ def build_pyramid(img: np.ndarray, config: "SiftConfig" = None, ctx: Context | N
         out.append((blk[: S + 3], blk[S + 3:]))
         off += (2 * S + 5) * a * b
     return out
+
+
+# ---------------------------------------------------------------- panorama
+class CRgbaImage(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("height", C.c_uint32), ("width", C.c_uint32), ("row_stride", C.c_size_t)]
+
+
+class PanoramaOptions(C.Structure):
+    """``PanoramaOptions`` (src/stitch.rs:45-89).  projection: PROJECTION_PLANAR /
+    PROJECTION_CYLINDRICAL (with focal_px); blend: BLEND_FEATHER / BLEND_MULTIBAND
+    (with levels)."""
+    _fields_ = [("octaves", C.c_uint32), ("scales", C.c_uint32), ("threshold", C.c_float), ("ratio", C.c_float),
+                ("ransac_threshold", C.c_float), ("projection", C.c_int32), ("focal_px", C.c_float),
+                ("blend", C.c_int32), ("levels", C.c_uint32), ("exposure_compensation", C.c_int32),
+                ("max_canvas_dim", C.c_uint32), ("max_canvas_pixels", C.c_uint64), ("tile_size", C.c_uint32)]
+    PROJECTION_PLANAR, PROJECTION_CYLINDRICAL = 0, 1
+    BLEND_FEATHER, BLEND_MULTIBAND = 0, 1
+
+    @classmethod
+    def default(cls, **kw) -> "PanoramaOptions":
+        o = cls()
+        load_library().psift_panorama_options_default(C.byref(o))
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+
+class CPanoramaInfo(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("reference_index", C.c_int32),
+                ("registered_count", C.c_int32), ("origin_x", C.c_double), ("origin_y", C.c_double)]
+
+
+class PanoramaResult:
+    """``PanoramaResult`` (src/stitch.rs:91-103): image (H, W, 4) u8, reference_index,
+    registered_indices, gains (per input), homographies (per input: 3x3 f32 image ->
+    reference, or None), plus the canvas origin in reference coordinates."""
+
+    def __init__(self, image, reference_index, registered, gains, homographies, origin):
+        self.image = image
+        self.reference_index = reference_index
+        self.registered_indices = [i for i, r in enumerate(registered) if r]
+        self.gains = gains
+        self.homographies = [homographies[i].reshape(3, 3) if r else None for i, r in enumerate(registered)]
+        self.origin = origin
+
+
+def _rgba_images(images):
+    imgs = [np.ascontiguousarray(im, dtype=np.uint8).reshape(im.shape[0], im.shape[1], 4) for im in images]
+    arr = (CRgbaImage * max(len(imgs), 1))(*[CRgbaImage(im.ctypes.data, im.shape[0], im.shape[1], im.shape[1] * 4)
+                                             for im in imgs])
+    return imgs, arr
+
+
+def stitch_panorama(images, options: PanoramaOptions | None = None, ctx: Context | None = None) -> PanoramaResult:
+    """``stitch_panorama`` (src/stitch.rs:472-948) on the GPU: images are (h, w, 4) u8
+    RGBA.  Raises ValueError with the reference's message when it returns Err."""
+    ctx = ctx or default_context()
+    options = options or PanoramaOptions.default()
+    imgs, arr = _rgba_images(images)
+    n = len(imgs)
+    info = CPanoramaInfo()
+    reg = np.zeros(max(n, 1), np.uint8)
+    gains = np.zeros(max(n, 1), np.float32)
+    hs = np.zeros((max(n, 1), 9), np.float32)
+    cap = sum(im.shape[0] * im.shape[1] for im in imgs) * 4 * 4 + 4096
+    canvas = np.empty(cap, np.uint8)
+    while True:
+        st = ctx.lib.psift_stitch_panorama(ctx.handle, arr, n, C.byref(options), canvas.ctypes.data, canvas.nbytes,
+                                           C.byref(info), reg.ctypes.data, gains.ctypes.data, hs.ctypes.data)
+        if st == PSIFT_ERR_CAPACITY and info.width * info.height * 4 > canvas.nbytes:
+            canvas = np.empty(info.width * info.height * 4, np.uint8)
+            continue
+        break
+    if st == PSIFT_ERR_INVALID_ARGUMENT:
+        raise ValueError(ctx.lib.psift_last_error(ctx.handle).decode())
+    ctx.check(st)
+    image = canvas[:info.width * info.height * 4].reshape(info.height, info.width, 4).copy()
+    return PanoramaResult(image, info.reference_index, reg[:n].astype(bool), gains[:n], hs[:n],
+                          (info.origin_x, info.origin_y))
+
+
+def warp_cylindrical(image, focal_px: float, ctx: Context | None = None) -> np.ndarray:
+    """``warp_image_cylindrical`` (src/stitch.rs:166-201) on the GPU."""
+    ctx = ctx or default_context()
+    imgs, arr = _rgba_images([image])
+    out = np.zeros_like(imgs[0])
+    ctx.check(ctx.lib.psift_warp_cylindrical(ctx.handle, arr, float(focal_px), out.ctypes.data))
+    return out
+
+
+def panorama_composite(images, registered, gains, inverses, origin, width: int, height: int, blend: int,
+                       levels: int = 4, ctx: Context | None = None) -> np.ndarray:
+    """The compositing half of ``stitch_panorama`` on given registration results:
+    inverses (n, 3, 3) f64 reference -> image; returns the (height, width, 4) canvas."""
+    ctx = ctx or default_context()
+    imgs, arr = _rgba_images(images)
+    regm = np.ascontiguousarray(registered, dtype=np.uint8)
+    g = np.ascontiguousarray(gains, dtype=np.float32)
+    inv = np.ascontiguousarray(inverses, dtype=np.float64).reshape(-1, 9)
+    canvas = np.zeros((height, width, 4), np.uint8)
+    ctx.check(ctx.lib.psift_panorama_composite(ctx.handle, arr, len(imgs), regm.ctypes.data, g.ctypes.data,
+                                               inv.ctypes.data, float(origin[0]), float(origin[1]), width, height,
+                                               int(blend), int(levels), canvas.ctypes.data))
+    return canvas
