@@ -507,6 +507,53 @@ def catalog_search_bench(ctx, torch, n_entries: int = 10_000, per_entry: int = 2
     }
 
 
+def panorama_bench(ctx, torch, reps: int = 3):
+    """stitch_panorama: four overlapping 1280x720 RGBA tiles of a synthetic colour
+    field (three independent 2000-blob planes as R, G, B; tile step 900 px,
+    exposures 0.9 / 1.0 / 1.1 / 0.95), multi-band blending with 4 levels and
+    exposure compensation, through the host API (registration: detection,
+    matching, RANSAC of the 6 pairs; compositing on the GPU); the compositing
+    alone on the host API with the registration's results; the CPU restatement
+    of both on the same tiles."""
+    import psift
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W, H, tile, step = 3980, 720, 1280, 900
+    chans = [synth.blob_image(W, H, 4000, 1.5, 20.0, seed=s) for s in (91, 92, 93)]
+    rgb = np.stack(chans, axis=-1).astype(np.float32)
+    tiles = []
+    for i, f in enumerate((0.9, 1.0, 1.1, 0.95)):
+        v = np.clip(np.round(rgb[:, i * step:i * step + tile] * np.float32(f)), 0, 255).astype(np.uint8)
+        tiles.append(np.concatenate([v, np.full(v.shape[:2] + (1,), 255, np.uint8)], axis=-1))
+    opt = psift.PanoramaOptions.default()
+    res = psift.stitch_panorama(tiles, opt, ctx=ctx)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        res = psift.stitch_panorama(tiles, opt, ctx=ctx)
+    full_s = (time.perf_counter() - t0) / reps
+    reg = O.panorama_register(tiles, O.PanoramaOptions.default())
+    comp = lambda: psift.panorama_composite(tiles, reg["registered"], reg["gains"], reg["inv"], reg["origin"],
+                                            reg["width"], reg["height"], 1, 4, ctx=ctx)
+    comp()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        got = comp()
+    comp_s = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    want = O.panorama_composite(tiles, reg, 1, 4)
+    cpu_comp_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.panorama_register(tiles, O.PanoramaOptions.default())
+    cpu_reg_s = time.perf_counter() - t0
+    h, w = res.image.shape[:2]
+    return {"workload": "4 overlapping 1280x720 RGBA tiles (synthetic colour field), multi-band 4 levels, "
+                        "exposure compensation", "canvas": [w, h], "registered": len(res.registered_indices),
+            "stitch_host_api_ms": full_s * 1e3, "composite_host_api_ms": comp_s * 1e3,
+            "composite_mpx_per_s": w * h / comp_s / 1e6,
+            "cpu_restatement_ms": {"registration": cpu_reg_s * 1e3, "composite": cpu_comp_s * 1e3},
+            "composite_identical_to_restatement": bool(np.array_equal(got, want))}
+
+
 def warp_bench(ctx, torch, reps: int = 50):
     """warp_and_stitch on a 1080p RGBA pair: the query warped by a C2-style
     homography (rotation, scale, perspective about the centre) onto the target's
@@ -811,6 +858,8 @@ def run_ours(args):
         o["d"] = torch.empty((cap, 128), dtype=torch.float32, device="cuda")
     d_counts = torch.zeros(B, dtype=torch.int32, device="cuda")
     ctx = psift.Context(local)
+    if args.blur == "fused":
+        ctx.set_blur_rounding(ctx.BLUR_FUSED)  # profiling case: the single-rounding blur in the main loop
     cfg = psift.SiftConfig().with_octaves(OCTAVES).with_scales(SCALES).with_contrast_threshold(THRESH)
     ccfg = cfg.to_c()
     # tile shapes: the library's autotuner on this geometry (one chunk of the batch;
@@ -1032,7 +1081,7 @@ def run_ours(args):
         for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench),
                         ("catalog_search", catalog_search_bench), ("warp", warp_bench),
                         ("fundamental", fundamental_bench),
-                        ("learned_ransac", ransac_bench), ("jpeg", jpeg_bench)):
+                        ("learned_ransac", ransac_bench), ("jpeg", jpeg_bench), ("panorama", panorama_bench)):
             if getattr(args, "no_" + key):
                 continue
             try:
@@ -1072,9 +1121,11 @@ def main():
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
     ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "warp", "fundamental",
-                                               "learned_ransac", "uneven_batch", "jpeg"],
+                                               "learned_ransac", "uneven_batch", "jpeg", "panorama"],
                     help="run one section alone (profiling case)")
     ap.add_argument("--ransac-pairs", type=int, default=1024, help="learned-RANSAC section: match sets")
+    ap.add_argument("--blur", choices=["reference", "fused"], default="reference",
+                    help="blur rounding of the main loop (profiling case; the default is the reference's)")
     ap.add_argument("--catalog-codes", type=int, default=2_000_000, help="catalog section: catalog codes")
     ap.add_argument("--catalog-entries", type=int, default=10_000, help="catalog-search section: entries")
     ap.add_argument("--no-catalog", action="store_true")
@@ -1086,6 +1137,7 @@ def main():
     ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
     ap.add_argument("--no-jpeg", dest="no_jpeg", action="store_true")
+    ap.add_argument("--no-panorama", dest="no_panorama", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if world != args.gpus:
@@ -1106,7 +1158,8 @@ def main():
                "learned_ransac": lambda: ransac_bench(ctx, torch, n_pairs=args.ransac_pairs),
                "catalog_search": lambda: catalog_search_bench(ctx, torch, n_entries=args.catalog_entries), "warp": lambda: warp_bench(ctx, torch),
                "fundamental": lambda: fundamental_bench(ctx, torch),
-               "uneven_batch": lambda: uneven_bench(ctx, torch), "jpeg": lambda: jpeg_bench(ctx, torch)}
+               "uneven_batch": lambda: uneven_bench(ctx, torch), "jpeg": lambda: jpeg_bench(ctx, torch),
+               "panorama": lambda: panorama_bench(ctx, torch)}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)
         ctx.close()
         return 0
