@@ -222,7 +222,8 @@ def _uneven_pair(k):
 
 def uneven_bench(ctx, torch, n_pairs: int = 32, reps: int = 3):
     """Uneven batch: 64 images (32 pairs A_i, B_i = perspective warp of A_i), widths
-    U(480, 3840), aspect U(0.5, 2), blobs in proportion to area; SiftConfig octaves 4,
+    U(480, 3840), aspect U(0.5, 2), blobs in proportion to area (6000 per 1080p
+    area, synth.uneven_pair); SiftConfig octaves 4,
     threshold 0.015, upsampling, uncapped features.  All 64 images in one device
     batch call (one launch per stage; CUDA-graph replay), then the 32 pairs matched
     in one call with the exact FP32 kernel and with BF16 + certified re-rank."""
@@ -286,7 +287,8 @@ def uneven_bench(ctx, torch, n_pairs: int = 32, reps: int = 3):
                     f"{n_pairs} pairs A_i vs warp(A_i), ratio 0.8",
         "detect_ms_batch": det_ms, "detect_images_per_s": B / (det_ms * 1e-3),
         "detect_mpx_per_s": mpx / (det_ms * 1e-3),
-        "features_per_image": {"min": int(cnt.min()), "median": int(np.median(cnt)), "max": int(cnt.max())},
+        "features_per_image": {"min": int(cnt.min()), "median": int(np.median(cnt)), "max": int(cnt.max()),
+                               "fraction_within_4k_20k": float(((cnt >= 4000) & (cnt <= 20000)).mean())},
         "match_fp32_ms_32_pairs": res["fp32"], "match_bf16_rerank_ms_32_pairs": res["bf16_rerank"],
         "match_speedup_bf16_vs_fp32": res["fp32"] / res["bf16_rerank"],
         "identical_match_lists": lists["fp32"] == lists["bf16_rerank"],

@@ -439,6 +439,8 @@ psift_status launch_detect_split(psift_ctx* ctx, DetectJob& job, const psift_sif
     v.d_plans = job.d_plans + b;
     v.kp_cap = job.kp_cap;
     v.sel_cap = job.sel_cap;
+    std::memcpy(v.blur_variant, job.blur_variant, sizeof v.blur_variant);  // the context's tuning
+    v.blur_fused = job.blur_fused;
     psift_status st = launch_detect(ctx, v, cfg, false, streams[c], true);
     if (st != PSIFT_OK) return st;
   }
@@ -919,6 +921,8 @@ psift_status detect_batch_host_out(psift_ctx* ctx, const psift_image_u8* images,
     v.d_plans = job.d_plans + b;
     v.kp_cap = job.kp_cap;
     v.sel_cap = job.sel_cap;
+    std::memcpy(v.blur_variant, job.blur_variant, sizeof v.blur_variant);  // the context's tuning
+    v.blur_fused = job.blur_fused;
     st = launch_detect(ctx, v, *cfg, false, sc, /*plans_uploaded=*/true);
     if (st != PSIFT_OK) return st;
     for (uint32_t i = b; i < e; ++i)

@@ -160,10 +160,17 @@ def uneven_batch_shapes(n: int, seed: int = 3):
 
 def uneven_pair(k: int, seed: int = 3):
     """Pair k of the uneven batch: A of shape uneven_batch_shapes(...)[k] with blobs in
-    proportion to its area (2000 per 1920x1080), B = A under a 1080p-pair-style
-    perspective warp about its centre.  Returns (A, B)."""
+    proportion to its area, B = A under a 1080p-pair-style perspective warp about its
+    centre.  Returns (A, B).
+
+    The density is 6000 blobs per 1920x1080 (three times the 1080p workload's): the
+    detected features grow sub-linearly with the blob count (overlapping blobs), and
+    this density puts the median image of the batch near 5k features, inside the
+    workload's "~4k-20k keypoints each"; with the count in proportion to the area,
+    the smallest images (0.14 Mpx) stay below that range and the largest (23 Mpx)
+    above it."""
     h, w = uneven_batch_shapes(k + 1, seed)[k]
-    n_blobs = max(1, int(round(2000 * (w * h) / (1920 * 1080))))
+    n_blobs = max(1, int(round(6000 * (w * h) / (1920 * 1080))))
     a = blob_image(w, h, n_blobs, 1.5, 20.0, seed * 100003 + k)
     u = SplitMix64((seed * 7919 + k) ^ 0xABCDEF).uniform(4)
     H = perspective_h(w, h, -30 + 60 * u[0], 0.7 + 0.7 * u[1], -2e-4 + 4e-4 * u[2], -2e-4 + 4e-4 * u[3])

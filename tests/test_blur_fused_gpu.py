@@ -101,3 +101,24 @@ def test_modes_switch_on_one_context():
     with pytest.raises(psift.PsiftError):
         ctx.set_blur_rounding(7)
     ctx.close()
+
+
+def test_batch_entries_follow_the_context_mode():
+    """The batch entries split the batch over two streams; each half must run the
+    context's blur mode (and tuning): reference mode equals the one-image path bit
+    for bit, fused mode differs from it."""
+    imgs = [synth.pair_640x480(1)[0], synth.pair_640x480(2)[1]]
+    ctx = psift.Context(0)
+    sift = _sift()
+    single = [sift.detect_and_compute_u8(im, ctx=ctx) for im in imgs]
+    ref = sift.detect_and_compute_batch_u8(imgs, ctx=ctx)
+    for a, b in zip(ref, single):
+        np.testing.assert_array_equal(a.response, b.response)
+        np.testing.assert_array_equal(a.descriptors, b.descriptors)
+    ctx.set_blur_rounding(psift.Context.BLUR_FUSED)
+    fz_single = [sift.detect_and_compute_u8(im, ctx=ctx) for im in imgs]
+    fz = sift.detect_and_compute_batch_u8(imgs, ctx=ctx)
+    for a, b, r in zip(fz, fz_single, ref):
+        np.testing.assert_array_equal(a.response, b.response)
+        assert len(a) != len(r) or not np.array_equal(a.response, r.response)
+    ctx.close()
