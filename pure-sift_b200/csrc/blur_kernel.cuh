@@ -38,8 +38,6 @@
 
 namespace psift {
 
-constexpr int kTileW = 64;
-constexpr int kTileH = 64;
 constexpr int kBlurThreads = 256;
 constexpr int kTmpStride = kTileW + 8;  // floats per intermediate row
 constexpr int kStageBatch = 4;          // staging units per thread with loads in flight
@@ -47,10 +45,31 @@ constexpr int kStageBatch = 4;          // staging units per thread with loads i
 // the context's tuning table (psift_ctx_autotune): 0 = 4 x 8, 1 = 8 x 8, 2 = 4 x 4.
 constexpr int kPrefetchWaves = 1;       // level blur: L2 prefetch distance in resident-CTA waves
 
+// Per-launch parameters (passed by value).
 struct Taps2 {
   float2 w[kMaxTaps];  // {w_k, w_k}
   float2 one;          // {1, 1}: the multiplier of the packed add (see mul_add2_rn)
+  TileMap tiles;
 };
+
+// Linear tile `lin` of a work list (reversed when zrev) -> image and tile; false
+// past the end.
+__device__ __forceinline__ bool tile_of(const TileMap& tm, long long lin, int zrev, int& z, int& bx, int& by) {
+  const int total = tm.prefix[tm.n];
+  if (lin >= total) return false;
+  const int l = zrev ? total - 1 - (int)lin : (int)lin;
+  int lo = 0, hi = tm.n - 1;  // the last z with prefix[z] <= l
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tm.prefix[mid] <= l) lo = mid;
+    else hi = mid - 1;
+  }
+  z = lo;
+  const int local = l - tm.prefix[z];
+  by = local / tm.tiles_x[z];
+  bx = local - by * tm.tiles_x[z];
+  return true;
+}
 
 enum BlurMode : int { MODE_LEVEL = 0, MODE_INIT_F32 = 1, MODE_INIT_U8 = 2, MODE_INIT_F32_UP = 3, MODE_INIT_U8_UP = 4 };
 
@@ -150,15 +169,22 @@ __device__ __forceinline__ float fetch_src(const ImagePlan& P, const OctaveDev& 
 // reads of the next wave overlap the arithmetic of this one.
 template <int R>
 __device__ __forceinline__ void prefetch_ahead_rows(const ImagePlan* __restrict__ plans, int octave, int level,
-                                                    int zrev, int ahead) {
+                                                    int zrev, int ahead, const TileMap& tm) {
   using Gm = BlurGeom<R>;
-  const long long nxy = (long long)gridDim.x * gridDim.y;
-  const long long lin = blockIdx.x + (long long)gridDim.x * blockIdx.y + nxy * blockIdx.z + ahead;
-  if (lin >= nxy * gridDim.z) return;
-  const int bz = (int)(lin / nxy);
-  const int rem = (int)(lin - (long long)bz * nxy);
-  const int by = rem / (int)gridDim.x, bx = rem - by * (int)gridDim.x;
-  const ImagePlan& P = plans[zrev ? (int)gridDim.z - 1 - bz : bz];
+  int z, bx, by;
+  if (tm.n > 0) {
+    if (!tile_of(tm, (long long)blockIdx.x + ahead, zrev, z, bx, by)) return;
+  } else {
+    const long long nxy = (long long)gridDim.x * gridDim.y;
+    const long long lin = blockIdx.x + (long long)gridDim.x * blockIdx.y + nxy * blockIdx.z + ahead;
+    if (lin >= nxy * gridDim.z) return;
+    const int bz = (int)(lin / nxy);
+    const int rem = (int)(lin - (long long)bz * nxy);
+    by = rem / (int)gridDim.x;
+    bx = rem - by * (int)gridDim.x;
+    z = zrev ? (int)gridDim.z - 1 - bz : bz;
+  }
+  const ImagePlan& P = plans[z];
   if (octave >= P.n_oct) return;
   const OctaveDev& O = P.oct[octave];
   const int tx0 = bx * kTileW, ty0 = by * kTileH;
@@ -172,7 +198,9 @@ __device__ __forceinline__ void prefetch_ahead_rows(const ImagePlan* __restrict_
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"((c1 - c0) * 4) : "memory");
 }
 
-// One blur level for every image of the batch (blockIdx.z = image, reversed when zrev).
+// One blur level for every image of the batch (blockIdx.z = image, reversed when
+// zrev; or, over images of different sizes, one CTA per existing tile of the
+// launch's tile work list, the list reversed when zrev).
 //   MODE_LEVEL: G[s] = blur(G[s-1]); D[s-1] = G[s] - G[s-1]; level `down_level` also
 //               writes the next octave's G[0] (even rows/columns).
 //   MODE_INIT_*: G[0] of octave 0 from the input image.
@@ -182,7 +210,7 @@ __global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const Image
                                                                    Taps2 taps) {
   using Gm = BlurGeom<R>;
   if constexpr (MODE == MODE_LEVEL) {
-    if (pf_ahead > 0 && threadIdx.x < Gm::IN_H) prefetch_ahead_rows<R>(plans, octave, level, zrev, pf_ahead);
+    if (pf_ahead > 0 && threadIdx.x < Gm::IN_H) prefetch_ahead_rows<R>(plans, octave, level, zrev, pf_ahead, taps.tiles);
   }
   static_assert(HC == 4 || HC == 8, "horizontal outputs per thread");
   // The Gaussian taps are bit-symmetric (gaussian_kernel_1d evaluates the same
@@ -193,12 +221,19 @@ __global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const Image
   for (int k = 0; k <= R; ++k) wv[k] = taps.w[k];
   const float2 one = taps.one;
   static_assert(RV % 2 == 0 && kTileH % (RV * (kBlurThreads / 32)) == 0, "vertical rows per thread");
-  const int z = zrev ? (int)gridDim.z - 1 - (int)blockIdx.z : (int)blockIdx.z;
+  int z, bx, by;
+  if (taps.tiles.n > 0) {
+    if (!tile_of(taps.tiles, blockIdx.x, zrev, z, bx, by)) return;
+  } else {
+    z = zrev ? (int)gridDim.z - 1 - (int)blockIdx.z : (int)blockIdx.z;
+    bx = blockIdx.x;
+    by = blockIdx.y;
+  }
   const ImagePlan& P = plans[z];
   if (octave >= P.n_oct) return;
   const OctaveDev& O = P.oct[octave];
   const int h = O.h, w = O.w;
-  const int tx0 = blockIdx.x * kTileW, ty0 = blockIdx.y * kTileH;
+  const int tx0 = bx * kTileW, ty0 = by * kTileH;
   if (tx0 >= w || ty0 >= h) return;
 
   extern __shared__ float4 smem4[];
@@ -433,6 +468,7 @@ static cudaError_t launch_blur_r(const ImagePlan* plans, int n_images, int octav
     pf_ahead *= kPrefetchWaves;
   }
   dim3 grid((max_w + kTileW - 1) / kTileW, (max_h + kTileH - 1) / kTileH, n_images);
+  if (taps.tiles.n > 0) grid = dim3((unsigned)taps.tiles.prefix[taps.tiles.n], 1, 1);
   blur_level_kernel<R, HC, RV, MODE, FUSED><<<grid, kBlurThreads, smem, st>>>(plans, octave, level, down_level, zrev,
                                                                       pf_ahead, taps);
   return cudaGetLastError();

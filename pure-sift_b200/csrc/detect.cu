@@ -25,7 +25,7 @@ namespace psift {
 // Declared in pyramid.cu / extrema.cu / describe.cu.
 cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
                         int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant = 0,
-                        bool fused = false);
+                        bool fused = false, const TileMap* tiles = nullptr);
 cudaError_t launch_extrema_mark(const ImagePlan* plans, int n, int octave, int max_h, const ExtremaParams& prm,
                                 cudaStream_t st);
 cudaError_t launch_row_scan(const ImagePlan* plans, int n, uint32_t kp_cap, uint32_t* err, cudaStream_t st);
@@ -251,12 +251,39 @@ psift_status build_job(psift_ctx* ctx, const std::vector<ImageDesc>& imgs, const
   return PSIFT_OK;
 }
 
+// Tile work list of octave o over the job's images, so that a blur launch over
+// images of different sizes runs one CTA per existing tile; n = 0 (the (tiles x,
+// tiles y, images) grid over the largest image) when every image has that size
+// at octave o or the job has more than kTileMapMax images.
+TileMap tile_map(const DetectJob& job, int o, int mh, int mw) {
+  TileMap tm;
+  tm.n = 0;
+  tm.prefix[0] = 0;
+  if (job.n > kTileMapMax) return tm;
+  bool uneven = false;
+  for (int i = 0; i < job.n; ++i) {
+    const HostOctave& H = job.oct[(size_t)i * kMaxOctaves + o];
+    uneven |= o >= job.n_oct[i] || H.h != mh || H.w != mw;
+  }
+  if (!uneven) return tm;
+  for (int i = 0; i < job.n; ++i) {
+    const HostOctave& H = job.oct[(size_t)i * kMaxOctaves + o];
+    const bool has = o < job.n_oct[i];
+    const int tx = has ? (H.w + kTileW - 1) / kTileW : 0, ty = has ? (H.h + kTileH - 1) / kTileH : 0;
+    tm.tiles_x[i] = std::max(tx, 1);
+    tm.prefix[i + 1] = tm.prefix[i] + tx * ty;
+  }
+  tm.n = tm.prefix[job.n] > 0 ? job.n : 0;
+  return tm;
+}
+
 // One blur level (octave o, level s >= 1) of every image of the job.
 cudaError_t launch_level(const DetectJob& job, const SigmaSchedule& sc, int o, int s, int S, int mh, int mw,
                          cudaStream_t st) {
   const int r = sc.level_radius[s];
+  const TileMap tm = tile_map(job, o, mh, mw);
   return launch_blur(0, sc.level_taps[s].data(), r, job.d_plans, job.n, o, s, S, mh, mw, st,
-                     r >= 0 && r < 16 ? job.blur_variant[r] : 0, job.blur_fused);
+                     r >= 0 && r < 16 ? job.blur_variant[r] : 0, job.blur_fused, &tm);
 }
 
 // Queue every stage of the path for the batch (no host synchronisation).
@@ -295,8 +322,9 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
     const bool up = cfg.upsample_first_octave != 0;
     const int kind = job.plans[0].src_kind;
     const int mode = kind == SRC_U8 ? (up ? 4 : 2) : (up ? 3 : 1);
+    const TileMap tm0 = tile_map(job, 0, mh, mw);
     cudaError_t e = launch_blur(mode, sc.init_taps.data(), sc.init_radius, job.d_plans, n, 0, 0, -1, mh, mw, st, 0,
-                                job.blur_fused);
+                                job.blur_fused, &tm0);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_error(ctx, e, "blur(init)");
   }
@@ -386,8 +414,9 @@ psift_status launch_pyramid_only(psift_ctx* ctx, DetectJob& job, const psift_sif
     if (o == 0) {
       const bool up = cfg.upsample_first_octave != 0;
       const int mode = job.plans[0].src_kind == SRC_U8 ? (up ? 4 : 2) : (up ? 3 : 1);
+      const TileMap tm0 = tile_map(job, 0, mh, mw);
       cudaError_t e = launch_blur(mode, sc.init_taps.data(), sc.init_radius, job.d_plans, n, 0, 0, -1, mh, mw, st, 0,
-                                job.blur_fused);
+                                  job.blur_fused, &tm0);
       ctx->launches++;
       if (e != cudaSuccess) return cuda_error(ctx, e, "blur(init)");
     }

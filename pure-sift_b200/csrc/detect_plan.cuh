@@ -64,6 +64,20 @@ struct ImagePlan {
   uint32_t feat_cap;
 };
 
+// Output tile of a blur CTA.
+constexpr int kTileW = 64;
+constexpr int kTileH = 64;
+
+// Tile work list of a blur launch over images of different sizes: image z owns
+// the linear tiles [prefix[z], prefix[z + 1]), tiles_x[z] per row of tiles.
+// n = 0: the launch is a (tiles x, tiles y, images) grid over the largest image.
+constexpr int kTileMapMax = 64;
+struct TileMap {
+  int n;
+  int prefix[kTileMapMax + 1];
+  int tiles_x[kTileMapMax];
+};
+
 // Kernel parameters of the extrema stage (passed by value).
 struct ExtremaParams {
   float threshold;

@@ -10,8 +10,15 @@ namespace psift {
 // every variant computes the same values.  fused: the single-rounding blur
 // (one fused multiply-add per tap; not the reference's rounding).
 cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
-                        int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant, bool fused) {
+                        int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant, bool fused,
+                        const TileMap* tiles) {
   Taps2 t;
+  if (tiles && tiles->n > 0) {
+    t.tiles = *tiles;
+  } else {
+    t.tiles.n = 0;
+    t.tiles.prefix[0] = 0;
+  }
   for (int i = 0; i < kMaxTaps; ++i) {
     const float v = i <= 2 * radius ? taps_host[i] : 0.0f;
     t.w[i] = make_float2(v, v);
