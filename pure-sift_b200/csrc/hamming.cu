@@ -108,27 +108,58 @@ __global__ void quantize_kernel(const float* __restrict__ desc, int n, uint64_t*
   }
 }
 
-// dequantize_descriptor_u8: v/512 then L2 renormalisation (sequential sum).
-__global__ void dequantize_kernel(const uint8_t* __restrict__ q, int n, float* __restrict__ out) {
-  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= n) return;
-  const uint32_t p = reinterpret_cast<const uint32_t*>(q + (size_t)row * 128)[lane];
-  float e[4];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) e[j] = (float)((p >> (8 * j)) & 0xFF) * (1.0f / 512.0f);
-  float s = 0.0f;
-  for (int i = 0; i < 128; ++i) {
-    const float x = __shfl_sync(0xffffffffu, e[i & 3], i >> 2);
-    s += x * x;
+// dequantize_descriptor_u8: v/512 then L2 renormalisation (sequential sum).  A
+// warp per 32 rows: the u8 rows are read coalesced and staged in shared memory
+// as f32, lane j adds up row j's squared norm sequentially, and the scaled rows
+// are written back coalesced (a float4 per lane and row).
+constexpr int kDqWarps = 2;  // 33.8 KB of static shared memory per block
+constexpr int kDqStride = 132;  // floats per staged row (conflict-free 16-byte reads across rows)
+
+__global__ void __launch_bounds__(32 * kDqWarps) dequantize_kernel(const uint8_t* __restrict__ q, int n,
+                                                                   float* __restrict__ out) {
+  __shared__ __align__(16) float stage[kDqWarps][32 * kDqStride];
+  __shared__ float inv_s[kDqWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row0 = (blockIdx.x * kDqWarps + warp) * 32;
+  if (row0 >= n) return;
+  const int nr = min(32, n - row0);
+  float* st = stage[warp];
+  for (int r = 0; r < nr; ++r) {
+    const uint32_t p = reinterpret_cast<const uint32_t*>(q + (size_t)(row0 + r) * 128)[lane];
+    float4 v;
+    v.x = (float)(p & 0xFF) * (1.0f / 512.0f);
+    v.y = (float)((p >> 8) & 0xFF) * (1.0f / 512.0f);
+    v.z = (float)((p >> 16) & 0xFF) * (1.0f / 512.0f);
+    v.w = (float)(p >> 24) * (1.0f / 512.0f);
+    *reinterpret_cast<float4*>(st + r * kDqStride + 4 * lane) = v;
   }
-  const float norm = sqrtf(s);
-  if (norm > 1e-7f) {
-    const float inv = 1.0f / norm;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) e[j] *= inv;
+  __syncwarp();
+  if (lane < nr) {
+    const float* rr = st + lane * kDqStride;
+    float s = 0.0f;
+#pragma unroll 8
+    for (int c = 0; c < 32; ++c) {
+      const float4 v = *reinterpret_cast<const float4*>(rr + 4 * c);
+      s += v.x * v.x;
+      s += v.y * v.y;
+      s += v.z * v.z;
+      s += v.w * v.w;
+    }
+    const float norm = sqrtf(s);
+    inv_s[warp][lane] = norm > 1e-7f ? 1.0f / norm : 1.0f;  // 1: the row is kept as it is
   }
-  reinterpret_cast<float4*>(out + (size_t)row * 128)[lane] = make_float4(e[0], e[1], e[2], e[3]);
+  __syncwarp();
+  for (int r = 0; r < nr; ++r) {
+    float4 v = *reinterpret_cast<const float4*>(st + r * kDqStride + 4 * lane);
+    const float inv = inv_s[warp][r];
+    if (inv != 1.0f) {
+      v.x *= inv;
+      v.y *= inv;
+      v.z *= inv;
+      v.w *= inv;
+    }
+    reinterpret_cast<float4*>(out + (size_t)(row0 + r) * 128)[lane] = v;
+  }
 }
 
 // Votes: one block per entry, each thread owns queries tid, tid+blockDim, ...
@@ -357,7 +388,7 @@ cudaError_t launch_quantize(const float* desc, int n, uint64_t* codes, uint8_t* 
 
 cudaError_t launch_dequantize(const uint8_t* q, int n, float* out, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  dequantize_kernel<<<(n + 7) / 8, 256, 0, st>>>(q, n, out);
+  dequantize_kernel<<<(n + 32 * kDqWarps - 1) / (32 * kDqWarps), 32 * kDqWarps, 0, st>>>(q, n, out);
   return cudaGetLastError();
 }
 

@@ -32,11 +32,13 @@ struct Bf16Job {
   float* norm_max;
   uint16_t* ext;
   int n_pad;
+  float* top2;
 };
 cudaError_t launch_to_bf16(const void* jobs, int n_jobs, int max_rows, cudaStream_t st);
 cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const CUtensorMap& tmAx,
-                            const CUtensorMap& tmBx, const TcItem* items, int n_items, const TcPair* pairs,
-                            uint32_t* err, int mode, cudaStream_t st);
+                            const CUtensorMap& tmBx, const TcPair* problems, int n_problems, const TcPlan* plan,
+                            int ctas, uint32_t* err, int mode, cudaStream_t st);
+cudaError_t launch_tc_plan(TcPair* problems, int n_problems, TcPlan* plan, int ctas, cudaStream_t st);
 cudaError_t launch_window(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 cudaError_t launch_gather_rows(const GatherJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
@@ -44,8 +46,6 @@ cudaError_t launch_gather_rows(const GatherJob* jobs, int n_jobs, int max_rows, 
 namespace {
 
 constexpr int kTile = 128;
-constexpr int kTcBM = 128, kTcBN = 256;
-constexpr int kCollRows = 32;  // window indices kept per (split, row); equals kColl in match_tc.cu
 
 // Matcher::new (src/pipeline.rs:156-164): same message.
 psift_status validate_match_options(psift_ctx* ctx, const psift_match_options* o) {
@@ -60,7 +60,7 @@ psift_status validate_match_options(psift_ctx* ctx, const psift_match_options* o
   return PSIFT_OK;
 }
 
-long long pad_rows(int n) { return ((long long)n + 255) / 256 * 256; }
+long long pad_rows(int n) { return ((long long)n + kTcBN - 1) / kTcBN * kTcBN; }
 
 // Device-side batch: every pointer in jobs is device memory.  Queues all work.
 psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, const psift_match_options& opt) {
@@ -87,8 +87,6 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   long long part_total = 0, cpart_total = 0;
   long long q_rows = 0, t_rows = 0;
   long long cand_f = 0, cand_r = 0;
-  std::vector<int> tc_split_f(na), tc_split_r(na);
-  int n_items_f = 0, n_items_r = 0;
   const int target_ctas = ctx->tune.match_per_sm[tc ? 1 : 0] * ctx->num_sms;
   for (int k = 0; k < na; ++k) {
     const psift_match_job& J = jobs[active[k]];
@@ -107,18 +105,8 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     } else {
       q_rows += pad_rows((int)J.nq);
       t_rows += pad_rows((int)J.nt);
-      const int at = (int)((J.nq + kTcBM - 1) / kTcBM), bt = (int)((J.nt + kTcBN - 1) / kTcBN);
-      int sp = std::max(1, std::min(bt, (target_ctas + na * at - 1) / (na * at)));
-      tc_split_f[k] = sp;
-      n_items_f += at * sp;
-      cand_f += (long long)sp * J.nq;
-      if (mutual) {
-        const int at2 = (int)((J.nt + kTcBM - 1) / kTcBM), bt2 = (int)((J.nq + kTcBN - 1) / kTcBN);
-        int sp2 = std::max(1, std::min(bt2, (target_ctas + na * at2 - 1) / (na * at2)));
-        tc_split_r[k] = sp2;
-        n_items_r += at2 * sp2;
-        cand_r += (long long)sp2 * J.nt;
-      }
+      cand_f += (long long)kTcSplits * J.nq;
+      if (mutual) cand_r += (long long)kTcSplits * J.nt;
     }
   }
   int t_splits = 1;
@@ -136,8 +124,8 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   } else {
     bytes += (size_t)(q_rows + t_rows) * 256 + (size_t)(q_rows + t_rows) * 4 + 4096;
     bytes += (size_t)(q_rows + t_rows) * 32 + (size_t)kTcBM * 32 + 3 * 256;  // GEMM norm extensions
-    bytes += (size_t)(cand_f + cand_r) * (8 + 4 * kCollRows + 4) + (size_t)(q_rows + t_rows) * 4 +
-             sizeof(TcItem) * (n_items_f + n_items_r) +
+    bytes += (size_t)(cand_f + cand_r) * (8 + 4 * kTcColl + 4) + (size_t)(q_rows + t_rows) * 4 +
+             sizeof(TcPlan) * 4 + 256 +
              sizeof(TcPair) * 2 * na + sizeof(RerankJob) * 2 * na + 8192 + (size_t)t_rows * 4 +
              sizeof(Bf16Job) * 2 * na + 512;
     // pass 2's compacted operands, row maps, counts and gather jobs
@@ -210,10 +198,10 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   float* maxes = (float*)arena_alloc(ctx, sizeof(float) * 2 * na);  // [k]: t max, [na + k]: q max
   const long long cand = std::max<long long>(cand_f + cand_r, 1);
   float* top2 = (float*)arena_alloc(ctx, sizeof(float) * 2 * cand);
-  int* coll_idx = (int*)arena_alloc(ctx, sizeof(int) * kCollRows * cand);
+  int* coll_idx = (int*)arena_alloc(ctx, sizeof(int) * kTcColl * cand);
   int* coll_cnt = (int*)arena_alloc(ctx, sizeof(int) * cand);
   float* thr = (float*)arena_alloc(ctx, sizeof(float) * (q_rows + t_rows));
-  TcItem* d_items = (TcItem*)arena_alloc(ctx, sizeof(TcItem) * (n_items_f + n_items_r));
+  TcPlan* d_plan = (TcPlan*)arena_alloc(ctx, sizeof(TcPlan) * 4);  // [direction][pass]
   TcPair* d_tcp = (TcPair*)arena_alloc(ctx, sizeof(TcPair) * 2 * na);
   RerankJob* d_rj = (RerankJob*)arena_alloc(ctx, sizeof(RerankJob) * 2 * na);
   int* flags = mutual ? (int*)arena_alloc(ctx, sizeof(int) * t_rows) : nullptr;  // matched-target marks
@@ -232,7 +220,7 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   GatherJob* d_gj = (GatherJob*)arena_alloc(ctx, sizeof(GatherJob) * 2 * na);
   std::vector<GatherJob> gj(2 * na);
   if (!qb || !tb || !thr || !coll_cnt || !d_rj || !d_bj || (mutual && !flags) || !qbc || !tbc || !rowmap ||
-      !ccount || !d_gj || !qx || !tx || !ones)
+      !ccount || !d_gj || !qx || !tx || !ones || !d_plan)
     return set_error(ctx, PSIFT_ERR_INTERNAL, "match workspace carve overflow");
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ccount, 0, sizeof(int) * 2 * na, st));
   if (mutual) PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * t_rows, st));
@@ -256,14 +244,17 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
       (mutual && (!make_operand_map(&tmTA, tb, t_rows, kTcBM) || !make_operand_map(&tmQB, qb, q_rows, kTcBN) ||
                   !make_operand_map(&tmTAc, tbc, t_rows, kTcBM) || !make_ext_map(&tmQBx, qx, q_rows, kTcBN))))
     return set_error(ctx, PSIFT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-  std::vector<TcItem> items;
   std::vector<TcPair> tcp(2 * na);
   std::vector<RerankJob> rj(2 * na);
+  TcPlan plan[4] = {};
+  int ctas1[2] = {0, 0};
+  const int tc_ctas = target_ctas;  // tile ranges per pass (one CTA each; one resident per SM)
   long long cf = 0;
   // one direction: A rows matched against B rows
-  auto add_problem = [&](int slot, int pair_k, int nA, int nB, const float* an, const float* bn, int splits,
-                         long long a_row0, long long b_row0, float* thr_rows, int* rowmap_rows) {
+  auto add_problem = [&](int slot, int nA, int nB, const float* an, const float* bn, long long a_row0,
+                         long long b_row0, float* thr_rows, int* rowmap_rows) {
     TcPair& T = tcp[slot];
+    std::memset(&T, 0, sizeof T);
     T.ccount = ccount + slot;
     T.rowmap = rowmap_rows;
     T.na = nA;
@@ -272,17 +263,29 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     T.bn = bn;
     T.top2 = top2 + 2 * cf;
     T.thr = thr_rows;
-    T.coll_idx = coll_idx + (long long)kCollRows * cf;
+    T.coll_idx = coll_idx + (long long)kTcColl * cf;
     T.coll_cnt = coll_cnt + cf;
-    T.splits = splits;
-    cf += (long long)splits * nA;
-    const int at = (nA + kTcBM - 1) / kTcBM, bt = (nB + kTcBN - 1) / kTcBN;
-    for (int a = 0; a < at; ++a)
-      for (int sp = 0; sp < splits; ++sp) {
-        const int b0 = (int)((long long)bt * sp / splits), b1 = (int)((long long)bt * (sp + 1) / splits);
-        items.push_back({slot, (int)a_row0 + a * kTcBM, a * kTcBM, (int)b_row0 + b0 * kTcBN, b0 * kTcBN, b1 - b0, sp});
-      }
-    (void)pair_k;
+    cf += (long long)kTcSplits * nA;
+    T.a_row0 = (int)a_row0;
+    T.b_row0 = (int)b_row0;
+    T.bt = (nB + kTcBN - 1) / kTcBN;
+    T.at[0] = (nA + kTcBM - 1) / kTcBM;
+  };
+  // pass 1's tile order of one direction: problems in order, equal ranges over the CTAs
+  auto plan_pass1 = [&](int dir) {
+    long long total = 0;
+    int bt_max = 1;
+    for (int k = 0; k < na; ++k) {
+      TcPair& T = tcp[dir * na + k];
+      T.g0[0] = total;
+      total += (long long)T.at[0] * T.bt;
+      bt_max = std::max(bt_max, T.bt);
+    }
+    long long r = std::max<long long>((total + tc_ctas - 1) / tc_ctas,
+                                      (bt_max - 1 + kTcSplits - 2) / (kTcSplits - 1));
+    r = std::max<long long>(r, 1);
+    plan[2 * dir] = TcPlan{total, (int)r, 0};
+    ctas1[dir] = (int)((total + r - 1) / r);
   };
   for (int k = 0; k < na; ++k) {
     MatchPair& P = pairs[k];
@@ -292,33 +295,33 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     P.tn = tn + t0[k];
     P.tn_max = maxes + k;
     P.qn_max = maxes + na + k;
-    add_problem(k, k, P.nq, P.nt, P.qn, P.tn, tc_split_f[k], q0[k], t0[k], thr + q0[k], rowmap + q0[k]);
+    add_problem(k, P.nq, P.nt, P.qn, P.tn, q0[k], t0[k], thr + q0[k], rowmap + q0[k]);
     const TcPair& T = tcp[k];
     rj[k] = RerankJob{P.q, P.t, P.nq, P.nt, P.qn, P.tn_max, T.top2, thr + q0[k], T.coll_idx, T.coll_cnt,
-                      T.splits, P.best, P.second, P.best_idx, ctx->d_error + 1, opt.ratio,
+                      kTcSplits, P.best, P.second, P.best_idx, ctx->d_error + 1, opt.ratio,
                       mutual ? flags + t0[k] : nullptr};
     rj[k].ccount = ccount + k;
     rj[k].rowmap = rowmap + q0[k];
     gj[k] = GatherJob{qb + (size_t)q0[k] * 128, qbc + (size_t)q0[k] * 128, rowmap + q0[k], ccount + k};
   }
-  const int n_f = (int)items.size();
+  plan_pass1(0);
   if (mutual) {
     for (int k = 0; k < na; ++k) {
       MatchPair& P = pairs[k];
-      add_problem(na + k, k, P.nt, P.nq, P.tn, P.qn, tc_split_r[k], t0[k], q0[k], thr + q_rows + t0[k],
-                  rowmap + q_rows + t0[k]);
+      add_problem(na + k, P.nt, P.nq, P.tn, P.qn, t0[k], q0[k], thr + q_rows + t0[k], rowmap + q_rows + t0[k]);
       const TcPair& T = tcp[na + k];
       rj[na + k] = RerankJob{P.t, P.q, P.nt, P.nq, P.tn, P.qn_max, T.top2, thr + q_rows + t0[k], T.coll_idx,
-                             T.coll_cnt, T.splits, P.col_best, nullptr, P.col_idx, ctx->d_error + 1, opt.ratio,
+                             T.coll_cnt, kTcSplits, P.col_best, nullptr, P.col_idx, ctx->d_error + 1, opt.ratio,
                              flags + t0[k]};
       rj[na + k].ccount = ccount + na + k;
       rj[na + k].rowmap = rowmap + q_rows + t0[k];
       gj[na + k] = GatherJob{tb + (size_t)t0[k] * 128, tbc + (size_t)t0[k] * 128, rowmap + q_rows + t0[k],
                              ccount + na + k};
     }
+    plan_pass1(1);
   }
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(MatchPair) * na, cudaMemcpyHostToDevice, st));
-  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(TcItem) * items.size(), cudaMemcpyHostToDevice, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_plan, plan, sizeof plan, cudaMemcpyHostToDevice, st));
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_tcp, tcp.data(), sizeof(TcPair) * tcp.size(), cudaMemcpyHostToDevice, st));
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_rj, rj.data(), sizeof(RerankJob) * rj.size(), cudaMemcpyHostToDevice, st));
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_gj, gj.data(), sizeof(GatherJob) * gj.size(), cudaMemcpyHostToDevice, st));
@@ -327,13 +330,14 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   {
     for (int k = 0; k < na; ++k) {
       bj[2 * k] = Bf16Job{pairs[k].q, pairs[k].nq, qb + (size_t)q0[k] * 128, qn + q0[k], maxes + na + k,
-                          qx + (size_t)q0[k] * 16, (int)pad_rows(pairs[k].nq)};
+                          qx + (size_t)q0[k] * 16, (int)pad_rows(pairs[k].nq), tcp[k].top2};
       bj[2 * k + 1] = Bf16Job{pairs[k].t, pairs[k].nt, tb + (size_t)t0[k] * 128, tn + t0[k], maxes + k,
-                              tx + (size_t)t0[k] * 16, (int)pad_rows(pairs[k].nt)};
+                              tx + (size_t)t0[k] * 16, (int)pad_rows(pairs[k].nt),
+                              mutual ? tcp[na + k].top2 : nullptr};
       max_a = std::max(max_a, pairs[k].nq);
       max_b = std::max(max_b, pairs[k].nt);
     }
-    bj[2 * na] = Bf16Job{nullptr, 0, nullptr, nullptr, nullptr, ones, kTcBM};
+    bj[2 * na] = Bf16Job{nullptr, 0, nullptr, nullptr, nullptr, ones, kTcBM, nullptr};
     PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(d_bj, bj.data(), sizeof(Bf16Job) * bj.size(), cudaMemcpyHostToDevice, st));
     const int ext_rows = (int)std::max(pad_rows(std::max(max_a, max_b)), (long long)kTcBM);
     cudaError_t e = launch_to_bf16(d_bj, 2 * na + 1, ext_rows, st);
@@ -346,16 +350,17 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     const CUtensorMap& Ac = dir == 0 ? tmQAc : tmTAc;
     const CUtensorMap& B = dir == 0 ? tmTB : tmQB;
     const CUtensorMap& Bx = dir == 0 ? tmTBx : tmQBx;
-    const TcItem* it0 = d_items + (dir == 0 ? 0 : n_f);
-    const int n_it = dir == 0 ? n_f : (int)items.size() - n_f;
+    TcPair* probs = d_tcp + dir * na;
+    TcPlan* pl = d_plan + 2 * dir;
     const RerankJob* jobs_dir = d_rj + dir * na;
     const int rows = dir == 0 ? max_a : max_b;
-    cudaError_t e = launch_match_tc(A, B, tmOnes, Bx, it0, n_it, d_tcp, ctx->d_error, 0, st);
+    cudaError_t e = launch_match_tc(A, B, tmOnes, Bx, probs, na, pl, ctas1[dir], ctx->d_error, 0, st);
     if (e == cudaSuccess) e = launch_window(jobs_dir, na, rows, st);
+    if (e == cudaSuccess) e = launch_tc_plan(probs, na, pl, tc_ctas, st);
     if (e == cudaSuccess) e = launch_gather_rows(d_gj + dir * na, na, rows, st);
-    if (e == cudaSuccess) e = launch_match_tc(Ac, B, tmOnes, Bx, it0, n_it, d_tcp, ctx->d_error, 1, st);
+    if (e == cudaSuccess) e = launch_match_tc(Ac, B, tmOnes, Bx, probs, na, pl, tc_ctas, ctx->d_error, 1, st);
     if (e == cudaSuccess) e = launch_rerank(jobs_dir, na, rows, st);
-    ctx->launches += 5;
+    ctx->launches += 6;
     if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc / window / rerank");
   }
   cudaError_t e = launch_match_emit(d_pairs, na, opt.ratio, mutual, st);
@@ -366,9 +371,9 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
 
 }  // namespace
 
-// Autotuner, matchers: work items per SM in {1, 2, 4, 8} (how many ranges of
-// 256-wide target tiles each query tile is split into follows) for the FP32 and
-// the tensor-core paths, timed on n_pairs problems of n_desc x n_desc SIFT-like
+// Autotuner, matchers: work items per SM in {1, 2, 4, 8} for the FP32 path (how
+// many ranges of target tiles each query tile is split into follows) and the
+// tensor-core path (how many equal tile ranges, one CTA each, a pass is cut into), timed on n_pairs problems of n_desc x n_desc SIFT-like
 // descriptors (|N(0,1)|, L2-normalised, clipped at 0.2, renormalised; seeded);
 // the fastest is kept.  report: per path (path, ms for 1, 2, 4, 8, chosen).
 psift_status autotune_match(psift_ctx* ctx, uint32_t n_desc, uint32_t n_pairs, std::vector<double>& report) {

@@ -32,31 +32,39 @@ struct MatchPair {
   float* qn_max;       // scalar: max query squared norm
 };
 
-// Tensor-core matcher work item: one 128-row A tile x a range of 256-row B tiles.
-struct TcItem {
-  int pair;
-  int a_row;    // first row of the A tile in the concatenated A operand
-  int a_local;  // its index within the pair
-  int b_row;    // first row of the first B tile in the concatenated B operand
-  int b_local;  // its index within the pair
-  int n_tiles;  // B tiles (256 rows each) in this item
-  int split;
-};
+// Tensor-core matcher tiles: 128-row A tiles x 128-row B tiles.  A pass's tiles
+// are ordered (problem, A tile, B tile) and cut into equal ranges, one per CTA;
+// the pieces of one A tile (at most kTcSplits: ranges are at least
+// (B tiles - 1) / (kTcSplits - 1) long) write their partial results into their
+// own slots, merged by window_kernel (pass 1) and rerank_kernel (pass 2).
+constexpr int kTcBM = 128, kTcBN = 128;
+constexpr int kTcSplits = 4;
+constexpr int kTcColl = 32;  // window indices kept per (slot, row)
 
 // Tensor-core matcher problem (A rows matched against B rows).
 struct TcPair {
   int na, nb;
   const float* an;   // f32 squared norms of A rows
   const float* bn;   // f32 squared norms of B rows
-  float* top2;       // pass 1 output: [splits][na][2] two smallest approximate distances
+  float* top2;       // pass 1 output: [kTcSplits][na][2] two smallest approximate distances (+inf: no piece)
   const float* thr;  // pass 2 input: [na] candidate window (-inf: nothing to collect)
-  int* coll_idx;     // pass 2 output: [splits][na][kColl] window indices
-  int* coll_cnt;     // [splits][na] window sizes (may exceed kColl = overflow)
-  int splits;
-  // Pass 2 over the compacted A operand (null: pass 2 runs over every row): the
-  // number of rows window_kernel kept and, per compacted row, its row in the pair.
+  int* coll_idx;     // pass 2 output: [kTcSplits][na][kTcColl] window indices
+  int* coll_cnt;     // [kTcSplits][na] window sizes (may exceed kTcColl = overflow)
+  // Pass 2 runs over the compacted A operand: the number of rows window_kernel
+  // kept and, per compacted row, its row in the problem.
   const int* ccount;
   const int* rowmap;
+  int a_row0, b_row0;  // first rows of the problem in the concatenated A / B operands
+  int bt;              // B tiles
+  int at[2];           // A tiles in pass 1 / pass 2 (pass 2: written by tc_plan_kernel)
+  long long g0[2];     // the problem's first tile in pass 1 / pass 2 order
+};
+
+// Tiles of one pass and the length of each CTA's range.
+struct TcPlan {
+  long long total;
+  int per_cta;
+  int pad;
 };
 
 // Copies the kept rows' bf16 descriptors into the compacted operand (one per
@@ -77,9 +85,9 @@ struct RerankJob {
   const float* bn_max;  // scalar
   const float* top2;    // [splits][na][2]
   float* thr;           // [na]
-  const int* coll_idx;  // [splits][na][kColl]
-  const int* coll_cnt;  // [splits][na]
-  int splits;
+  const int* coll_idx;  // [splits][na][kTcColl]
+  int* coll_cnt;        // [splits][na] (window_kernel clears the slots of the rows it keeps)
+  int splits;           // kTcSplits
   float* best;          // outputs; `second` is null for the reverse (best-only) pass
   float* second;
   int* best_idx;

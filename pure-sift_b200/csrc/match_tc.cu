@@ -41,15 +41,19 @@
 
 namespace psift {
 
-constexpr int kEpiParts = 4;                    // epilogue warps per TMEM lane quarter (column parts)
-constexpr int kEpiWarps = 4 * kEpiParts;        // warps 2 .. 2 + kEpiWarps - 1
+constexpr int kEpiParts = 4;                      // epilogue warps per TMEM lane quarter (32-column parts)
+constexpr int kEpiWarps = 4 * kEpiParts;          // warps 2 .. 2 + kEpiWarps - 1
 constexpr int kTcThreads = 32 * (2 + kEpiWarps);  // warp 0 TMA, warp 1 MMA, then the epilogue
-static_assert(256 / kEpiParts == 64, "the epilogue folds four 16-column TMEM loads per part");
-constexpr int kBM = 128;
-constexpr int kBN = 256;
+constexpr int kBM = kTcBM;
+constexpr int kBN = kTcBN;       // B tile rows = MMA N = columns of one accumulator stage
+constexpr int kAccStages = 4;    // TMEM: four 128 x 128 f32 accumulators (512 columns)
+constexpr int kBStages = 3;      // B tiles in flight
+static_assert(kBN / kEpiParts == 32, "one 32-column TMEM load per epilogue warp and tile");
+static_assert(kAccStages * kBN == 512, "TMEM columns");
 constexpr uint32_t kSpinLimit = 1u << 25;
 constexpr int kColl = 32;   // window indices kept per (split, row)
 constexpr int kXColl = 16;  // window indices a column part 1..3 hands to part 0 (more: exact scan)
+static_assert(kColl == kTcColl, "window list length");
 
 // ---------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -114,7 +118,7 @@ __device__ __forceinline__ uint64_t sw32_desc(uint32_t saddr) {
   return d;
 }
 
-// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=256.
+// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=128.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
                             ((uint32_t)(kBM >> 4) << 24);
 
@@ -132,7 +136,9 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+// 32 columns of a TMEM lane quarter, without waiting: the registers are valid
+// only after tmem_wait32 on them.
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
       "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
@@ -141,69 +147,121 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
         "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// 16 columns of a TMEM lane quarter, without waiting: the registers are valid
-// only after tmem_wait16 on them.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-               : "r"(taddr));
 }
 // Waits for this thread's outstanding TMEM loads; r is tied so that no read of
 // it moves above the wait.
-__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+__device__ __forceinline__ void tmem_wait32(uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;"
-               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                 "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                 "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                 "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
                :
                : "memory");
 }
 
 // Smem map (offsets from a 1024-aligned base).
-constexpr uint32_t kSmA = 0;                      // 2 halves x 128 rows x 128 B = 32 KB
-constexpr uint32_t kSmAx = 32768;                 // A norm extension: 128 rows x 32 B
-constexpr uint32_t kSmB = 36864;                  // 2 stages of: 2 halves x 256 rows x 128 B, then 256 x 32 B
-constexpr uint32_t kSmBStage = 65536 + 8192;
-constexpr uint32_t kSmBar = kSmB + 2 * kSmBStage;  // barriers
+constexpr uint32_t kAStage = 2u * kBM * 128u;                     // two 64-column halves of 128 rows
+constexpr uint32_t kBStage = 2u * kBN * 128u + kBN * 32u;         // two halves, then the norm extension
+constexpr uint32_t kSmA = 0;                                      // 2 A stages
+constexpr uint32_t kSmAx = 2 * kAStage;                           // A norm extension: 128 rows x 32 B
+constexpr uint32_t kSmB = kSmAx + kBM * 32u;                      // kBStages B stages
+constexpr uint32_t kSmBar = kSmB + kBStages * kBStage;            // barriers
 // epilogue exchange, per row and column part 1..kEpiParts-1: pass 1 the part's two
 // largest values, pass 2 its count and up to kXColl indices
 constexpr uint32_t kSmX = kSmBar + 256;
 constexpr uint32_t kSmTotal = kSmX + (kEpiParts - 1) * kBM * (kXColl + 2) * 4 + 1024;  // + alignment slack
+static_assert(kSmB % 1024 == 0 && kBStage % 1024 == 0 && kAStage % 1024 == 0, "128B-swizzle atoms");
 static_assert(kSmTotal <= 227 * 1024, "shared memory per CTA");
 
-__global__ void __launch_bounds__(kTcThreads, 1)
+// The CTA's range of the pass's tiles is cut into pieces, one per A tile it
+// touches: problem k, A tile a, B tiles [b, b + len), and the piece's slot among
+// the A tile's pieces (ranges are R tiles long, R >= (bt - 1) / (kTcSplits - 1),
+// so an A tile meets at most kTcSplits ranges).
+struct Piece {
+  int k, a, b, len, split;
+};
+// The last problem whose first tile is <= g (problems without tiles share their
+// successor's first tile, so the one found has tiles at g).
+__device__ __forceinline__ int find_problem(const TcPair* P, int n, int mode, long long g) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (P[mid].g0[mode] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ Piece make_piece(const TcPair* P, int mode, int R, int k, long long g,
+                                            long long g_end) {
+  Piece p;
+  const int bt = P[k].bt;
+  const long long off = g - P[k].g0[mode];
+  p.k = k;
+  p.a = (int)(off / bt);
+  p.b = (int)(off - (long long)p.a * bt);
+  p.len = (int)min((long long)(bt - p.b), g_end - g);
+  p.split = (int)(g / R - (g - p.b) / R);
+  return p;
+}
+__device__ __forceinline__ int advance_problem(const TcPair* P, int n, int mode, int k, long long g) {
+  while (k + 1 < n && P[k + 1].g0[mode] <= g) ++k;
+  return k;
+}
+
+// Top-2 of a multiset kept as u0 >= u1: merge the pair {d0, d1}.
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ void top2_pair(float& u0, float& u1, float d0, float d1) {
+  const float hi = fmaxf(d0, d1), lo = fminf(d0, d1);
+  u1 = max3f(u1, lo, fminf(u0, hi));
+  u0 = fmaxf(u0, hi);
+}
+
+__global__ void __maxnreg__(112)
     match_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                     const __grid_constant__ CUtensorMap tmAx, const __grid_constant__ CUtensorMap tmBx,
-                    const TcItem* __restrict__ items, const TcPair* __restrict__ pairs, uint32_t* err, int mode) {
+                    const TcPair* __restrict__ P, int n_problems, const TcPlan* __restrict__ plan, uint32_t* err,
+                    int mode) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kSmBar);  // [2]
-  uint64_t* empty = full + 2;                                    // [2]
-  uint64_t* afull = full + 4;                                    // [1]
-  uint64_t* accf = full + 5;                                     // [2]
-  uint64_t* acce = full + 7;                                     // [2]
-  volatile uint32_t* taddr_slot = reinterpret_cast<volatile uint32_t*>(full + 9);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(full + 10);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kSmBar);  // [kBStages] B tile landed
+  uint64_t* empty = full + kBStages;                             // [kBStages] B tile consumed by its MMAs
+  uint64_t* afull = empty + kBStages;                            // [2] A tile landed
+  uint64_t* aempty = afull + 2;                                  // [2] A tile's last MMA done
+  uint64_t* accf = aempty + 2;                                   // [kAccStages] accumulator ready
+  uint64_t* acce = accf + kAccStages;                            // [kAccStages] accumulator read out
+  uint64_t* xfull = acce + kAccStages;                           // [1] A norm extension landed
+  volatile uint32_t* taddr_slot = reinterpret_cast<volatile uint32_t*>(xfull + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(xfull + 2);
 
-  const TcItem it = items[blockIdx.x];
-  const TcPair& PR = pairs[it.pair];
+  // this CTA's tiles [g_begin, g_end) of the pass (pass 2's plan is written on the device)
+  const long long total = plan[mode].total;
+  const int R = plan[mode].per_cta;
+  const long long g_begin = (long long)blockIdx.x * R;
+  if (g_begin >= total) return;
+  const long long g_end = min(total, g_begin + R);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // pass 2 over the compacted rows: a tile past the kept rows has nothing to do
-  const bool compact = mode == 1 && PR.ccount != nullptr;
-  const int n_rows = compact ? *PR.ccount : PR.na;
-  if (it.a_local >= n_rows) return;
+  const bool compact = mode == 1;
 
   if (threadIdx.x == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], 1);
-    mbar_init(&empty[1], 1);
-    mbar_init(afull, 1);
-    mbar_init(&accf[0], 1);
-    mbar_init(&accf[1], 1);
-    mbar_init(&acce[0], kEpiWarps);
-    mbar_init(&acce[1], kEpiWarps);
+    for (int i = 0; i < kBStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&afull[i], 1);
+      mbar_init(&aempty[i], 1);
+    }
+    for (int i = 0; i < kAccStages; ++i) {
+      mbar_init(&accf[i], 1);
+      mbar_init(&acce[i], kEpiWarps);
+    }
+    mbar_init(xfull, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -219,123 +277,175 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *taddr_slot;
-  const int nt = it.n_tiles;
-  // epilogue row state (warps 2..9)
-  const int quarter = warp & 3;
-  const int part = warp >= 2 ? (warp - 2) >> 2 : 0;  // column part of the tile
-  const int row = quarter * 32 + lane;
-  // the row's index in the pair (through the row map when the operand is compacted)
-  const bool row_ok = it.a_local + row < n_rows;
-  const int a_local = compact ? (row_ok ? PR.rowmap[it.a_local + row] : 0) : it.a_local + row;
-  const float inf = __int_as_float(0x7f800000);
-  float u0 = -inf, u1 = -inf;  // mode 0: the two largest D of the row
-  int cnt = 0;                 // mode 1: indices with D >= the row's window bound
-  // exchange slot of (part, row) for parts >= 1
-  int* xrow = reinterpret_cast<int*>(smem + kSmX) + ((part > 0 ? part - 1 : 0) * kBM + row) * (kXColl + 2);
 
   if (warp == 0) {
     if (lane == 0) {
-      // A tile: two 64-column boxes of 128 rows and the constant norm extension
-      mbar_expect_tx(afull, 2u * kBM * 128u + kBM * 32u);
-      tma_load_2d(&tmA, afull, smem + kSmA, 0, it.a_row);
-      tma_load_2d(&tmA, afull, smem + kSmA + kBM * 128, 64, it.a_row);
-      tma_load_2d(&tmAx, afull, smem + kSmAx, 0, 0);
-      for (int j = 0; j < nt; ++j) {
-        const int s = j & 1;
-        const uint32_t use = (uint32_t)(j >> 1);
-        if (!mbar_wait(&empty[s], (use & 1u) ^ 1u, abort_flag)) {
-          atomicOr(err, kErrTimeout);
-          *abort_flag = 1;
+      // the constant A norm extension once, then per piece its A tile and B tiles
+      mbar_expect_tx(xfull, kBM * 32u);
+      tma_load_2d(&tmAx, xfull, smem + kSmAx, 0, 0);
+      uint64_t* last_bar = xfull;  // the last load issued, for the drain on abort
+      uint32_t last_par = 0;
+      bool ok = true;
+      int bs = 0;
+      uint32_t bph = 0;  // B ring slot and its phase
+      long long g = g_begin;
+      int k = find_problem(P, n_problems, mode, g);
+      for (int pi = 0; ok && g < g_end; ++pi) {
+        const Piece pc = make_piece(P, mode, R, k, g, g_end);
+        const int as = pi & 1;
+        if (!mbar_wait(&aempty[as], (((uint32_t)pi >> 1) & 1u) ^ 1u, abort_flag)) {
+          ok = false;
           break;
         }
-        uint8_t* bst = smem + kSmB + s * kSmBStage;
-        mbar_expect_tx(&full[s], 2u * kBN * 128u + kBN * 32u);
-        tma_load_2d(&tmB, &full[s], bst, 0, it.b_row + j * kBN);
-        tma_load_2d(&tmB, &full[s], bst + kBN * 128, 64, it.b_row + j * kBN);
-        tma_load_2d(&tmBx, &full[s], bst + 2 * kBN * 128, 0, it.b_row + j * kBN);
+        const int a_row = P[k].a_row0 + pc.a * kBM;
+        uint8_t* ast = smem + kSmA + as * kAStage;
+        mbar_expect_tx(&afull[as], kAStage);
+        tma_load_2d(&tmA, &afull[as], ast, 0, a_row);
+        tma_load_2d(&tmA, &afull[as], ast + kBM * 128, 64, a_row);
+        last_bar = &afull[as];
+        last_par = ((uint32_t)pi >> 1) & 1u;
+        for (int j = 0; j < pc.len; ++j) {
+          if (!mbar_wait(&empty[bs], bph ^ 1u, abort_flag)) {
+            ok = false;
+            break;
+          }
+          const int b_row = P[k].b_row0 + (pc.b + j) * kBN;
+          uint8_t* bst = smem + kSmB + bs * kBStage;
+          mbar_expect_tx(&full[bs], kBStage);
+          tma_load_2d(&tmB, &full[bs], bst, 0, b_row);
+          tma_load_2d(&tmB, &full[bs], bst + kBN * 128, 64, b_row);
+          tma_load_2d(&tmBx, &full[bs], bst + 2 * kBN * 128, 0, b_row);
+          last_bar = &full[bs];
+          last_par = bph;
+          if (++bs == kBStages) {
+            bs = 0;
+            bph ^= 1u;
+          }
+        }
+        g += pc.len;
+        if (g < g_end) k = advance_problem(P, n_problems, mode, k, g);
+      }
+      if (!ok) {
+        atomicOr(err, kErrTimeout);
+        *abort_flag = 1;
+        // drain: the copies already issued land before the CTA leaves (bounded)
+        for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(last_bar, last_par); ++i) {
+        }
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
+      bool ok = mbar_wait(xfull, 0, abort_flag);
       int issued = 0;
-      bool ok = mbar_wait(afull, 0, abort_flag);
-      for (int j = 0; ok && j < nt; ++j) {
-        const int s = j & 1;
-        const uint32_t use = (uint32_t)(j >> 1);
-        if (!mbar_wait(&full[s], use & 1u, abort_flag) || !mbar_wait(&acce[s], (use & 1u) ^ 1u, abort_flag)) {
+      uint64_t* last_bar = nullptr;
+      uint32_t last_par = 0;
+      int bs = 0, s = 0;
+      uint32_t bph = 0, sph = 0;
+      long long g = g_begin;
+      int k = find_problem(P, n_problems, mode, g);
+      const uint32_t ax = smem_u32(smem + kSmAx);
+      for (int pi = 0; ok && g < g_end; ++pi) {
+        const Piece pc = make_piece(P, mode, R, k, g, g_end);
+        const int as = pi & 1;
+        if (!mbar_wait(&afull[as], ((uint32_t)pi >> 1) & 1u, abort_flag)) {
           ok = false;
           break;
         }
-        tc_fence_after();
-        const uint32_t a_base = smem_u32(smem + kSmA);
-        const uint32_t b_base = smem_u32(smem + kSmB + s * kSmBStage);
-        const uint32_t d = tmem + (uint32_t)(s * kBN);
+        const uint32_t a_base = smem_u32(smem + kSmA + as * kAStage);
+        for (int j = 0; j < pc.len; ++j) {
+          if (!mbar_wait(&full[bs], bph, abort_flag) || !mbar_wait(&acce[s], sph ^ 1u, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t b_base = smem_u32(smem + kSmB + bs * kBStage);
+          const uint32_t d = tmem + (uint32_t)(s * kBN);
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) {
-          const uint32_t half = (uint32_t)(kk >> 2), koff = (uint32_t)(kk & 3) * 32u;
-          umma_bf16(d, sw128_desc(a_base + half * (kBM * 128) + koff), sw128_desc(b_base + half * (kBN * 128) + koff),
-                    kk > 0 ? 1u : 0u);
+          for (int kk = 0; kk < 8; ++kk) {
+            const uint32_t half = (uint32_t)(kk >> 2), koff = (uint32_t)(kk & 3) * 32u;
+            umma_bf16(d, sw128_desc(a_base + half * (kBM * 128) + koff),
+                      sw128_desc(b_base + half * (kBN * 128) + koff), kk > 0 ? 1u : 0u);
+          }
+          // the norm extension: D += h_j + l_j
+          umma_bf16(d, sw32_desc(ax), sw32_desc(b_base + 2 * kBN * 128), 1u);
+          umma_commit(&empty[bs]);
+          umma_commit(&accf[s]);
+          last_bar = &accf[s];
+          last_par = sph;
+          ++issued;
+          if (++bs == kBStages) {
+            bs = 0;
+            bph ^= 1u;
+          }
+          if (++s == kAccStages) {
+            s = 0;
+            sph ^= 1u;
+          }
         }
-        // the norm extension: D += h_j + l_j
-        umma_bf16(d, sw32_desc(smem_u32(smem + kSmAx)), sw32_desc(b_base + 2 * kBN * 128), 1u);
-        umma_commit(&empty[s]);
-        umma_commit(&accf[s]);
-        ++issued;
+        if (!ok) break;
+        umma_commit(&aempty[as]);  // the A stage is free once this piece's MMAs are done
+        g += pc.len;
+        if (g < g_end) k = advance_problem(P, n_problems, mode, k, g);
       }
       if (!ok) {
         atomicOr(err, kErrTimeout);
         *abort_flag = 1;
         // drain: wait (bounded, ignoring the abort flag) for the last issued MMA group
-        if (issued > 0) {
-          const int j = issued - 1;
-          const int s = j & 1;
-          const uint32_t use = (uint32_t)(j >> 1);
-          for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(&accf[s], use & 1u); ++i) {
+        if (issued > 0)
+          for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(last_bar, last_par); ++i) {
           }
-        }
       }
     }
   } else {
-    // epilogue: TMEM lane quarter warp % 4, column part (warp - 2) / 4
-    const float an = row_ok ? PR.an[a_local] : 0.0f;
-    const float thr = (mode == 1 && row_ok) ? PR.thr[a_local] : -inf;
-    // pass 2 window in D: every D with |q|^2 - 2 D <= thr (one f32 rounding) has
-    // D >= (|q|^2 - thr) / 2 - 2^-24 (|q|^2 + |thr|); the margin below is larger
-    const float dthr = thr == -inf ? inf : 0.5f * (an - thr) - 1e-6f * (fabsf(an) + fabsf(thr));
-    // part 0 collects into the row's list, the other parts into their exchange slots
-    int* coll = part == 0 ? PR.coll_idx + ((long long)it.split * PR.na + (row_ok ? a_local : 0)) * kColl
-                          : xrow + 2;
-    const int ccap = part == 0 ? kColl : kXColl;
-    for (int j = 0; j < nt; ++j) {
-      const int s = j & 1;
-      const uint32_t use = (uint32_t)(j >> 1);
-      if (!mbar_wait(&accf[s], use & 1u, abort_flag)) {
-        atomicOr(err, kErrTimeout);
-        *abort_flag = 1;
-        break;
+    // epilogue: TMEM lane quarter warp % 4, 32-column part (warp - 2) / 4 of each tile
+    const int quarter = warp & 3;
+    const int part = (warp - 2) >> 2;
+    const int row_in_tile = quarter * 32 + lane;
+    int* xrow = reinterpret_cast<int*>(smem + kSmX) + ((part > 0 ? part - 1 : 0) * kBM + row_in_tile) * (kXColl + 2);
+    const float inf = __int_as_float(0x7f800000);
+    bool live = true;
+    int s = 0;
+    uint32_t sph = 0;
+    long long g = g_begin;
+    int k = find_problem(P, n_problems, mode, g);
+    while (g < g_end) {
+      const Piece pc = make_piece(P, mode, R, k, g, g_end);
+      const TcPair& PR = P[k];
+      // the previous piece's exchange slots have been merged
+      asm volatile("bar.sync 1, %0;" ::"n"(32 * kEpiWarps) : "memory");
+      const int n_rows = compact ? *PR.ccount : PR.na;
+      const int r = pc.a * kBM + row_in_tile;
+      const bool row_ok = r < n_rows;
+      const int a_local = compact ? (row_ok ? PR.rowmap[r] : 0) : r;
+      const long long o = (long long)pc.split * PR.na + a_local;
+      float u0 = -inf, u1 = -inf, w0 = -inf, w1 = -inf;  // pass 1: two chains of the row's two largest D
+      int cnt = 0;                                       // pass 2: indices with D >= the row's window bound
+      float dthr = inf;
+      int* coll = xrow + 2;
+      int ccap = kXColl;
+      if (mode == 1) {
+        const float an = row_ok ? PR.an[a_local] : 0.0f;
+        const float thr = row_ok ? PR.thr[a_local] : -inf;
+        // every D with |q|^2 - 2 D <= thr (one f32 rounding) has
+        // D >= (|q|^2 - thr) / 2 - 2^-24 (|q|^2 + |thr|); the margin below is larger
+        dthr = thr == -inf ? inf : 0.5f * (an - thr) - 1e-6f * (fabsf(an) + fabsf(thr));
+        if (part == 0) {
+          coll = PR.coll_idx + o * kColl;
+          ccap = kColl;
+        }
       }
-      tc_fence_after();
-      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(s * kBN);
-      const int col0 = it.b_local + j * kBN;
-      // This warp's 64 columns as four 16-column TMEM loads, double-buffered: the
-      // next load is in flight while the current 16 values are folded in.
-      const int cbase = col0 + part * (kBN / kEpiParts);
-      const uint32_t tbase = taddr + (uint32_t)(part * (kBN / kEpiParts));
-      auto fold16 = [&](const uint32_t(&rr)[16], int cstart) {
+      auto fold = [&](const uint32_t(&v)[32], int cstart) {
         if (mode == 0) {
 #pragma unroll
-          for (int q = 0; q < 16; ++q) {
-            const float d = __uint_as_float(rr[q]);
-            const float lo = fminf(u0, d);
-            u0 = fmaxf(u0, d);
-            u1 = fmaxf(u1, lo);
+          for (int q = 0; q < 32; q += 4) {
+            top2_pair(u0, u1, __uint_as_float(v[q]), __uint_as_float(v[q + 1]));
+            top2_pair(w0, w1, __uint_as_float(v[q + 2]), __uint_as_float(v[q + 3]));
           }
         } else {
           // the tests branch-free into a mask, then the (rare) hits in column order
           uint32_t hits = 0;
 #pragma unroll
-          for (int q = 0; q < 16; ++q) hits |= (__uint_as_float(rr[q]) >= dthr ? 1u : 0u) << q;
-          // a row past the kept ones reads stale operand rows: it collects nothing
+          for (int q = 0; q < 32; ++q) hits |= (__uint_as_float(v[q]) >= dthr ? 1u : 0u) << q;
           if (!row_ok) hits = 0;
           while (hits) {
             const int q = __ffs(hits) - 1;
@@ -345,65 +455,94 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           }
         }
       };
-      uint32_t ra[16], rb[16];
-      __syncwarp();
-      tmem_ld16(tbase, ra);
-      tmem_wait16(ra);
-      tmem_ld16(tbase + 16, rb);
-      fold16(ra, cbase);
-      tmem_wait16(rb);
-      tmem_ld16(tbase + 32, ra);
-      fold16(rb, cbase + 16);
-      tmem_wait16(ra);
-      tmem_ld16(tbase + 48, rb);
-      fold16(ra, cbase + 32);
-      tmem_wait16(rb);
-      fold16(rb, cbase + 48);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acce[s]);
-    }
-    if (part > 0) {
-      if (mode == 0) {
-        xrow[0] = __float_as_int(u0);
-        xrow[1] = __float_as_int(u1);
-      } else {
-        xrow[0] = cnt;
+      // Tiles of the piece, two register sets: tile j+1's TMEM load is in flight
+      // while tile j is folded; a stage is released as soon as its values are in
+      // registers.
+      const uint32_t tq = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(part * 32);
+      const int col0 = pc.b * kBN + part * 32;
+      uint32_t ra[32], rb[32];
+      auto acquire = [&](uint32_t(&rr)[32]) {
+        if (live && !__all_sync(0xffffffffu, mbar_wait(&accf[s], sph, abort_flag))) {
+          live = false;
+          atomicOr(err, kErrTimeout);
+          *abort_flag = 1;
+        }
+        if (live) {
+          tc_fence_after();
+          __syncwarp();
+          tmem_ld32_nowait(tq + (uint32_t)(s * kBN), rr);
+        }
+      };
+      auto release = [&](uint32_t(&rr)[32]) {
+        if (live) {
+          tmem_wait32(rr);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[s]);
+        }
+        if (++s == kAccStages) {
+          s = 0;
+          sph ^= 1u;
+        }
+      };
+      acquire(ra);
+      release(ra);
+      for (int j = 0; j < pc.len; j += 2) {
+        if (j + 1 < pc.len) acquire(rb);
+        if (live) fold(ra, col0 + j * kBN);
+        if (j + 1 >= pc.len) break;
+        release(rb);
+        if (j + 2 < pc.len) acquire(ra);
+        if (live) fold(rb, col0 + (j + 1) * kBN);
+        if (j + 2 < pc.len) release(ra);
       }
+      if (mode == 0) {
+        u1 = max3f(u1, w1, fminf(u0, w0));
+        u0 = fmaxf(u0, w0);
+      }
+      if (part > 0) {
+        if (mode == 0) {
+          xrow[0] = __float_as_int(u0);
+          xrow[1] = __float_as_int(u1);
+        } else {
+          xrow[0] = cnt;
+        }
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(32 * kEpiWarps) : "memory");
+      // Part 0 merges the other parts into its row, in part order: the two largest
+      // D of all, mapped to the two smallest a = |q|^2 - 2 D (pass 1), or the
+      // concatenated index lists with the summed count (pass 2; a count above
+      // kColl, or a part that overflowed its kXColl slots, sends the row to the
+      // exact scan).
+      if (part == 0 && row_ok && live) {
+        bool part_overflow = false;
+        for (int p = 1; p < kEpiParts; ++p) {
+          const int* x = reinterpret_cast<const int*>(smem + kSmX) + ((p - 1) * kBM + row_in_tile) * (kXColl + 2);
+          if (mode == 0) {
+            const float x0 = __int_as_float(x[0]), x1 = __int_as_float(x[1]);
+            u1 = max3f(u1, x1, fminf(u0, x0));
+            u0 = fmaxf(u0, x0);
+          } else {
+            const int c1 = x[0];
+            part_overflow |= c1 > kXColl;
+            for (int q = 0; q < c1 && q < kXColl && cnt + q < kColl; ++q) coll[cnt + q] = x[2 + q];
+            cnt += c1;
+          }
+        }
+        if (mode == 0) {
+          const float an = PR.an[a_local];
+          PR.top2[2 * o] = __fmaf_rn(-2.0f, u0, an);
+          PR.top2[2 * o + 1] = __fmaf_rn(-2.0f, u1, an);
+        } else {
+          PR.coll_cnt[o] = part_overflow ? max(cnt, kColl + 1) : cnt;
+        }
+      }
+      g += pc.len;
+      if (g < g_end) k = advance_problem(P, n_problems, mode, k, g);
     }
   }
   tc_fence_before();
   __syncthreads();
-  // Part 0 merges the other parts into its row, in part order: the two largest D
-  // of all, mapped to the two smallest a = |q|^2 - 2 D (pass 1), or the
-  // concatenated index lists with the summed count (pass 2; a count above kColl,
-  // or a part that overflowed its kXColl slots, sends the row to the exact scan).
-  if (warp >= 2 && part == 0 && row_ok) {
-    const long long o = (long long)it.split * PR.na + a_local;
-    int* coll0 = PR.coll_idx + o * kColl;
-    bool part_overflow = false;
-    for (int p = 1; p < kEpiParts; ++p) {
-      const int* x = reinterpret_cast<const int*>(smem + kSmX) + ((p - 1) * kBM + row) * (kXColl + 2);
-      if (mode == 0) {
-        const float w0 = __int_as_float(x[0]), w1 = __int_as_float(x[1]);
-        const float m1 = fmaxf(fminf(u0, w0), fmaxf(u1, w1));
-        u0 = fmaxf(u0, w0);
-        u1 = m1;
-      } else {
-        const int c1 = x[0];
-        part_overflow |= c1 > kXColl;
-        for (int k = 0; k < c1 && k < kXColl && cnt + k < kColl; ++k) coll0[cnt + k] = x[2 + k];
-        cnt += c1;
-      }
-    }
-    if (mode == 0) {
-      const float an = PR.an[a_local];
-      PR.top2[2 * o] = __fmaf_rn(-2.0f, u0, an);
-      PR.top2[2 * o + 1] = __fmaf_rn(-2.0f, u1, an);
-    } else {
-      PR.coll_cnt[o] = part_overflow ? max(cnt, kColl + 1) : cnt;
-    }
-  }
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
@@ -411,11 +550,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 }
 
 // ------------------------------------------------------------ bf16 operands
-// One warp per row: bf16 copy (zero rows for padding are pre-cleared), exact f32
-// squared norm (sequential), running max of the norms, and the row's GEMM norm
-// extension [h, l, 0, ...] with h = bf16(-|x|^2 / 2), l = bf16(-|x|^2 / 2 - h);
-// padding rows up to n_pad get [-inf, 0, ...], which no window or top-2 takes.
-// A job with x = null writes n_pad rows of the A operand's extension [1, 1, 0, ...].
+// Per row: bf16 copy (zero rows for padding are pre-cleared), exact f32 squared
+// norm (sequential), running max of the norms, the row's GEMM norm extension
+// [h, l, 0, ...] with h = bf16(-|x|^2 / 2), l = bf16(-|x|^2 / 2 - h), and its
+// pass-1 result slots set to +inf; padding rows up to n_pad get [-inf, 0, ...],
+// which no window or top-2 takes.  A job with x = null writes n_pad rows of the
+// A operand's extension [1, 1, 0, ...].
 struct Bf16Job {
   const float* x;
   int n;
@@ -424,6 +564,7 @@ struct Bf16Job {
   float* norm_max;
   uint16_t* ext;  // n_pad rows x 16
   int n_pad;
+  float* top2;    // null, or the pass-1 slots [kTcSplits][n][2] of the problem with these A rows: set to +inf
 };
 
 __device__ __forceinline__ uint16_t bf16_rne(float f) {
@@ -431,51 +572,69 @@ __device__ __forceinline__ uint16_t bf16_rne(float f) {
   return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
 }
 
-__global__ void to_bf16_kernel(const Bf16Job* __restrict__ jobs) {
+// A warp per 32 rows: the rows are read coalesced (a float4 per lane and row),
+// written as bf16 and staged in shared memory, then lane j adds up row j's
+// squared norm sequentially from there (the rows' sums run side by side instead
+// of one row's 128 terms being passed lane to lane).
+constexpr int kBf16Warps = 2;  // 33.8 KB of static shared memory per block
+constexpr int kBf16Stride = 132;  // floats per staged row: lanes reading 16 B of different rows hit distinct banks
+
+__global__ void __launch_bounds__(32 * kBf16Warps) to_bf16_kernel(const Bf16Job* __restrict__ jobs) {
+  __shared__ __align__(16) float stage[kBf16Warps][32 * kBf16Stride];
   const Bf16Job& J = jobs[blockIdx.y];
-  const float* __restrict__ x = J.x;
-  uint16_t* __restrict__ out = J.out;
-  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (!x) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row0 = (blockIdx.x * kBf16Warps + warp) * 32;
+  if (row0 >= J.n_pad) return;
+  const int row = row0 + lane;  // this lane's row for the norm and the extension
+  if (!J.x) {
     // the A operand's constant extension rows [1, 1, 0, ...]
-    if (row < J.n_pad && lane < 4)
-      reinterpret_cast<uint2*>(J.ext + (size_t)row * 16)[lane] = make_uint2(lane == 0 ? 0x3F803F80u : 0u, 0u);
+    if (row < J.n_pad) {
+      uint4* e = reinterpret_cast<uint4*>(J.ext + (size_t)row * 16);
+      e[0] = make_uint4(0x3F803F80u, 0u, 0u, 0u);
+      e[1] = make_uint4(0u, 0u, 0u, 0u);
+    }
     return;
   }
-  if (row >= J.n) {
-    if (row < J.n_pad && lane < 4)
-      reinterpret_cast<uint2*>(J.ext + (size_t)row * 16)[lane] = make_uint2(lane == 0 ? 0xFF80u : 0u, 0u);
-    return;
+  const float* __restrict__ x = J.x;
+  float* st = stage[warp];
+  const int nr = min(32, J.n - row0);  // rows with data
+  for (int r = 0; r < nr; ++r) {
+    const float4 v = reinterpret_cast<const float4*>(x + (size_t)(row0 + r) * 128)[lane];
+    uint2 packed;
+    packed.x = (uint32_t)bf16_rne(v.x) | ((uint32_t)bf16_rne(v.y) << 16);  // round to nearest even
+    packed.y = (uint32_t)bf16_rne(v.z) | ((uint32_t)bf16_rne(v.w) << 16);
+    reinterpret_cast<uint2*>(J.out + (size_t)(row0 + r) * 128)[lane] = packed;
+    *reinterpret_cast<float4*>(st + r * kBf16Stride + 4 * lane) = v;
   }
-  const float4 v = reinterpret_cast<const float4*>(x + (size_t)row * 128)[lane];
-  const float e[4] = {v.x, v.y, v.z, v.w};
-  unsigned short b[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) b[i] = bf16_rne(e[i]);  // round to nearest even
-  uint2 packed;
-  packed.x = (uint32_t)b[0] | ((uint32_t)b[1] << 16);
-  packed.y = (uint32_t)b[2] | ((uint32_t)b[3] << 16);
-  reinterpret_cast<uint2*>(out + (size_t)row * 128)[lane] = packed;
-  // exact sequential norm: lane 0 gathers the 128 values in order
-  float s = 0.0f;
-  for (int i = 0; i < 128; ++i) {
-    const float xi = __shfl_sync(0xffffffffu, e[i & 3], i >> 2);
-    s += xi * xi;
-  }
-  if (lane == 0) {
+  __syncwarp();
+  if (row < J.n) {
+    // exact sequential norm of row `row`
+    const float* rr = st + lane * kBf16Stride;
+    float s = 0.0f;
+#pragma unroll 8
+    for (int c = 0; c < 32; ++c) {
+      const float4 v = *reinterpret_cast<const float4*>(rr + 4 * c);
+      s += v.x * v.x;
+      s += v.y * v.y;
+      s += v.z * v.z;
+      s += v.w * v.w;
+    }
     J.norms[row] = s;
     atomicMax(reinterpret_cast<unsigned int*>(J.norm_max), __float_as_uint(s));
-  }
-  if (lane < 4) {
-    uint2 w = make_uint2(0u, 0u);
-    if (lane == 0) {
-      const float half = -0.5f * s;  // exact
-      const uint16_t hi = bf16_rne(half);
-      const uint16_t lo = bf16_rne(half - __uint_as_float((uint32_t)hi << 16));
-      w.x = (uint32_t)hi | ((uint32_t)lo << 16);
-    }
-    reinterpret_cast<uint2*>(J.ext + (size_t)row * 16)[lane] = w;
+    const float half = -0.5f * s;  // exact
+    const uint16_t hi = bf16_rne(half);
+    const uint16_t lo = bf16_rne(half - __uint_as_float((uint32_t)hi << 16));
+    uint4* e = reinterpret_cast<uint4*>(J.ext + (size_t)row * 16);
+    e[0] = make_uint4((uint32_t)hi | ((uint32_t)lo << 16), 0u, 0u, 0u);
+    e[1] = make_uint4(0u, 0u, 0u, 0u);
+    if (J.top2)
+      for (int q = 0; q < 2 * kTcSplits; ++q)
+        J.top2[((size_t)(q >> 1) * J.n + row) * 2 + (q & 1)] = __int_as_float(0x7f800000);
+  } else if (row < J.n_pad) {
+    // padding rows: [-inf, 0, ...], which no window or top-2 takes
+    uint4* e = reinterpret_cast<uint4*>(J.ext + (size_t)row * 16);
+    e[0] = make_uint4(0xFF80u, 0u, 0u, 0u);
+    e[1] = make_uint4(0u, 0u, 0u, 0u);
   }
 }
 
@@ -530,6 +689,8 @@ __global__ void window_kernel(const RerankJob* __restrict__ jobs) {
     if (lo1 > 0.0 && lo1 >= r * r * hi2 * (1.0 + 1e-5)) thr = -inf;
   }
   J.thr[row] = thr;
+  if (thr != -inf)
+    for (int s = 0; s < J.splits; ++s) J.coll_cnt[(long long)s * J.na + row] = 0;  // slots without a piece stay empty
   // rows with a window go to pass 2 (compacted; the order does not matter: every
   // row's collection depends on that row alone and lands in its own slot)
   if (J.ccount && thr != -inf) J.rowmap[atomicAdd(J.ccount, 1)] = row;
@@ -593,6 +754,63 @@ __global__ void rerank_kernel(const RerankJob* __restrict__ jobs) {
   }
 }
 
+// Pass 2's tile order, on the device (the kept row counts are known there): per
+// problem its A tiles (kept rows / 128) and first tile, and the range length of
+// each of `ctas` CTAs, at least (B tiles - 1) / (kTcSplits - 1) so that an A tile
+// meets at most kTcSplits ranges.  One block.
+__global__ void tc_plan_kernel(TcPair* __restrict__ P, int n, TcPlan* __restrict__ plan, int ctas) {
+  __shared__ long long warp_sums[32];
+  __shared__ long long carry;
+  __shared__ int bt_max;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) {
+    carry = 0;
+    bt_max = 1;
+  }
+  __syncthreads();
+  for (int base = 0; base < n; base += blockDim.x) {
+    const int k = base + tid;
+    long long tiles = 0;
+    if (k < n) {
+      const int at = (*P[k].ccount + kTcBM - 1) / kTcBM;
+      P[k].at[1] = at;
+      tiles = (long long)at * P[k].bt;
+      if (at > 0) atomicMax(&bt_max, P[k].bt);
+    }
+    // block-wide exclusive scan of the tile counts
+    long long v = tiles;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const long long u = __shfl_up_sync(0xffffffffu, v, off);
+      if (lane >= off) v += u;
+    }
+    if (lane == 31) warp_sums[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+      long long w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const long long u = __shfl_up_sync(0xffffffffu, w, off);
+        if (lane >= off) w += u;
+      }
+      warp_sums[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const long long before = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + v - tiles;
+    if (k < n) P[k].g0[1] = before;
+    __syncthreads();
+    if (tid == 0) carry += warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const long long total = carry;
+    long long r = (total + ctas - 1) / ctas;
+    r = max(r, (long long)((bt_max - 1 + kTcSplits - 2) / (kTcSplits - 1)));
+    plan[1].total = total;
+    plan[1].per_cta = (int)max(r, 1LL);
+  }
+}
+
 // ------------------------------------------------------------------- host
 namespace {
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -640,17 +858,24 @@ bool make_ext_map(CUtensorMap* tm, const void* base, long long rows, int box_row
 
 cudaError_t launch_to_bf16(const void* jobs, int n_jobs, int max_rows, cudaStream_t st) {
   if (n_jobs <= 0 || max_rows <= 0) return cudaSuccess;
-  dim3 grid((max_rows + 7) / 8, n_jobs);
-  to_bf16_kernel<<<grid, 256, 0, st>>>((const Bf16Job*)jobs);
+  dim3 grid((max_rows + 32 * kBf16Warps - 1) / (32 * kBf16Warps), n_jobs);
+  to_bf16_kernel<<<grid, 32 * kBf16Warps, 0, st>>>((const Bf16Job*)jobs);
   return cudaGetLastError();
 }
 
 cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, const CUtensorMap& tmAx,
-                            const CUtensorMap& tmBx, const TcItem* items, int n_items, const TcPair* pairs,
-                            uint32_t* err, int mode, cudaStream_t st) {
+                            const CUtensorMap& tmBx, const TcPair* problems, int n_problems, const TcPlan* plan,
+                            int ctas, uint32_t* err, int mode, cudaStream_t st) {
+  if (ctas <= 0 || n_problems <= 0) return cudaSuccess;
   cudaError_t e = ensure_smem_attr((const void*)match_tc_kernel, kSmTotal);
   if (e != cudaSuccess) return e;
-  match_tc_kernel<<<n_items, kTcThreads, kSmTotal, st>>>(tmA, tmB, tmAx, tmBx, items, pairs, err, mode);
+  match_tc_kernel<<<ctas, kTcThreads, kSmTotal, st>>>(tmA, tmB, tmAx, tmBx, problems, n_problems, plan, err, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_plan(TcPair* problems, int n_problems, TcPlan* plan, int ctas, cudaStream_t st) {
+  if (n_problems <= 0) return cudaSuccess;
+  tc_plan_kernel<<<1, 1024, 0, st>>>(problems, n_problems, plan, ctas);
   return cudaGetLastError();
 }
 

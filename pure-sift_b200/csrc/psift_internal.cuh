@@ -87,7 +87,7 @@ struct psift_ctx {
   // tensor-core path).  gen changes with them (part of the graph cache key).
   struct Tuning {
     int8_t blur[16] = {0};
-    int8_t match_per_sm[2] = {2, 2};
+    int8_t match_per_sm[2] = {2, 1};
     uint32_t gen = 0;
   } tune;
   // Single-rounding blur mode (psift_ctx_set_blur_rounding); part of the graph

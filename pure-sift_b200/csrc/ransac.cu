@@ -13,7 +13,7 @@
 // Identical results for the same seed.  The random stream does not depend on
 // the data except through the CDF, so samples are drawn ahead: splitmix64's
 // state advances by a constant, draw t is a pure function of (seed, t).
-// Hypotheses are generated and fitted 64 at a time: a quad of lanes per
+// Hypotheses are generated and fitted 32 at a time: a quad of lanes per
 // homography fit (f64 DLT; the cyclic Jacobi's rotations shared by the quad in
 // shared memory, each lane updating rows ql, ql + 4, ql + 8, so every value is
 // the sequential solver's), then counted by warps (two hypotheses per pass over
@@ -35,9 +35,14 @@
 
 namespace psift {
 
-constexpr int kRThreads = 256;
+// 128 threads and 32 hypotheses per batch: the serial parts (replay, sequential
+// sums, the Jacobi of a refit) leave most of a CTA idle, so four CTAs per SM
+// (128 registers, ~51 KB of shared memory each) overlap more match sets.
+constexpr int kRThreads = 128;
 constexpr int kRWarps = kRThreads / 32;
-constexpr int kBatch = 64;
+constexpr int kBatch = 32;
+constexpr int kRCtasPerSm = 4;
+static_assert(kBatch * 4 == kRThreads, "a quad of lanes per hypothesis fit");
 constexpr int kDrawChunk = kBatch * 16;
 // Jacobi matrix and eigenvectors (81 doubles each) of every hypothesis of a batch
 constexpr size_t kJacSmem = sizeof(double) * 162 * kBatch;
@@ -1029,7 +1034,7 @@ __device__ void local_optimize(const RansacJob& J, RShared& S, double* jac, doub
   }
 }
 
-__global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(kRThreads, kRCtasPerSm) ransac_kernel(const RansacJob* __restrict__ jobs) {
   __shared__ RShared S;
   extern __shared__ double jac[];
   const RansacJob& J = jobs[blockIdx.x];
@@ -1113,19 +1118,25 @@ __global__ void __launch_bounds__(kRThreads) ransac_kernel(const RansacJob* __re
         S.draws_ready = need < draw_cap ? need : draw_cap;
         int p = S.draw_ptr;
         for (int h = 0; h < kBatch; ++h) {
+          // distinct draws in order, held in registers (q0 first)
           int chosen = 0, attempts = 0;
-          int q[4] = {0, 0, 0, 0};
+          int q0 = 0, q1 = 0, q2 = 0, q3 = 0;
           while (chosen < 4 && attempts < 16) {
             ++attempts;
             const int c = S.draws_s[(p++) % (2 * kDrawChunk)];
-            bool dup = false;
-            for (int j = 0; j < chosen; ++j) dup |= q[j] == c;
-            if (!dup) q[chosen++] = c;
+            const bool dup = (chosen > 0 && q0 == c) || (chosen > 1 && q1 == c) || (chosen > 2 && q2 == c);
+            if (!dup) {
+              if (chosen == 0) q0 = c;
+              else if (chosen == 1) q1 = c;
+              else if (chosen == 2) q2 = c;
+              else q3 = c;
+              ++chosen;
+            }
           }
-          S.quad[h][0] = q[0];
-          S.quad[h][1] = q[1];
-          S.quad[h][2] = q[2];
-          S.quad[h][3] = q[3];
+          S.quad[h][0] = q0;
+          S.quad[h][1] = q1;
+          S.quad[h][2] = q2;
+          S.quad[h][3] = q3;
           S.hvalid[h] = chosen == 4 ? 1 : 0;
         }
         S.draw_ptr = p;
