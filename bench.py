@@ -722,6 +722,36 @@ def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int =
     }
 
 
+def pyramid_bench(ctx, torch, blur: str = "reference", reps: int = 5):
+    """One 1080p image through psift.build_pyramid (the gaussian_blur chain, DoG and
+    decimation of build_scale_space_pyramid_with_options, 4 octaves with the 2x
+    upsampled base): device time of the call's launches with CUDA events on the
+    context's stream, host wall clock with the planes' download; the rounding mode
+    of the blur taps as given.  Also the profiling case of the level blur (the
+    first launch per octave of each radius, e.g. the R = 10 level of octave 0)."""
+    import psift
+    img = synth.blob_image(WIDTH, HEIGHT, 2000, 1.5, 20.0, seed=7).astype(np.float32) / 255.0
+    cfg = psift.SiftConfig().with_octaves(4).with_contrast_threshold(0.015)
+    ctx.set_blur_rounding(ctx.BLUR_FUSED if blur == "fused" else ctx.BLUR_REFERENCE)
+    try:
+        for _ in range(2):
+            psift.build_pyramid(img, cfg, ctx=ctx)
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        ctx.enable_stage_timing(True)
+        ctx.stage_times(reset=True)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            psift.build_pyramid(img, cfg, ctx=ctx)
+        wall = (time.perf_counter() - t0) / reps
+        st = ctx.stage_times(reset=True)
+        ctx.enable_stage_timing(False)
+    finally:
+        ctx.set_blur_rounding(ctx.BLUR_REFERENCE)
+    del stream
+    return {"workload": f"{WIDTH}x{HEIGHT} blob image, 4 octaves, scales 3, upsampled base (3840x2160 octave 0)",
+            "blur": blur, "device_pyramid_ms": st["pyramid"][0] / reps, "host_api_ms_with_download": wall * 1e3}
+
+
 def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
     """Input step: 8 colour 1920x1080 JPEGs (three independent 2000-blob fields as
     R, G, B; 4:2:0, quality 90) in host memory -> features in host memory through
@@ -1123,7 +1153,7 @@ def main():
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
     ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "warp", "fundamental",
-                                               "learned_ransac", "uneven_batch", "jpeg", "panorama"],
+                                               "learned_ransac", "uneven_batch", "jpeg", "panorama", "pyramid"],
                     help="run one section alone (profiling case)")
     ap.add_argument("--ransac-pairs", type=int, default=1024, help="learned-RANSAC section: match sets")
     ap.add_argument("--blur", choices=["reference", "fused"], default="reference",
@@ -1161,7 +1191,8 @@ def main():
                "catalog_search": lambda: catalog_search_bench(ctx, torch, n_entries=args.catalog_entries), "warp": lambda: warp_bench(ctx, torch),
                "fundamental": lambda: fundamental_bench(ctx, torch),
                "uneven_batch": lambda: uneven_bench(ctx, torch), "jpeg": lambda: jpeg_bench(ctx, torch),
-               "panorama": lambda: panorama_bench(ctx, torch)}
+               "panorama": lambda: panorama_bench(ctx, torch),
+               "pyramid": lambda: pyramid_bench(ctx, torch, blur=args.blur, reps=min(args.steps, 10))}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)
         ctx.close()
         return 0

@@ -241,6 +241,29 @@ psift_status psift_decode_jpeg_luma(psift_ctx* ctx, const uint8_t* data, size_t 
 psift_status psift_detect_and_compute_jpeg_batch(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths,
                                                  uint32_t n, int32_t enforce_pixel_cap,
                                                  const psift_sift_config* cfg, psift_features* outs);
+/* PNG input (decode_validated_luma8 with the image crate's PNG decoder,
+ * src/cli.rs:129-170): the header checks and messages as for JPEG; every
+ * chunk's CRC is checked; colour types 0, 2, 3, 4, 6 at all their bit depths,
+ * Adam7 interlacing.  The zlib stream is inflated on host threads; the row
+ * filters are undone and the samples converted to luma on the GPU (into_luma8:
+ * rgb_to_luma on 8- or 16-bit samples, 16-bit results to u8 by rounding,
+ * alpha dropped, palettes and low bit depths expanded).  Lossless: the luma
+ * equals the reference's.  components = channels (1, 2, 3 or 4). */
+psift_status psift_png_info(psift_ctx* ctx, const uint8_t* data, size_t length, int32_t enforce_pixel_cap,
+                            uint32_t* width, uint32_t* height, uint32_t* components);
+/* One PNG to host u8 luma (width x height, dense rows; capacity in bytes). */
+psift_status psift_decode_png_luma(psift_ctx* ctx, const uint8_t* data, size_t length, int32_t enforce_pixel_cap,
+                                   uint8_t* luma, size_t capacity, uint32_t* width, uint32_t* height);
+/* The extract path from n PNG buffers (host), as psift_detect_and_compute_jpeg_batch. */
+psift_status psift_detect_and_compute_png_batch(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths,
+                                                uint32_t n, int32_t enforce_pixel_cap,
+                                                const psift_sift_config* cfg, psift_features* outs);
+/* The extract path from n image buffers of either format, told apart by their
+ * leading bytes (the PNG signature, else JPEG): each format's batch entry over
+ * its images, features into outs[i] in the callers' order. */
+psift_status psift_detect_and_compute_image_batch(psift_ctx* ctx, const uint8_t* const* data, const size_t* lengths,
+                                                  uint32_t n, int32_t enforce_pixel_cap,
+                                                  const psift_sift_config* cfg, psift_features* outs);
 /* How a context decodes a JPEG batch.  threads = 0 (default): the batch is split
  * into contiguous shares of at most 50 images over up to 16 host threads (the
  * hardware concurrency), each share decoded by nvJPEG's hybrid backend (Huffman

@@ -68,15 +68,23 @@ cudaError_t resident_ctas(const void* func, int threads, size_t smem, int* out) 
 cudaError_t ensure_smem_attr(const void* func, size_t bytes) {
   // The attribute is an upper bound: only ever raise it (a lower value set for a
   // small launch would make a later, larger launch fail).
+  // Static plus dynamic shared memory above 48 KB needs the opt-in.
   static std::mutex mu;
   static std::map<std::pair<const void*, int>, size_t> limit;
-  if (bytes <= 48 * 1024) return cudaSuccess;
+  if (bytes == 0) return cudaSuccess;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(mu);
   auto it = limit.find({func, dev});
   if (it != limit.end() && it->second >= bytes) return cudaSuccess;
+  cudaFuncAttributes fa;
+  e = cudaFuncGetAttributes(&fa, func);
+  if (e != cudaSuccess) return e;
+  if (fa.sharedSizeBytes + bytes <= 48 * 1024) {
+    limit[{func, dev}] = bytes;
+    return cudaSuccess;
+  }
   e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e == cudaSuccess) limit[{func, dev}] = bytes;
   return e;
@@ -231,6 +239,7 @@ psift_status psift_ctx_destroy(psift_ctx* ctx) {
   if (ctx->pinned.base) cudaFreeHost(ctx->pinned.base);
   if (ctx->d_error) cudaFree(ctx->d_error);
   psift::jpeg_release(ctx);
+  psift::png_release(ctx);
   for (auto& p : ctx->timer.pending) {
     cudaEventDestroy(p.second.first);
     cudaEventDestroy(p.second.second);

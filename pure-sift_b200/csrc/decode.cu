@@ -34,9 +34,6 @@
 namespace psift {
 namespace {
 
-constexpr uint32_t kMinImageDim = 8;            // MIN_IMAGE_DIM, src/cli.rs:46
-constexpr uint32_t kMaxImageDim = 8192;         // MAX_IMAGE_DIM, src/cli.rs:47
-constexpr uint64_t kMaxImagePixels = 25000000;  // MAX_IMAGE_PIXELS, src/cli.rs:48
 
 struct NvjpegApi {
   bool tried = false, ok = false;
@@ -256,20 +253,7 @@ psift_status read_header(psift_ctx* ctx, const uint8_t* data, size_t len, bool e
   d->w = (uint32_t)ws[0];
   d->h = (uint32_t)hs[0];
   d->comps = (uint32_t)nc;
-  if (d->w < kMinImageDim || d->h < kMinImageDim)
-    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
-                     "Image dimensions " + std::to_string(d->w) + "x" + std::to_string(d->h) +
-                         " are too small (minimum 8x8)");
-  const uint64_t total = (uint64_t)d->w * d->h;
-  if (total > (1ull << 31))
-    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
-                     "Image dimensions " + std::to_string(d->w) + "x" + std::to_string(d->h) +
-                         " exceed 2^31 pixels");
-  if (enforce_cap && (d->w > kMaxImageDim || d->h > kMaxImageDim || total > kMaxImagePixels))
-    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
-                     "Image dimensions " + std::to_string(d->w) + "x" + std::to_string(d->h) + " (" +
-                         std::to_string(total) + " px) exceed maximum allowed (8192x8192, 25000000 px)");
-  return PSIFT_OK;
+  return check_image_dims(ctx, d->w, d->h, enforce_cap);
 }
 
 // Decodes n JPEGs (host bytes) and writes their luma to luma[i] (dense rows) on st.
@@ -343,6 +327,27 @@ psift_status decode_range(psift_ctx* ctx, const uint8_t* const* data, const size
 }
 
 }  // namespace
+
+// The reference's size checks of a decoded image's header (src/cli.rs:137-158):
+// MIN_IMAGE_DIM, and MAX_IMAGE_DIM / MAX_IMAGE_PIXELS when the cap is enforced.
+psift_status check_image_dims(psift_ctx* ctx, uint32_t w, uint32_t h, bool enforce_cap) {
+  constexpr uint32_t kMinImageDim = 8;            // MIN_IMAGE_DIM, src/cli.rs:46
+  constexpr uint32_t kMaxImageDim = 8192;         // MAX_IMAGE_DIM, src/cli.rs:47
+  constexpr uint64_t kMaxImagePixels = 25000000;  // MAX_IMAGE_PIXELS, src/cli.rs:48
+  if (w < kMinImageDim || h < kMinImageDim)
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
+                     "Image dimensions " + std::to_string(w) + "x" + std::to_string(h) +
+                         " are too small (minimum 8x8)");
+  const uint64_t total = (uint64_t)w * h;
+  if (total > (1ull << 31))
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
+                     "Image dimensions " + std::to_string(w) + "x" + std::to_string(h) + " exceed 2^31 pixels");
+  if (enforce_cap && (w > kMaxImageDim || h > kMaxImageDim || total > kMaxImagePixels))
+    return set_error(ctx, PSIFT_ERR_INVALID_ARGUMENT,
+                     "Image dimensions " + std::to_string(w) + "x" + std::to_string(h) + " (" +
+                         std::to_string(total) + " px) exceed maximum allowed (8192x8192, 25000000 px)");
+  return PSIFT_OK;
+}
 
 void jpeg_release(psift_ctx* ctx) {
   if (!ctx->jpeg) return;

@@ -163,8 +163,9 @@ __device__ int jacobi_step(double (&a)[N][N], double (&v)[N][N], double tol) {
   if (max_off < tol) return 0;
   const double app = a[p][p], aqq = a[q][q], apq = a[p][q];
   const double tau = (aqq - app) / (2.0 * apq);
-  const double t = tau >= 0.0 ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
-  const double c = 1.0 / sqrt(1.0 + t * t);
+  // __drcp_rn(x) is 1.0 / x: both are IEEE round-to-nearest, the reciprocal is the cheaper sequence
+  const double t = tau >= 0.0 ? __drcp_rn(tau + sqrt(1.0 + tau * tau)) : -__drcp_rn(-tau + sqrt(1.0 + tau * tau));
+  const double c = __drcp_rn(sqrt(1.0 + t * t));
   const double s = t * c;
   a[p][p] = app - t * apq;
   a[q][q] = aqq + t * apq;
@@ -412,8 +413,8 @@ __device__ bool quad_jacobi(double* A, double* V, int ql, unsigned qmask) {
     const int q = p + 1 + rem;
     const double app = A[p * 9 + p], aqq = A[q * 9 + q], apq = A[p * 9 + q];
     const double tau = (aqq - app) / (2.0 * apq);
-    const double t = tau >= 0.0 ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
-    const double c = 1.0 / sqrt(1.0 + t * t);
+    const double t = tau >= 0.0 ? __drcp_rn(tau + sqrt(1.0 + tau * tau)) : -__drcp_rn(-tau + sqrt(1.0 + tau * tau));
+    const double c = __drcp_rn(sqrt(1.0 + t * t));
     const double s = t * c;
     __syncwarp(qmask);  // every pivot read precedes the writes
     if (ql == 0) {

@@ -109,48 +109,59 @@ __global__ void quantize_kernel(const float* __restrict__ desc, int n, uint64_t*
 }
 
 // dequantize_descriptor_u8: v/512 then L2 renormalisation (sequential sum).  A
-// warp per 32 rows: the u8 rows are read coalesced and staged in shared memory
-// as f32, lane j adds up row j's squared norm sequentially, and the scaled rows
-// are written back coalesced (a float4 per lane and row).
-constexpr int kDqWarps = 2;  // 33.8 KB of static shared memory per block
-constexpr int kDqStride = 132;  // floats per staged row (conflict-free 16-byte reads across rows)
+// warp per 32 rows: the u8 rows are copied into shared memory (16-byte
+// asynchronous copies, all in flight together), lane j adds up row j's squared
+// norm sequentially from there, and the scaled rows are written back coalesced
+// (a float4 per lane and row).
+constexpr int kDqWarps = 4;
+constexpr int kDqStride = 144;  // bytes per staged row: lanes reading 16 B of different rows hit distinct banks
+
+__device__ __forceinline__ float4 dq4(uint32_t p) {
+  return make_float4((float)(p & 0xFF) * (1.0f / 512.0f), (float)((p >> 8) & 0xFF) * (1.0f / 512.0f),
+                     (float)((p >> 16) & 0xFF) * (1.0f / 512.0f), (float)(p >> 24) * (1.0f / 512.0f));
+}
 
 __global__ void __launch_bounds__(32 * kDqWarps) dequantize_kernel(const uint8_t* __restrict__ q, int n,
                                                                    float* __restrict__ out) {
-  __shared__ __align__(16) float stage[kDqWarps][32 * kDqStride];
+  __shared__ __align__(16) uint8_t stage[kDqWarps][32 * kDqStride];
   __shared__ float inv_s[kDqWarps][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row0 = (blockIdx.x * kDqWarps + warp) * 32;
   if (row0 >= n) return;
   const int nr = min(32, n - row0);
-  float* st = stage[warp];
-  for (int r = 0; r < nr; ++r) {
-    const uint32_t p = reinterpret_cast<const uint32_t*>(q + (size_t)(row0 + r) * 128)[lane];
-    float4 v;
-    v.x = (float)(p & 0xFF) * (1.0f / 512.0f);
-    v.y = (float)((p >> 8) & 0xFF) * (1.0f / 512.0f);
-    v.z = (float)((p >> 16) & 0xFF) * (1.0f / 512.0f);
-    v.w = (float)(p >> 24) * (1.0f / 512.0f);
-    *reinterpret_cast<float4*>(st + r * kDqStride + 4 * lane) = v;
+  uint8_t* st = stage[warp];
+  // the warp's rows as 16-byte pieces: piece t of the block is row t / 8, bytes 16 (t % 8)
+  for (int t = lane; t < nr * 8; t += 32) {
+    const int r = t >> 3, c = (t & 7) * 16;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(st + r * kDqStride + c)),
+                 "l"(q + (size_t)(row0 + r) * 128 + c)
+                 : "memory");
   }
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
   __syncwarp();
   if (lane < nr) {
-    const float* rr = st + lane * kDqStride;
+    const uint8_t* rr = st + lane * kDqStride;
     float s = 0.0f;
-#pragma unroll 8
-    for (int c = 0; c < 32; ++c) {
-      const float4 v = *reinterpret_cast<const float4*>(rr + 4 * c);
-      s += v.x * v.x;
-      s += v.y * v.y;
-      s += v.z * v.z;
-      s += v.w * v.w;
+#pragma unroll 2
+    for (int c = 0; c < 8; ++c) {
+      const uint4 w = *reinterpret_cast<const uint4*>(rr + 16 * c);
+      const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float4 v = dq4(ws[k]);
+        s += v.x * v.x;
+        s += v.y * v.y;
+        s += v.z * v.z;
+        s += v.w * v.w;
+      }
     }
     const float norm = sqrtf(s);
     inv_s[warp][lane] = norm > 1e-7f ? 1.0f / norm : 1.0f;  // 1: the row is kept as it is
   }
   __syncwarp();
   for (int r = 0; r < nr; ++r) {
-    float4 v = *reinterpret_cast<const float4*>(st + r * kDqStride + 4 * lane);
+    float4 v = dq4(*reinterpret_cast<const uint32_t*>(st + r * kDqStride + 4 * lane));
     const float inv = inv_s[warp][r];
     if (inv != 1.0f) {
       v.x *= inv;

@@ -354,14 +354,16 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     TcPlan* pl = d_plan + 2 * dir;
     const RerankJob* jobs_dir = d_rj + dir * na;
     const int rows = dir == 0 ? max_a : max_b;
+    const char* what = "match_tc pass 1";
     cudaError_t e = launch_match_tc(A, B, tmOnes, Bx, probs, na, pl, ctas1[dir], ctx->d_error, 0, st);
-    if (e == cudaSuccess) e = launch_window(jobs_dir, na, rows, st);
-    if (e == cudaSuccess) e = launch_tc_plan(probs, na, pl, tc_ctas, st);
-    if (e == cudaSuccess) e = launch_gather_rows(d_gj + dir * na, na, rows, st);
-    if (e == cudaSuccess) e = launch_match_tc(Ac, B, tmOnes, Bx, probs, na, pl, tc_ctas, ctx->d_error, 1, st);
-    if (e == cudaSuccess) e = launch_rerank(jobs_dir, na, rows, st);
+    if (e == cudaSuccess && (what = "window", true)) e = launch_window(jobs_dir, na, rows, st);
+    if (e == cudaSuccess && (what = "tc_plan", true)) e = launch_tc_plan(probs, na, pl, tc_ctas, st);
+    if (e == cudaSuccess && (what = "gather_rows", true)) e = launch_gather_rows(d_gj + dir * na, na, rows, st);
+    if (e == cudaSuccess && (what = "match_tc pass 2", true))
+      e = launch_match_tc(Ac, B, tmOnes, Bx, probs, na, pl, tc_ctas, ctx->d_error, 1, st);
+    if (e == cudaSuccess && (what = "rerank", true)) e = launch_rerank(jobs_dir, na, rows, st);
     ctx->launches += 6;
-    if (e != cudaSuccess) return cuda_error(ctx, e, "match_tc / window / rerank");
+    if (e != cudaSuccess) return cuda_error(ctx, e, what);
   }
   cudaError_t e = launch_match_emit(d_pairs, na, opt.ratio, mutual, st);
   ctx->launches++;

@@ -1,4 +1,4 @@
-// K8: BF16 tcgen05 distance GEMM with a fused top-8 epilogue, and the certified
+// K8: BF16 tcgen05 distance GEMM with a fused top-2 epilogue, and the certified
 // exact FP32 re-rank that makes its match list identical to the FP32 path.
 //
 // Reference: match_descriptors_with_options (src/pipeline.rs:1744-1841).
@@ -13,26 +13,32 @@
 // (bf16 rounding of both operands <= 2^-8 relative per product, the hi/lo split
 // of the norm <= 2^-18 relative, tensor-core f32 accumulation, the f32 norms and
 // the reference's own sequential f32 rounding, all bounded with margin).  a_ij
-// is a non-increasing function of D_ij, so a row's two smallest a are the
-// images of its two largest D, and the epilogue works on D alone.  Every target
-// that can be the exact best or second has a_ij <= a_(2) + 2 eps_i.  Pass 1 of
-// the GEMM keeps each row's two largest D; window_kernel either certifies that
-// the row fails the ratio test (then no exact work is needed) or sets the row's
-// window thr = a_(2) + 2 eps_i; pass 2 (same GEMM, deterministic) collects every
-// index whose D is at least (|q_i|^2 - thr) / 2 less a margin that covers the
-// rounding of a (a superset of {a_ij <= thr}), and the exact reference distances
-// of those candidates give best/second/index equal to the FP32 path bit for bit.
-// A row whose window holds more than kColl indices in one split (or more than
-// kXColl in one column part) is matched by an exact scan of all targets.
+// is a non-increasing function of D_ij, so a row's smallest a are the images of
+// its largest D, and the epilogue works on D alone.  Every target that can be
+// the exact best or second has a_ij <= a_(2) + 2 eps_i.  Pass 1 of the GEMM keeps
+// each row's largest D and a lower bound on its second largest (the second
+// largest of 8 column-class maxima); window_kernel either certifies that the
+// row fails the ratio test (then no exact work is needed) or sets the row's
+// window thr = a'_(2) + 2 eps_i >= a_(2) + 2 eps_i; pass 2 (same GEMM,
+// deterministic) collects every index whose D is at least (|q_i|^2 - thr) / 2
+// less a margin that covers the rounding of a (a superset of {a_ij <= thr}), and
+// the exact reference distances of those candidates give best/second/index
+// equal to the FP32 path bit for bit.  A row whose window holds more than kColl
+// indices in one slot (or more than kXColl in one column part) is matched by an
+// exact scan of all targets.
 //
-// Kernel structure (one CTA = one 128-row A tile x a range of 256-row B tiles,
-// 576 threads): warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
-// operand tile plus the 16-column norm extension with SWIZZLE_32B,
-// double-buffered B), warp 1 owns TMEM (512 columns = two 128x256 f32
-// accumulators) and issues tcgen05.mma (M=128, N=256, K=16; nine per tile) from
-// one thread, warps 2-17 read the accumulators with tcgen05.ld (four warps per
-// TMEM lane quarter, one per 64-column part of the tile; the parts are merged per
-// row at the end).  All waits are bounded: on timeout the CTA records
+// Kernel structure: persistent, one CTA per SM, 576 threads.  A pass's tiles
+// (128-row A tile x 128-row B tile, ordered problem, A tile, B tile) are cut into
+// equal ranges, one per CTA; each range is walked as pieces (one A tile's run of
+// B tiles).  Warp 0 issues TMA loads (SWIZZLE_128B, two 64-column boxes per
+// operand tile plus the 16-column norm extension with SWIZZLE_32B; A tiles
+// double-buffered, B tiles in a ring of three), warp 1 owns TMEM (512 columns =
+// four 128x128 f32 accumulators) and issues tcgen05.mma (M=128, N=128, K=16;
+// nine per tile) from one thread, warps 2-17 read the accumulators with
+// tcgen05.ld (four warps per TMEM lane quarter, one per 32-column part; the next
+// tile's load in flight while the current one is folded, each accumulator
+// released as soon as it is in registers; the parts are merged per row at the
+// end of a piece).  All waits are bounded: on timeout the CTA records
 // kErrTimeout, stops issuing, drains what it issued and frees its TMEM.
 #include <cuda.h>
 
@@ -222,11 +228,14 @@ __device__ __forceinline__ void top2_pair(float& u0, float& u1, float d0, float 
   u0 = fmaxf(u0, hi);
 }
 
-__global__ void __maxnreg__(112)
+// MODE 0: pass 1 (top-2 per row); MODE 1: pass 2 (window collection over the
+// compacted rows).
+template <int MODE>
+__global__ void __launch_bounds__(kTcThreads, 1)
     match_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                     const __grid_constant__ CUtensorMap tmAx, const __grid_constant__ CUtensorMap tmBx,
-                    const TcPair* __restrict__ P, int n_problems, const TcPlan* __restrict__ plan, uint32_t* err,
-                    int mode) {
+                    const TcPair* __restrict__ P, int n_problems, const TcPlan* __restrict__ plan, uint32_t* err) {
+  constexpr int mode = MODE;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kSmBar);  // [kBStages] B tile landed
@@ -418,12 +427,16 @@ __global__ void __maxnreg__(112)
       const bool row_ok = r < n_rows;
       const int a_local = compact ? (row_ok ? PR.rowmap[r] : 0) : r;
       const long long o = (long long)pc.split * PR.na + a_local;
-      float u0 = -inf, u1 = -inf, w0 = -inf, w1 = -inf;  // pass 1: two chains of the row's two largest D
-      int cnt = 0;                                       // pass 2: indices with D >= the row's window bound
+      // pass 1: the largest D of each of 8 column classes (column mod 8), one
+      // three-input max per two values
+      float cm[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) cm[q] = -inf;
+      int cnt = 0;  // pass 2: indices with D >= the row's window bound
       float dthr = inf;
       int* coll = xrow + 2;
       int ccap = kXColl;
-      if (mode == 1) {
+      if constexpr (mode == 1) {
         const float an = row_ok ? PR.an[a_local] : 0.0f;
         const float thr = row_ok ? PR.thr[a_local] : -inf;
         // every D with |q|^2 - 2 D <= thr (one f32 rounding) has
@@ -435,11 +448,11 @@ __global__ void __maxnreg__(112)
         }
       }
       auto fold = [&](const uint32_t(&v)[32], int cstart) {
-        if (mode == 0) {
+        if constexpr (mode == 0) {
 #pragma unroll
-          for (int q = 0; q < 32; q += 4) {
-            top2_pair(u0, u1, __uint_as_float(v[q]), __uint_as_float(v[q + 1]));
-            top2_pair(w0, w1, __uint_as_float(v[q + 2]), __uint_as_float(v[q + 3]));
+          for (int q = 0; q < 8; ++q) {
+            cm[q] = max3f(cm[q], __uint_as_float(v[q]), __uint_as_float(v[q + 8]));
+            cm[q] = max3f(cm[q], __uint_as_float(v[q + 16]), __uint_as_float(v[q + 24]));
           }
         } else {
           // the tests branch-free into a mask, then the (rare) hits in column order
@@ -496,12 +509,16 @@ __global__ void __maxnreg__(112)
         if (live) fold(rb, col0 + (j + 1) * kBN);
         if (j + 2 < pc.len) release(ra);
       }
-      if (mode == 0) {
-        u1 = max3f(u1, w1, fminf(u0, w0));
-        u0 = fmaxf(u0, w0);
+      // The row's largest D, and the second largest of the class maxima: a lower
+      // bound on the row's second largest D (equal to it unless the two largest
+      // share a class), which can only widen the candidate window.
+      float u0 = -inf, u1 = -inf;
+      if constexpr (mode == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; q += 2) top2_pair(u0, u1, cm[q], cm[q + 1]);
       }
       if (part > 0) {
-        if (mode == 0) {
+        if constexpr (mode == 0) {
           xrow[0] = __float_as_int(u0);
           xrow[1] = __float_as_int(u1);
         } else {
@@ -518,7 +535,7 @@ __global__ void __maxnreg__(112)
         bool part_overflow = false;
         for (int p = 1; p < kEpiParts; ++p) {
           const int* x = reinterpret_cast<const int*>(smem + kSmX) + ((p - 1) * kBM + row_in_tile) * (kXColl + 2);
-          if (mode == 0) {
+          if constexpr (mode == 0) {
             const float x0 = __int_as_float(x[0]), x1 = __int_as_float(x[1]);
             u1 = max3f(u1, x1, fminf(u0, x0));
             u0 = fmaxf(u0, x0);
@@ -529,7 +546,7 @@ __global__ void __maxnreg__(112)
             cnt += c1;
           }
         }
-        if (mode == 0) {
+        if constexpr (mode == 0) {
           const float an = PR.an[a_local];
           PR.top2[2 * o] = __fmaf_rn(-2.0f, u0, an);
           PR.top2[2 * o + 1] = __fmaf_rn(-2.0f, u1, an);
@@ -572,10 +589,11 @@ __device__ __forceinline__ uint16_t bf16_rne(float f) {
   return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
 }
 
-// A warp per 32 rows: the rows are read coalesced (a float4 per lane and row),
-// written as bf16 and staged in shared memory, then lane j adds up row j's
-// squared norm sequentially from there (the rows' sums run side by side instead
-// of one row's 128 terms being passed lane to lane).
+// A warp per 32 rows: the rows are copied coalesced into shared memory (a 16-byte
+// asynchronous copy per lane and row, all in flight together), written out as
+// bf16, and lane j adds up row j's squared norm sequentially from there (the
+// rows' sums run side by side instead of one row's 128 terms being passed lane
+// to lane).
 constexpr int kBf16Warps = 2;  // 33.8 KB of static shared memory per block
 constexpr int kBf16Stride = 132;  // floats per staged row: lanes reading 16 B of different rows hit distinct banks
 
@@ -598,15 +616,20 @@ __global__ void __launch_bounds__(32 * kBf16Warps) to_bf16_kernel(const Bf16Job*
   const float* __restrict__ x = J.x;
   float* st = stage[warp];
   const int nr = min(32, J.n - row0);  // rows with data
+  // all of the warp's row loads in flight at once: asynchronous copies into the stage
+  for (int r = 0; r < nr; ++r)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(st + r * kBf16Stride + 4 * lane)),
+                 "l"(x + (size_t)(row0 + r) * 128 + 4 * lane)
+                 : "memory");
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+  __syncwarp();
   for (int r = 0; r < nr; ++r) {
-    const float4 v = reinterpret_cast<const float4*>(x + (size_t)(row0 + r) * 128)[lane];
+    const float4 v = *reinterpret_cast<const float4*>(st + r * kBf16Stride + 4 * lane);
     uint2 packed;
     packed.x = (uint32_t)bf16_rne(v.x) | ((uint32_t)bf16_rne(v.y) << 16);  // round to nearest even
     packed.y = (uint32_t)bf16_rne(v.z) | ((uint32_t)bf16_rne(v.w) << 16);
     reinterpret_cast<uint2*>(J.out + (size_t)(row0 + r) * 128)[lane] = packed;
-    *reinterpret_cast<float4*>(st + r * kBf16Stride + 4 * lane) = v;
   }
-  __syncwarp();
   if (row < J.n) {
     // exact sequential norm of row `row`
     const float* rr = st + lane * kBf16Stride;
@@ -758,7 +781,7 @@ __global__ void rerank_kernel(const RerankJob* __restrict__ jobs) {
 // problem its A tiles (kept rows / 128) and first tile, and the range length of
 // each of `ctas` CTAs, at least (B tiles - 1) / (kTcSplits - 1) so that an A tile
 // meets at most kTcSplits ranges.  One block.
-__global__ void tc_plan_kernel(TcPair* __restrict__ P, int n, TcPlan* __restrict__ plan, int ctas) {
+__global__ void __launch_bounds__(1024) tc_plan_kernel(TcPair* __restrict__ P, int n, TcPlan* __restrict__ plan, int ctas) {
   __shared__ long long warp_sums[32];
   __shared__ long long carry;
   __shared__ int bt_max;
@@ -867,9 +890,13 @@ cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, cons
                             const CUtensorMap& tmBx, const TcPair* problems, int n_problems, const TcPlan* plan,
                             int ctas, uint32_t* err, int mode, cudaStream_t st) {
   if (ctas <= 0 || n_problems <= 0) return cudaSuccess;
-  cudaError_t e = ensure_smem_attr((const void*)match_tc_kernel, kSmTotal);
+  const void* fn = mode == 0 ? (const void*)match_tc_kernel<0> : (const void*)match_tc_kernel<1>;
+  cudaError_t e = ensure_smem_attr(fn, kSmTotal);
   if (e != cudaSuccess) return e;
-  match_tc_kernel<<<ctas, kTcThreads, kSmTotal, st>>>(tmA, tmB, tmAx, tmBx, problems, n_problems, plan, err, mode);
+  if (mode == 0)
+    match_tc_kernel<0><<<ctas, kTcThreads, kSmTotal, st>>>(tmA, tmB, tmAx, tmBx, problems, n_problems, plan, err);
+  else
+    match_tc_kernel<1><<<ctas, kTcThreads, kSmTotal, st>>>(tmA, tmB, tmAx, tmBx, problems, n_problems, plan, err);
   return cudaGetLastError();
 }
 

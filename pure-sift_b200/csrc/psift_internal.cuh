@@ -99,6 +99,8 @@ struct psift_ctx {
   uint64_t graph_replays = 0;
   // nvJPEG decoder of the JPEG entries (decode.cu), created on first use.
   void* jpeg = nullptr;
+  // PNG decoder state (png.cu): staging buffers, created on first use.
+  void* png = nullptr;
 };
 
 namespace psift {
@@ -139,6 +141,9 @@ using DeviceFill = std::function<psift_status(char* extra, const std::vector<siz
 psift_status detect_batch_host_out(psift_ctx* ctx, const psift_image_u8* images, uint32_t n,
                                    const psift_sift_config* cfg, psift_features* outs, const DeviceFill* fill);
 void jpeg_release(psift_ctx* ctx);
+void png_release(psift_ctx* ctx);
+// The reference's size checks of a decoded image's header (decode.cu).
+psift_status check_image_dims(psift_ctx* ctx, uint32_t w, uint32_t h, bool enforce_cap);
 
 // Stage timing: `StageScope sc(ctx, STAGE_X);` records events around the launches
 // issued while it is alive (no-op unless timing is enabled).

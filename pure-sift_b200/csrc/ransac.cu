@@ -48,6 +48,8 @@ constexpr int kDrawChunk = kBatch * 16;
 constexpr size_t kJacSmem = sizeof(double) * 162 * kBatch;
 // LO refits stage row values (10 doubles per point) in the same buffer
 constexpr int kRowChunk = (int)(kJacSmem / (sizeof(double) * 10));
+// sequential sums over an inlier list stage its points (float4) there
+constexpr int kPtChunk = (int)(kJacSmem / sizeof(float4));
 
 struct RShared {
   int n;
@@ -188,23 +190,41 @@ __device__ int adaptive_iters_w(double w, int ss, int min_it, int cap) {
   return (int)c;
 }
 
-// Sequential sum of v[0..n) in order (one thread); the loads are issued 16 ahead
-// of the dependent additions.  Terms of matches that are not inliers are zero,
-// which leaves the running sum unchanged (x + 0 == x for the finite, non-negative
-// partial sums), so this equals the reference's sum over the inliers alone.
-template <typename T>
-__device__ T seq_sum(const T* __restrict__ v, int n) {
+// Sequential sum, in match order, of term(i) for i < n: the CTA computes the
+// terms of a chunk into shared memory (the batch's Jacobi space, free whenever a
+// sum is taken), thread 0 adds them in order with its loads issued ahead of the
+// dependent additions; the result is returned to every thread.  Terms of matches
+// that are not inliers are zero, which leaves the running sum unchanged (x + 0 ==
+// x for the finite, non-negative partial sums), so this equals the reference's
+// sum over the inliers alone.
+template <typename T, typename Term>
+__device__ T ordered_sum(RShared& S, int n, Term term) {
+  extern __shared__ double jac[];
+  T* buf = reinterpret_cast<T*>(jac);
+  constexpr int cap = (int)(kJacSmem / sizeof(T));
   T s = T(0);
-  int i = 0;
-  for (; i + 16 <= n; i += 16) {
-    T e[16];
+  for (int c0 = 0; c0 < n; c0 += cap) {
+    const int cn = min(cap, n - c0);
+    for (int j = threadIdx.x; j < cn; j += kRThreads) buf[j] = term(c0 + j);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int j = 0;
+      for (; j + 16 <= cn; j += 16) {
+        T e[16];
 #pragma unroll
-    for (int u = 0; u < 16; ++u) e[u] = v[i + u];
+        for (int u = 0; u < 16; ++u) e[u] = buf[j + u];
 #pragma unroll
-    for (int u = 0; u < 16; ++u) s += e[u];
+        for (int u = 0; u < 16; ++u) s += e[u];
+      }
+      for (; j < cn; ++j) s += buf[j];
+    }
+    __syncthreads();
   }
-  for (; i < n; ++i) s += v[i];
-  return s;
+  if (threadIdx.x == 0) S.dres[15] = (double)s;  // exact for float too
+  __syncthreads();
+  const T r = (T)S.dres[15];
+  __syncthreads();
+  return r;
 }
 
 // ------------------------------------------------------------- similarity
@@ -268,17 +288,11 @@ __device__ double sim_mass(const RansacJob& J, RShared& S, float a, float b, flo
 
 // Sequential f32 error sum over inliers in input order (whole CTA; result broadcast).
 __device__ float sim_err(const RansacJob& J, RShared& S, float a, float b, float tx, float ty) {
-  float* buf = reinterpret_cast<float*>(J.err);
-  for (int i = threadIdx.x; i < S.n; i += kRThreads) {
+  const float tsq = S.tsq_f;
+  return ordered_sum<float>(S, S.n, [&](int i) {
     float e;
-    buf[i] = sim_inlier(J.xy[i], a, b, tx, ty, S.tsq_f, e) ? e : 0.0f;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) S.fres[0] = seq_sum(buf, S.n);
-  __syncthreads();
-  const float r = S.fres[0];
-  __syncthreads();
-  return r;
+    return sim_inlier(J.xy[i], a, b, tx, ty, tsq, e) ? e : 0.0f;
+  });
 }
 
 // Ordered inlier list of a similarity model into J.list; returns its length.
@@ -311,7 +325,7 @@ __device__ int sim_collect(const RansacJob& J, RShared& S, float a, float b, flo
 }
 
 // fit_procrustes_similarity over J.list[0..k) (sequential sums; threads 0..6).
-__device__ bool procrustes(const RansacJob& J, RShared& S, int k, float* out6) {
+__device__ bool procrustes(const RansacJob& J, RShared& S, float* jac, int k, float* out6) {
   if (k == 0) return false;
   if (k == 1) {
     if (threadIdx.x == 0) {
@@ -329,34 +343,47 @@ __device__ bool procrustes(const RansacJob& J, RShared& S, int k, float* out6) {
     return true;
   }
   const float inv_n = 1.0f / (float)k;
-  // Gather the inliers (list order): P[j] = (q.x, q.y, t.x, t.y); the sums stay
-  // sequential in list order, their loads contiguous and issued ahead.
-  float4* P = reinterpret_cast<float4*>(J.pts);
-  for (int j = threadIdx.x; j < k; j += kRThreads) P[j] = J.xy[J.list[j]];
-  __syncthreads();
-  if (threadIdx.x < 4) {
-    float s = 0.0f;
-    const int c = threadIdx.x;
+  // The inliers' points (list order) staged in shared memory a chunk at a time;
+  // the sums stay sequential in list order (threads 0..3, then 0..2), their
+  // terms read at shared-memory latency.  One chunk is staged once for both.
+  float4* st = reinterpret_cast<float4*>(jac);
+  auto stage = [&](int c0, int cn) {
+    for (int j = threadIdx.x; j < cn; j += kRThreads) st[j] = J.xy[J.list[c0 + j]];
+  };
+  float s = 0.0f;
+  for (int c0 = 0; c0 < k; c0 += kPtChunk) {
+    const int cn = min(kPtChunk, k - c0);
+    stage(c0, cn);
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      const float* col = reinterpret_cast<const float*>(st) + threadIdx.x;
 #pragma unroll 8
-    for (int j = 0; j < k; ++j) {
-      const float4 p = P[j];
-      s += c == 0 ? p.x : c == 1 ? p.y : c == 2 ? p.z : p.w;
+      for (int j = 0; j < cn; ++j) s += col[4 * j];
     }
-    S.fres[threadIdx.x] = s * inv_n;
+    __syncthreads();
   }
+  if (threadIdx.x < 4) S.fres[threadIdx.x] = s * inv_n;
   __syncthreads();
   const float mqx = S.fres[0], mqy = S.fres[1], mtx = S.fres[2], mty = S.fres[3];
-  if (threadIdx.x < 3) {
-    float s = 0.0f;
-#pragma unroll 8
-    for (int j = 0; j < k; ++j) {
-      const float4 p = P[j];
-      const float qx = p.x - mqx, qy = p.y - mqy, tx = p.z - mtx, ty = p.w - mty;
-      const float v = threadIdx.x == 0 ? qx * qx + qy * qy : threadIdx.x == 1 ? qx * tx + qy * ty : qx * ty - qy * tx;
-      s += v;
+  s = 0.0f;
+  for (int c0 = 0; c0 < k; c0 += kPtChunk) {
+    const int cn = min(kPtChunk, k - c0);
+    if (k > kPtChunk) {
+      stage(c0, cn);
+      __syncthreads();
     }
-    S.fres[4 + threadIdx.x] = s;
+    if (threadIdx.x < 3) {
+#pragma unroll 8
+      for (int j = 0; j < cn; ++j) {
+        const float4 p = st[j];
+        const float qx = p.x - mqx, qy = p.y - mqy, tx = p.z - mtx, ty = p.w - mty;
+        const float v = threadIdx.x == 0 ? qx * qx + qy * qy : threadIdx.x == 1 ? qx * tx + qy * ty : qx * ty - qy * tx;
+        s += v;
+      }
+    }
+    __syncthreads();
   }
+  if (threadIdx.x < 3) S.fres[4 + threadIdx.x] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
     const float sqq = S.fres[4], na = S.fres[5], nb = S.fres[6];
@@ -423,7 +450,7 @@ __device__ bool sim_consider(const RansacJob& J, RShared& S, SimBest& B, int h) 
 
 // filter_matches_ransac_with_seed (src/pipeline.rs:2055-2191).  Writes the
 // inlier list (J.list, length S.sim_count) and S.sim_model / S.has_sim.
-__device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed, float thr) {
+__device__ void similarity_ransac(const RansacJob& J, RShared& S, double* jac, uint64_t seed, float thr) {
   const int n = S.n;
   if (threadIdx.x == 0) {
     S.has_sim = 0;
@@ -435,7 +462,7 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
     if (threadIdx.x == 0) J.list[0] = 0;
     __syncthreads();
     float m6[6];
-    procrustes(J, S, 1, m6);
+    procrustes(J, S, reinterpret_cast<float*>(jac), 1, m6);
     if (threadIdx.x == 0) {
       for (int i = 0; i < 6; ++i) S.sim_model[i] = m6[i];
       S.has_sim = 1;
@@ -555,7 +582,7 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
   // consensus, Procrustes refit, re-collection
   int k = sim_collect(J, S, B.a, B.b, B.tx, B.ty);
   float refined[6];
-  const bool has_ref = procrustes(J, S, k, refined);
+  const bool has_ref = procrustes(J, S, reinterpret_cast<float*>(jac), k, refined);
   if (has_ref) {
     // count of the refined model's consensus (same expression as the collection)
     int c = 0;
@@ -569,7 +596,7 @@ __device__ void similarity_ransac(const RansacJob& J, RShared& S, uint64_t seed,
     if (c >= k) k = sim_collect(J, S, refined[0], refined[1], refined[2], refined[3]);
   }
   float fin[6];
-  const bool has_fin = procrustes(J, S, k, fin);
+  const bool has_fin = procrustes(J, S, reinterpret_cast<float*>(jac), k, fin);
   if (threadIdx.x == 0) {
     S.sim_count = k;
     if (has_fin) {
@@ -652,16 +679,13 @@ __device__ double h_mass(const RansacJob& J, RShared& S, const double* H) {
 
 // Sequential f64 error sum over the inliers in input order (whole CTA).
 __device__ double h_err(const RansacJob& J, RShared& S, const double* H) {
-  for (int i = threadIdx.x; i < S.n; i += kRThreads) {
+  const double tsq = S.tsq_d;
+  double Hl[9];
+  for (int i = 0; i < 9; ++i) Hl[i] = H[i];
+  return ordered_sum<double>(S, S.n, [&](int i) {
     double e;
-    J.err[i] = h_inlier(J.xy[i], H, S.tsq_d, e) ? e : 0.0;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) S.dres[15] = seq_sum(J.err, S.n);
-  __syncthreads();
-  const double r = S.dres[15];
-  __syncthreads();
-  return r;
+    return h_inlier(J.xy[i], Hl, tsq, e) ? e : 0.0;
+  });
 }
 
 __device__ int h_collect(const RansacJob& J, RShared& S, const double* H) {
@@ -743,8 +767,9 @@ __device__ int quad_cyclic_jacobi(double* A, double* V, int ql, unsigned qmask) 
         if (fabs(apq) < 1e-15) continue;
         const double app = A[p * 9 + p], aqq = A[q * 9 + q];
         const double tau = (aqq - app) / (2.0 * apq);
-        const double t = tau >= 0.0 ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
-        const double c = 1.0 / sqrt(1.0 + t * t);
+        // __drcp_rn(x) is 1.0 / x: both are IEEE round-to-nearest, the reciprocal is the cheaper sequence
+        const double t = tau >= 0.0 ? __drcp_rn(tau + sqrt(1.0 + tau * tau)) : -__drcp_rn(-tau + sqrt(1.0 + tau * tau));
+        const double c = __drcp_rn(sqrt(1.0 + t * t));
         const double s = t * c;
         __syncwarp(qmask);  // every pivot read precedes the writes
         if (ql == 0) {
@@ -887,84 +912,104 @@ __device__ bool quad_fit4(const float4* __restrict__ xy, const int* idx, double*
 // free A / V pair.  Result in H (every thread); false if the fit fails.
 __device__ bool fit_dlt_list(const RansacJob& J, RShared& S, double* jac, int k, double* H) {
   const double inv_n = 1.0 / (double)k;
-  // Gather the inliers (list order) as doubles: P[j] = (q.x, q.y, t.x, t.y).  The
-  // sums below stay sequential in list order (the reference's order); only the
-  // loads change: contiguous, issued ahead of the dependent additions.
-  double4* P = reinterpret_cast<double4*>(J.pts);
-  for (int j = threadIdx.x; j < k; j += kRThreads) {
-    const float4 p = J.xy[J.list[j]];
-    P[j] = make_double4((double)p.x, (double)p.y, (double)p.z, (double)p.w);
-  }
-  __syncthreads();
-  if (threadIdx.x < 4) {
-    double s = 0.0;
-    bool finite = true;
-    const int c = threadIdx.x;
-#pragma unroll 8
-    for (int j = 0; j < k; ++j) {
-      const double4 p = P[j];
-      const double v = c == 0 ? p.x : c == 1 ? p.y : c == 2 ? p.z : p.w;
-      if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(p.w)) finite = false;
-      s += v;
+  // The inliers' points (list order) staged in shared memory a chunk at a time;
+  // every sum below stays sequential in list order, its terms read at
+  // shared-memory latency (the centroids by threads 0..3, the mean distances'
+  // terms computed by the CTA and added by threads 0, 1).
+  constexpr int kChunk = (int)(kJacSmem / (sizeof(float4) + 2 * sizeof(double)));
+  float4* st = reinterpret_cast<float4*>(jac);
+  double* dq = reinterpret_cast<double*>(st + kChunk);
+  double* dt = dq + kChunk;
+  auto stage = [&](int c0, int cn) {
+    for (int j = threadIdx.x; j < cn; j += kRThreads) st[j] = J.xy[J.list[c0 + j]];
+  };
+  if (threadIdx.x == 0) S.flag = 1;
+  double s = 0.0;
+  for (int c0 = 0; c0 < k; c0 += kChunk) {
+    const int cn = min(kChunk, k - c0);
+    stage(c0, cn);
+    __syncthreads();
+    for (int j = threadIdx.x; j < cn; j += kRThreads) {
+      const float4 p = st[j];
+      if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(p.w)) S.flag = 0;
     }
-    S.dres[threadIdx.x] = s * inv_n;
-    if (threadIdx.x == 0) S.flag = finite ? 1 : 0;
+    if (threadIdx.x < 4) {
+      const float* col = reinterpret_cast<const float*>(st) + threadIdx.x;
+#pragma unroll 8
+      for (int j = 0; j < cn; ++j) s += (double)col[4 * j];
+    }
+    __syncthreads();
   }
+  if (threadIdx.x < 4) S.dres[threadIdx.x] = s * inv_n;
   __syncthreads();
   const bool finite = S.flag != 0;
   const double cxq = S.dres[0], cyq = S.dres[1], cxt = S.dres[2], cyt = S.dres[3];
   __syncthreads();
   if (!finite) return false;
-  if (threadIdx.x < 2) {
-    double s = 0.0;
-    const double cx = threadIdx.x == 0 ? cxq : cxt, cy = threadIdx.x == 0 ? cyq : cyt;
-#pragma unroll 8
-    for (int j = 0; j < k; ++j) {
-      const double4 p = P[j];
-      const double dx = (threadIdx.x == 0 ? p.x : p.z) - cx;
-      const double dy = (threadIdx.x == 0 ? p.y : p.w) - cy;
-      s += sqrt(dx * dx + dy * dy);
+  s = 0.0;
+  for (int c0 = 0; c0 < k; c0 += kChunk) {
+    const int cn = min(kChunk, k - c0);
+    if (k > kChunk) {
+      stage(c0, cn);
+      __syncthreads();
     }
-    S.dres[4 + threadIdx.x] = s * inv_n;
+    for (int j = threadIdx.x; j < cn; j += kRThreads) {
+      const float4 p = st[j];
+      const double ax = (double)p.x - cxq, ay = (double)p.y - cyq;
+      const double bx = (double)p.z - cxt, by = (double)p.w - cyt;
+      dq[j] = sqrt(ax * ax + ay * ay);
+      dt[j] = sqrt(bx * bx + by * by);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      const double* d = threadIdx.x == 0 ? dq : dt;
+      int j = 0;
+      for (; j + 16 <= cn; j += 16) {
+        double e[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) e[u] = d[j + u];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) s += e[u];
+      }
+      for (; j < cn; ++j) s += d[j];
+    }
+    __syncthreads();
   }
+  if (threadIdx.x < 2) S.dres[4 + threadIdx.x] = s * inv_n;
   __syncthreads();
   const double mdq = S.dres[4], mdt = S.dres[5];
   __syncthreads();
   if (!isfinite(mdq) || !isfinite(mdt) || mdq < 1e-6 || mdt < 1e-6) return false;
-  const double sq = 1.41421356237309504880 / mdq, st = 1.41421356237309504880 / mdt;
-  // normalised coordinates in place: (x, y, x', y')
-  for (int j = threadIdx.x; j < k; j += kRThreads) {
-    const double4 p = P[j];
-    P[j] = make_double4((p.x - cxq) * sq, (p.y - cyq) * sq, (p.z - cxt) * st, (p.w - cyt) * st);
-  }
-  __syncthreads();
+  const double sq = 1.41421356237309504880 / mdq, st_ = 1.41421356237309504880 / mdt;
   // upper triangle of A^T A: entry (a, b), a <= b, one thread each, sequential
-  // over the list; the points' row values staged through jac a chunk at a time
+  // over the list; the points' normalised row values staged through jac a chunk
+  // at a time
   {
     int a = 0, b = 0;
     if (threadIdx.x < 45) upper_entry(threadIdx.x, a, b);
     const int s1a = (int)(kSlot1 >> (4 * a)) & 15, s1b = (int)(kSlot1 >> (4 * b)) & 15;
     const int s2a = (int)(kSlot2 >> (4 * a)) & 15, s2b = (int)(kSlot2 >> (4 * b)) & 15;
-    double s = 0.0;
+    double sum = 0.0;
     for (int c0 = 0; c0 < k; c0 += kRowChunk) {
       const int cn = min(kRowChunk, k - c0);
       for (int j = threadIdx.x; j < cn; j += kRThreads) {
-        const double4 p = P[c0 + j];
-        dlt_row_values(p.x, p.y, p.z, p.w, jac + j * kRowVals);
+        const float4 p = J.xy[J.list[c0 + j]];
+        dlt_row_values(((double)p.x - cxq) * sq, ((double)p.y - cyq) * sq, ((double)p.z - cxt) * st_,
+                       ((double)p.w - cyt) * st_, jac + j * kRowVals);
       }
       __syncthreads();
       if (threadIdx.x < 45) {
 #pragma unroll 8
         for (int j = 0; j < cn; ++j) {
           const double* r = jac + j * kRowVals;
-          s += r[s1a] * r[s1b] + r[s2a] * r[s2b];
+          sum += r[s1a] * r[s1b] + r[s2a] * r[s2b];
         }
       }
       __syncthreads();
     }
     if (threadIdx.x < 45) {
-      S.ata[a][b] = s;
-      S.ata[b][a] = s;
+      S.ata[a][b] = sum;
+      S.ata[b][a] = sum;
     }
   }
   __syncthreads();
@@ -980,7 +1025,7 @@ __device__ bool fit_dlt_list(const RansacJob& J, RShared& S, double* jac, int k,
       if (mi >= 0) {
         double hv[9], Hl[9];
         for (int r = 0; r < 9; ++r) hv[r] = V[r * 9 + mi];
-        denormalise(hv, sq, st, cxq, cyq, cxt, cyt, Hl);
+        denormalise(hv, sq, st_, cxq, cyq, cxt, cyt, Hl);
         for (int i = 0; i < 9; ++i) S.dres[i] = Hl[i];
       }
     }
@@ -1046,7 +1091,7 @@ __global__ void __launch_bounds__(kRThreads, kRCtasPerSm) ransac_kernel(const Ra
     J.xy[i] = make_float4(m.query_x, m.query_y, m.target_x, m.target_y);
   }
   __syncthreads();
-  similarity_ransac(J, S, J.sim_seed, J.thr);
+  similarity_ransac(J, S, jac, J.sim_seed, J.thr);
   if (!J.homography) {
     const int k = S.sim_count;
     for (int j = threadIdx.x; j < k; j += kRThreads) J.mask[J.list[j]] = 1;

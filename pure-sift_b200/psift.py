@@ -184,6 +184,14 @@ _SIGS = {
                                          C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "psift_detect_and_compute_jpeg_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32,
                                                       C.POINTER(CSiftConfig), C.c_void_p]),
+    "psift_png_info": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32, C.POINTER(C.c_uint32),
+                                 C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "psift_decode_png_luma": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32, C.c_void_p, C.c_size_t,
+                                        C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "psift_detect_and_compute_png_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32,
+                                                     C.POINTER(CSiftConfig), C.c_void_p]),
+    "psift_detect_and_compute_image_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32,
+                                                       C.POINTER(CSiftConfig), C.c_void_p]),
     "psift_ctx_jpeg_backend": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "psift_ctx_set_jpeg_threads": (C.c_int, [C.c_void_p, C.c_int32]),
     "psift_detect_and_compute_u8_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(CSiftConfig),
@@ -584,11 +592,7 @@ class Sift:
             ctx.check(st)
             return [outs[i].view(int(couts[i].count)) for i in range(n)]
 
-    def detect_and_compute_jpeg_batch(self, blobs, enforce_pixel_cap: bool = False, outs=None,
-                                      ctx: Context | None = None) -> "list[Features]":
-        """JPEG bytes -> features (psift_detect_and_compute_jpeg_batch): decoded on the
-        GPU into the batch's inputs (decode_validated_luma8, src/cli.rs:164-170), then
-        as ``detect_and_compute_batch_u8``."""
+    def _bytes_batch(self, fn_name, blobs, enforce_pixel_cap, outs, ctx):
         ctx = ctx or default_context()
         bufs = [bytes(b) for b in blobs]
         n = len(bufs)
@@ -599,10 +603,10 @@ class Sift:
         cfg = self.config.to_c()
         cap = self.config.max_features_ or 16384
         outs = list(outs) if outs is not None else [Features.empty(cap) for _ in range(n)]
+        fn = getattr(ctx.lib, fn_name)
         while True:
             couts = (CFeatures * n)(*[_c_features(o) for o in outs])
-            st = ctx.lib.psift_detect_and_compute_jpeg_batch(ctx.handle, ptrs, lens, n, int(bool(enforce_pixel_cap)),
-                                                             C.byref(cfg), couts)
+            st = fn(ctx.handle, ptrs, lens, n, int(bool(enforce_pixel_cap)), C.byref(cfg), couts)
             short = [i for i in range(n) if couts[i].count > len(outs[i])]
             if st == PSIFT_ERR_CAPACITY and short:
                 for i in short:
@@ -610,6 +614,25 @@ class Sift:
                 continue
             ctx.check(st)
             return [outs[i].view(int(couts[i].count)) for i in range(n)]
+
+    def detect_and_compute_jpeg_batch(self, blobs, enforce_pixel_cap: bool = False, outs=None,
+                                      ctx: Context | None = None) -> "list[Features]":
+        """JPEG bytes -> features (psift_detect_and_compute_jpeg_batch): decoded on the
+        GPU into the batch's inputs (decode_validated_luma8, src/cli.rs:164-170), then
+        as ``detect_and_compute_batch_u8``."""
+        return self._bytes_batch("psift_detect_and_compute_jpeg_batch", blobs, enforce_pixel_cap, outs, ctx)
+
+    def detect_and_compute_png_batch(self, blobs, enforce_pixel_cap: bool = False, outs=None,
+                                     ctx: Context | None = None) -> "list[Features]":
+        """PNG bytes -> features (psift_detect_and_compute_png_batch): inflated on host
+        threads, unfiltered and converted to luma on the GPU into the batch's inputs."""
+        return self._bytes_batch("psift_detect_and_compute_png_batch", blobs, enforce_pixel_cap, outs, ctx)
+
+    def detect_and_compute_image_batch(self, blobs, enforce_pixel_cap: bool = False, outs=None,
+                                       ctx: Context | None = None) -> "list[Features]":
+        """JPEG or PNG bytes (told apart by their leading bytes) -> features, in order
+        (``run_extract_from_bytes``, src/cli.rs:173-185, for a batch)."""
+        return self._bytes_batch("psift_detect_and_compute_image_batch", blobs, enforce_pixel_cap, outs, ctx)
 
     def detect_and_compute_u8(self, img: np.ndarray, ctx: Context | None = None) -> Features:
         return self._run(img, True, ctx)
@@ -707,6 +730,35 @@ def decode_jpeg_luma(blob: bytes, enforce_pixel_cap: bool = False, ctx: Context 
     ctx.check(ctx.lib.psift_decode_jpeg_luma(ctx.handle, blob, len(blob), int(bool(enforce_pixel_cap)),
                                              out.ctypes.data, out.size, C.byref(ww), C.byref(hh)))
     return out
+
+
+# ---------------------------------------------------------------- PNG input
+def png_info(blob: bytes, enforce_pixel_cap: bool = False, ctx: Context | None = None):
+    """(width, height, channels) of a PNG, with the reference's size checks."""
+    ctx = ctx or default_context()
+    w, h, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    ctx.check(ctx.lib.psift_png_info(ctx.handle, blob, len(blob), int(bool(enforce_pixel_cap)), C.byref(w),
+                                     C.byref(h), C.byref(c)))
+    return int(w.value), int(h.value), int(c.value)
+
+
+def decode_png_luma(blob: bytes, enforce_pixel_cap: bool = False, ctx: Context | None = None) -> np.ndarray:
+    """``decode_validated_luma8`` (src/cli.rs:164-170) for a PNG: inflated on the host,
+    row filters and the luma conversion on the GPU."""
+    ctx = ctx or default_context()
+    w, h, _ = png_info(blob, enforce_pixel_cap, ctx)
+    out = np.zeros((h, w), np.uint8)
+    ww, hh = C.c_uint32(), C.c_uint32()
+    ctx.check(ctx.lib.psift_decode_png_luma(ctx.handle, blob, len(blob), int(bool(enforce_pixel_cap)),
+                                            out.ctypes.data, out.size, C.byref(ww), C.byref(hh)))
+    return out
+
+
+def decode_image_luma(blob: bytes, enforce_pixel_cap: bool = False, ctx: Context | None = None) -> np.ndarray:
+    """``decode_validated_luma8`` for either supported format (PNG signature, else JPEG)."""
+    if bytes(blob[:8]) == b"\x89PNG\r\n\x1a\n":
+        return decode_png_luma(blob, enforce_pixel_cap, ctx)
+    return decode_jpeg_luma(blob, enforce_pixel_cap, ctx)
 
 
 # ---------------------------------------------------------------- catalog codes
