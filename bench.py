@@ -194,6 +194,8 @@ def match_bench(ctx, torch, n_pairs: int = 32, n: int = 4096, reps: int = 5):
         for _ in range(2):
             call()
         ctx.synchronize()
+        fb0 = C.c_uint64()
+        ctx.check(ctx.lib.psift_ctx_rerank_fallbacks(ctx.handle, C.byref(fb0)))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(reps):
@@ -202,6 +204,10 @@ def match_bench(ctx, torch, n_pairs: int = 32, n: int = 4096, reps: int = 5):
         ctx.synchronize()
         ms = e0.elapsed_time(e1) / reps
         res[name] = ms / n_pairs
+        fb1 = C.c_uint64()
+        ctx.check(ctx.lib.psift_ctx_rerank_fallbacks(ctx.handle, C.byref(fb1)))
+        if name == "bf16_rerank":
+            res["fallback_rows_per_call"] = (fb1.value - fb0.value) / reps
         lists[name] = [(int(c.item()), outs[i][: int(c.item())].cpu().numpy().tobytes()) for i, c in enumerate(counts)]
     flops = 2.0 * n * n * 128
     return {
@@ -211,6 +217,7 @@ def match_bench(ctx, torch, n_pairs: int = 32, n: int = 4096, reps: int = 5):
         "identical_match_lists": lists["fp32"] == lists["bf16_rerank"],
         "matches_per_pair": lists["fp32"][0][0],
         "bf16_tflops_effective": flops / (res["bf16_rerank"] * 1e-3) / 1e12,
+        "rerank_exact_scan_rows_per_call": res["fallback_rows_per_call"],
     }
 
 
@@ -752,6 +759,58 @@ def pyramid_bench(ctx, torch, blur: str = "reference", reps: int = 5):
             "blur": blur, "device_pyramid_ms": st["pyramid"][0] / reps, "host_api_ms_with_download": wall * 1e3}
 
 
+def png_bench(ctx, torch, n: int = 8, reps: int = 10):
+    """Input step, PNG: 8 colour 1920x1080 PNGs (the JPEG section's images, written
+    by PIL at its default compression, adaptive row filters) in host memory ->
+    features in host memory through psift_detect_and_compute_png_batch (inflate on
+    host threads, row filters and luma on the GPU into the batch's inputs), against
+    the host u8 batch entry given the decoded luma, and the CPU decode (PIL + the
+    image crate's luma formula, one thread) per image."""
+    import io
+    from PIL import Image
+    import psift
+    rgbs = [np.stack([synth.blob_image(WIDTH, HEIGHT, 2000, 1.5, 20.0, seed=900 + 3 * i + k) for k in range(3)],
+                     axis=2) for i in range(n)]
+    blobs = []
+    for im in rgbs:
+        buf = io.BytesIO()
+        Image.fromarray(im).save(buf, format="PNG")
+        blobs.append(buf.getvalue())
+    sift = psift.Sift.new(psift.SiftConfig().with_octaves(4).with_contrast_threshold(0.015))
+    outs = [psift.Features.pinned(4096, ctx) for _ in range(n)]
+    for _ in range(2):
+        sift.detect_and_compute_png_batch(blobs, outs=outs, ctx=ctx)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        sift.detect_and_compute_png_batch(blobs, outs=outs, ctx=ctx)
+    png_s = (time.perf_counter() - t0) / reps
+    lumas = [psift.decode_png_luma(b, ctx=ctx) for b in blobs]
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for b in blobs:
+            psift.decode_png_luma(b, ctx=ctx)
+    dec_s = (time.perf_counter() - t0) / reps / n
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        sift.detect_and_compute_batch_u8(lumas, outs=outs, ctx=ctx)
+    u8_s = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    cpu = []
+    for b in blobs[:2]:
+        rgb = np.asarray(Image.open(io.BytesIO(b)).convert("RGB")).astype(np.uint32)
+        cpu.append(((2126 * rgb[:, :, 0] + 7152 * rgb[:, :, 1] + 722 * rgb[:, :, 2]) // 10000).astype(np.uint8))
+    cpu_s = (time.perf_counter() - t0) / 2
+    return {
+        "workload": f"{n} colour {WIDTH}x{HEIGHT} PNGs (PIL, default compression, {sum(map(len, blobs)) // n // 1024} KB "
+                    "each), host bytes -> pinned host features, host API wall clock",
+        "png_images_per_s": n / png_s, "u8_batch_images_per_s": n / u8_s,
+        "png_minus_u8_input_ms_per_batch": (png_s - u8_s) * 1e3,
+        "decode_png_luma_ms_per_image_host_api": dec_s * 1e3,
+        "cpu_decode_ms_per_image_1_thread": cpu_s * 1e3,
+        "luma_equal_to_cpu_decode": all(np.array_equal(c, l) for c, l in zip(cpu, lumas[:2])),
+    }
+
+
 def jpeg_bench(ctx, torch, n: int = 8, reps: int = 20):
     """Input step: 8 colour 1920x1080 JPEGs (three independent 2000-blob fields as
     R, G, B; 4:2:0, quality 90) in host memory -> features in host memory through
@@ -1113,7 +1172,8 @@ def run_ours(args):
         for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench),
                         ("catalog_search", catalog_search_bench), ("warp", warp_bench),
                         ("fundamental", fundamental_bench),
-                        ("learned_ransac", ransac_bench), ("jpeg", jpeg_bench), ("panorama", panorama_bench)):
+                        ("learned_ransac", ransac_bench), ("jpeg", jpeg_bench), ("png", png_bench),
+                        ("panorama", panorama_bench)):
             if getattr(args, "no_" + key):
                 continue
             try:
@@ -1153,7 +1213,7 @@ def main():
     ap.add_argument("--match-only", action="store_true", help="run only the pair-matching measurement")
     ap.add_argument("--match-pairs", type=int, default=32)
     ap.add_argument("--only-section", choices=["match", "catalog", "catalog_search", "warp", "fundamental",
-                                               "learned_ransac", "uneven_batch", "jpeg", "panorama", "pyramid"],
+                                               "learned_ransac", "uneven_batch", "jpeg", "png", "panorama", "pyramid"],
                     help="run one section alone (profiling case)")
     ap.add_argument("--ransac-pairs", type=int, default=1024, help="learned-RANSAC section: match sets")
     ap.add_argument("--blur", choices=["reference", "fused"], default="reference",
@@ -1169,6 +1229,7 @@ def main():
     ap.add_argument("--no-uneven-batch", dest="no_uneven_batch", action="store_true")
     ap.add_argument("--no-learned-ransac", dest="no_learned_ransac", action="store_true")
     ap.add_argument("--no-jpeg", dest="no_jpeg", action="store_true")
+    ap.add_argument("--no-png", dest="no_png", action="store_true")
     ap.add_argument("--no-panorama", dest="no_panorama", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1191,6 +1252,7 @@ def main():
                "catalog_search": lambda: catalog_search_bench(ctx, torch, n_entries=args.catalog_entries), "warp": lambda: warp_bench(ctx, torch),
                "fundamental": lambda: fundamental_bench(ctx, torch),
                "uneven_batch": lambda: uneven_bench(ctx, torch), "jpeg": lambda: jpeg_bench(ctx, torch),
+               "png": lambda: png_bench(ctx, torch),
                "panorama": lambda: panorama_bench(ctx, torch),
                "pyramid": lambda: pyramid_bench(ctx, torch, blur=args.blur, reps=min(args.steps, 10))}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)

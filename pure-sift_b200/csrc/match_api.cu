@@ -40,7 +40,8 @@ cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, cons
                             int ctas, uint32_t* err, int mode, cudaStream_t st);
 cudaError_t launch_tc_plan(TcPair* problems, int n_problems, TcPlan* plan, int ctas, cudaStream_t st);
 cudaError_t launch_window(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
-cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
+cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, const int2* scan_rows,
+                          const int* scan_count, int scan_ctas, cudaStream_t st);
 cudaError_t launch_gather_rows(const GatherJob* jobs, int n_jobs, int max_rows, cudaStream_t st);
 
 namespace {
@@ -131,6 +132,7 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     // pass 2's compacted operands, row maps, counts and gather jobs
     bytes += (size_t)(q_rows + t_rows) * 256 + (size_t)(q_rows + t_rows) * 4 + sizeof(int) * 2 * na +
              sizeof(GatherJob) * 2 * na + 5 * 256;
+    bytes += sizeof(int2) * (size_t)(q_rows + t_rows) + 2 * 256;  // exact-scan row lists
   }
   psift_status s = arena_reserve(ctx, bytes);
   if (s != PSIFT_OK) return s;
@@ -217,12 +219,15 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   uint16_t* tbc = (uint16_t*)arena_alloc(ctx, (size_t)t_rows * 256);
   int* rowmap = (int*)arena_alloc(ctx, sizeof(int) * (q_rows + t_rows));
   int* ccount = (int*)arena_alloc(ctx, sizeof(int) * 2 * na);
+  int* scan_count = (int*)arena_alloc(ctx, sizeof(int) * 2);  // per direction
+  int2* scan_rows = (int2*)arena_alloc(ctx, sizeof(int2) * (q_rows + t_rows));
   GatherJob* d_gj = (GatherJob*)arena_alloc(ctx, sizeof(GatherJob) * 2 * na);
   std::vector<GatherJob> gj(2 * na);
   if (!qb || !tb || !thr || !coll_cnt || !d_rj || !d_bj || (mutual && !flags) || !qbc || !tbc || !rowmap ||
-      !ccount || !d_gj || !qx || !tx || !ones || !d_plan)
+      !ccount || !d_gj || !qx || !tx || !ones || !d_plan || !scan_count || !scan_rows)
     return set_error(ctx, PSIFT_ERR_INTERNAL, "match workspace carve overflow");
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ccount, 0, sizeof(int) * 2 * na, st));
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(scan_count, 0, sizeof(int) * 2, st));
   if (mutual) PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * t_rows, st));
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(qb, 0, (size_t)q_rows * 256, st));
   PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(tb, 0, (size_t)t_rows * 256, st));
@@ -301,6 +306,8 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
                       kTcSplits, P.best, P.second, P.best_idx, ctx->d_error + 1, opt.ratio,
                       mutual ? flags + t0[k] : nullptr};
     rj[k].ccount = ccount + k;
+    rj[k].scan_count = scan_count;
+    rj[k].scan_rows = scan_rows;
     rj[k].rowmap = rowmap + q0[k];
     gj[k] = GatherJob{qb + (size_t)q0[k] * 128, qbc + (size_t)q0[k] * 128, rowmap + q0[k], ccount + k};
   }
@@ -314,6 +321,8 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
                              T.coll_cnt, kTcSplits, P.col_best, nullptr, P.col_idx, ctx->d_error + 1, opt.ratio,
                              flags + t0[k]};
       rj[na + k].ccount = ccount + na + k;
+      rj[na + k].scan_count = scan_count + 1;
+      rj[na + k].scan_rows = scan_rows + q_rows;
       rj[na + k].rowmap = rowmap + q_rows + t0[k];
       gj[na + k] = GatherJob{tb + (size_t)t0[k] * 128, tbc + (size_t)t0[k] * 128, rowmap + q_rows + t0[k],
                              ccount + na + k};
@@ -361,7 +370,8 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     if (e == cudaSuccess && (what = "gather_rows", true)) e = launch_gather_rows(d_gj + dir * na, na, rows, st);
     if (e == cudaSuccess && (what = "match_tc pass 2", true))
       e = launch_match_tc(Ac, B, tmOnes, Bx, probs, na, pl, tc_ctas, ctx->d_error, 1, st);
-    if (e == cudaSuccess && (what = "rerank", true)) e = launch_rerank(jobs_dir, na, rows, st);
+    if (e == cudaSuccess && (what = "rerank", true))
+      e = launch_rerank(jobs_dir, na, rows, scan_rows + (dir == 0 ? 0 : q_rows), scan_count + dir, 2 * ctx->num_sms, st);
     ctx->launches += 6;
     if (e != cudaSuccess) return cuda_error(ctx, e, what);
   }

@@ -97,6 +97,8 @@ struct RerankJob {
                         // reverse: only rows with flags[row] != 0 are ranked (null = all)
   int* ccount;          // window_kernel: rows kept for pass 2 (null: no compaction)
   int* rowmap;          // [na] their rows, in the order they were kept
+  int* scan_count;      // rows handed to rerank_scan_kernel (all jobs of a direction share it)
+  int2* scan_rows;      // their (job, row)
 };
 
 // Merge of two (best, idx, second) triples over disjoint target sets where ties

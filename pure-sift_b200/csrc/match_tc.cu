@@ -729,6 +729,19 @@ __global__ void gather_rows_kernel(const GatherJob* __restrict__ jobs) {
   reinterpret_cast<uint2*>(G.dst + (size_t)c * 128)[lane] = reinterpret_cast<const uint2*>(G.src + (size_t)r * 128)[lane];
 }
 
+// A row's result: best / index / second, and for the forward pass of a mutual
+// match the target's mark when the reference's ratio test (src/pipeline.rs:1789-1794)
+// accepts the row.
+__device__ __forceinline__ void rerank_row_out(const RerankJob& J, int row, float b, int bi, float sec) {
+  const bool forward = J.second != nullptr;
+  if (forward && J.flags && sec > 1e-12f && b < __int_as_float(0x7f800000) && bi < J.nb) {
+    if (sqrtf(b) / sqrtf(sec) < J.ratio) J.flags[bi] = 1;
+  }
+  J.best[row] = b;
+  J.best_idx[row] = bi;
+  if (forward) J.second[row] = sec;
+}
+
 // One warp per A row: exact reference distances over the window candidates
 // (every index with a <= thr, collected by the second GEMM pass), or over all
 // B rows when a split's window overflowed kColl.
@@ -737,7 +750,6 @@ __global__ void rerank_kernel(const RerankJob* __restrict__ jobs) {
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= J.na) return;
-  const bool forward = J.second != nullptr;
   const float inf = __int_as_float(0x7f800000);
   float b = inf, sec = inf;
   int bi = 0x7fffffff;
@@ -755,8 +767,12 @@ __global__ void rerank_kernel(const RerankJob* __restrict__ jobs) {
         }
       }
     } else {
-      if (lane == 0) atomicAdd(J.fallbacks, 1u);
-      for (int t = lane; t < J.nb; t += 32) top2_push(b, bi, sec, exact_d2(arow, J.b + (size_t)t * 128), t);
+      // the exact scan over all B rows is left to rerank_scan_kernel (a CTA per row)
+      if (lane == 0) {
+        atomicAdd(J.fallbacks, 1u);
+        J.scan_rows[atomicAdd(J.scan_count, 1)] = make_int2((int)blockIdx.y, row);
+      }
+      return;
     }
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) {
@@ -765,15 +781,79 @@ __global__ void rerank_kernel(const RerankJob* __restrict__ jobs) {
       const float s2 = __shfl_xor_sync(0xffffffffu, sec, off);
       top2_merge(b, bi, sec, b2, i2, s2);
     }
-    if (forward && J.flags && lane == 0 && sec > 1e-12f && b < inf && bi < J.nb) {
-      // the reference's ratio test (src/pipeline.rs:1789-1794): mark the target for the reverse pass
-      if (sqrtf(b) / sqrtf(sec) < J.ratio) J.flags[bi] = 1;
-    }
+    if (lane == 0) rerank_row_out(J, row, b, bi, sec);
+    return;
   }
-  if (lane == 0) {
-    J.best[row] = b;
-    J.best_idx[row] = bi;
-    if (forward) J.second[row] = sec;
+  if (lane == 0) rerank_row_out(J, row, b, bi, sec);
+}
+
+// A row whose window overflowed: one CTA computes the exact reference distances
+// to all B rows (a thread per B row, two at a time), merged order-independently.
+// The CTAs walk the list of such rows that rerank_kernel left.
+__device__ __forceinline__ void exact_d2_x2(const float* __restrict__ a, const float* __restrict__ b0,
+                                            const float* __restrict__ b1, float& s0, float& s1) {
+  s0 = 0.0f;
+  s1 = 0.0f;
+#pragma unroll 4
+  for (int i = 0; i < 128; i += 4) {
+    const float4 x = *reinterpret_cast<const float4*>(a + i);
+    const float4 y = *reinterpret_cast<const float4*>(b0 + i);
+    const float4 z = *reinterpret_cast<const float4*>(b1 + i);
+    float d = x.x - y.x, e = x.x - z.x;
+    s0 += d * d;
+    s1 += e * e;
+    d = x.y - y.y, e = x.y - z.y;
+    s0 += d * d;
+    s1 += e * e;
+    d = x.z - y.z, e = x.z - z.z;
+    s0 += d * d;
+    s1 += e * e;
+    d = x.w - y.w, e = x.w - z.w;
+    s0 += d * d;
+    s1 += e * e;
+  }
+}
+
+__global__ void __launch_bounds__(256) rerank_scan_kernel(const RerankJob* __restrict__ jobs,
+                                                          const int2* __restrict__ rows, const int* __restrict__ count) {
+  __shared__ float sb[8], ss[8];
+  __shared__ int si[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float inf = __int_as_float(0x7f800000);
+  const int n = *count;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const int2 e = rows[it];
+    const RerankJob& J = jobs[e.x];
+    const int row = e.y;
+    const float* arow = J.a + (size_t)row * 128;
+    float b = inf, sec = inf;
+    int bi = 0x7fffffff;
+    int t = threadIdx.x;
+    for (; t + 256 < J.nb; t += 512) {
+      float d0, d1;
+      exact_d2_x2(arow, J.b + (size_t)t * 128, J.b + (size_t)(t + 256) * 128, d0, d1);
+      top2_push(b, bi, sec, d0, t);
+      top2_push(b, bi, sec, d1, t + 256);
+    }
+    if (t < J.nb) top2_push(b, bi, sec, exact_d2(arow, J.b + (size_t)t * 128), t);
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+      const float b2 = __shfl_xor_sync(0xffffffffu, b, off);
+      const int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
+      const float s2 = __shfl_xor_sync(0xffffffffu, sec, off);
+      top2_merge(b, bi, sec, b2, i2, s2);
+    }
+    if (lane == 0) {
+      sb[warp] = b;
+      si[warp] = bi;
+      ss[warp] = sec;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < 8; ++w) top2_merge(b, bi, sec, sb[w], si[w], ss[w]);
+      rerank_row_out(J, row, b, bi, sec);
+    }
+    __syncthreads();
   }
 }
 
@@ -919,9 +999,13 @@ cudaError_t launch_gather_rows(const GatherJob* jobs, int n_jobs, int max_rows, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, cudaStream_t st) {
+cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, const int2* scan_rows,
+                          const int* scan_count, int scan_ctas, cudaStream_t st) {
   dim3 grid((max_rows + 7) / 8, n_jobs);
   rerank_kernel<<<grid, 256, 0, st>>>(jobs);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  rerank_scan_kernel<<<scan_ctas, 256, 0, st>>>(jobs, scan_rows, scan_count);
   return cudaGetLastError();
 }
 
