@@ -61,7 +61,7 @@ psift_status validate_match_options(psift_ctx* ctx, const psift_match_options* o
   return PSIFT_OK;
 }
 
-long long pad_rows(int n) { return ((long long)n + kTcBN - 1) / kTcBN * kTcBN; }
+long long pad_rows(int n) { return ((long long)n + kTcBN1 - 1) / kTcBN1 * kTcBN1; }
 
 // Device-side batch: every pointer in jobs is device memory.  Queues all work.
 psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, const psift_match_options& opt) {
@@ -242,13 +242,19 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
       b += pad_rows(pairs[k].nt);
     }
   }
-  CUtensorMap tmQA, tmTB, tmTA, tmQB, tmQAc, tmTAc, tmOnes, tmTBx, tmQBx;
-  if (!make_operand_map(&tmQA, qb, q_rows, kTcBM) || !make_operand_map(&tmTB, tb, t_rows, kTcBN) ||
-      !make_operand_map(&tmQAc, qbc, q_rows, kTcBM) || !make_ext_map(&tmOnes, ones, kTcBM, kTcBM) ||
-      !make_ext_map(&tmTBx, tx, t_rows, kTcBN) ||
-      (mutual && (!make_operand_map(&tmTA, tb, t_rows, kTcBM) || !make_operand_map(&tmQB, qb, q_rows, kTcBN) ||
-                  !make_operand_map(&tmTAc, tbc, t_rows, kTcBM) || !make_ext_map(&tmQBx, qx, q_rows, kTcBN))))
-    return set_error(ctx, PSIFT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  // B operands per pass: boxes of the pass's B tile rows (pass 1: 256, pass 2: 128)
+  CUtensorMap tmQA, tmTA, tmQAc, tmTAc, tmOnes, tmTB[2], tmTBx[2], tmQB[2], tmQBx[2];
+  bool maps_ok = make_operand_map(&tmQA, qb, q_rows, kTcBM) && make_operand_map(&tmQAc, qbc, q_rows, kTcBM) &&
+                 make_ext_map(&tmOnes, ones, kTcBM, kTcBM);
+  for (int ps = 0; ps < 2 && maps_ok; ++ps) {
+    const int box = ps == 0 ? kTcBN1 : kTcBN;
+    maps_ok = make_operand_map(&tmTB[ps], tb, t_rows, box) && make_ext_map(&tmTBx[ps], tx, t_rows, box);
+    if (maps_ok && mutual)
+      maps_ok = make_operand_map(&tmQB[ps], qb, q_rows, box) && make_ext_map(&tmQBx[ps], qx, q_rows, box);
+  }
+  if (maps_ok && mutual)
+    maps_ok = make_operand_map(&tmTA, tb, t_rows, kTcBM) && make_operand_map(&tmTAc, tbc, t_rows, kTcBM);
+  if (!maps_ok) return set_error(ctx, PSIFT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   std::vector<TcPair> tcp(2 * na);
   std::vector<RerankJob> rj(2 * na);
   TcPlan plan[4] = {};
@@ -273,7 +279,8 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     cf += (long long)kTcSplits * nA;
     T.a_row0 = (int)a_row0;
     T.b_row0 = (int)b_row0;
-    T.bt = (nB + kTcBN - 1) / kTcBN;
+    T.bt[0] = (nB + kTcBN1 - 1) / kTcBN1;
+    T.bt[1] = (nB + kTcBN - 1) / kTcBN;
     T.at[0] = (nA + kTcBM - 1) / kTcBM;
   };
   // pass 1's tile order of one direction: problems in order, equal ranges over the CTAs
@@ -283,8 +290,8 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     for (int k = 0; k < na; ++k) {
       TcPair& T = tcp[dir * na + k];
       T.g0[0] = total;
-      total += (long long)T.at[0] * T.bt;
-      bt_max = std::max(bt_max, T.bt);
+      total += (long long)T.at[0] * T.bt[0];
+      bt_max = std::max(bt_max, T.bt[0]);
     }
     long long r = std::max<long long>((total + tc_ctas - 1) / tc_ctas,
                                       (bt_max - 1 + kTcSplits - 2) / (kTcSplits - 1));
@@ -357,19 +364,19 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
   for (int dir = 0; dir < (mutual ? 2 : 1); ++dir) {
     const CUtensorMap& A = dir == 0 ? tmQA : tmTA;
     const CUtensorMap& Ac = dir == 0 ? tmQAc : tmTAc;
-    const CUtensorMap& B = dir == 0 ? tmTB : tmQB;
-    const CUtensorMap& Bx = dir == 0 ? tmTBx : tmQBx;
+    const CUtensorMap* B = dir == 0 ? tmTB : tmQB;    // [pass]
+    const CUtensorMap* Bx = dir == 0 ? tmTBx : tmQBx;
     TcPair* probs = d_tcp + dir * na;
     TcPlan* pl = d_plan + 2 * dir;
     const RerankJob* jobs_dir = d_rj + dir * na;
     const int rows = dir == 0 ? max_a : max_b;
     const char* what = "match_tc pass 1";
-    cudaError_t e = launch_match_tc(A, B, tmOnes, Bx, probs, na, pl, ctas1[dir], ctx->d_error, 0, st);
+    cudaError_t e = launch_match_tc(A, B[0], tmOnes, Bx[0], probs, na, pl, ctas1[dir], ctx->d_error, 0, st);
     if (e == cudaSuccess && (what = "window", true)) e = launch_window(jobs_dir, na, rows, st);
     if (e == cudaSuccess && (what = "tc_plan", true)) e = launch_tc_plan(probs, na, pl, tc_ctas, st);
     if (e == cudaSuccess && (what = "gather_rows", true)) e = launch_gather_rows(d_gj + dir * na, na, rows, st);
     if (e == cudaSuccess && (what = "match_tc pass 2", true))
-      e = launch_match_tc(Ac, B, tmOnes, Bx, probs, na, pl, tc_ctas, ctx->d_error, 1, st);
+      e = launch_match_tc(Ac, B[1], tmOnes, Bx[1], probs, na, pl, tc_ctas, ctx->d_error, 1, st);
     if (e == cudaSuccess && (what = "rerank", true))
       e = launch_rerank(jobs_dir, na, rows, scan_rows + (dir == 0 ? 0 : q_rows), scan_count + dir, 2 * ctx->num_sms, st);
     ctx->launches += 6;

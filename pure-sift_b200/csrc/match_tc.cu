@@ -51,11 +51,21 @@ constexpr int kEpiParts = 4;                      // epilogue warps per TMEM lan
 constexpr int kEpiWarps = 4 * kEpiParts;          // warps 2 .. 2 + kEpiWarps - 1
 constexpr int kTcThreads = 32 * (2 + kEpiWarps);  // warp 0 TMA, warp 1 MMA, then the epilogue
 constexpr int kBM = kTcBM;
-constexpr int kBN = kTcBN;       // B tile rows = MMA N = columns of one accumulator stage
-constexpr int kAccStages = 4;    // TMEM: four 128 x 128 f32 accumulators (512 columns)
-constexpr int kBStages = 3;      // B tiles in flight
-static_assert(kBN / kEpiParts == 32, "one 32-column TMEM load per epilogue warp and tile");
-static_assert(kAccStages * kBN == 512, "TMEM columns");
+// Per pass: B tile rows = MMA N = columns of one accumulator stage.  Pass 1 uses
+// N = 256 (two 128 x 256 accumulators): its fold is cheap, and an M = 128, N = 128
+// MMA keeps the tensor pipe about half busy.  Pass 2, with the heavier collection
+// fold, uses N = 128 (four accumulators).
+template <int MODE>
+struct TcShape {
+  static constexpr int BN = MODE == 0 ? kTcBN1 : kTcBN;
+  static constexpr int AccStages = 512 / BN;  // TMEM: 512 columns
+  static constexpr int Cols = BN / kEpiParts;  // columns per epilogue warp and tile
+  static constexpr uint32_t BStage = 2u * BN * 128u + BN * 32u;  // two halves, then the norm extension
+  // kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M = 128, N = BN
+  static constexpr uint32_t Idesc =
+      (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+};
+static_assert(TcShape<0>::Cols == 64 && TcShape<1>::Cols == 32, "epilogue TMEM loads of 32 columns");
 constexpr uint32_t kSpinLimit = 1u << 25;
 constexpr int kColl = 32;   // window indices kept per (split, row)
 constexpr int kXColl = 16;  // window indices a column part 1..3 hands to part 0 (more: exact scan)
@@ -124,17 +134,14 @@ __device__ __forceinline__ uint64_t sw32_desc(uint32_t saddr) {
   return d;
 }
 
-// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=128.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
-                            ((uint32_t)(kBM >> 4) << 24);
-
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
   const uint32_t z = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
       : "memory");
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
@@ -169,17 +176,24 @@ __device__ __forceinline__ void tmem_wait32(uint32_t (&r)[32]) {
 
 // Smem map (offsets from a 1024-aligned base).
 constexpr uint32_t kAStage = 2u * kBM * 128u;                     // two 64-column halves of 128 rows
-constexpr uint32_t kBStage = 2u * kBN * 128u + kBN * 32u;         // two halves, then the norm extension
 constexpr uint32_t kSmA = 0;                                      // 2 A stages
 constexpr uint32_t kSmAx = 2 * kAStage;                           // A norm extension: 128 rows x 32 B
-constexpr uint32_t kSmB = kSmAx + kBM * 32u;                      // kBStages B stages
-constexpr uint32_t kSmBar = kSmB + kBStages * kBStage;            // barriers
-// epilogue exchange, per row and column part 1..kEpiParts-1: pass 1 the part's two
-// largest values, pass 2 its count and up to kXColl indices
-constexpr uint32_t kSmX = kSmBar + 256;
-constexpr uint32_t kSmTotal = kSmX + (kEpiParts - 1) * kBM * (kXColl + 2) * 4 + 1024;  // + alignment slack
-static_assert(kSmB % 1024 == 0 && kBStage % 1024 == 0 && kAStage % 1024 == 0, "128B-swizzle atoms");
-static_assert(kSmTotal <= 227 * 1024, "shared memory per CTA");
+constexpr uint32_t kSmB = kSmAx + kBM * 32u;                      // the B stages
+static_assert(kSmB % 1024 == 0 && TcShape<0>::BStage % 1024 == 0 && TcShape<1>::BStage % 1024 == 0 &&
+                  kAStage % 1024 == 0,
+              "128B-swizzle atoms");
+// Per pass: B tiles in flight, then barriers, then the epilogue exchange per row and column part
+// 1..kEpiParts-1 (pass 1: the part's two largest values; pass 2: its count and up
+// to kXColl indices).
+template <int MODE>
+struct TcLayout {
+  static constexpr int kBStages = MODE == 0 ? 2 : 3;
+  static constexpr int kXStride = MODE == 0 ? 2 : kXColl + 2;  // ints per (part, row)
+  static constexpr uint32_t kSmBar = kSmB + kBStages * TcShape<MODE>::BStage;
+  static constexpr uint32_t kSmX = kSmBar + 256;
+  static constexpr uint32_t kSmTotal = kSmX + (kEpiParts - 1) * kBM * kXStride * 4 + 1024;  // + alignment slack
+  static_assert(kSmTotal <= 227 * 1024, "shared memory per CTA");
+};
 
 // The CTA's range of the pass's tiles is cut into pieces, one per A tile it
 // touches: problem k, A tile a, B tiles [b, b + len), and the piece's slot among
@@ -202,7 +216,7 @@ __device__ __forceinline__ int find_problem(const TcPair* P, int n, int mode, lo
 __device__ __forceinline__ Piece make_piece(const TcPair* P, int mode, int R, int k, long long g,
                                             long long g_end) {
   Piece p;
-  const int bt = P[k].bt;
+  const int bt = P[k].bt[mode];
   const long long off = g - P[k].g0[mode];
   p.k = k;
   p.a = (int)(off / bt);
@@ -236,9 +250,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const __grid_constant__ CUtensorMap tmAx, const __grid_constant__ CUtensorMap tmBx,
                     const TcPair* __restrict__ P, int n_problems, const TcPlan* __restrict__ plan, uint32_t* err) {
   constexpr int mode = MODE;
+  using L = TcLayout<MODE>;
+  using Sh = TcShape<MODE>;
+  constexpr int kBStages = L::kBStages;
+  constexpr int kBN = Sh::BN;
+  constexpr int kAccStages = Sh::AccStages;
+  constexpr uint32_t kBStage = Sh::BStage;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kSmBar);  // [kBStages] B tile landed
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::kSmBar);  // [kBStages] B tile landed
   uint64_t* empty = full + kBStages;                             // [kBStages] B tile consumed by its MMAs
   uint64_t* afull = empty + kBStages;                            // [2] A tile landed
   uint64_t* aempty = afull + 2;                                  // [2] A tile's last MMA done
@@ -373,10 +393,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           for (int kk = 0; kk < 8; ++kk) {
             const uint32_t half = (uint32_t)(kk >> 2), koff = (uint32_t)(kk & 3) * 32u;
             umma_bf16(d, sw128_desc(a_base + half * (kBM * 128) + koff),
-                      sw128_desc(b_base + half * (kBN * 128) + koff), kk > 0 ? 1u : 0u);
+                      sw128_desc(b_base + half * (kBN * 128) + koff), Sh::Idesc, kk > 0 ? 1u : 0u);
           }
           // the norm extension: D += h_j + l_j
-          umma_bf16(d, sw32_desc(ax), sw32_desc(b_base + 2 * kBN * 128), 1u);
+          umma_bf16(d, sw32_desc(ax), sw32_desc(b_base + 2 * kBN * 128), Sh::Idesc, 1u);
           umma_commit(&empty[bs]);
           umma_commit(&accf[s]);
           last_bar = &accf[s];
@@ -410,7 +430,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int quarter = warp & 3;
     const int part = (warp - 2) >> 2;
     const int row_in_tile = quarter * 32 + lane;
-    int* xrow = reinterpret_cast<int*>(smem + kSmX) + ((part > 0 ? part - 1 : 0) * kBM + row_in_tile) * (kXColl + 2);
+    int* xrow = reinterpret_cast<int*>(smem + L::kSmX) + ((part > 0 ? part - 1 : 0) * kBM + row_in_tile) * L::kXStride;
     const float inf = __int_as_float(0x7f800000);
     bool live = true;
     int s = 0;
@@ -468,46 +488,73 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           }
         }
       };
-      // Tiles of the piece, two register sets: tile j+1's TMEM load is in flight
-      // while tile j is folded; a stage is released as soon as its values are in
-      // registers.
-      const uint32_t tq = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(part * 32);
-      const int col0 = pc.b * kBN + part * 32;
+      // Each wait covers two 32-column TMEM loads (twice the bytes in flight per
+      // warp): pass 1 the warp's 64 columns of one tile, pass 2 its 32 columns of
+      // two consecutive tiles.  The accumulators are released as soon as their
+      // values are in registers, then the values are folded.
+      const uint32_t tq = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(part * Sh::Cols);
+      const int col0 = pc.b * kBN + part * Sh::Cols;
       uint32_t ra[32], rb[32];
-      auto acquire = [&](uint32_t(&rr)[32]) {
-        if (live && !__all_sync(0xffffffffu, mbar_wait(&accf[s], sph, abort_flag))) {
+      // waits for accumulator st; false (nothing to load) on timeout
+      auto ready = [&](int st, uint32_t ph) -> bool {
+        if (live && !__all_sync(0xffffffffu, mbar_wait(&accf[st], ph, abort_flag))) {
           live = false;
           atomicOr(err, kErrTimeout);
           *abort_flag = 1;
         }
-        if (live) {
-          tc_fence_after();
-          __syncwarp();
-          tmem_ld32_nowait(tq + (uint32_t)(s * kBN), rr);
-        }
+        if (!live) return false;
+        tc_fence_after();
+        __syncwarp();
+        return true;
       };
-      auto release = [&](uint32_t(&rr)[32]) {
-        if (live) {
-          tmem_wait32(rr);
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&acce[s]);
-        }
-        if (++s == kAccStages) {
-          s = 0;
+      auto advance = [&](int n) {
+        s += n;
+        if (s >= kAccStages) {
+          s -= kAccStages;
           sph ^= 1u;
         }
       };
-      acquire(ra);
-      release(ra);
-      for (int j = 0; j < pc.len; j += 2) {
-        if (j + 1 < pc.len) acquire(rb);
-        if (live) fold(ra, col0 + j * kBN);
-        if (j + 1 >= pc.len) break;
-        release(rb);
-        if (j + 2 < pc.len) acquire(ra);
-        if (live) fold(rb, col0 + (j + 1) * kBN);
-        if (j + 2 < pc.len) release(ra);
+      if constexpr (mode == 0) {
+        for (int j = 0; j < pc.len; ++j) {
+          const bool la = ready(s, sph);
+          if (la) {
+            tmem_ld32_nowait(tq + (uint32_t)(s * kBN), ra);
+            tmem_ld32_nowait(tq + (uint32_t)(s * kBN) + 32u, rb);
+            // every issued load completes before the registers are read (or the CTA leaves)
+            tmem_wait32(ra);
+            tmem_wait32(rb);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[s]);
+            fold(ra, col0 + j * kBN);
+            fold(rb, col0 + j * kBN + 32);
+          }
+          advance(1);
+        }
+      } else {
+        for (int j = 0; j < pc.len; j += 2) {
+          const bool two = j + 1 < pc.len;
+          const int s1 = s + 1 == kAccStages ? 0 : s + 1;
+          const uint32_t ph1 = s + 1 == kAccStages ? sph ^ 1u : sph;
+          const bool la = ready(s, sph);
+          if (la) tmem_ld32_nowait(tq + (uint32_t)(s * kBN), ra);
+          const bool lb = two && ready(s1, ph1);
+          if (lb) tmem_ld32_nowait(tq + (uint32_t)(s1 * kBN), rb);
+          // every issued load completes before the registers are read (or the CTA leaves)
+          if (la) tmem_wait32(ra);
+          if (lb) tmem_wait32(rb);
+          if (live) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+              mbar_arrive(&acce[s]);
+              if (two) mbar_arrive(&acce[s1]);
+            }
+            fold(ra, col0 + j * kBN);
+            if (two) fold(rb, col0 + (j + 1) * kBN);
+          }
+          advance(two ? 2 : 1);
+        }
       }
       // The row's largest D, and the second largest of the class maxima: a lower
       // bound on the row's second largest D (equal to it unless the two largest
@@ -534,7 +581,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if (part == 0 && row_ok && live) {
         bool part_overflow = false;
         for (int p = 1; p < kEpiParts; ++p) {
-          const int* x = reinterpret_cast<const int*>(smem + kSmX) + ((p - 1) * kBM + row_in_tile) * (kXColl + 2);
+          const int* x = reinterpret_cast<const int*>(smem + L::kSmX) + ((p - 1) * kBM + row_in_tile) * L::kXStride;
           if constexpr (mode == 0) {
             const float x0 = __int_as_float(x[0]), x1 = __int_as_float(x[1]);
             u1 = max3f(u1, x1, fminf(u0, x0));
@@ -680,6 +727,19 @@ __device__ __forceinline__ float exact_d2(const float* __restrict__ a, const flo
   return s;
 }
 
+// A row's result: best / index / second, and for the forward pass of a mutual
+// match the target's mark when the reference's ratio test (src/pipeline.rs:1789-1794)
+// accepts the row.
+__device__ __forceinline__ void rerank_row_out(const RerankJob& J, int row, float b, int bi, float sec) {
+  const bool forward = J.second != nullptr;
+  if (forward && J.flags && sec > 1e-12f && b < __int_as_float(0x7f800000) && bi < J.nb) {
+    if (sqrtf(b) / sqrtf(sec) < J.ratio) J.flags[bi] = 1;
+  }
+  J.best[row] = b;
+  J.best_idx[row] = bi;
+  if (forward) J.second[row] = sec;
+}
+
 // Per A row (thread): merge the splits' two smallest values, certify rejection
 // or set the candidate window thr = a_(2) + 2 eps (forward) / a_(1) + 2 eps (reverse).
 __global__ void window_kernel(const RerankJob* __restrict__ jobs) {
@@ -712,11 +772,15 @@ __global__ void window_kernel(const RerankJob* __restrict__ jobs) {
     if (lo1 > 0.0 && lo1 >= r * r * hi2 * (1.0 + 1e-5)) thr = -inf;
   }
   J.thr[row] = thr;
-  if (thr != -inf)
-    for (int s = 0; s < J.splits; ++s) J.coll_cnt[(long long)s * J.na + row] = 0;  // slots without a piece stay empty
-  // rows with a window go to pass 2 (compacted; the order does not matter: every
-  // row's collection depends on that row alone and lands in its own slot)
-  if (J.ccount && thr != -inf) J.rowmap[atomicAdd(J.ccount, 1)] = row;
+  if (thr == -inf) {
+    // nothing to rank: the row's result is final here (no match / not a candidate)
+    rerank_row_out(J, row, inf, 0x7fffffff, inf);
+    return;
+  }
+  for (int s = 0; s < J.splits; ++s) J.coll_cnt[(long long)s * J.na + row] = 0;  // slots without a piece stay empty
+  // rows with a window go to pass 2 and the re-rank (compacted; the order does not
+  // matter: every row's collection depends on that row alone and lands in its own slot)
+  J.rowmap[atomicAdd(J.ccount, 1)] = row;
 }
 
 // One warp per compacted row: its 256 bytes of bf16 descriptor, coalesced.
@@ -729,60 +793,103 @@ __global__ void gather_rows_kernel(const GatherJob* __restrict__ jobs) {
   reinterpret_cast<uint2*>(G.dst + (size_t)c * 128)[lane] = reinterpret_cast<const uint2*>(G.src + (size_t)r * 128)[lane];
 }
 
-// A row's result: best / index / second, and for the forward pass of a mutual
-// match the target's mark when the reference's ratio test (src/pipeline.rs:1789-1794)
-// accepts the row.
-__device__ __forceinline__ void rerank_row_out(const RerankJob& J, int row, float b, int bi, float sec) {
-  const bool forward = J.second != nullptr;
-  if (forward && J.flags && sec > 1e-12f && b < __int_as_float(0x7f800000) && bi < J.nb) {
-    if (sqrtf(b) / sqrtf(sec) < J.ratio) J.flags[bi] = 1;
-  }
-  J.best[row] = b;
-  J.best_idx[row] = bi;
-  if (forward) J.second[row] = sec;
-}
+// One warp per kept A row (window_kernel's compacted list): exact reference
+// distances over the window candidates (every index with a <= thr, collected by
+// the second GEMM pass).  Candidates go
+// eight at a time: every lane loads its 16 bytes of each candidate's B row (all
+// eight loads in flight) and writes the squared differences to shared memory,
+// then lane c adds up candidate c's 128 terms in the reference's order.  A row
+// whose window overflowed kColl in some slot is left to rerank_scan_kernel.
+constexpr int kRrBatch = 8;
+constexpr int kRrStride = 132;  // floats per staged candidate (conflict-free reads across candidates)
 
-// One warp per A row: exact reference distances over the window candidates
-// (every index with a <= thr, collected by the second GEMM pass), or over all
-// B rows when a split's window overflowed kColl.
-__global__ void rerank_kernel(const RerankJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(256) rerank_kernel(const RerankJob* __restrict__ jobs) {
+  __shared__ __align__(16) float terms[8][kRrBatch * kRrStride];
   const RerankJob& J = jobs[blockIdx.y];
-  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= J.na) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // the rows window_kernel kept (the others' results are final already)
+  const int c_row = blockIdx.x * 8 + warp;
+  if (c_row >= *J.ccount) return;
+  const int row = J.rowmap[c_row];
   const float inf = __int_as_float(0x7f800000);
   float b = inf, sec = inf;
   int bi = 0x7fffffff;
-  if (J.thr[row] != -inf) {
-    bool overflow = false;
-    for (int s = 0; s < J.splits; ++s) overflow |= J.coll_cnt[(long long)s * J.na + row] > kColl;
-    const float* arow = J.a + (size_t)row * 128;
-    if (!overflow) {
-      for (int s = 0; s < J.splits; ++s) {
-        const long long o = (long long)s * J.na + row;
-        const int c = J.coll_cnt[o];
-        for (int k = lane; k < c; k += 32) {
-          const int t = J.coll_idx[o * kColl + k];
-          top2_push(b, bi, sec, exact_d2(arow, J.b + (size_t)t * 128), t);
+  // the slots' counts and their running offsets (same in every lane)
+  int cnt[kTcSplits], total = 0;
+  bool overflow = false;
+#pragma unroll
+  for (int sl = 0; sl < kTcSplits; ++sl) {
+    cnt[sl] = J.coll_cnt[(long long)sl * J.na + row];
+    overflow |= cnt[sl] > kColl;
+    total += cnt[sl];
+  }
+  if (overflow) {
+    // the exact scan over all B rows is left to rerank_scan_kernel (a CTA per row)
+    if (lane == 0) {
+      atomicAdd(J.fallbacks, 1u);
+      J.scan_rows[atomicAdd(J.scan_count, 1)] = make_int2((int)blockIdx.y, row);
+    }
+    return;
+  }
+  const float4 a4 = reinterpret_cast<const float4*>(J.a + (size_t)row * 128)[lane];
+  float* tw = terms[warp];
+  for (int c0 = 0; c0 < total; c0 += kRrBatch) {
+    const int nb = min(kRrBatch, total - c0);
+    int idx[kRrBatch];
+    float4 bv[kRrBatch];
+#pragma unroll
+    for (int c = 0; c < kRrBatch; ++c) {
+      // candidate c0 + c: its slot and position there
+      int m = c0 + c, sl = 0;
+#pragma unroll
+      for (int q = 0; q < kTcSplits - 1; ++q)
+        if (sl == q && m >= cnt[q]) {
+          m -= cnt[q];
+          sl = q + 1;
         }
-      }
-    } else {
-      // the exact scan over all B rows is left to rerank_scan_kernel (a CTA per row)
-      if (lane == 0) {
-        atomicAdd(J.fallbacks, 1u);
-        J.scan_rows[atomicAdd(J.scan_count, 1)] = make_int2((int)blockIdx.y, row);
-      }
-      return;
+      idx[c] = c < nb ? J.coll_idx[((long long)sl * J.na + row) * kColl + m] : 0;
     }
 #pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) {
-      const float b2 = __shfl_xor_sync(0xffffffffu, b, off);
-      const int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
-      const float s2 = __shfl_xor_sync(0xffffffffu, sec, off);
-      top2_merge(b, bi, sec, b2, i2, s2);
+    for (int c = 0; c < kRrBatch; ++c)
+      if (c < nb) bv[c] = reinterpret_cast<const float4*>(J.b + (size_t)idx[c] * 128)[lane];
+#pragma unroll
+    for (int c = 0; c < kRrBatch; ++c) {
+      if (c < nb) {
+        float4 d;
+        d.x = a4.x - bv[c].x;
+        d.y = a4.y - bv[c].y;
+        d.z = a4.z - bv[c].z;
+        d.w = a4.w - bv[c].w;
+        *reinterpret_cast<float4*>(tw + c * kRrStride + 4 * lane) =
+            make_float4(d.x * d.x, d.y * d.y, d.z * d.z, d.w * d.w);
+      }
     }
-    if (lane == 0) rerank_row_out(J, row, b, bi, sec);
-    return;
+    __syncwarp();
+    if (lane < nb) {
+      const float* t = tw + lane * kRrStride;
+      float sum = 0.0f;
+#pragma unroll 8
+      for (int i = 0; i < 128; i += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(t + i);
+        sum += v.x;
+        sum += v.y;
+        sum += v.z;
+        sum += v.w;
+      }
+      int my = idx[0];
+#pragma unroll
+      for (int c = 1; c < kRrBatch; ++c)
+        if (lane == c) my = idx[c];
+      top2_push(b, bi, sec, sum, my);
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    const float b2 = __shfl_xor_sync(0xffffffffu, b, off);
+    const int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
+    const float s2 = __shfl_xor_sync(0xffffffffu, sec, off);
+    top2_merge(b, bi, sec, b2, i2, s2);
   }
   if (lane == 0) rerank_row_out(J, row, b, bi, sec);
 }
@@ -877,8 +984,8 @@ __global__ void __launch_bounds__(1024) tc_plan_kernel(TcPair* __restrict__ P, i
     if (k < n) {
       const int at = (*P[k].ccount + kTcBM - 1) / kTcBM;
       P[k].at[1] = at;
-      tiles = (long long)at * P[k].bt;
-      if (at > 0) atomicMax(&bt_max, P[k].bt);
+      tiles = (long long)at * P[k].bt[1];
+      if (at > 0) atomicMax(&bt_max, P[k].bt[1]);
     }
     // block-wide exclusive scan of the tile counts
     long long v = tiles;
@@ -971,12 +1078,13 @@ cudaError_t launch_match_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, cons
                             int ctas, uint32_t* err, int mode, cudaStream_t st) {
   if (ctas <= 0 || n_problems <= 0) return cudaSuccess;
   const void* fn = mode == 0 ? (const void*)match_tc_kernel<0> : (const void*)match_tc_kernel<1>;
-  cudaError_t e = ensure_smem_attr(fn, kSmTotal);
+  const uint32_t smem = mode == 0 ? TcLayout<0>::kSmTotal : TcLayout<1>::kSmTotal;
+  cudaError_t e = ensure_smem_attr(fn, smem);
   if (e != cudaSuccess) return e;
   if (mode == 0)
-    match_tc_kernel<0><<<ctas, kTcThreads, kSmTotal, st>>>(tmA, tmB, tmAx, tmBx, problems, n_problems, plan, err);
+    match_tc_kernel<0><<<ctas, kTcThreads, smem, st>>>(tmA, tmB, tmAx, tmBx, problems, n_problems, plan, err);
   else
-    match_tc_kernel<1><<<ctas, kTcThreads, kSmTotal, st>>>(tmA, tmB, tmAx, tmBx, problems, n_problems, plan, err);
+    match_tc_kernel<1><<<ctas, kTcThreads, smem, st>>>(tmA, tmB, tmAx, tmBx, problems, n_problems, plan, err);
   return cudaGetLastError();
 }
 
@@ -1001,7 +1109,7 @@ cudaError_t launch_gather_rows(const GatherJob* jobs, int n_jobs, int max_rows, 
 
 cudaError_t launch_rerank(const RerankJob* jobs, int n_jobs, int max_rows, const int2* scan_rows,
                           const int* scan_count, int scan_ctas, cudaStream_t st) {
-  dim3 grid((max_rows + 7) / 8, n_jobs);
+  dim3 grid((max_rows + 7) / 8, n_jobs);  // a warp per row
   rerank_kernel<<<grid, 256, 0, st>>>(jobs);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;

@@ -56,7 +56,8 @@ struct PngImage {
   int n_pass = 1;
   uint32_t pass_w[7] = {0}, pass_h[7] = {0};
   size_t pass_rb[7] = {0};         // bytes per row, filter byte excluded
-  size_t pass_in[7] = {0};         // offset of the pass in the inflated stream
+  size_t pass_in[7] = {0};         // offset of the pass's row slots in the inflated buffer
+  size_t pass_stride[7] = {0};     // bytes per row slot: filter byte at +15, the row at +16 (16-byte aligned)
   size_t pass_out[7] = {0};        // offset of the pass in the unfiltered buffer
   size_t raw_bytes = 0, unf_bytes = 0;
 };
@@ -148,8 +149,9 @@ psift_status parse_png(psift_ctx* ctx, const uint8_t* data, size_t len, bool enf
     P->pass_rb[p] = (pw == 0 || ph == 0) ? 0 : ((size_t)pw * bits_pp + 7) / 8;
     P->pass_in[p] = in;
     P->pass_out[p] = out;
+    P->pass_stride[p] = align_up(P->pass_rb[p], 16) + 16;
     if (P->pass_rb[p]) {
-      in += (size_t)ph * (1 + P->pass_rb[p]);
+      in += (size_t)ph * P->pass_stride[p];
       out += (size_t)ph * P->pass_rb[p];
     }
   }
@@ -158,33 +160,50 @@ psift_status parse_png(psift_ctx* ctx, const uint8_t* data, size_t len, bool enf
   return PSIFT_OK;
 }
 
-// The zlib stream of the IDAT chunks into dst (exactly raw_bytes; a stream with
-// trailing data past the image is accepted).  Returns an empty string or the error.
+// The zlib stream of the IDAT chunks into dst, each scanline (filter byte, then
+// the row) into its slot: filter byte at +15, row at +16, so that every row
+// starts 16-byte aligned for the device's copies.  A stream with trailing data
+// past the image is accepted.  Returns an empty string or the error.
 std::string inflate_png(const PngImage& P, uint8_t* dst) {
   z_stream zs;
   std::memset(&zs, 0, sizeof zs);
   if (inflateInit(&zs) != Z_OK) return "zlib initialisation failed";
-  zs.next_out = dst;
-  zs.avail_out = (uInt)P.raw_bytes;
+  size_t chunk = 0;
+  zs.next_in = const_cast<Bytef*>(P.idat[0].first);
+  zs.avail_in = (uInt)P.idat[0].second;
   int r = Z_OK;
-  for (size_t c = 0; c < P.idat.size() && r == Z_OK && zs.avail_out > 0; ++c) {
-    zs.next_in = const_cast<Bytef*>(P.idat[c].first);
-    zs.avail_in = (uInt)P.idat[c].second;
-    while (zs.avail_in > 0 && zs.avail_out > 0 && r == Z_OK) r = inflate(&zs, Z_NO_FLUSH);
+  std::string err;
+  for (int p = 0; p < P.n_pass && err.empty(); ++p) {
+    if (!P.pass_rb[p]) continue;
+    for (uint32_t row = 0; row < P.pass_h[p] && err.empty(); ++row) {
+      zs.next_out = dst + P.pass_in[p] + (size_t)row * P.pass_stride[p] + 15;
+      zs.avail_out = (uInt)(1 + P.pass_rb[p]);
+      while (zs.avail_out > 0) {
+        if (zs.avail_in == 0) {
+          if (++chunk >= P.idat.size()) break;
+          zs.next_in = const_cast<Bytef*>(P.idat[chunk].first);
+          zs.avail_in = (uInt)P.idat[chunk].second;
+          continue;
+        }
+        r = inflate(&zs, Z_NO_FLUSH);
+        if (r == Z_STREAM_END) break;
+        if (r != Z_OK) break;
+      }
+      if (r != Z_OK && r != Z_STREAM_END) err = "corrupt deflate stream (zlib " + std::to_string(r) + ")";
+      else if (zs.avail_out > 0) err = "image data is truncated";
+    }
   }
-  const size_t got = P.raw_bytes - zs.avail_out;
   inflateEnd(&zs);
-  if (r != Z_OK && r != Z_STREAM_END) return "corrupt deflate stream (zlib " + std::to_string(r) + ")";
-  if (got != P.raw_bytes) return "image data is truncated";
-  return std::string();
+  return err;
 }
 
 // ------------------------------------------------------------------ kernels
 struct PngPlane {
-  const uint8_t* in;  // rows x (1 + row_bytes): filter byte (checked on the host), then the filtered row
+  const uint8_t* in;  // row slots: filter byte at +15 (checked on the host), the filtered row at +16
   uint8_t* out;       // rows x row_bytes
   uint32_t rows;
   uint32_t row_bytes;
+  uint32_t stride;    // bytes per row slot (a multiple of 16)
 };
 
 // Adam7 constants of pass p as nibble p of a word (device code).
@@ -197,34 +216,68 @@ __device__ __forceinline__ uint32_t paeth(uint32_t a, uint32_t b, uint32_t c) {
   return (pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c);
 }
 
-// One warp per plane.  Rows go 32 at a time; at step s lane t reconstructs
-// unit (pixel) s - t of row g + t.  The row above at that unit is what lane t - 1
-// reconstructed at step s - 1 (a shuffle), the unit before it lane t - 1's value
-// one step earlier; lane 0 reads the previous group's last row from memory.
-// Units are UNIT bytes (the filter's byte distance), packed in two words.
+constexpr int kRing = 512;  // bytes of a lane's row staged in shared memory (four 128-byte chunks)
+
+// One warp per plane (a CTA per plane).  Rows go 32 at a time; at step s lane t
+// reconstructs unit (pixel) s - t of row g + t, so the row above at that unit
+// is what lane t - 1 reconstructed at step s - 1 (a shuffle) and the unit before
+// it lane t - 1's value one step earlier; lane 0 takes the previous group's last
+// row from shared memory (above_smem) or memory.  Each lane's filtered row
+// streams through a ring of 128-byte chunks in shared memory, the next chunk
+// copied asynchronously while the current one is consumed (lane 31 trails lane 0
+// by at most 31 units = 248 bytes, inside the ring).  Units are UNIT bytes, the
+// filter's byte distance.
 template <int UNIT>
-__global__ void __launch_bounds__(128) png_unfilter_kernel(const PngPlane* __restrict__ planes, int n_planes) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int pi = blockIdx.x * 4 + warp;
-  if (pi >= n_planes) return;
-  const PngPlane P = planes[pi];
+__global__ void __launch_bounds__(32) png_unfilter_kernel(const PngPlane* __restrict__ planes, int above_smem) {
+  extern __shared__ __align__(16) uint8_t psm[];
+  uint8_t* ring = psm;                      // [32][kRing]
+  uint8_t* last = psm + 32 * kRing;         // [2][row_bytes rounded to 16]: the groups' last rows
+  const int lane = threadIdx.x;
+  const PngPlane P = planes[blockIdx.x];
   const uint32_t rb = P.row_bytes, npix = rb / UNIT;
+  const uint32_t rb16 = (rb + 15) & ~15u;
+  const uint32_t nchunks = (rb + 127) / 128;
+  uint8_t* my_ring = ring + lane * kRing;
   for (uint32_t g = 0; g < P.rows; g += 32) {
     const uint32_t r = g + lane;
     const bool row_ok = r < P.rows;
-    const uint8_t* src = P.in + (size_t)r * (1 + rb) + 1;
+    const uint8_t* slot = P.in + (size_t)r * P.stride;
+    const uint32_t f = row_ok ? slot[15] : 0u;
+    const uint8_t* src = slot + 16;
     uint8_t* dst = P.out + (size_t)r * rb;
-    const uint8_t* above = (r > 0) ? P.out + (size_t)(r - 1) * rb : nullptr;
-    const uint32_t f = row_ok ? P.in[(size_t)r * (1 + rb)] : 0u;
-    uint8_t a[UNIT], c[UNIT];  // left unit, above-left unit
+    const uint8_t* above_g = (g > 0) ? P.out + (size_t)(g - 1) * rb : nullptr;  // row g - 1 (lane 0)
+    const uint8_t* above_s = last + ((g / 32 + 1) & 1) * rb16;                  // the same row, staged
+    uint8_t* last_w = last + ((g / 32) & 1) * rb16;                              // this group's last row
+    // chunk c of this lane's row into ring slot c % 4 (16-byte copies inside the row slot)
+    auto fetch = [&](uint32_t c) {
+      if (row_ok && c < nchunks)
+        for (uint32_t q = 0; q < 8 && c * 128 + 16 * q < rb16; ++q)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                           (uint32_t)__cvta_generic_to_shared(my_ring + (c & 3) * 128 + 16 * q)),
+                       "l"(src + c * 128 + 16 * q)
+                       : "memory");
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    fetch(0);
+    fetch(1);
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    __syncwarp();
+    uint32_t cur = 0;
+    uint8_t a[UNIT], c[UNIT], mine_prev[UNIT];  // left unit, above-left unit, this lane's last unit
 #pragma unroll
-    for (int k = 0; k < UNIT; ++k) a[k] = c[k] = 0;
-    uint8_t mine_prev[UNIT];  // this lane's unit of the previous step (handed to lane + 1)
-#pragma unroll
-    for (int k = 0; k < UNIT; ++k) mine_prev[k] = 0;
+    for (int k = 0; k < UNIT; ++k) a[k] = c[k] = mine_prev[k] = 0;
     const uint32_t steps = npix + 31;
     for (uint32_t s = 0; s < steps; ++s) {
-      // the unit lane - 1 reconstructed at step s - 1, = this lane's above unit
+      // lane 0 (the leading lane) reached a new chunk with its unit's last byte:
+      // the chunk's successor is copied, the chunk itself is waited for
+      const uint32_t lead = min(s, npix - 1) * UNIT + UNIT - 1;
+      if ((lead >> 7) != cur) {
+        cur = lead >> 7;
+        fetch(cur + 1);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncwarp();
+      }
+      // the unit lane - 1 reconstructed at step s - 1 = this lane's above unit
       uint32_t w0 = 0, w1 = 0;
 #pragma unroll
       for (int k = 0; k < UNIT; ++k) {
@@ -239,9 +292,9 @@ __global__ void __launch_bounds__(128) png_unfilter_kernel(const PngPlane* __res
 #pragma unroll
       for (int k = 0; k < UNIT; ++k) b[k] = (uint8_t)((k < 4 ? w0 >> (8 * k) : w1 >> (8 * (k - 4))) & 0xFF);
       if (lane == 0) {
-        // the row above belongs to the previous group (already in memory) or is absent
 #pragma unroll
-        for (int k = 0; k < UNIT; ++k) b[k] = (act && above) ? above[(size_t)i * UNIT + k] : 0;
+        for (int k = 0; k < UNIT; ++k)
+          b[k] = (act && g > 0) ? (above_smem ? above_s[(size_t)i * UNIT + k] : above_g[(size_t)i * UNIT + k]) : 0;
       }
       if (act) {
         if (i == 0) {
@@ -250,18 +303,20 @@ __global__ void __launch_bounds__(128) png_unfilter_kernel(const PngPlane* __res
         }
 #pragma unroll
         for (int k = 0; k < UNIT; ++k) {
-          const uint32_t x = src[(size_t)i * UNIT + k];
+          const uint32_t x = my_ring[((uint32_t)i * UNIT + k) & (kRing - 1)];
           const uint32_t av = a[k], bv = r > 0 ? b[k] : 0u, cv = r > 0 ? c[k] : 0u;
           const uint32_t pred = f == 1 ? av : f == 2 ? bv : f == 3 ? (av + bv) >> 1 : f == 4 ? paeth(av, bv, cv) : 0u;
           const uint8_t v = (uint8_t)(x + pred);
           dst[(size_t)i * UNIT + k] = v;
+          if (lane == 31 && above_smem) last_w[(size_t)i * UNIT + k] = v;
           a[k] = v;
           c[k] = (uint8_t)bv;
           mine_prev[k] = v;
         }
       }
-      __syncwarp();  // this group's writes are visible to lane 0 of the next group
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncwarp();  // this group's rows (memory and the staged last row) are visible to the next group
   }
 }
 
@@ -421,8 +476,8 @@ psift_status inflate_range(psift_ctx* ctx, const std::vector<PngImage>& P, const
       std::string err = inflate_png(I, dst);
       for (int p = 0; err.empty() && p < I.n_pass; ++p) {
         if (!I.pass_rb[p]) continue;
-        const uint8_t* row = dst + I.pass_in[p];
-        for (uint32_t r = 0; r < I.pass_h[p]; ++r, row += 1 + I.pass_rb[p])
+        const uint8_t* row = dst + I.pass_in[p] + 15;
+        for (uint32_t r = 0; r < I.pass_h[p]; ++r, row += I.pass_stride[p])
           if (*row > 4) {
             err = "invalid filter type " + std::to_string((int)*row);
             break;
@@ -447,9 +502,15 @@ psift_status inflate_range(psift_ctx* ctx, const std::vector<PngImage>& P, const
 }
 
 template <int UNIT>
-cudaError_t launch_unfilter(const PngPlane* planes, int n, cudaStream_t st) {
+cudaError_t launch_unfilter(const PngPlane* planes, int n, uint32_t max_rb, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  png_unfilter_kernel<UNIT><<<(n + 3) / 4, 128, 0, st>>>(planes, n);
+  // the groups' last rows staged in shared memory when two of them fit
+  const size_t rb16 = (max_rb + 15) & ~size_t(15);
+  const bool above_smem = 32 * kRing + 2 * rb16 <= 200 * 1024;
+  const size_t smem = 32 * kRing + (above_smem ? 2 * rb16 : 0);
+  cudaError_t e = ensure_smem_attr((const void*)png_unfilter_kernel<UNIT>, smem);
+  if (e != cudaSuccess) return e;
+  png_unfilter_kernel<UNIT><<<n, 32, smem, st>>>(planes, above_smem ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -472,6 +533,7 @@ psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, co
   PngLumaJob* hj = reinterpret_cast<PngLumaJob*>(pin_desc + job_base) + b;
   const int units[6] = {1, 2, 3, 4, 6, 8};
   int count[6] = {0, 0, 0, 0, 0, 0};
+  uint32_t max_rb[6] = {0, 0, 0, 0, 0, 0};
   int np = 0;
   uint32_t max_px = 0;
   for (int u = 0; u < 6; ++u) {
@@ -481,8 +543,9 @@ psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, co
       for (int p = 0; p < I.n_pass; ++p) {
         if (!I.pass_rb[p]) continue;
         hp[np++] = PngPlane{S->dev + L.dev_raw[i] + I.pass_in[p], S->dev + L.dev_unf[i] + I.pass_out[p],
-                            I.pass_h[p], (uint32_t)I.pass_rb[p]};
+                            I.pass_h[p], (uint32_t)I.pass_rb[p], (uint32_t)I.pass_stride[p]};
         ++count[u];
+        max_rb[u] = std::max(max_rb[u], (uint32_t)I.pass_rb[p]);
       }
     }
   }
@@ -522,12 +585,12 @@ psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, co
   for (int u = 0; u < 6 && ce == cudaSuccess; ++u) {
     if (!count[u]) continue;
     switch (units[u]) {
-      case 1: ce = launch_unfilter<1>(dp + off, count[u], st); break;
-      case 2: ce = launch_unfilter<2>(dp + off, count[u], st); break;
-      case 3: ce = launch_unfilter<3>(dp + off, count[u], st); break;
-      case 4: ce = launch_unfilter<4>(dp + off, count[u], st); break;
-      case 6: ce = launch_unfilter<6>(dp + off, count[u], st); break;
-      default: ce = launch_unfilter<8>(dp + off, count[u], st); break;
+      case 1: ce = launch_unfilter<1>(dp + off, count[u], max_rb[u], st); break;
+      case 2: ce = launch_unfilter<2>(dp + off, count[u], max_rb[u], st); break;
+      case 3: ce = launch_unfilter<3>(dp + off, count[u], max_rb[u], st); break;
+      case 4: ce = launch_unfilter<4>(dp + off, count[u], max_rb[u], st); break;
+      case 6: ce = launch_unfilter<6>(dp + off, count[u], max_rb[u], st); break;
+      default: ce = launch_unfilter<8>(dp + off, count[u], max_rb[u], st); break;
     }
     off += count[u];
     ctx->launches++;
