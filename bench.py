@@ -1151,7 +1151,7 @@ def run_ours(args):
                            "blur_ms_per_variant": {r: e["ms"] for r, e in tune["blur"].items()},
                            "match_fp32_items_per_sm": tune["match_fp32"]["per_sm"],
                            "match_tc_items_per_sm": tune["match_tc"]["per_sm"],
-                           "variants": "blur outputs per thread 0: 4x8, 1: 8x8, 2: 4x4 (columns x rows)"}},
+                           "variants": "blur 0: 4x8, 1: 8x8, 2: 4x4 outputs per thread (columns x rows); 3: TMA tiles, persistent CTAs"}},
             "gpu_launches": int(launches),
             "e2e": {"value": e2e_value, "unit": "images/s", "h2d_bytes_per_step": B * WIDTH * HEIGHT,
                     "d2h_bytes_per_step": int(d2h),

@@ -115,8 +115,10 @@ psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
 
 /* Tile shapes, chosen by the library's autotuner.  No counterpart in the
  * reference.  Every choice computes identical results; only time differs.
- *  - PSIFT_TUNE_BLUR, index = radius 1..15: the level blur's outputs per thread
- *    (0: 4 columns x 8 rows, the default; 1: 8 x 8; 2: 4 x 4).
+ *  - PSIFT_TUNE_BLUR, index = radius 1..15: the level blur's kernel: outputs per
+ *    thread 0: 4 columns x 8 rows (the default), 1: 8 x 8, 2: 4 x 4; or 3: TMA
+ *    tiles with persistent CTAs (batches of at most 64 images; larger ones use 0).
+ *    Every variant computes the same values.
  *  - PSIFT_TUNE_MATCH_FP32 / PSIFT_TUNE_MATCH_TC, index 0: the matchers' work items
  *    per SM (default 2); a query tile's target tiles are split into that many
  *    ranges overall, which sets each CTA's target extent.
@@ -125,7 +127,7 @@ psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
  * n_pairs matching problems of n_desc x n_desc descriptors, both matcher paths)
  * and keeps the fastest in the context.  report (optional, report_capacity
  * doubles; report_count = the doubles written): per blur radius (radius, ms of
- * variants 0..2, chosen), then -1, then per matcher path (path 0 FP32 / 1 tensor
+ * variants 0..3, chosen), then -1, then per matcher path (path 0 FP32 / 1 tensor
  * core, ms for 1, 2, 4, 8 work items per SM, chosen). */
 #define PSIFT_TUNE_BLUR 0
 #define PSIFT_TUNE_MATCH_FP32 1

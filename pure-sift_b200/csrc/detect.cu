@@ -25,7 +25,8 @@ namespace psift {
 // Declared in pyramid.cu / extrema.cu / describe.cu.
 cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
                         int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant = 0,
-                        bool fused = false, const TileMap* tiles = nullptr);
+                        bool fused = false, const TileMap* tiles = nullptr, const ImagePlan* h_plans = nullptr,
+                        uint32_t* err = nullptr);
 cudaError_t launch_extrema_mark(const ImagePlan* plans, int n, int octave, int max_h, const ExtremaParams& prm,
                                 cudaStream_t st);
 cudaError_t launch_row_scan(const ImagePlan* plans, int n, uint32_t kp_cap, uint32_t* err, cudaStream_t st);
@@ -279,11 +280,13 @@ TileMap tile_map(const DetectJob& job, int o, int mh, int mw) {
 
 // One blur level (octave o, level s >= 1) of every image of the job.
 cudaError_t launch_level(const DetectJob& job, const SigmaSchedule& sc, int o, int s, int S, int mh, int mw,
-                         cudaStream_t st) {
+                         cudaStream_t st, uint32_t* err) {
   const int r = sc.level_radius[s];
   const TileMap tm = tile_map(job, o, mh, mw);
-  return launch_blur(0, sc.level_taps[s].data(), r, job.d_plans, job.n, o, s, S, mh, mw, st,
-                     r >= 0 && r < 16 ? job.blur_variant[r] : 0, job.blur_fused, &tm);
+  int variant = r >= 0 && r < 16 ? job.blur_variant[r] : 0;
+  if (variant == 3 && job.n > kTileMapMax) variant = 0;  // the TMA kernel's tile list holds kTileMapMax images
+  return launch_blur(0, sc.level_taps[s].data(), r, job.d_plans, job.n, o, s, S, mh, mw, st, variant,
+                     job.blur_fused, &tm, job.plans.data(), err);
 }
 
 // Queue every stage of the path for the batch (no host synchronisation).
@@ -344,7 +347,7 @@ psift_status launch_detect(psift_ctx* ctx, DetectJob& job, const psift_sift_conf
     {
       StageScope sc_pyr(ctx, STAGE_PYRAMID, st);
       for (int s = 1; s <= S + 2; ++s) {
-        cudaError_t e = launch_level(job, sc, o, s, S, mh, mw, st);
+        cudaError_t e = launch_level(job, sc, o, s, S, mh, mw, st, ctx->d_error);
         ctx->launches++;
         if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
       }
@@ -421,7 +424,7 @@ psift_status launch_pyramid_only(psift_ctx* ctx, DetectJob& job, const psift_sif
       if (e != cudaSuccess) return cuda_error(ctx, e, "blur(init)");
     }
     for (int s = 1; s <= S + 2; ++s) {
-      cudaError_t e = launch_level(job, sc, o, s, S, mh, mw, st);
+      cudaError_t e = launch_level(job, sc, o, s, S, mh, mw, st, ctx->d_error);
       ctx->launches++;
       if (e != cudaSuccess) return cuda_error(ctx, e, "blur(level)");
     }
@@ -636,7 +639,7 @@ psift_status detect_host(psift_ctx* ctx, const void* image, int kind, uint32_t h
 // timed on octave 0 of n synthetic u8 images of h x w (pseudo-random bytes, the
 // pyramid built once first); the fastest variant per radius is kept.  report:
 // per distinct radius (radius, ms of each variant, chosen).
-constexpr int kBlurVariantCount = 3;
+constexpr int kBlurVariantCount = 4;  // 0-2: outputs per thread; 3: TMA tiles
 psift_status autotune_blur(psift_ctx* ctx, uint32_t h, uint32_t w, uint32_t n, const psift_sift_config& cfg,
                            std::vector<double>& report) {
   if (h == 0 || w == 0 || n == 0) return PSIFT_OK;
@@ -689,7 +692,7 @@ psift_status autotune_blur(psift_ctx* ctx, uint32_t h, uint32_t w, uint32_t n, c
       for (int rep = 0; rep < 4 && ce == cudaSuccess; ++rep) {  // rep 0 warms up
         if (rep > 0) ce = cudaEventRecord(e0, ctx->stream);
         if (ce == cudaSuccess) ce = launch_blur(0, sc.level_taps[s].data(), r, job.d_plans, (int)n, 0, s, -1, mh, mw,
-                                                ctx->stream, v);
+                                                ctx->stream, v, false, nullptr, job.plans.data(), ctx->d_error);
         ctx->launches++;
         if (rep == 0 || ce != cudaSuccess) continue;
         ce = cudaEventRecord(e1, ctx->stream);

@@ -242,12 +242,12 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
       b += pad_rows(pairs[k].nt);
     }
   }
-  // B operands per pass: boxes of the pass's B tile rows (pass 1: 256, pass 2: 128)
+  // B operands per pass: boxes of the B tile rows
   CUtensorMap tmQA, tmTA, tmQAc, tmTAc, tmOnes, tmTB[2], tmTBx[2], tmQB[2], tmQBx[2];
   bool maps_ok = make_operand_map(&tmQA, qb, q_rows, kTcBM) && make_operand_map(&tmQAc, qbc, q_rows, kTcBM) &&
                  make_ext_map(&tmOnes, ones, kTcBM, kTcBM);
   for (int ps = 0; ps < 2 && maps_ok; ++ps) {
-    const int box = ps == 0 ? kTcBN1 : kTcBN;
+    const int box = kTcBN1;
     maps_ok = make_operand_map(&tmTB[ps], tb, t_rows, box) && make_ext_map(&tmTBx[ps], tx, t_rows, box);
     if (maps_ok && mutual)
       maps_ok = make_operand_map(&tmQB[ps], qb, q_rows, box) && make_ext_map(&tmQBx[ps], qx, q_rows, box);
@@ -279,8 +279,7 @@ psift_status match_batch(psift_ctx* ctx, const psift_match_job* jobs, int n, con
     cf += (long long)kTcSplits * nA;
     T.a_row0 = (int)a_row0;
     T.b_row0 = (int)b_row0;
-    T.bt[0] = (nB + kTcBN1 - 1) / kTcBN1;
-    T.bt[1] = (nB + kTcBN - 1) / kTcBN;
+    T.bt[0] = T.bt[1] = (nB + kTcBN1 - 1) / kTcBN1;
     T.at[0] = (nA + kTcBM - 1) / kTcBM;
   };
   // pass 1's tile order of one direction: problems in order, equal ranges over the CTAs

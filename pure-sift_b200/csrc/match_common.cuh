@@ -32,15 +32,13 @@ struct MatchPair {
   float* qn_max;       // scalar: max query squared norm
 };
 
-// Tensor-core matcher tiles: 128-row A tiles x 256-row (pass 1) or 128-row (pass
-// 2) B tiles.  A pass's tiles
+// Tensor-core matcher tiles: 128-row A tiles x 256-row B tiles.  A pass's tiles
 // are ordered (problem, A tile, B tile) and cut into equal ranges, one per CTA;
 // the pieces of one A tile (at most kTcSplits: ranges are at least
 // (B tiles - 1) / (kTcSplits - 1) long) write their partial results into their
 // own slots, merged by window_kernel (pass 1) and rerank_kernel (pass 2).
 constexpr int kTcBM = 128;
-constexpr int kTcBN1 = 256;  // pass 1 B tile rows (MMA N)
-constexpr int kTcBN = 128;   // pass 2 B tile rows
+constexpr int kTcBN1 = 256;  // B tile rows (MMA N) of both passes
 constexpr int kTcSplits = 4;
 constexpr int kTcColl = 32;  // window indices kept per (slot, row)
 

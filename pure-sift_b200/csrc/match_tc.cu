@@ -51,13 +51,12 @@ constexpr int kEpiParts = 4;                      // epilogue warps per TMEM lan
 constexpr int kEpiWarps = 4 * kEpiParts;          // warps 2 .. 2 + kEpiWarps - 1
 constexpr int kTcThreads = 32 * (2 + kEpiWarps);  // warp 0 TMA, warp 1 MMA, then the epilogue
 constexpr int kBM = kTcBM;
-// Per pass: B tile rows = MMA N = columns of one accumulator stage.  Pass 1 uses
-// N = 256 (two 128 x 256 accumulators): its fold is cheap, and an M = 128, N = 128
-// MMA keeps the tensor pipe about half busy.  Pass 2, with the heavier collection
-// fold, uses N = 128 (four accumulators).
+// B tile rows = MMA N = columns of one accumulator stage: N = 256 (two 128 x 256
+// accumulators in TMEM); an M = 128, N = 128 MMA keeps the tensor pipe only about
+// half busy.
 template <int MODE>
 struct TcShape {
-  static constexpr int BN = MODE == 0 ? kTcBN1 : kTcBN;
+  static constexpr int BN = kTcBN1;
   static constexpr int AccStages = 512 / BN;  // TMEM: 512 columns
   static constexpr int Cols = BN / kEpiParts;  // columns per epilogue warp and tile
   static constexpr uint32_t BStage = 2u * BN * 128u + BN * 32u;  // two halves, then the norm extension
@@ -65,7 +64,7 @@ struct TcShape {
   static constexpr uint32_t Idesc =
       (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 };
-static_assert(TcShape<0>::Cols == 64 && TcShape<1>::Cols == 32, "epilogue TMEM loads of 32 columns");
+static_assert(TcShape<0>::Cols == 64 && TcShape<1>::Cols == 64, "two 32-column TMEM loads per warp and tile");
 constexpr uint32_t kSpinLimit = 1u << 25;
 constexpr int kColl = 32;   // window indices kept per (split, row)
 constexpr int kXColl = 16;  // window indices a column part 1..3 hands to part 0 (more: exact scan)
@@ -176,19 +175,20 @@ __device__ __forceinline__ void tmem_wait32(uint32_t (&r)[32]) {
 
 // Smem map (offsets from a 1024-aligned base).
 constexpr uint32_t kAStage = 2u * kBM * 128u;                     // two 64-column halves of 128 rows
-constexpr uint32_t kSmA = 0;                                      // 2 A stages
-constexpr uint32_t kSmAx = 2 * kAStage;                           // A norm extension: 128 rows x 32 B
-constexpr uint32_t kSmB = kSmAx + kBM * 32u;                      // the B stages
-static_assert(kSmB % 1024 == 0 && TcShape<0>::BStage % 1024 == 0 && TcShape<1>::BStage % 1024 == 0 &&
-                  kAStage % 1024 == 0,
+constexpr uint32_t kSmA = 0;                                      // the A stages
+static_assert(TcShape<0>::BStage % 1024 == 0 && TcShape<1>::BStage % 1024 == 0 && kAStage % 1024 == 0,
               "128B-swizzle atoms");
-// Per pass: B tiles in flight, then barriers, then the epilogue exchange per row and column part
+// Per pass: A tiles (double-buffered in pass 1), B tiles in flight, then barriers, then the epilogue exchange per row and column part
 // 1..kEpiParts-1 (pass 1: the part's two largest values; pass 2: its count and up
 // to kXColl indices).
 template <int MODE>
 struct TcLayout {
-  static constexpr int kBStages = MODE == 0 ? 2 : 3;
+  static constexpr int kAStages = MODE == 0 ? 2 : 1;  // pass 2's larger exchange leaves room for one A tile
+  static constexpr int kBStages = 2;
   static constexpr int kXStride = MODE == 0 ? 2 : kXColl + 2;  // ints per (part, row)
+  static constexpr uint32_t kSmAx = kAStages * kAStage;     // A norm extension: 128 rows x 32 B
+  static constexpr uint32_t kSmB = kSmAx + kBM * 32u;       // the B stages
+  static_assert(kSmB % 1024 == 0, "128B-swizzle atoms");
   static constexpr uint32_t kSmBar = kSmB + kBStages * TcShape<MODE>::BStage;
   static constexpr uint32_t kSmX = kSmBar + 256;
   static constexpr uint32_t kSmTotal = kSmX + (kEpiParts - 1) * kBM * kXStride * 4 + 1024;  // + alignment slack
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       // the constant A norm extension once, then per piece its A tile and B tiles
       mbar_expect_tx(xfull, kBM * 32u);
-      tma_load_2d(&tmAx, xfull, smem + kSmAx, 0, 0);
+      tma_load_2d(&tmAx, xfull, smem + L::kSmAx, 0, 0);
       uint64_t* last_bar = xfull;  // the last load issued, for the drain on abort
       uint32_t last_par = 0;
       bool ok = true;
@@ -321,8 +321,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       int k = find_problem(P, n_problems, mode, g);
       for (int pi = 0; ok && g < g_end; ++pi) {
         const Piece pc = make_piece(P, mode, R, k, g, g_end);
-        const int as = pi & 1;
-        if (!mbar_wait(&aempty[as], (((uint32_t)pi >> 1) & 1u) ^ 1u, abort_flag)) {
+        const int as = pi % L::kAStages;
+        const uint32_t apar = ((uint32_t)(pi / L::kAStages)) & 1u;
+        if (!mbar_wait(&aempty[as], apar ^ 1u, abort_flag)) {
           ok = false;
           break;
         }
@@ -332,14 +333,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tma_load_2d(&tmA, &afull[as], ast, 0, a_row);
         tma_load_2d(&tmA, &afull[as], ast + kBM * 128, 64, a_row);
         last_bar = &afull[as];
-        last_par = ((uint32_t)pi >> 1) & 1u;
+        last_par = apar;
         for (int j = 0; j < pc.len; ++j) {
           if (!mbar_wait(&empty[bs], bph ^ 1u, abort_flag)) {
             ok = false;
             break;
           }
           const int b_row = P[k].b_row0 + (pc.b + j) * kBN;
-          uint8_t* bst = smem + kSmB + bs * kBStage;
+          uint8_t* bst = smem + L::kSmB + bs * kBStage;
           mbar_expect_tx(&full[bs], kBStage);
           tma_load_2d(&tmB, &full[bs], bst, 0, b_row);
           tma_load_2d(&tmB, &full[bs], bst + kBN * 128, 64, b_row);
@@ -372,11 +373,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       uint32_t bph = 0, sph = 0;
       long long g = g_begin;
       int k = find_problem(P, n_problems, mode, g);
-      const uint32_t ax = smem_u32(smem + kSmAx);
+      const uint32_t ax = smem_u32(smem + L::kSmAx);
       for (int pi = 0; ok && g < g_end; ++pi) {
         const Piece pc = make_piece(P, mode, R, k, g, g_end);
-        const int as = pi & 1;
-        if (!mbar_wait(&afull[as], ((uint32_t)pi >> 1) & 1u, abort_flag)) {
+        const int as = pi % L::kAStages;
+        if (!mbar_wait(&afull[as], ((uint32_t)(pi / L::kAStages)) & 1u, abort_flag)) {
           ok = false;
           break;
         }
@@ -387,7 +388,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             break;
           }
           tc_fence_after();
-          const uint32_t b_base = smem_u32(smem + kSmB + bs * kBStage);
+          const uint32_t b_base = smem_u32(smem + L::kSmB + bs * kBStage);
           const uint32_t d = tmem + (uint32_t)(s * kBN);
 #pragma unroll
           for (int kk = 0; kk < 8; ++kk) {
@@ -475,22 +476,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             cm[q] = max3f(cm[q], __uint_as_float(v[q + 16]), __uint_as_float(v[q + 24]));
           }
         } else {
-          // the tests branch-free into a mask, then the (rare) hits in column order
-          uint32_t hits = 0;
+          // the 8 column-class maxima (column mod 8) against the window bound; only
+          // a class that reaches it (rare) has its four values tested and collected
+          uint32_t cls = 0;
 #pragma unroll
-          for (int q = 0; q < 32; ++q) hits |= (__uint_as_float(v[q]) >= dthr ? 1u : 0u) << q;
-          if (!row_ok) hits = 0;
-          while (hits) {
-            const int q = __ffs(hits) - 1;
-            hits &= hits - 1;
-            if (cnt < ccap) coll[cnt] = cstart + q;
-            ++cnt;
+          for (int q = 0; q < 8; ++q) {
+            const float m = fmaxf(max3f(__uint_as_float(v[q]), __uint_as_float(v[q + 8]), __uint_as_float(v[q + 16])),
+                                  __uint_as_float(v[q + 24]));
+            cls |= (m >= dthr ? 1u : 0u) << q;
+          }
+          if (!row_ok) cls = 0;
+          if (cls) {
+            // the hit classes' values in column order (static indices: v stays in registers)
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+              if (((cls >> (c & 7)) & 1u) && __uint_as_float(v[c]) >= dthr) {
+                if (cnt < ccap) coll[cnt] = cstart + c;
+                ++cnt;
+              }
+            }
           }
         }
       };
-      // Each wait covers two 32-column TMEM loads (twice the bytes in flight per
-      // warp): pass 1 the warp's 64 columns of one tile, pass 2 its 32 columns of
-      // two consecutive tiles.  The accumulators are released as soon as their
+      // Each wait covers the warp's 64 columns of a tile as two 32-column TMEM
+      // loads in flight together; the accumulator is released as soon as its
       // values are in registers, then the values are folded.
       const uint32_t tq = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(part * Sh::Cols);
       const int col0 = pc.b * kBN + part * Sh::Cols;
@@ -514,47 +523,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           sph ^= 1u;
         }
       };
-      if constexpr (mode == 0) {
-        for (int j = 0; j < pc.len; ++j) {
-          const bool la = ready(s, sph);
-          if (la) {
-            tmem_ld32_nowait(tq + (uint32_t)(s * kBN), ra);
-            tmem_ld32_nowait(tq + (uint32_t)(s * kBN) + 32u, rb);
-            // every issued load completes before the registers are read (or the CTA leaves)
-            tmem_wait32(ra);
-            tmem_wait32(rb);
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acce[s]);
-            fold(ra, col0 + j * kBN);
-            fold(rb, col0 + j * kBN + 32);
-          }
-          advance(1);
-        }
-      } else {
-        for (int j = 0; j < pc.len; j += 2) {
-          const bool two = j + 1 < pc.len;
-          const int s1 = s + 1 == kAccStages ? 0 : s + 1;
-          const uint32_t ph1 = s + 1 == kAccStages ? sph ^ 1u : sph;
-          const bool la = ready(s, sph);
-          if (la) tmem_ld32_nowait(tq + (uint32_t)(s * kBN), ra);
-          const bool lb = two && ready(s1, ph1);
-          if (lb) tmem_ld32_nowait(tq + (uint32_t)(s1 * kBN), rb);
+      for (int j = 0; j < pc.len; ++j) {
+        const bool la = ready(s, sph);
+        if (la) {
+          tmem_ld32_nowait(tq + (uint32_t)(s * kBN), ra);
+          tmem_ld32_nowait(tq + (uint32_t)(s * kBN) + 32u, rb);
           // every issued load completes before the registers are read (or the CTA leaves)
-          if (la) tmem_wait32(ra);
-          if (lb) tmem_wait32(rb);
-          if (live) {
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) {
-              mbar_arrive(&acce[s]);
-              if (two) mbar_arrive(&acce[s1]);
-            }
-            fold(ra, col0 + j * kBN);
-            if (two) fold(rb, col0 + (j + 1) * kBN);
-          }
-          advance(two ? 2 : 1);
+          tmem_wait32(ra);
+          tmem_wait32(rb);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[s]);
+          fold(ra, col0 + j * kBN);
+          fold(rb, col0 + j * kBN + 32);
         }
+        advance(1);
       }
       // The row's largest D, and the second largest of the class maxima: a lower
       // bound on the row's second largest D (equal to it unless the two largest
@@ -796,14 +779,14 @@ __global__ void gather_rows_kernel(const GatherJob* __restrict__ jobs) {
 // One warp per kept A row (window_kernel's compacted list): exact reference
 // distances over the window candidates (every index with a <= thr, collected by
 // the second GEMM pass).  Candidates go
-// eight at a time: every lane loads its 16 bytes of each candidate's B row (all
-// eight loads in flight) and writes the squared differences to shared memory,
+// four at a time: every lane loads its 16 bytes of each candidate's B row (all
+// four loads in flight) and writes the squared differences to shared memory,
 // then lane c adds up candidate c's 128 terms in the reference's order.  A row
 // whose window overflowed kColl in some slot is left to rerank_scan_kernel.
-constexpr int kRrBatch = 8;
+constexpr int kRrBatch = 4;
 constexpr int kRrStride = 132;  // floats per staged candidate (conflict-free reads across candidates)
 
-__global__ void __launch_bounds__(256) rerank_kernel(const RerankJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(256, 4) rerank_kernel(const RerankJob* __restrict__ jobs) {
   __shared__ __align__(16) float terms[8][kRrBatch * kRrStride];
   const RerankJob& J = jobs[blockIdx.y];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -6,12 +6,17 @@
 namespace psift {
 
 // Host entry: mode 0 = level blur (octave, level >= 1); modes 1..4 = octave-0 base.
-// variant (level blur only) picks the outputs per thread (see blur_kernel.cuh);
-// every variant computes the same values.  fused: the single-rounding blur
+// variant (level blur only) picks the outputs per thread (0-2, see
+// blur_kernel.cuh) or the TMA-tile kernel (3, blur_tma.cuh; needs the host copy
+// of the plans for its tensor maps); every variant computes the same values.  fused: the single-rounding blur
 // (one fused multiply-add per tap; not the reference's rounding).
+cudaError_t launch_blur_tma(int radius, bool fused, const ImagePlan* d_plans, const ImagePlan* h_plans, int n,
+                            int octave, int level, int down_level, int zrev, const Taps2& taps, uint32_t* err,
+                            cudaStream_t st);
+
 cudaError_t launch_blur(int mode, const float* taps_host, int radius, const ImagePlan* plans, int n, int octave,
                         int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant, bool fused,
-                        const TileMap* tiles) {
+                        const TileMap* tiles, const ImagePlan* h_plans, uint32_t* err) {
   Taps2 t;
   if (tiles && tiles->n > 0) {
     t.tiles = *tiles;
@@ -25,6 +30,9 @@ cudaError_t launch_blur(int mode, const float* taps_host, int radius, const Imag
   }
   t.one = make_float2(1.0f, 1.0f);
   const int zrev = (octave * 8 + level) & 1;
+  // variant 3: TMA tiles, persistent CTAs (blur_tma.cuh), either rounding
+  if (mode == MODE_LEVEL && variant == 3)
+    return launch_blur_tma(radius, fused, plans, h_plans, n, octave, level, down_level, zrev, t, err, st);
   if (fused) return launch_blur_fused(mode, radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
   switch (mode) {
     case MODE_LEVEL:

@@ -352,6 +352,8 @@ class Context:
         self.check(self.lib.psift_ctx_enable_stage_timing(self.handle, int(on)))
 
     TUNE_BLUR, TUNE_MATCH_FP32, TUNE_MATCH_TC = 0, 1, 2
+    # level-blur variants: 0-2 outputs per thread (4x8, 8x8, 4x4), 3 TMA tiles (persistent CTAs)
+    BLUR_VARIANTS = 4
 
     def autotune(self, height: int, width: int, n_images: int, config: "SiftConfig" = None, n_desc: int = 4096,
                  n_pairs: int = 8) -> dict:
@@ -368,9 +370,10 @@ class Context:
         r = rep[:cnt.value].tolist()
         out = {"blur": {}}
         i = 0
+        nv = self.BLUR_VARIANTS
         while i < len(r) and r[i] != -1.0:
-            out["blur"][int(r[i])] = {"ms": r[i + 1:i + 4], "variant": int(r[i + 4])}
-            i += 5
+            out["blur"][int(r[i])] = {"ms": r[i + 1:i + 1 + nv], "variant": int(r[i + 1 + nv])}
+            i += 2 + nv
         i += 1
         while i + 6 <= len(r):
             key = "match_tc" if r[i] == 1.0 else "match_fp32"
