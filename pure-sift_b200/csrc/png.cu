@@ -518,9 +518,11 @@ cudaError_t launch_unfilter(const PngPlane* planes, int n, uint32_t max_rb, cuda
 // on st: inflate on host threads, the filtered streams to the device, the row
 // filters undone per filter unit, then expansion and luma.
 psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, const PngLayout& L, uint32_t b,
-                              uint32_t e, uint8_t* const* luma, cudaStream_t st) {
-  psift_status rs = inflate_range(ctx, P, L, b, e);
-  if (rs != PSIFT_OK) return rs;
+                              uint32_t e, uint8_t* const* luma, cudaStream_t st, bool inflated = false) {
+  if (!inflated) {
+    psift_status rs = inflate_range(ctx, P, L, b, e);
+    if (rs != PSIFT_OK) return rs;
+  }
   PngState* S = png_state(ctx);
   const uint32_t n = e - b;
   // descriptors of the chunk: its slots of the per-image regions (planes of
@@ -675,13 +677,19 @@ psift_status psift_detect_and_compute_png_batch(psift_ctx* ctx, const uint8_t* c
   PngLayout L;
   psift_status rs = png_reserve(ctx, P, L);
   if (rs != PSIFT_OK) return rs;
-  // per chunk, just before its stages: chunk 1's inflate (host threads) overlaps
-  // chunk 0's kernels
+  // The whole batch is inflated before chunk 0's stages, on as many host threads
+  // as there are images (up to 16): with fewer images than threads, inflating per
+  // chunk would leave threads idle for longer than the overlap with chunk 0's
+  // kernels gains.  Each chunk's device part runs on its own stream.
   const DeviceFill fill = [&](char* extra, const std::vector<size_t>& dev_off, uint32_t b, uint32_t e,
                               cudaStream_t st) -> psift_status {
+    if (b == 0) {
+      psift_status rs = inflate_range(ctx, P, L, 0, n);
+      if (rs != PSIFT_OK) return rs;
+    }
     std::vector<uint8_t*> luma(e - b);
     for (uint32_t i = b; i < e; ++i) luma[i - b] = (uint8_t*)extra + dev_off[i];
-    return decode_png_range(ctx, P, L, b, e, luma.data(), st);
+    return decode_png_range(ctx, P, L, b, e, luma.data(), st, true);
   };
   return detect_batch_host_out(ctx, imgs.data(), n, cfg, outs, &fill);
 }
