@@ -729,17 +729,21 @@ def ransac_bench(ctx, torch, n_pairs: int = 1024, n_train: int = 64, reps: int =
     }
 
 
-def pyramid_bench(ctx, torch, blur: str = "reference", reps: int = 5):
+def pyramid_bench(ctx, torch, blur: str = "reference", reps: int = 5, variant: int | None = None):
     """One 1080p image through psift.build_pyramid (the gaussian_blur chain, DoG and
     decimation of build_scale_space_pyramid_with_options, 4 octaves with the 2x
     upsampled base): device time of the call's launches with CUDA events on the
     context's stream, host wall clock with the planes' download; the rounding mode
     of the blur taps as given.  Also the profiling case of the level blur (the
-    first launch per octave of each radius, e.g. the R = 10 level of octave 0)."""
+    first launch per octave of each radius, e.g. the R = 10 level of octave 0).  With
+    `variant`, every radius runs that level-blur variant (3 = TMA tiles)."""
     import psift
     img = synth.blob_image(WIDTH, HEIGHT, 2000, 1.5, 20.0, seed=7).astype(np.float32) / 255.0
     cfg = psift.SiftConfig().with_octaves(4).with_contrast_threshold(0.015)
     ctx.set_blur_rounding(ctx.BLUR_FUSED if blur == "fused" else ctx.BLUR_REFERENCE)
+    if variant is not None:
+        for r in range(1, 16):
+            ctx.set_tuning(ctx.TUNE_BLUR, r, variant)
     try:
         for _ in range(2):
             psift.build_pyramid(img, cfg, ctx=ctx)
@@ -756,7 +760,8 @@ def pyramid_bench(ctx, torch, blur: str = "reference", reps: int = 5):
         ctx.set_blur_rounding(ctx.BLUR_REFERENCE)
     del stream
     return {"workload": f"{WIDTH}x{HEIGHT} blob image, 4 octaves, scales 3, upsampled base (3840x2160 octave 0)",
-            "blur": blur, "device_pyramid_ms": st["pyramid"][0] / reps, "host_api_ms_with_download": wall * 1e3}
+            "blur": blur, "blur_variant": "autotuner default" if variant is None else variant,
+            "device_pyramid_ms": st["pyramid"][0] / reps, "host_api_ms_with_download": wall * 1e3}
 
 
 def png_bench(ctx, torch, n: int = 8, reps: int = 10):
@@ -1218,6 +1223,8 @@ def main():
     ap.add_argument("--ransac-pairs", type=int, default=1024, help="learned-RANSAC section: match sets")
     ap.add_argument("--blur", choices=["reference", "fused"], default="reference",
                     help="blur rounding of the main loop (profiling case; the default is the reference's)")
+    ap.add_argument("--blur-variant", type=int, choices=[0, 1, 2, 3], default=None,
+                    help="pyramid section: run this level-blur variant at every radius (profiling case)")
     ap.add_argument("--catalog-codes", type=int, default=2_000_000, help="catalog section: catalog codes")
     ap.add_argument("--catalog-entries", type=int, default=10_000, help="catalog-search section: entries")
     ap.add_argument("--no-catalog", action="store_true")
@@ -1254,7 +1261,8 @@ def main():
                "uneven_batch": lambda: uneven_bench(ctx, torch), "jpeg": lambda: jpeg_bench(ctx, torch),
                "png": lambda: png_bench(ctx, torch),
                "panorama": lambda: panorama_bench(ctx, torch),
-               "pyramid": lambda: pyramid_bench(ctx, torch, blur=args.blur, reps=min(args.steps, 10))}
+               "pyramid": lambda: pyramid_bench(ctx, torch, blur=args.blur, reps=min(args.steps, 10),
+                                                 variant=args.blur_variant)}
         print(json.dumps({args.only_section: fns[args.only_section]()}), flush=True)
         ctx.close()
         return 0

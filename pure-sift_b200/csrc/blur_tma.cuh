@@ -1,23 +1,25 @@
 // Level blur with 2-D TMA tiles: the input tile of G[s-1] (tile + halo) arrives
 // in shared memory by one cp.async.bulk.tensor.2d (no multicast) on an mbarrier,
-// issued for the CTA's next tile while the current one's vertical pass runs.
+// into a double-buffered stage: the CTA's next tile is copied during the whole of
+// the current tile's horizontal and vertical passes.
 //
 // Reference: gaussian_blur (src/pipeline.rs:314-425), build_scale_space_pyramid
 // (:550-638); the same values as blur_level_kernel<R, HC, RV, MODE_LEVEL, FUSED>
 // (same taps, order and roundings), so both kernels' planes are identical.
 //
-// Structure: persistent CTAs (resident ones only) walk the launch's tile list
+// Structure: persistent CTAs (the resident ones) walk the launch's tile list
 // (every existing 64x64 tile of every image; reversed on odd levels), 256
-// threads each.  Interior tiles (tile + halo inside the plane) load by TMA into
-// a row-major stage; border tiles, whose halo clamps to the plane like
-// `(x + k).saturating_sub(r).min(w - 1)`, are staged by the threads.  The
-// horizontal pass takes two rows at a time: a thread's four outputs of rows 2p
-// and 2p + 1 as packed f32x2 pairs, each pair's operand {x[2p][c], x[2p+1][c]}
-// built from the two rows' 128-bit loads.  Once the horizontal pass has read
-// the stage, thread 0 issues the next tile's TMA into it and the vertical pass
-// runs from the intermediate; D = G[s] - G[s-1] takes G[s-1] from memory (the
-// tile just loaded, still in L2).  The wait on the copy is bounded: on timeout
-// the CTA records kErrTimeout and leaves.
+// threads each.  Every tile's box (IN_W x IN_H from (tx0 - RP, ty0 - R)) is one
+// TMA copy; where the box leaves the plane the copy fills zeros, and the threads
+// then replace each such element by the in-plane element that the reference's
+// clamp `(x + k).saturating_sub(r).min(w - 1)` selects (it lies inside the box,
+// and only out-of-plane elements are written, so the fix-up has no read/write
+// overlap).  The horizontal pass takes two rows at a time: a thread's four
+// outputs of rows 2p and 2p + 1 as packed f32x2 pairs, each pair's operand
+// {x[2p][c], x[2p+1][c]} built from the two rows' 128-bit loads.  The vertical
+// pass runs from the intermediate and forms D = G[s] - G[s-1] with G[s-1] from
+// the stage.  Waits on the copies are bounded: on timeout the CTA records
+// kErrTimeout, waits (bounded) for its copies in flight and leaves.
 #pragma once
 #include <cuda.h>
 
@@ -43,9 +45,12 @@ struct TmaGeom {
   static constexpr int NQ = (OFF + 2 * R + 4 + 3) / 4;  // float4 loads per row for four outputs
   static constexpr uint32_t STAGE_BYTES = (uint32_t)IN_W * IN_H * 4;
   static constexpr uint32_t SMEM_STAGE = (STAGE_BYTES + 127) / 128 * 128;
-  static constexpr uint32_t SMEM_BYTES = SMEM_STAGE + IN_H * kTmpStride * 4 + 128;
+  static constexpr uint32_t SMEM_BYTES = 2 * SMEM_STAGE + IN_H * kTmpStride * 4 + 128;
+  // CTAs per SM that the shared memory allows (228 KB per SM, 1 KB reserved per CTA)
+  static constexpr int MIN_CTAS = 3 * (SMEM_BYTES + 1024) <= 228 * 1024 ? 3 : 2;
   static_assert(IN_W <= 256 && IN_H <= 256, "TMA box");
   static_assert((IN_W * 4) % 16 == 0, "TMA box rows are whole 16-byte units");
+  static_assert(IN_W % 2 == 0 && RP % 2 == 0, "float2 reads of G[s-1] from the stage");
 };
 
 __device__ __forceinline__ bool tma_mbar_wait(uint64_t* bar, uint32_t parity) {
@@ -65,15 +70,14 @@ __device__ __forceinline__ bool tma_mbar_wait(uint64_t* bar, uint32_t parity) {
 }
 
 template <int R, bool FUSED>
-__global__ void __launch_bounds__(kBlurThreads, 3)
+__global__ void __launch_bounds__(kBlurThreads, TmaGeom<R>::MIN_CTAS)
     blur_tma_kernel(const ImagePlan* __restrict__ plans, int octave, int level, int down_level, int zrev,
                     const __grid_constant__ Taps2 taps, const __grid_constant__ TmaPlanes maps, uint32_t* err) {
   using G = TmaGeom<R>;
   constexpr int RV = 8;
   extern __shared__ __align__(128) uint8_t tsm[];
-  float* s_in = reinterpret_cast<float*>(tsm);                               // [IN_H][IN_W]
-  float* s_tmp = reinterpret_cast<float*>(tsm + G::SMEM_STAGE);              // [IN_H][kTmpStride]
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + G::SMEM_BYTES - 128);
+  float* s_tmp = reinterpret_cast<float*>(tsm + 2 * G::SMEM_STAGE);  // [IN_H][kTmpStride]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tsm + G::SMEM_BYTES - 128);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float2 wv[R + 1];
 #pragma unroll
@@ -82,64 +86,72 @@ __global__ void __launch_bounds__(kBlurThreads, 3)
   const TileMap& tm = taps.tiles;
   const int total = tm.prefix[tm.n];
 
-  // tile lin -> image, tile origin, interior?
-  auto tile_info = [&](int lin, int& z, int& tx0, int& ty0, bool& interior) {
+  // tile lin -> image and tile origin
+  auto tile_info = [&](int lin, int& z, int& tx0, int& ty0) {
     int bx, by;
     tile_of(tm, lin, zrev, z, bx, by);
-    const OctaveDev& O = plans[z].oct[octave];
     tx0 = bx * kTileW;
     ty0 = by * kTileH;
-    interior = tx0 - G::RP >= 0 && tx0 + kTileW + G::RP <= O.w && ty0 - R >= 0 && ty0 + kTileH + R <= O.h;
   };
-  auto issue = [&](int z, int tx0, int ty0) {  // thread 0
+  auto issue = [&](int b, int z, int tx0, int ty0) {  // thread 0
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(bars + b);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                     (uint32_t)__cvta_generic_to_shared(bar)),
-                 "r"(G::STAGE_BYTES)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(G::STAGE_BYTES)
                  : "memory");
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
-            "r"((uint32_t)__cvta_generic_to_shared(s_in)),
-        "l"(reinterpret_cast<uint64_t>(&maps.m[z])), "r"((uint32_t)__cvta_generic_to_shared(bar)), "r"(tx0 - G::RP),
-        "r"(ty0 - R)
+            "r"((uint32_t)__cvta_generic_to_shared(tsm + b * G::SMEM_STAGE)),
+        "l"(reinterpret_cast<uint64_t>(&maps.m[z])), "r"(bar), "r"(tx0 - G::RP), "r"(ty0 - R)
         : "memory");
   };
 
   if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(bar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(bars)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(bars + 1))
+                 : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  int lin = blockIdx.x;
-  if (lin >= total) return;
-  uint32_t phase = 0;
-  {
+  if ((int)blockIdx.x >= total) return;
+  if (threadIdx.x == 0) {
     int z, tx0, ty0;
-    bool in;
-    tile_info(lin, z, tx0, ty0, in);
-    if (in && threadIdx.x == 0) issue(z, tx0, ty0);
+    tile_info(blockIdx.x, z, tx0, ty0);
+    issue(0, z, tx0, ty0);
   }
-  while (lin < total) {
+  int it = 0;
+  for (int lin = blockIdx.x; lin < total; lin += (int)gridDim.x, ++it) {
+    const int b = it & 1;
+    // stage b ^ 1 was last read by the previous tile, finished at the loop's end barrier
+    const int next = lin + (int)gridDim.x;
+    if (next < total && threadIdx.x == 0) {
+      int nz, nx0, ny0;
+      tile_info(next, nz, nx0, ny0);
+      issue(b ^ 1, nz, nx0, ny0);
+    }
     int z, tx0, ty0;
-    bool interior;
-    tile_info(lin, z, tx0, ty0, interior);
+    tile_info(lin, z, tx0, ty0);
     const ImagePlan& P = plans[z];
     const OctaveDev& O = P.oct[octave];
     const int h = O.h, w = O.w;
-    const float* src_plane = O.g + (long long)(level - 1) * O.plane_stride;
-    if (interior) {
-      const bool ok = tma_mbar_wait(bar, phase);
-      phase ^= 1u;
-      if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
-        return;
+    const bool ok = tma_mbar_wait(bars + b, (uint32_t)(it >> 1) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicOr(err, kErrTimeout);
+        // the copies in flight land in this CTA's shared memory: wait (bounded) for them
+        tma_mbar_wait(bars + b, (uint32_t)(it >> 1) & 1u);
+        if (next < total) tma_mbar_wait(bars + (b ^ 1), (uint32_t)((it + 1) >> 1) & 1u);
       }
-    } else {
-      // border tile: clamped staging by the threads (row-major, like the TMA box)
+      return;
+    }
+    float* s_in = reinterpret_cast<float*>(tsm + b * G::SMEM_STAGE);  // [IN_H][IN_W]
+    const int x_lo = tx0 - G::RP, y_lo = ty0 - R;
+    if (x_lo < 0 || y_lo < 0 || x_lo + G::IN_W > w || y_lo + G::IN_H > h) {
+      // border tile: the zero-filled out-of-plane elements take their clamped values
       for (int i = threadIdx.x; i < G::IN_H * G::IN_W; i += kBlurThreads) {
         const int r = i / G::IN_W, c = i - r * G::IN_W;
-        const int gy = clampi(ty0 - R + r, 0, h - 1), gx = clampi(tx0 - G::RP + c, 0, w - 1);
-        s_in[i] = src_plane[(long long)gy * O.pitch + gx];
+        const int gy = y_lo + r, gx = x_lo + c;
+        const int cy = clampi(gy, 0, h - 1), cx = clampi(gx, 0, w - 1);
+        if (cy != gy || cx != gx) s_in[i] = s_in[(cy - y_lo) * G::IN_W + (cx - x_lo)];
       }
       __syncthreads();
     }
@@ -156,9 +168,9 @@ __global__ void __launch_bounds__(kBlurThreads, 3)
         for (int j = 0; j < 4; ++j) acc[j] = make_float2(0.0f, 0.0f);
 #pragma unroll
         for (int q = 0; q < G::NQ; ++q) {
-          const float4 a = r0[q], b = r1[q];
-          const float2 p[4] = {make_float2(a.x, b.x), make_float2(a.y, b.y), make_float2(a.z, b.z),
-                               make_float2(a.w, b.w)};
+          const float4 a = r0[q], c = r1[q];
+          const float2 p[4] = {make_float2(a.x, c.x), make_float2(a.y, c.y), make_float2(a.z, c.z),
+                               make_float2(a.w, c.w)};
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int m = 4 * q + e;  // window column
@@ -175,19 +187,10 @@ __global__ void __launch_bounds__(kBlurThreads, 3)
       }
     }
     __syncthreads();
-    // the stage is free: the next tile's TMA runs under the vertical pass
-    const int next = lin + (int)gridDim.x;
-    if (next < total) {
-      int nz, nx0, ny0;
-      bool nin;
-      tile_info(next, nz, nx0, ny0, nin);
-      if (nin && threadIdx.x == 0) issue(nz, nx0, ny0);
-    }
 
     // Vertical pass: a column pair x RV rows per thread (as blur_level_kernel).
     {
-      const long long gbase = (long long)level * O.plane_stride;
-      float* gout = O.g + gbase;
+      float* gout = O.g + (long long)level * O.plane_stride;
       float* dout = O.d + (long long)(level - 1) * O.plane_stride;
       const bool do_down = level == down_level && octave + 1 < P.n_oct;
       const int x = 2 * lane;
@@ -208,20 +211,21 @@ __global__ void __launch_bounds__(kBlurThreads, 3)
         }
         if (gx >= w) continue;
         const bool pair_ok = gx + 1 < w;
+        // G[s-1] at (ty0 + yb + j, gx): stage row yb + j + R, column x + RP
+        const float* prev = s_in + (yb + R) * G::IN_W + x + G::RP;
 #pragma unroll
         for (int j = 0; j < RV; ++j) {
           const int gy = ty0 + yb + j;
           if (gy >= h) break;
+          const float2 pv = *reinterpret_cast<const float2*>(prev + j * G::IN_W);
           float* grow = gout + (long long)gy * O.pitch + gx;
-          const float* prow = src_plane + (long long)gy * O.pitch + gx;
           float* drow = dout + (long long)gy * O.pitch + gx;
           if (pair_ok) {
-            const float2 pv = __ldg(reinterpret_cast<const float2*>(prow));
             *reinterpret_cast<float2*>(grow) = acc[j];
             __stcs(reinterpret_cast<float2*>(drow), make_float2(__fsub_rn(acc[j].x, pv.x), __fsub_rn(acc[j].y, pv.y)));
           } else {
             grow[0] = acc[j].x;
-            __stcs(drow, __fsub_rn(acc[j].x, __ldg(prow)));
+            __stcs(drow, __fsub_rn(acc[j].x, pv.x));
           }
           if (do_down && !(gy & 1)) {
             const OctaveDev& N = P.oct[octave + 1];
@@ -231,8 +235,7 @@ __global__ void __launch_bounds__(kBlurThreads, 3)
         }
       }
     }
-    __syncthreads();  // the intermediate is free for the next tile
-    lin = next;
+    __syncthreads();  // the intermediate and stage b are free for the next tiles
   }
 }
 

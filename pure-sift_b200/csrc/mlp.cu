@@ -194,13 +194,23 @@ __global__ void mlp_adam_kernel(float* __restrict__ params, const float* __restr
   params[p] -= lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
 }
 
-// Sequential sum of the per-sample losses (deterministic) into loss[step].
-__global__ void mlp_loss_kernel(const float* __restrict__ l, int B, float* __restrict__ out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    float s = 0.0f;
-    for (int b = 0; b < B; ++b) s += l[b];
-    *out = s / (float)B;
+// Mean of the per-sample losses into loss[step], in a fixed order (deterministic):
+// thread t sums samples t, t + 256, t + 512, ... in that order (coalesced loads
+// across a warp), then a fixed pairwise tree over the 256 partial sums.  One CTA.
+constexpr int kLossThreads = 256;
+__global__ void __launch_bounds__(kLossThreads) mlp_loss_kernel(const float* __restrict__ l, int B,
+                                                                float* __restrict__ out) {
+  __shared__ float part[kLossThreads];
+  const int t = threadIdx.x;
+  float s = 0.0f;
+  for (int b = t; b < B; b += kLossThreads) s += l[b];
+  part[t] = s;
+  __syncthreads();
+  for (int h = kLossThreads / 2; h > 0; h >>= 1) {
+    if (t < h) part[t] += part[t + h];
+    __syncthreads();
   }
+  if (t == 0) *out = part[0] / (float)B;
 }
 
 // ------------------------------------------------------------ tensor-core inference
@@ -425,7 +435,7 @@ cudaError_t launch_mlp_step(float* params, const float* X, const float* Y, const
   mlp_fwd_bwd_kernel<<<(B + 127) / 128, 128, 0, st>>>(params, X, Y, idx, B, xb, h1b, h2b, dz1, dz2, dz3, lb);
   mlp_grad_partial_kernel<<<dim3((kNP + 127) / 128, chunks), 128, 0, st>>>(B, xb, h1b, h2b, dz1, dz2, dz3, partial);
   mlp_grad_reduce_kernel<<<(kNP + 127) / 128, 128, 0, st>>>(chunks, partial, grad);
-  if (loss_out) mlp_loss_kernel<<<1, 32, 0, st>>>(lb, B, loss_out);
+  if (loss_out) mlp_loss_kernel<<<1, kLossThreads, 0, st>>>(lb, B, loss_out);
   if (update) {
     const float b1 = 0.9f, b2 = 0.999f;
     const float bc1 = 1.0f - powf(b1, (float)t), bc2 = 1.0f - powf(b2, (float)t);
