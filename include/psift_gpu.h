@@ -125,7 +125,8 @@ psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
  * psift_ctx_autotune times every candidate on synthetic inputs of the caller's
  * geometry (n_images u8 images of height x width with cfg's blur schedule;
  * n_pairs matching problems of n_desc x n_desc descriptors, both matcher paths)
- * and keeps the fastest in the context.  report (optional, report_capacity
+ * and keeps the fastest in the context (for the blur, another variant replaces
+ * variant 0 only when it is at least 3 % faster).  report (optional, report_capacity
  * doubles; report_count = the doubles written): per blur radius (radius, ms of
  * variants 0..3, chosen), then -1, then per matcher path (path 0 FP32 / 1 tensor
  * core, ms for 1, 2, 4, 8 work items per SM, chosen). */

@@ -95,41 +95,78 @@ cudaError_t copy_range(FeatureArrays& d, uint64_t dst_off, const FeatureArrays& 
   return e;
 }
 
-// PSIFTCAT records -> feature arrays: one warp per record.  The records of
-// entry e start at byte file_off[e] of the uploaded file (any alignment) and
-// fill features [out_off[e], out_off[e + 1]).  Descriptor bytes go to q8 for
-// dequantize_descriptor_u8; the stored signature is kept as it is.
+// PSIFTCAT records -> feature arrays.  The records of entry e start at byte
+// file_off[e] of the uploaded file (any alignment) and fill features
+// [out_off[e], out_off[e + 1]); out_off has n_entries + 1 items, the last being
+// the total.  A warp takes kSplitPerWarp consecutive records, finds the first
+// one's entry by binary search and walks the entries forward.  Per record,
+// lane l loads 32-bit words l and 32 + l of the record's span (whole words
+// around its 164 bytes; the uploaded region is padded to 256 bytes, and the
+// word after the record is read only when the record is not word-aligned), and
+// funnel shifts give the record's own words 0..40: x, y, scale, response,
+// orientation, the stored 128-bit signature (kept as it is), then the 128
+// descriptor bytes, which go to q8 for dequantize_descriptor_u8.
 constexpr int kSplitWarps = 8;
+constexpr int kSplitPerWarp = 32;
+constexpr int kSplitBatch = 4;
 __global__ void __launch_bounds__(kSplitWarps * 32)
     psiftcat_split_kernel(const uint8_t* __restrict__ file, const long long* __restrict__ file_off,
                           const long long* __restrict__ out_off, int n_entries, long long total, float2* xy,
                           float* scale, float* resp, float* ori, uint64_t* codes, uint8_t* q8) {
-  __shared__ __align__(16) uint8_t rec[kSplitWarps][kRecordBytes + 12];
+  constexpr unsigned kFull = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long i = (long long)blockIdx.x * kSplitWarps + warp;
-  if (i >= total) return;
-  int lo = 0, hi = n_entries - 1;  // last entry with out_off[e] <= i
+  const long long i0 = ((long long)blockIdx.x * kSplitWarps + warp) * kSplitPerWarp;
+  if (i0 >= total) return;
+  const long long i1 = i0 + kSplitPerWarp < total ? i0 + kSplitPerWarp : total;
+  int lo = 0, hi = n_entries - 1;  // last entry with out_off[e] <= i0
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (out_off[mid] <= i) lo = mid;
+    if (out_off[mid] <= i0) lo = mid;
     else hi = mid - 1;
   }
-  const uint8_t* src = file + file_off[lo] + (i - out_off[lo]) * kRecordBytes;
-  uint8_t* r = rec[warp];
-  for (int b = lane; b < kRecordBytes; b += 32) r[b] = src[b];
-  __syncwarp();
-  auto u32_at = [&](int b) {
-    return (uint32_t)r[b] | ((uint32_t)r[b + 1] << 8) | ((uint32_t)r[b + 2] << 16) | ((uint32_t)r[b + 3] << 24);
-  };
-  if (lane == 0) xy[i] = make_float2(__uint_as_float(u32_at(0)), __uint_as_float(u32_at(4)));
-  if (lane == 1) scale[i] = __uint_as_float(u32_at(8));
-  if (lane == 2) resp[i] = __uint_as_float(u32_at(12));
-  if (lane == 3) ori[i] = __uint_as_float(u32_at(16));
-  if (lane == 4 || lane == 5) {
-    const int b = 20 + 8 * (lane - 4);
-    codes[2 * i + (lane - 4)] = (uint64_t)u32_at(b) | ((uint64_t)u32_at(b + 4) << 32);
+  int e = lo;
+  long long e_begin = out_off[e], e_end = out_off[e + 1], e_file = file_off[e];
+  // kSplitBatch records at a time: every record's loads are issued before the first is used
+  for (long long ib = i0; ib < i1; ib += kSplitBatch) {
+    uint32_t a[kSplitBatch], b[kSplitBatch], sh[kSplitBatch];
+#pragma unroll
+    for (int j = 0; j < kSplitBatch; ++j) {
+      const long long i = ib + j;
+      a[j] = b[j] = sh[j] = 0u;
+      if (i >= i1) continue;
+      while (e_end <= i) {  // entries without records are passed over
+        ++e;
+        e_begin = e_end;
+        e_end = out_off[e + 1];
+        e_file = file_off[e];
+      }
+      const unsigned long long s = (unsigned long long)(e_file + (i - e_begin) * kRecordBytes);
+      const uint32_t* wbase = reinterpret_cast<const uint32_t*>(file + (s & ~3ull));
+      sh[j] = (uint32_t)(s & 3u) * 8u;
+      a[j] = __ldg(wbase + lane);  // span words 0..31
+      if (lane < 9 || (lane == 9 && sh[j] != 0u)) b[j] = __ldg(wbase + 32 + lane);  // 32..41
+    }
+#pragma unroll
+    for (int j = 0; j < kSplitBatch; ++j) {
+      const long long i = ib + j;
+      if (i >= i1) break;
+      const uint32_t a_next = __shfl_down_sync(kFull, a[j], 1);
+      const uint32_t b_first = __shfl_sync(kFull, b[j], 0);
+      const uint32_t b_next = __shfl_down_sync(kFull, b[j], 1);
+      const uint32_t o0 = __funnelshift_r(a[j], lane == 31 ? b_first : a_next, sh[j]);  // record word lane
+      const uint32_t o1 = __funnelshift_r(b[j], b_next, sh[j]);  // record word 32 + lane (lanes 0..8)
+      // descriptor word l = record word 9 + l
+      const uint32_t qa = __shfl_sync(kFull, o0, lane + 9 < 32 ? lane + 9 : 31);
+      const uint32_t qb = __shfl_sync(kFull, o1, lane >= 23 ? lane - 23 : 0);
+      reinterpret_cast<uint32_t*>(q8 + i * 128)[lane] = lane <= 22 ? qa : qb;
+      const uint32_t nx = __shfl_down_sync(kFull, o0, 1);
+      if (lane == 0) xy[i] = make_float2(__uint_as_float(o0), __uint_as_float(nx));
+      if (lane == 2) scale[i] = __uint_as_float(o0);
+      if (lane == 3) resp[i] = __uint_as_float(o0);
+      if (lane == 4) ori[i] = __uint_as_float(o0);
+      if (lane == 5 || lane == 7) codes[2 * i + (lane - 5) / 2] = (uint64_t)o0 | ((uint64_t)nx << 32);
+    }
   }
-  reinterpret_cast<uint32_t*>(q8 + i * 128)[lane] = u32_at(36 + 4 * lane);
 }
 
 // Rust's str::from_utf8 acceptance rule (shortest forms, no surrogates, <= U+10FFFF).
@@ -662,7 +699,8 @@ psift_status psift_catalog_load_binary(psift_ctx* ctx, const char* path, psift_c
       if (ce == cudaSuccess)
         ce = cudaMemcpyAsync(d_ooff, out_off.data(), 8 * out_off.size(), cudaMemcpyHostToDevice, ctx->stream);
       if (ce == cudaSuccess) {
-        const long long blocks = ((long long)total + kSplitWarps - 1) / kSplitWarps;
+        const long long per_block = (long long)kSplitWarps * kSplitPerWarp;
+        const long long blocks = ((long long)total + per_block - 1) / per_block;
         psiftcat_split_kernel<<<(unsigned)blocks, kSplitWarps * 32, 0, ctx->stream>>>(
             d_file, d_foff, d_ooff, (int)file_off.size(), (long long)total, cat->a.xy, cat->a.scale, cat->a.resp,
             cat->a.ori, cat->a.codes, d_q8);

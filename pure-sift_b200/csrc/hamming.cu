@@ -67,8 +67,8 @@ __global__ void __launch_bounds__(256) quantize_codes_kernel(const float* __rest
     uint32_t word[4];
 #pragma unroll
     for (int w = 0; w < 4; ++w) word[w] = __ballot_sync(0xffffffffu, v[d][w] > 0.065f);
-    if (lane < 2 && row0 + d < n)
-      codes[2 * (size_t)(row0 + d) + lane] = (uint64_t)word[2 * lane] | ((uint64_t)word[2 * lane + 1] << 32);
+    const uint32_t lo = lane ? word[2] : word[0], hi = lane ? word[3] : word[1];  // no indexed local array
+    if (lane < 2 && row0 + d < n) codes[2 * (size_t)(row0 + d) + lane] = (uint64_t)lo | ((uint64_t)hi << 32);
   }
 }
 
@@ -292,37 +292,116 @@ __global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4*
   }
 }
 
-// Per query (one warp): bitonic sort of the chunks' n_chunks*k keys in shared
-// memory, keep the k smallest.
-__global__ void topk_merge_kernel(const unsigned long long* __restrict__ part, int nq, int k, int n_chunks, int n2,
-                                  uint32_t* __restrict__ out_idx, uint32_t* __restrict__ out_dist) {
-  extern __shared__ unsigned long long s_keys[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
-  unsigned long long* keys = s_keys + (size_t)warp * n2;
-  if (qi >= nq) return;
-  const int total = n_chunks * k;
-  const unsigned long long* src = part + (long long)qi * total;
-  for (int t = lane; t < n2; t += 32) keys[t] = t < total ? src[t] : ~0ull;
-  __syncwarp();
-  for (int kk = 2; kk <= n2; kk <<= 1) {
+// Ascending bitonic sort of a[0..m) (m a power of two) by one warp.
+__device__ __forceinline__ void warp_bitonic_u64(unsigned long long* a, int m, int lane) {
+  for (int kk = 2; kk <= m; kk <<= 1) {
     for (int j = kk >> 1; j > 0; j >>= 1) {
-      for (int i = lane; i < n2; i += 32) {
+      for (int i = lane; i < m; i += 32) {
         const int ixj = i ^ j;
         if (ixj > i) {
-          const unsigned long long a = keys[i], b = keys[ixj];
+          const unsigned long long x = a[i], y = a[ixj];
           const bool up = (i & kk) == 0;
-          if ((a > b) == up) {
-            keys[i] = b;
-            keys[ixj] = a;
+          if ((x > y) == up) {
+            a[i] = y;
+            a[ixj] = x;
           }
         }
       }
       __syncwarp();
     }
   }
+}
+
+// Per query (one warp): the k smallest of the chunks' n_chunks * k keys
+// (distance << 32 | index; empty slots ~0), ascending.  Keys are unique apart
+// from the empty slots (the chunks partition the catalog).  A histogram of the
+// distances (0..128, bin 129 for empty slots) gives the distance D of the k-th
+// smallest key and the count `below` of keys under D (< k).  Those keys are
+// compacted into `low`, the keys at D into the front of `keys` (in place: a
+// round writes only at or below the positions it has read), each group is
+// sorted, and the result is low[0..below) followed by the first k - below keys
+// at D, i.e. by index.  Shared memory per warp: keys[n2], low[64], hist[132].
+constexpr int kMergeBins = 130;
+constexpr int kMergeHist = 132;
+__global__ void topk_merge_kernel(const unsigned long long* __restrict__ part, int nq, int k, int n_chunks, int n2,
+                                  uint32_t* __restrict__ out_idx, uint32_t* __restrict__ out_dist) {
+  extern __shared__ unsigned long long s_keys[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
+  unsigned long long* keys = s_keys + (size_t)warp * (n2 + kTopKMax + kMergeHist / 2);
+  unsigned long long* low = keys + n2;
+  uint32_t* hist = reinterpret_cast<uint32_t*>(low + kTopKMax);
+  if (qi >= nq) return;
+  const int total = n_chunks * k;
+  const unsigned long long* src = part + (long long)qi * total;
+  for (int t = lane; t < kMergeHist; t += 32) hist[t] = 0;
+  for (int t = lane; t < total; t += 32) keys[t] = src[t];
+  __syncwarp();
+  auto bin_of = [](unsigned long long key) {
+    const uint32_t d = (uint32_t)(key >> 32);
+    return d <= 128u ? (int)d : kMergeBins - 1;
+  };
+  for (int t = lane; t < total; t += 32) atomicAdd(&hist[bin_of(keys[t])], 1u);
+  __syncwarp();
+  // D: the bin where the running count reaches k (lane l scans bins 5l .. 5l + 4)
+  int local = 0;
+#pragma unroll
+  for (int b = 0; b < 5; ++b) local += 5 * lane + b < kMergeBins ? (int)hist[5 * lane + b] : 0;
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int excl = incl - local;
+  int my_d = -1, my_below = 0;
+  if (excl < k && incl >= k) {
+    int run = excl;
+    for (int b = 5 * lane; b < 5 * lane + 5; ++b) {
+      const int c = (int)hist[b];
+      if (run + c >= k) {
+        my_d = b;
+        my_below = run;
+        break;
+      }
+      run += c;
+    }
+  }
+  const int owner = __ffs(__ballot_sync(0xffffffffu, my_d >= 0)) - 1;
+  const int D = __shfl_sync(0xffffffffu, my_d, owner);
+  const int below = __shfl_sync(0xffffffffu, my_below, owner);
+  const int n_tie = (int)hist[D];
+  // compaction, in key order of the chunks
+  int n_low = 0, n_at = 0;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int base = 0; base < total; base += 32) {
+    const int t = base + lane;
+    const unsigned long long key = t < total ? keys[t] : ~0ull;
+    const int b = t < total ? bin_of(key) : kMergeBins;
+    const unsigned ml = __ballot_sync(0xffffffffu, b < D);
+    const unsigned mt = __ballot_sync(0xffffffffu, b == D);
+    __syncwarp();
+    if (b < D) low[n_low + __popc(ml & lt)] = key;
+    if (b == D) keys[n_at + __popc(mt & lt)] = key;
+    n_low += __popc(ml);
+    n_at += __popc(mt);
+    __syncwarp();
+  }
+  // sort the group under D (padded to a power of two) and, unless they are all
+  // empty slots, the keys at D
+  int m = 1;
+  while (m < below) m <<= 1;
+  for (int t = below + lane; t < m; t += 32) low[t] = ~0ull;
+  int m2 = 1;
+  while (m2 < n_tie) m2 <<= 1;
+  const bool sort_tie = D < kMergeBins - 1 && n_tie > 1;
+  if (sort_tie)
+    for (int t = n_tie + lane; t < m2; t += 32) keys[t] = ~0ull;
+  __syncwarp();
+  if (below > 1) warp_bitonic_u64(low, m, lane);
+  if (sort_tie) warp_bitonic_u64(keys, m2, lane);
   for (int t = lane; t < k; t += 32) {
-    const unsigned long long key = keys[t];
+    const unsigned long long key = t < below ? low[t] : keys[t - below];
     const bool ok = key != ~0ull;
     out_idx[(long long)qi * k + t] = ok ? (uint32_t)(key & 0xFFFFFFFFu) : 0xFFFFFFFFu;
     out_dist[(long long)qi * k + t] = ok ? (uint32_t)(key >> 32) : 0xFFFFFFFFu;
@@ -428,8 +507,9 @@ cudaError_t launch_topk(const uint64_t* q, int nq, const uint64_t* cat, long lon
   if (e != cudaSuccess) return e;
   int n2 = 1;
   while (n2 < n_chunks * k) n2 <<= 1;
-  const int warps = std::max(1, std::min(8, (int)(96 * 1024 / (n2 * 8))));
-  const size_t smem = (size_t)warps * n2 * 8;
+  const size_t per_warp = ((size_t)n2 + kTopKMax + kMergeHist / 2) * 8;
+  const int warps = std::max(1, std::min(8, (int)(96 * 1024 / per_warp)));
+  const size_t smem = (size_t)warps * per_warp;
   e = ensure_smem_attr((const void*)topk_merge_kernel, smem);
   if (e != cudaSuccess) return e;
   topk_merge_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, st>>>(part, nq, k, n_chunks, n2, out_idx, out_dist);
