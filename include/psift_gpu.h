@@ -118,7 +118,8 @@ psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
  *  - PSIFT_TUNE_BLUR, index = radius 1..15: the level blur's kernel: outputs per
  *    thread 0: 4 columns x 8 rows (the default), 1: 8 x 8, 2: 4 x 4; or 3: TMA
  *    tiles with persistent CTAs (batches of at most 64 images; larger ones use 0).
- *    Every variant computes the same values.
+ *    A batch of images of different sizes runs variant 0's shape (or 3) over a
+ *    list of every image's tiles.  Every variant computes the same values.
  *  - PSIFT_TUNE_MATCH_FP32 / PSIFT_TUNE_MATCH_TC, index 0: the matchers' work items
  *    per SM (default 2); a query tile's target tiles are split into that many
  *    ranges overall, which sets each CTA's target extent.

@@ -45,11 +45,13 @@ constexpr int kStageBatch = 4;          // staging units per thread with loads i
 // the context's tuning table (psift_ctx_autotune): 0 = 4 x 8, 1 = 8 x 8, 2 = 4 x 4.
 constexpr int kPrefetchWaves = 1;       // level blur: L2 prefetch distance in resident-CTA waves
 
-// Per-launch parameters (passed by value).
+// Per-launch parameters (passed by value).  The tile work list of a launch over
+// images of different sizes is a separate parameter of the tiled kernels only,
+// so the equal-size launches keep the small parameter block and a kernel body
+// without the work-list lookup (measured: 2 % of the 8-image 1080p step).
 struct Taps2 {
   float2 w[kMaxTaps];  // {w_k, w_k}
   float2 one;          // {1, 1}: the multiplier of the packed add (see mul_add2_rn)
-  TileMap tiles;
 };
 
 // Linear tile `lin` of a work list (reversed when zrev) -> image and tile; false
@@ -167,13 +169,13 @@ __device__ __forceinline__ float fetch_src(const ImagePlan& P, const OctaveDev& 
 // (one thread per staged row).  With `ahead` = the CTAs resident at once, that
 // tile is staged about one tile-time later and its loads hit L2, so the HBM
 // reads of the next wave overlap the arithmetic of this one.
-template <int R>
+template <int R, bool TILED>
 __device__ __forceinline__ void prefetch_ahead_rows(const ImagePlan* __restrict__ plans, int octave, int level,
-                                                    int zrev, int ahead, const TileMap& tm) {
+                                                    int zrev, int ahead, const TileMap* tm) {
   using Gm = BlurGeom<R>;
   int z, bx, by;
-  if (tm.n > 0) {
-    if (!tile_of(tm, (long long)blockIdx.x + ahead, zrev, z, bx, by)) return;
+  if constexpr (TILED) {
+    if (!tile_of(*tm, (long long)blockIdx.x + ahead, zrev, z, bx, by)) return;
   } else {
     const long long nxy = (long long)gridDim.x * gridDim.y;
     const long long lin = blockIdx.x + (long long)gridDim.x * blockIdx.y + nxy * blockIdx.z + ahead;
@@ -204,13 +206,13 @@ __device__ __forceinline__ void prefetch_ahead_rows(const ImagePlan* __restrict_
 //   MODE_LEVEL: G[s] = blur(G[s-1]); D[s-1] = G[s] - G[s-1]; level `down_level` also
 //               writes the next octave's G[0] (even rows/columns).
 //   MODE_INIT_*: G[0] of octave 0 from the input image.
-template <int R, int HC, int RV, int MODE, bool FUSED>
-__global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const ImagePlan* __restrict__ plans, int octave,
-                                                                   int level, int down_level, int zrev, int pf_ahead,
-                                                                   Taps2 taps) {
+template <int R, int HC, int RV, int MODE, bool FUSED, bool TILED>
+__device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ plans, int octave, int level,
+                                                int down_level, int zrev, int pf_ahead, const Taps2& taps,
+                                                const TileMap* tm) {
   using Gm = BlurGeom<R>;
   if constexpr (MODE == MODE_LEVEL) {
-    if (pf_ahead > 0 && threadIdx.x < Gm::IN_H) prefetch_ahead_rows<R>(plans, octave, level, zrev, pf_ahead, taps.tiles);
+    if (pf_ahead > 0 && threadIdx.x < Gm::IN_H) prefetch_ahead_rows<R, TILED>(plans, octave, level, zrev, pf_ahead, tm);
   }
   static_assert(HC == 4 || HC == 8, "horizontal outputs per thread");
   // The Gaussian taps are bit-symmetric (gaussian_kernel_1d evaluates the same
@@ -222,8 +224,8 @@ __global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const Image
   const float2 one = taps.one;
   static_assert(RV % 2 == 0 && kTileH % (RV * (kBlurThreads / 32)) == 0, "vertical rows per thread");
   int z, bx, by;
-  if (taps.tiles.n > 0) {
-    if (!tile_of(taps.tiles, blockIdx.x, zrev, z, bx, by)) return;
+  if constexpr (TILED) {
+    if (!tile_of(*tm, blockIdx.x, zrev, z, bx, by)) return;
   } else {
     z = zrev ? (int)gridDim.z - 1 - (int)blockIdx.z : (int)blockIdx.z;
     bx = blockIdx.x;
@@ -454,11 +456,28 @@ __global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const Image
 }
 
 template <int R, int HC, int RV, int MODE, bool FUSED>
+__global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const ImagePlan* __restrict__ plans, int octave,
+                                                                   int level, int down_level, int zrev, int pf_ahead,
+                                                                   const __grid_constant__ Taps2 taps) {
+  blur_level_body<R, HC, RV, MODE, FUSED, false>(plans, octave, level, down_level, zrev, pf_ahead, taps, nullptr);
+}
+
+// The same over a tile work list (one CTA per listed tile).
+template <int R, int HC, int RV, int MODE, bool FUSED>
+__global__ void __launch_bounds__(kBlurThreads, 4)
+    blur_level_tiled_kernel(const ImagePlan* __restrict__ plans, int octave, int level, int down_level, int zrev,
+                            int pf_ahead, const __grid_constant__ Taps2 taps, const __grid_constant__ TileMap tiles) {
+  blur_level_body<R, HC, RV, MODE, FUSED, true>(plans, octave, level, down_level, zrev, pf_ahead, taps, &tiles);
+}
+
+template <int R, int HC, int RV, int MODE, bool FUSED, bool TILED>
 static cudaError_t launch_blur_r(const ImagePlan* plans, int n_images, int octave, int level, int down_level,
-                                 int zrev, const Taps2& taps, int max_h, int max_w, cudaStream_t st) {
+                                 int zrev, const Taps2& taps, const TileMap* tiles, int max_h, int max_w,
+                                 cudaStream_t st) {
   using Gm = BlurGeom<R>;
   const size_t smem = Gm::SMEM_BYTES;
-  const void* fn = (const void*)blur_level_kernel<R, HC, RV, MODE, FUSED>;
+  const void* fn = TILED ? (const void*)blur_level_tiled_kernel<R, HC, RV, MODE, FUSED>
+                         : (const void*)blur_level_kernel<R, HC, RV, MODE, FUSED>;
   cudaError_t e = ensure_smem_attr(fn, smem);
   if (e != cudaSuccess) return e;
   int pf_ahead = 0;
@@ -467,19 +486,28 @@ static cudaError_t launch_blur_r(const ImagePlan* plans, int n_images, int octav
     if (e != cudaSuccess) return e;
     pf_ahead *= kPrefetchWaves;
   }
-  dim3 grid((max_w + kTileW - 1) / kTileW, (max_h + kTileH - 1) / kTileH, n_images);
-  if (taps.tiles.n > 0) grid = dim3((unsigned)taps.tiles.prefix[taps.tiles.n], 1, 1);
-  blur_level_kernel<R, HC, RV, MODE, FUSED><<<grid, kBlurThreads, smem, st>>>(plans, octave, level, down_level, zrev,
-                                                                      pf_ahead, taps);
+  if constexpr (TILED) {
+    const dim3 grid((unsigned)tiles->prefix[tiles->n], 1, 1);
+    blur_level_tiled_kernel<R, HC, RV, MODE, FUSED><<<grid, kBlurThreads, smem, st>>>(plans, octave, level,
+                                                                                down_level, zrev, pf_ahead, taps,
+                                                                                *tiles);
+  } else {
+    const dim3 grid((max_w + kTileW - 1) / kTileW, (max_h + kTileH - 1) / kTileH, n_images);
+    blur_level_kernel<R, HC, RV, MODE, FUSED><<<grid, kBlurThreads, smem, st>>>(plans, octave, level, down_level,
+                                                                          zrev, pf_ahead, taps);
+  }
   return cudaGetLastError();
 }
 
-template <int MODE, int HC, int RV, bool FUSED>
+template <int MODE, int HC, int RV, bool FUSED, bool TILED = false>
 static cudaError_t launch_blur_mode(int radius, const ImagePlan* plans, int n, int octave, int level, int down_level,
-                                    int zrev, const Taps2& taps, int max_h, int max_w, cudaStream_t st) {
+                                    int zrev, const Taps2& taps, const TileMap* tiles, int max_h, int max_w,
+                                    cudaStream_t st) {
   switch (radius) {
-#define PSIFT_R(RR) \
-  case RR: return launch_blur_r<RR, HC, RV, MODE, FUSED>(plans, n, octave, level, down_level, zrev, taps, max_h, max_w, st);
+#define PSIFT_R(RR)                                                                                          \
+  case RR:                                                                                                   \
+    return launch_blur_r<RR, HC, RV, MODE, FUSED, TILED>(plans, n, octave, level, down_level, zrev, taps, tiles, \
+                                                         max_h, max_w, st);
     PSIFT_R(1) PSIFT_R(2) PSIFT_R(3) PSIFT_R(4) PSIFT_R(5) PSIFT_R(6) PSIFT_R(7) PSIFT_R(8)
     PSIFT_R(9) PSIFT_R(10) PSIFT_R(11) PSIFT_R(12) PSIFT_R(13) PSIFT_R(14) PSIFT_R(15)
 #undef PSIFT_R
@@ -492,5 +520,10 @@ static cudaError_t launch_blur_mode(int radius, const ImagePlan* plans, int n, i
 // 4 x 8 outputs per thread, and the four octave-base modes.
 cudaError_t launch_blur_fused(int mode, int radius, const ImagePlan* plans, int n, int octave, int level,
                               int down_level, int zrev, const Taps2& taps, int max_h, int max_w, cudaStream_t st);
+// Launches over a tile work list (images of different sizes; pyramid_tiled.cu):
+// the level blur with 4 x 8 outputs per thread and the four octave-base modes,
+// either rounding.
+cudaError_t launch_blur_tiled(int mode, bool fused, int radius, const ImagePlan* plans, int n, int octave, int level,
+                              int down_level, int zrev, const Taps2& taps, const TileMap& tiles, cudaStream_t st);
 
 }  // namespace psift

@@ -25,12 +25,11 @@ EncodeTiledFn encode_tiled() {
 
 template <int R, bool FUSED>
 cudaError_t launch_tma_r(const ImagePlan* d_plans, const ImagePlan* h_plans, int n, int octave, int level,
-                         int down_level, int zrev, const Taps2& taps_in, uint32_t* err, cudaStream_t st) {
+                         int down_level, int zrev, const Taps2& taps, uint32_t* err, cudaStream_t st) {
   using G = TmaGeom<R>;
   EncodeTiledFn enc = encode_tiled();
   if (!enc) return cudaErrorNotSupported;
-  Taps2 taps = taps_in;
-  TileMap& tm = taps.tiles;
+  TileMap tm;
   tm.n = n;
   tm.prefix[0] = 0;
   TmaPlanes maps;
@@ -64,7 +63,7 @@ cudaError_t launch_tma_r(const ImagePlan* d_plans, const ImagePlan* h_plans, int
   if (e != cudaSuccess) return e;
   const int grid = resident < total ? resident : total;
   blur_tma_kernel<R, FUSED><<<grid, kBlurThreads, G::SMEM_BYTES, st>>>(d_plans, octave, level, down_level, zrev, taps,
-                                                                    maps, err);
+                                                                    tm, maps, err);
   return cudaGetLastError();
 }
 

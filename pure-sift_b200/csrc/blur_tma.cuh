@@ -72,7 +72,8 @@ __device__ __forceinline__ bool tma_mbar_wait(uint64_t* bar, uint32_t parity) {
 template <int R, bool FUSED>
 __global__ void __launch_bounds__(kBlurThreads, TmaGeom<R>::MIN_CTAS)
     blur_tma_kernel(const ImagePlan* __restrict__ plans, int octave, int level, int down_level, int zrev,
-                    const __grid_constant__ Taps2 taps, const __grid_constant__ TmaPlanes maps, uint32_t* err) {
+                    const __grid_constant__ Taps2 taps, const __grid_constant__ TileMap tm,
+                    const __grid_constant__ TmaPlanes maps, uint32_t* err) {
   using G = TmaGeom<R>;
   constexpr int RV = 8;
   extern __shared__ __align__(128) uint8_t tsm[];
@@ -83,7 +84,6 @@ __global__ void __launch_bounds__(kBlurThreads, TmaGeom<R>::MIN_CTAS)
 #pragma unroll
   for (int k = 0; k <= R; ++k) wv[k] = taps.w[k];
   const float2 one = taps.one;
-  const TileMap& tm = taps.tiles;
   const int total = tm.prefix[tm.n];
 
   // tile lin -> image and tile origin

@@ -1,6 +1,7 @@
 // K1-K3 host dispatch: octave base and level blurs (the kernel template lives in
-// blur_kernel.cuh; this file instantiates the reference-rounding blur, and
-// pyramid_fused.cu the single-rounding one).
+// blur_kernel.cuh; this file instantiates the reference-rounding blur over a
+// (tiles x, tiles y, images) grid, pyramid_fused.cu the single-rounding one, and
+// pyramid_tiled*.cu both over a tile work list).
 #include "blur_kernel.cuh"
 
 namespace psift {
@@ -18,12 +19,6 @@ cudaError_t launch_blur(int mode, const float* taps_host, int radius, const Imag
                         int level, int down_level, int max_h, int max_w, cudaStream_t st, int variant, bool fused,
                         const TileMap* tiles, const ImagePlan* h_plans, uint32_t* err) {
   Taps2 t;
-  if (tiles && tiles->n > 0) {
-    t.tiles = *tiles;
-  } else {
-    t.tiles.n = 0;
-    t.tiles.prefix[0] = 0;
-  }
   for (int i = 0; i < kMaxTaps; ++i) {
     const float v = i <= 2 * radius ? taps_host[i] : 0.0f;
     t.w[i] = make_float2(v, v);
@@ -33,19 +28,22 @@ cudaError_t launch_blur(int mode, const float* taps_host, int radius, const Imag
   // variant 3: TMA tiles, persistent CTAs (blur_tma.cuh), either rounding
   if (mode == MODE_LEVEL && variant == 3)
     return launch_blur_tma(radius, fused, plans, h_plans, n, octave, level, down_level, zrev, t, err, st);
+  // images of different sizes: one CTA per listed tile (4 x 8 outputs per thread)
+  if (tiles && tiles->n > 0)
+    return launch_blur_tiled(mode, fused, radius, plans, n, octave, level, down_level, zrev, t, *tiles, st);
   if (fused) return launch_blur_fused(mode, radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
   switch (mode) {
     case MODE_LEVEL:
       switch (variant) {
-        case 0: return launch_blur_mode<MODE_LEVEL, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-        case 1: return launch_blur_mode<MODE_LEVEL, 8, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-        case 2: return launch_blur_mode<MODE_LEVEL, 4, 4, false>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+        case 0: return launch_blur_mode<MODE_LEVEL, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
+        case 1: return launch_blur_mode<MODE_LEVEL, 8, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
+        case 2: return launch_blur_mode<MODE_LEVEL, 4, 4, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
         default: return cudaErrorInvalidValue;
       }
-    case MODE_INIT_F32: return launch_blur_mode<MODE_INIT_F32, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-    case MODE_INIT_U8: return launch_blur_mode<MODE_INIT_U8, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-    case MODE_INIT_F32_UP: return launch_blur_mode<MODE_INIT_F32_UP, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
-    case MODE_INIT_U8_UP: return launch_blur_mode<MODE_INIT_U8_UP, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, max_h, max_w, st);
+    case MODE_INIT_F32: return launch_blur_mode<MODE_INIT_F32, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
+    case MODE_INIT_U8: return launch_blur_mode<MODE_INIT_U8, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
+    case MODE_INIT_F32_UP: return launch_blur_mode<MODE_INIT_F32_UP, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
+    case MODE_INIT_U8_UP: return launch_blur_mode<MODE_INIT_U8_UP, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -12,20 +12,20 @@ cudaError_t launch_blur_fused(int mode, int radius, const ImagePlan* plans, int 
                               int down_level, int zrev, const Taps2& taps, int max_h, int max_w, cudaStream_t st) {
   switch (mode) {
     case MODE_LEVEL:
-      return launch_blur_mode<MODE_LEVEL, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, max_h,
-                                                max_w, st);
+      return launch_blur_mode<MODE_LEVEL, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, nullptr,
+                                                      max_h, max_w, st);
     case MODE_INIT_F32:
-      return launch_blur_mode<MODE_INIT_F32, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, max_h,
-                                                max_w, st);
+      return launch_blur_mode<MODE_INIT_F32, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, nullptr,
+                                                      max_h, max_w, st);
     case MODE_INIT_U8:
-      return launch_blur_mode<MODE_INIT_U8, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, max_h,
-                                                max_w, st);
+      return launch_blur_mode<MODE_INIT_U8, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, nullptr,
+                                                      max_h, max_w, st);
     case MODE_INIT_F32_UP:
-      return launch_blur_mode<MODE_INIT_F32_UP, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, max_h,
-                                                max_w, st);
+      return launch_blur_mode<MODE_INIT_F32_UP, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, nullptr,
+                                                      max_h, max_w, st);
     case MODE_INIT_U8_UP:
-      return launch_blur_mode<MODE_INIT_U8_UP, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, max_h,
-                                                max_w, st);
+      return launch_blur_mode<MODE_INIT_U8_UP, 4, 8, true>(radius, plans, n, octave, level, down_level, zrev, taps, nullptr,
+                                                      max_h, max_w, st);
     default:
       return cudaErrorInvalidValue;
   }
