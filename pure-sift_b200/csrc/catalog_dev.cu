@@ -105,7 +105,9 @@ cudaError_t copy_range(FeatureArrays& d, uint64_t dst_off, const FeatureArrays& 
 // word after the record is read only when the record is not word-aligned), and
 // funnel shifts give the record's own words 0..40: x, y, scale, response,
 // orientation, the stored 128-bit signature (kept as it is), then the 128
-// descriptor bytes, which go to q8 for dequantize_descriptor_u8.
+// descriptor bytes, which go to q8 for dequantize_descriptor_u8 (one 128-byte
+// store per record); the other fields are gathered in shared memory and stored
+// once per warp, each array's 32 entries together.
 constexpr int kSplitWarps = 8;
 constexpr int kSplitPerWarp = 32;
 constexpr int kSplitBatch = 4;
@@ -114,6 +116,9 @@ __global__ void __launch_bounds__(kSplitWarps * 32)
                           const long long* __restrict__ out_off, int n_entries, long long total, float2* xy,
                           float* scale, float* resp, float* ori, uint64_t* codes, uint8_t* q8) {
   constexpr unsigned kFull = 0xffffffffu;
+  // record words 0..8 (x, y, scale, response, orientation, signature) of the
+  // warp's records, field-major, written out coalesced at the end
+  __shared__ uint32_t s_fld[kSplitWarps][9][kSplitPerWarp + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long i0 = ((long long)blockIdx.x * kSplitWarps + warp) * kSplitPerWarp;
   if (i0 >= total) return;
@@ -159,13 +164,18 @@ __global__ void __launch_bounds__(kSplitWarps * 32)
       const uint32_t qa = __shfl_sync(kFull, o0, lane + 9 < 32 ? lane + 9 : 31);
       const uint32_t qb = __shfl_sync(kFull, o1, lane >= 23 ? lane - 23 : 0);
       reinterpret_cast<uint32_t*>(q8 + i * 128)[lane] = lane <= 22 ? qa : qb;
-      const uint32_t nx = __shfl_down_sync(kFull, o0, 1);
-      if (lane == 0) xy[i] = make_float2(__uint_as_float(o0), __uint_as_float(nx));
-      if (lane == 2) scale[i] = __uint_as_float(o0);
-      if (lane == 3) resp[i] = __uint_as_float(o0);
-      if (lane == 4) ori[i] = __uint_as_float(o0);
-      if (lane == 5 || lane == 7) codes[2 * i + (lane - 5) / 2] = (uint64_t)o0 | ((uint64_t)nx << 32);
+      if (lane < 9) s_fld[warp][lane][i - i0] = o0;
     }
+  }
+  __syncwarp();
+  const long long i = i0 + lane;
+  if (i < i1) {
+    const uint32_t(*f)[kSplitPerWarp + 1] = s_fld[warp];
+    xy[i] = make_float2(__uint_as_float(f[0][lane]), __uint_as_float(f[1][lane]));
+    scale[i] = __uint_as_float(f[2][lane]);
+    resp[i] = __uint_as_float(f[3][lane]);
+    ori[i] = __uint_as_float(f[4][lane]);
+    reinterpret_cast<uint4*>(codes)[i] = make_uint4(f[5][lane], f[6][lane], f[7][lane], f[8][lane]);
   }
 }
 
