@@ -216,38 +216,54 @@ __device__ __forceinline__ uint32_t paeth(uint32_t a, uint32_t b, uint32_t c) {
   return (pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c);
 }
 
-constexpr int kRing = 512;  // bytes of a lane's row staged in shared memory (four 128-byte chunks)
+constexpr int kRing = 512;          // bytes of a lane's row staged in shared memory (four 128-byte chunks)
+constexpr int kUnfWarps = 12;       // row groups of a plane in flight at once (one warp each)
+constexpr uint32_t kUnfSpin = 1u << 22;  // bounded wait on the previous group (with nanosleep)
 
-// One warp per plane (a CTA per plane).  Rows go 32 at a time; at step s lane t
-// reconstructs unit (pixel) s - t of row g + t, so the row above at that unit
-// is what lane t - 1 reconstructed at step s - 1 (a shuffle) and the unit before
-// it lane t - 1's value one step earlier; lane 0 takes the previous group's last
-// row from shared memory (above_smem) or memory.  Each lane's filtered row
-// streams through a ring of 128-byte chunks in shared memory, the next chunk
-// copied asynchronously while the current one is consumed (lane 31 trails lane 0
-// by at most 31 units = 248 bytes, inside the ring).  Units are UNIT bytes, the
-// filter's byte distance.
+// One CTA (kUnfWarps warps) per plane.  Rows go in groups of 32; group k is
+// warp k mod kUnfWarps's, so up to kUnfWarps groups run at once, each behind the
+// one above it.  Inside a group, at step s lane t reconstructs unit (pixel) s - t
+// of row 32k + t: the row above at that unit is what lane t - 1 reconstructed at
+// step s - 1 (a shuffle) and the unit before it lane t - 1's value one step
+// earlier.  Lane 0's row above is the previous group's last row: every 32 steps
+// the warp waits until that row is done up to the units of its next 32 steps
+// (the previous group's lane 31 publishes its count after each 32 steps with a
+// release store; lanes read it with acquire loads), then copies those units to
+// shared memory.  Each lane's filtered row streams through a ring of 128-byte
+// chunks in shared memory, the next chunk copied asynchronously while the
+// current one is consumed (lane 31 trails lane 0 by at most 31 units = 248
+// bytes, inside the ring).  Units are UNIT bytes, the filter's byte distance.
+// The waits are bounded: on timeout the warp records kErrTimeout and leaves
+// (the groups after it then time out too).
 template <int UNIT>
-__global__ void __launch_bounds__(32) png_unfilter_kernel(const PngPlane* __restrict__ planes, int above_smem) {
+__global__ void __launch_bounds__(32 * kUnfWarps) png_unfilter_kernel(const PngPlane* __restrict__ planes,
+                                                                      uint32_t* err) {
   extern __shared__ __align__(16) uint8_t psm[];
-  uint8_t* ring = psm;                      // [32][kRing]
-  uint8_t* last = psm + 32 * kRing;         // [2][row_bytes rounded to 16]: the groups' last rows
-  const int lane = threadIdx.x;
+  unsigned long long* progress = reinterpret_cast<unsigned long long*>(psm);         // [kUnfWarps]
+  uint8_t* abuf_all = psm + 16 * kUnfWarps;                                        // [kUnfWarps][32 * 8]
+  uint8_t* ring_all = abuf_all + 256 * kUnfWarps;                                  // [kUnfWarps][32][kRing]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const PngPlane P = planes[blockIdx.x];
   const uint32_t rb = P.row_bytes, npix = rb / UNIT;
   const uint32_t rb16 = (rb + 15) & ~15u;
   const uint32_t nchunks = (rb + 127) / 128;
-  uint8_t* my_ring = ring + lane * kRing;
-  for (uint32_t g = 0; g < P.rows; g += 32) {
+  uint8_t* my_ring = ring_all + ((size_t)warp * 32 + lane) * kRing;
+  uint8_t* abuf = abuf_all + warp * 256;
+  if (threadIdx.x < kUnfWarps) progress[threadIdx.x] = 0ull;
+  __syncthreads();
+  const unsigned long long span = (unsigned long long)npix + 1ull;  // progress of group k = k * span + units
+  const uint32_t groups = (P.rows + 31) / 32;
+  for (uint32_t k = warp; k < groups; k += kUnfWarps) {
+    const uint32_t g = 32 * k;
     const uint32_t r = g + lane;
     const bool row_ok = r < P.rows;
     const uint8_t* slot = P.in + (size_t)r * P.stride;
     const uint32_t f = row_ok ? slot[15] : 0u;
     const uint8_t* src = slot + 16;
     uint8_t* dst = P.out + (size_t)r * rb;
-    const uint8_t* above_g = (g > 0) ? P.out + (size_t)(g - 1) * rb : nullptr;  // row g - 1 (lane 0)
-    const uint8_t* above_s = last + ((g / 32 + 1) & 1) * rb16;                  // the same row, staged
-    uint8_t* last_w = last + ((g / 32) & 1) * rb16;                              // this group's last row
+    const uint8_t* above_g = (g > 0) ? P.out + (size_t)(g - 1) * rb : nullptr;  // row g - 1 (lane 0's above)
+    const unsigned long long* prev = progress + (k + kUnfWarps - 1) % kUnfWarps;
+    unsigned long long* mine = progress + warp;
     // chunk c of this lane's row into ring slot c % 4 (16-byte copies inside the row slot)
     auto fetch = [&](uint32_t c) {
       if (row_ok && c < nchunks)
@@ -265,58 +281,94 @@ __global__ void __launch_bounds__(32) png_unfilter_kernel(const PngPlane* __rest
     uint32_t cur = 0;
     uint8_t a[UNIT], c[UNIT], mine_prev[UNIT];  // left unit, above-left unit, this lane's last unit
 #pragma unroll
-    for (int k = 0; k < UNIT; ++k) a[k] = c[k] = mine_prev[k] = 0;
+    for (int q = 0; q < UNIT; ++q) a[q] = c[q] = mine_prev[q] = 0;
     const uint32_t steps = npix + 31;
-    for (uint32_t s = 0; s < steps; ++s) {
-      // lane 0 (the leading lane) reached a new chunk with its unit's last byte:
-      // the chunk's successor is copied, the chunk itself is waited for
-      const uint32_t lead = min(s, npix - 1) * UNIT + UNIT - 1;
-      if ((lead >> 7) != cur) {
-        cur = lead >> 7;
-        fetch(cur + 1);
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
+    for (uint32_t s0 = 0; s0 < steps; s0 += 32) {
+      // lane 0's row above, units s0 .. s0 + 31
+      if (g > 0 && s0 < npix) {
+        const uint32_t need = min(npix, s0 + 32);
+        const unsigned long long target = (unsigned long long)(k - 1) * span + need;
+        bool ok = false;
+        for (uint32_t it = 0; it < kUnfSpin; ++it) {
+          unsigned long long v;
+          asm volatile("ld.acquire.cta.shared.u64 %0, [%1];" : "=l"(v) : "r"((uint32_t)__cvta_generic_to_shared(prev))
+                       : "memory");
+          if (v >= target) {
+            ok = true;
+            break;
+          }
+          __nanosleep(64);
+        }
+        if (!__all_sync(0xffffffffu, ok)) {
+          if (lane == 0) atomicOr(err, kErrTimeout);
+          asm volatile("cp.async.wait_group 0;" ::: "memory");
+          return;
+        }
+        const uint32_t u = s0 + lane;
+        if (u < npix)
+#pragma unroll
+          for (int q = 0; q < UNIT; ++q) abuf[lane * UNIT + q] = __ldcg(above_g + (size_t)u * UNIT + q);
         __syncwarp();
       }
-      // the unit lane - 1 reconstructed at step s - 1 = this lane's above unit
-      uint32_t w0 = 0, w1 = 0;
-#pragma unroll
-      for (int k = 0; k < UNIT; ++k) {
-        if (k < 4) w0 |= (uint32_t)mine_prev[k] << (8 * k);
-        else w1 |= (uint32_t)mine_prev[k] << (8 * (k - 4));
-      }
-      w0 = __shfl_up_sync(0xffffffffu, w0, 1);
-      if (UNIT > 4) w1 = __shfl_up_sync(0xffffffffu, w1, 1);
-      const int i = (int)s - lane;
-      const bool act = row_ok && i >= 0 && (uint32_t)i < npix;
-      uint8_t b[UNIT];
-#pragma unroll
-      for (int k = 0; k < UNIT; ++k) b[k] = (uint8_t)((k < 4 ? w0 >> (8 * k) : w1 >> (8 * (k - 4))) & 0xFF);
-      if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < UNIT; ++k)
-          b[k] = (act && g > 0) ? (above_smem ? above_s[(size_t)i * UNIT + k] : above_g[(size_t)i * UNIT + k]) : 0;
-      }
-      if (act) {
-        if (i == 0) {
-#pragma unroll
-          for (int k = 0; k < UNIT; ++k) a[k] = c[k] = 0;
+      const uint32_t s1 = min(steps, s0 + 32);
+      for (uint32_t s = s0; s < s1; ++s) {
+        // lane 0 (the leading lane) reached a new chunk with its unit's last byte:
+        // the chunk's successor is copied, the chunk itself is waited for
+        const uint32_t lead = min(s, npix - 1) * UNIT + UNIT - 1;
+        if ((lead >> 7) != cur) {
+          cur = lead >> 7;
+          fetch(cur + 1);
+          asm volatile("cp.async.wait_group 1;" ::: "memory");
+          __syncwarp();
         }
+        // the unit lane - 1 reconstructed at step s - 1 = this lane's above unit
+        uint32_t w0 = 0, w1 = 0;
 #pragma unroll
-        for (int k = 0; k < UNIT; ++k) {
-          const uint32_t x = my_ring[((uint32_t)i * UNIT + k) & (kRing - 1)];
-          const uint32_t av = a[k], bv = r > 0 ? b[k] : 0u, cv = r > 0 ? c[k] : 0u;
-          const uint32_t pred = f == 1 ? av : f == 2 ? bv : f == 3 ? (av + bv) >> 1 : f == 4 ? paeth(av, bv, cv) : 0u;
-          const uint8_t v = (uint8_t)(x + pred);
-          dst[(size_t)i * UNIT + k] = v;
-          if (lane == 31 && above_smem) last_w[(size_t)i * UNIT + k] = v;
-          a[k] = v;
-          c[k] = (uint8_t)bv;
-          mine_prev[k] = v;
+        for (int q = 0; q < UNIT; ++q) {
+          if (q < 4) w0 |= (uint32_t)mine_prev[q] << (8 * q);
+          else w1 |= (uint32_t)mine_prev[q] << (8 * (q - 4));
         }
+        w0 = __shfl_up_sync(0xffffffffu, w0, 1);
+        if (UNIT > 4) w1 = __shfl_up_sync(0xffffffffu, w1, 1);
+        const int i = (int)s - lane;
+        const bool act = row_ok && i >= 0 && (uint32_t)i < npix;
+        uint8_t bb[UNIT];
+#pragma unroll
+        for (int q = 0; q < UNIT; ++q) bb[q] = (uint8_t)((q < 4 ? w0 >> (8 * q) : w1 >> (8 * (q - 4))) & 0xFF);
+        if (lane == 0) {
+#pragma unroll
+          for (int q = 0; q < UNIT; ++q) bb[q] = (act && g > 0) ? abuf[(s - s0) * UNIT + q] : 0;
+        }
+        if (act) {
+          if (i == 0) {
+#pragma unroll
+            for (int q = 0; q < UNIT; ++q) a[q] = c[q] = 0;
+          }
+#pragma unroll
+          for (int q = 0; q < UNIT; ++q) {
+            const uint32_t x = my_ring[((uint32_t)i * UNIT + q) & (kRing - 1)];
+            const uint32_t av = a[q], bv = r > 0 ? bb[q] : 0u, cv = r > 0 ? c[q] : 0u;
+            const uint32_t pred =
+                f == 1 ? av : f == 2 ? bv : f == 3 ? (av + bv) >> 1 : f == 4 ? paeth(av, bv, cv) : 0u;
+            const uint8_t v = (uint8_t)(x + pred);
+            dst[(size_t)i * UNIT + q] = v;
+            a[q] = v;
+            c[q] = (uint8_t)bv;
+            mine_prev[q] = v;
+          }
+        }
+      }
+      // this group's last row (lane 31) is done up to unit s1 - 32: publish
+      __syncwarp();
+      if (lane == 31) {
+        const uint32_t done = s1 >= 32 ? min(npix, s1 - 31) : 0u;
+        const unsigned long long v = (unsigned long long)k * span + done;
+        asm volatile("st.release.cta.shared.u64 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(mine)), "l"(v)
+                     : "memory");
       }
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
-    __syncwarp();  // this group's rows (memory and the staged last row) are visible to the next group
+    __syncwarp();
   }
 }
 
@@ -502,15 +554,12 @@ psift_status inflate_range(psift_ctx* ctx, const std::vector<PngImage>& P, const
 }
 
 template <int UNIT>
-cudaError_t launch_unfilter(const PngPlane* planes, int n, uint32_t max_rb, cudaStream_t st) {
+cudaError_t launch_unfilter(const PngPlane* planes, int n, uint32_t* err, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  // the groups' last rows staged in shared memory when two of them fit
-  const size_t rb16 = (max_rb + 15) & ~size_t(15);
-  const bool above_smem = 32 * kRing + 2 * rb16 <= 200 * 1024;
-  const size_t smem = 32 * kRing + (above_smem ? 2 * rb16 : 0);
+  const size_t smem = (size_t)kUnfWarps * (16 + 256 + 32 * kRing);
   cudaError_t e = ensure_smem_attr((const void*)png_unfilter_kernel<UNIT>, smem);
   if (e != cudaSuccess) return e;
-  png_unfilter_kernel<UNIT><<<n, 32, smem, st>>>(planes, above_smem ? 1 : 0);
+  png_unfilter_kernel<UNIT><<<n, 32 * kUnfWarps, smem, st>>>(planes, err);
   return cudaGetLastError();
 }
 
@@ -535,7 +584,6 @@ psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, co
   PngLumaJob* hj = reinterpret_cast<PngLumaJob*>(pin_desc + job_base) + b;
   const int units[6] = {1, 2, 3, 4, 6, 8};
   int count[6] = {0, 0, 0, 0, 0, 0};
-  uint32_t max_rb[6] = {0, 0, 0, 0, 0, 0};
   int np = 0;
   uint32_t max_px = 0;
   for (int u = 0; u < 6; ++u) {
@@ -547,7 +595,6 @@ psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, co
         hp[np++] = PngPlane{S->dev + L.dev_raw[i] + I.pass_in[p], S->dev + L.dev_unf[i] + I.pass_out[p],
                             I.pass_h[p], (uint32_t)I.pass_rb[p], (uint32_t)I.pass_stride[p]};
         ++count[u];
-        max_rb[u] = std::max(max_rb[u], (uint32_t)I.pass_rb[p]);
       }
     }
   }
@@ -587,12 +634,12 @@ psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, co
   for (int u = 0; u < 6 && ce == cudaSuccess; ++u) {
     if (!count[u]) continue;
     switch (units[u]) {
-      case 1: ce = launch_unfilter<1>(dp + off, count[u], max_rb[u], st); break;
-      case 2: ce = launch_unfilter<2>(dp + off, count[u], max_rb[u], st); break;
-      case 3: ce = launch_unfilter<3>(dp + off, count[u], max_rb[u], st); break;
-      case 4: ce = launch_unfilter<4>(dp + off, count[u], max_rb[u], st); break;
-      case 6: ce = launch_unfilter<6>(dp + off, count[u], max_rb[u], st); break;
-      default: ce = launch_unfilter<8>(dp + off, count[u], max_rb[u], st); break;
+      case 1: ce = launch_unfilter<1>(dp + off, count[u], ctx->d_error, st); break;
+      case 2: ce = launch_unfilter<2>(dp + off, count[u], ctx->d_error, st); break;
+      case 3: ce = launch_unfilter<3>(dp + off, count[u], ctx->d_error, st); break;
+      case 4: ce = launch_unfilter<4>(dp + off, count[u], ctx->d_error, st); break;
+      case 6: ce = launch_unfilter<6>(dp + off, count[u], ctx->d_error, st); break;
+      default: ce = launch_unfilter<8>(dp + off, count[u], ctx->d_error, st); break;
     }
     off += count[u];
     ctx->launches++;
@@ -656,9 +703,13 @@ psift_status psift_decode_png_luma(psift_ctx* ctx, const uint8_t* data, size_t l
   if ((st = png_reserve(ctx, P, L)) != PSIFT_OK) return st;
   uint8_t* d_luma = (uint8_t*)ctx->io.base;
   uint8_t* const outs[1] = {d_luma};
+  PSIFT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, 4, ctx->stream));
   if ((st = decode_png_range(ctx, P, L, 0, 1, outs, ctx->stream)) != PSIFT_OK) return st;
   PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(luma, d_luma, px, cudaMemcpyDeviceToHost, ctx->stream));
+  uint32_t word = 0;  // pageable: the copy completes before the synchronisation returns
+  PSIFT_CUDA_TRY(ctx, cudaMemcpyAsync(&word, ctx->d_error, 4, cudaMemcpyDeviceToHost, ctx->stream));
   PSIFT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (word & kErrTimeout) return set_error(ctx, PSIFT_ERR_TIMEOUT, "device wait timed out (png row filters)");
   return PSIFT_OK;
 }
 
