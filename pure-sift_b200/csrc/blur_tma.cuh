@@ -1,5 +1,5 @@
 // Level blur with 2-D TMA tiles: the input tile of G[s-1] (tile + halo) arrives
-// in shared memory by one cp.async.bulk.tensor.2d (no multicast) on an mbarrier,
+// in shared memory by one cp.async.bulk.tensor.2d on an mbarrier,
 // into a double-buffered stage: the CTA's next tile is copied during the whole of
 // the current tile's horizontal and vertical passes.
 //
