@@ -1156,7 +1156,7 @@ def run_ours(args):
                            "blur_ms_per_variant": {r: e["ms"] for r, e in tune["blur"].items()},
                            "match_fp32_items_per_sm": tune["match_fp32"]["per_sm"],
                            "match_tc_items_per_sm": tune["match_tc"]["per_sm"],
-                           "variants": "blur 0: 4x8, 1: 8x8, 2: 4x4 outputs per thread (columns x rows); 3: TMA tiles, persistent CTAs"}},
+                           "variants": "blur 0: 4x8, 1: 8x8, 2: 4x4 outputs per thread (columns x rows); 3: TMA tiles, persistent CTAs; 4: 128-row tiles, 512 threads"}},
             "gpu_launches": int(launches),
             "e2e": {"value": e2e_value, "unit": "images/s", "h2d_bytes_per_step": B * WIDTH * HEIGHT,
                     "d2h_bytes_per_step": int(d2h),
@@ -1223,7 +1223,7 @@ def main():
     ap.add_argument("--ransac-pairs", type=int, default=1024, help="learned-RANSAC section: match sets")
     ap.add_argument("--blur", choices=["reference", "fused"], default="reference",
                     help="blur rounding of the main loop (profiling case; the default is the reference's)")
-    ap.add_argument("--blur-variant", type=int, choices=[0, 1, 2, 3], default=None,
+    ap.add_argument("--blur-variant", type=int, choices=[0, 1, 2, 3, 4], default=None,
                     help="pyramid section: run this level-blur variant at every radius (profiling case)")
     ap.add_argument("--catalog-codes", type=int, default=2_000_000, help="catalog section: catalog codes")
     ap.add_argument("--catalog-entries", type=int, default=10_000, help="catalog-search section: entries")

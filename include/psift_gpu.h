@@ -116,8 +116,9 @@ psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
 /* Tile shapes, chosen by the library's autotuner.  No counterpart in the
  * reference.  Every choice computes identical results; only time differs.
  *  - PSIFT_TUNE_BLUR, index = radius 1..15: the level blur's kernel: outputs per
- *    thread 0: 4 columns x 8 rows (the default), 1: 8 x 8, 2: 4 x 4; or 3: TMA
- *    tiles with persistent CTAs (batches of at most 64 images; larger ones use 0).
+ *    thread 0: 4 columns x 8 rows (the default), 1: 8 x 8, 2: 4 x 4; 3: TMA
+ *    tiles with persistent CTAs (batches of at most 64 images; larger ones use 0);
+ *    4: 128-row tiles of 512 threads (4 x 8 outputs per thread).
  *    A batch of images of different sizes runs variant 0's shape (or 3) over a
  *    list of every image's tiles.  Every variant computes the same values.
  *  - PSIFT_TUNE_MATCH_FP32 / PSIFT_TUNE_MATCH_TC, index 0: the matchers' work items
@@ -129,7 +130,7 @@ psift_status psift_ctx_enable_stage_timing(psift_ctx* ctx, int enable);
  * and keeps the fastest in the context (for the blur, another variant replaces
  * variant 0 only when it is at least 3 % faster).  report (optional, report_capacity
  * doubles; report_count = the doubles written): per blur radius (radius, ms of
- * variants 0..3, chosen), then -1, then per matcher path (path 0 FP32 / 1 tensor
+ * variants 0..4, chosen), then -1, then per matcher path (path 0 FP32 / 1 tensor
  * core, ms for 1, 2, 4, 8 work items per SM, chosen). */
 #define PSIFT_TUNE_BLUR 0
 #define PSIFT_TUNE_MATCH_FP32 1

@@ -75,11 +75,11 @@ __device__ __forceinline__ bool tile_of(const TileMap& tm, long long lin, int zr
 
 enum BlurMode : int { MODE_LEVEL = 0, MODE_INIT_F32 = 1, MODE_INIT_U8 = 2, MODE_INIT_F32_UP = 3, MODE_INIT_U8_UP = 4 };
 
-template <int R>
+template <int R, int TH = kTileH>
 struct BlurGeom {
   static constexpr int RP = (R + 3) / 4 * 4;                          // column halo, whole float4 chunks
   static constexpr int IN_W = kTileW + 2 * RP;                        // staged columns
-  static constexpr int IN_H = kTileH + 2 * R;                         // staged rows (even)
+  static constexpr int IN_H = TH + 2 * R;                             // staged rows (even)
   static constexpr int IN_PAIRS = IN_H / 2;
   static constexpr int IN_S = IN_W + (((2 - IN_W) % 16) + 16) % 16;   // float2 per row pair, = 2 (mod 16)
   static constexpr int C4 = IN_W / 4;
@@ -169,10 +169,10 @@ __device__ __forceinline__ float fetch_src(const ImagePlan& P, const OctaveDev& 
 // (one thread per staged row).  With `ahead` = the CTAs resident at once, that
 // tile is staged about one tile-time later and its loads hit L2, so the HBM
 // reads of the next wave overlap the arithmetic of this one.
-template <int R, bool TILED>
+template <int R, bool TILED, int TH>
 __device__ __forceinline__ void prefetch_ahead_rows(const ImagePlan* __restrict__ plans, int octave, int level,
                                                     int zrev, int ahead, const TileMap* tm) {
-  using Gm = BlurGeom<R>;
+  using Gm = BlurGeom<R, TH>;
   int z, bx, by;
   if constexpr (TILED) {
     if (!tile_of(*tm, (long long)blockIdx.x + ahead, zrev, z, bx, by)) return;
@@ -189,7 +189,7 @@ __device__ __forceinline__ void prefetch_ahead_rows(const ImagePlan* __restrict_
   const ImagePlan& P = plans[z];
   if (octave >= P.n_oct) return;
   const OctaveDev& O = P.oct[octave];
-  const int tx0 = bx * kTileW, ty0 = by * kTileH;
+  const int tx0 = bx * kTileW, ty0 = by * TH;
   if (tx0 >= O.w || ty0 >= O.h) return;
   // rows clamped like the staging; columns [c0, c1) are 16-byte aligned and end
   // inside the row pitch (a multiple of 32 floats)
@@ -206,13 +206,16 @@ __device__ __forceinline__ void prefetch_ahead_rows(const ImagePlan* __restrict_
 //   MODE_LEVEL: G[s] = blur(G[s-1]); D[s-1] = G[s] - G[s-1]; level `down_level` also
 //               writes the next octave's G[0] (even rows/columns).
 //   MODE_INIT_*: G[0] of octave 0 from the input image.
-template <int R, int HC, int RV, int MODE, bool FUSED, bool TILED>
+// TH x 64 tiles (TH = 64, or 128 for the tall variant), NT threads.
+template <int R, int HC, int RV, int MODE, bool FUSED, bool TILED, int TH = kTileH, int NT = kBlurThreads>
 __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ plans, int octave, int level,
                                                 int down_level, int zrev, int pf_ahead, const Taps2& taps,
                                                 const TileMap* tm) {
-  using Gm = BlurGeom<R>;
+  using Gm = BlurGeom<R, TH>;
+  static_assert(!TILED || TH == kTileH, "tile work lists are in 64 x 64 tiles");
   if constexpr (MODE == MODE_LEVEL) {
-    if (pf_ahead > 0 && threadIdx.x < Gm::IN_H) prefetch_ahead_rows<R, TILED>(plans, octave, level, zrev, pf_ahead, tm);
+    if (pf_ahead > 0 && threadIdx.x < Gm::IN_H)
+      prefetch_ahead_rows<R, TILED, TH>(plans, octave, level, zrev, pf_ahead, tm);
   }
   static_assert(HC == 4 || HC == 8, "horizontal outputs per thread");
   // The Gaussian taps are bit-symmetric (gaussian_kernel_1d evaluates the same
@@ -222,7 +225,7 @@ __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ pl
 #pragma unroll
   for (int k = 0; k <= R; ++k) wv[k] = taps.w[k];
   const float2 one = taps.one;
-  static_assert(RV % 2 == 0 && kTileH % (RV * (kBlurThreads / 32)) == 0, "vertical rows per thread");
+  static_assert(RV % 2 == 0 && TH % (RV * (NT / 32)) == 0, "vertical rows per thread");
   int z, bx, by;
   if constexpr (TILED) {
     if (!tile_of(*tm, blockIdx.x, zrev, z, bx, by)) return;
@@ -235,7 +238,7 @@ __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ pl
   if (octave >= P.n_oct) return;
   const OctaveDev& O = P.oct[octave];
   const int h = O.h, w = O.w;
-  const int tx0 = bx * kTileW, ty0 = by * kTileH;
+  const int tx0 = bx * kTileW, ty0 = by * TH;
   if (tx0 >= w || ty0 >= h) return;
 
   extern __shared__ float4 smem4[];
@@ -256,11 +259,11 @@ __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ pl
     sx_lo = clampi(tx0 - Gm::RP, 0, w - 1) >> 1;
     const int sh = min(SRC_H, P.src_h - sy_lo), sw = min(SRC_W, P.src_w - sx_lo);
     // every load of the thread is issued before the first store
-    constexpr int kSrcIter = (SRC_H * SRC_W + kBlurThreads - 1) / kBlurThreads;
+    constexpr int kSrcIter = (SRC_H * SRC_W + NT - 1) / NT;
     float v[kSrcIter];
 #pragma unroll
     for (int q = 0; q < kSrcIter; ++q) {
-      const int i = threadIdx.x + q * kBlurThreads;
+      const int i = threadIdx.x + q * NT;
       const int r = i / SRC_W, c = i - r * SRC_W;
       v[q] = 0.0f;
       if (i < SRC_H * SRC_W && r < sh && c < sw) {
@@ -275,7 +278,7 @@ __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ pl
     }
 #pragma unroll
     for (int q = 0; q < kSrcIter; ++q) {
-      const int i = threadIdx.x + q * kBlurThreads;
+      const int i = threadIdx.x + q * NT;
       if (i < SRC_H * SRC_W) s_tmp[i] = v[q];
     }
     __syncthreads();
@@ -339,14 +342,14 @@ __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ pl
     }
   };
   constexpr int kUnits = Gm::IN_PAIRS * Gm::C4;
-  for (int u0 = threadIdx.x; u0 < kUnits; u0 += kStageBatch * kBlurThreads) {
+  for (int u0 = threadIdx.x; u0 < kUnits; u0 += kStageBatch * NT) {
     float4 a[kStageBatch], b[kStageBatch];
 #pragma unroll
     for (int q = 0; q < kStageBatch; ++q)
-      if (u0 + q * kBlurThreads < kUnits) load_unit(u0 + q * kBlurThreads, a[q], b[q]);
+      if (u0 + q * NT < kUnits) load_unit(u0 + q * NT, a[q], b[q]);
 #pragma unroll
     for (int q = 0; q < kStageBatch; ++q) {
-      const int u = u0 + q * kBlurThreads;
+      const int u = u0 + q * NT;
       if (u < kUnits) {
         const int rp = u / Gm::C4, c4 = u - rp * Gm::C4;
         float4* d = reinterpret_cast<float4*>(s_in + rp * Gm::IN_S + 4 * c4);
@@ -365,7 +368,7 @@ __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ pl
     const int qi = lane & 7;
     const int rsub = qi / QX;
     const int xg = (lane >> 3) * QX + (qi % QX);
-    for (int rp = warp * QR + rsub; rp < Gm::IN_PAIRS; rp += (kBlurThreads / 32) * QR) {
+    for (int rp = warp * QR + rsub; rp < Gm::IN_PAIRS; rp += (NT / 32) * QR) {
       const float4* src = reinterpret_cast<const float4*>(s_in + rp * Gm::IN_S + HC * xg + OFF - SH);
       float2 acc[HC];
 #pragma unroll
@@ -400,7 +403,7 @@ __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ pl
   const bool do_down = (MODE == MODE_LEVEL) && level == down_level && octave + 1 < P.n_oct;
   const int x = 2 * lane;
   const int gx = tx0 + x;
-  for (int yb = warp * RV; yb < kTileH; yb += RV * (kBlurThreads / 32)) {
+  for (int yb = warp * RV; yb < TH; yb += RV * (NT / 32)) {
     if (ty0 + yb >= h) break;
     float2 acc[RV];
 #pragma unroll
@@ -455,11 +458,12 @@ __device__ __forceinline__ void blur_level_body(const ImagePlan* __restrict__ pl
   }
 }
 
-template <int R, int HC, int RV, int MODE, bool FUSED>
-__global__ void __launch_bounds__(kBlurThreads, 4) blur_level_kernel(const ImagePlan* __restrict__ plans, int octave,
-                                                                   int level, int down_level, int zrev, int pf_ahead,
-                                                                   const __grid_constant__ Taps2 taps) {
-  blur_level_body<R, HC, RV, MODE, FUSED, false>(plans, octave, level, down_level, zrev, pf_ahead, taps, nullptr);
+template <int R, int HC, int RV, int MODE, bool FUSED, int TH = kTileH, int NT = kBlurThreads>
+__global__ void __launch_bounds__(NT, NT == kBlurThreads ? 4 : 2)
+    blur_level_kernel(const ImagePlan* __restrict__ plans, int octave, int level, int down_level, int zrev,
+                      int pf_ahead, const __grid_constant__ Taps2 taps) {
+  blur_level_body<R, HC, RV, MODE, FUSED, false, TH, NT>(plans, octave, level, down_level, zrev, pf_ahead, taps,
+                                                         nullptr);
 }
 
 // The same over a tile work list (one CTA per listed tile).
@@ -470,19 +474,19 @@ __global__ void __launch_bounds__(kBlurThreads, 4)
   blur_level_body<R, HC, RV, MODE, FUSED, true>(plans, octave, level, down_level, zrev, pf_ahead, taps, &tiles);
 }
 
-template <int R, int HC, int RV, int MODE, bool FUSED, bool TILED>
+template <int R, int HC, int RV, int MODE, bool FUSED, bool TILED, int TH = kTileH, int NT = kBlurThreads>
 static cudaError_t launch_blur_r(const ImagePlan* plans, int n_images, int octave, int level, int down_level,
                                  int zrev, const Taps2& taps, const TileMap* tiles, int max_h, int max_w,
                                  cudaStream_t st) {
-  using Gm = BlurGeom<R>;
+  using Gm = BlurGeom<R, TH>;
   const size_t smem = Gm::SMEM_BYTES;
   const void* fn = TILED ? (const void*)blur_level_tiled_kernel<R, HC, RV, MODE, FUSED>
-                         : (const void*)blur_level_kernel<R, HC, RV, MODE, FUSED>;
+                         : (const void*)blur_level_kernel<R, HC, RV, MODE, FUSED, TH, NT>;
   cudaError_t e = ensure_smem_attr(fn, smem);
   if (e != cudaSuccess) return e;
   int pf_ahead = 0;
   if (MODE == MODE_LEVEL) {
-    e = resident_ctas(fn, kBlurThreads, smem, &pf_ahead);
+    e = resident_ctas(fn, NT, smem, &pf_ahead);
     if (e != cudaSuccess) return e;
     pf_ahead *= kPrefetchWaves;
   }
@@ -492,22 +496,22 @@ static cudaError_t launch_blur_r(const ImagePlan* plans, int n_images, int octav
                                                                                 down_level, zrev, pf_ahead, taps,
                                                                                 *tiles);
   } else {
-    const dim3 grid((max_w + kTileW - 1) / kTileW, (max_h + kTileH - 1) / kTileH, n_images);
-    blur_level_kernel<R, HC, RV, MODE, FUSED><<<grid, kBlurThreads, smem, st>>>(plans, octave, level, down_level,
-                                                                          zrev, pf_ahead, taps);
+    const dim3 grid((max_w + kTileW - 1) / kTileW, (max_h + TH - 1) / TH, n_images);
+    blur_level_kernel<R, HC, RV, MODE, FUSED, TH, NT><<<grid, NT, smem, st>>>(plans, octave, level, down_level,
+                                                                            zrev, pf_ahead, taps);
   }
   return cudaGetLastError();
 }
 
-template <int MODE, int HC, int RV, bool FUSED, bool TILED = false>
+template <int MODE, int HC, int RV, bool FUSED, bool TILED = false, int TH = kTileH, int NT = kBlurThreads>
 static cudaError_t launch_blur_mode(int radius, const ImagePlan* plans, int n, int octave, int level, int down_level,
                                     int zrev, const Taps2& taps, const TileMap* tiles, int max_h, int max_w,
                                     cudaStream_t st) {
   switch (radius) {
-#define PSIFT_R(RR)                                                                                          \
-  case RR:                                                                                                   \
-    return launch_blur_r<RR, HC, RV, MODE, FUSED, TILED>(plans, n, octave, level, down_level, zrev, taps, tiles, \
-                                                         max_h, max_w, st);
+#define PSIFT_R(RR)                                                                                              \
+  case RR:                                                                                                       \
+    return launch_blur_r<RR, HC, RV, MODE, FUSED, TILED, TH, NT>(plans, n, octave, level, down_level, zrev, taps, \
+                                                                 tiles, max_h, max_w, st);
     PSIFT_R(1) PSIFT_R(2) PSIFT_R(3) PSIFT_R(4) PSIFT_R(5) PSIFT_R(6) PSIFT_R(7) PSIFT_R(8)
     PSIFT_R(9) PSIFT_R(10) PSIFT_R(11) PSIFT_R(12) PSIFT_R(13) PSIFT_R(14) PSIFT_R(15)
 #undef PSIFT_R

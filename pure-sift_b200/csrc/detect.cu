@@ -641,7 +641,7 @@ psift_status detect_host(psift_ctx* ctx, const void* image, int kind, uint32_t h
 // when its time is under kBlurTuneMargin x variant 0's (3 % faster): the batch
 // entries run two chunks' stages concurrently on two streams, where smaller
 // gains measured alone did not carry over.  report: per distinct radius (radius, ms of each variant, chosen).
-constexpr int kBlurVariantCount = 4;  // 0-2: outputs per thread; 3: TMA tiles
+constexpr int kBlurVariantCount = 5;  // 0-2: outputs per thread; 3: TMA tiles; 4: 128-row tiles
 constexpr double kBlurTuneMargin = 0.97;
 psift_status autotune_blur(psift_ctx* ctx, uint32_t h, uint32_t w, uint32_t n, const psift_sift_config& cfg,
                            std::vector<double>& report) {

@@ -8,8 +8,10 @@ namespace psift {
 
 // Host entry: mode 0 = level blur (octave, level >= 1); modes 1..4 = octave-0 base.
 // variant (level blur only) picks the outputs per thread (0-2, see
-// blur_kernel.cuh) or the TMA-tile kernel (3, blur_tma.cuh; needs the host copy
-// of the plans for its tensor maps); every variant computes the same values.  fused: the single-rounding blur
+// blur_kernel.cuh), the TMA-tile kernel (3, blur_tma.cuh; needs the host copy
+// of the plans for its tensor maps) or 128 x 64 tiles of 512 threads (4: half
+// the horizontal pass's halo rows per output); every variant computes the same
+// values.  fused: the single-rounding blur
 // (one fused multiply-add per tap; not the reference's rounding).
 cudaError_t launch_blur_tma(int radius, bool fused, const ImagePlan* d_plans, const ImagePlan* h_plans, int n,
                             int octave, int level, int down_level, int zrev, const Taps2& taps, uint32_t* err,
@@ -38,6 +40,9 @@ cudaError_t launch_blur(int mode, const float* taps_host, int radius, const Imag
         case 0: return launch_blur_mode<MODE_LEVEL, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
         case 1: return launch_blur_mode<MODE_LEVEL, 8, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
         case 2: return launch_blur_mode<MODE_LEVEL, 4, 4, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);
+        case 4:  // 128-row tiles, 512 threads
+          return launch_blur_mode<MODE_LEVEL, 4, 8, false, false, 128, 512>(radius, plans, n, octave, level, down_level,
+                                                                            zrev, t, nullptr, max_h, max_w, st);
         default: return cudaErrorInvalidValue;
       }
     case MODE_INIT_F32: return launch_blur_mode<MODE_INIT_F32, 4, 8, false>(radius, plans, n, octave, level, down_level, zrev, t, nullptr, max_h, max_w, st);

@@ -352,8 +352,9 @@ class Context:
         self.check(self.lib.psift_ctx_enable_stage_timing(self.handle, int(on)))
 
     TUNE_BLUR, TUNE_MATCH_FP32, TUNE_MATCH_TC = 0, 1, 2
-    # level-blur variants: 0-2 outputs per thread (4x8, 8x8, 4x4), 3 TMA tiles (persistent CTAs)
-    BLUR_VARIANTS = 4
+    # level-blur variants: 0-2 outputs per thread (4x8, 8x8, 4x4), 3 TMA tiles (persistent CTAs),
+    # 4 128-row tiles of 512 threads
+    BLUR_VARIANTS = 5
 
     def autotune(self, height: int, width: int, n_images: int, config: "SiftConfig" = None, n_desc: int = 4096,
                  n_pairs: int = 8) -> dict:

@@ -17,7 +17,7 @@ def _same_features(a, b):
         np.testing.assert_array_equal(getattr(a, k), getattr(b, k), err_msg=k)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 def test_blur_variants_equal_default_and_oracle(variant):
     img = O.luma_to_f32(synth.blob_image(333, 251, 90, 1.5, 10.0, seed=41))
     cfg = psift.SiftConfig().with_octaves(4).with_scales(4)
@@ -68,7 +68,7 @@ def test_autotune_picks_valid_choices_and_keeps_results():
     rep = ctx.autotune(480, 640, 2, cfg, n_desc=1024, n_pairs=2)
     assert set(rep["blur"]) == {4, 5, 6, 8, 10}  # the default schedule's level radii
     for r, e in rep["blur"].items():
-        assert e["variant"] in (0, 1, 2, 3) and len(e["ms"]) == 4 and min(e["ms"]) > 0
+        assert e["variant"] in (0, 1, 2, 3, 4) and len(e["ms"]) == 5 and min(e["ms"]) > 0
         assert ctx.tuning()["blur"][r] == e["variant"]
     assert rep["match_fp32"]["per_sm"] in (1, 2, 4, 8) and rep["match_tc"]["per_sm"] in (1, 2, 4, 8)
     tun = ctx.tuning()
