@@ -144,6 +144,47 @@ def pyramid_bytes_per_image(h: int, w: int) -> tuple[float, int]:
     return total, launches
 
 
+def _blur_radius(sigma: float) -> int:
+    # gaussian_kernel_1d's radius: ceil(3 sigma), at least 1 (f32 on the host)
+    cs = float(np.float32(max(sigma, 1e-3)))
+    return max(1, int(np.ceil(np.float32(3.0) * np.float32(cs))))
+
+
+def pyramid_fp32_ops_per_image(h: int, w: int) -> tuple[float, float]:
+    """FP32 lane operations of the pyramid stage for one image: (reference rounding,
+    single rounding).  Each blur tap is a rounded multiply and a rounded add (one
+    fused multiply-add in the single-rounding mode); the horizontal pass of a 64 x 64
+    tile also covers the 2R halo rows, so it costs (64 + 2R) / 64 of the vertical
+    one; the DoG is one subtraction per pixel; the octave base adds the bilinear
+    upsampling's three adds and a multiply.  Radii of the schedule's incremental
+    sigmas (base 1.6, the input's 0.5 doubled by the upsampling)."""
+    k = np.float32(2.0) ** (np.float32(1.0) / np.float32(SCALES))
+    radii, prev = [], np.float32(1.6)
+    for s in range(1, SCALES + 3):
+        target = np.float32(1.6) * k ** s
+        radii.append(_blur_radius(np.sqrt(max(target * target - prev * prev, 1e-4))))
+        prev = target
+    r0 = _blur_radius(np.sqrt(max(1.6 * 1.6 - 1.0, 1e-4)))
+
+    def per_px(r: int, fused: bool) -> float:
+        taps = 2 * r + 1
+        per_tap = 1.0 if fused else 2.0
+        return per_tap * taps * (64 + 2 * r) / 64 + per_tap * taps
+
+    ref = fused = 0.0
+    hh, ww = 2 * h, 2 * w
+    ref += hh * ww * (per_px(r0, False) + 4.0)
+    fused += hh * ww * (per_px(r0, True) + 4.0)
+    for o in range(OCTAVES):
+        if hh < 3 or ww < 3:
+            break
+        for r in radii:
+            ref += hh * ww * (per_px(r, False) + 1.0)
+            fused += hh * ww * (per_px(r, True) + 1.0)
+        hh, ww = hh // 2, ww // 2
+    return ref, fused
+
+
 def cpu_reference(steps: int, warmup: int, budget_s: float):
     """Time the CPU restatement (OpenMP over all host cores) on 1080p images."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -1023,6 +1064,10 @@ def run_ours(args):
     bytes_per_launch = B * bytes_img / blur_launches
     achieved = bytes_per_launch / avg_launch_s / 1e9
     peak, peak_kind = peaks()
+    # the same stage against the FP32 pipe: lane operations over the stage time,
+    # peak = SMs x 128 FP32 lanes x the SM clock seen under load
+    ops_ref, ops_fused = pyramid_fp32_ops_per_image(HEIGHT, WIDTH)
+    n_sms = torch.cuda.get_device_properties(0).multi_processor_count
 
     # The single-rounding blur mode (PSIFT_BLUR_FUSED: one fused multiply-add per
     # tap; not bit-equal to the reference, held to the f32 path's tolerances
@@ -1058,6 +1103,19 @@ def run_ours(args):
                      "avg_launch_ms": fused_launch_s * 1e3},
         "note": "PSIFT_BLUR_FUSED: one fused multiply-add per blur tap; error against an f64 run within 0.01 px / "
                 "0.01 scale / 1e-4 descriptor L2 (tests/test_blur_fused_gpu.py), not bit-equal to the reference"}
+    clocks = clk.summary()
+    mhz = clocks.get("sm_mhz") or 1965.0
+    fp32_peak = n_sms * 128 * mhz * 1e6 / 1e12
+
+    def fp32_view(ops_img: float, stage_ms: float, kernel: str) -> dict:
+        achieved_t = B * ops_img / (stage_ms / 1e3) / 1e12
+        return {"kernel": kernel, "bound": "fp32", "achieved": achieved_t, "peak": fp32_peak,
+                "unit": "T lane-ops/s", "frac": achieved_t / fp32_peak, "ops_per_image": ops_img,
+                "peak_source": f"nominal: {n_sms} SMs x 128 FP32 lanes x {mhz:.0f} MHz (median SM clock in the "
+                               "timed region)"}
+    roofline_fp32 = fp32_view(ops_ref, pyr_ms / reps, "pyramid stage, reference rounding (2 rounded ops per tap)")
+    blur_fused["roofline_fp32"] = fp32_view(ops_fused, st_f["pyramid"][0] / reps,
+                                            "pyramid stage, single rounding (1 fused op per tap)")
 
     # End to end through the public host-pointer API: the batch entry with page-locked
     # images and outputs (every step uploads the 8 images and downloads all features).
@@ -1170,9 +1228,10 @@ def run_ours(args):
                          "peak_source": peak_kind, "traffic": NCU_TRAFFIC_BLUR_LEVEL,
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": avg_launch_s * 1e3},
+            "roofline_fp32": roofline_fp32,
             "stage_ms_per_step": {k: v[0] / reps for k, v in st.items() if v[1]},
             "blur_fused": blur_fused,
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
         for key, fn in (("uneven_batch", uneven_bench), ("catalog", catalog_bench),
                         ("catalog_search", catalog_search_bench), ("warp", warp_bench),
