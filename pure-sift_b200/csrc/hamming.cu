@@ -205,29 +205,94 @@ __global__ void __launch_bounds__(256) votes_kernel(const uint4* __restrict__ q,
   }
 }
 
-__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    const unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
-    v = t > v ? t : v;
-  }
-  return v;
-}
-
 // Per (16-query group, code chunk): the k smallest (distance, index) keys.
 // Grid (n_chunks, ceil(n_groups / kHamWarps)), kHamWarps warps per block.
-__global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4* __restrict__ q, int nq,
-                                                                     const uint4* __restrict__ cat, long long ncat,
-                                                                     int k, int n_chunks,
-                                                                     unsigned long long* __restrict__ part) {
-  __shared__ unsigned long long s_list[kHamWarps][kQG][kTopKMax];
+//
+// Each query keeps its list sorted, entries [k, 64) at ~0, and maxd = the
+// distance of its k-th key.  Within a chunk the codes come in increasing index,
+// so every listed entry has a smaller index than the current code: a code can
+// only enter when its distance is below maxd.  Such codes are appended to the
+// query's buffer (up to kTopKBuf keys); a full buffer (and the buffer at the end
+// of the chunk) is merged into the list: the buffer sorted across the warp's
+// lanes, each key's place in the merged order found by binary search in the
+// other sorted sequence (ties: the list's key first; only the empty ~0 keys tie),
+// the first k kept.  A candidate that passed against an older maxd and no longer
+// belongs falls out at its merge.
+constexpr int kTopKBuf = 32;
+constexpr size_t kTopKWarpSmem = (size_t)kQG * (kTopKMax + kTopKBuf) * 8 + kTopKMax * 8 + kQG * 4;
+
+__device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int o) {
+  return __shfl_xor_sync(0xffffffffu, v, o);
+}
+
+// Merges buf[0..n) into the sorted list (k entries kept); returns the new k-th distance.
+__device__ __forceinline__ uint32_t topk_merge_buffer(unsigned long long* list, unsigned long long* buf, int n,
+                                                      int k, unsigned long long* scratch, int lane) {
+  __syncwarp();
+  // sort the buffer across the lanes (ascending; missing entries ~0)
+  unsigned long long v = lane < n ? buf[lane] : ~0ull;
+#pragma unroll
+  for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      const unsigned long long o = shfl_xor_u64(v, j);
+      const bool up = (lane & kk) == 0, low = (lane & j) == 0;
+      v = (low == up) ? (o < v ? o : v) : (o > v ? o : v);
+    }
+  }
+  buf[lane] = v;
+  __syncwarp();
+  // buffer key at lane: rank = lane + (list keys <= it)
+  {
+    int lo = 0, hi = kTopKMax;  // first list index with key > v
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (list[mid] <= v) lo = mid + 1;
+      else hi = mid;
+    }
+    const int r = lane + lo;
+    if (r < k) scratch[r] = v;
+  }
+  // list keys at lane and lane + 32: rank = i + (buffer keys < it)
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int i = lane + 32 * h;
+    const unsigned long long x = list[i];
+    int lo = 0, hi = 32;  // first buffer index with key >= x
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (buf[mid] < x) lo = mid + 1;
+      else hi = mid;
+    }
+    const int r = i + lo;
+    if (r < k) scratch[r] = x;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int i = lane + 32 * h;
+    if (i < k) list[i] = scratch[i];
+  }
+  __syncwarp();
+  return (uint32_t)(list[k - 1] >> 32);
+}
+
+__global__ void __launch_bounds__(kHamWarps * 32, 4) topk_chunk_kernel(const uint4* __restrict__ q, int nq,
+                                                                        const uint4* __restrict__ cat, long long ncat,
+                                                                        int k, int n_chunks,
+                                                                        unsigned long long* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned long long s_topk[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int group = blockIdx.y * kHamWarps + warp;
   const int q0 = group * kQG;
   if (q0 >= nq) return;
   const int chunk = blockIdx.x;
   const long long c_begin = ncat * chunk / n_chunks, c_end = ncat * (chunk + 1) / n_chunks;
-  unsigned long long(*list)[kTopKMax] = s_list[warp];
+  unsigned long long* wbase = s_topk + (size_t)warp * (kTopKWarpSmem / 8);
+  unsigned long long(*list)[kTopKMax] = reinterpret_cast<unsigned long long(*)[kTopKMax]>(wbase);
+  unsigned long long(*buf)[kTopKBuf] = reinterpret_cast<unsigned long long(*)[kTopKBuf]>(wbase + kQG * kTopKMax);
+  unsigned long long* scratch = wbase + kQG * (kTopKMax + kTopKBuf);
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(scratch + kTopKMax);
   uint32_t qw[kQG][4];
 #pragma unroll
   for (int j = 0; j < kQG; ++j) {
@@ -237,19 +302,16 @@ __global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4*
     qw[j][2] = v.z;
     qw[j][3] = v.w;
   }
-  // Within a chunk the codes come in increasing index, so every listed entry has
-  // a smaller index than the current code: key < max key is exactly
-  // distance < max distance (the empty entries have distance 2^32 - 1).  Only
-  // the distance is compared per pair; keys are built on insertion.
   uint32_t maxd[kQG];
-  int maxpos[kQG];
 #pragma unroll
   for (int j = 0; j < kQG; ++j) {
-    for (int t = lane; t < kTopKMax; t += 32) list[j][t] = t < k ? ~0ull : 0ull;
+    list[j][lane] = ~0ull;
+    list[j][lane + 32] = ~0ull;
     maxd[j] = 0xFFFFFFFFu;
-    maxpos[j] = 0;
   }
+  if (lane < kQG) cnt[lane] = 0;
   __syncwarp();
+  const unsigned lt = (1u << lane) - 1u;
   // the next 32 codes are loaded while the current ones are compared
   uint4 c_next = c_begin + lane < c_end ? cat[c_begin + lane] : make_uint4(0, 0, 0, 0);
   for (long long base = c_begin; base < c_end; base += 32) {
@@ -260,33 +322,27 @@ __global__ void __launch_bounds__(kHamWarps * 32) topk_chunk_kernel(const uint4*
 #pragma unroll
     for (int j = 0; j < kQG; ++j) {
       const uint32_t d = (uint32_t)ham128(qw[j][0], qw[j][1], qw[j][2], qw[j][3], c);
-      unsigned m = __ballot_sync(0xffffffffu, valid && d < maxd[j]);
-      while (m) {
-        const int L = __ffs(m) - 1;
-        m &= m - 1;
-        const uint32_t dl = __shfl_sync(0xffffffffu, d, L);
-        if (dl < maxd[j]) {
-          const unsigned long long kl = ((unsigned long long)dl << 32) | (unsigned long long)(uint32_t)(base + L);
-          if (lane == 0) list[j][maxpos[j]] = kl;
-          __syncwarp();
-          // new maximum of the k entries (slots >= k hold 0 and never win)
-          unsigned long long a = list[j][lane], b = list[j][lane + 32];
-          unsigned long long mine = a > b ? a : b;
-          const int mine_pos = a > b ? lane : lane + 32;
-          const unsigned long long mx = warp_max_u64(mine);
-          const unsigned who = __ballot_sync(0xffffffffu, mine == mx);
-          const int src = __ffs(who) - 1;
-          maxpos[j] = __shfl_sync(0xffffffffu, mine_pos, src);
-          maxd[j] = (uint32_t)(mx >> 32);
-          __syncwarp();
+      const unsigned m = __ballot_sync(0xffffffffu, valid && d < maxd[j]);
+      if (m) {
+        const int nc = __popc(m);
+        int n = (int)cnt[j];
+        if (n + nc > kTopKBuf) {
+          maxd[j] = topk_merge_buffer(list[j], buf[j], n, k, scratch, lane);
+          n = 0;
         }
+        if (m & (1u << lane))
+          buf[j][n + __popc(m & lt)] = ((unsigned long long)d << 32) | (unsigned long long)(uint32_t)idx;
+        __syncwarp();
+        if (lane == 0) cnt[j] = (uint32_t)(n + nc);
+        __syncwarp();
       }
     }
   }
-  // write this chunk's lists: part[(query * n_chunks + chunk) * k + t]
+  // the buffers' last keys, then this chunk's lists: part[(query * n_chunks + chunk) * k + t]
 #pragma unroll
   for (int j = 0; j < kQG; ++j) {
-    if (q0 + j >= nq) break;
+    if (cnt[j] > 0) topk_merge_buffer(list[j], buf[j], (int)cnt[j], k, scratch, lane);
+    if (q0 + j >= nq) continue;
     unsigned long long* dst = part + ((long long)(q0 + j) * n_chunks + chunk) * k;
     for (int t = lane; t < k; t += 32) dst[t] = list[j][t];
   }
@@ -502,8 +558,12 @@ cudaError_t launch_topk(const uint64_t* q, int nq, const uint64_t* cat, long lon
   if (nq <= 0) return cudaSuccess;
   const int groups = (nq + kQG - 1) / kQG;
   dim3 g1(n_chunks, (groups + kHamWarps - 1) / kHamWarps);
-  topk_chunk_kernel<<<g1, kHamWarps * 32, 0, st>>>((const uint4*)q, nq, (const uint4*)cat, ncat, k, n_chunks, part);
-  cudaError_t e = cudaGetLastError();
+  const size_t smem1 = kHamWarps * kTopKWarpSmem;
+  cudaError_t e = ensure_smem_attr((const void*)topk_chunk_kernel, smem1);
+  if (e != cudaSuccess) return e;
+  topk_chunk_kernel<<<g1, kHamWarps * 32, smem1, st>>>((const uint4*)q, nq, (const uint4*)cat, ncat, k, n_chunks,
+                                                      part);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   int n2 = 1;
   while (n2 < n_chunks * k) n2 <<= 1;
