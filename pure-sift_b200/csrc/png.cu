@@ -58,7 +58,8 @@ struct PngImage {
   size_t pass_rb[7] = {0};         // bytes per row, filter byte excluded
   size_t pass_in[7] = {0};         // offset of the pass's row slots in the inflated buffer
   size_t pass_stride[7] = {0};     // bytes per row slot: filter byte at +15, the row at +16 (16-byte aligned)
-  size_t pass_out[7] = {0};        // offset of the pass in the unfiltered buffer
+  size_t pass_out[7] = {0};        // offset of the pass in the unfiltered buffer (16-byte aligned)
+  size_t pass_ostride[7] = {0};    // bytes per unfiltered row: the row rounded up to 16
   size_t raw_bytes = 0, unf_bytes = 0;
 };
 
@@ -150,9 +151,10 @@ psift_status parse_png(psift_ctx* ctx, const uint8_t* data, size_t len, bool enf
     P->pass_in[p] = in;
     P->pass_out[p] = out;
     P->pass_stride[p] = align_up(P->pass_rb[p], 16) + 16;
+    P->pass_ostride[p] = align_up(P->pass_rb[p], 16);
     if (P->pass_rb[p]) {
       in += (size_t)ph * P->pass_stride[p];
-      out += (size_t)ph * P->pass_rb[p];
+      out += (size_t)ph * P->pass_ostride[p];
     }
   }
   P->raw_bytes = in;
@@ -200,10 +202,11 @@ std::string inflate_png(const PngImage& P, uint8_t* dst) {
 // ------------------------------------------------------------------ kernels
 struct PngPlane {
   const uint8_t* in;  // row slots: filter byte at +15 (checked on the host), the filtered row at +16
-  uint8_t* out;       // rows x row_bytes
+  uint8_t* out;       // rows of row_bytes at ostride
   uint32_t rows;
   uint32_t row_bytes;
   uint32_t stride;    // bytes per row slot (a multiple of 16)
+  uint32_t ostride;   // bytes per unfiltered row (row_bytes rounded up to 16)
 };
 
 // Adam7 constants of pass p as nibble p of a word (device code).
@@ -260,8 +263,8 @@ __global__ void __launch_bounds__(32 * kUnfWarps) png_unfilter_kernel(const PngP
     const uint8_t* slot = P.in + (size_t)r * P.stride;
     const uint32_t f = row_ok ? slot[15] : 0u;
     const uint8_t* src = slot + 16;
-    uint8_t* dst = P.out + (size_t)r * rb;
-    const uint8_t* above_g = (g > 0) ? P.out + (size_t)(g - 1) * rb : nullptr;  // row g - 1 (lane 0's above)
+    uint8_t* dst = P.out + (size_t)r * P.ostride;
+    const uint8_t* above_g = (g > 0) ? P.out + (size_t)(g - 1) * P.ostride : nullptr;  // row g - 1 (lane 0's above)
     const unsigned long long* prev = progress + (k + kUnfWarps - 1) % kUnfWarps;
     unsigned long long* mine = progress + warp;
     // chunk c of this lane's row into ring slot c % 4 (16-byte copies inside the row slot)
@@ -273,6 +276,14 @@ __global__ void __launch_bounds__(32 * kUnfWarps) png_unfilter_kernel(const PngP
                        "l"(src + c * 128 + 16 * q)
                        : "memory");
       asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    // chunk c of this lane's reconstructed row (written over its filtered bytes in
+    // the ring) to the output row as 16-byte stores; rows are padded to 16 bytes
+    auto flush = [&](uint32_t c) {
+      if (!row_ok || c >= nchunks) return;
+      const uint4* from = reinterpret_cast<const uint4*>(my_ring + (c & 3) * 128);
+      for (uint32_t q = 0; q < 8 && c * 128 + 16 * q < rb16; ++q)
+        *reinterpret_cast<uint4*>(dst + c * 128 + 16 * q) = from[q];
     };
     fetch(0);
     fetch(1);
@@ -317,6 +328,9 @@ __global__ void __launch_bounds__(32 * kUnfWarps) png_unfilter_kernel(const PngP
         const uint32_t lead = min(s, npix - 1) * UNIT + UNIT - 1;
         if ((lead >> 7) != cur) {
           cur = lead >> 7;
+          // every lane is past chunk cur - 3 (lane 31 trails lane 0 by at most 248
+          // bytes): it leaves the ring before chunk cur + 1 takes its slot
+          if (cur >= 3) flush(cur - 3);
           fetch(cur + 1);
           asm volatile("cp.async.wait_group 1;" ::: "memory");
           __syncwarp();
@@ -351,7 +365,10 @@ __global__ void __launch_bounds__(32 * kUnfWarps) png_unfilter_kernel(const PngP
             const uint32_t pred =
                 f == 1 ? av : f == 2 ? bv : f == 3 ? (av + bv) >> 1 : f == 4 ? paeth(av, bv, cv) : 0u;
             const uint8_t v = (uint8_t)(x + pred);
-            dst[(size_t)i * UNIT + q] = v;
+            my_ring[((uint32_t)i * UNIT + q) & (kRing - 1)] = v;
+            // the group's last row also goes out byte by byte: the next group reads it
+            // as soon as its progress is published
+            if (lane == 31) dst[(size_t)i * UNIT + q] = v;
             a[q] = v;
             c[q] = (uint8_t)bv;
             mine_prev[q] = v;
@@ -369,6 +386,9 @@ __global__ void __launch_bounds__(32 * kUnfWarps) png_unfilter_kernel(const PngP
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncwarp();
+    // the chunks still in the ring
+    for (uint32_t c = cur >= 2 ? cur - 2 : 0; c <= cur; ++c) flush(c);
+    __syncwarp();
   }
 }
 
@@ -378,6 +398,7 @@ struct PngLumaJob {
   const uint8_t* plte;    // 256 RGB triples (zero past the file's palette)
   uint32_t w, h;
   uint32_t pass_rb[7];
+  uint32_t pass_ostride[7];
   uint32_t pass_out[7];
   int depth, color, interlace;
 };
@@ -408,7 +429,7 @@ __global__ void png_luma_kernel(const PngLumaJob* __restrict__ jobs) {
     px = (x - a7(kA7X0w, p)) / a7(kA7DXw, p);
     py = (y - a7(kA7Y0w, p)) / a7(kA7DYw, p);
   }
-  const uint8_t* row = J.unf + J.pass_out[p] + (size_t)py * J.pass_rb[p];
+  const uint8_t* row = J.unf + J.pass_out[p] + (size_t)py * J.pass_ostride[p];
   const int d = J.depth;
   uint32_t L;
   if (J.color == 0 || J.color == 3) {
@@ -593,7 +614,8 @@ psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, co
       for (int p = 0; p < I.n_pass; ++p) {
         if (!I.pass_rb[p]) continue;
         hp[np++] = PngPlane{S->dev + L.dev_raw[i] + I.pass_in[p], S->dev + L.dev_unf[i] + I.pass_out[p],
-                            I.pass_h[p], (uint32_t)I.pass_rb[p], (uint32_t)I.pass_stride[p]};
+                            I.pass_h[p], (uint32_t)I.pass_rb[p], (uint32_t)I.pass_stride[p],
+                            (uint32_t)I.pass_ostride[p]};
         ++count[u];
       }
     }
@@ -612,6 +634,7 @@ psift_status decode_png_range(psift_ctx* ctx, const std::vector<PngImage>& P, co
     J.h = I.h;
     for (int p = 0; p < 7; ++p) {
       J.pass_rb[p] = (uint32_t)I.pass_rb[p];
+      J.pass_ostride[p] = (uint32_t)I.pass_ostride[p];
       J.pass_out[p] = (uint32_t)I.pass_out[p];
     }
     J.depth = I.depth;
