@@ -306,8 +306,9 @@ __global__ void __launch_bounds__(1024) feature_scan_kernel(const ImagePlan* __r
 // square (the reference's r_bin/c_bin test; about half of the window passes) and
 // the passing ones are compacted into the warp's queue; phase 2: full lanes take
 // queued pixels for the gradient, weight and trilinear binning.  Histograms: 16
-// private columns per warp ([bin][16], 8 KB); lanes l and l + 16 share column l
-// and add in two fixed phases.  Bin b's value is the sum over (warp, column) in a
+// private columns per warp ([bin][16], 8 KB); the pixels of lanes l and l + 16 both
+// go to column l, in two fixed rounds in which the two lanes split each pixel's
+// cells (see the binning loop).  Bin b's value is the sum over (warp, column) in a
 // fixed order, so the result does not depend on scheduling (deterministic).
 constexpr int kDescChunk = 256;
 constexpr int kHistCols = 16;
@@ -444,25 +445,36 @@ __device__ void describe_one(const ImagePlan& P, const DescribeParams& prm, uint
         // and every bin starts at +0, so adding +0 leaves the bin unchanged and
         // the real contributions keep their order.
         if (!live) wm = 0.0f;
+        // Two rounds, all lanes busy: round 0 bins the pixels of lanes 0-15, round 1
+        // those of lanes 16-31.  In each, the pixel's own lane adds its row-bin r0
+        // cells and the partner lane (lane ^ 16) its row-bin r0 + 1 cells, both into
+        // the pixel's column (lane & 15).  The two lanes' cells are never the same
+        // address in one instruction: their row bins differ, and a row bin outside
+        // the grid (+0 added) is sent to row 3 (own lane) or row 0 (partner), which
+        // the other lane's valid row cannot be.
+        const int pr0 = __shfl_xor_sync(0xffffffffu, r0, 16), pc0 = __shfl_xor_sync(0xffffffffu, c0, 16);
+        const int po0 = __shfl_xor_sync(0xffffffffu, o0, 16);
+        const float pdr = __shfl_xor_sync(0xffffffffu, dr, 16), pdc = __shfl_xor_sync(0xffffffffu, dc, 16);
+        const float pdof = __shfl_xor_sync(0xffffffffu, dof, 16), pwm = __shfl_xor_sync(0xffffffffu, wm, 16);
 #pragma unroll
-        for (int hp = 0; hp < 2; ++hp) {
-          if (half == hp) {
+        for (int rnd = 0; rnd < 2; ++rnd) {
+          const bool own = half == rnd;
+          const int R0 = own ? r0 : pr0, C0 = own ? c0 : pc0, O0 = own ? o0 : po0;
+          const float DR = own ? dr : pdr, DC = own ? dc : pdc, DOF = own ? dof : pdof, WM = own ? wm : pwm;
+          const int ir = own ? 0 : 1;
+          const int rb = R0 + ir;
+          const bool vr = (unsigned)rb < 4u;
+          const float wr = vr ? (ir == 0 ? 1.0f - DR : DR) : 0.0f;
+          const int row = vr ? rb : (own ? 3 : 0);
 #pragma unroll
-            for (int ir = 0; ir <= 1; ++ir) {
-              const int rb = r0 + ir;
-              const bool vr = (unsigned)rb < 4u;
-              const float wr = vr ? (ir == 0 ? 1.0f - dr : dr) : 0.0f;
-#pragma unroll
-              for (int ic = 0; ic <= 1; ++ic) {
-                const int cb = c0 + ic;
-                const bool vc = (unsigned)cb < 4u;
-                const float wc = vc ? (ic == 0 ? 1.0f - dc : dc) : 0.0f;
-                float* cell = &hist[((vr ? rb : 0) * 4 + (vc ? cb : 0)) * 8][col];
-                const float wrc = wm * wr * wc;
-                cell[(o0 & 7) * kHistCols] += wrc * (1.0f - dof);
-                cell[((o0 + 1) & 7) * kHistCols] += wrc * dof;
-              }
-            }
+          for (int ic = 0; ic <= 1; ++ic) {
+            const int cb = C0 + ic;
+            const bool vc = (unsigned)cb < 4u;
+            const float wc = vc ? (ic == 0 ? 1.0f - DC : DC) : 0.0f;
+            float* cell = &hist[(row * 4 + (vc ? cb : 0)) * 8][col];
+            const float wrc = WM * wr * wc;
+            cell[(O0 & 7) * kHistCols] += wrc * (1.0f - DOF);
+            cell[((O0 + 1) & 7) * kHistCols] += wrc * DOF;
           }
           __syncwarp();
         }
