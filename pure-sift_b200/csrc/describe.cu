@@ -151,8 +151,15 @@ __device__ void orient_one(const ImagePlan& P, const DescribeParams& prm, uint32
   const int wx = x_max - x_min + 1;
   const int n = (y_max >= y_min && x_max >= x_min) ? (y_max - y_min + 1) * wx : 0;
   const bool planes_ok = O.h >= 3 && O.w >= 3;
-  for (int t = lane; planes_ok && t < n; t += 32) {
-    const int yy = y_min + t / wx, xx = x_min + t % wx;
+  // lane's pixel t = lane, lane + 32, ...: its (row, column) stepped by 32 pixels
+  // (q32 whole rows plus r32 columns, at most one wrap) instead of a division each
+  const int q32 = wx > 0 ? 32 / wx : 0, r32 = wx > 0 ? 32 - q32 * wx : 0;
+  int yy = wx > 0 ? y_min + lane / wx : 0, xx = wx > 0 ? x_min + lane % wx : 0;
+  for (int t = lane; planes_ok && t < n; t += 32, xx += r32, yy += q32) {
+    if (xx > x_max) {
+      xx -= wx;
+      ++yy;
+    }
     const float dy = (float)(yy - cy), dx = (float)(xx - cx);
     const float r_sq = dx * dx + dy * dy;
     if (r_sq > r_sq_max) continue;
