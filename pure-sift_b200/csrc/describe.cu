@@ -378,6 +378,10 @@ __device__ void describe_one(const ImagePlan& P, const DescribeParams& prm, uint
     for (int b = lane; b < kDescLen * kHistCols / 4; b += 32)
       reinterpret_cast<float4*>(&hist[0][0])[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float cos_t = cosf(theta), sin_t = sinf(theta);
+    // phase 1's square test only: the rotated bins by two fused steps each (a pixel
+    // that this moves across the square's edge has a weight of about 0 there: its
+    // trilinear share in the edge cell is the distance past the edge)
+    const float ci = cos_t * inv_hw, si = sin_t * inv_hw;
     for (int base = warp * kDescChunk; base < n; base += kDescWarps * kDescChunk) {
       // Phase 1: rotated-square test for 8 pixels per lane.
       const int t0 = base + lane;
@@ -398,8 +402,8 @@ __device__ void describe_one(const ImagePlan& P, const DescribeParams& prm, uint
         if (t < n) {
           const float dy = (float)py - ok.y;
           const float dx = (float)px - ok.x;
-          const float r_bin = (dx * cos_t + dy * sin_t) * inv_hw + 4.0f * 0.5f - 0.5f;
-          const float c_bin = (-dx * sin_t + dy * cos_t) * inv_hw + 4.0f * 0.5f - 0.5f;
+          const float r_bin = __fmaf_rn(dx, ci, __fmaf_rn(dy, si, 1.5f));
+          const float c_bin = __fmaf_rn(-dx, si, __fmaf_rn(dy, ci, 1.5f));
           if (!(r_bin <= -1.0f || r_bin >= 4.0f || c_bin <= -1.0f || c_bin >= 4.0f)) m |= 1u << k;
         }
       }
