@@ -90,17 +90,15 @@ __device__ __forceinline__ bool accept_pixel(const float* __restrict__ p, const 
                                              const float* __restrict__ n, long long pitch, int x, float thr) {
   const float v = c[x];
   if (fabsf(v) <= thr) return false;
+  // All 26 neighbours are loaded before the first test: a warp's candidates are
+  // tested together, so one of them passing the same-slice test would otherwise
+  // make the whole warp wait for a second round of loads.
   const float* ca = c - pitch;
   const float* cb = c + pitch;
   float nb[9];
   nb[0] = ca[x - 1]; nb[1] = ca[x]; nb[2] = ca[x + 1];
   nb[3] = c[x - 1];  nb[4] = c[x + 1];
   nb[5] = cb[x - 1]; nb[6] = cb[x]; nb[7] = cb[x + 1];
-  const bool pos = v > 0.0f;
-  bool ext = true;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) ext = ext && (pos ? v > nb[k] : v < nb[k]);
-  if (!ext) return false;
   float pn[18];
   {
     const float* pa = p - pitch;
@@ -114,6 +112,11 @@ __device__ __forceinline__ bool accept_pixel(const float* __restrict__ p, const 
     pn[12] = n[x - 1];  pn[13] = n[x];  pn[14] = n[x + 1];
     pn[15] = nbp[x - 1]; pn[16] = nbp[x]; pn[17] = nbp[x + 1];
   }
+  const bool pos = v > 0.0f;
+  bool ext = true;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) ext = ext && (pos ? v > nb[k] : v < nb[k]);
+  if (!ext) return false;
 #pragma unroll
   for (int k = 0; k < 18; ++k) ext = ext && (pos ? v > pn[k] : v < pn[k]);
   if (!ext) return false;
